@@ -1,0 +1,293 @@
+"""ctypes front end of the oracle (``zipref``), the CPU restatement of the
+reference Zip+ path.  Test infrastructure only: imported by ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``.
+
+The shared library is built by ``oracle/Makefile`` into ``oracle/_build``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libzipref.so")
+
+EVAL_I32, EVAL_BINPOLY = 0, 1
+CODE_IPRS, CODE_RAA = 0, 1
+
+
+class Desc(C.Structure):
+    """Mirror of ``zr_desc`` (same fields as the product's ``zg_params_desc``)."""
+
+    _fields_ = [
+        ("eval_kind", C.c_uint32),
+        ("degree_plus_one", C.c_uint32),
+        ("code_kind", C.c_uint32),
+        ("rep", C.c_uint32),
+        ("num_vars", C.c_uint32),
+        ("row_len", C.c_uint32),
+        ("iprs_depth", C.c_uint32),
+        ("comb_limbs", C.c_uint32),
+        ("field_limbs", C.c_uint32),
+        ("num_openings", C.c_uint32),
+    ]
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        vp, u8p, sz = C.c_void_p, C.c_void_p, C.c_size_t
+        L.zr_blake3.argtypes = [vp, sz, vp]
+        L.zr_blake3_xof.argtypes = [vp, sz, vp, sz]
+        L.zr_blake3_parent.argtypes = [vp, vp, C.c_int, vp]
+        L.zr_blake3_chunk_cv.argtypes = [vp, sz, C.c_uint64, vp]
+        L.zr_octet_reversal.argtypes = [sz, sz]
+        L.zr_octet_reversal.restype = sz
+        L.zr_iprs_dims.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, vp]
+        L.zr_iprs_tables.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, vp, vp]
+        L.zr_roots_of_unity.argtypes = [C.c_uint32, vp]
+        L.zr_shuffle_identity.argtypes = [C.c_uint64, C.c_uint32, vp]
+        L.zr_stdrng_u32.argtypes = [C.c_uint64, C.c_uint32]
+        L.zr_stdrng_u32.restype = C.c_uint32
+        L.zr_encode_rows.argtypes = [C.POINTER(Desc), vp, vp]
+        L.zr_encode_wide.argtypes = [C.POINTER(Desc), vp, C.c_uint32, vp]
+        L.zr_cw_bytes.argtypes = [C.POINTER(Desc)]
+        L.zr_cw_bytes.restype = sz
+        L.zr_num_rows.argtypes = [C.POINTER(Desc)]
+        L.zr_num_rows.restype = C.c_uint32
+        L.zr_codeword_len.argtypes = [C.POINTER(Desc)]
+        L.zr_codeword_len.restype = C.c_uint32
+        L.zr_merkle_root_rows.argtypes = [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp]
+        L.zr_commit.argtypes = [C.POINTER(Desc), vp, C.c_uint32, vp]
+        L.zr_proof_size.argtypes = [C.POINTER(Desc), C.c_uint32]
+        L.zr_proof_size.restype = sz
+        L.zr_commit_prove.argtypes = [C.POINTER(Desc), vp, C.c_uint32, vp, vp, vp, sz,
+                                      C.POINTER(C.c_size_t), vp, vp]
+        L.zr_verify.argtypes = [C.POINTER(Desc), vp, C.c_uint32, vp, vp, vp, sz]
+        L.zr_tr_new.restype = vp
+        L.zr_tr_free.argtypes = [vp]
+        L.zr_tr_absorb.argtypes = [vp, vp, sz]
+        L.zr_tr_absorb_slice.argtypes = [vp, vp, sz]
+        L.zr_tr_challenge.argtypes = [vp, vp, sz]
+        L.zr_tr_get_prime.argtypes = [vp, C.c_uint32, vp]
+        L.zr_is_probable_prime_base2.argtypes = [vp, C.c_uint32]
+        L.zr_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _buf(b: bytes):
+    return C.c_char_p(b)
+
+
+def make_desc(eval_kind, D, code_kind, num_vars, row_len, depth=0, comb_limbs=None,
+              field_limbs=4, num_openings=147, rep=4) -> Desc:
+    if comb_limbs is None:
+        comb_limbs = 3 if eval_kind == EVAL_I32 else 5
+    return Desc(eval_kind, D if eval_kind == EVAL_BINPOLY else 1, code_kind, rep, num_vars,
+                row_len, depth, comb_limbs, field_limbs, num_openings)
+
+
+def set_threads(n: int) -> None:
+    lib().zr_set_threads(int(n))
+
+
+def blake3(data: bytes) -> bytes:
+    out = C.create_string_buffer(32)
+    lib().zr_blake3(_buf(data), len(data), out)
+    return out.raw
+
+
+def blake3_xof(data: bytes, n: int) -> bytes:
+    out = C.create_string_buffer(n)
+    lib().zr_blake3_xof(_buf(data), len(data), out, n)
+    return out.raw
+
+
+def blake3_parent(left: bytes, right: bytes, root: bool) -> bytes:
+    out = C.create_string_buffer(32)
+    lib().zr_blake3_parent(_buf(left), _buf(right), int(root), out)
+    return out.raw
+
+
+def blake3_chunk_cv(data: bytes, counter: int) -> bytes:
+    out = C.create_string_buffer(32)
+    lib().zr_blake3_chunk_cv(_buf(data), len(data), counter, out)
+    return out.raw
+
+
+def octet_reversal(x: int, n: int) -> int:
+    return lib().zr_octet_reversal(x, n)
+
+
+def iprs_dims(row_len, depth, rep=4):
+    out = np.zeros(4, np.uint32)
+    if lib().zr_iprs_dims(row_len, depth, rep, _ptr(out)):
+        return None
+    cw, base_len, base_dim, d = (int(v) for v in out)
+    return dict(codeword_len=cw, base_len=base_len, base_dim=base_dim, depth=d)
+
+
+def iprs_tables(row_len, depth, rep=4):
+    dims = iprs_dims(row_len, depth, rep)
+    bm = np.zeros((dims["base_dim"], dims["base_len"]), np.int64)
+    ntw = sum(dims["base_dim"] * 8 ** k * 56 for k in range(depth))
+    tw = np.zeros(max(ntw, 1), np.int64)
+    assert lib().zr_iprs_tables(row_len, depth, rep, _ptr(bm), _ptr(tw)) == 0
+    return bm, tw[:ntw]
+
+
+def roots_of_unity(n):
+    out = np.zeros(n, np.int64)
+    assert lib().zr_roots_of_unity(n, _ptr(out)) == 0
+    return out
+
+
+def shuffle_identity(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.uint32)
+    lib().zr_shuffle_identity(seed, n, _ptr(out))
+    return out
+
+
+def stdrng_u32(seed: int, index: int) -> int:
+    return lib().zr_stdrng_u32(seed, index)
+
+
+def cw_bytes(desc: Desc) -> int:
+    return lib().zr_cw_bytes(C.byref(desc))
+
+
+def num_rows(desc: Desc) -> int:
+    return lib().zr_num_rows(C.byref(desc))
+
+
+def codeword_len(desc: Desc) -> int:
+    return lib().zr_codeword_len(C.byref(desc))
+
+
+def encode_rows(desc: Desc, evals: np.ndarray) -> np.ndarray:
+    """Row-major num_rows x codeword_len codeword matrix, as raw bytes view."""
+    R, Cl, cb = num_rows(desc), codeword_len(desc), cw_bytes(desc)
+    out = np.zeros(R * Cl * cb, np.uint8)
+    evals = np.ascontiguousarray(evals)
+    assert lib().zr_encode_rows(C.byref(desc), _ptr(evals), _ptr(out)) == 0
+    return out.reshape(R, Cl, cb)
+
+
+def encode_wide(desc: Desc, row: np.ndarray, limbs: int) -> np.ndarray:
+    """``LinearCode::encode_wide`` over Int<limbs>: row is (row_len, limbs) u64."""
+    Cl = codeword_len(desc)
+    out = np.zeros((Cl, limbs), np.uint64)
+    row = np.ascontiguousarray(row, dtype=np.uint64)
+    assert lib().zr_encode_wide(C.byref(desc), _ptr(row), limbs, _ptr(out)) == 0
+    return out
+
+
+def merkle_root_rows(rows: np.ndarray, elem_bytes: int) -> bytes:
+    """rows: (n_rows, width*elem_bytes) uint8."""
+    rows = np.ascontiguousarray(rows, dtype=np.uint8)
+    n_rows = rows.shape[0]
+    width = rows.shape[1] // elem_bytes
+    out = C.create_string_buffer(32)
+    rc = lib().zr_merkle_root_rows(_ptr(rows), n_rows, width, elem_bytes, out)
+    if rc:
+        raise ValueError("invalid merkle input")
+    return out.raw
+
+
+def commit(desc: Desc, polys: np.ndarray, batch: int) -> bytes:
+    polys = np.ascontiguousarray(polys)
+    out = C.create_string_buffer(32)
+    rc = lib().zr_commit(C.byref(desc), _ptr(polys), batch, out)
+    if rc:
+        raise ValueError(f"commit failed ({rc})")
+    return out.raw
+
+
+def point_array(point) -> np.ndarray:
+    """i128 coordinates -> (lo, hi) int64 pairs."""
+    arr = np.zeros(2 * len(point), np.int64)
+    for i, v in enumerate(point):
+        v = int(v) & ((1 << 128) - 1)
+        lo, hi = v & ((1 << 64) - 1), v >> 64
+        arr[2 * i] = np.uint64(lo).astype(np.int64)
+        arr[2 * i + 1] = np.uint64(hi).astype(np.int64)
+    return arr
+
+
+def proof_size(desc: Desc, batch: int) -> int:
+    return lib().zr_proof_size(C.byref(desc), batch)
+
+
+def commit_prove(desc: Desc, polys: np.ndarray, batch: int, point):
+    """Returns (root, proof bytes, eval inner bytes, modulus bytes)."""
+    polys = np.ascontiguousarray(polys)
+    pt = point_array(point)
+    cap = proof_size(desc, batch) + 64
+    proof = C.create_string_buffer(cap)
+    plen = C.c_size_t(0)
+    root = C.create_string_buffer(32)
+    ev = C.create_string_buffer(8 * desc.field_limbs)
+    mod = C.create_string_buffer(8 * desc.field_limbs)
+    rc = lib().zr_commit_prove(C.byref(desc), _ptr(polys), batch, _ptr(pt), root, proof, cap,
+                               C.byref(plen), ev, mod)
+    if rc:
+        raise ValueError(f"commit_prove failed ({rc})")
+    return root.raw, proof.raw[: plen.value], ev.raw, mod.raw
+
+
+def verify(desc: Desc, root: bytes, batch: int, point, eval_inner: bytes, proof: bytes) -> int:
+    pt = point_array(point)
+    return lib().zr_verify(C.byref(desc), _buf(root), batch, _ptr(pt), _buf(eval_inner),
+                           _buf(proof), len(proof))
+
+
+class Transcript:
+    """``Blake3Transcript`` restated (transcript/src/lib.rs:12-77)."""
+
+    def __init__(self):
+        self._t = lib().zr_tr_new()
+
+    def __del__(self):
+        if getattr(self, "_t", None):
+            lib().zr_tr_free(self._t)
+            self._t = None
+
+    def absorb(self, b: bytes):
+        lib().zr_tr_absorb(self._t, _buf(b), len(b))
+
+    def absorb_slice(self, b: bytes):
+        lib().zr_tr_absorb_slice(self._t, _buf(b), len(b))
+
+    def challenge(self, n: int) -> bytes:
+        out = C.create_string_buffer(n)
+        lib().zr_tr_challenge(self._t, out, n)
+        return out.raw
+
+    def get_prime(self, limbs: int = 4) -> int:
+        out = np.zeros(limbs, np.uint64)
+        lib().zr_tr_get_prime(self._t, limbs, _ptr(out))
+        return sum(int(v) << (64 * i) for i, v in enumerate(out))
+
+
+def is_probable_prime_base2(n: int, limbs: int = 4) -> bool:
+    arr = np.array([(n >> (64 * i)) & ((1 << 64) - 1) for i in range(limbs)], np.uint64)
+    return bool(lib().zr_is_probable_prime_base2(_ptr(arr), limbs))

@@ -1,0 +1,98 @@
+/*
+ * zipref: CPU restatement of the Zip+ commit/prove/verify path of
+ * NethermindEth/zinc-plus, used ONLY as test infrastructure (the checker) and
+ * as the timed CPU baseline.  Nothing in the product links this code.
+ *
+ * Parity status: pinned by the reference's own known-answer tests (octet
+ * reversal, F65537 twiddles, pNTT == NTT mod 65537, RAA 16-element codeword,
+ * Merkle round trip, proof-size formula) and by the `blake3` Python wheel for
+ * every hash.  Montgomery-form field bytes follow crypto-bigint MontyForm
+ * (R = 2^(64*LIMBS)); the reference ships no golden proof bytes, so byte
+ * parity of whole proofs is anchored on those pins, not on reference output.
+ */
+#ifndef ZIPREF_H
+#define ZIPREF_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ZR_EVAL_I32 = 0, ZR_EVAL_BINPOLY = 1 };
+enum { ZR_CODE_IPRS = 0, ZR_CODE_RAA = 1 };
+
+/* Same meaning as the product's zg_params_desc. */
+typedef struct {
+    uint32_t eval_kind;
+    uint32_t degree_plus_one;
+    uint32_t code_kind;
+    uint32_t rep;
+    uint32_t num_vars;
+    uint32_t row_len;
+    uint32_t iprs_depth; /* 0 => optimal depth */
+    uint32_t comb_limbs;
+    uint32_t field_limbs;
+    uint32_t num_openings;
+} zr_desc;
+
+/* BLAKE3 */
+void zr_blake3(const uint8_t *in, size_t n, uint8_t out[32]);
+void zr_blake3_xof(const uint8_t *in, size_t n, uint8_t *out, size_t out_len);
+void zr_blake3_chunk_cv(const uint8_t *in, size_t n, uint64_t counter, uint8_t out[32]);
+void zr_blake3_parent(const uint8_t l[32], const uint8_t r[32], int root, uint8_t out[32]);
+
+/* pNTT pieces */
+size_t zr_octet_reversal(size_t x, size_t num_octets);
+int zr_iprs_dims(uint32_t row_len, uint32_t depth, uint32_t rep, uint32_t out[4]);
+int zr_iprs_tables(uint32_t row_len, uint32_t depth, uint32_t rep, int64_t *base_matrix,
+                   int64_t *twiddles);
+int zr_roots_of_unity(uint32_t n, int64_t *out);
+
+/* rand 0.9 StdRng shuffle of 0..n */
+void zr_shuffle_identity(uint64_t seed, uint32_t n, uint32_t *perm);
+uint32_t zr_stdrng_u32(uint64_t seed, uint32_t index);
+
+/* encodings (row-major rows of Cw) */
+int zr_encode_rows(const zr_desc *d, const void *evals, void *cw_out);
+/* encode_wide over Int<limbs> rows (verifier side) */
+int zr_encode_wide(const zr_desc *d, const uint64_t *row, uint32_t limbs, uint64_t *out);
+
+size_t zr_cw_bytes(const zr_desc *d);
+size_t zr_eval_bytes(const zr_desc *d);
+uint32_t zr_num_rows(const zr_desc *d);
+uint32_t zr_codeword_len(const zr_desc *d);
+
+/* Merkle */
+int zr_merkle_root_rows(const uint8_t *rows, uint32_t n_rows, uint32_t width, uint32_t elem_bytes,
+                        uint8_t root[32]);
+
+/* Commit/prove/verify.  polys: batch eval arrays laid out back to back. */
+int zr_commit(const zr_desc *d, const void *polys, uint32_t batch, uint8_t root[32]);
+/* point: num_vars i128 values as (lo,hi) int64 pairs.  proof/eval buffers
+ * sized by zr_proof_size / 8*field_limbs. */
+size_t zr_proof_size(const zr_desc *d, uint32_t batch);
+int zr_commit_prove(const zr_desc *d, const void *polys, uint32_t batch, const int64_t *point,
+                    uint8_t root[32], uint8_t *proof, size_t proof_cap, size_t *proof_len,
+                    uint8_t *eval_out, uint8_t *modulus_out);
+int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const int64_t *point,
+              const uint8_t *eval_inner, const uint8_t *proof, size_t proof_len);
+
+/* FS transcript (Blake3Transcript) for direct tests */
+typedef struct zr_transcript zr_transcript;
+zr_transcript *zr_tr_new(void);
+void zr_tr_free(zr_transcript *t);
+void zr_tr_absorb(zr_transcript *t, const uint8_t *buf, size_t n);
+void zr_tr_absorb_slice(zr_transcript *t, const uint8_t *buf, size_t n);
+void zr_tr_challenge(zr_transcript *t, uint8_t *out, size_t n);
+void zr_tr_get_prime(zr_transcript *t, uint32_t limbs, uint64_t *prime_out);
+int zr_is_probable_prime_base2(const uint64_t *n, uint32_t limbs);
+
+/* threads used by the parallel regions */
+void zr_set_threads(int n);
+int zr_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
