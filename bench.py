@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Zip+ commit+prove throughput on B200: evals/s, per-step latency p50/p99.
+
+One step = one plain Zip+ commit + prove of one polynomial: encode, Merkle
+commitment, Fiat-Shamir transcript (root absorbed, random 256-bit prime field
+sampled), alpha projection, b rows, combined row and 147 column openings.
+The default workload is the Zip+ benchmark of the reference
+(zip-plus/benches/zip_plus_benches.rs:37-65): num_vars 16 (65536 evaluations),
+BinaryPoly<32> with Bernoulli(0.5) coefficients, IPRS rate 1/4 over F65537 with
+row_len 2^14 (4 rows, depth 2), MontyField<4>, CombR Int<5>, 147 openings,
+evaluation point [1; 16] (zip_common.rs:271).  Inputs are seeded synthetic.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank drives its own GPU with its own polynomials (replicas,
+weak scaling); times are the max over ranks.  `--impl reference` times the
+CPU restatement of the reference path (the oracle; the Rust reference cannot
+be built in this image) with all host threads, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "zinc-plus_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Zip+ commit+prove evals/s on 1 B200 (batched vs plain, bit-exact); p50/p99 ms"
+WORKLOADS = {
+    # name: (eval_kind, D, code_kind, num_vars, row_len)
+    "zipplus_binpoly32_iprs_nv16": (1, 32, 0, 16, 1 << 14),
+    "zipplus_binpoly32_raa_nv16": (1, 32, 1, 16, 256),
+    "zip_i32_iprs_nv12": (0, 1, 0, 12, 4096),
+}
+DEFAULT_WORKLOAD = "zipplus_binpoly32_iprs_nv16"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def make_inputs(workload, count, seed):
+    ek, D, _, nv, _ = WORKLOADS[workload]
+    rng = np.random.default_rng(seed)
+    n = 1 << nv
+    if ek == 1:
+        bits = rng.integers(0, 2, size=(count, n, D), dtype=np.uint8)
+        w = np.left_shift(np.uint64(1), np.arange(D, dtype=np.uint64))
+        return (bits.astype(np.uint64) * w).sum(axis=2, dtype=np.uint64)
+    return rng.integers(-(2**15), 2**15, size=(count, n), dtype=np.int32)
+
+
+def config_of(workload, num_rows, depth):
+    ek, D, ck, nv, L = WORKLOADS[workload]
+    code = (f"IPRS F65537 rate 1/4 row_len {L} depth {depth}" if ck == 0
+            else f"RAA rate 1/4 row_len {L} (rand 0.9 StdRng seeds 1, 2)")
+    return {
+        "workload": workload,
+        "num_vars": nv,
+        "evals_per_poly": 1 << nv,
+        "eval": f"BinaryPoly<{D}> u64-packed, Bernoulli(0.5)" if ek else "i32 uniform [-2^15, 2^15)",
+        "code": code,
+        "num_rows": num_rows,
+        "field": "MontyField<4> (random 256-bit prime from the transcript)",
+        "comb": "Int<5>" if ek else "Int<3>",
+        "openings": 147,
+        "point": f"[1; {nv}]",
+        "l2": "flushed between timed steps (256 MiB device memset, untimed)",
+        "parallelism": "replicas (one polynomial per step per GPU)",
+    }
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_commit_prove_rate(workload, seconds, max_steps, inputs):
+    """Oracle (CPU restatement of the reference path) with all host threads."""
+    from oracle import oracle as O
+
+    O.build()
+    ek, D, ck, nv, L = WORKLOADS[workload]
+    desc = O.make_desc(ek, D, ck, nv, L)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    O.commit_prove(desc, inputs[0], 1, [1] * nv)  # warm-up (page faults, tables)
+    steps, t0 = 0, time.perf_counter()
+    lat = []
+    while steps < max_steps and (time.perf_counter() - t0 < seconds or steps < 1):
+        t = time.perf_counter()
+        O.commit_prove(desc, inputs[steps % len(inputs)], 1, [1] * nv)
+        lat.append(time.perf_counter() - t)
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": steps * (1 << nv) / dt, "unit": "evals/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} full commit+prove steps of the workload ({1 << nv} evals each), "
+                      f"{dt:.1f} s, OpenMP over rows/columns/pairs like the reference's rayon",
+            "latency_ms": lat}
+
+
+def run_reference(args):
+    """--impl reference: the oracle port on the host cores, rank 0 only."""
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    workload = args.workload
+    ek, D, ck, nv, L = WORKLOADS[workload]
+    from oracle import oracle as O
+
+    O.build()
+    desc = O.make_desc(ek, D, ck, nv, L)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    inputs = make_inputs(workload, min(args.steps + args.warmup, 4), 1234)
+    for i in range(args.warmup):
+        O.commit_prove(desc, inputs[i % len(inputs)], 1, [1] * nv)
+    lat = []
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        t = time.perf_counter()
+        O.commit_prove(desc, inputs[i % len(inputs)], 1, [1] * nv)
+        lat.append((time.perf_counter() - t) * 1e3)
+    dt = time.perf_counter() - t0
+    value = args.steps * (1 << nv) / dt
+    R = O.num_rows(desc)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": config_of(workload, R, 0 if ck else O.iprs_optimal_depth(L)),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full commit+prove steps, OpenMP, the Rust "
+                                   "reference is not buildable here (no cargo)"},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------- ours
+def algorithmic_bytes(kernel, info, nv, D):
+    """Algorithmic HBM bytes of one launch of `kernel` for one polynomial."""
+    R, C, L = info.num_rows, info.codeword_len, info.row_len
+    N = R * L
+    table = {
+        "k_base_bin": N * 8 + info.base_dim * info.base_len * 4 + R * C * D * 4,
+        "k_stage_bin[0]": R * C * D * 4 + R * C * D * 8,
+        "k_stage_bin[1+]": 2 * R * C * D * 8,
+        "k_leaf_small": R * C * D * 8 + C * 32,
+        "k_project_rows": N * 8 + L * 32 + N * 40,
+        "k_raa_bin": N * 8 + R * C * D * 4,
+    }
+    return table.get(kernel)
+
+
+def run_ours(args):
+    import torch
+
+    rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import zipgpu as Z
+
+    workload = args.workload
+    ek, D, ck, nv, L = WORKLOADS[workload]
+    ctx = Z.Context(local)
+    zt = Z.ZipTypes(ek, D if ek else 1, 5 if ek else 3, 4, 147)
+    code = Z.IprsCode(L) if ck == 0 else Z.RaaCode(L)
+    pp = Z.ZipPlus.setup(1 << nv, code, zt, ctx=ctx)
+    lib = Z.lib()
+    K, W = args.steps, args.warmup
+    n = 1 << nv
+    host = make_inputs(workload, K + W, 1000 + rank)
+    dtype = torch.int64 if ek else torch.int32
+    host_t = torch.from_numpy(host.view(np.int64) if ek else host).pin_memory()
+    dev_t = host_t.to("cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    point = Z.i128_bytes([1] * nv)
+    cap = pp.proof_size(1)
+    proof = C.create_string_buffer(cap)
+    root = C.create_string_buffer(32)
+    ev = C.create_string_buffer(32)
+    plen = C.c_size_t(cap)
+    eb = host_t.element_size() * n
+
+    def step_device(i):
+        plen.value = cap
+        Z.check(lib.zg_commit_prove_d(pp.handle, C.c_void_p(dev_t[i].data_ptr()), 1,
+                                      C.c_char_p(point), root, ev, proof, C.byref(plen)))
+
+    def step_host(i):
+        plen.value = cap
+        ptrs = (C.c_void_p * 1)(host_t[i].data_ptr())
+        Z.check(lib.zg_commit_prove(pp.handle, ptrs, 1, C.c_char_p(point), root, ev, proof,
+                                    C.byref(plen)))
+
+    def timed(step):
+        times = []
+        for i in range(K):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(W + i)
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in times]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up: device path and host path
+    for i in range(W):
+        step_device(i)
+        step_host(i)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = ctx.kernel_launches
+    barrier()
+    lat_dev = timed(step_device)
+    barrier()
+    launches = ctx.kernel_launches - launches0
+    clock_info = clocks.stop()
+    total_dev = max_over_ranks(sum(lat_dev))
+    barrier()
+    lat_host = timed(step_host)
+    barrier()
+    total_host = max_over_ranks(sum(lat_host))
+    proof_len = plen.value
+
+    # per-kernel CUDA-event timing pass (same workload, separate K steps)
+    ctx.set_kernel_timing(True)
+    ctx.kernel_times()
+    timed(step_device)
+    ktimes = ctx.kernel_times()
+    ctx.set_kernel_timing(False)
+
+    value = world * K * n / (total_dev / 1e3)
+    e2e = world * K * n / (total_host / 1e3)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs")
+    peak_kind = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    dom = max(ktimes.items(), key=lambda kv: kv[1][1]) if ktimes else None
+    roofline = None
+    if dom:
+        name, (cnt, ms) = dom
+        avg_ms = ms / cnt
+        info = pp.info
+        ab = algorithmic_bytes(name, info, nv, D)
+        launches_per_step = cnt / K
+        traffic = None
+        try:
+            tr = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
+            traffic = tr.get(workload, {}).get(name)
+        except Exception:
+            pass
+        achieved = (ab / (avg_ms / 1e3) / 1e9) if ab else None
+        roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm,
+                    "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+                    "traffic": traffic, "algorithmic_bytes": ab, "avg_launch_ms": avg_ms,
+                    "launches_per_step": launches_per_step,
+                    "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                    "kernel_share": {k: round(v[1] / sum(x[1] for x in ktimes.values()), 4)
+                                     for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][1])}}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_commit_prove_rate(workload, args.cpu_seconds, 50, host[:4])
+        cpu.pop("latency_ms", None)
+    if rank == 0:
+        all_lat = lat_dev
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": total_dev / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": config_of(workload, pp.num_rows, pp.info.depth),
+            "latency_ms": {"p50": float(np.percentile(all_lat, 50)),
+                           "p99": float(np.percentile(all_lat, 99))},
+            "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": eb,
+                    "d2h_bytes_per_step": proof_len + 64,
+                    "ms_per_step": total_host / K,
+                    "latency_ms": {"p50": float(np.percentile(lat_host, 50)),
+                                   "p99": float(np.percentile(lat_host, 99))}},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clock_info,
+            "impl": "ours",
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,203 @@
+/*
+ * zipgpu.h -- C ABI of the B200 (sm_100a) Zip+ commit/prove/verify backend.
+ *
+ * The reference (NethermindEth/zinc-plus) is a Rust workspace with no FFI; its
+ * boundary for this path is a set of Rust traits and associated functions.
+ * Each entry point below names the reference item it stands in for, so a Rust
+ * host can bind this header and keep its call sites:
+ *
+ *   LinearCode::{row_len, codeword_len, encode, encode_wide}
+ *                                   zip-plus/src/code.rs:10-72
+ *   IprsCode::{new, new_with_optimal_depth}   zip-plus/src/code/iprs.rs:30-51
+ *   RaaCode::new                    zip-plus/src/code/raa.rs:38-90
+ *   ZipPlus::setup                  zip-plus/src/pcs/structs.rs:74-88
+ *   ZipPlus::{commit, commit_single, encode_rows}
+ *                                   zip-plus/src/pcs/phase_commit.rs:61,135,159
+ *   ZipPlus::{prove, prove_f}       zip-plus/src/pcs/phase_prove.rs:85,119
+ *   ZipPlus::verify                 zip-plus/src/pcs/phase_verify.rs:100
+ *   MerkleTree::{new, root}         zip-plus/src/merkle.rs:74-103
+ *   PcsProverTranscript / Blake3Transcript
+ *                                   zip-plus/src/pcs_transcript.rs:44-222,
+ *                                   transcript/src/lib.rs:12-77
+ *
+ * Conventions
+ *  - Every function returns a zg_status (0 = ZG_OK).  No exception or panic
+ *    crosses the ABI.  zg_last_error() gives a message for the calling thread.
+ *  - Host buffers are owned by the caller.  Device hints (codewords and Merkle
+ *    layers, the reference's ZipPlusHint) are owned by the library until
+ *    zg_hint_free.  "_d" entry points take device pointers and a cudaStream_t
+ *    passed as void*.
+ *  - Evaluations: ZG_EVAL_I32 is one int32 per evaluation (Zip, Eval = i32);
+ *    ZG_EVAL_BINPOLY is one uint64 per evaluation holding the {0,1}
+ *    coefficients of a BinaryPoly<D> (bit i = coefficient of X^i, bits >= D
+ *    must be zero), as the reference's `simd` feature stores it
+ *    (poly/src/univariate/binary_u64.rs:28).
+ *  - Codewords are laid out like the reference's DenseRowMatrix (row-major
+ *    num_rows x codeword_len) when copied to the host; Cw is i128 (I32 evals),
+ *    DensePolynomial<i64, D> (BINPOLY + IPRS) or DensePolynomial<i32, D>
+ *    (BINPOLY + RAA), little-endian, coefficient 0 first.
+ *  - Field elements (MontyField<field_limbs>) are exchanged as their
+ *    Montgomery-form inner value, 8*field_limbs little-endian bytes.
+ *  - i128 values (challenges, points) are exchanged as little-endian 16-byte
+ *    two's complement.
+ */
+#ifndef ZIPGPU_H
+#define ZIPGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; the first four mirror ZipError (zip-plus/src/lib.rs:13-29). */
+typedef enum {
+    ZG_OK = 0,
+    ZG_ERR_INVALID_PARAM = 1,   /* ZipError::InvalidPcsParam, setup asserts   */
+    ZG_ERR_INVALID_OPEN = 2,    /* ZipError::InvalidPcsOpen: verifier rejects */
+    ZG_ERR_SERIALIZATION = 3,   /* ZipError::Transcript: truncated proof      */
+    ZG_ERR_OVERFLOW = 4,        /* validate_input bit budget exceeded         */
+    ZG_ERR_CUDA = 5,            /* CUDA runtime error                          */
+    ZG_ERR_OOM = 6,             /* device or host allocation failed            */
+    ZG_ERR_TIMEOUT = 7,         /* a bounded device wait gave up               */
+    ZG_ERR_NO_DEVICE = 8,       /* no CUDA device / extension unusable         */
+    ZG_ERR_BUFFER_TOO_SMALL = 9 /* caller buffer shorter than required         */
+} zg_status;
+
+typedef enum { ZG_EVAL_I32 = 0, ZG_EVAL_BINPOLY = 1 } zg_eval_kind;
+typedef enum { ZG_CODE_IPRS = 0, ZG_CODE_RAA = 1 } zg_code_kind;
+
+/* One ZipTypes instantiation plus its linear code and matrix shape.
+ * The reference fixes these through type parameters (pcs/structs.rs:15-60):
+ *   Zip    (zip-plus/benches/zip_benches.rs:25-40): I32, comb_limbs 3, field_limbs 4
+ *   Zip+   (zip-plus/benches/zip_plus_benches.rs:37-65): BINPOLY D=32|64,
+ *          comb_limbs 5, field_limbs 4; Cw coefficients i64 (IPRS) / i32 (RAA)
+ * Chal and Pt are i128 in both. */
+typedef struct {
+    uint32_t eval_kind;       /* zg_eval_kind                                   */
+    uint32_t degree_plus_one; /* D of BinaryPoly<D> (1..64); 1 for I32          */
+    uint32_t code_kind;       /* zg_code_kind                                   */
+    uint32_t rep;             /* repetition factor (inverse rate), 4            */
+    uint32_t num_vars;        /* poly_size = 2^num_vars                         */
+    uint32_t row_len;         /* power of two dividing poly_size                */
+    uint32_t iprs_depth;      /* 0 => IprsCode::new_with_optimal_depth          */
+    uint32_t comb_limbs;      /* CombR = Int<comb_limbs> (64-bit limbs)          */
+    uint32_t field_limbs;     /* F = MontyField<field_limbs>, 3 or 4            */
+    uint32_t num_openings;    /* NUM_COLUMN_OPENINGS (147 in the reference)     */
+} zg_params_desc;
+
+/* Derived dimensions of a parameter set. */
+typedef struct {
+    uint32_t num_rows, row_len, codeword_len;
+    uint32_t depth, base_len, base_dim; /* IPRS only */
+    uint32_t eval_bytes, cw_bytes, comb_bytes, field_bytes;
+} zg_params_info;
+
+typedef struct zg_ctx zg_ctx;
+typedef struct zg_params zg_params;
+typedef struct zg_hint zg_hint;
+typedef struct zg_transcript zg_transcript;
+
+/* ---- library / context --------------------------------------------------- */
+const char *zg_last_error(void);
+const char *zg_version(void);
+/* Creates a context on a CUDA device (one stream, scratch arenas). */
+zg_status zg_ctx_create(int device, zg_ctx **out);
+zg_status zg_ctx_destroy(zg_ctx *ctx);
+/* Number of kernels this context launched so far (for measurement). */
+uint64_t zg_ctx_kernel_launches(const zg_ctx *ctx);
+/* Stream used by the context (a cudaStream_t). */
+void *zg_ctx_stream(zg_ctx *ctx);
+/* Measurement (no counterpart in the reference): when enabled, CUDA events are
+ * recorded on the launching stream around every kernel launch.  The report
+ * (synchronizes the stream) writes "name,launches,total_ms\n" lines and resets
+ * the totals; *len receives the length needed. */
+zg_status zg_ctx_set_kernel_timing(zg_ctx *ctx, int enable);
+zg_status zg_ctx_kernel_timing_report(zg_ctx *ctx, char *buf, size_t cap, size_t *len);
+
+/* ---- setup: ZipPlus::setup + IprsCode::new / RaaCode::new -----------------
+ * ctx may be NULL for host-only parameters (tables, encode_wide, verify);
+ * device entry points then return ZG_ERR_NO_DEVICE. */
+zg_status zg_params_create(zg_ctx *ctx, const zg_params_desc *desc, zg_params **out);
+zg_status zg_params_destroy(zg_params *p);
+zg_status zg_params_get_info(const zg_params *p, zg_params_info *info);
+/* Twiddle tables exactly as Radix8PnttParams holds them (params.rs:31-57):
+ * base_matrix base_dim x base_len, butterfly twiddles per stage k
+ * (base_dim*8^k x 7 x 8), all int64.  Either pointer may be NULL. */
+zg_status zg_params_iprs_tables(const zg_params *p, int64_t *base_matrix, int64_t *twiddles);
+/* The two RAA permutations (raa.rs:76-80), codeword_len uint32 each. */
+zg_status zg_params_raa_perms(const zg_params *p, uint32_t *perm1, uint32_t *perm2);
+
+/* ---- LinearCode::encode via ZipPlus::encode_rows (phase_commit.rs:159) ----
+ * evals: num_rows*row_len evaluations; cw_out: num_rows x codeword_len Cw. */
+zg_status zg_encode_rows(zg_params *p, const void *evals, void *cw_out);
+zg_status zg_encode_rows_d(zg_params *p, const void *evals_d, void *cw_out_d, void *stream);
+/* LinearCode::encode_wide on Int<limbs> rows (iprs.rs:148-150): row is
+ * row_len x limbs uint64, out codeword_len x limbs. */
+zg_status zg_encode_wide(zg_params *p, const uint64_t *row, uint32_t limbs, uint64_t *out);
+
+/* ---- MerkleTree::new(rows).root() (merkle.rs:74-103) ----------------------
+ * rows: n_rows x (width*elem_bytes) bytes, row-major; width a power of two. */
+zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_t width,
+                         uint32_t elem_bytes, uint8_t root[32]);
+
+/* ---- ZipPlus::commit (phase_commit.rs:61-101) ------------------------------
+ * polys[i] points at poly i's 2^num_vars evaluations.  The hint (codewords and
+ * Merkle layers) stays on the device.  commit_single == batch 1. */
+zg_status zg_commit(zg_params *p, const void *const *polys, uint32_t batch, zg_hint **hint,
+                    uint8_t root[32]);
+/* Same with device-resident evaluations: polys_d holds batch polys back to back. */
+zg_status zg_commit_d(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **hint,
+                      uint8_t root[32]);
+zg_status zg_hint_free(zg_hint *hint);
+uint32_t zg_hint_batch(const zg_hint *hint);
+/* Copies the hint's codeword of poly `poly` to the host, row-major. */
+zg_status zg_hint_codeword(const zg_hint *hint, uint32_t poly, void *cw_out);
+
+/* ---- PcsProverTranscript (pcs_transcript.rs:44-222) ------------------------ */
+/* new_from_commitments: absorbs each root as a slice. */
+zg_status zg_transcript_new(const uint8_t *roots, uint32_t n_roots, zg_transcript **out);
+zg_status zg_transcript_free(zg_transcript *t);
+zg_status zg_transcript_absorb(zg_transcript *t, const uint8_t *buf, size_t n);
+zg_status zg_transcript_absorb_slice(zg_transcript *t, const uint8_t *buf, size_t n);
+/* get_challenge::<T>() for a T of n bytes (traits.rs:329-335). */
+zg_status zg_transcript_challenge(zg_transcript *t, uint8_t *out, size_t n);
+/* get_random_field_cfg::<MontyField<limbs>, Uint<limbs>, MillerRabin>
+ * (traits.rs:364-374): samples and remembers the prime; modulus_out may be
+ * NULL (else 8*limbs bytes). */
+zg_status zg_transcript_sample_field(zg_transcript *t, uint32_t limbs, uint8_t *modulus_out);
+/* Proof bytes written so far (the reference's `stream`). */
+zg_status zg_transcript_proof(const zg_transcript *t, const uint8_t **data, size_t *len);
+
+/* ---- ZipPlus::prove (phase_prove.rs:85-253) --------------------------------
+ * Requires zg_transcript_sample_field first.  polys as for zg_commit (host);
+ * point: num_vars i128 coordinates (Pt = i128).  eval_out: 8*field_limbs
+ * bytes (Montgomery inner of the returned F).  Appends the proof to t. */
+zg_status zg_prove(zg_params *p, zg_transcript *t, const void *const *polys, uint32_t batch,
+                   const uint8_t *point, const zg_hint *hint, uint8_t *eval_out);
+zg_status zg_prove_d(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
+                     const uint8_t *point, const zg_hint *hint, uint8_t *eval_out);
+
+/* Whole-request convenience: commit, new_from_commitment, sample field, prove.
+ * Writes root, eval and the proof (proof_len in/out: capacity/size). */
+zg_status zg_commit_prove(zg_params *p, const void *const *polys, uint32_t batch,
+                          const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
+                          uint8_t *proof, size_t *proof_len);
+zg_status zg_commit_prove_d(zg_params *p, const void *polys_d, uint32_t batch,
+                            const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
+                            uint8_t *proof, size_t *proof_len);
+/* Exact proof length for a batch (phase_commit.rs:739-805 formula). */
+size_t zg_proof_size(const zg_params *p, uint32_t batch);
+
+/* ---- ZipPlus::verify (phase_verify.rs:100-304) ------------------------------
+ * Fresh verifier transcript: absorbs root, samples the field, samples alphas,
+ * then runs the four checks.  ZG_OK accepts; ZG_ERR_INVALID_OPEN rejects;
+ * ZG_ERR_SERIALIZATION for a truncated/malformed proof. */
+zg_status zg_verify(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
+                    const uint8_t *eval, const uint8_t *proof, size_t proof_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZIPGPU_H */

@@ -58,6 +58,8 @@ def lib():
         L.zr_octet_reversal.argtypes = [sz, sz]
         L.zr_octet_reversal.restype = sz
         L.zr_iprs_dims.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, vp]
+        L.zr_iprs_optimal_depth.argtypes = [C.c_uint32]
+        L.zr_iprs_optimal_depth.restype = C.c_uint32
         L.zr_iprs_tables.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, vp, vp]
         L.zr_roots_of_unity.argtypes = [C.c_uint32, vp]
         L.zr_shuffle_identity.argtypes = [C.c_uint64, C.c_uint32, vp]
@@ -144,6 +146,10 @@ def iprs_dims(row_len, depth, rep=4):
         return None
     cw, base_len, base_dim, d = (int(v) for v in out)
     return dict(codeword_len=cw, base_len=base_len, base_dim=base_dim, depth=d)
+
+
+def iprs_optimal_depth(row_len: int) -> int:
+    return int(lib().zr_iprs_optimal_depth(row_len))
 
 
 def iprs_tables(row_len, depth, rep=4):

@@ -486,6 +486,8 @@ static uint32_t iprs_optimal_depth(uint32_t row_len) {
     return d < 1 ? 1 : d;
 }
 
+uint32_t zr_iprs_optimal_depth(uint32_t row_len) { return iprs_optimal_depth(row_len); }
+
 int zr_iprs_dims(uint32_t row_len, uint32_t depth, uint32_t rep, uint32_t out[4]) {
     return iprs_check(row_len, depth, rep, out);
 }
@@ -1193,7 +1195,10 @@ void zr_tr_get_prime(zr_transcript *t, uint32_t L, uint64_t *prime_out) {
         uint64_t c[4] = {0};
         memcpy(c, buf, 8 * L);
         if (uiszero(c, L)) continue;
-        if (!(c[0] & 1)) c[0] -= 1;
+        if (!(c[0] & 1)) { /* prime_candidate -= ONE, full width */
+            for (uint32_t i = 0; i < L; i++)
+                if (c[i]-- != 0) break;
+        }
         if (zr_is_probable_prime_base2(c, L)) {
             memcpy(prime_out, c, 8 * L);
             return;
@@ -1650,7 +1655,6 @@ int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const in
             if (merkle_verify(root, col, colbytes, li, lc, sib, np, idx)) { rc = 2; goto out; }
         }
     }
-    if (rd.pos != rd.len) rc = 3;
 out:
     free(col);
     free(sib);

@@ -44,6 +44,7 @@ void zr_blake3_parent(const uint8_t l[32], const uint8_t r[32], int root, uint8_
 
 /* pNTT pieces */
 size_t zr_octet_reversal(size_t x, size_t num_octets);
+uint32_t zr_iprs_optimal_depth(uint32_t row_len);
 int zr_iprs_dims(uint32_t row_len, uint32_t depth, uint32_t rep, uint32_t out[4]);
 int zr_iprs_tables(uint32_t row_len, uint32_t depth, uint32_t rep, int64_t *base_matrix,
                    int64_t *twiddles);

@@ -1,0 +1,164 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle, byte for
+byte: codewords, Merkle roots, commitments, proofs and evaluations.  Sizes the
+oracle finishes in seconds, plus the full-size workloads of the benchmark
+checked through the same equality and through the verifier."""
+import numpy as np
+import pytest
+
+from util import binary_evals, desc_for, i32_evals, params_for
+
+pytestmark = pytest.mark.gpu
+
+ENCODE_CASES = [
+    # (eval_kind, D, code_kind, num_vars, row_len, depth)
+    (0, 1, 0, 12, 4096, 0),   # Zip flat: depth 2, base 256 x 64
+    (0, 1, 0, 12, 64, 0),     # Zip square: depth 1
+    (0, 1, 0, 10, 1024, 3),   # explicit depth 3 over a tiny base
+    (0, 1, 0, 6, 64, 0),
+    (1, 32, 0, 12, 1024, 0),  # Zip+ deg 32: depth 1
+    (1, 32, 0, 14, 4096, 0),  # depth 2
+    (1, 64, 0, 12, 4096, 0),
+    (1, 3, 0, 10, 256, 0),    # the reference tests' BinaryPoly<3>
+    (1, 32, 0, 10, 1024, 1),
+    (1, 32, 0, 10, 32, 0),
+    (1, 17, 0, 9, 512, 0),
+    (1, 32, 1, 12, 64, 0),    # RAA
+    (1, 64, 1, 12, 64, 0),
+    (1, 3, 1, 8, 16, 0),
+    (1, 32, 1, 16, 256, 0),   # RAA at the Zip+ benchmark shape
+]
+
+
+def _evals(rng, ek, D, n):
+    return binary_evals(rng, n, D) if ek else i32_evals(rng, n, -(2**31), 2**31 - 1)
+
+
+@pytest.mark.parametrize("case", ENCODE_CASES)
+def test_encode_rows_matches_oracle(zipgpu, oracle, ctx, rng, case):
+    ek, D, ck, nv, L, depth = case
+    pp = params_for(zipgpu, ek, D, ck, nv, L, depth, ctx=ctx)
+    ev = _evals(rng, ek, D, 1 << nv)
+    got = zipgpu.ZipPlus.encode_rows(pp, ev)
+    want = oracle.encode_rows(desc_for(ek, D, ck, nv, L, depth), ev)
+    assert got.shape == want.shape
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("rows,width,eb", [(1, 1024, 16), (4, 4096, 256), (64, 256, 16),
+                                           (3, 64, 12), (256, 16, 128), (1, 1, 16)])
+def test_merkle_root_matches_oracle(zipgpu, oracle, ctx, rows, width, eb):
+    data = np.random.default_rng(rows * width).integers(0, 256, (rows, width * eb), dtype=np.uint8)
+    assert zipgpu.MerkleTree.new(data, eb, ctx).root() == oracle.merkle_root_rows(data, eb)
+
+
+COMMIT_CASES = [
+    # (eval_kind, D, code_kind, num_vars, row_len, batch)
+    (0, 1, 0, 12, 4096, 1), (0, 1, 0, 12, 64, 1), (0, 1, 0, 10, 256, 5),
+    (1, 32, 0, 12, 1024, 1), (1, 32, 0, 12, 1024, 2), (1, 64, 0, 10, 1024, 1),
+    (1, 3, 0, 10, 256, 3), (1, 32, 1, 12, 64, 1), (1, 64, 1, 12, 64, 2),
+    (1, 32, 0, 3, 8, 1),
+]
+
+
+@pytest.mark.parametrize("case", COMMIT_CASES)
+def test_commit_prove_matches_oracle(zipgpu, oracle, ctx, rng, case):
+    ek, D, ck, nv, L, batch = case
+    pp = params_for(zipgpu, ek, D, ck, nv, L, ctx=ctx)
+    polys = [_evals(rng, ek, D, 1 << nv) for _ in range(batch)]
+    point = [(-1) ** i * (7 * i + 2) for i in range(nv)]
+    desc = desc_for(ek, D, ck, nv, L)
+    root_o, proof_o, ev_o, _ = oracle.commit_prove(desc, np.concatenate(polys), batch, point)
+    hint, comm = zipgpu.ZipPlus.commit(pp, polys)
+    assert comm.root == root_o
+    t = zipgpu.PcsProverTranscript.new_from_commitment(comm)
+    t.get_random_field_cfg(4)
+    ev = zipgpu.ZipPlus.prove(t, pp, polys, point, hint)
+    assert ev == ev_o
+    assert t.stream == proof_o
+    # the hint's codewords are the encode_rows output
+    for b in range(batch):
+        assert np.array_equal(hint.codeword(b), oracle.encode_rows(desc, polys[b]))
+    zipgpu.ZipPlus.verify(pp, comm, point, ev, t.stream)
+    assert oracle.verify(desc, comm.root, batch, point, ev, t.stream) == 0
+    root2, ev2, proof2 = zipgpu.ZipPlus.commit_prove(pp, polys, point)
+    assert (root2, ev2, proof2) == (root_o, ev_o, proof_o)
+
+
+def test_edge_value_polynomials(zipgpu, oracle, ctx):
+    """Zero, all-ones, extreme i32 values (commit_succeeds_for_zero_polynomial,
+    commit_succeeds_for_alternating_values, encode_rows_handles_large_integer_values)."""
+    nv = 10
+    for ek, D, vals in [
+        (0, 1, np.zeros(1 << nv, np.int32)),
+        (0, 1, np.full(1 << nv, 2**31 - 1, np.int32)),
+        (0, 1, np.full(1 << nv, -(2**31), np.int32)),
+        (0, 1, np.where(np.arange(1 << nv) % 2 == 0, 1, -1).astype(np.int32)),
+        (1, 32, np.zeros(1 << nv, np.uint64)),
+        (1, 32, np.full(1 << nv, 0xFFFFFFFF, np.uint64)),
+        (1, 64, np.full(1 << nv, 0xFFFFFFFFFFFFFFFF, np.uint64)),
+    ]:
+        L = 256
+        pp = params_for(zipgpu, ek, D, 0, nv, L, ctx=ctx)
+        desc = desc_for(ek, D, 0, nv, L)
+        point = [1] * nv
+        root, ev, proof = zipgpu.ZipPlus.commit_prove(pp, [vals], point)
+        ro, po, eo, _ = oracle.commit_prove(desc, vals, 1, point)
+        assert (root, ev, proof) == (ro, eo, po)
+
+
+def test_commit_is_deterministic_and_input_sensitive(zipgpu, ctx, rng):
+    pp = params_for(zipgpu, 1, 32, 0, 12, 1024, ctx=ctx)
+    ev = binary_evals(rng, 1 << 12, 32)
+    _, c1 = zipgpu.ZipPlus.commit_single(pp, ev)
+    _, c2 = zipgpu.ZipPlus.commit_single(pp, ev)
+    assert c1.root == c2.root
+    ev2 = ev.copy()
+    ev2[100] ^= np.uint64(1)
+    _, c3 = zipgpu.ZipPlus.commit_single(pp, ev2)
+    assert c3.root != c1.root
+    _, cb = zipgpu.ZipPlus.commit(pp, [ev, ev2])
+    assert cb.root not in (c1.root, c3.root) and cb.batch_size == 2
+
+
+def test_batch_and_size_errors(zipgpu, ctx, rng):
+    pp = params_for(zipgpu, 1, 32, 0, 10, 1024, ctx=ctx)
+    with pytest.raises(ValueError):
+        zipgpu.ZipPlus.commit(pp, [])
+    with pytest.raises(ValueError):
+        zipgpu.ZipPlus.commit(pp, [binary_evals(rng, 512, 32)])
+    hint, comm = zipgpu.ZipPlus.commit(pp, [binary_evals(rng, 1024, 32)])
+    t = zipgpu.PcsProverTranscript.new_from_commitment(comm)
+    with pytest.raises(zipgpu.ZipError):  # field not sampled yet
+        zipgpu.ZipPlus.prove(t, pp, [binary_evals(rng, 1024, 32)], [1] * 10, hint)
+    t.get_random_field_cfg(4)
+    with pytest.raises(zipgpu.ZipError):  # point of the wrong length
+        zipgpu.ZipPlus.prove(t, pp, [binary_evals(rng, 1024, 32)], [1] * 9, hint)
+    with pytest.raises(zipgpu.ZipError):  # hint for another batch size
+        zipgpu.ZipPlus.prove(t, pp, [binary_evals(rng, 1024, 32)] * 2, [1] * 10, hint)
+
+
+@pytest.mark.parametrize("ck,L", [(0, 1 << 14), (1, 256)])
+def test_benchmark_workload_matches_oracle(zipgpu, oracle, ctx, rng, ck, L):
+    """The Zip+ benchmark workload at full size: num_vars 16, BinaryPoly<32>,
+    IPRS (row_len 2^14, 4 rows) and RAA (row_len 256, 256 rows)."""
+    nv, D = 16, 32
+    pp = params_for(zipgpu, 1, D, ck, nv, L, ctx=ctx)
+    ev = binary_evals(rng, 1 << nv, D)
+    point = [1] * nv
+    root, inner, proof = zipgpu.ZipPlus.commit_prove(pp, [ev], point)
+    ro, po, eo, _ = oracle.commit_prove(desc_for(1, D, ck, nv, L), ev, 1, point)
+    assert root == ro and inner == eo and proof == po
+    zipgpu.ZipPlus.verify(pp, zipgpu.ZipPlusCommitment(root, 1), point, inner, proof)
+
+
+@pytest.mark.parametrize("nv", [18, 20])
+def test_large_commit_prove_verifies(zipgpu, ctx, rng, nv):
+    """Sizes beyond the oracle's quick range: the proof must verify (the
+    verifier re-encodes the combined row and checks 147 opened columns against
+    it and against the Merkle root) and have the exact size."""
+    pp = params_for(zipgpu, 1, 32, 0, nv, 1 << 14, ctx=ctx)
+    ev = binary_evals(rng, 1 << nv, 32)
+    point = [(-1) ** i * (i + 1) for i in range(nv)]
+    root, inner, proof = zipgpu.ZipPlus.commit_prove(pp, [ev], point)
+    zipgpu.ZipPlus.verify(pp, zipgpu.ZipPlusCommitment(root, 1), point, inner, proof)
+    assert len(proof) == pp.proof_size(1)

@@ -1,0 +1,109 @@
+"""CPU tests of the product library: it loads, exports every symbol that
+include/zipgpu.h declares, and its host-side logic (code tables, RAA
+permutations, Fiat-Shamir transcript, prime sampling, encode_wide, verifier)
+matches the oracle.  No GPU compute is called here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from util import binary_evals, desc_for, i32_evals, params_for
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "zipgpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(zg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(zipgpu):
+    names = _declared_symbols()
+    assert len(names) >= 30
+    lib = C.CDLL(zipgpu.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(zipgpu.EXPORTS)
+
+
+def test_version_and_errors(zipgpu):
+    assert b"sm_100a" in zipgpu.lib().zg_version()
+    with pytest.raises(zipgpu.ZipError) as e:  # row_len does not divide poly_size
+        params_for(zipgpu, 1, 32, 0, 4, 32, device=False)
+    assert e.value.status == 1
+    with pytest.raises(zipgpu.ZipError):  # codeword longer than F65537
+        params_for(zipgpu, 1, 32, 0, 16, 1 << 15, device=False)
+    with pytest.raises(zipgpu.ZipError):  # RaaCode::new width check
+        params_for(zipgpu, 1, 32, 1, 30, 1 << 15, device=False)
+
+
+@pytest.mark.parametrize("row_len,depth", [(4096, 0), (64, 0), (16384, 0), (256, 1), (2048, 3),
+                                           (8, 0), (1024, 0)])
+def test_iprs_tables_match_oracle(zipgpu, oracle, row_len, depth):
+    pp = params_for(zipgpu, 1, 32, 0, 14 if row_len <= 16384 else 15, row_len, depth, device=False)
+    bm, tw = pp.iprs_tables()
+    bo, to = oracle.iprs_tables(row_len, pp.info.depth)
+    assert np.array_equal(bm, bo) and np.array_equal(tw, to)
+
+
+def test_raa_perms_match_oracle(zipgpu, oracle):
+    pp = params_for(zipgpu, 1, 32, 1, 16, 256, device=False)
+    p1, p2 = pp.raa_perms()
+    assert np.array_equal(p1, oracle.shuffle_identity(1, 1024))
+    assert np.array_equal(p2, oracle.shuffle_identity(2, 1024))
+
+
+def test_transcript_and_prime_match_oracle(zipgpu, oracle):
+    t = zipgpu.PcsProverTranscript([b"\x42" * 32])
+    o = oracle.Transcript()
+    o.absorb_slice(b"\x42" * 32)
+    assert t.get_challenge(16) == o.challenge(16)
+    t.absorb(b"xyz" * 1000)
+    o.absorb(b"xyz" * 1000)
+    assert t.get_challenge(77) == o.challenge(77)
+    assert t.get_random_field_cfg(4) == o.get_prime(4)
+    assert t.get_challenge(4) == o.challenge(4)
+    assert t.get_random_field_cfg(3) == o.get_prime(3)
+    assert t.get_challenge(32) == o.challenge(32)
+
+
+@pytest.mark.parametrize("code_kind,row_len", [(0, 1024), (0, 64), (1, 64)])
+def test_encode_wide_matches_oracle(zipgpu, oracle, code_kind, row_len):
+    pp = params_for(zipgpu, 1, 32, code_kind, 12, row_len, device=False)
+    desc = desc_for(1, 32, code_kind, 12, row_len)
+    row = np.random.default_rng(9).integers(0, 2**63, (row_len, 5), dtype=np.uint64)
+    assert np.array_equal(zipgpu.ZipPlus.encode_wide(pp, row, 5), oracle.encode_wide(desc, row, 5))
+
+
+@pytest.mark.parametrize("case", [(0, 1, 0, 12, 4096, 1), (0, 1, 0, 12, 64, 2),
+                                  (1, 32, 0, 12, 1024, 1), (1, 32, 1, 12, 64, 1),
+                                  (1, 64, 0, 10, 256, 2)])
+def test_host_verifier_accepts_oracle_proofs(zipgpu, oracle, rng, case):
+    ek, D, ck, nv, L, batch = case
+    desc = desc_for(ek, D, ck, nv, L)
+    polys = np.concatenate([binary_evals(rng, 1 << nv, D) if ek else i32_evals(rng, 1 << nv)
+                            for _ in range(batch)])
+    point = [(-1) ** i * (3 * i + 1) for i in range(nv)]
+    root, proof, inner, _ = oracle.commit_prove(desc, polys, batch, point)
+    pp = params_for(zipgpu, ek, D, ck, nv, L, device=False)
+    comm = zipgpu.ZipPlusCommitment(root, batch)
+    zipgpu.ZipPlus.verify(pp, comm, point, inner, proof)
+    for pos in (5, len(proof) // 3, len(proof) - 3):
+        bad = bytearray(proof)
+        bad[pos] ^= 4
+        with pytest.raises(zipgpu.ZipError) as e:
+            zipgpu.ZipPlus.verify(pp, comm, point, inner, bytes(bad))
+        assert e.value.status in (2, 3)
+    with pytest.raises(zipgpu.ZipError) as e:
+        zipgpu.ZipPlus.verify(pp, comm, point, inner, proof[: len(proof) // 2])
+    assert e.value.status == 3
+
+
+def test_device_entry_points_need_a_context(zipgpu):
+    pp = params_for(zipgpu, 1, 32, 0, 10, 1024, device=False)
+    with pytest.raises(zipgpu.ZipError) as e:
+        zipgpu.ZipPlus.commit(pp, [np.zeros(1024, np.uint64)])
+    assert e.value.status == 8

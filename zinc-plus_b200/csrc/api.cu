@@ -1,0 +1,1127 @@
+// Commit / prove / verify pipelines and the extern "C" ABI of include/zipgpu.h.
+#include <omp.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+
+#include "zg_internal.h"
+#include "zg_prove.h"
+
+namespace zg {
+const char *last_error();
+}
+
+using namespace zg;
+
+#define ZG_GUARD(expr)                                                                            \
+    try {                                                                                         \
+        return (expr);                                                                            \
+    } catch (const std::bad_alloc &) {                                                            \
+        set_error("host allocation failed");                                                      \
+        return ZG_ERR_OOM;                                                                        \
+    } catch (...) {                                                                               \
+        set_error("unexpected C++ exception");                                                    \
+        return ZG_ERR_INVALID_PARAM;                                                              \
+    }
+
+namespace {
+
+bool is_pow2(uint64_t x) { return x && !(x & (x - 1)); }
+uint32_t ilog2u(uint64_t x) { return 63 - __builtin_clzll(x); }
+uint32_t ilog_round_up(uint64_t x) { return is_pow2(x) ? ilog2u(x) : ilog2u(x) + 1; }
+
+// validate_input's bit budget for linear combinations (pcs/utils.rs:24-54).
+zg_status validate_budget(const zg_params *p, uint32_t batch) {
+    if (batch == 0) {
+        set_error("Batch must contain at least one polynomial");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    const uint32_t d = ilog2u(p->info.row_len);
+    const uint32_t codeword_bits = ilog_round_up(std::max<uint64_t>((uint64_t)p->d.rep * d, 1));
+    const uint32_t challenge_bits = p->D > 1 ? 256 : 128;  // Chal = i128; doubled with alphas
+    const uint32_t eval_bits = p->d.eval_kind == ZG_EVAL_BINPOLY ? 1 : 32;
+    const uint32_t actual = 2 * codeword_bits + ilog_round_up(std::max<uint32_t>(d, 1)) +
+                            challenge_bits + (eval_bits - 1) + ilog_round_up(batch);
+    if (actual > 64 * p->d.comb_limbs) {
+        set_error("The number of bits used for linear combinations is too large: %u bits, max "
+                  "allowed is %u bits",
+                  actual, 64 * p->d.comb_limbs);
+        return ZG_ERR_OVERFLOW;
+    }
+    return ZG_OK;
+}
+
+uint64_t dmask_of(uint32_t D) { return D >= 64 ? ~0ull : ((1ull << D) - 1); }
+
+i128 load_i128(const uint8_t *b) {
+    u128 v = 0;
+    for (int i = 15; i >= 0; i--) v = (v << 8) | b[i];
+    return (i128)v;
+}
+
+template <int L>
+void host_eq_table(const FieldCfg &f, const uint64_t *r, uint32_t n, std::vector<uint64_t> &out) {
+    // eq(x, r)[i] = prod_k (bit_k(i) ? r_k : 1 - r_k)   (poly/src/utils.rs:24-101)
+    out.assign((size_t)L << n, 0);
+    for (int w = 0; w < L; w++) out[w] = f.one[w];
+    size_t len = 1;
+    for (int k = (int)n - 1; k >= 0; k--) {
+        for (long i = (long)len - 1; i >= 0; i--) {
+            uint64_t b[L], t[L];
+            for (int w = 0; w < L; w++) b[w] = out[(size_t)i * L + w];
+            fmul<L>(r + (size_t)k * L, b, f.p, f.n0, t);
+            for (int w = 0; w < L; w++) out[(size_t)(2 * i + 1) * L + w] = t[w];
+            fsub<L>(b, t, f.p);
+            for (int w = 0; w < L; w++) out[(size_t)(2 * i) * L + w] = b[w];
+        }
+        len *= 2;
+    }
+}
+
+void host_eq(const FieldCfg &f, const uint64_t *r, uint32_t n, std::vector<uint64_t> &out) {
+    if (f.L == 3) host_eq_table<3>(f, r, n, out);
+    else host_eq_table<4>(f, r, n, out);
+}
+
+void f_from_i128(const FieldCfg &f, i128 v, uint64_t *out) {
+    if (f.L == 3) from_i128<3>(v, f, out);
+    else from_i128<4>(v, f, out);
+}
+void f_from_signed(const FieldCfg &f, const uint64_t *x, int limbs, uint64_t *out) {
+    if (f.L == 3) from_signed<3>(x, limbs, f, out);
+    else from_signed<4>(x, limbs, f, out);
+}
+void f_mul(const FieldCfg &f, const uint64_t *a, const uint64_t *b, uint64_t *out) {
+    if (f.L == 3) fmul<3>(a, b, f.p, f.n0, out);
+    else fmul<4>(a, b, f.p, f.n0, out);
+}
+void f_add(const FieldCfg &f, uint64_t *a, const uint64_t *b) {
+    if (f.L == 3) fadd<3>(a, b, f.p);
+    else fadd<4>(a, b, f.p);
+}
+void f_sub(const FieldCfg &f, uint64_t *a, const uint64_t *b) {
+    if (f.L == 3) fsub<3>(a, b, f.p);
+    else fsub<4>(a, b, f.p);
+}
+
+size_t leaf_bytes_of(const zg_params *p, uint32_t batch) {
+    return (size_t)batch * p->info.num_rows * p->info.cw_bytes;
+}
+
+// Host encode_wide on Int<limbs> (wrapping), the verifier's re-encoding of the
+// combined row (iprs.rs:148-150 -> radix8.rs:21-161; raa.rs encode_wide).
+void host_encode_wide(const zg_params *p, const uint64_t *row, uint32_t limbs, uint64_t *out) {
+    const zg_params_info &I = p->info;
+    const uint32_t C = I.codeword_len;
+    if (p->d.code_kind == ZG_CODE_RAA) {
+        const uint32_t Lr = I.row_len;
+        std::vector<uint64_t> a((size_t)C * limbs), b((size_t)C * limbs);
+        for (uint32_t i = 0; i < C; i++)
+            std::memcpy(&a[(size_t)i * limbs], row + (size_t)(p->perm1[i] % Lr) * limbs, 8 * limbs);
+        for (uint32_t i = 1; i < C; i++) wide_add(&a[(size_t)i * limbs], &a[(size_t)(i - 1) * limbs], limbs);
+        for (uint32_t i = 0; i < C; i++)
+            std::memcpy(&b[(size_t)i * limbs], &a[(size_t)p->perm2[i] * limbs], 8 * limbs);
+        for (uint32_t i = 1; i < C; i++) wide_add(&b[(size_t)i * limbs], &b[(size_t)(i - 1) * limbs], limbs);
+        std::memcpy(out, b.data(), 8 * (size_t)C * limbs);
+        return;
+    }
+    const uint32_t bd = I.base_dim, bl = I.base_len, depth = I.depth;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)C; i++) {
+        uint32_t ch = (uint32_t)i / bd, rb = (uint32_t)i % bd, oct = 0, x = ch;
+        for (uint32_t k = 0; k < depth; k++) {
+            oct = (oct << 3) | (x & 7);
+            x >>= 3;
+        }
+        uint64_t *o = out + (size_t)i * limbs;
+        std::memset(o, 0, 8 * limbs);
+        for (uint32_t c = 0; c < bl; c++)
+            wide_mul_i128_add(o, row + ((size_t)oct + ((size_t)c << (3 * depth))) * limbs,
+                              (i128)p->bm[(size_t)rb * bl + c], (int)limbs);
+    }
+    std::vector<uint64_t> xs((size_t)8 * limbs);
+    for (uint32_t k = 0; k < depth; k++) {
+        const size_t sub = (size_t)bd << (3 * k);
+        const int64_t *tw = p->tw.data() + p->tw_off[k];
+        for (size_t blk = 0; blk < C; blk += 8 * sub) {
+            uint64_t *chunk = out + blk * limbs;
+            for (size_t i = 0; i < sub; i++) {
+                for (int j = 0; j < 8; j++)
+                    std::memcpy(&xs[(size_t)j * limbs], chunk + (j * sub + i) * limbs, 8 * limbs);
+                for (int r = 0; r < 8; r++) {
+                    uint64_t *y = chunk + (r * sub + i) * limbs;
+                    std::memcpy(y, xs.data(), 8 * limbs);
+                    for (int j = 1; j < 8; j++)
+                        wide_mul_i128_add(y, &xs[(size_t)j * limbs],
+                                          (i128)tw[(i * 7 + (j - 1)) * 8 + ((r * j) & 7)], (int)limbs);
+                }
+            }
+        }
+    }
+}
+
+// get_path_directions + MerkleProof::verify (merkle.rs:282-410).
+bool merkle_verify(const uint8_t root[32], const uint8_t *col, size_t col_len, uint64_t li,
+                   uint64_t lc, const uint8_t *sib, uint64_t ns, uint64_t expected) {
+    if (li != expected) return false;
+    uint8_t cur8[32];
+    b3::hash(col, col_len, cur8);
+    if (lc == 1) return li == 0 && ns == 0 && std::memcmp(cur8, root, 32) == 0;
+    std::vector<int> dirs;
+    uint64_t size = lc, idx = li;
+    while (size > 1) {
+        uint64_t p2 = 1;
+        while (p2 < size) p2 <<= 1;
+        const uint64_t split = p2 / 2;
+        if (idx < split) {
+            dirs.push_back(0);
+            size = split;
+        } else {
+            dirs.push_back(1);
+            size -= split;
+            idx -= split;
+        }
+    }
+    std::reverse(dirs.begin(), dirs.end());
+    if (dirs.size() != ns) return false;
+    uint32_t cur[8];
+    for (int i = 0; i < 8; i++) cur[i] = b3::load_le32(cur8 + 4 * i);
+    for (size_t i = 0; i < dirs.size(); i++) {
+        uint32_t s[8];
+        for (int w = 0; w < 8; w++) s[w] = b3::load_le32(sib + 32 * i + 4 * w);
+        const bool root_merge = i + 1 == dirs.size();
+        if (dirs[i] == 0) b3::parent_cv(cur, s, root_merge, cur);
+        else b3::parent_cv(s, cur, root_merge, cur);
+    }
+    uint8_t out[32];
+    for (int i = 0; i < 8; i++) b3::store_le32(out + 4 * i, cur[i]);
+    return std::memcmp(out, root, 32) == 0;
+}
+
+}  // namespace
+
+namespace zg {
+
+// ------------------------------------------------------------------- commit
+zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **out) {
+    ZG_TRY(validate_budget(p, batch));
+    zg_ctx *ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    const uint32_t C = p->info.codeword_len;
+    const uint32_t nrows = batch * p->info.num_rows;
+    const size_t leaf_bytes = leaf_bytes_of(p, batch);
+    if (leaf_bytes > 0xFFFFFFFFull) {
+        set_error("leaf too large");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    std::unique_ptr<zg_hint> h(new zg_hint());
+    h->params = p;
+    h->batch = batch;
+    h->nrows = nrows;
+    h->depth = ilog2u(C);
+    size_t off = 0;
+    for (uint32_t k = 0, n = C; k <= h->depth; k++, n /= 2) {
+        h->layer_off.push_back(off);
+        off += n;
+    }
+    ZG_CUDA(cudaMalloc(&h->d_cw, (size_t)C * leaf_bytes));
+    cudaError_t e = cudaMalloc(&h->d_tree, off * 32);
+    if (e != cudaSuccess) {
+        cudaFree(h->d_cw);
+        h->d_cw = nullptr;
+        ZG_CUDA(e);
+    }
+    e = cudaMalloc(&h->d_layer_off, sizeof(uint64_t) * h->layer_off.size());
+    if (e != cudaSuccess) {
+        cudaFree(h->d_cw);
+        cudaFree(h->d_tree);
+        h->d_cw = nullptr;
+        h->d_tree = nullptr;
+        ZG_CUDA(e);
+    }
+    std::vector<uint64_t> lo(h->layer_off.begin(), h->layer_off.end());
+    auto fail = [&](zg_status st) {
+        cudaFree(h->d_cw);
+        cudaFree(h->d_tree);
+        cudaFree(h->d_layer_off);
+        h->d_cw = h->d_tree = nullptr;
+        h->d_layer_off = nullptr;
+        return st;
+    };
+    if (cudaMemcpyAsync(h->d_layer_off, lo.data(), sizeof(uint64_t) * lo.size(),
+                        cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(ZG_ERR_CUDA);
+    zg_status st = launch_encode(p, polys_d, nrows, h->d_cw, true, s);
+    if (st != ZG_OK) return fail(st);
+    st = launch_leaf_hash(ctx, h->d_cw, C, (uint32_t)leaf_bytes, h->d_tree, s);
+    if (st != ZG_OK) return fail(st);
+    st = launch_merkle_levels(ctx, h->d_tree, C, h->layer_off, s);
+    if (st != ZG_OK) return fail(st);
+    if (cudaMemcpyAsync(h->root, h->d_tree + h->layer_off.back() * 32, 32, cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        set_error("commit failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return fail(ZG_ERR_CUDA);
+    }
+    *out = h.release();
+    return ZG_OK;
+}
+
+// -------------------------------------------------------------------- prove
+zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
+                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out) {
+    if (!t->has_field || t->f.L != (int)p->d.field_limbs) {
+        set_error("transcript has no field configuration of %u limbs (sample it first)",
+                  p->d.field_limbs);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (!hint || hint->params != p || hint->batch != batch) {
+        set_error("hint does not match the parameters or batch size");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    ZG_TRY(validate_budget(p, batch));
+    zg_ctx *ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    const FieldCfg &f = t->f;
+    const int L = f.L;
+    const uint32_t R = p->info.num_rows, RL = p->info.row_len, C = p->info.codeword_len;
+    const uint32_t CL = p->d.comb_limbs, D = p->D, nv = p->d.num_vars;
+    const uint32_t lr = ilog2u(R), nhi = nv - lr;
+    const bool binary = p->d.eval_kind == ZG_EVAL_BINPOLY;
+
+    // point -> F, q0 (host), q1 (device) (point_to_tensor, pcs/utils.rs:90-114)
+    std::vector<uint64_t> pf((size_t)(nv + 1) * L), omr((size_t)(nv + 1) * L);
+    for (uint32_t i = 0; i < nv; i++) {
+        f_from_i128(f, load_i128(point + 16 * i), &pf[(size_t)i * L]);
+        std::memcpy(&omr[(size_t)i * L], f.one, 8 * L);
+        f_sub(f, &omr[(size_t)i * L], &pf[(size_t)i * L]);
+    }
+    std::vector<uint64_t> q0;
+    if (lr) host_eq(f, &pf[(size_t)nhi * L], lr, q0);
+    else q0.assign(f.one, f.one + L);
+
+    // alphas (phase_prove.rs:157-161): Comb::DEGREE_BOUND + 1 = D challenges
+    const uint32_t na = binary && D > 1 ? D : 0;
+    std::vector<i128> alphas((size_t)batch * std::max<uint32_t>(na, 1), (i128)1);
+    if (binary && D == 1) {
+        for (uint32_t b = 0; b < batch; b++) alphas[b] = 1;
+    }
+    for (uint32_t b = 0; b < batch; b++)
+        for (uint32_t i = 0; i < na; i++) alphas[(size_t)b * na + i] = tr_challenge_i128(t);
+    const uint32_t Da = binary ? std::max<uint32_t>(na, 1) : 1;
+
+    // device inputs: alphas | r_hi | omr_hi
+    const size_t a_bytes = alphas.size() * 16, r_bytes = (size_t)std::max<uint32_t>(nhi, 1) * L * 8;
+    const size_t in_bytes = a_bytes + 2 * r_bytes + 16 * (size_t)R + 4 * (size_t)p->d.num_openings + 256;
+    ZG_TRY(ctx->prove_in.ensure(in_bytes));
+    ZG_TRY(ctx->pin_in.ensure(in_bytes));
+    uint8_t *hin = ctx->pin_in.as<uint8_t>();
+    uint8_t *din = ctx->prove_in.as<uint8_t>();
+    std::memcpy(hin, alphas.data(), a_bytes);
+    std::memcpy(hin + a_bytes, pf.data(), (size_t)nhi * L * 8);
+    std::memcpy(hin + a_bytes + r_bytes, omr.data(), (size_t)nhi * L * 8);
+    ZG_CUDA(cudaMemcpyAsync(din, hin, a_bytes + 2 * r_bytes, cudaMemcpyHostToDevice, s));
+
+    const uint32_t nparts = (RL + 255) / 256;
+    const size_t q1_bytes = (size_t)RL * L * 8;
+    const size_t part_bytes = (size_t)batch * R * nparts * L * 8;
+    const size_t b_bytes = (size_t)R * L * 8;
+    const size_t comb_bytes = (size_t)RL * CL * 8;
+    const size_t leaf_bytes = leaf_bytes_of(p, batch);
+    const size_t open_bytes = leaf_bytes + 24 + 32 * (size_t)hint->depth;
+    const size_t tail_bytes = comb_bytes + open_bytes * p->d.num_openings;
+    const size_t out_bytes = q1_bytes + part_bytes + b_bytes + tail_bytes + 64;
+    ZG_TRY(ctx->prove_out.ensure(out_bytes));
+    ZG_TRY(ctx->wprime.ensure((size_t)batch * R * RL * CL * 8));
+    uint8_t *dout = ctx->prove_out.as<uint8_t>();
+    uint64_t *q1_d = reinterpret_cast<uint64_t *>(dout);
+    uint64_t *part_d = reinterpret_cast<uint64_t *>(dout + q1_bytes);
+    uint64_t *b_d = reinterpret_cast<uint64_t *>(dout + q1_bytes + part_bytes);
+    uint8_t *tail_d = dout + q1_bytes + part_bytes + b_bytes;
+    tail_d = reinterpret_cast<uint8_t *>(((uintptr_t)tail_d + 15) & ~(uintptr_t)15);
+
+    if (nhi) {
+        ZG_TRY(launch_eq_table(ctx, reinterpret_cast<const uint64_t *>(din + a_bytes),
+                               reinterpret_cast<const uint64_t *>(din + a_bytes + r_bytes), nhi, f,
+                               q1_d, s));
+    } else {
+        ZG_CUDA(cudaMemcpyAsync(q1_d, f.one, 8 * L, cudaMemcpyHostToDevice, s));
+    }
+    ProjectArgs pa{polys_d, binary ? 1 : 0, reinterpret_cast<const i128 *>(din), Da,
+                   dmask_of(D), q1_d, RL, R, batch, CL, &f, ctx->wprime.as<uint64_t>(), part_d, b_d};
+    ZG_TRY(launch_project_rows(ctx, pa, s));
+    ZG_TRY(ctx->pin_out.ensure(std::max(b_bytes, tail_bytes) + 64));
+    uint64_t *hb = ctx->pin_out.as<uint64_t>();
+    ZG_CUDA(cudaMemcpyAsync(hb, b_d, b_bytes, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(cudaStreamSynchronize(s));
+
+    // write_field_elements(b) (pcs_transcript.rs:99-142): no length prefix for
+    // Uint<L>; modulus | inner per element, each absorbed.
+    std::vector<uint64_t> bv(hb, hb + (size_t)R * L);
+    const size_t fb = 8 * (size_t)L;
+    for (uint32_t j = 0; j < R; j++) {
+        tr_absorb_field(t, &bv[(size_t)j * L]);
+        const uint8_t *mod = reinterpret_cast<const uint8_t *>(f.p);
+        const uint8_t *inr = reinterpret_cast<const uint8_t *>(&bv[(size_t)j * L]);
+        t->stream.insert(t->stream.end(), mod, mod + fb);
+        t->stream.insert(t->stream.end(), inr, inr + fb);
+    }
+    uint64_t ev[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
+    for (uint32_t j = 0; j < R; j++) {
+        uint64_t tmp[MAX_FIELD_LIMBS];
+        f_mul(f, &q0[(size_t)j * L], &bv[(size_t)j * L], tmp);
+        f_add(f, ev, tmp);
+    }
+    std::vector<i128> coeffs(R, (i128)1);
+    if (R > 1)
+        for (uint32_t j = 0; j < R; j++) coeffs[j] = tr_challenge_i128(t);
+    std::vector<uint32_t> idxs(p->d.num_openings);
+    for (uint32_t o = 0; o < p->d.num_openings; o++) idxs[o] = tr_challenge_u32(t) % C;
+
+    // second upload: coeffs | indices
+    const size_t c_off = 0, i_off = 16 * (size_t)R;
+    uint8_t *hin2 = hin + ((a_bytes + 2 * r_bytes + 15) & ~(size_t)15);
+    uint8_t *din2 = din + ((a_bytes + 2 * r_bytes + 15) & ~(size_t)15);
+    std::memcpy(hin2 + c_off, coeffs.data(), 16 * (size_t)R);
+    std::memcpy(hin2 + i_off, idxs.data(), 4 * idxs.size());
+    ZG_CUDA(cudaMemcpyAsync(din2, hin2, i_off + 4 * idxs.size(), cudaMemcpyHostToDevice, s));
+    CombineArgs ca{ctx->wprime.as<uint64_t>(), reinterpret_cast<const i128 *>(din2 + c_off),
+                   batch, R, RL, CL, reinterpret_cast<uint64_t *>(tail_d), hint->d_cw,
+                   (uint32_t)leaf_bytes, hint->d_tree, hint->d_layer_off, hint->depth, C,
+                   p->d.num_openings, reinterpret_cast<const uint32_t *>(din2 + i_off),
+                   tail_d + comb_bytes};
+    ZG_TRY(launch_combined_and_openings(ctx, ca, s));
+    uint8_t *htail = ctx->pin_out.as<uint8_t>();
+    ZG_CUDA(cudaMemcpyAsync(htail, tail_d, tail_bytes, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(cudaStreamSynchronize(s));
+    t->stream.insert(t->stream.end(), htail, htail + tail_bytes);
+    if (eval_out) std::memcpy(eval_out, ev, fb);
+    return ZG_OK;
+}
+
+// ------------------------------------------------------------------- verify
+zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
+                      const uint8_t *eval, const uint8_t *proof, size_t proof_len) {
+    ZG_TRY(validate_budget(p, batch));
+    zg_transcript tr;
+    tr_absorb_slice(&tr, root, 32);
+    const int L = (int)p->d.field_limbs;
+    uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
+    tr_get_prime(&tr, L, prime);
+    field_cfg_init(tr.f, prime, L);
+    tr.has_field = true;
+    const FieldCfg &f = tr.f;
+    const uint32_t R = p->info.num_rows, RL = p->info.row_len, C = p->info.codeword_len;
+    const uint32_t CL = p->d.comb_limbs, D = p->D, nv = p->d.num_vars;
+    const uint32_t lr = ilog2u(R), nhi = nv - lr;
+    const bool binary = p->d.eval_kind == ZG_EVAL_BINPOLY;
+    // sample_alphas (phase_verify.rs:247-261)
+    const uint32_t na = binary && D > 1 ? D : 1;
+    std::vector<i128> alphas((size_t)batch * na, (i128)1);
+    if (binary && D > 1)
+        for (auto &a : alphas) a = tr_challenge_i128(&tr);
+    std::vector<uint64_t> pf((size_t)(nv + 1) * L);
+    for (uint32_t i = 0; i < nv; i++) f_from_i128(f, load_i128(point + 16 * i), &pf[(size_t)i * L]);
+    std::vector<uint64_t> q0, q1;
+    if (lr) host_eq(f, &pf[(size_t)nhi * L], lr, q0);
+    else q0.assign(f.one, f.one + L);
+    if (nhi) host_eq(f, pf.data(), nhi, q1);
+    else q1.assign(f.one, f.one + L);
+
+    size_t pos = 0;
+    auto take = [&](size_t n) -> const uint8_t * {
+        if (pos + n > proof_len) return nullptr;
+        const uint8_t *r = proof + pos;
+        pos += n;
+        return r;
+    };
+    const size_t fb = 8 * (size_t)L;
+    std::vector<uint64_t> bv((size_t)R * L);
+    for (uint32_t j = 0; j < R; j++) {
+        const uint8_t *mod = take(fb), *inr = take(fb);
+        if (!mod || !inr) {
+            set_error("proof truncated while reading b");
+            return ZG_ERR_SERIALIZATION;
+        }
+        if (std::memcmp(mod, f.p, fb) != 0) {
+            set_error("field element modulus differs from the sampled field");
+            return ZG_ERR_INVALID_OPEN;
+        }
+        std::memcpy(&bv[(size_t)j * L], inr, fb);
+        tr_absorb_field(&tr, &bv[(size_t)j * L]);
+    }
+    // check 1: <q0, b> == eval
+    uint64_t acc[MAX_FIELD_LIMBS] = {0, 0, 0, 0}, tmp[MAX_FIELD_LIMBS];
+    for (uint32_t j = 0; j < R; j++) {
+        f_mul(f, &q0[(size_t)j * L], &bv[(size_t)j * L], tmp);
+        f_add(f, acc, tmp);
+    }
+    if (std::memcmp(acc, eval, fb) != 0) {
+        set_error("Evaluation consistency failure");
+        return ZG_ERR_INVALID_OPEN;
+    }
+    std::vector<i128> coeffs(R, (i128)1);
+    if (R > 1)
+        for (auto &c : coeffs) c = tr_challenge_i128(&tr);
+    const uint8_t *cr = take((size_t)RL * CL * 8);
+    if (!cr) {
+        set_error("proof truncated while reading the combined row");
+        return ZG_ERR_SERIALIZATION;
+    }
+    std::vector<uint64_t> comb((size_t)RL * CL), enc((size_t)C * CL);
+    std::memcpy(comb.data(), cr, comb.size() * 8);
+    host_encode_wide(p, comb.data(), CL, enc.data());
+    // check 2: <F(comb), q1> == <F(coeffs), b>
+    uint64_t lhs[MAX_FIELD_LIMBS] = {0, 0, 0, 0}, rhs[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
+    for (uint32_t c = 0; c < RL; c++) {
+        uint64_t fe[MAX_FIELD_LIMBS];
+        f_from_signed(f, &comb[(size_t)c * CL], (int)CL, fe);
+        f_mul(f, fe, &q1[(size_t)c * L], tmp);
+        f_add(f, lhs, tmp);
+    }
+    for (uint32_t j = 0; j < R; j++) {
+        uint64_t fe[MAX_FIELD_LIMBS];
+        f_from_i128(f, coeffs[j], fe);
+        f_mul(f, fe, &bv[(size_t)j * L], tmp);
+        f_add(f, rhs, tmp);
+    }
+    if (std::memcmp(lhs, rhs, fb) != 0) {
+        set_error("Coherence failure");
+        return ZG_ERR_INVALID_OPEN;
+    }
+    const size_t cwb = p->info.cw_bytes, colbytes = (size_t)batch * R * cwb;
+    for (uint32_t o = 0; o < p->d.num_openings; o++) {
+        const uint32_t idx = tr_challenge_u32(&tr) % C;
+        const uint8_t *col = take(colbytes), *hdr = take(24);
+        if (!col || !hdr) {
+            set_error("proof truncated in column opening %u", o);
+            return ZG_ERR_SERIALIZATION;
+        }
+        uint64_t li, lc, np;
+        std::memcpy(&li, hdr, 8);
+        std::memcpy(&lc, hdr + 8, 8);
+        std::memcpy(&np, hdr + 16, 8);
+        if (np == 0 || li >= lc || np > 64) {
+            set_error("malformed Merkle proof in opening %u", o);
+            return ZG_ERR_SERIALIZATION;
+        }
+        const uint8_t *sib = take(32 * np);
+        if (!sib) {
+            set_error("proof truncated in Merkle path %u", o);
+            return ZG_ERR_SERIALIZATION;
+        }
+        // check 3 (verify_column_testing_batched, phase_verify.rs:267-304)
+        uint64_t sum[MAX_COMB_LIMBS] = {0};
+        for (uint32_t b = 0; b < batch; b++)
+            for (uint32_t j = 0; j < R; j++) {
+                const uint8_t *e = col + ((size_t)b * R + j) * cwb;
+                uint64_t v[MAX_COMB_LIMBS] = {0};
+                if (!binary) {
+                    uint64_t x[2];
+                    std::memcpy(x, e, 16);
+                    wide_sext(x, 2, v, (int)CL);
+                } else {
+                    for (uint32_t i = 0; i < D; i++) {
+                        int64_t c64;
+                        if (cwb == 8 * (size_t)D) {
+                            std::memcpy(&c64, e + 8 * i, 8);
+                        } else {
+                            int32_t c32;
+                            std::memcpy(&c32, e + 4 * i, 4);
+                            c64 = c32;
+                        }
+                        uint64_t x[MAX_COMB_LIMBS], one = (uint64_t)c64;
+                        wide_sext(&one, 1, x, (int)CL);
+                        wide_mul_i128_add(v, x, alphas[(size_t)b * na + (na > 1 ? i : 0)], (int)CL);
+                    }
+                }
+                wide_mul_i128_add(sum, v, coeffs[j], (int)CL);
+            }
+        if (std::memcmp(sum, &enc[(size_t)idx * CL], 8 * CL) != 0) {
+            set_error("Proximity failure");
+            return ZG_ERR_INVALID_OPEN;
+        }
+        if (!merkle_verify(root, col, colbytes, li, lc, sib, np, idx)) {
+            set_error("Column opening verification failed");
+            return ZG_ERR_INVALID_OPEN;
+        }
+    }
+    return ZG_OK;
+}
+
+}  // namespace zg
+
+// ======================================================================= ABI
+extern "C" {
+
+const char *zg_last_error(void) { return zg::last_error(); }
+const char *zg_version(void) { return "zipgpu 0.1 (sm_100a)"; }
+
+zg_status zg_ctx_create(int device, zg_ctx **out) {
+    if (!out) return ZG_ERR_INVALID_PARAM;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        set_error("no CUDA device available");
+        return ZG_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) {
+        set_error("device %d out of range (%d devices)", device, n);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    ZG_CUDA(cudaSetDevice(device));
+    std::unique_ptr<zg_ctx> c(new zg_ctx());
+    c->device = device;
+    ZG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    ZG_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    *out = c.release();
+    return ZG_OK;
+}
+
+zg_status zg_ctx_destroy(zg_ctx *ctx) {
+    if (!ctx) return ZG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out})
+        b->release();
+    ctx->pin_in.release();
+    ctx->pin_out.release();
+    ktimer_collect(ctx);
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ZG_OK;
+}
+
+uint64_t zg_ctx_kernel_launches(const zg_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+zg_status zg_ctx_set_kernel_timing(zg_ctx *ctx, int enable) {
+    if (!ctx) return ZG_ERR_INVALID_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    ktimer_collect(ctx);
+    ctx->timing = enable != 0;
+    return ZG_OK;
+}
+
+zg_status zg_ctx_kernel_timing_report(zg_ctx *ctx, char *buf, size_t cap, size_t *len) {
+    if (!ctx || !len) return ZG_ERR_INVALID_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    ktimer_collect(ctx);
+    std::string out;
+    for (auto &t : ctx->totals) {
+        char line[256];
+        snprintf(line, sizeof line, "%s,%llu,%.6f\n", t.first.c_str(),
+                 (unsigned long long)t.second.second, t.second.first);
+        out += line;
+    }
+    *len = out.size();
+    if (buf && cap) {
+        size_t n = std::min(cap - 1, out.size());
+        std::memcpy(buf, out.data(), n);
+        buf[n] = 0;
+    }
+    ctx->totals.clear();
+    return ZG_OK;
+}
+void *zg_ctx_stream(zg_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+// ctx may be NULL: the parameters are then host-only (tables, encode_wide,
+// verify) and the device entry points report ZG_ERR_NO_DEVICE.
+static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_params **out) {
+    if (!desc || !out) return ZG_ERR_INVALID_PARAM;
+    *out = nullptr;
+    zg_params_desc d = *desc;
+    if (d.eval_kind > ZG_EVAL_BINPOLY || d.code_kind > ZG_CODE_RAA) {
+        set_error("unknown evaluation or code kind");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (d.eval_kind == ZG_EVAL_I32) d.degree_plus_one = 1;
+    if (d.eval_kind == ZG_EVAL_BINPOLY && (d.degree_plus_one < 1 || d.degree_plus_one > 64)) {
+        set_error("BinaryPoly coefficient count must be in 1..64");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (!is_pow2(d.rep)) {
+        set_error("Repetition factor must be a power of two");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (d.num_vars > 30 || !is_pow2(d.row_len) || ((1ull << d.num_vars) % d.row_len) != 0) {
+        set_error("poly_size (2^%u) must be divisible by row_len (%u)", d.num_vars, d.row_len);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (d.comb_limbs < 1 || d.comb_limbs > MAX_COMB_LIMBS || (d.field_limbs != 3 && d.field_limbs != 4)) {
+        set_error("comb_limbs must be 1..8 and field_limbs 3 or 4");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (d.num_openings == 0) d.num_openings = 147;
+    std::unique_ptr<zg_params> p(new zg_params());
+    p->ctx = ctx;
+    p->d = d;
+    p->D = d.eval_kind == ZG_EVAL_BINPOLY ? d.degree_plus_one : 1;
+    zg_params_info &I = p->info;
+    I.row_len = d.row_len;
+    I.num_rows = (uint32_t)((1ull << d.num_vars) / d.row_len);
+    I.eval_bytes = d.eval_kind == ZG_EVAL_BINPOLY ? 8 : 4;
+    I.comb_bytes = 8 * d.comb_limbs;
+    I.field_bytes = 8 * d.field_limbs;
+    if (ctx) ZG_CUDA(cudaSetDevice(ctx->device));
+    if (d.code_kind == ZG_CODE_IPRS) {
+        const uint32_t depth = d.iprs_depth ? d.iprs_depth : iprs_optimal_depth(d.row_len);
+        if (!iprs_build_tables(d.row_len, depth, d.rep, p.get())) {
+            set_error("invalid IPRS parameters: row_len %u, depth %u, rate 1/%u", d.row_len,
+                      depth, d.rep);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        I.cw_bytes = d.eval_kind == ZG_EVAL_BINPOLY ? 8 * p->D : 16;
+        const uint32_t bd = I.base_dim, bl = I.base_len;
+        std::vector<int32_t> bmT((size_t)bd * bl);
+        for (uint32_t r = 0; r < bd; r++)
+            for (uint32_t c = 0; c < bl; c++) bmT[(size_t)c * bd + r] = (int32_t)p->bm[(size_t)r * bl + c];
+        std::vector<int32_t> tw32(p->tw.size());
+        std::vector<size_t> offs;
+        size_t o = 0;
+        for (uint32_t k = 0; k < depth; k++) {
+            const size_t sub = (size_t)bd << (3 * k);
+            offs.push_back(o);
+            for (size_t i = 0; i < sub; i++)
+                for (int e = 0; e < 56; e++) tw32[o + (size_t)e * sub + i] = (int32_t)p->tw[p->tw_off[k] + i * 56 + e];
+            o += sub * 56;
+        }
+        p->tw_dev_off = offs;
+        if (ctx) {
+            ZG_CUDA(cudaMalloc(&p->d_bmT, bmT.size() * 4));
+            ZG_CUDA(cudaMemcpy(p->d_bmT, bmT.data(), bmT.size() * 4, cudaMemcpyHostToDevice));
+            ZG_CUDA(cudaMalloc(&p->d_tw, std::max<size_t>(tw32.size(), 1) * 4));
+            if (!tw32.empty())
+                ZG_CUDA(cudaMemcpy(p->d_tw, tw32.data(), tw32.size() * 4, cudaMemcpyHostToDevice));
+        }
+    } else {
+        const uint64_t n = (uint64_t)d.row_len * d.rep;
+        if (n > (1u << 24)) {
+            set_error("RAA codeword too long");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        // RaaCode::new width check (raa.rs:54-74): Cw coefficients are i32.
+        const uint32_t eval_bits = d.eval_kind == ZG_EVAL_BINPOLY ? 1 : 32;
+        const uint32_t need = eval_bits + 2 * ilog2u(d.row_len) + 2 * ilog2u(d.rep);
+        if (need > 32) {
+            set_error("Cannot fit %u-bit wide codeword entries in 32 bits entries", need);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        I.codeword_len = (uint32_t)n;
+        I.cw_bytes = 4 * p->D;
+        p->perm1.resize(n);
+        p->perm2.resize(n);
+        stdrng_shuffle_identity(1, (uint32_t)n, p->perm1.data());
+        stdrng_shuffle_identity(2, (uint32_t)n, p->perm2.data());
+        if (ctx) {
+            ZG_CUDA(cudaMalloc(&p->d_perm, n * 8));
+            ZG_CUDA(cudaMemcpy(p->d_perm, p->perm1.data(), n * 4, cudaMemcpyHostToDevice));
+            ZG_CUDA(cudaMemcpy(p->d_perm + n, p->perm2.data(), n * 4, cudaMemcpyHostToDevice));
+        }
+    }
+    *out = p.release();
+    return ZG_OK;
+}
+
+zg_status zg_params_create(zg_ctx *ctx, const zg_params_desc *desc, zg_params **out) {
+    ZG_GUARD(params_create_impl(ctx, desc, out));
+}
+
+zg_status zg_params_destroy(zg_params *p) {
+    if (!p) return ZG_OK;
+    if (p->ctx) {
+        cudaSetDevice(p->ctx->device);
+        cudaFree(p->d_bmT);
+        cudaFree(p->d_tw);
+        cudaFree(p->d_perm);
+    }
+    delete p;
+    return ZG_OK;
+}
+
+zg_status zg_params_get_info(const zg_params *p, zg_params_info *info) {
+    if (!p || !info) return ZG_ERR_INVALID_PARAM;
+    *info = p->info;
+    return ZG_OK;
+}
+
+zg_status zg_params_iprs_tables(const zg_params *p, int64_t *base_matrix, int64_t *twiddles) {
+    if (!p || p->d.code_kind != ZG_CODE_IPRS) return ZG_ERR_INVALID_PARAM;
+    if (base_matrix) std::memcpy(base_matrix, p->bm.data(), p->bm.size() * 8);
+    if (twiddles && !p->tw.empty()) std::memcpy(twiddles, p->tw.data(), p->tw.size() * 8);
+    return ZG_OK;
+}
+
+zg_status zg_params_raa_perms(const zg_params *p, uint32_t *perm1, uint32_t *perm2) {
+    if (!p || p->d.code_kind != ZG_CODE_RAA) return ZG_ERR_INVALID_PARAM;
+    if (perm1) std::memcpy(perm1, p->perm1.data(), p->perm1.size() * 4);
+    if (perm2) std::memcpy(perm2, p->perm2.data(), p->perm2.size() * 4);
+    return ZG_OK;
+}
+
+static zg_status need_device(const zg_params *p) {
+    if (!p->ctx) {
+        set_error("parameters were created without a device context");
+        return ZG_ERR_NO_DEVICE;
+    }
+    return ZG_OK;
+}
+
+static zg_status encode_rows_impl(zg_params *p, const void *evals, void *cw_out) {
+    if (!p || !evals || !cw_out) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    zg_ctx *ctx = p->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    const zg_params_info &I = p->info;
+    const size_t in_bytes = (size_t)I.num_rows * I.row_len * I.eval_bytes;
+    const size_t out_bytes = (size_t)I.num_rows * I.codeword_len * I.cw_bytes;
+    ZG_TRY(ctx->evals.ensure(in_bytes));
+    DevBuf outb;
+    ZG_TRY(outb.ensure(out_bytes));
+    ZG_CUDA(cudaMemcpyAsync(ctx->evals.ptr, evals, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    zg_status st = launch_encode(p, ctx->evals.ptr, I.num_rows, outb.as<uint8_t>(), false, ctx->stream);
+    if (st == ZG_OK) {
+        cudaError_t e = cudaMemcpyAsync(cw_out, outb.ptr, out_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+            set_error("encode failed: %s", cudaGetErrorString(e));
+            st = ZG_ERR_CUDA;
+        }
+    }
+    outb.release();
+    return st;
+}
+
+zg_status zg_encode_rows(zg_params *p, const void *evals, void *cw_out) {
+    ZG_GUARD(encode_rows_impl(p, evals, cw_out));
+}
+
+zg_status zg_encode_rows_d(zg_params *p, const void *evals_d, void *cw_out_d, void *stream) {
+    if (!p || !evals_d || !cw_out_d) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : p->ctx->stream;
+    ZG_GUARD(launch_encode(p, evals_d, p->info.num_rows, static_cast<uint8_t *>(cw_out_d), false, s));
+}
+
+zg_status zg_encode_wide(zg_params *p, const uint64_t *row, uint32_t limbs, uint64_t *out) {
+    if (!p || !row || !out || limbs < 1 || limbs > MAX_COMB_LIMBS) return ZG_ERR_INVALID_PARAM;
+    try {
+        host_encode_wide(p, row, limbs, out);
+    } catch (...) {
+        set_error("encode_wide failed");
+        return ZG_ERR_OOM;
+    }
+    return ZG_OK;
+}
+
+static zg_status merkle_root_impl(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_t width,
+                                  uint32_t eb, uint8_t root[32]) {
+    if (!ctx || !rows || !root || n_rows == 0 || width == 0) {
+        set_error("MerkleTree::new needs a non-empty matrix");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (!is_pow2(width)) {
+        set_error("row_width.is_power_of_two()");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (((size_t)n_rows * eb) % 4 != 0) {
+        set_error("leaf size must be a multiple of 4 bytes");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    const size_t leaf = (size_t)n_rows * eb, total = leaf * width;
+    // row-major to leaf-major on the host (a utility entry point)
+    std::vector<uint8_t> lm(total);
+    const uint8_t *src = static_cast<const uint8_t *>(rows);
+    for (uint32_t r = 0; r < n_rows; r++)
+        for (uint32_t j = 0; j < width; j++)
+            std::memcpy(&lm[(size_t)j * leaf + (size_t)r * eb], src + ((size_t)r * width + j) * eb, eb);
+    std::vector<size_t> off;
+    size_t o = 0;
+    for (uint32_t n = width;; n /= 2) {
+        off.push_back(o);
+        o += n;
+        if (n == 1) break;
+    }
+    DevBuf cw, tree;
+    ZG_TRY(cw.ensure(total));
+    zg_status st = tree.ensure(o * 32);
+    if (st != ZG_OK) {
+        cw.release();
+        return st;
+    }
+    cudaStream_t s = ctx->stream;
+    st = ZG_OK;
+    if (cudaMemcpyAsync(cw.ptr, lm.data(), total, cudaMemcpyHostToDevice, s) != cudaSuccess) st = ZG_ERR_CUDA;
+    if (st == ZG_OK) st = launch_leaf_hash(ctx, cw.as<uint8_t>(), width, (uint32_t)leaf, tree.as<uint8_t>(), s);
+    if (st == ZG_OK) st = launch_merkle_levels(ctx, tree.as<uint8_t>(), width, off, s);
+    if (st == ZG_OK) {
+        if (cudaMemcpyAsync(root, tree.as<uint8_t>() + off.back() * 32, 32, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            set_error("merkle root failed");
+            st = ZG_ERR_CUDA;
+        }
+    }
+    cw.release();
+    tree.release();
+    return st;
+}
+
+zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_t width,
+                         uint32_t elem_bytes, uint8_t root[32]) {
+    ZG_GUARD(merkle_root_impl(ctx, rows, n_rows, width, elem_bytes, root));
+}
+
+static zg_status stage_polys(zg_params *p, const void *const *polys, uint32_t batch) {
+    if (!polys) return ZG_ERR_INVALID_PARAM;
+    zg_ctx *ctx = p->ctx;
+    const size_t pb = (size_t)p->info.num_rows * p->info.row_len * p->info.eval_bytes;
+    ZG_TRY(ctx->evals.ensure(pb * batch));
+    for (uint32_t b = 0; b < batch; b++) {
+        if (!polys[b]) return ZG_ERR_INVALID_PARAM;
+        ZG_CUDA(cudaMemcpyAsync(ctx->evals.as<uint8_t>() + pb * b, polys[b], pb,
+                                cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return ZG_OK;
+}
+
+static zg_status commit_impl(zg_params *p, const void *const *polys, uint32_t batch,
+                             zg_hint **hint, uint8_t root[32]) {
+    if (!p || !hint || !root) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    if (batch == 0) {
+        set_error("Batch must contain at least one polynomial");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    ZG_TRY(stage_polys(p, polys, batch));
+    ZG_TRY(commit_device(p, p->ctx->evals.ptr, batch, hint));
+    std::memcpy(root, (*hint)->root, 32);
+    return ZG_OK;
+}
+
+zg_status zg_commit(zg_params *p, const void *const *polys, uint32_t batch, zg_hint **hint,
+                    uint8_t root[32]) {
+    ZG_GUARD(commit_impl(p, polys, batch, hint, root));
+}
+
+static zg_status commit_d_impl(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **hint,
+                               uint8_t root[32]) {
+    if (!p || !polys_d || !hint || !root) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    ZG_TRY(commit_device(p, polys_d, batch, hint));
+    std::memcpy(root, (*hint)->root, 32);
+    return ZG_OK;
+}
+
+zg_status zg_commit_d(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **hint,
+                      uint8_t root[32]) {
+    ZG_GUARD(commit_d_impl(p, polys_d, batch, hint, root));
+}
+
+zg_status zg_hint_free(zg_hint *h) {
+    if (!h) return ZG_OK;
+    cudaSetDevice(h->params->ctx->device);
+    cudaFree(h->d_cw);
+    cudaFree(h->d_tree);
+    cudaFree(h->d_layer_off);
+    delete h;
+    return ZG_OK;
+}
+
+uint32_t zg_hint_batch(const zg_hint *h) { return h ? h->batch : 0; }
+
+zg_status zg_hint_codeword(const zg_hint *h, uint32_t poly, void *cw_out) {
+    if (!h || !cw_out || poly >= h->batch) return ZG_ERR_INVALID_PARAM;
+    zg_params *p = h->params;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    const uint32_t C = p->info.codeword_len, R = p->info.num_rows;
+    const size_t cwb = p->info.cw_bytes, leaf = (size_t)h->nrows * cwb;
+    std::vector<uint8_t> all((size_t)C * leaf);
+    ZG_CUDA(cudaMemcpy(all.data(), h->d_cw, all.size(), cudaMemcpyDeviceToHost));
+    uint8_t *out = static_cast<uint8_t *>(cw_out);
+    for (uint32_t r = 0; r < R; r++)
+        for (uint32_t j = 0; j < C; j++)
+            std::memcpy(out + ((size_t)r * C + j) * cwb, &all[(size_t)j * leaf + ((size_t)poly * R + r) * cwb], cwb);
+    return ZG_OK;
+}
+
+zg_status zg_transcript_new(const uint8_t *roots, uint32_t n_roots, zg_transcript **out) {
+    if (!out || (n_roots && !roots)) return ZG_ERR_INVALID_PARAM;
+    try {
+        zg_transcript *t = new zg_transcript();
+        for (uint32_t i = 0; i < n_roots; i++) tr_absorb_slice(t, roots + 32 * (size_t)i, 32);
+        *out = t;
+    } catch (...) {
+        set_error("host allocation failed");
+        return ZG_ERR_OOM;
+    }
+    return ZG_OK;
+}
+
+zg_status zg_transcript_free(zg_transcript *t) {
+    delete t;
+    return ZG_OK;
+}
+
+zg_status zg_transcript_absorb(zg_transcript *t, const uint8_t *buf, size_t n) {
+    if (!t || (n && !buf)) return ZG_ERR_INVALID_PARAM;
+    tr_absorb(t, buf, n);
+    return ZG_OK;
+}
+
+zg_status zg_transcript_absorb_slice(zg_transcript *t, const uint8_t *buf, size_t n) {
+    if (!t || (n && !buf)) return ZG_ERR_INVALID_PARAM;
+    tr_absorb_slice(t, buf, n);
+    return ZG_OK;
+}
+
+zg_status zg_transcript_challenge(zg_transcript *t, uint8_t *out, size_t n) {
+    if (!t || (n && !out)) return ZG_ERR_INVALID_PARAM;
+    tr_challenge(t, out, n);
+    return ZG_OK;
+}
+
+zg_status zg_transcript_sample_field(zg_transcript *t, uint32_t limbs, uint8_t *modulus_out) {
+    if (!t || (limbs != 3 && limbs != 4)) return ZG_ERR_INVALID_PARAM;
+    uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
+    tr_get_prime(t, (int)limbs, prime);
+    field_cfg_init(t->f, prime, (int)limbs);
+    t->has_field = true;
+    if (modulus_out) std::memcpy(modulus_out, prime, 8 * limbs);
+    return ZG_OK;
+}
+
+zg_status zg_transcript_proof(const zg_transcript *t, const uint8_t **data, size_t *len) {
+    if (!t || !data || !len) return ZG_ERR_INVALID_PARAM;
+    *data = t->stream.data();
+    *len = t->stream.size();
+    return ZG_OK;
+}
+
+static zg_status prove_impl(zg_params *p, zg_transcript *t, const void *const *polys,
+                            uint32_t batch, const uint8_t *point, const zg_hint *hint,
+                            uint8_t *eval_out) {
+    if (!p || !t || !point) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    if (batch == 0) {
+        set_error("Batch must contain at least one polynomial");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    ZG_TRY(stage_polys(p, polys, batch));
+    return prove_device(p, t, p->ctx->evals.ptr, batch, point, hint, eval_out);
+}
+
+zg_status zg_prove(zg_params *p, zg_transcript *t, const void *const *polys, uint32_t batch,
+                   const uint8_t *point, const zg_hint *hint, uint8_t *eval_out) {
+    ZG_GUARD(prove_impl(p, t, polys, batch, point, hint, eval_out));
+}
+
+static zg_status prove_d_impl(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
+                              const uint8_t *point, const zg_hint *hint, uint8_t *eval_out) {
+    if (!p || !t || !polys_d || !point) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    return prove_device(p, t, polys_d, batch, point, hint, eval_out);
+}
+
+zg_status zg_prove_d(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
+                     const uint8_t *point, const zg_hint *hint, uint8_t *eval_out) {
+    ZG_GUARD(prove_d_impl(p, t, polys_d, batch, point, hint, eval_out));
+}
+
+size_t zg_proof_size(const zg_params *p, uint32_t batch) {
+    if (!p) return 0;
+    const zg_params_info &I = p->info;
+    const size_t depth = ilog2u(I.codeword_len);
+    return (size_t)I.num_rows * 2 * I.field_bytes + (size_t)I.row_len * I.comb_bytes +
+           (size_t)p->d.num_openings * ((size_t)batch * I.num_rows * I.cw_bytes + 24 + 32 * depth);
+}
+
+static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t batch,
+                                     const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
+                                     uint8_t *proof, size_t *proof_len) {
+    zg_hint *h = nullptr;
+    ZG_TRY(commit_device(p, polys_d, batch, &h));
+    std::memcpy(root, h->root, 32);
+    zg_transcript t;
+    t.stream.reserve(zg_proof_size(p, batch));
+    tr_absorb_slice(&t, h->root, 32);
+    uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
+    tr_get_prime(&t, (int)p->d.field_limbs, prime);
+    field_cfg_init(t.f, prime, (int)p->d.field_limbs);
+    t.has_field = true;
+    zg_status st = prove_device(p, &t, polys_d, batch, point, h, eval_out);
+    zg_hint_free(h);
+    if (st != ZG_OK) return st;
+    if (*proof_len < t.stream.size()) {
+        *proof_len = t.stream.size();
+        set_error("proof buffer too small (%zu bytes needed)", t.stream.size());
+        return ZG_ERR_BUFFER_TOO_SMALL;
+    }
+    std::memcpy(proof, t.stream.data(), t.stream.size());
+    *proof_len = t.stream.size();
+    return ZG_OK;
+}
+
+static zg_status commit_prove_impl(zg_params *p, const void *const *polys, uint32_t batch,
+                                   const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
+                                   uint8_t *proof, size_t *proof_len) {
+    if (!p || !polys || !point || !root || !proof || !proof_len) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    if (batch == 0) {
+        set_error("Batch must contain at least one polynomial");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    ZG_TRY(stage_polys(p, polys, batch));
+    return commit_prove_common(p, p->ctx->evals.ptr, batch, point, root, eval_out, proof, proof_len);
+}
+
+zg_status zg_commit_prove(zg_params *p, const void *const *polys, uint32_t batch,
+                          const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
+                          uint8_t *proof, size_t *proof_len) {
+    ZG_GUARD(commit_prove_impl(p, polys, batch, point, root, eval_out, proof, proof_len));
+}
+
+static zg_status commit_prove_d_impl(zg_params *p, const void *polys_d, uint32_t batch,
+                                     const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
+                                     uint8_t *proof, size_t *proof_len) {
+    if (!p || !polys_d || !point || !root || !proof || !proof_len) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    return commit_prove_common(p, polys_d, batch, point, root, eval_out, proof, proof_len);
+}
+
+zg_status zg_commit_prove_d(zg_params *p, const void *polys_d, uint32_t batch,
+                            const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
+                            uint8_t *proof, size_t *proof_len) {
+    ZG_GUARD(commit_prove_d_impl(p, polys_d, batch, point, root, eval_out, proof, proof_len));
+}
+
+zg_status zg_verify(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
+                    const uint8_t *eval, const uint8_t *proof, size_t proof_len) {
+    if (!p || !root || !point || !eval || (proof_len && !proof)) return ZG_ERR_INVALID_PARAM;
+    ZG_GUARD(verify_host(p, root, batch, point, eval, proof, proof_len));
+}
+
+}  // extern "C"

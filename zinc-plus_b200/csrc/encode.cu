@@ -1,0 +1,432 @@
+// Linear-code encoders on sm_100a: the IPRS radix-8 pseudo-NTT over the
+// integers (zip-plus/src/code/iprs/pntt/radix8.rs:21-161) and the RAA code
+// (zip-plus/src/code/raa.rs:93-127).
+//
+// Layouts.  Evaluations: nrows rows of row_len values, row-major.
+// Intermediates: row-major [grow][position][lane].  The final codeword is
+// written either leaf-major [position][grow][lane] (a Merkle leaf's preimage
+// is then contiguous) or row-major like the reference's DenseRowMatrix.
+//
+// Arithmetic is wrapping two's complement at the codeword width (i64 lanes for
+// binary polynomials, i128 for i32 evaluations).  Wrapping arithmetic is a
+// ring homomorphism, so the order of additions does not change any output,
+// and when the reference's checked arithmetic does not overflow the values are
+// identical.
+#include "zg_internal.h"
+
+namespace zg {
+
+__device__ __forceinline__ uint32_t octet_reverse(uint32_t x, uint32_t digits) {
+    // octet_reversal.rs:6-29: reverse the base-8 digits of x.
+    uint32_t r = 0;
+    for (uint32_t i = 0; i < digits; i++) {
+        r = (r << 3) | (x & 7u);
+        x >>= 3;
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Base layer, binary evaluations (base_multiply_into_output, radix8.rs:117-161):
+//   out[ch*bd + rb][lane] = sum_c bit_lane(in[octrev(ch) + c*8^depth]) * bm[rb][c]
+// Block: 32 base rows x ceil(D/8) lane groups; the chunk's inputs are staged
+// in shared memory.  Binary sums are < 2^31 for every legal code (|bm| <= 32769,
+// base_len < 2^14), so they accumulate in int32.
+template <bool FINAL, bool LEAF_MAJOR>
+__global__ void __launch_bounds__(256) k_base_bin(const uint64_t *__restrict__ evals,
+                                                  const int32_t *__restrict__ bmT, void *out,
+                                                  uint32_t row_len, uint32_t bd, uint32_t bl,
+                                                  uint32_t depth, uint32_t C, uint32_t D,
+                                                  uint64_t dmask, uint32_t nrows) {
+    extern __shared__ uint64_t sx[];
+    const uint32_t grow = blockIdx.z, ch = blockIdx.y;
+    const uint32_t oct = octet_reverse(ch, depth);
+    const uint32_t shift = 3 * depth;
+    const uint64_t *row = evals + (size_t)grow * row_len;
+    const uint32_t tid = threadIdx.y * 32 + threadIdx.x, nthr = 32 * blockDim.y;
+    for (uint32_t c = tid; c < bl; c += nthr) sx[c] = row[oct + ((size_t)c << shift)] & dmask;
+    __syncthreads();
+    const uint32_t rb = blockIdx.x * 32 + threadIdx.x;
+    if (rb >= bd) return;
+    const uint32_t g = threadIdx.y;
+    int32_t acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[j] = 0;
+    const int32_t *bcol = bmT + rb;
+    for (uint32_t c = 0; c < bl; c++) {
+        const uint32_t x = (uint32_t)(sx[c] >> (8 * g));
+        const int32_t b = __ldg(bcol + (size_t)c * bd);
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[j] += (int32_t)((x >> j) & 1u) * b;
+    }
+    const size_t p = (size_t)ch * bd + rb;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const uint32_t lane = 8 * g + j;
+        if (lane >= D) break;
+        if (FINAL) {
+            int64_t *o = static_cast<int64_t *>(out);
+            size_t idx = LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane;
+            o[idx] = acc[j];
+        } else {
+            static_cast<int32_t *>(out)[((size_t)grow * C + p) * D + lane] = acc[j];
+        }
+    }
+}
+
+// One radix-8 stage (combine_stages, radix8.rs:58-113 with
+// apply_radix_8_butterflies, butterfly.rs:24-43) on 64-bit lanes:
+//   y_r = x_0 + sum_{j=1..7} x_j * tw[k][i][j-1][(r*j) mod 8]
+// One thread per (row, block position q, lane) computes all eight outputs.
+// Twiddles are stored [(j-1)*8 + t][i] for stage k.
+template <typename Tin, bool FINAL, bool LEAF_MAJOR>
+__global__ void __launch_bounds__(256) k_stage_bin(const Tin *__restrict__ in,
+                                                   int64_t *__restrict__ out,
+                                                   const int32_t *__restrict__ tw, uint32_t C,
+                                                   uint32_t sub, uint32_t D, uint32_t nrows) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t C8 = C / 8;
+    const size_t total = (size_t)nrows * C8 * D;
+    if (t >= total) return;
+    const uint32_t lane = (uint32_t)(t % D);
+    const size_t rq = t / D;
+    const uint32_t q = (uint32_t)(rq % C8), grow = (uint32_t)(rq / C8);
+    const uint32_t blk = q / sub, i = q % sub;
+    const size_t base = (size_t)grow * C + (size_t)blk * 8 * sub + i;
+    uint64_t x[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) x[j] = (uint64_t)(int64_t)in[(base + (size_t)j * sub) * D + lane];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        uint64_t y = x[0];
+#pragma unroll
+        for (int j = 1; j < 8; j++)
+            y += x[j] * (uint64_t)(int64_t)__ldg(tw + (size_t)((j - 1) * 8 + ((r * j) & 7)) * sub + i);
+        const size_t p = (size_t)blk * 8 * sub + (size_t)r * sub + i;
+        const size_t idx = (FINAL && LEAF_MAJOR) ? (p * nrows + grow) * D + lane
+                                                 : ((size_t)grow * C + p) * D + lane;
+        out[idx] = (int64_t)y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Base layer, i32 evaluations -> i128 codeword (MulByScalar i32 x i64 -> i128,
+// utils/src/mul_by_scalar.rs:89-95).  |sum| < 2^31 * 32769 * 2^14 < 2^61 fits i64.
+template <bool FINAL, bool LEAF_MAJOR>
+__global__ void __launch_bounds__(256) k_base_i32(const int32_t *__restrict__ evals,
+                                                  const int32_t *__restrict__ bmT, void *out,
+                                                  uint32_t row_len, uint32_t bd, uint32_t bl,
+                                                  uint32_t depth, uint32_t C, uint32_t nrows) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nrows * C) return;
+    const uint32_t p = (uint32_t)(t % C), grow = (uint32_t)(t / C);
+    const uint32_t ch = p / bd, rb = p % bd;
+    const uint32_t oct = octet_reverse(ch, depth), shift = 3 * depth;
+    const int32_t *row = evals + (size_t)grow * row_len;
+    int64_t acc = 0;
+    for (uint32_t c = 0; c < bl; c++)
+        acc += (int64_t)__ldg(row + oct + ((size_t)c << shift)) * (int64_t)__ldg(bmT + (size_t)c * bd + rb);
+    if (FINAL) {
+        i128 *o = static_cast<i128 *>(out);
+        o[LEAF_MAJOR ? (size_t)p * nrows + grow : (size_t)grow * C + p] = (i128)acc;
+    } else {
+        static_cast<int64_t *>(out)[(size_t)grow * C + p] = acc;
+    }
+}
+
+// Radix-8 stage on i128 values (MulByScalar i128 x i64, mul_by_scalar.rs:97-108).
+template <typename Tin, bool FINAL, bool LEAF_MAJOR>
+__global__ void __launch_bounds__(256) k_stage_i128(const Tin *__restrict__ in,
+                                                    i128 *__restrict__ out,
+                                                    const int32_t *__restrict__ tw, uint32_t C,
+                                                    uint32_t sub, uint32_t nrows) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t C8 = C / 8;
+    if (t >= (size_t)nrows * C8) return;
+    const uint32_t q = (uint32_t)(t % C8), grow = (uint32_t)(t / C8);
+    const uint32_t blk = q / sub, i = q % sub;
+    const size_t base = (size_t)grow * C + (size_t)blk * 8 * sub + i;
+    u128 x[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) x[j] = (u128)(i128)in[base + (size_t)j * sub];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        u128 y = x[0];
+#pragma unroll
+        for (int j = 1; j < 8; j++)
+            y += x[j] * (u128)(i128)__ldg(tw + (size_t)((j - 1) * 8 + ((r * j) & 7)) * sub + i);
+        const size_t p = (size_t)blk * 8 * sub + (size_t)r * sub + i;
+        out[(FINAL && LEAF_MAJOR) ? p * nrows + grow : (size_t)grow * C + p] = (i128)y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// RAA (raa.rs:93-127) for binary evaluations: repeat x rep, permute by perm1,
+// prefix-sum, permute by perm2, prefix-sum, on i32 lanes (wrapping).  One
+// block per (row, group of LG lanes); the first prefix sum stays in shared
+// memory.  perm[i] is the source position of output i (clone_shuffled).
+template <int LG>
+__device__ void block_exclusive_scan(uint32_t (&v)[LG], uint32_t *warp_tot) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    uint32_t inc[LG];
+#pragma unroll
+    for (int l = 0; l < LG; l++) {
+        uint32_t s = v[l];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t u = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += u;
+        }
+        inc[l] = s;
+        if (lane == 31) warp_tot[wid * LG + l] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int l = 0; l < LG; l++) {
+            uint32_t s = lane < nw ? warp_tot[lane * LG + l] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t u = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += u;
+            }
+            if (lane < nw) warp_tot[lane * LG + l] = s;  // inclusive over warps
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < LG; l++) {
+        uint32_t before = wid > 0 ? warp_tot[(wid - 1) * LG + l] : 0;
+        v[l] = before + inc[l] - v[l];
+    }
+    __syncthreads();
+}
+
+template <int LG>
+__global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__restrict__ perm1,
+                          const uint32_t *__restrict__ perm2, int32_t *__restrict__ out,
+                          uint32_t row_len, uint32_t n, uint32_t D, uint64_t dmask,
+                          uint32_t nrows, bool leaf_major) {
+    extern __shared__ uint32_t sm[];
+    uint32_t *pre = sm;                 // n x LG
+    uint32_t *wt = sm + (size_t)n * LG; // 32 x LG
+    const uint32_t grow = blockIdx.x, lane0 = blockIdx.y * LG;
+    const uint64_t *row = evals + (size_t)grow * row_len;
+    // positions [i0, i0 + per) of this thread; n is a power of two, and
+    // blockDim.x is 32 or 256, so either n is a multiple or per == 1.
+    const uint32_t per = n >= blockDim.x ? n / blockDim.x : 1;
+    const uint32_t i0 = threadIdx.x * per;
+    const uint32_t cnt = i0 < n ? min(per, n - i0) : 0;
+    // pass 1
+    uint32_t tot[LG];
+#pragma unroll
+    for (int l = 0; l < LG; l++) tot[l] = 0;
+    for (uint32_t k = 0; k < cnt; k++) {
+        const uint32_t i = i0 + k;
+        const uint64_t x = (row[perm1[i] % row_len] & dmask) >> lane0;
+#pragma unroll
+        for (int l = 0; l < LG; l++) {
+            tot[l] += (uint32_t)((x >> l) & 1u);
+            pre[(size_t)i * LG + l] = tot[l];
+        }
+    }
+    uint32_t off[LG];
+#pragma unroll
+    for (int l = 0; l < LG; l++) off[l] = tot[l];
+    block_exclusive_scan<LG>(off, wt);
+    for (uint32_t k = 0; k < cnt; k++)
+#pragma unroll
+        for (int l = 0; l < LG; l++) pre[(size_t)(i0 + k) * LG + l] += off[l];
+    __syncthreads();
+    // pass 2
+#pragma unroll
+    for (int l = 0; l < LG; l++) tot[l] = 0;
+    for (uint32_t k = 0; k < cnt; k++) {
+        const uint32_t src = perm2[i0 + k];
+#pragma unroll
+        for (int l = 0; l < LG; l++) tot[l] += pre[(size_t)src * LG + l];
+    }
+#pragma unroll
+    for (int l = 0; l < LG; l++) off[l] = tot[l];
+    block_exclusive_scan<LG>(off, wt);
+#pragma unroll
+    for (int l = 0; l < LG; l++) tot[l] = off[l];
+    for (uint32_t k = 0; k < cnt; k++) {
+        const uint32_t i = i0 + k;
+        const uint32_t src = perm2[i];
+#pragma unroll
+        for (int l = 0; l < LG; l++) {
+            tot[l] += pre[(size_t)src * LG + l];
+            const uint32_t lane = lane0 + l;
+            if (lane < D) {
+                size_t idx = leaf_major ? ((size_t)i * nrows + grow) * D + lane
+                                        : ((size_t)grow * n + i) * D + lane;
+                out[idx] = (int32_t)tot[l];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8_t *out_d,
+                        bool leaf_major, cudaStream_t s) {
+    zg_ctx *ctx = p->ctx;
+    const zg_params_info &I = p->info;
+    const uint32_t C = I.codeword_len, L = I.row_len, D = p->D;
+    const uint64_t dmask = D >= 64 ? ~0ull : ((1ull << D) - 1);
+    if (p->d.code_kind == ZG_CODE_RAA) {
+        if (p->d.eval_kind != ZG_EVAL_BINPOLY) {
+            set_error("RAA encoding is defined for binary polynomial evaluations");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        // lanes per block so that n x LG x 4 bytes fits the shared memory budget
+        int LG = 8;
+        while (LG > 1 && (size_t)C * LG * 4 > 96 * 1024) LG /= 2;
+        if ((size_t)C * LG * 4 > 200 * 1024) {
+            set_error("RAA codeword length %u exceeds the shared-memory kernel", C);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        unsigned threads = C >= 256 ? 256 : 32;
+        size_t smem = ((size_t)C * LG + 32 * LG) * 4;
+        dim3 grid(nrows, (D + LG - 1) / LG);
+        const uint32_t *p1 = p->d_perm, *p2 = p->d_perm + C;
+        int32_t *o = reinterpret_cast<int32_t *>(out_d);
+        const uint64_t *ev = static_cast<const uint64_t *>(evals_d);
+#define ZG_RAA(LGV)                                                                               \
+    do {                                                                                          \
+        ZG_CUDA(cudaFuncSetAttribute(k_raa_bin<LGV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)smem));                                                 \
+        k_raa_bin<LGV><<<grid, threads, smem, s>>>(ev, p1, p2, o, L, C, D, dmask, nrows,          \
+                                                   leaf_major);                                   \
+    } while (0)
+        ZG_KBEGIN(ctx, s, "k_raa_bin");
+        switch (LG) {
+            case 8: ZG_RAA(8); break;
+            case 4: ZG_RAA(4); break;
+            case 2: ZG_RAA(2); break;
+            default: ZG_RAA(1); break;
+        }
+#undef ZG_RAA
+        ZG_KEND(ctx, s);
+        return ZG_OK;
+    }
+
+    const uint32_t bd = I.base_dim, bl = I.base_len, depth = I.depth;
+    const uint32_t nch = 1u << (3 * depth);
+    if (p->d.eval_kind == ZG_EVAL_BINPOLY) {
+        const uint64_t *ev = static_cast<const uint64_t *>(evals_d);
+        dim3 block(32, (D + 7) / 8);
+        dim3 grid((bd + 31) / 32, nch, nrows);
+        size_t smem = (size_t)bl * 8;
+        if (smem > 48 * 1024) {
+            ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ZG_CUDA(cudaFuncSetAttribute(k_base_bin<false, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
+        if (depth == 0) {
+            ZG_KBEGIN(ctx, s, "k_base_bin");
+            if (leaf_major)
+                k_base_bin<true, true><<<grid, block, smem, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, D, dmask, nrows);
+            else
+                k_base_bin<true, false><<<grid, block, smem, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, D, dmask, nrows);
+            ZG_KEND(ctx, s);
+            return ZG_OK;
+        }
+        ZG_TRY(ctx->stage_a.ensure((size_t)nrows * C * D * 4));
+        ZG_TRY(ctx->stage_b.ensure((size_t)nrows * C * D * 8 * (depth > 1 ? 1 : 0) + 8));
+        int32_t *base = ctx->stage_a.as<int32_t>();
+        ZG_KBEGIN(ctx, s, "k_base_bin");
+        k_base_bin<false, false><<<grid, block, smem, s>>>(ev, p->d_bmT, base, L, bd, bl, depth, C, D, dmask, nrows);
+        ZG_KEND(ctx, s);
+        const size_t nthr = (size_t)nrows * (C / 8) * D;
+        const unsigned tb = 256, nb = blocks_for(nthr, tb);
+        int64_t *prev = nullptr;
+        for (uint32_t k = 0; k < depth; k++) {
+            const uint32_t sub = bd << (3 * k);
+            const int32_t *tw = p->d_tw + p->tw_dev_off[k];
+            const bool last = k + 1 == depth;
+            int64_t *dst = last ? reinterpret_cast<int64_t *>(out_d)
+                                : (k % 2 == 0 ? ctx->stage_b.as<int64_t>() : nullptr);
+            if (!last && k % 2 == 1) {
+                // a third buffer is needed only for depth >= 3
+                ZG_TRY(ctx->stage_c.ensure((size_t)nrows * C * D * 8));
+                dst = ctx->stage_c.as<int64_t>();
+            }
+            ZG_KBEGIN(ctx, s, k == 0 ? "k_stage_bin[0]" : "k_stage_bin[1+]");
+            if (k == 0) {
+                if (last && leaf_major)
+                    k_stage_bin<int32_t, true, true><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows);
+                else if (last)
+                    k_stage_bin<int32_t, true, false><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows);
+                else
+                    k_stage_bin<int32_t, false, false><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows);
+            } else {
+                if (last && leaf_major)
+                    k_stage_bin<int64_t, true, true><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows);
+                else if (last)
+                    k_stage_bin<int64_t, true, false><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows);
+                else
+                    k_stage_bin<int64_t, false, false><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows);
+            }
+            ZG_KEND(ctx, s);
+            prev = dst;
+        }
+        return ZG_OK;
+    }
+
+    // i32 evaluations
+    const int32_t *ev = static_cast<const int32_t *>(evals_d);
+    const size_t nbase = (size_t)nrows * C;
+    if (depth == 0) {
+        ZG_KBEGIN(ctx, s, "k_base_i32");
+        if (leaf_major)
+            k_base_i32<true, true><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows);
+        else
+            k_base_i32<true, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows);
+        ZG_KEND(ctx, s);
+        return ZG_OK;
+    }
+    ZG_TRY(ctx->stage_a.ensure(nbase * 8));
+    ZG_TRY(ctx->stage_b.ensure(nbase * 16));
+    ZG_TRY(ctx->stage_c.ensure(depth > 2 ? nbase * 16 : 16));
+    int64_t *base = ctx->stage_a.as<int64_t>();
+    ZG_KBEGIN(ctx, s, "k_base_i32");
+    k_base_i32<false, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, base, L, bd, bl, depth, C, nrows);
+    ZG_KEND(ctx, s);
+    const size_t nthr = (size_t)nrows * (C / 8);
+    const unsigned nb = blocks_for(nthr, 256);
+    i128 *prev = nullptr;
+    for (uint32_t k = 0; k < depth; k++) {
+        const uint32_t sub = bd << (3 * k);
+        const int32_t *tw = p->d_tw + p->tw_dev_off[k];
+        const bool last = k + 1 == depth;
+        i128 *dst = last ? reinterpret_cast<i128 *>(out_d)
+                         : (k % 2 == 0 ? ctx->stage_b.as<i128>() : ctx->stage_c.as<i128>());
+        ZG_KBEGIN(ctx, s, k == 0 ? "k_stage_i128[0]" : "k_stage_i128[1+]");
+        if (k == 0) {
+            if (last && leaf_major)
+                k_stage_i128<int64_t, true, true><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows);
+            else if (last)
+                k_stage_i128<int64_t, true, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows);
+            else
+                k_stage_i128<int64_t, false, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows);
+        } else {
+            if (last && leaf_major)
+                k_stage_i128<i128, true, true><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows);
+            else if (last)
+                k_stage_i128<i128, true, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows);
+            else
+                k_stage_i128<i128, false, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows);
+        }
+        ZG_KEND(ctx, s);
+        prev = dst;
+    }
+    return ZG_OK;
+}
+
+}  // namespace zg

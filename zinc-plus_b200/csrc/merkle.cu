@@ -1,0 +1,136 @@
+// Merkle commitment kernels (zip-plus/src/merkle.rs:74-221).
+//
+// Leaf j is BLAKE3 of the column's bytes over all rows (hash_leaves,
+// merkle.rs:148-168).  The codeword is stored leaf-major, so each leaf's
+// preimage is one contiguous range.  Interior nodes are BLAKE3 parent
+// compressions (hazmat::merge_subtrees_non_root), the top one with the ROOT
+// flag (merge_subtrees_root).
+#include "zg_internal.h"
+
+namespace zg {
+
+namespace {
+
+struct GlobalWords {
+    const uint32_t *base;  // 4-byte aligned
+    uint32_t n;            // bytes, multiple of 4
+    __device__ __forceinline__ uint32_t operator()(uint32_t block, int w) const {
+        const uint32_t off = 64u * block + 4u * (uint32_t)w;
+        return off < n ? __ldg(base + off / 4) : 0u;
+    }
+};
+
+}  // namespace
+
+// Leaves of at most one chunk (1024 bytes): one thread per leaf, root output.
+__global__ void __launch_bounds__(128) k_leaf_small(const uint8_t *__restrict__ cw, uint32_t width,
+                                                    uint32_t leaf_bytes, uint32_t *__restrict__ leaves) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= width) return;
+    GlobalWords ld{reinterpret_cast<const uint32_t *>(cw + (size_t)j * leaf_bytes), leaf_bytes};
+    uint32_t h[8];
+    b3::chunk_hash(ld, leaf_bytes, 0, true, h);
+#pragma unroll
+    for (int i = 0; i < 8; i++) leaves[(size_t)j * 8 + i] = h[i];
+}
+
+// Chunk chaining values of long leaves: one thread per (leaf, chunk).
+__global__ void __launch_bounds__(128) k_leaf_chunks(const uint8_t *__restrict__ cw, uint32_t width,
+                                                     uint32_t leaf_bytes, uint32_t nchunks,
+                                                     uint32_t *__restrict__ cvs) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)width * nchunks) return;
+    const uint32_t j = (uint32_t)(t / nchunks), c = (uint32_t)(t % nchunks);
+    const uint32_t start = c * b3::CHUNK_LEN;
+    const uint32_t len = min(b3::CHUNK_LEN, leaf_bytes - start);
+    GlobalWords ld{reinterpret_cast<const uint32_t *>(cw + (size_t)j * leaf_bytes + start), len};
+    uint32_t h[8];
+    b3::chunk_hash(ld, len, c, false, h);
+#pragma unroll
+    for (int i = 0; i < 8; i++) cvs[t * 8 + i] = h[i];
+}
+
+// Merge the chunk chaining values of each leaf in BLAKE3 tree order (the
+// incremental hasher's stack discipline), root flag on the final parent.
+__global__ void __launch_bounds__(128) k_leaf_merge(const uint32_t *__restrict__ cvs, uint32_t width,
+                                                    uint32_t nchunks, uint32_t *__restrict__ leaves) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= width) return;
+    const uint32_t *cv = cvs + (size_t)j * nchunks * 8;
+    uint32_t stack[33][8];
+    int len = 0;
+    uint32_t cur[8];
+    for (uint32_t c = 0; c + 1 < nchunks; c++) {
+        for (int i = 0; i < 8; i++) cur[i] = cv[(size_t)c * 8 + i];
+        uint64_t total = (uint64_t)c + 1;
+        while ((total & 1) == 0) {
+            b3::parent_cv(stack[--len], cur, false, cur);
+            total >>= 1;
+        }
+        for (int i = 0; i < 8; i++) stack[len][i] = cur[i];
+        len++;
+    }
+    for (int i = 0; i < 8; i++) cur[i] = cv[(size_t)(nchunks - 1) * 8 + i];
+    for (int s = len - 1; s >= 0; s--) b3::parent_cv(stack[s], cur, s == 0, cur);
+    for (int i = 0; i < 8; i++) leaves[(size_t)j * 8 + i] = cur[i];
+}
+
+// One tree level: node i of the next layer from nodes 2i, 2i+1.
+__global__ void __launch_bounds__(256) k_merkle_level(const uint32_t *__restrict__ prev,
+                                                      uint32_t *__restrict__ next, uint32_t n_out,
+                                                      bool root) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_out) return;
+    uint32_t l[8], r[8], o[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        l[k] = prev[(size_t)(2 * i) * 8 + k];
+        r[k] = prev[(size_t)(2 * i + 1) * 8 + k];
+    }
+    b3::parent_cv(l, r, root, o);
+#pragma unroll
+    for (int k = 0; k < 8; k++) next[(size_t)i * 8 + k] = o[k];
+}
+
+zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
+                           uint8_t *leaves_d, cudaStream_t s) {
+    if (leaf_bytes % 4 != 0) {
+        set_error("leaf size %u is not a multiple of 4 bytes", leaf_bytes);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    uint32_t *leaves = reinterpret_cast<uint32_t *>(leaves_d);
+    if (leaf_bytes <= b3::CHUNK_LEN) {
+        ZG_KBEGIN(ctx, s, "k_leaf_small");
+        k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves);
+        ZG_KEND(ctx, s);
+        return ZG_OK;
+    }
+    const uint32_t nchunks = (leaf_bytes + b3::CHUNK_LEN - 1) / b3::CHUNK_LEN;
+    const size_t n = (size_t)width * nchunks;
+    ZG_TRY(ctx->chunk_cv.ensure(n * 32));
+    uint32_t *cvs = ctx->chunk_cv.as<uint32_t>();
+    ZG_KBEGIN(ctx, s, "k_leaf_chunks");
+    k_leaf_chunks<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw_d, width, leaf_bytes, nchunks, cvs);
+    ZG_KEND(ctx, s);
+    ZG_KBEGIN(ctx, s, "k_leaf_merge");
+    k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, nchunks, leaves);
+    ZG_KEND(ctx, s);
+    return ZG_OK;
+}
+
+zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width,
+                               const std::vector<size_t> &layer_off, cudaStream_t s) {
+    uint32_t *tree = reinterpret_cast<uint32_t *>(tree_d);
+    uint32_t n = width;
+    for (size_t k = 1; k < layer_off.size(); k++) {
+        n /= 2;
+        const bool root = (k + 1 == layer_off.size());
+        ZG_KBEGIN(ctx, s, "k_merkle_level");
+        k_merkle_level<<<(n + 255) / 256, 256, 0, s>>>(tree + layer_off[k - 1] * 8,
+                                                       tree + layer_off[k] * 8, n, root);
+        ZG_KEND(ctx, s);
+    }
+    return ZG_OK;
+}
+
+}  // namespace zg

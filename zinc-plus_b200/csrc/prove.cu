@@ -1,0 +1,197 @@
+// Prove-phase kernels (zip-plus/src/pcs/phase_prove.rs:119-304).
+//
+//  k_eq_table      eq(x, r) over the hypercube (poly/src/utils.rs:24-101)
+//  k_project_rows  w'[j][c] = <eval, alphas> in CombR (phase_prove.rs:154-174)
+//                  and per-block partial sums of F(w') * q1 (b rows, :179-193)
+//  k_reduce_rows   b[j] = sum of the partials (field addition)
+//  k_combined_row  combined_row[c] = sum_poly sum_j s_j * w'[j][c] (:205-244)
+//  k_openings      column values and Merkle siblings of the opened columns in
+//                  proof byte order (open_merkle_trees_for_column, :285-304;
+//                  write_merkle_proof, pcs_transcript.rs:210-221)
+#include "zg_internal.h"
+#include "zg_prove.h"
+
+namespace zg {
+
+template <int L>
+__global__ void k_eq_table(const uint64_t *__restrict__ r, const uint64_t *__restrict__ omr,
+                           uint32_t n, FieldCfg f, uint64_t *__restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (1u << n)) return;
+    uint64_t acc[L];
+    for (int k = 0; k < L; k++) acc[k] = f.one[k];
+    for (uint32_t k = 0; k < n; k++) {
+        const uint64_t *sel = ((i >> k) & 1u) ? r + (size_t)k * L : omr + (size_t)k * L;
+        uint64_t t[L];
+        fmul<L>(acc, sel, f.p, f.n0, t);
+        for (int w = 0; w < L; w++) acc[w] = t[w];
+    }
+    for (int w = 0; w < L; w++) out[(size_t)i * L + w] = acc[w];
+}
+
+// One thread per (poly, row j, column c).  Binary evaluations project to
+// sum_{bit i set} alpha_i; i32 evaluations project to themselves (alphas = [1]).
+// The projection fits in 3 limbs (|w'| < 64 * 2^127); it is sign-extended (or
+// truncated) to comb_limbs.
+template <int L>
+__global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ evals, int binary,
+                                                      const i128 *__restrict__ alphas, uint32_t D,
+                                                      uint64_t dmask, const uint64_t *__restrict__ q1,
+                                                      uint32_t row_len, uint32_t num_rows,
+                                                      uint32_t comb_limbs, FieldCfg f,
+                                                      uint64_t *__restrict__ wprime,
+                                                      uint64_t *__restrict__ partial) {
+    __shared__ i128 s_alpha[64];
+    __shared__ uint64_t s_red[256 * L];
+    const uint32_t b = blockIdx.z, j = blockIdx.y;
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (binary) {
+        for (uint32_t i = threadIdx.x; i < D; i += blockDim.x) s_alpha[i] = alphas[(size_t)b * D + i];
+    }
+    __syncthreads();
+    uint64_t fe[L];
+    for (int w = 0; w < L; w++) fe[w] = 0;
+    if (c < row_len) {
+        const size_t e = ((size_t)b * num_rows + j) * row_len + c;
+        uint64_t w3[3] = {0, 0, 0};
+        if (binary) {
+            uint64_t x = static_cast<const uint64_t *>(evals)[e] & dmask;
+            while (x) {
+                const int bit = __ffsll((long long)x) - 1;
+                const i128 a = s_alpha[bit];
+                const uint64_t add[3] = {(uint64_t)(u128)a, (uint64_t)((u128)a >> 64),
+                                         a < 0 ? ~0ull : 0ull};
+                wide_add(w3, add, 3);
+                x &= x - 1;
+            }
+        } else {
+            const int64_t v = static_cast<const int32_t *>(evals)[e];
+            w3[0] = (uint64_t)v;
+            w3[1] = w3[2] = v < 0 ? ~0ull : 0ull;
+        }
+        uint64_t *wo = wprime + e * comb_limbs;
+        const uint64_t sg = (w3[2] >> 63) ? ~0ull : 0ull;
+        for (uint32_t k = 0; k < comb_limbs; k++) wo[k] = k < 3 ? w3[k] : sg;
+        uint64_t fw[L];
+        from_signed<L>(w3, 3, f, fw);
+        fmul<L>(fw, q1 + (size_t)c * L, f.p, f.n0, fe);
+    }
+    for (int w = 0; w < L; w++) s_red[threadIdx.x * L + w] = fe[w];
+    __syncthreads();
+    for (uint32_t h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) fadd<L>(&s_red[threadIdx.x * L], &s_red[(threadIdx.x + h) * L], f.p);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        uint64_t *po = partial + (((size_t)b * num_rows + j) * gridDim.x + blockIdx.x) * L;
+        for (int w = 0; w < L; w++) po[w] = s_red[w];
+    }
+}
+
+template <int L>
+__global__ void k_reduce_rows(const uint64_t *__restrict__ partial, uint32_t batch,
+                              uint32_t num_rows, uint32_t nparts, FieldCfg f,
+                              uint64_t *__restrict__ bvec) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= num_rows) return;
+    uint64_t acc[L];
+    for (int w = 0; w < L; w++) acc[w] = 0;
+    for (uint32_t b = 0; b < batch; b++)
+        for (uint32_t q = 0; q < nparts; q++)
+            fadd<L>(acc, partial + (((size_t)b * num_rows + j) * nparts + q) * L, f.p);
+    for (int w = 0; w < L; w++) bvec[(size_t)j * L + w] = acc[w];
+}
+
+__global__ void __launch_bounds__(256) k_combined_row(const uint64_t *__restrict__ wprime,
+                                                      const i128 *__restrict__ coeffs,
+                                                      uint32_t batch, uint32_t num_rows,
+                                                      uint32_t row_len, uint32_t comb_limbs,
+                                                      uint64_t *__restrict__ out) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= row_len) return;
+    uint64_t acc[MAX_COMB_LIMBS];
+    for (uint32_t k = 0; k < comb_limbs; k++) acc[k] = 0;
+    for (uint32_t b = 0; b < batch; b++)
+        for (uint32_t j = 0; j < num_rows; j++)
+            wide_mul_i128_add(acc, wprime + (((size_t)b * num_rows + j) * row_len + c) * comb_limbs,
+                              coeffs[j], (int)comb_limbs);
+    for (uint32_t k = 0; k < comb_limbs; k++) out[(size_t)c * comb_limbs + k] = acc[k];
+}
+
+// One block per opening: column bytes, u64 leaf_index, u64 leaf_count,
+// u64 path length, then the sibling path bottom-up.
+__global__ void k_openings(const uint8_t *__restrict__ cw, uint32_t leaf_bytes,
+                           const uint8_t *__restrict__ tree, const uint64_t *__restrict__ layer_off,
+                           uint32_t depth, uint32_t width, const uint32_t *__restrict__ idxs,
+                           uint8_t *__restrict__ out) {
+    const uint32_t o = blockIdx.x, idx = idxs[o];
+    const size_t open_bytes = (size_t)leaf_bytes + 24 + 32 * (size_t)depth;
+    uint8_t *dst = out + (size_t)o * open_bytes;
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(cw + (size_t)idx * leaf_bytes);
+    uint32_t *d32 = reinterpret_cast<uint32_t *>(dst);
+    for (uint32_t w = threadIdx.x; w < leaf_bytes / 4; w += blockDim.x) d32[w] = src[w];
+    if (threadIdx.x < 6) {
+        const uint64_t v[3] = {idx, width, depth};
+        const uint32_t word = threadIdx.x & 1 ? (uint32_t)(v[threadIdx.x / 2] >> 32)
+                                              : (uint32_t)v[threadIdx.x / 2];
+        reinterpret_cast<uint32_t *>(dst + leaf_bytes)[threadIdx.x] = word;
+    }
+    const uint32_t nw = 8 * depth;
+    for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
+        const uint32_t k = w / 8, part = w % 8;
+        const uint64_t node = layer_off[k] + ((idx >> k) ^ 1u);
+        reinterpret_cast<uint32_t *>(dst + leaf_bytes + 24)[w] =
+            reinterpret_cast<const uint32_t *>(tree)[node * 8 + part];
+    }
+}
+
+// ---------------------------------------------------------------------------
+template <int L>
+static zg_status eq_table_t(zg_ctx *ctx, const uint64_t *r_d, const uint64_t *omr_d, uint32_t n,
+                            const FieldCfg &f, uint64_t *out_d, cudaStream_t s) {
+    const uint32_t m = 1u << n;
+    ZG_KBEGIN(ctx, s, "k_eq_table");
+    k_eq_table<L><<<(m + 255) / 256, 256, 0, s>>>(r_d, omr_d, n, f, out_d);
+    ZG_KEND(ctx, s);
+    return ZG_OK;
+}
+
+zg_status launch_eq_table(zg_ctx *ctx, const uint64_t *r_d, const uint64_t *omr_d, uint32_t n,
+                          const FieldCfg &f, uint64_t *out_d, cudaStream_t s) {
+    return f.L == 3 ? eq_table_t<3>(ctx, r_d, omr_d, n, f, out_d, s)
+                    : eq_table_t<4>(ctx, r_d, omr_d, n, f, out_d, s);
+}
+
+template <int L>
+static zg_status project_t(zg_ctx *ctx, const ProjectArgs &a, cudaStream_t s) {
+    dim3 grid((a.row_len + 255) / 256, a.num_rows, a.batch);
+    ZG_KBEGIN(ctx, s, "k_project_rows");
+    k_project_rows<L><<<grid, 256, 0, s>>>(a.evals, a.binary, a.alphas, a.D, a.dmask, a.q1,
+                                           a.row_len, a.num_rows, a.comb_limbs, *a.f, a.wprime,
+                                           a.partial);
+    ZG_KEND(ctx, s);
+    ZG_KBEGIN(ctx, s, "k_reduce_rows");
+    k_reduce_rows<L><<<(a.num_rows + 127) / 128, 128, 0, s>>>(a.partial, a.batch, a.num_rows,
+                                                               grid.x, *a.f, a.bvec);
+    ZG_KEND(ctx, s);
+    return ZG_OK;
+}
+
+zg_status launch_project_rows(zg_ctx *ctx, const ProjectArgs &a, cudaStream_t s) {
+    return a.f->L == 3 ? project_t<3>(ctx, a, s) : project_t<4>(ctx, a, s);
+}
+
+zg_status launch_combined_and_openings(zg_ctx *ctx, const CombineArgs &a, cudaStream_t s) {
+    ZG_KBEGIN(ctx, s, "k_combined_row");
+    k_combined_row<<<(a.row_len + 255) / 256, 256, 0, s>>>(a.wprime, a.coeffs, a.batch,
+                                                           a.num_rows, a.row_len, a.comb_limbs,
+                                                           a.comb_out);
+    ZG_KEND(ctx, s);
+    ZG_KBEGIN(ctx, s, "k_openings");
+    k_openings<<<a.n_open, 128, 0, s>>>(a.cw, a.leaf_bytes, a.tree, a.layer_off, a.depth, a.width,
+                                        a.idxs, a.open_out);
+    ZG_KEND(ctx, s);
+    return ZG_OK;
+}
+
+}  // namespace zg

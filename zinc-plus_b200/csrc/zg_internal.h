@@ -1,0 +1,185 @@
+// Internal declarations shared by the zipgpu translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/zipgpu.h"
+#include "zg_blake3.cuh"
+#include "zg_field.cuh"
+
+namespace zg {
+
+// ----------------------------------------------------------------- errors
+void set_error(const char *fmt, ...);
+
+#define ZG_TRY(expr)                                                                              \
+    do {                                                                                          \
+        zg_status _s = (expr);                                                                    \
+        if (_s != ZG_OK) return _s;                                                               \
+    } while (0)
+
+#define ZG_CUDA(call)                                                                             \
+    do {                                                                                          \
+        cudaError_t _e = (call);                                                                  \
+        if (_e != cudaSuccess) {                                                                  \
+            ::zg::set_error("CUDA error %s (%s) at %s:%d", cudaGetErrorName(_e),                  \
+                            cudaGetErrorString(_e), __FILE__, __LINE__);                          \
+            return _e == cudaErrorMemoryAllocation ? ZG_ERR_OOM : ZG_ERR_CUDA;                   \
+        }                                                                                         \
+    } while (0)
+
+#define ZG_CHECK_LAUNCH(ctx)                                                                      \
+    do {                                                                                          \
+        (ctx)->launches++;                                                                        \
+        ZG_CUDA(cudaGetLastError());                                                              \
+    } while (0)
+
+// Optional per-kernel CUDA-event timing (zg_ctx_set_kernel_timing): events are
+// recorded on the launching stream around each launch.
+#define ZG_KBEGIN(ctx, s, name) ::zg::ktimer_begin((ctx), (s), (name))
+#define ZG_KEND(ctx, s)                                                                           \
+    do {                                                                                          \
+        ::zg::ktimer_end((ctx), (s));                                                             \
+        ZG_CHECK_LAUNCH(ctx);                                                                     \
+    } while (0)
+
+// ------------------------------------------------------- device buffers
+// A growable device allocation owned by a context and reused across calls.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    zg_status ensure(size_t bytes);
+    void release();
+    template <class T>
+    T *as() const {
+        return static_cast<T *>(ptr);
+    }
+};
+
+// A growable pinned host allocation.
+struct HostBuf {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    zg_status ensure(size_t bytes);
+    void release();
+    template <class T>
+    T *as() const {
+        return static_cast<T *>(ptr);
+    }
+};
+
+struct zg_ctx_timer;
+void ktimer_begin(zg_ctx *ctx, cudaStream_t s, const char *name);
+void ktimer_end(zg_ctx *ctx, cudaStream_t s);
+void ktimer_collect(zg_ctx *ctx);
+
+// One pending timed launch.
+struct KernelEvent {
+    const char *name;
+    cudaEvent_t start, stop;
+};
+
+}  // namespace zg
+
+struct zg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t launches = 0;
+    int num_sms = 0;
+    std::mutex mu;  // one call at a time per context
+    // scratch arenas
+    zg::DevBuf evals;     // staged evaluations
+    zg::DevBuf stage_a;   // pNTT intermediates
+    zg::DevBuf stage_b;
+    zg::DevBuf stage_c;   // third pNTT buffer (depth >= 3)
+    zg::DevBuf chunk_cv;  // per-chunk BLAKE3 chaining values for long leaves
+    zg::DevBuf wprime;    // alpha-projected rows (CombR)
+    zg::DevBuf prove_in;  // small per-prove inputs (alphas, points, coeffs, indices)
+    zg::DevBuf prove_out; // b partials, combined row + openings
+    zg::HostBuf pin_in, pin_out;
+    // kernel timing
+    bool timing = false;
+    std::vector<zg::KernelEvent> pending;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<std::pair<std::string, std::pair<double, uint64_t>>> totals;  // name -> (ms, n)
+};
+
+struct zg_params {
+    zg_ctx *ctx = nullptr;
+    zg_params_desc d{};
+    zg_params_info info{};
+    uint32_t D = 1;  // lanes per evaluation (coefficients of BinaryPoly)
+    // IPRS tables (host: exactly the reference's layout; device: int32 copies)
+    std::vector<int64_t> bm;  // base_dim x base_len
+    std::vector<int64_t> tw;  // stage k: (base_dim*8^k) x 7 x 8, stages back to back
+    int32_t *d_bmT = nullptr; // base_len x base_dim (transposed)
+    int32_t *d_tw = nullptr;  // stage k: [56][sub_k], stages back to back
+    std::vector<size_t> tw_off;      // offset of each stage in tw (host, [i][j-1][t])
+    std::vector<size_t> tw_dev_off;  // offset of each stage in d_tw (device, [56][sub])
+    // RAA permutations
+    std::vector<uint32_t> perm1, perm2;
+    uint32_t *d_perm = nullptr;  // perm1 then perm2
+};
+
+struct zg_hint {
+    zg_params *params = nullptr;
+    uint32_t batch = 0;
+    uint32_t nrows = 0;        // batch * num_rows
+    uint8_t *d_cw = nullptr;   // leaf-major: codeword_len x nrows x cw_bytes
+    uint8_t *d_tree = nullptr; // Merkle layers, leaves first, root last, 32 B nodes
+    uint32_t depth = 0;        // log2(codeword_len)
+    std::vector<size_t> layer_off;  // node offset of each layer
+    uint64_t *d_layer_off = nullptr;
+    uint8_t root[32];
+};
+
+struct zg_transcript {
+    zg::b3::Hasher h;
+    std::vector<uint8_t> stream;
+    bool has_field = false;
+    zg::FieldCfg f{};
+};
+
+namespace zg {
+
+// ------------------------------------------------------- host utilities
+void tr_absorb(zg_transcript *t, const void *buf, size_t n);
+void tr_absorb_slice(zg_transcript *t, const void *buf, size_t n);
+void tr_challenge(zg_transcript *t, uint8_t *out, size_t n);
+i128 tr_challenge_i128(zg_transcript *t);
+uint32_t tr_challenge_u32(zg_transcript *t);
+void tr_absorb_field(zg_transcript *t, const uint64_t *inner);
+// get_prime::<Uint<L>, MillerRabin> (transcript/src/lib.rs:58-72).
+void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out);
+bool is_probable_prime_base2(const uint64_t *n, int L);
+
+// IPRS parameters (params.rs:59-196); returns false if the reference rejects.
+bool iprs_build_tables(uint32_t row_len, uint32_t depth, uint32_t rep, zg_params *p);
+uint32_t iprs_optimal_depth(uint32_t row_len);
+// rand 0.9 StdRng::seed_from_u64(seed) shuffle of 0..n (zip-plus/src/utils.rs:7-10).
+void stdrng_shuffle_identity(uint64_t seed, uint32_t n, uint32_t *perm);
+
+// ---------------------------------------------------------- pipelines
+zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **out);
+zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
+                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out);
+zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
+                      const uint8_t *eval, const uint8_t *proof, size_t proof_len);
+
+// ------------------------------------------------------------- kernels
+// (defined in the .cu files; all launched on the given stream)
+zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8_t *out_d,
+                        bool leaf_major, cudaStream_t s);
+zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
+                           uint8_t *leaves_d, cudaStream_t s);
+zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width,
+                               const std::vector<size_t> &layer_off, cudaStream_t s);
+
+}  // namespace zg

@@ -1,0 +1,484 @@
+"""Python front end of libzipgpu, the B200 (sm_100a) backend of the Zip+
+polynomial commitment scheme of NethermindEth/zinc-plus.
+
+The classes mirror the reference's Rust API for the commit/prove path, with
+the same names and argument meaning:
+
+  ``IprsCode.new`` / ``IprsCode.new_with_optimal_depth``  (zip-plus/src/code/iprs.rs:30-51)
+  ``RaaCode.new``                                          (zip-plus/src/code/raa.rs:38-90)
+  ``ZipPlus.setup`` / ``commit`` / ``commit_single`` / ``encode_rows``
+                                                           (pcs/structs.rs:74, pcs/phase_commit.rs)
+  ``ZipPlus.prove`` / ``ZipPlus.verify``                   (pcs/phase_prove.rs:85, pcs/phase_verify.rs:100)
+  ``PcsProverTranscript.new_from_commitment(s)``           (zip-plus/src/pcs_transcript.rs:58-73)
+  ``MerkleTree.new(rows).root()``                          (zip-plus/src/merkle.rs:74-103)
+
+Every call goes through the C ABI declared in include/zipgpu.h.  There is no
+CPU fallback: a missing or unloadable library raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzipgpu.so")
+
+ZG_OK = 0
+STATUS = {
+    0: "ZG_OK", 1: "ZG_ERR_INVALID_PARAM", 2: "ZG_ERR_INVALID_OPEN", 3: "ZG_ERR_SERIALIZATION",
+    4: "ZG_ERR_OVERFLOW", 5: "ZG_ERR_CUDA", 6: "ZG_ERR_OOM", 7: "ZG_ERR_TIMEOUT",
+    8: "ZG_ERR_NO_DEVICE", 9: "ZG_ERR_BUFFER_TOO_SMALL",
+}
+EVAL_I32, EVAL_BINPOLY = 0, 1
+CODE_IPRS, CODE_RAA = 0, 1
+
+# Every symbol include/zipgpu.h declares.
+EXPORTS = (
+    "zg_last_error", "zg_version", "zg_ctx_create", "zg_ctx_destroy", "zg_ctx_kernel_launches",
+    "zg_ctx_stream", "zg_ctx_set_kernel_timing", "zg_ctx_kernel_timing_report", "zg_params_create", "zg_params_destroy", "zg_params_get_info",
+    "zg_params_iprs_tables", "zg_params_raa_perms", "zg_encode_rows", "zg_encode_rows_d",
+    "zg_encode_wide", "zg_merkle_root", "zg_commit", "zg_commit_d", "zg_hint_free",
+    "zg_hint_batch", "zg_hint_codeword", "zg_transcript_new", "zg_transcript_free",
+    "zg_transcript_absorb", "zg_transcript_absorb_slice", "zg_transcript_challenge",
+    "zg_transcript_sample_field", "zg_transcript_proof", "zg_prove", "zg_prove_d",
+    "zg_commit_prove", "zg_commit_prove_d", "zg_proof_size", "zg_verify",
+)
+
+
+class ZipError(RuntimeError):
+    """Error status from libzipgpu (mirrors zip_plus::ZipError)."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class ParamsDesc(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "eval_kind", "degree_plus_one", "code_kind", "rep", "num_vars", "row_len",
+        "iprs_depth", "comb_limbs", "field_limbs", "num_openings")]
+
+
+class ParamsInfo(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "num_rows", "row_len", "codeword_len", "depth", "base_len", "base_dim",
+        "eval_bytes", "cw_bytes", "comb_bytes", "field_bytes")]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libzipgpu.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libzipgpu.so not built at {LIB_PATH}; run `make -C zinc-plus_b200`")
+    L = C.CDLL(LIB_PATH)
+    vp, sz, u32, st = C.c_void_p, C.c_size_t, C.c_uint32, C.c_int
+    sig = {
+        "zg_last_error": ([], C.c_char_p), "zg_version": ([], C.c_char_p),
+        "zg_ctx_create": ([C.c_int, C.POINTER(vp)], st), "zg_ctx_destroy": ([vp], st),
+        "zg_ctx_kernel_launches": ([vp], C.c_uint64), "zg_ctx_stream": ([vp], vp),
+        "zg_ctx_set_kernel_timing": ([vp, C.c_int], st),
+        "zg_ctx_kernel_timing_report": ([vp, C.c_char_p, sz, C.POINTER(sz)], st),
+        "zg_params_create": ([vp, C.POINTER(ParamsDesc), C.POINTER(vp)], st),
+        "zg_params_destroy": ([vp], st),
+        "zg_params_get_info": ([vp, C.POINTER(ParamsInfo)], st),
+        "zg_params_iprs_tables": ([vp, vp, vp], st), "zg_params_raa_perms": ([vp, vp, vp], st),
+        "zg_encode_rows": ([vp, vp, vp], st), "zg_encode_rows_d": ([vp, vp, vp, vp], st),
+        "zg_encode_wide": ([vp, vp, u32, vp], st),
+        "zg_merkle_root": ([vp, vp, u32, u32, u32, vp], st),
+        "zg_commit": ([vp, vp, u32, C.POINTER(vp), vp], st),
+        "zg_commit_d": ([vp, vp, u32, C.POINTER(vp), vp], st),
+        "zg_hint_free": ([vp], st), "zg_hint_batch": ([vp], u32),
+        "zg_hint_codeword": ([vp, u32, vp], st),
+        "zg_transcript_new": ([vp, u32, C.POINTER(vp)], st), "zg_transcript_free": ([vp], st),
+        "zg_transcript_absorb": ([vp, vp, sz], st), "zg_transcript_absorb_slice": ([vp, vp, sz], st),
+        "zg_transcript_challenge": ([vp, vp, sz], st),
+        "zg_transcript_sample_field": ([vp, u32, vp], st),
+        "zg_transcript_proof": ([vp, C.POINTER(vp), C.POINTER(sz)], st),
+        "zg_prove": ([vp, vp, vp, u32, vp, vp, vp], st),
+        "zg_prove_d": ([vp, vp, vp, u32, vp, vp, vp], st),
+        "zg_commit_prove": ([vp, vp, u32, vp, vp, vp, vp, C.POINTER(sz)], st),
+        "zg_commit_prove_d": ([vp, vp, u32, vp, vp, vp, vp, C.POINTER(sz)], st),
+        "zg_proof_size": ([vp, u32], sz),
+        "zg_verify": ([vp, vp, u32, vp, vp, vp, sz], st),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != ZG_OK:
+        raise ZipError(status, lib().zg_last_error().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def i128_bytes(values: Sequence[int]) -> bytes:
+    return b"".join((int(v) & ((1 << 128) - 1)).to_bytes(16, "little") for v in values)
+
+
+# --------------------------------------------------------------------- context
+class Context:
+    """A CUDA device context (stream and scratch arenas)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().zg_ctx_create(device, C.byref(h)))
+        self.handle = h
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().zg_ctx_kernel_launches(self.handle))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().zg_ctx_stream(self.handle) or 0)
+
+    def set_kernel_timing(self, enable: bool) -> None:
+        check(lib().zg_ctx_set_kernel_timing(self.handle, int(enable)))
+
+    def kernel_times(self) -> dict:
+        """{kernel: (launches, total_ms)} since the last report (CUDA events)."""
+        n = C.c_size_t()
+        buf = C.create_string_buffer(1 << 16)
+        check(lib().zg_ctx_kernel_timing_report(self.handle, buf, 1 << 16, C.byref(n)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, cnt, ms = line.rsplit(",", 2)
+            out[name] = (int(cnt), float(ms))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().zg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Context | None = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+# ---------------------------------------------------------------------- codes
+@dataclass(frozen=True)
+class IprsCode:
+    """IPRS code over F65537 (IprsCode<Zt, PnttConfigF65537, REP, CHECK>)."""
+
+    row_len: int
+    depth: int = 0  # 0: new_with_optimal_depth
+    rep: int = 4
+    kind: int = CODE_IPRS
+
+    @staticmethod
+    def new(row_len: int, depth: int, rep: int = 4) -> "IprsCode":
+        return IprsCode(row_len, depth, rep)
+
+    @staticmethod
+    def new_with_optimal_depth(row_len: int, rep: int = 4) -> "IprsCode":
+        return IprsCode(row_len, 0, rep)
+
+
+@dataclass(frozen=True)
+class RaaCode:
+    """Repeat-accumulate-accumulate code (RaaCode<Zt, Config, REP>)."""
+
+    row_len: int
+    rep: int = 4
+    depth: int = 0
+    kind: int = CODE_RAA
+
+    @staticmethod
+    def new(row_len: int, rep: int = 4) -> "RaaCode":
+        return RaaCode(row_len, rep)
+
+
+@dataclass(frozen=True)
+class ZipTypes:
+    """The ZipTypes instantiation (pcs/structs.rs:15-60)."""
+
+    eval_kind: int = EVAL_BINPOLY
+    degree_plus_one: int = 32
+    comb_limbs: int = 5
+    field_limbs: int = 4
+    num_openings: int = 147
+
+
+# The reference benches' instantiations.
+ZIP_I32 = ZipTypes(EVAL_I32, 1, 3, 4, 147)  # zip_benches.rs:25-40
+
+
+def zip_plus_binary(degree_plus_one: int) -> ZipTypes:  # zip_plus_benches.rs:37-65
+    return ZipTypes(EVAL_BINPOLY, degree_plus_one, 5, 4, 147)
+
+
+class ZipPlusParams:
+    """ZipPlusParams (setup output) backed by device-resident code tables."""
+
+    def __init__(self, zt: ZipTypes, code, num_vars: int, ctx: Context | None):
+        self.zt, self.code, self.num_vars, self.ctx = zt, code, num_vars, ctx
+        d = ParamsDesc(zt.eval_kind, zt.degree_plus_one, code.kind, code.rep, num_vars,
+                       code.row_len, code.depth, zt.comb_limbs, zt.field_limbs, zt.num_openings)
+        self.desc = d
+        h = C.c_void_p()
+        check(lib().zg_params_create(ctx.handle if ctx else None, C.byref(d), C.byref(h)))
+        self.handle = h
+        info = ParamsInfo()
+        check(lib().zg_params_get_info(h, C.byref(info)))
+        self.info = info
+        self.num_rows = info.num_rows
+        self.row_len = info.row_len
+        self.codeword_len = info.codeword_len
+
+    @property
+    def eval_dtype(self):
+        return np.int32 if self.zt.eval_kind == EVAL_I32 else np.uint64
+
+    def proof_size(self, batch: int = 1) -> int:
+        return int(lib().zg_proof_size(self.handle, batch))
+
+    def iprs_tables(self):
+        i = self.info
+        bm = np.zeros((i.base_dim, i.base_len), np.int64)
+        ntw = sum(i.base_dim * 8 ** k * 56 for k in range(i.depth))
+        tw = np.zeros(max(ntw, 1), np.int64)
+        check(lib().zg_params_iprs_tables(self.handle, _ptr(bm), _ptr(tw)))
+        return bm, tw[:ntw]
+
+    def raa_perms(self):
+        p1 = np.zeros(self.codeword_len, np.uint32)
+        p2 = np.zeros(self.codeword_len, np.uint32)
+        check(lib().zg_params_raa_perms(self.handle, _ptr(p1), _ptr(p2)))
+        return p1, p2
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().zg_params_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ZipPlusCommitment:
+    root: bytes
+    batch_size: int
+
+    def to_bytes(self) -> bytes:  # pcs/structs.rs:140-157
+        return self.root + int(self.batch_size).to_bytes(8, "little")
+
+
+class ZipPlusHint:
+    """Device-resident codewords and Merkle layers (ZipPlusHint)."""
+
+    def __init__(self, handle, params: ZipPlusParams):
+        self.handle, self.params = handle, params
+
+    @property
+    def batch(self) -> int:
+        return int(lib().zg_hint_batch(self.handle))
+
+    def codeword(self, poly: int = 0) -> np.ndarray:
+        p = self.params
+        out = np.zeros(p.num_rows * p.codeword_len * p.info.cw_bytes, np.uint8)
+        check(lib().zg_hint_codeword(self.handle, poly, _ptr(out)))
+        return out.reshape(p.num_rows, p.codeword_len, p.info.cw_bytes)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().zg_hint_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PcsProverTranscript:
+    """PcsProverTranscript: Blake3 Fiat-Shamir sponge plus the proof stream."""
+
+    def __init__(self, roots: Sequence[bytes] = ()):
+        h = C.c_void_p()
+        buf = b"".join(roots)
+        check(lib().zg_transcript_new(C.c_char_p(buf) if buf else None, len(roots), C.byref(h)))
+        self.handle = h
+        self.modulus: int | None = None
+
+    @staticmethod
+    def new_from_commitment(comm: ZipPlusCommitment) -> "PcsProverTranscript":
+        return PcsProverTranscript([comm.root])
+
+    @staticmethod
+    def new_from_commitments(comms: Sequence[ZipPlusCommitment]) -> "PcsProverTranscript":
+        return PcsProverTranscript([c.root for c in comms])
+
+    def absorb(self, b: bytes):
+        check(lib().zg_transcript_absorb(self.handle, C.c_char_p(b), len(b)))
+
+    def absorb_slice(self, b: bytes):
+        check(lib().zg_transcript_absorb_slice(self.handle, C.c_char_p(b), len(b)))
+
+    def get_challenge(self, nbytes: int) -> bytes:
+        out = C.create_string_buffer(nbytes)
+        check(lib().zg_transcript_challenge(self.handle, out, nbytes))
+        return out.raw
+
+    def get_random_field_cfg(self, limbs: int = 4) -> int:
+        out = C.create_string_buffer(8 * limbs)
+        check(lib().zg_transcript_sample_field(self.handle, limbs, out))
+        self.modulus = int.from_bytes(out.raw, "little")
+        return self.modulus
+
+    @property
+    def stream(self) -> bytes:
+        data, n = C.c_void_p(), C.c_size_t()
+        check(lib().zg_transcript_proof(self.handle, C.byref(data), C.byref(n)))
+        return C.string_at(data, n.value) if n.value else b""
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().zg_transcript_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _poly_ptrs(params: ZipPlusParams, polys):
+    arrs = [np.ascontiguousarray(p, dtype=params.eval_dtype) for p in polys]
+    n = params.num_rows * params.row_len
+    for a in arrs:
+        if a.size != n:
+            raise ValueError(f"Polynomial has an incorrect number of evaluations ({a.size}) for "
+                             f"the expected matrix size ({n})")
+    ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    return arrs, ptrs
+
+
+class ZipPlus:
+    """ZipPlus<Zt, Lc> associated functions."""
+
+    @staticmethod
+    def setup(poly_size: int, code, zt: ZipTypes = ZipTypes(), ctx: Context | None = None,
+              device: bool = True) -> ZipPlusParams:
+        if poly_size <= 0 or poly_size & (poly_size - 1):
+            raise ValueError("poly_size must be a power of two")
+        num_vars = poly_size.bit_length() - 1
+        if device and ctx is None:
+            ctx = default_context()
+        return ZipPlusParams(zt, code, num_vars, ctx if device else None)
+
+    @staticmethod
+    def encode_rows(pp: ZipPlusParams, evals) -> np.ndarray:
+        ev = np.ascontiguousarray(evals, dtype=pp.eval_dtype)
+        out = np.zeros(pp.num_rows * pp.codeword_len * pp.info.cw_bytes, np.uint8)
+        check(lib().zg_encode_rows(pp.handle, _ptr(ev), _ptr(out)))
+        return out.reshape(pp.num_rows, pp.codeword_len, pp.info.cw_bytes)
+
+    @staticmethod
+    def encode_wide(pp: ZipPlusParams, row: np.ndarray, limbs: int) -> np.ndarray:
+        row = np.ascontiguousarray(row, dtype=np.uint64)
+        out = np.zeros((pp.codeword_len, limbs), np.uint64)
+        check(lib().zg_encode_wide(pp.handle, _ptr(row), limbs, _ptr(out)))
+        return out
+
+    @staticmethod
+    def commit(pp: ZipPlusParams, polys) -> tuple[ZipPlusHint, ZipPlusCommitment]:
+        if len(polys) == 0:
+            raise ValueError("Batch must contain at least one polynomial")
+        _keep, ptrs = _poly_ptrs(pp, polys)
+        h = C.c_void_p()
+        root = C.create_string_buffer(32)
+        check(lib().zg_commit(pp.handle, ptrs, len(polys), C.byref(h), root))
+        return ZipPlusHint(h, pp), ZipPlusCommitment(root.raw, len(polys))
+
+    @staticmethod
+    def commit_single(pp: ZipPlusParams, poly) -> tuple[ZipPlusHint, ZipPlusCommitment]:
+        return ZipPlus.commit(pp, [poly])
+
+    @staticmethod
+    def prove(transcript: PcsProverTranscript, pp: ZipPlusParams, polys, point: Sequence[int],
+              hint: ZipPlusHint) -> bytes:
+        """Returns the evaluation as its Montgomery inner bytes; appends the proof."""
+        _keep, ptrs = _poly_ptrs(pp, polys)
+        if len(point) != pp.num_vars:
+            raise ZipError(1, f"Invalid point (expect point to have {pp.num_vars} variates but "
+                              f"got {len(point)})")
+        pt = i128_bytes(point)
+        ev = C.create_string_buffer(8 * pp.zt.field_limbs)
+        check(lib().zg_prove(pp.handle, transcript.handle, ptrs, len(polys), C.c_char_p(pt),
+                             hint.handle, ev))
+        return ev.raw
+
+    @staticmethod
+    def commit_prove(pp: ZipPlusParams, polys, point: Sequence[int]):
+        """commit + new_from_commitment + get_random_field_cfg + prove in one call."""
+        _keep, ptrs = _poly_ptrs(pp, polys)
+        pt = i128_bytes(point)
+        cap = C.c_size_t(pp.proof_size(len(polys)))
+        proof = C.create_string_buffer(cap.value)
+        root = C.create_string_buffer(32)
+        ev = C.create_string_buffer(8 * pp.zt.field_limbs)
+        check(lib().zg_commit_prove(pp.handle, ptrs, len(polys), C.c_char_p(pt), root, ev, proof,
+                                    C.byref(cap)))
+        return root.raw, ev.raw, proof.raw[: cap.value]
+
+    @staticmethod
+    def verify(pp: ZipPlusParams, comm: ZipPlusCommitment, point: Sequence[int], eval_inner: bytes,
+               proof: bytes) -> None:
+        """Raises ZipError unless the proof verifies."""
+        pt = i128_bytes(point)
+        check(lib().zg_verify(pp.handle, C.c_char_p(comm.root), comm.batch_size, C.c_char_p(pt),
+                              C.c_char_p(eval_inner), C.c_char_p(proof), len(proof)))
+
+
+class MerkleTree:
+    """MerkleTree::new over the columns of a row-major matrix (root only)."""
+
+    def __init__(self, root: bytes):
+        self._root = root
+
+    @staticmethod
+    def new(rows: np.ndarray, elem_bytes: int, ctx: Context | None = None) -> "MerkleTree":
+        rows = np.ascontiguousarray(rows, dtype=np.uint8)
+        n_rows, width = rows.shape[0], rows.shape[1] // elem_bytes
+        root = C.create_string_buffer(32)
+        check(lib().zg_merkle_root((ctx or default_context()).handle, _ptr(rows), n_rows, width,
+                                   elem_bytes, root))
+        return MerkleTree(root.raw)
+
+    def root(self) -> bytes:
+        return self._root
