@@ -142,6 +142,27 @@ zg_status zg_encode_wide(zg_params *p, const uint64_t *row, uint32_t limbs, uint
 zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_t width,
                          uint32_t elem_bytes, uint8_t root[32]);
 
+/* ---- Allocation-free Merkle root ---------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory on their request path (a serving loop that reserves its device-memory
+ * budget up front, or a host whose device buffers all come from its own pool):
+ * cudaMalloc/cudaFree synchronize the device and can fail under memory
+ * pressure, and this entry point calls neither, nor any other allocating
+ * routine.  It computes the same root as zg_merkle_root over `width` leaves
+ * whose preimages are consecutive `leaf_bytes`-byte ranges at leaves_d (device
+ * memory, leaf-major), and writes the 32-byte root to root_d (device memory),
+ * asynchronously on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * Its scratch is a fixed 4 MiB device array inside the library, held by every
+ * GPU that loads it until the process exits: (2*width - 1) * 32 bytes of nodes
+ * plus width * ceil(leaf_bytes / 1024) * 32 bytes of chunk chaining values for
+ * leaves longer than 1024 bytes must fit (e.g. 65536 leaves of at most 1024
+ * bytes); larger inputs return ZG_ERR_INVALID_PARAM.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress, with that
+ * device current); make that first call before any stream capture.  All calls
+ * on a device share the array: calls that overlap on the GPU race. */
+zg_status zg_merkle_root_noalloc_d(const void *leaves_d, uint32_t width, uint32_t leaf_bytes,
+                                   uint8_t *root_d, void *stream);
+
 /* ---- ZipPlus::commit (phase_commit.rs:61-101) ------------------------------
  * polys[i] points at poly i's 2^num_vars evaluations.  The hint (codewords and
  * Merkle layers) stays on the device.  commit_single == batch 1. */

@@ -134,3 +134,104 @@ zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width,
 }
 
 }  // namespace zg
+
+// ---------------------------------------------------------------------------
+// Allocation-free Merkle root (no counterpart in the reference).
+//
+// Some callers of this library cannot allocate device memory on their request
+// path: a serving loop that reserves its whole device-memory budget up front,
+// or a host whose device buffers all come from its own pool.  For them
+// cudaMalloc/cudaFree are off limits: they synchronize the device, stall other
+// streams and can fail under memory pressure in the middle of a request.
+// zg_merkle_root_noalloc_d allocates nothing.  Its scratch (the node layers,
+// plus the chunk chaining values of leaves longer than one BLAKE3 chunk) is the
+// file-scope 4 MiB array below, which every GPU that loads this library holds
+// until the process exits.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kNoAllocMaxDevices] = {};  // device address of the array, per device
+
+}  // namespace
+
+extern "C" zg_status zg_merkle_root_noalloc_d(const void *leaves_d, uint32_t width,
+                                              uint32_t leaf_bytes, uint8_t *root_d,
+                                              void *stream) {
+    using namespace zg;
+    if (!leaves_d || !root_d) {
+        set_error("zg_merkle_root_noalloc_d: null leaf or root pointer");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (width == 0 || (width & (width - 1)) != 0) {
+        set_error("zg_merkle_root_noalloc_d: width %u is not a power of two", width);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (leaf_bytes == 0 || leaf_bytes % 4 != 0) {
+        set_error("zg_merkle_root_noalloc_d: leaf size %u is not a positive multiple of 4",
+                  leaf_bytes);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    const uint64_t nchunks =
+        leaf_bytes <= b3::CHUNK_LEN ? 0 : (leaf_bytes + b3::CHUNK_LEN - 1) / b3::CHUNK_LEN;
+    const uint64_t nodes = 2 * (uint64_t)width - 1;
+    const uint64_t need = (nodes + (uint64_t)width * nchunks) * 32;
+    if (need > kNoAllocScratchBytes) {
+        set_error("zg_merkle_root_noalloc_d: %u leaves of %u bytes need %llu bytes of scratch; "
+                  "the limit is %zu bytes (for example 65536 leaves of at most 1024 bytes)",
+                  width, leaf_bytes, (unsigned long long)need, kNoAllocScratchBytes);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    int dev = 0;
+    ZG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error("zg_merkle_root_noalloc_d: device ordinal %d out of range", dev);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    void *base = nullptr;
+    {
+        // One-time set-up per device, with that device current: the array's
+        // name is only a host-side stand-in, so its device address is looked up.
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *addr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+            if (e != cudaSuccess || !addr) {
+                set_error("cudaGetSymbolAddress of the scratch array failed: %s",
+                          cudaGetErrorString(e));
+                return ZG_ERR_CUDA;
+            }
+            g_noalloc_addr[dev] = addr;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t *tree = static_cast<uint32_t *>(base);
+    const uint8_t *cw = static_cast<const uint8_t *>(leaves_d);
+    // Every node is written before it is read, so nothing needs clearing.
+    if (nchunks == 0) {
+        k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw, width, leaf_bytes, tree);
+    } else {
+        uint32_t *cvs = tree + nodes * 8;
+        const uint64_t n = (uint64_t)width * nchunks;
+        k_leaf_chunks<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw, width, leaf_bytes,
+                                                                   (uint32_t)nchunks, cvs);
+        k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, (uint32_t)nchunks, tree);
+    }
+    ZG_CUDA(cudaGetLastError());
+    uint64_t off = 0;
+    for (uint32_t n = width; n > 1; n /= 2) {
+        const uint32_t half = n / 2;
+        k_merkle_level<<<(half + 255) / 256, 256, 0, s>>>(tree + off * 8, tree + (off + n) * 8,
+                                                          half, half == 1);
+        ZG_CUDA(cudaGetLastError());
+        off += n;
+    }
+    ZG_CUDA(cudaMemcpyAsync(root_d, tree + off * 8, 32, cudaMemcpyDeviceToDevice, s));
+    return ZG_OK;
+}
+
+

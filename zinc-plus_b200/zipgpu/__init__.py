@@ -41,7 +41,7 @@ EXPORTS = (
     "zg_last_error", "zg_version", "zg_ctx_create", "zg_ctx_destroy", "zg_ctx_kernel_launches",
     "zg_ctx_stream", "zg_ctx_set_kernel_timing", "zg_ctx_kernel_timing_report", "zg_params_create", "zg_params_destroy", "zg_params_get_info",
     "zg_params_iprs_tables", "zg_params_raa_perms", "zg_encode_rows", "zg_encode_rows_d",
-    "zg_encode_wide", "zg_merkle_root", "zg_commit", "zg_commit_d", "zg_hint_free",
+    "zg_encode_wide", "zg_merkle_root", "zg_merkle_root_noalloc_d", "zg_commit", "zg_commit_d", "zg_hint_free",
     "zg_hint_batch", "zg_hint_codeword", "zg_transcript_new", "zg_transcript_free",
     "zg_transcript_absorb", "zg_transcript_absorb_slice", "zg_transcript_challenge",
     "zg_transcript_sample_field", "zg_transcript_proof", "zg_prove", "zg_prove_d",
@@ -94,6 +94,7 @@ def lib() -> C.CDLL:
         "zg_encode_rows": ([vp, vp, vp], st), "zg_encode_rows_d": ([vp, vp, vp, vp], st),
         "zg_encode_wide": ([vp, vp, u32, vp], st),
         "zg_merkle_root": ([vp, vp, u32, u32, u32, vp], st),
+        "zg_merkle_root_noalloc_d": ([vp, u32, u32, vp, vp], st),
         "zg_commit": ([vp, vp, u32, C.POINTER(vp), vp], st),
         "zg_commit_d": ([vp, vp, u32, C.POINTER(vp), vp], st),
         "zg_hint_free": ([vp], st), "zg_hint_batch": ([vp], u32),
