@@ -209,6 +209,8 @@ def algorithmic_bytes(kernel, info, nv, D):
     N = R * L
     table = {
         "k_base_bin": N * 8 + info.base_dim * info.base_len * 4 + R * C * D * 4,
+        "k_stages2_bin": R * C * D * 4 + R * C * D * 8,
+        "k_tree_levels": C * 32,
         "k_stage_bin[0]": R * C * D * 4 + R * C * D * 8,
         "k_stage_bin[1+]": 2 * R * C * D * 8,
         "k_leaf_small": R * C * D * 8 + C * 32,
@@ -319,8 +321,10 @@ def run_ours(args):
     ctx.set_kernel_timing(True)
     ctx.kernel_times()
     timed(step_device)
-    ktimes = ctx.kernel_times()
+    alltimes = ctx.kernel_times()
     ctx.set_kernel_timing(False)
+    ktimes = {k: v for k, v in alltimes.items() if not k.startswith("host:")}
+    host_phases = {k[5:]: round(v[1] / K, 4) for k, v in alltimes.items() if k.startswith("host:")}
 
     value = world * K * n / (total_dev / 1e3)
     e2e = world * K * n / (total_host / 1e3)
@@ -373,6 +377,9 @@ def run_ours(args):
                     "latency_ms": {"p50": float(np.percentile(lat_host, 50)),
                                    "p99": float(np.percentile(lat_host, 99))}},
             "gpu_launches": int(launches),
+            "host_phases_ms_per_step": host_phases,
+            "kernel_ms_per_step": {k: round(v[1] / K, 4) for k, v in
+                                   sorted(ktimes.items(), key=lambda kv: -kv[1][1])},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clock_info,

@@ -211,8 +211,8 @@ zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hi
     const uint32_t C = p->info.codeword_len;
     const uint32_t nrows = batch * p->info.num_rows;
     const size_t leaf_bytes = leaf_bytes_of(p, batch);
-    if (leaf_bytes > 0xFFFFFFFFull) {
-        set_error("leaf too large");
+    if (leaf_bytes > 0xFFFFFFFFull || nrows > 65535) {
+        set_error("commitment too large: %u rows, %zu-byte leaves", nrows, leaf_bytes);
         return ZG_ERR_INVALID_PARAM;
     }
     std::unique_ptr<zg_hint> h(new zg_hint());
@@ -220,50 +220,34 @@ zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hi
     h->batch = batch;
     h->nrows = nrows;
     h->depth = ilog2u(C);
-    size_t off = 0;
-    for (uint32_t k = 0, n = C; k <= h->depth; k++, n /= 2) {
-        h->layer_off.push_back(off);
-        off += n;
-    }
-    ZG_CUDA(cudaMalloc(&h->d_cw, (size_t)C * leaf_bytes));
-    cudaError_t e = cudaMalloc(&h->d_tree, off * 32);
-    if (e != cudaSuccess) {
-        cudaFree(h->d_cw);
-        h->d_cw = nullptr;
-        ZG_CUDA(e);
-    }
-    e = cudaMalloc(&h->d_layer_off, sizeof(uint64_t) * h->layer_off.size());
-    if (e != cudaSuccess) {
-        cudaFree(h->d_cw);
-        cudaFree(h->d_tree);
-        h->d_cw = nullptr;
-        h->d_tree = nullptr;
-        ZG_CUDA(e);
-    }
-    std::vector<uint64_t> lo(h->layer_off.begin(), h->layer_off.end());
+    const size_t cw_bytes = ((size_t)C * leaf_bytes + 255) & ~(size_t)255;
+    const size_t tree_bytes = (2 * (size_t)C - 1) * 32;
+    h->block = ctx_alloc(ctx, cw_bytes + tree_bytes, &h->block_bytes);
+    if (!h->block) return ZG_ERR_OOM;
+    h->d_cw = static_cast<uint8_t *>(h->block);
+    h->d_tree = h->d_cw + cw_bytes;
+    hphase(ctx, "commit_alloc");
     auto fail = [&](zg_status st) {
-        cudaFree(h->d_cw);
-        cudaFree(h->d_tree);
-        cudaFree(h->d_layer_off);
-        h->d_cw = h->d_tree = nullptr;
-        h->d_layer_off = nullptr;
+        ctx_release(ctx, h->block, h->block_bytes);
+        h->block = nullptr;
         return st;
     };
-    if (cudaMemcpyAsync(h->d_layer_off, lo.data(), sizeof(uint64_t) * lo.size(),
-                        cudaMemcpyHostToDevice, s) != cudaSuccess)
-        return fail(ZG_ERR_CUDA);
     zg_status st = launch_encode(p, polys_d, nrows, h->d_cw, true, s);
     if (st != ZG_OK) return fail(st);
     st = launch_leaf_hash(ctx, h->d_cw, C, (uint32_t)leaf_bytes, h->d_tree, s);
     if (st != ZG_OK) return fail(st);
-    st = launch_merkle_levels(ctx, h->d_tree, C, h->layer_off, s);
+    st = launch_merkle_levels(ctx, h->d_tree, C, s);
     if (st != ZG_OK) return fail(st);
-    if (cudaMemcpyAsync(h->root, h->d_tree + h->layer_off.back() * 32, 32, cudaMemcpyDeviceToHost,
-                        s) != cudaSuccess ||
+    if ((st = ctx->pin_out.ensure(64)) != ZG_OK) return fail(st);
+    uint8_t *hroot = ctx->pin_out.as<uint8_t>();
+    if (cudaMemcpyAsync(hroot, h->d_tree + merkle_layer_off(C, h->depth) * 32, 32,
+                        cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
         set_error("commit failed: %s", cudaGetErrorString(cudaGetLastError()));
         return fail(ZG_ERR_CUDA);
     }
+    std::memcpy(h->root, hroot, 32);
+    hphase(ctx, "commit_gpu");
     *out = h.release();
     return ZG_OK;
 }
@@ -289,6 +273,7 @@ zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint
     const uint32_t CL = p->d.comb_limbs, D = p->D, nv = p->d.num_vars;
     const uint32_t lr = ilog2u(R), nhi = nv - lr;
     const bool binary = p->d.eval_kind == ZG_EVAL_BINPOLY;
+    hphase(ctx, "prove_enter");
 
     // point -> F, q0 (host), q1 (device) (point_to_tensor, pcs/utils.rs:90-114)
     std::vector<uint64_t> pf((size_t)(nv + 1) * L), omr((size_t)(nv + 1) * L);
@@ -326,19 +311,17 @@ zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint
     const uint32_t nparts = (RL + 255) / 256;
     const size_t q1_bytes = (size_t)RL * L * 8;
     const size_t part_bytes = (size_t)batch * R * nparts * L * 8;
-    const size_t b_bytes = (size_t)R * L * 8;
     const size_t comb_bytes = (size_t)RL * CL * 8;
     const size_t leaf_bytes = leaf_bytes_of(p, batch);
     const size_t open_bytes = leaf_bytes + 24 + 32 * (size_t)hint->depth;
     const size_t tail_bytes = comb_bytes + open_bytes * p->d.num_openings;
-    const size_t out_bytes = q1_bytes + part_bytes + b_bytes + tail_bytes + 64;
+    const size_t out_bytes = q1_bytes + part_bytes + tail_bytes + 64;
     ZG_TRY(ctx->prove_out.ensure(out_bytes));
     ZG_TRY(ctx->wprime.ensure((size_t)batch * R * RL * CL * 8));
     uint8_t *dout = ctx->prove_out.as<uint8_t>();
     uint64_t *q1_d = reinterpret_cast<uint64_t *>(dout);
     uint64_t *part_d = reinterpret_cast<uint64_t *>(dout + q1_bytes);
-    uint64_t *b_d = reinterpret_cast<uint64_t *>(dout + q1_bytes + part_bytes);
-    uint8_t *tail_d = dout + q1_bytes + part_bytes + b_bytes;
+    uint8_t *tail_d = dout + q1_bytes + part_bytes;
     tail_d = reinterpret_cast<uint8_t *>(((uintptr_t)tail_d + 15) & ~(uintptr_t)15);
 
     if (nhi) {
@@ -349,16 +332,23 @@ zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint
         ZG_CUDA(cudaMemcpyAsync(q1_d, f.one, 8 * L, cudaMemcpyHostToDevice, s));
     }
     ProjectArgs pa{polys_d, binary ? 1 : 0, reinterpret_cast<const i128 *>(din), Da,
-                   dmask_of(D), q1_d, RL, R, batch, CL, &f, ctx->wprime.as<uint64_t>(), part_d, b_d};
+                   dmask_of(D), q1_d, RL, R, batch, CL, &f, ctx->wprime.as<uint64_t>(), part_d};
     ZG_TRY(launch_project_rows(ctx, pa, s));
-    ZG_TRY(ctx->pin_out.ensure(std::max(b_bytes, tail_bytes) + 64));
+    ZG_TRY(ctx->pin_out.ensure(std::max(part_bytes, tail_bytes) + 64));
     uint64_t *hb = ctx->pin_out.as<uint64_t>();
-    ZG_CUDA(cudaMemcpyAsync(hb, b_d, b_bytes, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(cudaMemcpyAsync(hb, part_d, part_bytes, cudaMemcpyDeviceToHost, s));
+    hphase(ctx, "prove_setup");
     ZG_CUDA(cudaStreamSynchronize(s));
+    hphase(ctx, "prove_rows_gpu");
+    // b[j] = sum over polys and blocks of the partials (field addition)
+    std::vector<uint64_t> bv((size_t)R * L, 0);
+    for (uint32_t b = 0; b < batch; b++)
+        for (uint32_t j = 0; j < R; j++)
+            for (uint32_t q = 0; q < nparts; q++)
+                f_add(f, &bv[(size_t)j * L], hb + (((size_t)b * R + j) * nparts + q) * L);
 
     // write_field_elements(b) (pcs_transcript.rs:99-142): no length prefix for
     // Uint<L>; modulus | inner per element, each absorbed.
-    std::vector<uint64_t> bv(hb, hb + (size_t)R * L);
     const size_t fb = 8 * (size_t)L;
     for (uint32_t j = 0; j < R; j++) {
         tr_absorb_field(t, &bv[(size_t)j * L]);
@@ -378,6 +368,7 @@ zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint
         for (uint32_t j = 0; j < R; j++) coeffs[j] = tr_challenge_i128(t);
     std::vector<uint32_t> idxs(p->d.num_openings);
     for (uint32_t o = 0; o < p->d.num_openings; o++) idxs[o] = tr_challenge_u32(t) % C;
+    hphase(ctx, "prove_fs");
 
     // second upload: coeffs | indices
     const size_t c_off = 0, i_off = 16 * (size_t)R;
@@ -388,15 +379,17 @@ zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint
     ZG_CUDA(cudaMemcpyAsync(din2, hin2, i_off + 4 * idxs.size(), cudaMemcpyHostToDevice, s));
     CombineArgs ca{ctx->wprime.as<uint64_t>(), reinterpret_cast<const i128 *>(din2 + c_off),
                    batch, R, RL, CL, reinterpret_cast<uint64_t *>(tail_d), hint->d_cw,
-                   (uint32_t)leaf_bytes, hint->d_tree, hint->d_layer_off, hint->depth, C,
+                   (uint32_t)leaf_bytes, hint->d_tree, hint->depth, C,
                    p->d.num_openings, reinterpret_cast<const uint32_t *>(din2 + i_off),
                    tail_d + comb_bytes};
     ZG_TRY(launch_combined_and_openings(ctx, ca, s));
     uint8_t *htail = ctx->pin_out.as<uint8_t>();
     ZG_CUDA(cudaMemcpyAsync(htail, tail_d, tail_bytes, cudaMemcpyDeviceToHost, s));
     ZG_CUDA(cudaStreamSynchronize(s));
+    hphase(ctx, "prove_tail_gpu");
     t->stream.insert(t->stream.end(), htail, htail + tail_bytes);
     if (eval_out) std::memcpy(eval_out, ev, fb);
+    hphase(ctx, "prove_stream");
     return ZG_OK;
 }
 
@@ -591,6 +584,7 @@ zg_status zg_ctx_destroy(zg_ctx *ctx) {
     ctx->pin_out.release();
     ktimer_collect(ctx);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    ctx_cache_clear(ctx);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ZG_OK;
@@ -695,6 +689,12 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
         if (ctx) {
             ZG_CUDA(cudaMalloc(&p->d_bmT, bmT.size() * 4));
             ZG_CUDA(cudaMemcpy(p->d_bmT, bmT.data(), bmT.size() * 4, cudaMemcpyHostToDevice));
+            const uint32_t bdp = (bd + 7) / 8 * 8;
+            std::vector<int32_t> bmP((size_t)bdp * bl, 0);
+            for (uint32_t c = 0; c < bl; c++)
+                for (uint32_t r = 0; r < bd; r++) bmP[(size_t)c * bdp + r] = (int32_t)p->bm[(size_t)r * bl + c];
+            ZG_CUDA(cudaMalloc(&p->d_bmP, bmP.size() * 4));
+            ZG_CUDA(cudaMemcpy(p->d_bmP, bmP.data(), bmP.size() * 4, cudaMemcpyHostToDevice));
             ZG_CUDA(cudaMalloc(&p->d_tw, std::max<size_t>(tw32.size(), 1) * 4));
             if (!tw32.empty())
                 ZG_CUDA(cudaMemcpy(p->d_tw, tw32.data(), tw32.size() * 4, cudaMemcpyHostToDevice));
@@ -737,6 +737,7 @@ zg_status zg_params_destroy(zg_params *p) {
     if (p->ctx) {
         cudaSetDevice(p->ctx->device);
         cudaFree(p->d_bmT);
+        cudaFree(p->d_bmP);
         cudaFree(p->d_tw);
         cudaFree(p->d_perm);
     }
@@ -845,13 +846,7 @@ static zg_status merkle_root_impl(zg_ctx *ctx, const void *rows, uint32_t n_rows
     for (uint32_t r = 0; r < n_rows; r++)
         for (uint32_t j = 0; j < width; j++)
             std::memcpy(&lm[(size_t)j * leaf + (size_t)r * eb], src + ((size_t)r * width + j) * eb, eb);
-    std::vector<size_t> off;
-    size_t o = 0;
-    for (uint32_t n = width;; n /= 2) {
-        off.push_back(o);
-        o += n;
-        if (n == 1) break;
-    }
+    const size_t o = 2 * (size_t)width - 1;
     DevBuf cw, tree;
     ZG_TRY(cw.ensure(total));
     zg_status st = tree.ensure(o * 32);
@@ -863,9 +858,9 @@ static zg_status merkle_root_impl(zg_ctx *ctx, const void *rows, uint32_t n_rows
     st = ZG_OK;
     if (cudaMemcpyAsync(cw.ptr, lm.data(), total, cudaMemcpyHostToDevice, s) != cudaSuccess) st = ZG_ERR_CUDA;
     if (st == ZG_OK) st = launch_leaf_hash(ctx, cw.as<uint8_t>(), width, (uint32_t)leaf, tree.as<uint8_t>(), s);
-    if (st == ZG_OK) st = launch_merkle_levels(ctx, tree.as<uint8_t>(), width, off, s);
+    if (st == ZG_OK) st = launch_merkle_levels(ctx, tree.as<uint8_t>(), width, s);
     if (st == ZG_OK) {
-        if (cudaMemcpyAsync(root, tree.as<uint8_t>() + off.back() * 32, 32, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        if (cudaMemcpyAsync(root, tree.as<uint8_t>() + (o - 1) * 32, 32, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
             set_error("merkle root failed");
             st = ZG_ERR_CUDA;
@@ -933,10 +928,8 @@ zg_status zg_commit_d(zg_params *p, const void *polys_d, uint32_t batch, zg_hint
 
 zg_status zg_hint_free(zg_hint *h) {
     if (!h) return ZG_OK;
-    cudaSetDevice(h->params->ctx->device);
-    cudaFree(h->d_cw);
-    cudaFree(h->d_tree);
-    cudaFree(h->d_layer_off);
+    // the block returns to the context's cache (freed by zg_ctx_destroy)
+    if (h->block) ctx_release(h->params->ctx, h->block, h->block_bytes);
     delete h;
     return ZG_OK;
 }
@@ -1059,6 +1052,7 @@ static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t
                                      const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
                                      uint8_t *proof, size_t *proof_len) {
     zg_hint *h = nullptr;
+    hphase_start(p->ctx);
     ZG_TRY(commit_device(p, polys_d, batch, &h));
     std::memcpy(root, h->root, 32);
     zg_transcript t;
@@ -1068,6 +1062,7 @@ static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t
     tr_get_prime(&t, (int)p->d.field_limbs, prime);
     field_cfg_init(t.f, prime, (int)p->d.field_limbs);
     t.has_field = true;
+    hphase(p->ctx, "prime");
     zg_status st = prove_device(p, &t, polys_d, batch, point, h, eval_out);
     zg_hint_free(h);
     if (st != ZG_OK) return st;
@@ -1078,6 +1073,7 @@ static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t
     }
     std::memcpy(proof, t.stream.data(), t.stream.size());
     *proof_len = t.stream.size();
+    hphase(p->ctx, "proof_copy");
     return ZG_OK;
 }
 

@@ -74,6 +74,129 @@ __global__ void __launch_bounds__(256) k_base_bin(const uint64_t *__restrict__ e
     }
 }
 
+// Base layer, binary evaluations, two coefficient lanes per 64-bit multiply.
+// A lane's sum is |sum_c bm[rb][c] * bit| <= base_len * 32769 < 2^29 whenever
+// base_len < 16383, so lanes 2j and 2j+1 share one int64 accumulator as
+// lane_2j + 2^30 * lane_2j+1: each step adds bm * (b_2j + 2^30 b_2j+1), one
+// 32x32->64 multiply-add for two lanes.  The packed multipliers of a byte of
+// lane bits come from a 256-entry table.  Each thread owns 8 base rows x 8
+// lanes; a block owns 128 base rows and every lane group of one chunk.
+constexpr uint32_t kBase2Rows = 128;
+
+template <bool FINAL, bool LEAF_MAJOR>
+__global__ void __launch_bounds__(128) k_base_bin2(const uint64_t *__restrict__ evals,
+                                                   const int32_t *__restrict__ bmP, void *out,
+                                                   uint32_t row_len, uint32_t bd, uint32_t bdp,
+                                                   uint32_t bl, uint32_t depth, uint32_t C,
+                                                   uint32_t D, uint64_t dmask, uint32_t nrows) {
+    extern __shared__ __align__(16) uint8_t smem2[];
+    uint4 *lut = reinterpret_cast<uint4 *>(smem2);  // 256 x 4 packed multipliers
+    uint8_t *sxb = smem2 + 256 * sizeof(uint4);     // [group][c] lane bits
+    const uint32_t ngroups = blockDim.y;
+    const uint32_t grow = blockIdx.z, ch = blockIdx.y;
+    const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * ngroups;
+    for (uint32_t v = tid; v < 256; v += nthr) {
+        uint32_t m[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) m[j] = ((v >> (2 * j)) & 1u) | (((v >> (2 * j + 1)) & 1u) << 30);
+        lut[v] = make_uint4(m[0], m[1], m[2], m[3]);
+    }
+    const uint32_t oct = octet_reverse(ch, depth), shift = 3 * depth;
+    const uint64_t *row = evals + (size_t)grow * row_len;
+    for (uint32_t c = tid; c < bl; c += nthr) {
+        const uint64_t x = row[oct + ((size_t)c << shift)] & dmask;
+        for (uint32_t g = 0; g < ngroups; g++) sxb[(size_t)g * bl + c] = (uint8_t)(x >> (8 * g));
+    }
+    __syncthreads();
+    const uint32_t r0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
+    if (r0 >= bd) return;
+    const uint32_t g = threadIdx.y;
+    long long acc[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[r][j] = 0;
+    const int4 *bp = reinterpret_cast<const int4 *>(bmP + r0);
+    const uint32_t bstride = bdp / 4;
+    const uint8_t *xg = sxb + (size_t)g * bl;
+#pragma unroll 2
+    for (uint32_t c = 0; c < bl; c++) {
+        const uint4 m = lut[xg[c]];
+        const int4 b0 = __ldg(bp + (size_t)c * bstride), b1 = __ldg(bp + (size_t)c * bstride + 1);
+        const int bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        const int mv[4] = {(int)m.x, (int)m.y, (int)m.z, (int)m.w};
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[r][j] += (long long)bv[r] * mv[j];
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const uint32_t rb = r0 + r;
+        if (rb >= bd) break;
+        const size_t p = (size_t)ch * bd + rb;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const long long a = acc[r][j];
+            const long long lo = (long long)((unsigned long long)a << 34) >> 34;
+            const long long hi = (a - lo) >> 30;
+            const long long v2[2] = {lo, hi};
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const uint32_t lane = 8 * g + 2 * j + h;
+                if (lane >= D) continue;
+                if (FINAL) {
+                    int64_t *o = static_cast<int64_t *>(out);
+                    o[LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane] = v2[h];
+                } else {
+                    static_cast<int32_t *>(out)[((size_t)grow * C + p) * D + lane] = (int32_t)v2[h];
+                }
+            }
+        }
+    }
+}
+
+// Both radix-8 stages of a depth-2 code (combine_stages, radix8.rs:58-113) for
+// one base row rb of one codeword row, with the stage-0 outputs exchanged in
+// shared memory.  Thread (lane, q): stage 0 combines the chunks 8q..8q+7,
+// stage 1 combines, for r0 = q, the eight stage-0 outputs of each chunk group.
+// Output position (8 r1 + r0) * bd + rb.
+template <bool LEAF_MAJOR>
+__global__ void __launch_bounds__(512) k_stages2_bin(const int32_t *__restrict__ base,
+                                                     int64_t *__restrict__ out,
+                                                     const int32_t *__restrict__ tw0,
+                                                     const int32_t *__restrict__ tw1, uint32_t C,
+                                                     uint32_t bd, uint32_t D, uint32_t nrows) {
+    extern __shared__ int64_t ys[];  // [r0][c1][lane]
+    const uint32_t lane = threadIdx.x, q = threadIdx.y;
+    const uint32_t rb = blockIdx.x, grow = blockIdx.y;
+    uint64_t x[8];
+#pragma unroll
+    for (int c0 = 0; c0 < 8; c0++)
+        x[c0] = (uint64_t)(int64_t)base[((size_t)grow * C + (size_t)(8 * q + c0) * bd + rb) * D + lane];
+#pragma unroll
+    for (int r0 = 0; r0 < 8; r0++) {
+        uint64_t y = x[0];
+#pragma unroll
+        for (int j = 1; j < 8; j++)
+            y += x[j] * (uint64_t)(int64_t)__ldg(tw0 + (size_t)((j - 1) * 8 + ((r0 * j) & 7)) * bd + rb);
+        ys[((size_t)r0 * 8 + q) * D + lane] = (int64_t)y;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c1 = 0; c1 < 8; c1++) x[c1] = (uint64_t)ys[((size_t)q * 8 + c1) * D + lane];
+    const size_t i1 = (size_t)q * bd + rb, sub1 = 8 * (size_t)bd;
+#pragma unroll
+    for (int r1 = 0; r1 < 8; r1++) {
+        uint64_t z = x[0];
+#pragma unroll
+        for (int j = 1; j < 8; j++)
+            z += x[j] * (uint64_t)(int64_t)__ldg(tw1 + (size_t)((j - 1) * 8 + ((r1 * j) & 7)) * sub1 + i1);
+        const size_t p = (size_t)(8 * r1 + q) * bd + rb;
+        out[LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane] = (int64_t)z;
+    }
+}
+
 // One radix-8 stage (combine_stages, radix8.rs:58-113 with
 // apply_radix_8_butterflies, butterfly.rs:24-43) on 64-bit lanes:
 //   y_r = x_0 + sum_{j=1..7} x_j * tw[k][i][j-1][(r*j) mod 8]
@@ -317,32 +440,62 @@ zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8
     const uint32_t nch = 1u << (3 * depth);
     if (p->d.eval_kind == ZG_EVAL_BINPOLY) {
         const uint64_t *ev = static_cast<const uint64_t *>(evals_d);
-        dim3 block(32, (D + 7) / 8);
+        const uint32_t ngroups = (D + 7) / 8;
+        // packed-lane base kernel when every lane sum fits the 30-bit field
+        const bool packed = (uint64_t)bl * 32769u < (1ull << 29);
+        const uint32_t bdp = (bd + 7) / 8 * 8;
+        dim3 block2(16, ngroups), grid2((bd + kBase2Rows - 1) / kBase2Rows, nch, nrows);
+        const size_t smem2 = 256 * sizeof(uint4) + (size_t)ngroups * bl;
+        dim3 block(32, ngroups);
         dim3 grid((bd + 31) / 32, nch, nrows);
         size_t smem = (size_t)bl * 8;
-        if (smem > 48 * 1024) {
-            ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            ZG_CUDA(cudaFuncSetAttribute(k_base_bin<false, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        }
-        if (depth == 0) {
+        auto base_launch = [&](void *dst, bool final_out, bool lm) -> zg_status {
             ZG_KBEGIN(ctx, s, "k_base_bin");
-            if (leaf_major)
-                k_base_bin<true, true><<<grid, block, smem, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, D, dmask, nrows);
-            else
-                k_base_bin<true, false><<<grid, block, smem, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, D, dmask, nrows);
+            if (packed) {
+                if (smem2 > 48 * 1024) {
+                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+                }
+                if (final_out && lm)
+                    k_base_bin2<true, true><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows);
+                else if (final_out)
+                    k_base_bin2<true, false><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows);
+                else
+                    k_base_bin2<false, false><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows);
+            } else {
+                if (smem > 48 * 1024) {
+                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                }
+                if (final_out && lm)
+                    k_base_bin<true, true><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows);
+                else if (final_out)
+                    k_base_bin<true, false><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows);
+                else
+                    k_base_bin<false, false><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows);
+            }
+            ZG_KEND(ctx, s);
+            return ZG_OK;
+        };
+        if (depth == 0) return base_launch(out_d, true, leaf_major);
+        ZG_TRY(ctx->stage_a.ensure((size_t)nrows * C * D * 4));
+        int32_t *base = ctx->stage_a.as<int32_t>();
+        ZG_TRY(base_launch(base, false, false));
+        if (depth == 2 && D * 8 <= 512) {
+            // both stages in one kernel
+            dim3 b2(D, 8), g2(bd, nrows);
+            const size_t sm = (size_t)64 * D * 8;
+            const int32_t *tw0 = p->d_tw + p->tw_dev_off[0], *tw1 = p->d_tw + p->tw_dev_off[1];
+            int64_t *o = reinterpret_cast<int64_t *>(out_d);
+            ZG_KBEGIN(ctx, s, "k_stages2_bin");
+            if (leaf_major) k_stages2_bin<true><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows);
+            else k_stages2_bin<false><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows);
             ZG_KEND(ctx, s);
             return ZG_OK;
         }
-        ZG_TRY(ctx->stage_a.ensure((size_t)nrows * C * D * 4));
         ZG_TRY(ctx->stage_b.ensure((size_t)nrows * C * D * 8 * (depth > 1 ? 1 : 0) + 8));
-        int32_t *base = ctx->stage_a.as<int32_t>();
-        ZG_KBEGIN(ctx, s, "k_base_bin");
-        k_base_bin<false, false><<<grid, block, smem, s>>>(ev, p->d_bmT, base, L, bd, bl, depth, C, D, dmask, nrows);
-        ZG_KEND(ctx, s);
         const size_t nthr = (size_t)nrows * (C / 8) * D;
         const unsigned tb = 256, nb = blocks_for(nthr, tb);
         int64_t *prev = nullptr;

@@ -65,6 +65,7 @@ void HostBuf::release() {
 }
 
 // ------------------------------------------------------------ kernel timing
+static void add_total(zg_ctx *ctx, const std::string &name, double ms);
 static cudaEvent_t pool_get(zg_ctx *ctx) {
     if (!ctx->event_pool.empty()) {
         cudaEvent_t e = ctx->event_pool.back();
@@ -96,19 +97,77 @@ void ktimer_collect(zg_ctx *ctx) {
         cudaEventSynchronize(k.stop);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, k.start, k.stop);
-        bool found = false;
-        for (auto &t : ctx->totals)
-            if (t.first == k.name) {
-                t.second.first += ms;
-                t.second.second += 1;
-                found = true;
-                break;
-            }
-        if (!found) ctx->totals.push_back({k.name, {(double)ms, 1}});
+        add_total(ctx, k.name, ms);
         ctx->event_pool.push_back(k.start);
         ctx->event_pool.push_back(k.stop);
     }
     ctx->pending.clear();
+}
+
+static void add_total(zg_ctx *ctx, const std::string &name, double ms) {
+    for (auto &t : ctx->totals)
+        if (t.first == name) {
+            t.second.first += ms;
+            t.second.second += 1;
+            return;
+        }
+    ctx->totals.push_back({name, {ms, 1}});
+}
+
+void hphase_start(zg_ctx *ctx) {
+    if (ctx && ctx->timing) ctx->hmark = std::chrono::steady_clock::now();
+}
+
+void hphase(zg_ctx *ctx, const char *name) {
+    if (!ctx || !ctx->timing) return;
+    auto now = std::chrono::steady_clock::now();
+    add_total(ctx, std::string("host:") + name,
+              std::chrono::duration<double, std::milli>(now - ctx->hmark).count());
+    ctx->hmark = now;
+}
+
+// ------------------------------------------------------------ block cache
+static size_t cache_round(size_t bytes) {
+    const size_t g = bytes >= (2u << 20) ? (2u << 20) : 4096;
+    return (bytes + g - 1) / g * g;
+}
+
+void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got) {
+    const size_t want = cache_round(bytes);
+    {
+        std::lock_guard<std::mutex> lk(ctx->cache_mu);
+        auto it = ctx->cache.lower_bound(want);
+        if (it != ctx->cache.end() && it->first <= want + want / 2) {
+            void *p = it->second;
+            *got = it->first;
+            ctx->cache.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+        cudaGetLastError();
+        ctx_cache_clear(ctx);  // give cached blocks back and retry once
+        if (cudaMalloc(&p, want) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc(%zu) failed", want);
+            return nullptr;
+        }
+    }
+    *got = want;
+    return p;
+}
+
+void ctx_release(zg_ctx *ctx, void *p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(ctx->cache_mu);
+    ctx->cache.insert({bytes, p});
+}
+
+void ctx_cache_clear(zg_ctx *ctx) {
+    std::lock_guard<std::mutex> lk(ctx->cache_mu);
+    for (auto &kv : ctx->cache) cudaFree(kv.second);
+    ctx->cache.clear();
 }
 
 // -------------------------------------------------------------- transcript

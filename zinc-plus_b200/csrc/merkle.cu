@@ -92,6 +92,59 @@ __global__ void __launch_bounds__(256) k_merkle_level(const uint32_t *__restrict
     for (int k = 0; k < 8; k++) next[(size_t)i * 8 + k] = o[k];
 }
 
+// Tree levels k0+1 .. k0+nlev of a Merkle tree stored layer after layer
+// (layer k at node 2W - 2(W >> k)).  Block b reduces the 2^nlev nodes
+// [b * 2^nlev, (b+1) * 2^nlev) of layer k0 to one node, writing every
+// intermediate node; the tree's top node gets the ROOT flag.
+__global__ void __launch_bounds__(256) k_tree_levels(uint32_t *__restrict__ tree, uint32_t width,
+                                                     uint32_t k0, uint32_t nlev, uint32_t depth) {
+    __shared__ uint32_t cvs[256][8];
+    const uint32_t t = threadIdx.x;
+    const uint32_t half = 1u << (nlev - 1);
+    const size_t in_off = 2ull * width - 2ull * (width >> k0);
+    uint32_t cur[8];
+    if (t < half) {
+        const size_t node = in_off + ((size_t)blockIdx.x << nlev) + 2 * t;
+        uint32_t l[8], r[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            l[i] = tree[node * 8 + i];
+            r[i] = tree[(node + 1) * 8 + i];
+        }
+        b3::parent_cv(l, r, k0 + 1 == depth, cur);
+        const size_t out = 2ull * width - 2ull * (width >> (k0 + 1)) + ((size_t)blockIdx.x << (nlev - 1)) + t;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            tree[out * 8 + i] = cur[i];
+            cvs[t][i] = cur[i];
+        }
+    }
+    __syncthreads();
+    for (uint32_t lev = 2; lev <= nlev; lev++) {
+        const uint32_t n = 1u << (nlev - lev);
+        uint32_t l[8], r[8];
+        if (t < n) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                l[i] = cvs[2 * t][i];
+                r[i] = cvs[2 * t + 1][i];
+            }
+        }
+        __syncthreads();
+        if (t < n) {
+            const uint32_t k = k0 + lev;
+            b3::parent_cv(l, r, k == depth, cur);
+            const size_t out = 2ull * width - 2ull * (width >> k) + ((size_t)blockIdx.x << (nlev - lev)) + t;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                tree[out * 8 + i] = cur[i];
+                cvs[t][i] = cur[i];
+            }
+        }
+        __syncthreads();
+    }
+}
+
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
                            uint8_t *leaves_d, cudaStream_t s) {
     if (leaf_bytes % 4 != 0) {
@@ -118,17 +171,16 @@ zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uin
     return ZG_OK;
 }
 
-zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width,
-                               const std::vector<size_t> &layer_off, cudaStream_t s) {
+zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s) {
     uint32_t *tree = reinterpret_cast<uint32_t *>(tree_d);
-    uint32_t n = width;
-    for (size_t k = 1; k < layer_off.size(); k++) {
-        n /= 2;
-        const bool root = (k + 1 == layer_off.size());
-        ZG_KBEGIN(ctx, s, "k_merkle_level");
-        k_merkle_level<<<(n + 255) / 256, 256, 0, s>>>(tree + layer_off[k - 1] * 8,
-                                                       tree + layer_off[k] * 8, n, root);
+    const uint32_t depth = 31 - __builtin_clz(width);
+    for (uint32_t k0 = 0; k0 < depth;) {
+        const uint32_t nlev = depth - k0 < 9 ? depth - k0 : 9;
+        const uint32_t blocks = width >> (k0 + nlev);
+        ZG_KBEGIN(ctx, s, "k_tree_levels");
+        k_tree_levels<<<blocks, 1u << (nlev - 1), 0, s>>>(tree, width, k0, nlev, depth);
         ZG_KEND(ctx, s);
+        k0 += nlev;
     }
     return ZG_OK;
 }

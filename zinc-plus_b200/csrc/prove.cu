@@ -3,7 +3,6 @@
 //  k_eq_table      eq(x, r) over the hypercube (poly/src/utils.rs:24-101)
 //  k_project_rows  w'[j][c] = <eval, alphas> in CombR (phase_prove.rs:154-174)
 //                  and per-block partial sums of F(w') * q1 (b rows, :179-193)
-//  k_reduce_rows   b[j] = sum of the partials (field addition)
 //  k_combined_row  combined_row[c] = sum_poly sum_j s_j * w'[j][c] (:205-244)
 //  k_openings      column values and Merkle siblings of the opened columns in
 //                  proof byte order (open_merkle_trees_for_column, :285-304;
@@ -27,6 +26,39 @@ __global__ void k_eq_table(const uint64_t *__restrict__ r, const uint64_t *__res
         for (int w = 0; w < L; w++) acc[w] = t[w];
     }
     for (int w = 0; w < L; w++) out[(size_t)i * L + w] = acc[w];
+}
+
+// eq(x, r) over n <= 20 variables as an outer product: with n = a + b,
+// eq[i] = eq_lo[i mod 2^a] * eq_hi[i >> a], the half tables (over the first a
+// and the last b coordinates) being rebuilt by every block in shared memory.
+// Field products are exact, so the grouping does not change any value.
+template <int L>
+__global__ void __launch_bounds__(256) k_eq_table_split(const uint64_t *__restrict__ r,
+                                                        const uint64_t *__restrict__ omr,
+                                                        uint32_t n, FieldCfg f,
+                                                        uint64_t *__restrict__ out) {
+    extern __shared__ uint64_t tab[];  // [2^a + 2^b][L]
+    const uint32_t a = n / 2, b = n - a;
+    const uint32_t na = 1u << a, nb = 1u << b;
+    for (uint32_t e = threadIdx.x; e < na + nb; e += blockDim.x) {
+        const bool hi = e >= na;
+        const uint32_t idx = hi ? e - na : e, k0 = hi ? a : 0, kn = hi ? b : a;
+        uint64_t acc[L];
+        for (int w = 0; w < L; w++) acc[w] = f.one[w];
+        for (uint32_t k = 0; k < kn; k++) {
+            const uint64_t *sel = ((idx >> k) & 1u) ? r + (size_t)(k0 + k) * L : omr + (size_t)(k0 + k) * L;
+            uint64_t t[L];
+            fmul<L>(acc, sel, f.p, f.n0, t);
+            for (int w = 0; w < L; w++) acc[w] = t[w];
+        }
+        for (int w = 0; w < L; w++) tab[(size_t)e * L + w] = acc[w];
+    }
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (1u << n)) return;
+    uint64_t t[L];
+    fmul<L>(&tab[(size_t)(i & (na - 1)) * L], &tab[(size_t)(na + (i >> a)) * L], f.p, f.n0, t);
+    for (int w = 0; w < L; w++) out[(size_t)i * L + w] = t[w];
 }
 
 // One thread per (poly, row j, column c).  Binary evaluations project to
@@ -88,20 +120,6 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
     }
 }
 
-template <int L>
-__global__ void k_reduce_rows(const uint64_t *__restrict__ partial, uint32_t batch,
-                              uint32_t num_rows, uint32_t nparts, FieldCfg f,
-                              uint64_t *__restrict__ bvec) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= num_rows) return;
-    uint64_t acc[L];
-    for (int w = 0; w < L; w++) acc[w] = 0;
-    for (uint32_t b = 0; b < batch; b++)
-        for (uint32_t q = 0; q < nparts; q++)
-            fadd<L>(acc, partial + (((size_t)b * num_rows + j) * nparts + q) * L, f.p);
-    for (int w = 0; w < L; w++) bvec[(size_t)j * L + w] = acc[w];
-}
-
 __global__ void __launch_bounds__(256) k_combined_row(const uint64_t *__restrict__ wprime,
                                                       const i128 *__restrict__ coeffs,
                                                       uint32_t batch, uint32_t num_rows,
@@ -121,9 +139,8 @@ __global__ void __launch_bounds__(256) k_combined_row(const uint64_t *__restrict
 // One block per opening: column bytes, u64 leaf_index, u64 leaf_count,
 // u64 path length, then the sibling path bottom-up.
 __global__ void k_openings(const uint8_t *__restrict__ cw, uint32_t leaf_bytes,
-                           const uint8_t *__restrict__ tree, const uint64_t *__restrict__ layer_off,
-                           uint32_t depth, uint32_t width, const uint32_t *__restrict__ idxs,
-                           uint8_t *__restrict__ out) {
+                           const uint8_t *__restrict__ tree, uint32_t depth, uint32_t width,
+                           const uint32_t *__restrict__ idxs, uint8_t *__restrict__ out) {
     const uint32_t o = blockIdx.x, idx = idxs[o];
     const size_t open_bytes = (size_t)leaf_bytes + 24 + 32 * (size_t)depth;
     uint8_t *dst = out + (size_t)o * open_bytes;
@@ -139,7 +156,7 @@ __global__ void k_openings(const uint8_t *__restrict__ cw, uint32_t leaf_bytes,
     const uint32_t nw = 8 * depth;
     for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
         const uint32_t k = w / 8, part = w % 8;
-        const uint64_t node = layer_off[k] + ((idx >> k) ^ 1u);
+        const uint64_t node = 2ull * width - 2ull * (width >> k) + ((idx >> k) ^ 1u);
         reinterpret_cast<uint32_t *>(dst + leaf_bytes + 24)[w] =
             reinterpret_cast<const uint32_t *>(tree)[node * 8 + part];
     }
@@ -151,7 +168,14 @@ static zg_status eq_table_t(zg_ctx *ctx, const uint64_t *r_d, const uint64_t *om
                             const FieldCfg &f, uint64_t *out_d, cudaStream_t s) {
     const uint32_t m = 1u << n;
     ZG_KBEGIN(ctx, s, "k_eq_table");
-    k_eq_table<L><<<(m + 255) / 256, 256, 0, s>>>(r_d, omr_d, n, f, out_d);
+    if (n >= 2 && n <= 20) {
+        const size_t sm = ((size_t)(1u << (n / 2)) + (1u << (n - n / 2))) * L * 8;
+        if (sm > 48 * 1024)
+            ZG_CUDA(cudaFuncSetAttribute(k_eq_table_split<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_eq_table_split<L><<<(m + 255) / 256, 256, sm, s>>>(r_d, omr_d, n, f, out_d);
+    } else {
+        k_eq_table<L><<<(m + 255) / 256, 256, 0, s>>>(r_d, omr_d, n, f, out_d);
+    }
     ZG_KEND(ctx, s);
     return ZG_OK;
 }
@@ -170,10 +194,6 @@ static zg_status project_t(zg_ctx *ctx, const ProjectArgs &a, cudaStream_t s) {
                                            a.row_len, a.num_rows, a.comb_limbs, *a.f, a.wprime,
                                            a.partial);
     ZG_KEND(ctx, s);
-    ZG_KBEGIN(ctx, s, "k_reduce_rows");
-    k_reduce_rows<L><<<(a.num_rows + 127) / 128, 128, 0, s>>>(a.partial, a.batch, a.num_rows,
-                                                               grid.x, *a.f, a.bvec);
-    ZG_KEND(ctx, s);
     return ZG_OK;
 }
 
@@ -188,8 +208,8 @@ zg_status launch_combined_and_openings(zg_ctx *ctx, const CombineArgs &a, cudaSt
                                                            a.comb_out);
     ZG_KEND(ctx, s);
     ZG_KBEGIN(ctx, s, "k_openings");
-    k_openings<<<a.n_open, 128, 0, s>>>(a.cw, a.leaf_bytes, a.tree, a.layer_off, a.depth, a.width,
-                                        a.idxs, a.open_out);
+    k_openings<<<a.n_open, 128, 0, s>>>(a.cw, a.leaf_bytes, a.tree, a.depth, a.width, a.idxs,
+                                        a.open_out);
     ZG_KEND(ctx, s);
     return ZG_OK;
 }

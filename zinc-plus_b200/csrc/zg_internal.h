@@ -3,7 +3,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <cstdarg>
+#include <map>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -79,6 +81,13 @@ struct zg_ctx_timer;
 void ktimer_begin(zg_ctx *ctx, cudaStream_t s, const char *name);
 void ktimer_end(zg_ctx *ctx, cudaStream_t s);
 void ktimer_collect(zg_ctx *ctx);
+// Host phase wall time since the previous mark, reported as "host:<name>".
+void hphase_start(zg_ctx *ctx);
+void hphase(zg_ctx *ctx, const char *name);
+// Device block cache of a context.
+void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got);
+void ctx_release(zg_ctx *ctx, void *p, size_t bytes);
+void ctx_cache_clear(zg_ctx *ctx);
 
 // One pending timed launch.
 struct KernelEvent {
@@ -109,6 +118,11 @@ struct zg_ctx {
     std::vector<zg::KernelEvent> pending;
     std::vector<cudaEvent_t> event_pool;
     std::vector<std::pair<std::string, std::pair<double, uint64_t>>> totals;  // name -> (ms, n)
+    std::chrono::steady_clock::time_point hmark;
+    // device block cache: freed hint blocks are kept for reuse (no cudaFree on
+    // the request path); released by zg_ctx_destroy.
+    std::mutex cache_mu;
+    std::multimap<size_t, void *> cache;
 };
 
 struct zg_params {
@@ -120,6 +134,7 @@ struct zg_params {
     std::vector<int64_t> bm;  // base_dim x base_len
     std::vector<int64_t> tw;  // stage k: (base_dim*8^k) x 7 x 8, stages back to back
     int32_t *d_bmT = nullptr; // base_len x base_dim (transposed)
+    int32_t *d_bmP = nullptr; // base_len x round_up(base_dim, 8) (transposed, zero padded)
     int32_t *d_tw = nullptr;  // stage k: [56][sub_k], stages back to back
     std::vector<size_t> tw_off;      // offset of each stage in tw (host, [i][j-1][t])
     std::vector<size_t> tw_dev_off;  // offset of each stage in d_tw (device, [56][sub])
@@ -132,11 +147,12 @@ struct zg_hint {
     zg_params *params = nullptr;
     uint32_t batch = 0;
     uint32_t nrows = 0;        // batch * num_rows
+    void *block = nullptr;     // one cached device block holding both arrays
+    size_t block_bytes = 0;
     uint8_t *d_cw = nullptr;   // leaf-major: codeword_len x nrows x cw_bytes
-    uint8_t *d_tree = nullptr; // Merkle layers, leaves first, root last, 32 B nodes
+    uint8_t *d_tree = nullptr; // Merkle layers, leaves first, root last, 32 B nodes;
+                               // layer k starts at node 2C - 2(C >> k)
     uint32_t depth = 0;        // log2(codeword_len)
-    std::vector<size_t> layer_off;  // node offset of each layer
-    uint64_t *d_layer_off = nullptr;
     uint8_t root[32];
 };
 
@@ -179,7 +195,9 @@ zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8
                         bool leaf_major, cudaStream_t s);
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
                            uint8_t *leaves_d, cudaStream_t s);
-zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width,
-                               const std::vector<size_t> &layer_off, cudaStream_t s);
+zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s);
+
+// Node offset of Merkle layer k for `width` leaves (layers stored leaves first).
+inline size_t merkle_layer_off(size_t width, uint32_t k) { return 2 * width - 2 * (width >> k); }
 
 }  // namespace zg

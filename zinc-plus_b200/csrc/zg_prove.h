@@ -14,8 +14,7 @@ struct ProjectArgs {
     uint32_t row_len, num_rows, batch, comb_limbs;
     const FieldCfg *f;
     uint64_t *wprime;       // batch x num_rows x row_len x comb_limbs
-    uint64_t *partial;      // batch x num_rows x ceil(row_len/256) x L
-    uint64_t *bvec;         // num_rows x L
+    uint64_t *partial;      // batch x num_rows x ceil(row_len/256) x L (summed on the host)
 };
 
 struct CombineArgs {
@@ -26,7 +25,6 @@ struct CombineArgs {
     const uint8_t *cw;      // leaf-major codeword
     uint32_t leaf_bytes;
     const uint8_t *tree;
-    const uint64_t *layer_off;  // device copy, depth+1 entries
     uint32_t depth, width, n_open;
     const uint32_t *idxs;
     uint8_t *open_out;
