@@ -253,7 +253,8 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(ctx.stream)
     point = Z.i128_bytes([1] * nv)
     cap = pp.proof_size(1)
-    proof = C.create_string_buffer(cap)
+    proof_t = torch.empty(cap, dtype=torch.uint8).pin_memory()  # page-locked: D2H lands in place
+    proof = C.c_void_p(proof_t.data_ptr())
     root = C.create_string_buffer(32)
     ev = C.create_string_buffer(32)
     plen = C.c_size_t(cap)

@@ -254,7 +254,8 @@ zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hi
 
 // -------------------------------------------------------------------- prove
 zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
-                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out) {
+                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
+                       uint8_t *tail_out) {
     if (!t->has_field || t->f.L != (int)p->d.field_limbs) {
         set_error("transcript has no field configuration of %u limbs (sample it first)",
                   p->d.field_limbs);
@@ -383,11 +384,24 @@ zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint
                    p->d.num_openings, reinterpret_cast<const uint32_t *>(din2 + i_off),
                    tail_d + comb_bytes};
     ZG_TRY(launch_combined_and_openings(ctx, ca, s));
-    uint8_t *htail = ctx->pin_out.as<uint8_t>();
+    // The proof tail (combined row + openings) goes straight to tail_out when
+    // the caller gave one that is page-locked; otherwise through pinned staging.
+    bool direct = false;
+    if (tail_out) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, tail_out) == cudaSuccess && at.type == cudaMemoryTypeHost)
+            direct = true;
+        cudaGetLastError();
+    }
+    uint8_t *htail = direct ? tail_out : ctx->pin_out.as<uint8_t>();
     ZG_CUDA(cudaMemcpyAsync(htail, tail_d, tail_bytes, cudaMemcpyDeviceToHost, s));
     ZG_CUDA(cudaStreamSynchronize(s));
     hphase(ctx, "prove_tail_gpu");
-    t->stream.insert(t->stream.end(), htail, htail + tail_bytes);
+    if (tail_out) {
+        if (!direct) std::memcpy(tail_out, htail, tail_bytes);
+    } else {
+        t->stream.insert(t->stream.end(), htail, htail + tail_bytes);
+    }
     if (eval_out) std::memcpy(eval_out, ev, fb);
     hphase(ctx, "prove_stream");
     return ZG_OK;
@@ -695,6 +709,19 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
                 for (uint32_t r = 0; r < bd; r++) bmP[(size_t)c * bdp + r] = (int32_t)p->bm[(size_t)r * bl + c];
             ZG_CUDA(cudaMalloc(&p->d_bmP, bmP.size() * 4));
             ZG_CUDA(cudaMemcpy(p->d_bmP, bmP.data(), bmP.size() * 4, cudaMemcpyHostToDevice));
+            // u8 limbs: bm = l0 + 256 l1 - 65536 [bm < 0]
+            const uint32_t blp = (bl + 31) / 32 * 32;
+            std::vector<uint8_t> bmL((size_t)3 * bd * blp, 0);
+            for (uint32_t r = 0; r < bd; r++)
+                for (uint32_t c = 0; c < bl; c++) {
+                    const int64_t v = p->bm[(size_t)r * bl + c];
+                    const uint32_t u = (uint32_t)(v & 0xFFFF);
+                    bmL[((size_t)0 * bd + r) * blp + c] = (uint8_t)(u & 0xFF);
+                    bmL[((size_t)1 * bd + r) * blp + c] = (uint8_t)(u >> 8);
+                    bmL[((size_t)2 * bd + r) * blp + c] = v < 0 ? 1 : 0;
+                }
+            ZG_CUDA(cudaMalloc(&p->d_bmL, bmL.size()));
+            ZG_CUDA(cudaMemcpy(p->d_bmL, bmL.data(), bmL.size(), cudaMemcpyHostToDevice));
             ZG_CUDA(cudaMalloc(&p->d_tw, std::max<size_t>(tw32.size(), 1) * 4));
             if (!tw32.empty())
                 ZG_CUDA(cudaMemcpy(p->d_tw, tw32.data(), tw32.size() * 4, cudaMemcpyHostToDevice));
@@ -738,6 +765,7 @@ zg_status zg_params_destroy(zg_params *p) {
         cudaSetDevice(p->ctx->device);
         cudaFree(p->d_bmT);
         cudaFree(p->d_bmP);
+        cudaFree(p->d_bmL);
         cudaFree(p->d_tw);
         cudaFree(p->d_perm);
     }
@@ -1018,7 +1046,7 @@ static zg_status prove_impl(zg_params *p, zg_transcript *t, const void *const *p
         return ZG_ERR_INVALID_PARAM;
     }
     ZG_TRY(stage_polys(p, polys, batch));
-    return prove_device(p, t, p->ctx->evals.ptr, batch, point, hint, eval_out);
+    return prove_device(p, t, p->ctx->evals.ptr, batch, point, hint, eval_out, nullptr);
 }
 
 zg_status zg_prove(zg_params *p, zg_transcript *t, const void *const *polys, uint32_t batch,
@@ -1032,7 +1060,7 @@ static zg_status prove_d_impl(zg_params *p, zg_transcript *t, const void *polys_
     ZG_TRY(need_device(p));
     std::lock_guard<std::mutex> lk(p->ctx->mu);
     ZG_CUDA(cudaSetDevice(p->ctx->device));
-    return prove_device(p, t, polys_d, batch, point, hint, eval_out);
+    return prove_device(p, t, polys_d, batch, point, hint, eval_out, nullptr);
 }
 
 zg_status zg_prove_d(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
@@ -1051,28 +1079,35 @@ size_t zg_proof_size(const zg_params *p, uint32_t batch) {
 static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t batch,
                                      const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
                                      uint8_t *proof, size_t *proof_len) {
+    const size_t need = zg_proof_size(p, batch);
+    if (*proof_len < need) {
+        *proof_len = need;
+        set_error("proof buffer too small (%zu bytes needed)", need);
+        return ZG_ERR_BUFFER_TOO_SMALL;
+    }
     zg_hint *h = nullptr;
     hphase_start(p->ctx);
     ZG_TRY(commit_device(p, polys_d, batch, &h));
     std::memcpy(root, h->root, 32);
     zg_transcript t;
-    t.stream.reserve(zg_proof_size(p, batch));
     tr_absorb_slice(&t, h->root, 32);
     uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
     tr_get_prime(&t, (int)p->d.field_limbs, prime);
     field_cfg_init(t.f, prime, (int)p->d.field_limbs);
     t.has_field = true;
     hphase(p->ctx, "prime");
-    zg_status st = prove_device(p, &t, polys_d, batch, point, h, eval_out);
+    // The b rows are written to the transcript stream; the rest of the proof
+    // lands directly after them in the caller's buffer.
+    const size_t head = (size_t)p->info.num_rows * 2 * p->info.field_bytes;
+    zg_status st = prove_device(p, &t, polys_d, batch, point, h, eval_out, proof + head);
     zg_hint_free(h);
     if (st != ZG_OK) return st;
-    if (*proof_len < t.stream.size()) {
-        *proof_len = t.stream.size();
-        set_error("proof buffer too small (%zu bytes needed)", t.stream.size());
-        return ZG_ERR_BUFFER_TOO_SMALL;
+    if (t.stream.size() != head) {
+        set_error("internal: unexpected proof head size %zu", t.stream.size());
+        return ZG_ERR_INVALID_PARAM;
     }
-    std::memcpy(proof, t.stream.data(), t.stream.size());
-    *proof_len = t.stream.size();
+    std::memcpy(proof, t.stream.data(), head);
+    *proof_len = need;
     hphase(p->ctx, "proof_copy");
     return ZG_OK;
 }

@@ -156,6 +156,238 @@ __global__ void __launch_bounds__(128) k_base_bin2(const uint64_t *__restrict__ 
     }
 }
 
+// Base layer, binary evaluations: the packed-lane multiply of k_base_bin2
+// with the block's slice of the base matrix (TR rows x base_len) staged in
+// shared memory once and reused by kBase3Chunks chunks, so the inner loop reads
+// only shared memory.  Thread = (row octet, lane group, chunk); a warp holds
+// all row octets of one chunk, so its base-matrix reads are broadcasts.
+constexpr uint32_t kBase3Chunks = 8;
+
+template <uint32_t TR, bool FINAL, bool LEAF_MAJOR>
+__global__ void __launch_bounds__(512) k_base_bin3(const uint64_t *__restrict__ evals,
+                                                   const int32_t *__restrict__ bmP, void *out,
+                                                   uint32_t row_len, uint32_t bd, uint32_t bdp,
+                                                   uint32_t bl, uint32_t depth, uint32_t nch,
+                                                   uint32_t C, uint32_t D, uint32_t ngroups,
+                                                   uint64_t dmask, uint32_t nrows) {
+    extern __shared__ __align__(16) uint8_t smem3[];
+    constexpr uint32_t RO = TR / 8;
+    int4 *bmS = reinterpret_cast<int4 *>(smem3);                  // [bl][TR/4]
+    uint4 *lut = reinterpret_cast<uint4 *>(smem3 + (size_t)bl * TR * 4);
+    uint8_t *xs = reinterpret_cast<uint8_t *>(lut + 256);           // [chunk][group][bl]
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t rb0 = blockIdx.x * TR, ch0 = blockIdx.y * kBase3Chunks, grow = blockIdx.z;
+    // base-matrix slice (rows past bd read as zero)
+    for (uint32_t e = tid; e < bl * (TR / 4); e += nthr) {
+        const uint32_t c = e / (TR / 4), r4 = (e % (TR / 4)) * 4;
+        int4 v = make_int4(0, 0, 0, 0);
+        if (rb0 + r4 < bdp) v = __ldg(reinterpret_cast<const int4 *>(bmP + (size_t)c * bdp + rb0 + r4));
+        bmS[e] = v;
+    }
+    for (uint32_t v = tid; v < 256; v += nthr) {
+        uint32_t m[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) m[j] = ((v >> (2 * j)) & 1u) | (((v >> (2 * j + 1)) & 1u) << 30);
+        lut[v] = make_uint4(m[0], m[1], m[2], m[3]);
+    }
+    const uint32_t shift = 3 * depth;
+    const uint64_t *row = evals + (size_t)grow * row_len;
+    for (uint32_t e = tid; e < kBase3Chunks * bl; e += nthr) {
+        const uint32_t chl = e / bl, c = e % bl, ch = ch0 + chl;
+        uint64_t x = 0;
+        if (ch < nch) x = row[octet_reverse(ch, depth) + ((size_t)c << shift)] & dmask;
+        for (uint32_t g = 0; g < ngroups; g++) xs[((size_t)chl * ngroups + g) * bl + c] = (uint8_t)(x >> (8 * g));
+    }
+    __syncthreads();
+    const uint32_t ro = tid % RO, g = (tid / RO) % ngroups, chl = tid / (RO * ngroups);
+    const uint32_t ch = ch0 + chl, r0 = rb0 + 8 * ro;
+    if (chl >= kBase3Chunks || ch >= nch || r0 >= bd) return;
+    long long acc[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[r][j] = 0;
+    const uint8_t *xg = xs + ((size_t)chl * ngroups + g) * bl;
+    const int4 *bs = bmS + 2 * ro;
+#pragma unroll 4
+    for (uint32_t c = 0; c < bl; c++) {
+        const uint4 m = lut[xg[c]];
+        const int4 b0 = bs[(size_t)c * (TR / 4)], b1 = bs[(size_t)c * (TR / 4) + 1];
+        const int bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        const int mv[4] = {(int)m.x, (int)m.y, (int)m.z, (int)m.w};
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[r][j] += (long long)bv[r] * mv[j];
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const uint32_t rb = r0 + r;
+        if (rb >= bd) break;
+        const size_t p = (size_t)ch * bd + rb;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const long long a = acc[r][j];
+            const long long lo = (long long)((unsigned long long)a << 34) >> 34;
+            const long long hi = (a - lo) >> 30;
+            const long long v2[2] = {lo, hi};
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const uint32_t lane = 8 * g + 2 * j + h;
+                if (lane >= D) continue;
+                if (FINAL) {
+                    int64_t *o = static_cast<int64_t *>(out);
+                    o[LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane] = v2[h];
+                } else {
+                    static_cast<int32_t *>(out)[((size_t)grow * C + p) * D + lane] = (int32_t)v2[h];
+                }
+            }
+        }
+    }
+}
+
+// Base layer, binary evaluations, on the tensor cores.  For one chunk of one
+// codeword row the base layer is the exact integer product
+//   base[rb][lane] = sum_c bm[rb][c] * bit_lane(x_c),
+// an (bd x bl) by (bl x D) matrix product with {0,1} entries on the right.
+// bm in [-32769, 32767] splits exactly into unsigned bytes,
+//   bm = l0 + 256 l1 - 65536 [bm < 0],   l0, l1 in [0, 255],
+// so three u8 x u8 -> s32 MMAs (m16n8k32) per tile give the exact result; no
+// partial sum exceeds 255 * bl < 2^31.  A (the limbs) is staged in shared
+// memory and read with ldmatrix; B is built in registers from the lane masks
+// with byte permutes (bit n of the input words is column n of B).
+//
+// Block: 4 warps over a 64-row slice of the base matrix; warp (mw, cw) owns
+// rows 32 mw .. 32 mw + 31 (two m16 tiles) and every other (row, chunk) pair of
+// the block's kMmaPairs pairs.  Lanes are processed 32 at a time (four n8 tiles).
+constexpr uint32_t kMmaRows = 64;
+constexpr uint32_t kMmaPairs = 8;
+
+__device__ __forceinline__ void mma_u8_16x8x32(int (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                               uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void *smem_ptr) {
+    const uint32_t addr = (uint32_t)__cvta_generic_to_shared(smem_ptr);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+
+// B fragments of four n8 tiles from four input words: word i holds the lanes
+// of input k0 + 4t + i; the result for tile nt has byte i = bit (8 nt + g).
+__device__ __forceinline__ void bits_to_bfrag(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3,
+                                              uint32_t g, uint32_t (&b)[4]) {
+    const uint32_t y0 = (x0 >> g) & 0x01010101u, y1 = (x1 >> g) & 0x01010101u;
+    const uint32_t y2 = (x2 >> g) & 0x01010101u, y3 = (x3 >> g) & 0x01010101u;
+    const uint32_t lo01 = __byte_perm(y0, y1, 0x5140), hi01 = __byte_perm(y0, y1, 0x7362);
+    const uint32_t lo23 = __byte_perm(y2, y3, 0x5140), hi23 = __byte_perm(y2, y3, 0x7362);
+    b[0] = __byte_perm(lo01, lo23, 0x5410);
+    b[1] = __byte_perm(lo01, lo23, 0x7632);
+    b[2] = __byte_perm(hi01, hi23, 0x5410);
+    b[3] = __byte_perm(hi01, hi23, 0x7632);
+}
+
+__global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ evals,
+                                                  const uint8_t *__restrict__ bmL,
+                                                  int32_t *__restrict__ out, uint32_t row_len,
+                                                  uint32_t bd, uint32_t bl, uint32_t blp,
+                                                  uint32_t depth, uint32_t nch, uint32_t C,
+                                                  uint32_t D, uint64_t dmask, uint32_t nrows) {
+    extern __shared__ __align__(16) uint8_t smem_m[];
+    const uint32_t astride = blp + 16;  // padded row: conflict-free ldmatrix
+    uint8_t *As = smem_m;                                               // [3][64][astride]
+    uint64_t *Xs = reinterpret_cast<uint64_t *>(smem_m + 3 * kMmaRows * astride);  // [pairs][blp]
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t rb0 = blockIdx.x * kMmaRows;
+    const uint32_t pair0 = blockIdx.y * kMmaPairs, npairs = nrows * nch;
+    // A slice: 16-byte pieces (limb, row, k); rows past bd and k past bl are zero
+    const uint32_t pieces_per_row = blp / 16;
+    for (uint32_t e = tid; e < 3 * kMmaRows * pieces_per_row; e += nthr) {
+        const uint32_t limb = e / (kMmaRows * pieces_per_row);
+        const uint32_t rem = e % (kMmaRows * pieces_per_row);
+        const uint32_t row = rem / pieces_per_row, k = (rem % pieces_per_row) * 16;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (rb0 + row < bd && k < bl)
+            v = __ldg(reinterpret_cast<const uint4 *>(bmL + ((size_t)limb * bd + rb0 + row) * blp + k));
+        *reinterpret_cast<uint4 *>(As + ((size_t)limb * kMmaRows + row) * astride + k) = v;
+    }
+    const uint32_t shift = 3 * depth;
+    for (uint32_t e = tid; e < kMmaPairs * blp; e += nthr) {
+        const uint32_t pi = e / blp, c = e % blp, pair = pair0 + pi;
+        uint64_t x = 0;
+        if (pair < npairs && c < bl) {
+            const uint32_t grow = pair / nch, ch = pair % nch;
+            x = evals[(size_t)grow * row_len + octet_reverse(ch, depth) + ((size_t)c << shift)] & dmask;
+        }
+        Xs[e] = x;
+    }
+    __syncthreads();
+    const uint32_t lane = tid & 31, warp = tid >> 5;
+    const uint32_t mw = warp & 1, cw = warp >> 1;
+    const uint32_t g = lane >> 2, t = lane & 3;
+    const uint32_t lrow = lane & 15, lk = (lane >> 4) * 16;
+    for (uint32_t pi = cw; pi < kMmaPairs; pi += 2) {
+        const uint32_t pair = pair0 + pi;
+        if (pair >= npairs) break;
+        const uint32_t grow = pair / nch, ch = pair % nch;
+        const uint64_t *xp = Xs + (size_t)pi * blp;
+        for (uint32_t half = 0; half * 32 < D; half++) {
+            int acc[2][4][3][4];
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++)
+#pragma unroll
+                        for (int d = 0; d < 4; d++) acc[a][b][c][d] = 0;
+            for (uint32_t k0 = 0; k0 < blp; k0 += 32) {
+                uint32_t afr[2][3][4];
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                    for (int limb = 0; limb < 3; limb++)
+                        ldmatrix_x4(afr[mt][limb], As + ((size_t)limb * kMmaRows + 32 * mw + 16 * mt + lrow) * astride + k0 + lk);
+                uint32_t xw[8];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    xw[i] = (uint32_t)(xp[k0 + 4 * t + i] >> (32 * half));
+                    xw[4 + i] = (uint32_t)(xp[k0 + 16 + 4 * t + i] >> (32 * half));
+                }
+                uint32_t b0[4], b1[4];
+                bits_to_bfrag(xw[0], xw[1], xw[2], xw[3], g, b0);
+                bits_to_bfrag(xw[4], xw[5], xw[6], xw[7], g, b1);
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                        for (int limb = 0; limb < 3; limb++) mma_u8_16x8x32(acc[mt][nt][limb], afr[mt][limb], b0[nt], b1[nt]);
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const uint32_t r = rb0 + 32 * mw + 16 * mt + g + (e >= 2 ? 8 : 0);
+                        const uint32_t ln = 32 * half + 8 * nt + 2 * t + (e & 1);
+                        if (r < bd && ln < D) {
+                            const long long v = (long long)acc[mt][nt][0][e] + 256ll * acc[mt][nt][1][e] -
+                                                65536ll * acc[mt][nt][2][e];
+                            out[((size_t)grow * C + (size_t)ch * bd + r) * D + ln] = (int32_t)v;
+                        }
+                    }
+        }
+    }
+}
+
 // Both radix-8 stages of a depth-2 code (combine_stages, radix8.rs:58-113) for
 // one base row rb of one codeword row, with the stage-0 outputs exchanged in
 // shared memory.  Thread (lane, q): stage 0 combines the chunks 8q..8q+7,
@@ -167,31 +399,38 @@ __global__ void __launch_bounds__(512) k_stages2_bin(const int32_t *__restrict__
                                                      const int32_t *__restrict__ tw0,
                                                      const int32_t *__restrict__ tw1, uint32_t C,
                                                      uint32_t bd, uint32_t D, uint32_t nrows) {
-    extern __shared__ int64_t ys[];  // [r0][c1][lane]
+    extern __shared__ int64_t ys[];  // [r0][c1][lane], then the twiddles
+    int32_t *tws = reinterpret_cast<int32_t *>(ys + (size_t)64 * D);  // [9][56]
     const uint32_t lane = threadIdx.x, q = threadIdx.y;
     const uint32_t rb = blockIdx.x, grow = blockIdx.y;
+    const uint32_t tid = q * blockDim.x + lane, nthr = blockDim.x * blockDim.y;
+    // stage-0 twiddles of position rb, stage-1 twiddles of positions q*bd + rb
+    for (uint32_t e = tid; e < 9 * 56; e += nthr) {
+        const uint32_t which = e / 56, k = e % 56;
+        tws[e] = which == 0 ? tw0[(size_t)k * bd + rb]
+                            : tw1[(size_t)k * 8 * bd + (size_t)(which - 1) * bd + rb];
+    }
     uint64_t x[8];
 #pragma unroll
     for (int c0 = 0; c0 < 8; c0++)
         x[c0] = (uint64_t)(int64_t)base[((size_t)grow * C + (size_t)(8 * q + c0) * bd + rb) * D + lane];
+    __syncthreads();
 #pragma unroll
     for (int r0 = 0; r0 < 8; r0++) {
         uint64_t y = x[0];
 #pragma unroll
-        for (int j = 1; j < 8; j++)
-            y += x[j] * (uint64_t)(int64_t)__ldg(tw0 + (size_t)((j - 1) * 8 + ((r0 * j) & 7)) * bd + rb);
+        for (int j = 1; j < 8; j++) y += x[j] * (uint64_t)(int64_t)tws[(j - 1) * 8 + ((r0 * j) & 7)];
         ys[((size_t)r0 * 8 + q) * D + lane] = (int64_t)y;
     }
     __syncthreads();
 #pragma unroll
     for (int c1 = 0; c1 < 8; c1++) x[c1] = (uint64_t)ys[((size_t)q * 8 + c1) * D + lane];
-    const size_t i1 = (size_t)q * bd + rb, sub1 = 8 * (size_t)bd;
+    const int32_t *t1 = tws + 56 * (1 + q);
 #pragma unroll
     for (int r1 = 0; r1 < 8; r1++) {
         uint64_t z = x[0];
 #pragma unroll
-        for (int j = 1; j < 8; j++)
-            z += x[j] * (uint64_t)(int64_t)__ldg(tw1 + (size_t)((j - 1) * 8 + ((r1 * j) & 7)) * sub1 + i1);
+        for (int j = 1; j < 8; j++) z += x[j] * (uint64_t)(int64_t)t1[(j - 1) * 8 + ((r1 * j) & 7)];
         const size_t p = (size_t)(8 * r1 + q) * bd + rb;
         out[LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane] = (int64_t)z;
     }
@@ -449,9 +688,25 @@ zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8
         dim3 block(32, ngroups);
         dim3 grid((bd + 31) / 32, nch, nrows);
         size_t smem = (size_t)bl * 8;
+        // shared-memory staged variant: 64-row slices, 8 chunks per block
+        constexpr uint32_t TR3 = 64;
+        const size_t smem3 = (size_t)bl * TR3 * 4 + 256 * sizeof(uint4) + (size_t)kBase3Chunks * ngroups * bl;
+        const uint32_t threads3 = (TR3 / 8) * ngroups * kBase3Chunks;
+        const bool staged = packed && smem3 <= 200 * 1024 && threads3 <= 512;
         auto base_launch = [&](void *dst, bool final_out, bool lm) -> zg_status {
             ZG_KBEGIN(ctx, s, "k_base_bin");
-            if (packed) {
+            if (staged) {
+                dim3 g3((bd + TR3 - 1) / TR3, (nch + kBase3Chunks - 1) / kBase3Chunks, nrows);
+                ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
+                ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
+                ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
+                if (final_out && lm)
+                    k_base_bin3<TR3, true, true><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows);
+                else if (final_out)
+                    k_base_bin3<TR3, true, false><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows);
+                else
+                    k_base_bin3<TR3, false, false><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows);
+            } else if (packed) {
                 if (smem2 > 48 * 1024) {
                     ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
                     ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
@@ -482,11 +737,21 @@ zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8
         if (depth == 0) return base_launch(out_d, true, leaf_major);
         ZG_TRY(ctx->stage_a.ensure((size_t)nrows * C * D * 4));
         int32_t *base = ctx->stage_a.as<int32_t>();
-        ZG_TRY(base_launch(base, false, false));
+        const uint32_t blp = (bl + 31) / 32 * 32;
+        const size_t smem_m = (size_t)3 * kMmaRows * (blp + 16) + (size_t)kMmaPairs * blp * 8;
+        if (p->d_bmL && smem_m <= 200 * 1024) {
+            dim3 gm((bd + kMmaRows - 1) / kMmaRows, (nrows * nch + kMmaPairs - 1) / kMmaPairs);
+            ZG_CUDA(cudaFuncSetAttribute(k_base_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m));
+            ZG_KBEGIN(ctx, s, "k_base_bin");
+            k_base_mma<<<gm, 128, smem_m, s>>>(ev, p->d_bmL, base, L, bd, bl, blp, depth, nch, C, D, dmask, nrows);
+            ZG_KEND(ctx, s);
+        } else {
+            ZG_TRY(base_launch(base, false, false));
+        }
         if (depth == 2 && D * 8 <= 512) {
             // both stages in one kernel
             dim3 b2(D, 8), g2(bd, nrows);
-            const size_t sm = (size_t)64 * D * 8;
+            const size_t sm = (size_t)64 * D * 8 + 9 * 56 * 4;
             const int32_t *tw0 = p->d_tw + p->tw_dev_off[0], *tw1 = p->d_tw + p->tw_dev_off[1];
             int64_t *o = reinterpret_cast<int64_t *>(out_d);
             ZG_KBEGIN(ctx, s, "k_stages2_bin");

@@ -34,6 +34,52 @@ __global__ void __launch_bounds__(128) k_leaf_small(const uint8_t *__restrict__ 
     for (int i = 0; i < 8; i++) leaves[(size_t)j * 8 + i] = h[i];
 }
 
+// Leaves of at most one chunk whose size is a multiple of 16 bytes: each warp
+// hashes 32 leaves, one per lane.  For every 64-byte block the warp first
+// loads the 32 leaves' blocks with 16-byte loads (four lanes per leaf, so each
+// instruction reads eight 64-byte runs) into shared memory, then every lane
+// compresses its own leaf's block from there.
+__global__ void __launch_bounds__(128) k_leaf_small_coalesced(const uint8_t *__restrict__ cw,
+                                                              uint32_t width, uint32_t leaf_bytes,
+                                                              uint32_t *__restrict__ leaves) {
+    __shared__ uint32_t tile[4][32 * 17];  // per warp: 32 leaves x 16 words (+1 pad)
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t first = (blockIdx.x * 4 + warp) * 32;
+    uint32_t *t = tile[warp];
+    uint32_t cv[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) cv[i] = b3::iv(i);
+    const uint32_t nblocks = leaf_bytes == 0 ? 1 : (leaf_bytes + 63) / 64;
+    for (uint32_t blk = 0; blk < nblocks; blk++) {
+#pragma unroll
+        for (int it = 0; it < 4; it++) {
+            const uint32_t l = it * 8 + lane / 4, piece = lane & 3;
+            const uint32_t off = 64 * blk + 16 * piece;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (first + l < width && off < leaf_bytes)
+                v = __ldg(reinterpret_cast<const uint4 *>(cw + (size_t)(first + l) * leaf_bytes + off));
+            uint32_t *d = t + l * 17 + 4 * piece;
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            d[3] = v.w;
+        }
+        __syncwarp();
+        uint32_t m[16];
+#pragma unroll
+        for (int w = 0; w < 16; w++) m[w] = t[lane * 17 + w];
+        __syncwarp();
+        const uint32_t blen = (blk + 1 < nblocks) ? 64u : leaf_bytes - 64u * blk;
+        const uint32_t flags = (blk == 0 ? b3::CHUNK_START : 0u) |
+                               (blk + 1 == nblocks ? (b3::CHUNK_END | b3::ROOT) : 0u);
+        b3::compress_cv(cv, m, 0, blen, flags);
+    }
+    if (first + lane < width) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) leaves[(size_t)(first + lane) * 8 + i] = cv[i];
+    }
+}
+
 // Chunk chaining values of long leaves: one thread per (leaf, chunk).
 __global__ void __launch_bounds__(128) k_leaf_chunks(const uint8_t *__restrict__ cw, uint32_t width,
                                                      uint32_t leaf_bytes, uint32_t nchunks,
@@ -154,7 +200,10 @@ zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uin
     uint32_t *leaves = reinterpret_cast<uint32_t *>(leaves_d);
     if (leaf_bytes <= b3::CHUNK_LEN) {
         ZG_KBEGIN(ctx, s, "k_leaf_small");
-        k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves);
+        if (leaf_bytes % 16 == 0 && leaf_bytes > 0)
+            k_leaf_small_coalesced<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves);
+        else
+            k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves);
         ZG_KEND(ctx, s);
         return ZG_OK;
     }

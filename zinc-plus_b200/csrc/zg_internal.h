@@ -135,6 +135,7 @@ struct zg_params {
     std::vector<int64_t> tw;  // stage k: (base_dim*8^k) x 7 x 8, stages back to back
     int32_t *d_bmT = nullptr; // base_len x base_dim (transposed)
     int32_t *d_bmP = nullptr; // base_len x round_up(base_dim, 8) (transposed, zero padded)
+    uint8_t *d_bmL = nullptr; // [3][base_dim][round_up(base_len, 32)] u8 limbs of the base matrix
     int32_t *d_tw = nullptr;  // stage k: [56][sub_k], stages back to back
     std::vector<size_t> tw_off;      // offset of each stage in tw (host, [i][j-1][t])
     std::vector<size_t> tw_dev_off;  // offset of each stage in d_tw (device, [56][sub])
@@ -184,8 +185,11 @@ void stdrng_shuffle_identity(uint64_t seed, uint32_t n, uint32_t *perm);
 
 // ---------------------------------------------------------- pipelines
 zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **out);
+// tail_out: when not NULL, the proof after the b rows (combined row and column
+// openings) is written there instead of being appended to t->stream.
 zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
-                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out);
+                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
+                       uint8_t *tail_out);
 zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
                       const uint8_t *eval, const uint8_t *proof, size_t proof_len);
 
