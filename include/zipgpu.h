@@ -208,6 +208,20 @@ zg_status zg_commit_prove(zg_params *p, const void *const *polys, uint32_t batch
 zg_status zg_commit_prove_d(zg_params *p, const void *polys_d, uint32_t batch,
                             const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
                             uint8_t *proof, size_t *proof_len);
+/* Batched form: n independent requests, each one commit_single +
+ * new_from_commitment + get_random_field_cfg + prove of one polynomial at its
+ * own point, spread over `lanes` concurrent lanes (each a CUDA stream with its
+ * own scratch, driven by its own host thread, so one lane's Fiat-Shamir work
+ * overlaps the others' kernels).  Every output is byte-identical to a
+ * sequential zg_commit_prove of the same request.  polys[i]: 2^num_vars
+ * evaluations in host memory, or in device memory when polys_on_device != 0.
+ * points: n x num_vars i128.  roots: n x 32; evals: n x 8*field_limbs bytes;
+ * proofs[i]: buffer of proof_lens[i] bytes (in: capacity, out: size).
+ * latency_ms (may be NULL): per-request service time. */
+zg_status zg_commit_prove_many(zg_params *p, uint32_t n, const void *const *polys,
+                               int polys_on_device, const uint8_t *points, uint8_t *roots,
+                               uint8_t *evals, uint8_t *const *proofs, size_t *proof_lens,
+                               uint32_t lanes, double *latency_ms);
 /* Exact proof length for a batch (phase_commit.rs:739-805 formula). */
 size_t zg_proof_size(const zg_params *p, uint32_t batch);
 

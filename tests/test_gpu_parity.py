@@ -162,3 +162,19 @@ def test_large_commit_prove_verifies(zipgpu, ctx, rng, nv):
     root, inner, proof = zipgpu.ZipPlus.commit_prove(pp, [ev], point)
     zipgpu.ZipPlus.verify(pp, zipgpu.ZipPlusCommitment(root, 1), point, inner, proof)
     assert len(proof) == pp.proof_size(1)
+
+
+@pytest.mark.parametrize("lanes", [1, 3, 4])
+def test_commit_prove_many_equals_sequential(zipgpu, oracle, ctx, rng, lanes):
+    """The batched, multi-lane form returns for every request exactly the bytes
+    of a single commit_prove of that request (and of the oracle)."""
+    nv, D, L = 12, 32, 1024
+    pp = params_for(zipgpu, 1, D, 0, nv, L, ctx=ctx)
+    polys = [binary_evals(rng, 1 << nv, D) for _ in range(7)]
+    points = [[(i + 3) * (j + 1) - 5 for j in range(nv)] for i in range(7)]
+    got = zipgpu.ZipPlus.commit_prove_many(pp, polys, points, lanes=lanes)
+    desc = desc_for(1, D, 0, nv, L)
+    for i, (root, ev, proof) in enumerate(got):
+        assert (root, ev, proof) == zipgpu.ZipPlus.commit_prove(pp, [polys[i]], points[i])
+        ro, po, eo, _ = oracle.commit_prove(desc, polys[i], 1, points[i])
+        assert (root, ev, proof) == (ro, eo, po)

@@ -2,8 +2,10 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
+#include <thread>
 
 #include "zg_internal.h"
 #include "zg_prove.h"
@@ -204,9 +206,10 @@ bool merkle_verify(const uint8_t root[32], const uint8_t *col, size_t col_len, u
 namespace zg {
 
 // ------------------------------------------------------------------- commit
-zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **out) {
+zg_status commit_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t batch,
+                        zg_hint **out) {
     ZG_TRY(validate_budget(p, batch));
-    zg_ctx *ctx = p->ctx;
+    zg_ctx *ctx = lane;
     cudaStream_t s = ctx->stream;
     const uint32_t C = p->info.codeword_len;
     const uint32_t nrows = batch * p->info.num_rows;
@@ -217,6 +220,7 @@ zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hi
     }
     std::unique_ptr<zg_hint> h(new zg_hint());
     h->params = p;
+    h->lane = ctx;
     h->batch = batch;
     h->nrows = nrows;
     h->depth = ilog2u(C);
@@ -232,7 +236,7 @@ zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hi
         h->block = nullptr;
         return st;
     };
-    zg_status st = launch_encode(p, polys_d, nrows, h->d_cw, true, s);
+    zg_status st = launch_encode(p, ctx, polys_d, nrows, h->d_cw, true, s);
     if (st != ZG_OK) return fail(st);
     st = launch_leaf_hash(ctx, h->d_cw, C, (uint32_t)leaf_bytes, h->d_tree, s);
     if (st != ZG_OK) return fail(st);
@@ -253,8 +257,8 @@ zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hi
 }
 
 // -------------------------------------------------------------------- prove
-zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
-                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
+zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void *polys_d,
+                       uint32_t batch, const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
                        uint8_t *tail_out) {
     if (!t->has_field || t->f.L != (int)p->d.field_limbs) {
         set_error("transcript has no field configuration of %u limbs (sample it first)",
@@ -266,7 +270,7 @@ zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint
         return ZG_ERR_INVALID_PARAM;
     }
     ZG_TRY(validate_budget(p, batch));
-    zg_ctx *ctx = p->ctx;
+    zg_ctx *ctx = lane;
     cudaStream_t s = ctx->stream;
     const FieldCfg &f = t->f;
     const int L = f.L;
@@ -415,7 +419,7 @@ zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, cons
     tr_absorb_slice(&tr, root, 32);
     const int L = (int)p->d.field_limbs;
     uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
-    tr_get_prime(&tr, L, prime);
+    tr_get_prime(&tr, L, prime, 0);
     field_cfg_init(tr.f, prime, L);
     tr.has_field = true;
     const FieldCfg &f = tr.f;
@@ -589,6 +593,8 @@ zg_status zg_ctx_create(int device, zg_ctx **out) {
 
 zg_status zg_ctx_destroy(zg_ctx *ctx) {
     if (!ctx) return ZG_OK;
+    for (zg_ctx *l : ctx->lanes) zg_ctx_destroy(l);
+    ctx->lanes.clear();
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
@@ -604,7 +610,12 @@ zg_status zg_ctx_destroy(zg_ctx *ctx) {
     return ZG_OK;
 }
 
-uint64_t zg_ctx_kernel_launches(const zg_ctx *ctx) { return ctx ? ctx->launches : 0; }
+uint64_t zg_ctx_kernel_launches(const zg_ctx *ctx) {
+    if (!ctx) return 0;
+    uint64_t n = ctx->launches;
+    for (const zg_ctx *l : ctx->lanes) n += l->launches;
+    return n;
+}
 
 zg_status zg_ctx_set_kernel_timing(zg_ctx *ctx, int enable) {
     if (!ctx) return ZG_ERR_INVALID_PARAM;
@@ -814,7 +825,7 @@ static zg_status encode_rows_impl(zg_params *p, const void *evals, void *cw_out)
     DevBuf outb;
     ZG_TRY(outb.ensure(out_bytes));
     ZG_CUDA(cudaMemcpyAsync(ctx->evals.ptr, evals, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
-    zg_status st = launch_encode(p, ctx->evals.ptr, I.num_rows, outb.as<uint8_t>(), false, ctx->stream);
+    zg_status st = launch_encode(p, ctx, ctx->evals.ptr, I.num_rows, outb.as<uint8_t>(), false, ctx->stream);
     if (st == ZG_OK) {
         cudaError_t e = cudaMemcpyAsync(cw_out, outb.ptr, out_bytes, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -837,7 +848,7 @@ zg_status zg_encode_rows_d(zg_params *p, const void *evals_d, void *cw_out_d, vo
     std::lock_guard<std::mutex> lk(p->ctx->mu);
     ZG_CUDA(cudaSetDevice(p->ctx->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : p->ctx->stream;
-    ZG_GUARD(launch_encode(p, evals_d, p->info.num_rows, static_cast<uint8_t *>(cw_out_d), false, s));
+    ZG_GUARD(launch_encode(p, p->ctx, evals_d, p->info.num_rows, static_cast<uint8_t *>(cw_out_d), false, s));
 }
 
 zg_status zg_encode_wide(zg_params *p, const uint64_t *row, uint32_t limbs, uint64_t *out) {
@@ -904,9 +915,8 @@ zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_
     ZG_GUARD(merkle_root_impl(ctx, rows, n_rows, width, elem_bytes, root));
 }
 
-static zg_status stage_polys(zg_params *p, const void *const *polys, uint32_t batch) {
+static zg_status stage_polys(zg_params *p, zg_ctx *ctx, const void *const *polys, uint32_t batch) {
     if (!polys) return ZG_ERR_INVALID_PARAM;
-    zg_ctx *ctx = p->ctx;
     const size_t pb = (size_t)p->info.num_rows * p->info.row_len * p->info.eval_bytes;
     ZG_TRY(ctx->evals.ensure(pb * batch));
     for (uint32_t b = 0; b < batch; b++) {
@@ -927,8 +937,8 @@ static zg_status commit_impl(zg_params *p, const void *const *polys, uint32_t ba
         set_error("Batch must contain at least one polynomial");
         return ZG_ERR_INVALID_PARAM;
     }
-    ZG_TRY(stage_polys(p, polys, batch));
-    ZG_TRY(commit_device(p, p->ctx->evals.ptr, batch, hint));
+    ZG_TRY(stage_polys(p, p->ctx, polys, batch));
+    ZG_TRY(commit_device(p, p->ctx, p->ctx->evals.ptr, batch, hint));
     std::memcpy(root, (*hint)->root, 32);
     return ZG_OK;
 }
@@ -944,7 +954,7 @@ static zg_status commit_d_impl(zg_params *p, const void *polys_d, uint32_t batch
     ZG_TRY(need_device(p));
     std::lock_guard<std::mutex> lk(p->ctx->mu);
     ZG_CUDA(cudaSetDevice(p->ctx->device));
-    ZG_TRY(commit_device(p, polys_d, batch, hint));
+    ZG_TRY(commit_device(p, p->ctx, polys_d, batch, hint));
     std::memcpy(root, (*hint)->root, 32);
     return ZG_OK;
 }
@@ -957,7 +967,7 @@ zg_status zg_commit_d(zg_params *p, const void *polys_d, uint32_t batch, zg_hint
 zg_status zg_hint_free(zg_hint *h) {
     if (!h) return ZG_OK;
     // the block returns to the context's cache (freed by zg_ctx_destroy)
-    if (h->block) ctx_release(h->params->ctx, h->block, h->block_bytes);
+    if (h->block) ctx_release(h->lane, h->block, h->block_bytes);
     delete h;
     return ZG_OK;
 }
@@ -1020,7 +1030,7 @@ zg_status zg_transcript_challenge(zg_transcript *t, uint8_t *out, size_t n) {
 zg_status zg_transcript_sample_field(zg_transcript *t, uint32_t limbs, uint8_t *modulus_out) {
     if (!t || (limbs != 3 && limbs != 4)) return ZG_ERR_INVALID_PARAM;
     uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
-    tr_get_prime(t, (int)limbs, prime);
+    tr_get_prime(t, (int)limbs, prime, 0);
     field_cfg_init(t->f, prime, (int)limbs);
     t->has_field = true;
     if (modulus_out) std::memcpy(modulus_out, prime, 8 * limbs);
@@ -1045,8 +1055,8 @@ static zg_status prove_impl(zg_params *p, zg_transcript *t, const void *const *p
         set_error("Batch must contain at least one polynomial");
         return ZG_ERR_INVALID_PARAM;
     }
-    ZG_TRY(stage_polys(p, polys, batch));
-    return prove_device(p, t, p->ctx->evals.ptr, batch, point, hint, eval_out, nullptr);
+    ZG_TRY(stage_polys(p, p->ctx, polys, batch));
+    return prove_device(p, p->ctx, t, p->ctx->evals.ptr, batch, point, hint, eval_out, nullptr);
 }
 
 zg_status zg_prove(zg_params *p, zg_transcript *t, const void *const *polys, uint32_t batch,
@@ -1060,7 +1070,7 @@ static zg_status prove_d_impl(zg_params *p, zg_transcript *t, const void *polys_
     ZG_TRY(need_device(p));
     std::lock_guard<std::mutex> lk(p->ctx->mu);
     ZG_CUDA(cudaSetDevice(p->ctx->device));
-    return prove_device(p, t, polys_d, batch, point, hint, eval_out, nullptr);
+    return prove_device(p, p->ctx, t, polys_d, batch, point, hint, eval_out, nullptr);
 }
 
 zg_status zg_prove_d(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
@@ -1076,9 +1086,10 @@ size_t zg_proof_size(const zg_params *p, uint32_t batch) {
            (size_t)p->d.num_openings * ((size_t)batch * I.num_rows * I.cw_bytes + 24 + 32 * depth);
 }
 
-static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t batch,
-                                     const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
-                                     uint8_t *proof, size_t *proof_len) {
+static zg_status commit_prove_common(zg_params *p, zg_ctx *lane, const void *polys_d,
+                                     uint32_t batch, const uint8_t *point, uint8_t root[32],
+                                     uint8_t *eval_out, uint8_t *proof, size_t *proof_len,
+                                     int prime_threads) {
     const size_t need = zg_proof_size(p, batch);
     if (*proof_len < need) {
         *proof_len = need;
@@ -1086,20 +1097,20 @@ static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t
         return ZG_ERR_BUFFER_TOO_SMALL;
     }
     zg_hint *h = nullptr;
-    hphase_start(p->ctx);
-    ZG_TRY(commit_device(p, polys_d, batch, &h));
+    hphase_start(lane);
+    ZG_TRY(commit_device(p, lane, polys_d, batch, &h));
     std::memcpy(root, h->root, 32);
     zg_transcript t;
     tr_absorb_slice(&t, h->root, 32);
     uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
-    tr_get_prime(&t, (int)p->d.field_limbs, prime);
+    tr_get_prime(&t, (int)p->d.field_limbs, prime, prime_threads);
     field_cfg_init(t.f, prime, (int)p->d.field_limbs);
     t.has_field = true;
-    hphase(p->ctx, "prime");
+    hphase(lane, "prime");
     // The b rows are written to the transcript stream; the rest of the proof
     // lands directly after them in the caller's buffer.
     const size_t head = (size_t)p->info.num_rows * 2 * p->info.field_bytes;
-    zg_status st = prove_device(p, &t, polys_d, batch, point, h, eval_out, proof + head);
+    zg_status st = prove_device(p, lane, &t, polys_d, batch, point, h, eval_out, proof + head);
     zg_hint_free(h);
     if (st != ZG_OK) return st;
     if (t.stream.size() != head) {
@@ -1108,7 +1119,7 @@ static zg_status commit_prove_common(zg_params *p, const void *polys_d, uint32_t
     }
     std::memcpy(proof, t.stream.data(), head);
     *proof_len = need;
-    hphase(p->ctx, "proof_copy");
+    hphase(lane, "proof_copy");
     return ZG_OK;
 }
 
@@ -1123,8 +1134,9 @@ static zg_status commit_prove_impl(zg_params *p, const void *const *polys, uint3
         set_error("Batch must contain at least one polynomial");
         return ZG_ERR_INVALID_PARAM;
     }
-    ZG_TRY(stage_polys(p, polys, batch));
-    return commit_prove_common(p, p->ctx->evals.ptr, batch, point, root, eval_out, proof, proof_len);
+    ZG_TRY(stage_polys(p, p->ctx, polys, batch));
+    return commit_prove_common(p, p->ctx, p->ctx->evals.ptr, batch, point, root, eval_out, proof,
+                               proof_len, 0);
 }
 
 zg_status zg_commit_prove(zg_params *p, const void *const *polys, uint32_t batch,
@@ -1140,13 +1152,86 @@ static zg_status commit_prove_d_impl(zg_params *p, const void *polys_d, uint32_t
     ZG_TRY(need_device(p));
     std::lock_guard<std::mutex> lk(p->ctx->mu);
     ZG_CUDA(cudaSetDevice(p->ctx->device));
-    return commit_prove_common(p, polys_d, batch, point, root, eval_out, proof, proof_len);
+    return commit_prove_common(p, p->ctx, polys_d, batch, point, root, eval_out, proof, proof_len,
+                               0);
 }
 
 zg_status zg_commit_prove_d(zg_params *p, const void *polys_d, uint32_t batch,
                             const uint8_t *point, uint8_t root[32], uint8_t *eval_out,
                             uint8_t *proof, size_t *proof_len) {
     ZG_GUARD(commit_prove_d_impl(p, polys_d, batch, point, root, eval_out, proof, proof_len));
+}
+
+static zg_status commit_prove_many_impl(zg_params *p, uint32_t n, const void *const *polys,
+                                        int on_device, const uint8_t *points, uint8_t *roots,
+                                        uint8_t *evals, uint8_t *const *proofs, size_t *proof_lens,
+                                        uint32_t nlanes, double *latency_ms) {
+    if (!p || !polys || !points || !roots || !evals || !proofs || !proof_lens || n == 0)
+        return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    zg_ctx *ctx = p->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    nlanes = std::max<uint32_t>(1, std::min<uint32_t>({nlanes, n, 16}));
+    while (ctx->lanes.size() < nlanes) {
+        zg_ctx *l = nullptr;
+        ZG_TRY(zg_ctx_create(ctx->device, &l));
+        ctx->lanes.push_back(l);
+    }
+    const int cores = std::max(1, omp_get_num_procs());
+    const int per_lane = std::max(1, cores / (int)nlanes);
+    const size_t pt_bytes = 16 * (size_t)p->d.num_vars, fb = 8 * (size_t)p->d.field_limbs;
+    std::atomic<uint32_t> next{0};
+    std::atomic<bool> failed{false};
+    std::mutex err_mu;
+    zg_status first_st = ZG_OK;
+    std::string first_msg;
+    auto worker = [&](uint32_t li) {
+        cudaSetDevice(ctx->device);
+        zg_ctx *lane = ctx->lanes[li];
+        for (;;) {
+            const uint32_t i = next.fetch_add(1);
+            if (i >= n || failed.load()) break;
+            const auto t0 = std::chrono::steady_clock::now();
+            zg_status st = ZG_OK;
+            const void *pd = polys[i];
+            if (!on_device) {
+                st = stage_polys(p, lane, &polys[i], 1);
+                pd = lane->evals.ptr;
+            }
+            if (st == ZG_OK) {
+                size_t plen = proof_lens[i];
+                st = commit_prove_common(p, lane, pd, 1, points + pt_bytes * i, roots + 32 * (size_t)i,
+                                         evals + fb * i, proofs[i], &plen, per_lane);
+                proof_lens[i] = plen;
+            }
+            if (st != ZG_OK) {
+                std::lock_guard<std::mutex> g(err_mu);
+                if (first_st == ZG_OK) {
+                    first_st = st;
+                    first_msg = last_error();
+                }
+                failed.store(true);
+                break;
+            }
+            if (latency_ms)
+                latency_ms[i] = std::chrono::duration<double, std::milli>(
+                                    std::chrono::steady_clock::now() - t0).count();
+        }
+    };
+    std::vector<std::thread> th;
+    for (uint32_t li = 0; li < nlanes; li++) th.emplace_back(worker, li);
+    for (auto &t : th) t.join();
+    if (first_st != ZG_OK) set_error("%s", first_msg.c_str());
+    return first_st;
+}
+
+zg_status zg_commit_prove_many(zg_params *p, uint32_t n, const void *const *polys,
+                               int polys_on_device, const uint8_t *points, uint8_t *roots,
+                               uint8_t *evals, uint8_t *const *proofs, size_t *proof_lens,
+                               uint32_t lanes, double *latency_ms) {
+    ZG_GUARD(commit_prove_many_impl(p, n, polys, polys_on_device, points, roots, evals, proofs,
+                                    proof_lens, lanes, latency_ms));
 }
 
 zg_status zg_verify(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,

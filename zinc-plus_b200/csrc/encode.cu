@@ -632,9 +632,13 @@ __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__
 // ---------------------------------------------------------------------------
 static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
-zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8_t *out_d,
-                        bool leaf_major, cudaStream_t s) {
-    zg_ctx *ctx = p->ctx;
+zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_t nrows,
+                        uint8_t *out_d, bool leaf_major, cudaStream_t s) {
+    zg_ctx *ctx = lane;
+    if (nrows > 65535) {
+        set_error("too many codeword rows (%u) for one launch", nrows);
+        return ZG_ERR_INVALID_PARAM;
+    }
     const zg_params_info &I = p->info;
     const uint32_t C = I.codeword_len, L = I.row_len, D = p->D;
     const uint64_t dmask = D >= 64 ? ~0ull : ((1ull << D) - 1);

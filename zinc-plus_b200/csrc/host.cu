@@ -267,9 +267,11 @@ bool is_probable_prime_base2(const uint64_t *n, int L) {
 // are generated ahead in groups and tested in parallel; the transcript is
 // then rewound to the state right after the accepted candidate, so the result
 // and the transcript state equal the sequential loop's.
-void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out) {
+void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads) {
     const int nb = 8 * L;
-    int group = std::max(32, 2 * omp_get_max_threads());
+    const int team = threads > 0 ? threads : omp_get_max_threads();
+    // candidates generated ahead per round (speculative; a single thread tests one at a time)
+    const int group = team == 1 ? 1 : std::max(8, 2 * team);
     std::vector<b3::Hasher> states(group);
     std::vector<uint64_t> cand((size_t)group * 4);
     std::vector<char> ok(group);
@@ -284,7 +286,7 @@ void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out) {
             std::memset(c, 0, 32);
             std::memcpy(c, buf, nb);
         }
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(team)
         for (int g = 0; g < group; g++) {
             uint64_t *c = &cand[(size_t)g * 4];
             bool zero = true;

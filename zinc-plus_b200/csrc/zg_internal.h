@@ -123,6 +123,8 @@ struct zg_ctx {
     // the request path); released by zg_ctx_destroy.
     std::mutex cache_mu;
     std::multimap<size_t, void *> cache;
+    // child contexts (same device) used as concurrent lanes by batched calls
+    std::vector<zg_ctx *> lanes;
 };
 
 struct zg_params {
@@ -146,6 +148,7 @@ struct zg_params {
 
 struct zg_hint {
     zg_params *params = nullptr;
+    zg_ctx *lane = nullptr;    // context whose block cache owns `block`
     uint32_t batch = 0;
     uint32_t nrows = 0;        // batch * num_rows
     void *block = nullptr;     // one cached device block holding both arrays
@@ -174,7 +177,8 @@ i128 tr_challenge_i128(zg_transcript *t);
 uint32_t tr_challenge_u32(zg_transcript *t);
 void tr_absorb_field(zg_transcript *t, const uint64_t *inner);
 // get_prime::<Uint<L>, MillerRabin> (transcript/src/lib.rs:58-72).
-void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out);
+// threads: 0 = the OpenMP default team.
+void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads);
 bool is_probable_prime_base2(const uint64_t *n, int L);
 
 // IPRS parameters (params.rs:59-196); returns false if the reference rejects.
@@ -184,19 +188,21 @@ uint32_t iprs_optimal_depth(uint32_t row_len);
 void stdrng_shuffle_identity(uint64_t seed, uint32_t n, uint32_t *perm);
 
 // ---------------------------------------------------------- pipelines
-zg_status commit_device(zg_params *p, const void *polys_d, uint32_t batch, zg_hint **out);
+// `lane` supplies the stream, scratch and pinned buffers (a zg_ctx on p's device).
+zg_status commit_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t batch,
+                        zg_hint **out);
 // tail_out: when not NULL, the proof after the b rows (combined row and column
 // openings) is written there instead of being appended to t->stream.
-zg_status prove_device(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
-                       const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
+zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void *polys_d,
+                       uint32_t batch, const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
                        uint8_t *tail_out);
 zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
                       const uint8_t *eval, const uint8_t *proof, size_t proof_len);
 
 // ------------------------------------------------------------- kernels
 // (defined in the .cu files; all launched on the given stream)
-zg_status launch_encode(zg_params *p, const void *evals_d, uint32_t nrows, uint8_t *out_d,
-                        bool leaf_major, cudaStream_t s);
+zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_t nrows,
+                        uint8_t *out_d, bool leaf_major, cudaStream_t s);
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
                            uint8_t *leaves_d, cudaStream_t s);
 zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s);

@@ -45,7 +45,7 @@ EXPORTS = (
     "zg_hint_batch", "zg_hint_codeword", "zg_transcript_new", "zg_transcript_free",
     "zg_transcript_absorb", "zg_transcript_absorb_slice", "zg_transcript_challenge",
     "zg_transcript_sample_field", "zg_transcript_proof", "zg_prove", "zg_prove_d",
-    "zg_commit_prove", "zg_commit_prove_d", "zg_proof_size", "zg_verify",
+    "zg_commit_prove", "zg_commit_prove_d", "zg_commit_prove_many", "zg_proof_size", "zg_verify",
 )
 
 
@@ -108,6 +108,7 @@ def lib() -> C.CDLL:
         "zg_prove_d": ([vp, vp, vp, u32, vp, vp, vp], st),
         "zg_commit_prove": ([vp, vp, u32, vp, vp, vp, vp, C.POINTER(sz)], st),
         "zg_commit_prove_d": ([vp, vp, u32, vp, vp, vp, vp, C.POINTER(sz)], st),
+        "zg_commit_prove_many": ([vp, u32, vp, C.c_int, vp, vp, vp, vp, vp, u32, vp], st),
         "zg_proof_size": ([vp, u32], sz),
         "zg_verify": ([vp, vp, u32, vp, vp, vp, sz], st),
     }
@@ -456,6 +457,26 @@ class ZipPlus:
         check(lib().zg_commit_prove(pp.handle, ptrs, len(polys), C.c_char_p(pt), root, ev, proof,
                                     C.byref(cap)))
         return root.raw, ev.raw, proof.raw[: cap.value]
+
+    @staticmethod
+    def commit_prove_many(pp: ZipPlusParams, polys, points, lanes: int = 4):
+        """Batched commit+prove of independent polynomials (one per request);
+        returns [(root, eval, proof)] identical to sequential commit_prove."""
+        n = len(polys)
+        arrs = [np.ascontiguousarray(p, dtype=pp.eval_dtype) for p in polys]
+        ptrs = (C.c_void_p * n)(*[a.ctypes.data for a in arrs])
+        pts = b"".join(i128_bytes(pt) for pt in points)
+        cap = pp.proof_size(1)
+        bufs = [C.create_string_buffer(cap) for _ in range(n)]
+        bptrs = (C.c_void_p * n)(*[C.addressof(b) for b in bufs])
+        lens = (C.c_size_t * n)(*([cap] * n))
+        roots = C.create_string_buffer(32 * n)
+        fb = 8 * pp.zt.field_limbs
+        evs = C.create_string_buffer(fb * n)
+        check(lib().zg_commit_prove_many(pp.handle, n, ptrs, 0, C.c_char_p(pts), roots, evs, bptrs,
+                                         lens, lanes, None))
+        return [(roots.raw[32 * i:32 * i + 32], evs.raw[fb * i:fb * i + fb],
+                 bufs[i].raw[: lens[i]]) for i in range(n)]
 
     @staticmethod
     def verify(pp: ZipPlusParams, comm: ZipPlusCommitment, point: Sequence[int], eval_inner: bytes,
