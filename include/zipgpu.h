@@ -232,6 +232,47 @@ size_t zg_proof_size(const zg_params *p, uint32_t batch);
 zg_status zg_verify(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
                     const uint8_t *eval, const uint8_t *proof, size_t proof_len);
 
+/* ---- PIOP sumcheck prover ----------------------------------------------------
+ * One group of MLEs with the combination function
+ *   comb(v) = sum_k coeffs[k] * prod_{q in [offsets[k], offsets[k+1])} v[indices[q]],
+ * i.e. the `comb_fn: Fn(&[F]) -> F` of MLSumcheck::prove_as_subprotocol
+ * (piop/src/sumcheck.rs:163-215) and of MultiDegreeSumcheckGroup
+ * (piop/src/sumcheck/multi_degree.rs:44-67) written as a sum of products.
+ * mles: n_mles x 2^nvars field elements, Montgomery inner values of `limbs`
+ * u64 each (DenseMultilinearExtension<F::Inner>), MLE-major; coeffs:
+ * n_products Montgomery inners; offsets: n_products + 1 entries. */
+typedef struct {
+    uint32_t degree;     /* the group's degree (max product length), <= 8 */
+    uint32_t n_mles;
+    uint32_t n_products;
+    const void *mles;    /* host, or device memory when mles_on_device != 0 */
+    const uint64_t *coeffs;
+    const uint32_t *offsets;
+    const uint32_t *indices;
+} zg_sumcheck_group;
+
+/* multi == 0: MLSumcheck::prove_as_subprotocol with one group; the proof is the
+ * transcription of SumcheckProof (piop/src/sumcheck.rs:35-111).
+ * multi != 0: MultiDegreeSumcheck::prove_as_subprotocol
+ * (piop/src/sumcheck/multi_degree.rs:259-355), one shared challenge per round;
+ * the proof is the transcription of MultiDegreeSumcheckProof
+ * (multi_degree.rs:86-190).  modulus: `limbs` u64 LE (3 or 4), odd.  The round
+ * messages and challenges go through `t` (the reference's Blake3Transcript).
+ * proof_len: in capacity, out size (ZG_ERR_BUFFER_TOO_SMALL sets the size).
+ * point_out (may be NULL): nvars challenges; finals_out (may be NULL): every
+ * MLE of every group evaluated at the point (ProverState::randomness and the
+ * final fold of prover.rs:95-247), in group order. */
+zg_status zg_sumcheck_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                            uint32_t nvars, int multi, const zg_sumcheck_group *groups,
+                            uint32_t ngroups, int mles_on_device, uint8_t *proof,
+                            size_t *proof_len, uint64_t *point_out, uint64_t *finals_out);
+
+/* sum_x mle[x] * eq(x, point) (mle_eval_with_eq_table, poly/src/utils.rs:267-284):
+ * the MLE (2^nvars Montgomery inners, host memory) at `point` (nvars inners,
+ * bit k of x pairs with point[k]). */
+zg_status zg_mle_evaluate(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs, const uint64_t *mle,
+                          uint32_t nvars, const uint64_t *point, uint64_t *out);
+
 #ifdef __cplusplus
 }
 #endif

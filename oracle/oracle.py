@@ -36,6 +36,14 @@ class Desc(C.Structure):
     ]
 
 
+class ScGroup(C.Structure):
+    """Mirror of ``zr_sc_group`` (same layout as the product's ``zg_sumcheck_group``)."""
+
+    _fields_ = [("degree", C.c_uint32), ("n_mles", C.c_uint32), ("n_products", C.c_uint32),
+                ("mles", C.c_void_p), ("coeffs", C.c_void_p), ("offsets", C.c_void_p),
+                ("indices", C.c_void_p)]
+
+
 def build() -> str:
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
@@ -88,6 +96,13 @@ def lib():
         L.zr_tr_get_prime.argtypes = [vp, C.c_uint32, vp]
         L.zr_is_probable_prime_base2.argtypes = [vp, C.c_uint32]
         L.zr_set_threads.argtypes = [C.c_int]
+        gp = C.POINTER(ScGroup)
+        L.zr_sumcheck_prove.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_int, gp, C.c_uint32,
+                                        vp, sz, C.POINTER(C.c_size_t), vp, vp]
+        L.zr_sumcheck_verify.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_int, vp, C.c_uint32,
+                                         vp, sz, vp, vp]
+        L.zr_sumcheck_comb.argtypes = [vp, C.c_uint32, gp, vp, vp]
+        L.zr_mle_evaluate.argtypes = [vp, C.c_uint32, vp, C.c_uint32, vp, vp]
         _lib = L
     return _lib
 
@@ -297,3 +312,77 @@ class Transcript:
 def is_probable_prime_base2(n: int, limbs: int = 4) -> bool:
     arr = np.array([(n >> (64 * i)) & ((1 << 64) - 1) for i in range(limbs)], np.uint64)
     return bool(lib().zr_is_probable_prime_base2(_ptr(arr), limbs))
+
+
+# ------------------------------------------------------------------ sumcheck
+def _limbs(x: int, L: int) -> np.ndarray:
+    return np.array([(x >> (64 * i)) & ((1 << 64) - 1) for i in range(L)], np.uint64)
+
+
+def _sc_groups(groups, L):
+    """groups: list of (degree, mles (K, 2^n, L) uint64, [(coeff_inner, [idx...]), ...])."""
+    keep, arr = [], (ScGroup * len(groups))()
+    for g, (deg, mles, prods) in zip(arr, groups):
+        mles = np.ascontiguousarray(mles, dtype=np.uint64)
+        coeffs = np.zeros((max(len(prods), 1), L), np.uint64)
+        offsets = np.zeros(len(prods) + 1, np.uint32)
+        idx = []
+        for k, (c, ids) in enumerate(prods):
+            coeffs[k] = _limbs(int(c), L)
+            idx.extend(int(i) for i in ids)
+            offsets[k + 1] = len(idx)
+        indices = np.array(idx or [0], np.uint32)
+        keep += [mles, coeffs, offsets, indices]
+        g.degree, g.n_mles, g.n_products = deg, mles.shape[0], len(prods)
+        g.mles, g.coeffs = mles.ctypes.data, coeffs.ctypes.data
+        g.offsets, g.indices = offsets.ctypes.data, indices.ctypes.data
+    return arr, keep
+
+
+def sumcheck_prove(t: Transcript, modulus: int, L: int, nvars: int, groups, multi: bool):
+    """MLSumcheck / MultiDegreeSumcheck prove_as_subprotocol restated; returns
+    (proof bytes, point (nvars, L), finals (total MLEs, L))."""
+    arr, keep = _sc_groups(groups, L)
+    fb = 8 * L
+    cap = fb + 8 + 4 * len(groups) + fb * len(groups) + sum(nvars * (fb * g[0] + 4) for g in groups)
+    proof = C.create_string_buffer(cap)
+    plen = C.c_size_t(0)
+    point = np.zeros((nvars, L), np.uint64)
+    nm = sum(np.asarray(g[1]).shape[0] for g in groups)
+    finals = np.zeros((max(nm, 1), L), np.uint64)
+    mod = _limbs(modulus, L)
+    rc = lib().zr_sumcheck_prove(t._t, _ptr(mod), L, nvars, int(multi), arr, len(groups), proof,
+                                 cap, C.byref(plen), _ptr(point), _ptr(finals))
+    if rc != 0:
+        raise ValueError(f"zr_sumcheck_prove failed ({rc})")
+    return proof.raw[: plen.value], point, finals[:nm]
+
+
+def sumcheck_verify(t: Transcript, modulus: int, L: int, nvars: int, degrees, proof: bytes,
+                    multi: bool):
+    """Returns (rc, point, expected evaluations per group); rc 0 = well formed."""
+    deg = np.array(list(degrees), np.uint32)
+    point = np.zeros((nvars, L), np.uint64)
+    expected = np.zeros((len(deg), L), np.uint64)
+    mod = _limbs(modulus, L)
+    rc = lib().zr_sumcheck_verify(t._t, _ptr(mod), L, nvars, int(multi), _ptr(deg), len(deg),
+                                  _buf(proof), len(proof), _ptr(point), _ptr(expected))
+    return rc, point, expected
+
+
+def sumcheck_comb(modulus: int, L: int, group, vals: np.ndarray) -> np.ndarray:
+    arr, keep = _sc_groups([group], L)
+    vals = np.ascontiguousarray(vals, dtype=np.uint64)
+    out = np.zeros(L, np.uint64)
+    mod = _limbs(modulus, L)
+    lib().zr_sumcheck_comb(_ptr(mod), L, arr, _ptr(vals), _ptr(out))
+    return out
+
+
+def mle_evaluate(modulus: int, L: int, mle: np.ndarray, point: np.ndarray) -> np.ndarray:
+    mle = np.ascontiguousarray(mle, dtype=np.uint64)
+    point = np.ascontiguousarray(point, dtype=np.uint64)
+    out = np.zeros(L, np.uint64)
+    mod = _limbs(modulus, L)
+    lib().zr_mle_evaluate(_ptr(mod), L, _ptr(mle), point.shape[0], _ptr(point), _ptr(out))
+    return out

@@ -1670,3 +1670,358 @@ out:
     zparams_free(&z);
     return rc;
 }
+
+/* ========================================================================
+ * Sumcheck (piop/src/sumcheck.rs:163-338, sumcheck/prover.rs:95-247,
+ * sumcheck/verifier.rs, sumcheck/multi_degree.rs:259-355) with the
+ * combination function comb(v) = sum_k coeff_k * prod_{i in S_k} v_i, the
+ * form of the reference's test comb functions (sumcheck/tests/utils.rs:60-80).
+ * Field elements are Montgomery inner values of L limbs.
+ * ====================================================================== */
+static void f_from_u64(const fcfg *f, uint64_t v, uint64_t *out) {
+    uint64_t x[2] = {v, 0};
+    f_from_int(f, x, 2, out);
+}
+
+/* comb(vals) for one group */
+static void sc_comb(const fcfg *f, const zr_sc_group *g, const uint64_t *vals, uint64_t *out) {
+    uint32_t L = f->L;
+    uint64_t acc[4] = {0};
+    for (uint32_t k = 0; k < g->n_products; k++) {
+        uint64_t t[4];
+        memcpy(t, g->coeffs + (size_t)k * L, 8 * L);
+        for (uint32_t q = g->offsets[k]; q < g->offsets[k + 1]; q++) {
+            uint64_t u[4];
+            fmul(f, t, vals + (size_t)g->indices[q] * L, u);
+            memcpy(t, u, 8 * L);
+        }
+        fadd(f, acc, t);
+    }
+    memcpy(out, acc, 8 * L);
+}
+
+/* ProverState::prove_round evaluations (before removing P(0)): evals[deg+1] */
+static void sc_round_evals(const fcfg *f, const zr_sc_group *g, uint64_t *const *m, size_t half,
+                           uint64_t *evals) {
+    uint32_t L = f->L, K = g->n_mles, D = g->degree;
+    memset(evals, 0, 8 * L * (size_t)(D + 1));
+    int nt = zr_get_threads();
+    (void)nt;
+#pragma omp parallel num_threads(nt)
+    {
+        uint64_t *loc = (uint64_t *)calloc((size_t)(D + 1) * L, 8);
+        uint64_t *v0 = (uint64_t *)malloc(8 * L * (size_t)K), *v1 = (uint64_t *)malloc(8 * L * (size_t)K);
+        uint64_t *st = (uint64_t *)malloc(8 * L * (size_t)K), *cur = (uint64_t *)malloc(8 * L * (size_t)K);
+#pragma omp for schedule(static)
+        for (long b = 0; b < (long)half; b++) {
+            for (uint32_t j = 0; j < K; j++) {
+                memcpy(v0 + j * L, m[j] + (size_t)(2 * b) * L, 8 * L);
+                memcpy(v1 + j * L, m[j] + (size_t)(2 * b + 1) * L, 8 * L);
+            }
+            uint64_t e[4];
+            sc_comb(f, g, v0, e);
+            fadd(f, loc, e);
+            if (D > 0) {
+                sc_comb(f, g, v1, e);
+                fadd(f, loc + L, e);
+                for (uint32_t j = 0; j < K; j++) {
+                    memcpy(st + j * L, v1 + j * L, 8 * L);
+                    fsub(f, st + j * L, v0 + j * L);
+                    memcpy(cur + j * L, v1 + j * L, 8 * L);
+                }
+                for (uint32_t t = 2; t <= D; t++) {
+                    for (uint32_t j = 0; j < K; j++) fadd(f, cur + j * L, st + j * L);
+                    sc_comb(f, g, cur, e);
+                    fadd(f, loc + (size_t)t * L, e);
+                }
+            }
+        }
+#pragma omp critical
+        for (uint32_t t = 0; t <= D; t++) fadd(f, evals + (size_t)t * L, loc + (size_t)t * L);
+        free(loc);
+        free(v0);
+        free(v1);
+        free(st);
+        free(cur);
+    }
+}
+
+/* fix_variables_with_config (poly/src/mle/dense.rs:243-279) with one point */
+static void sc_fold(const fcfg *f, uint64_t *m, size_t half, const uint64_t *r) {
+    uint32_t L = f->L;
+    for (size_t b = 0; b < half; b++) {
+        uint64_t a[4], t[4];
+        memcpy(a, m + (2 * b + 1) * L, 8 * L);
+        fsub(f, a, m + (2 * b) * L);
+        fmul(f, r, a, t);
+        uint64_t s[4];
+        memcpy(s, m + (2 * b) * L, 8 * L);
+        fadd(f, s, t);
+        memcpy(m + b * L, s, 8 * L);
+    }
+}
+
+static void tr_field_challenge(zr_transcript *t, const fcfg *f, uint64_t *out) {
+    /* get_field_challenge: XOF of 8L bytes as Uint<L>, F::new_with_cfg (a
+     * value converted to Montgomery form), then absorbed as a field element */
+    uint8_t b[32];
+    zr_tr_challenge(t, b, 8 * f->L);
+    uint64_t x[4] = {0};
+    memcpy(x, b, 8 * f->L);
+    /* value mod p in Montgomery form: montmul(x, R^2) */
+    fmul(f, x, f->r2, out);
+}
+
+int zr_sumcheck_prove(zr_transcript *t, const uint64_t *modulus, uint32_t L, uint32_t nvars,
+                      int multi, const zr_sc_group *groups, uint32_t ngroups, uint8_t *proof,
+                      size_t cap, size_t *plen, uint64_t *point_out, uint64_t *finals_out) {
+    if (nvars == 0 || ngroups == 0 || (!multi && ngroups != 1) || L < 1 || L > 4) return -1;
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    uint64_t fe[4];
+    f_from_u64(&f, nvars, fe);
+    tr_absorb_field(t, &f, fe);
+    f_from_u64(&f, multi ? ngroups : groups[0].degree, fe);
+    tr_absorb_field(t, &f, fe);
+    if (multi)
+        for (uint32_t g = 0; g < ngroups; g++) {
+            f_from_u64(&f, groups[g].degree, fe);
+            tr_absorb_field(t, &f, fe);
+        }
+    size_t n = (size_t)1 << nvars;
+    /* working copies */
+    uint64_t ***m = (uint64_t ***)calloc(ngroups, sizeof(uint64_t **));
+    for (uint32_t g = 0; g < ngroups; g++) {
+        m[g] = (uint64_t **)calloc(groups[g].n_mles, sizeof(uint64_t *));
+        for (uint32_t j = 0; j < groups[g].n_mles; j++) {
+            m[g][j] = (uint64_t *)malloc(8 * L * n);
+            memcpy(m[g][j], groups[g].mles + (size_t)j * n * L, 8 * L * n);
+        }
+    }
+    uint32_t maxd = 0;
+    for (uint32_t g = 0; g < ngroups; g++) maxd = groups[g].degree > maxd ? groups[g].degree : maxd;
+    uint64_t *msgs = (uint64_t *)calloc((size_t)ngroups * nvars * (maxd + 1), 8 * L);
+    uint64_t *claimed = (uint64_t *)calloc(ngroups, 8 * L);
+    uint64_t *ev = (uint64_t *)calloc(maxd + 1, 8 * L);
+    uint64_t r[4] = {0};
+    size_t len = n;
+    for (uint32_t rd = 0; rd < nvars; rd++) {
+        if (rd > 0) {
+            for (uint32_t g = 0; g < ngroups; g++)
+                for (uint32_t j = 0; j < groups[g].n_mles; j++) sc_fold(&f, m[g][j], len / 2, r);
+            len /= 2;
+        }
+        for (uint32_t g = 0; g < ngroups; g++) {
+            sc_round_evals(&f, &groups[g], m[g], len / 2, ev);
+            uint32_t D = groups[g].degree;
+            if (rd == 0) {
+                memcpy(claimed + (size_t)g * L, ev, 8 * L);
+                if (D > 0) fadd(&f, claimed + (size_t)g * L, ev + L);
+            }
+            memcpy(msgs + ((size_t)g * nvars + rd) * (maxd + 1) * L, ev + L, 8 * L * (size_t)D);
+            if (!multi)
+                for (uint32_t e = 1; e <= D; e++) tr_absorb_field(t, &f, ev + (size_t)e * L);
+        }
+        if (multi)
+            for (uint32_t g = 0; g < ngroups; g++)
+                for (uint32_t e = 0; e < groups[g].degree; e++)
+                    tr_absorb_field(t, &f, msgs + (((size_t)g * nvars + rd) * (maxd + 1) + e) * L);
+        tr_field_challenge(t, &f, r);
+        tr_absorb_field(t, &f, r);
+        memcpy(point_out + (size_t)rd * L, r, 8 * L);
+    }
+    /* final evaluations of every MLE at the point (one more fold) */
+    size_t fo = 0;
+    for (uint32_t g = 0; g < ngroups; g++)
+        for (uint32_t j = 0; j < groups[g].n_mles; j++) {
+            sc_fold(&f, m[g][j], 1, r);
+            memcpy(finals_out + fo * L, m[g][j], 8 * L);
+            fo++;
+        }
+    /* transcription */
+    wbuf w = {proof, 0, cap, 0};
+    wput(&w, f.p, 8 * L);
+    if (!multi) {
+        uint32_t nm = nvars;
+        wput(&w, &nm, 4);
+        for (uint32_t rd = 0; rd < nvars; rd++) {
+            uint32_t D = groups[0].degree;
+            wput(&w, &D, 4);
+            wput(&w, msgs + (size_t)rd * (maxd + 1) * L, 8 * L * (size_t)D);
+        }
+        wput(&w, claimed, 8 * L);
+    } else {
+        uint32_t ng = ngroups, nv = nvars;
+        wput(&w, &ng, 4);
+        wput(&w, &nv, 4);
+        for (uint32_t g = 0; g < ngroups; g++) wput(&w, &groups[g].degree, 4);
+        for (uint32_t g = 0; g < ngroups; g++)
+            for (uint32_t rd = 0; rd < nvars; rd++)
+                wput(&w, msgs + ((size_t)g * nvars + rd) * (maxd + 1) * L, 8 * L * (size_t)groups[g].degree);
+        wput(&w, claimed, 8 * L * (size_t)ngroups);
+    }
+    *plen = w.len;
+    for (uint32_t g = 0; g < ngroups; g++) {
+        for (uint32_t j = 0; j < groups[g].n_mles; j++) free(m[g][j]);
+        free(m[g]);
+    }
+    free(m);
+    free(msgs);
+    free(claimed);
+    free(ev);
+    return w.overflow ? -3 : 0;
+}
+
+/* Lagrange evaluation at x of the polynomial with values y[0..n) at 0..n-1
+ * (NatEvaluatedPoly::evaluate_at_point, poly/src/univariate/nat_evaluation.rs) */
+static void nat_eval(const fcfg *f, const uint64_t *y, uint32_t n, const uint64_t *x, uint64_t *out) {
+    uint32_t L = f->L;
+    uint64_t acc[4] = {0};
+    for (uint32_t i = 0; i < n; i++) {
+        uint64_t num[4], den[4];
+        memcpy(num, f->one, 8 * L);
+        memcpy(den, f->one, 8 * L);
+        for (uint32_t j = 0; j < n; j++) {
+            if (j == i) continue;
+            uint64_t xj[4], t[4], dj[4];
+            f_from_u64(f, j, xj);
+            memcpy(t, x, 8 * L);
+            fsub(f, t, xj);
+            uint64_t u[4];
+            fmul(f, num, t, u);
+            memcpy(num, u, 8 * L);
+            uint64_t xi[4];
+            f_from_u64(f, i, xi);
+            memcpy(dj, xi, 8 * L);
+            fsub(f, dj, xj);
+            fmul(f, den, dj, u);
+            memcpy(den, u, 8 * L);
+        }
+        /* den^-1 by Fermat: den^(p-2) */
+        uint64_t e[4], inv[4];
+        memcpy(e, f->p, 8 * L);
+        uint64_t two[4] = {2, 0, 0, 0};
+        usub(e, two, L);
+        memcpy(inv, f->one, 8 * L);
+        for (int b = 64 * (int)L - 1; b >= 0; b--) {
+            uint64_t u[4];
+            fmul(f, inv, inv, u);
+            memcpy(inv, u, 8 * L);
+            if ((e[b / 64] >> (b % 64)) & 1) {
+                fmul(f, inv, den, u);
+                memcpy(inv, u, 8 * L);
+            }
+        }
+        uint64_t t1[4], t2[4];
+        fmul(f, y + (size_t)i * L, num, t1);
+        fmul(f, t1, inv, t2);
+        fadd(f, acc, t2);
+    }
+    memcpy(out, acc, 8 * L);
+}
+
+/* verify_as_subprotocol + check_and_generate_subclaim: returns 0 and the
+ * subclaim (point, expected evaluation per group) if the transcription is
+ * well formed; the caller compares expected with comb(finals). */
+int zr_sumcheck_verify(zr_transcript *t, const uint64_t *modulus, uint32_t L, uint32_t nvars,
+                       int multi, const uint32_t *degrees, uint32_t ngroups, const uint8_t *proof,
+                       size_t len, uint64_t *point_out, uint64_t *expected_out) {
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    rbuf rd = {proof, len, 0};
+    uint64_t mod[4] = {0};
+    if (rget(&rd, mod, 8 * L) || memcmp(mod, f.p, 8 * L)) return 3;
+    uint64_t fe[4];
+    f_from_u64(&f, nvars, fe);
+    tr_absorb_field(t, &f, fe);
+    f_from_u64(&f, multi ? ngroups : degrees[0], fe);
+    tr_absorb_field(t, &f, fe);
+    if (multi)
+        for (uint32_t g = 0; g < ngroups; g++) {
+            f_from_u64(&f, degrees[g], fe);
+            tr_absorb_field(t, &f, fe);
+        }
+    uint32_t maxd = 0;
+    for (uint32_t g = 0; g < ngroups; g++) maxd = degrees[g] > maxd ? degrees[g] : maxd;
+    uint64_t *msgs = (uint64_t *)calloc((size_t)ngroups * nvars * (maxd + 1), 8 * L);
+    uint64_t *claimed = (uint64_t *)calloc(ngroups, 8 * L);
+    int rc = 0;
+    if (!multi) {
+        uint32_t nm;
+        if (rget(&rd, &nm, 4) || nm != nvars) { rc = 3; goto done; }
+        for (uint32_t r = 0; r < nvars; r++) {
+            uint32_t D;
+            if (rget(&rd, &D, 4) || D != degrees[0]) { rc = 3; goto done; }
+            if (rget(&rd, msgs + (size_t)r * (maxd + 1) * L, 8 * L * (size_t)D)) { rc = 3; goto done; }
+        }
+        if (rget(&rd, claimed, 8 * L)) { rc = 3; goto done; }
+    } else {
+        uint32_t ng, nv;
+        if (rget(&rd, &ng, 4) || rget(&rd, &nv, 4) || ng != ngroups || nv != nvars) { rc = 3; goto done; }
+        for (uint32_t g = 0; g < ngroups; g++) {
+            uint32_t D;
+            if (rget(&rd, &D, 4) || D != degrees[g]) { rc = 3; goto done; }
+        }
+        for (uint32_t g = 0; g < ngroups; g++)
+            for (uint32_t r = 0; r < nvars; r++)
+                if (rget(&rd, msgs + ((size_t)g * nvars + r) * (maxd + 1) * L, 8 * L * (size_t)degrees[g])) { rc = 3; goto done; }
+        if (rget(&rd, claimed, 8 * L * (size_t)ngroups)) { rc = 3; goto done; }
+    }
+    {
+        uint64_t r[4];
+        for (uint32_t k = 0; k < nvars; k++) {
+            for (uint32_t g = 0; g < ngroups; g++)
+                for (uint32_t e = 0; e < degrees[g]; e++)
+                    tr_absorb_field(t, &f, msgs + (((size_t)g * nvars + k) * (maxd + 1) + e) * L);
+            tr_field_challenge(t, &f, r);
+            tr_absorb_field(t, &f, r);
+            memcpy(point_out + (size_t)k * L, r, 8 * L);
+        }
+        for (uint32_t g = 0; g < ngroups; g++) {
+            uint64_t expected[4];
+            memcpy(expected, claimed + (size_t)g * L, 8 * L);
+            uint32_t D = degrees[g];
+            uint64_t *y = (uint64_t *)calloc((size_t)D + 1, 8 * L);
+            for (uint32_t k = 0; k < nvars; k++) {
+                const uint64_t *tail = msgs + ((size_t)g * nvars + k) * (maxd + 1) * L;
+                if (D == 0) continue; /* constant polynomial: expected unchanged */
+                memcpy(y, expected, 8 * L);
+                fsub(&f, y, tail);
+                memcpy(y + L, tail, 8 * L * (size_t)D);
+                nat_eval(&f, y, D + 1, point_out + (size_t)k * L, expected);
+            }
+            free(y);
+            memcpy(expected_out + (size_t)g * L, expected, 8 * L);
+        }
+    }
+done:
+    free(msgs);
+    free(claimed);
+    return rc;
+}
+
+void zr_sumcheck_comb(const uint64_t *modulus, uint32_t L, const zr_sc_group *g,
+                      const uint64_t *vals, uint64_t *out) {
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    sc_comb(&f, g, vals, out);
+}
+
+/* MLE evaluation sum_x mle[x] * eq(x, point) (mle_eval_with_eq_table,
+ * poly/src/utils.rs:267-284); point in Montgomery form, bit 0 = point[0]. */
+void zr_mle_evaluate(const uint64_t *modulus, uint32_t L, const uint64_t *mle, uint32_t nvars,
+                     const uint64_t *point, uint64_t *out) {
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    size_t n = (size_t)1 << nvars;
+    uint64_t *eq = (uint64_t *)malloc(8 * L * n);
+    build_eq(&f, point, nvars, eq);
+    uint64_t acc[4] = {0};
+    for (size_t x = 0; x < n; x++) {
+        uint64_t t[4];
+        fmul(&f, mle + x * L, eq + x * L, t);
+        fadd(&f, acc, t);
+    }
+    memcpy(out, acc, 8 * L);
+    free(eq);
+}

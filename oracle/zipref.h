@@ -89,6 +89,27 @@ void zr_tr_challenge(zr_transcript *t, uint8_t *out, size_t n);
 void zr_tr_get_prime(zr_transcript *t, uint32_t limbs, uint64_t *prime_out);
 int zr_is_probable_prime_base2(const uint64_t *n, uint32_t limbs);
 
+/* Sumcheck with a sum-of-products combination function:
+ * comb(v) = sum_k coeffs[k] * prod_{q in [offsets[k], offsets[k+1])} v[indices[q]].
+ * mles: n_mles x 2^nvars field elements (Montgomery inner, L limbs). */
+typedef struct {
+    uint32_t degree, n_mles, n_products;
+    const uint64_t *mles;
+    const uint64_t *coeffs;
+    const uint32_t *offsets;
+    const uint32_t *indices;
+} zr_sc_group;
+int zr_sumcheck_prove(zr_transcript *t, const uint64_t *modulus, uint32_t L, uint32_t nvars,
+                      int multi, const zr_sc_group *groups, uint32_t ngroups, uint8_t *proof,
+                      size_t cap, size_t *plen, uint64_t *point_out, uint64_t *finals_out);
+int zr_sumcheck_verify(zr_transcript *t, const uint64_t *modulus, uint32_t L, uint32_t nvars,
+                       int multi, const uint32_t *degrees, uint32_t ngroups, const uint8_t *proof,
+                       size_t len, uint64_t *point_out, uint64_t *expected_out);
+void zr_sumcheck_comb(const uint64_t *modulus, uint32_t L, const zr_sc_group *g,
+                      const uint64_t *vals, uint64_t *out);
+void zr_mle_evaluate(const uint64_t *modulus, uint32_t L, const uint64_t *mle, uint32_t nvars,
+                     const uint64_t *point, uint64_t *out);
+
 /* threads used by the parallel regions */
 void zr_set_threads(int n);
 int zr_get_threads(void);

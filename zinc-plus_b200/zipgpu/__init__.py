@@ -46,6 +46,7 @@ EXPORTS = (
     "zg_transcript_absorb", "zg_transcript_absorb_slice", "zg_transcript_challenge",
     "zg_transcript_sample_field", "zg_transcript_proof", "zg_prove", "zg_prove_d",
     "zg_commit_prove", "zg_commit_prove_d", "zg_commit_prove_many", "zg_proof_size", "zg_verify",
+    "zg_sumcheck_prove", "zg_mle_evaluate",
 )
 
 
@@ -67,6 +68,14 @@ class ParamsInfo(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in (
         "num_rows", "row_len", "codeword_len", "depth", "base_len", "base_dim",
         "eval_bytes", "cw_bytes", "comb_bytes", "field_bytes")]
+
+
+class SumcheckGroupDesc(C.Structure):
+    """Mirror of ``zg_sumcheck_group``."""
+
+    _fields_ = [("degree", C.c_uint32), ("n_mles", C.c_uint32), ("n_products", C.c_uint32),
+                ("mles", C.c_void_p), ("coeffs", C.c_void_p), ("offsets", C.c_void_p),
+                ("indices", C.c_void_p)]
 
 
 _lib = None
@@ -111,6 +120,9 @@ def lib() -> C.CDLL:
         "zg_commit_prove_many": ([vp, u32, vp, C.c_int, vp, vp, vp, vp, vp, u32, vp], st),
         "zg_proof_size": ([vp, u32], sz),
         "zg_verify": ([vp, vp, u32, vp, vp, vp, sz], st),
+        "zg_sumcheck_prove": ([vp, vp, vp, u32, u32, C.c_int, C.POINTER(SumcheckGroupDesc), u32,
+                               C.c_int, vp, C.POINTER(sz), vp, vp], st),
+        "zg_mle_evaluate": ([vp, vp, u32, vp, u32, vp, vp], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -504,3 +516,105 @@ class MerkleTree:
 
     def root(self) -> bytes:
         return self._root
+
+
+# -------------------------------------------------------------------- sumcheck
+def int_to_limbs(x: int, limbs: int) -> np.ndarray:
+    return np.array([(x >> (64 * i)) & ((1 << 64) - 1) for i in range(limbs)], np.uint64)
+
+
+def limbs_to_int(a) -> int:
+    return sum(int(v) << (64 * i) for i, v in enumerate(np.asarray(a, np.uint64).ravel()))
+
+
+def to_montgomery(x: int, modulus: int, limbs: int) -> int:
+    """The Montgomery inner of x mod modulus (R = 2^(64 limbs))."""
+    return (x % modulus) * (1 << (64 * limbs)) % modulus
+
+
+def from_montgomery(inner: int, modulus: int, limbs: int) -> int:
+    return inner * pow(1 << (64 * limbs), -1, modulus) % modulus
+
+
+@dataclass
+class SumcheckGroup:
+    """One group of MLEs and its combination function, written as
+    sum_k coeff_k * prod_{i in products[k]} mle_i (MultiDegreeSumcheckGroup,
+    piop/src/sumcheck/multi_degree.rs:44-67).
+
+    mles: (n_mles, 2^nvars, limbs) uint64 Montgomery inners; products: a list of
+    (coeff_inner, [mle indices]); degree: the longest product.
+    """
+
+    degree: int
+    mles: np.ndarray
+    products: list
+
+    def _arrays(self, limbs: int):
+        mles = np.ascontiguousarray(self.mles, dtype=np.uint64)
+        coeffs = np.zeros((max(len(self.products), 1), limbs), np.uint64)
+        offsets = np.zeros(len(self.products) + 1, np.uint32)
+        idx = []
+        for k, (c, ids) in enumerate(self.products):
+            coeffs[k] = int_to_limbs(int(c), limbs)
+            idx.extend(int(i) for i in ids)
+            offsets[k + 1] = len(idx)
+        indices = np.array(idx or [0], np.uint32)
+        return mles, coeffs, offsets, indices
+
+
+def _sumcheck_prove(transcript: PcsProverTranscript, modulus: int, limbs: int, nvars: int,
+                    groups: Sequence[SumcheckGroup], multi: bool, ctx: Context | None):
+    keep, descs = [], (SumcheckGroupDesc * len(groups))()
+    n_mles = 0
+    for g, grp in zip(descs, groups):
+        mles, coeffs, offsets, indices = grp._arrays(limbs)
+        keep += [mles, coeffs, offsets, indices]
+        g.degree, g.n_mles, g.n_products = grp.degree, mles.shape[0], len(grp.products)
+        g.mles, g.coeffs = mles.ctypes.data, coeffs.ctypes.data
+        g.offsets, g.indices = offsets.ctypes.data, indices.ctypes.data
+        n_mles += mles.shape[0]
+    fb = 8 * limbs
+    cap = fb + 8 + 4 * len(groups) + fb * len(groups) + sum(
+        nvars * (fb * g.degree + 4) for g in groups)
+    proof = C.create_string_buffer(cap)
+    plen = C.c_size_t(cap)
+    point = np.zeros((nvars, limbs), np.uint64)
+    finals = np.zeros((max(n_mles, 1), limbs), np.uint64)
+    mod = int_to_limbs(modulus, limbs).tobytes()
+    check(lib().zg_sumcheck_prove((ctx or default_context()).handle, transcript.handle,
+                                  C.c_char_p(mod), limbs, nvars, int(multi), descs, len(groups), 0,
+                                  proof, C.byref(plen), _ptr(point), _ptr(finals)))
+    return proof.raw[: plen.value], point, finals[:n_mles]
+
+
+class MLSumcheck:
+    """MLSumcheck::prove_as_subprotocol (piop/src/sumcheck.rs:163-215)."""
+
+    @staticmethod
+    def prove_as_subprotocol(transcript: PcsProverTranscript, modulus: int, limbs: int,
+                             nvars: int, group: SumcheckGroup, ctx: Context | None = None):
+        """Returns (SumcheckProof bytes, point inners (nvars, limbs), final MLE values)."""
+        return _sumcheck_prove(transcript, modulus, limbs, nvars, [group], False, ctx)
+
+
+class MultiDegreeSumcheck:
+    """MultiDegreeSumcheck::prove_as_subprotocol (piop/src/sumcheck/multi_degree.rs:259-355)."""
+
+    @staticmethod
+    def prove_as_subprotocol(transcript: PcsProverTranscript, modulus: int, limbs: int,
+                             nvars: int, groups: Sequence[SumcheckGroup],
+                             ctx: Context | None = None):
+        return _sumcheck_prove(transcript, modulus, limbs, nvars, list(groups), True, ctx)
+
+
+def mle_evaluate(modulus: int, limbs: int, mle: np.ndarray, point: np.ndarray,
+                 ctx: Context | None = None) -> np.ndarray:
+    """sum_x mle[x] * eq(x, point) (mle_eval_with_eq_table, poly/src/utils.rs:267-284)."""
+    mle = np.ascontiguousarray(mle, dtype=np.uint64)
+    point = np.ascontiguousarray(point, dtype=np.uint64)
+    out = np.zeros(limbs, np.uint64)
+    mod = int_to_limbs(modulus, limbs).tobytes()
+    check(lib().zg_mle_evaluate((ctx or default_context()).handle, C.c_char_p(mod), limbs,
+                                _ptr(mle), point.shape[0], _ptr(point), _ptr(out)))
+    return out
