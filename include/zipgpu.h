@@ -222,6 +222,33 @@ zg_status zg_commit_prove_many(zg_params *p, uint32_t n, const void *const *poly
                                int polys_on_device, const uint8_t *points, uint8_t *roots,
                                uint8_t *evals, uint8_t *const *proofs, size_t *proof_lens,
                                uint32_t lanes, double *latency_ms);
+/* ---- Batched commit of independent polynomials of mixed shapes ---------------
+ * n calls of ZipPlus::commit_single (phase_commit.rs:61-101, batch of one, one
+ * Merkle tree each), polynomial i under params[i] (all created on ctx's
+ * device).  Polynomials sharing a params handle are encoded and hashed in one
+ * launch chain; the chains run on `lanes` concurrent streams.  Roots-only calls
+ * (hints == NULL) keep a plan per batch shape (the sequence of params handles):
+ * the first call times the kernel variants of each group shape (autotune),
+ * then captures every launch of the batch as one CUDA graph, which later calls
+ * replay.  Results are identical to n sequential zg_commit calls.
+ * polys[i]: host memory, or device memory when polys_on_device != 0 (a
+ * captured graph is rebuilt when device pointers change).  roots: n x 32 (may
+ * be NULL when hints are requested); hints (may be NULL): n handles, each freed
+ * with zg_hint_free; their device memory is shared per group and released with
+ * the group's last hint.  The library keeps at most 8 plans per context, each
+ * with its own lanes and device arena (released by zg_ctx_destroy). */
+typedef struct {
+    uint32_t lanes;    /* concurrent streams, 0 = 4 (max 16) */
+    int use_graph;     /* roots-only calls: capture and replay a CUDA graph */
+    int autotune;      /* time the kernel variants of each group shape once */
+    int base_variant;  /* -1 = tuned/heuristic; binary IPRS base layer: 0 tensor-core,
+                          1 shared-memory staged, 2 packed-lane, 3 plain */
+    int leaf_variant;  /* -1 = tuned/heuristic; one-chunk leaves: 0 warp-coalesced, 1 per-thread */
+} zg_batch_opts;
+zg_status zg_commit_batch(zg_ctx *ctx, uint32_t n, zg_params *const *params,
+                          const void *const *polys, int polys_on_device, const zg_batch_opts *opts,
+                          uint8_t *roots, zg_hint **hints);
+
 /* Exact proof length for a batch (phase_commit.rs:739-805 formula). */
 size_t zg_proof_size(const zg_params *p, uint32_t batch);
 

@@ -33,8 +33,10 @@ bool is_pow2(uint64_t x) { return x && !(x & (x - 1)); }
 uint32_t ilog2u(uint64_t x) { return 63 - __builtin_clzll(x); }
 uint32_t ilog_round_up(uint64_t x) { return is_pow2(x) ? ilog2u(x) : ilog2u(x) + 1; }
 
+}  // namespace
+
 // validate_input's bit budget for linear combinations (pcs/utils.rs:24-54).
-zg_status validate_budget(const zg_params *p, uint32_t batch) {
+zg_status zg::validate_budget(const zg_params *p, uint32_t batch) {
     if (batch == 0) {
         set_error("Batch must contain at least one polynomial");
         return ZG_ERR_INVALID_PARAM;
@@ -53,6 +55,8 @@ zg_status validate_budget(const zg_params *p, uint32_t batch) {
     }
     return ZG_OK;
 }
+
+namespace {
 
 uint64_t dmask_of(uint32_t D) { return D >= 64 ? ~0ull : ((1ull << D) - 1); }
 
@@ -253,6 +257,74 @@ zg_status commit_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_
     std::memcpy(h->root, hroot, 32);
     hphase(ctx, "commit_gpu");
     *out = h.release();
+    return ZG_OK;
+}
+
+// ----------------------------------------------------------- group commit
+size_t group_cw_stride(const zg_params *p) {
+    return (size_t)p->info.codeword_len * leaf_bytes_of(p, 1);
+}
+size_t group_tree_stride(const zg_params *p) { return (2 * (size_t)p->info.codeword_len - 1) * 32; }
+
+bool group_fits(const zg_params *p, uint32_t m) {
+    if (m <= 1) return true;
+    const uint64_t rows = (uint64_t)m * p->info.num_rows;
+    return group_cw_stride(p) % 256 == 0 && rows <= 65535 && leaf_bytes_of(p, 1) <= 0xFFFFFFFFull &&
+           (uint64_t)m * p->info.codeword_len <= 0xFFFFFFFFull;
+}
+
+zg_status launch_commit_group(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t m,
+                              uint8_t *cw_d, uint8_t *tree_d, cudaStream_t s,
+                              const CommitTuning &tune) {
+    if (!group_fits(p, m)) {
+        set_error("%u polynomials of this shape do not fit one launch chain", m);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    const uint32_t C = p->info.codeword_len, R = p->info.num_rows;
+    ZG_TRY(launch_encode(p, lane, polys_d, m * R, cw_d, true, s, m > 1 ? R : 0, tune.base_variant));
+    ZG_TRY(launch_leaf_hash(lane, cw_d, m * C, (uint32_t)leaf_bytes_of(p, 1), tree_d, s,
+                            m > 1 ? C : 0, tune.leaf_variant));
+    return launch_merkle_levels(lane, tree_d, C, s, m);
+}
+
+zg_status commit_group_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t m,
+                              zg_hint **hints, uint8_t *roots, const CommitTuning &tune) {
+    ZG_TRY(validate_budget(p, 1));
+    const uint32_t C = p->info.codeword_len;
+    const size_t cws = group_cw_stride(p), trs = group_tree_stride(p);
+    const size_t cw_bytes = ((size_t)m * cws + 255) & ~(size_t)255;
+    auto blk = std::make_shared<SharedBlock>();
+    blk->lane = lane;
+    blk->ptr = ctx_alloc(lane, cw_bytes + (size_t)m * trs, &blk->bytes);
+    if (!blk->ptr) return ZG_ERR_OOM;
+    uint8_t *cw = static_cast<uint8_t *>(blk->ptr), *tree = cw + cw_bytes;
+    cudaStream_t s = lane->stream;
+    ZG_TRY(launch_commit_group(p, lane, polys_d, m, cw, tree, s, tune));
+    ZG_TRY(lane->pin_out.ensure((size_t)m * 32));
+    uint8_t *hr = lane->pin_out.as<uint8_t>();
+    // roots: node 2C - 2 of every tree, one strided copy
+    if (cudaMemcpy2DAsync(hr, 32, tree + (2 * (size_t)C - 2) * 32, trs, 32, m,
+                          cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        set_error("group commit failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return ZG_ERR_CUDA;
+    }
+    if (roots) std::memcpy(roots, hr, (size_t)m * 32);
+    if (hints) {
+        for (uint32_t k = 0; k < m; k++) {
+            zg_hint *h = new zg_hint();
+            h->shared = blk;
+            h->params = p;
+            h->lane = lane;
+            h->batch = 1;
+            h->nrows = p->info.num_rows;
+            h->depth = ilog2u(C);
+            h->d_cw = cw + (size_t)k * cws;
+            h->d_tree = tree + (size_t)k * trs;
+            std::memcpy(h->root, hr + (size_t)k * 32, 32);
+            hints[k] = h;
+        }
+    }
     return ZG_OK;
 }
 
@@ -593,6 +665,8 @@ zg_status zg_ctx_create(int device, zg_ctx **out) {
 
 zg_status zg_ctx_destroy(zg_ctx *ctx) {
     if (!ctx) return ZG_OK;
+    cudaSetDevice(ctx->device);
+    ctx->plans.clear();
     for (zg_ctx *l : ctx->lanes) zg_ctx_destroy(l);
     ctx->lanes.clear();
     cudaSetDevice(ctx->device);
@@ -612,7 +686,7 @@ zg_status zg_ctx_destroy(zg_ctx *ctx) {
 
 uint64_t zg_ctx_kernel_launches(const zg_ctx *ctx) {
     if (!ctx) return 0;
-    uint64_t n = ctx->launches;
+    uint64_t n = ctx->launches + (uint64_t)ctx->launch_adjust;
     for (const zg_ctx *l : ctx->lanes) n += l->launches;
     return n;
 }
@@ -1173,11 +1247,7 @@ static zg_status commit_prove_many_impl(zg_params *p, uint32_t n, const void *co
     std::lock_guard<std::mutex> lk(ctx->mu);
     ZG_CUDA(cudaSetDevice(ctx->device));
     nlanes = std::max<uint32_t>(1, std::min<uint32_t>({nlanes, n, 16}));
-    while (ctx->lanes.size() < nlanes) {
-        zg_ctx *l = nullptr;
-        ZG_TRY(zg_ctx_create(ctx->device, &l));
-        ctx->lanes.push_back(l);
-    }
+    ZG_TRY(ensure_lanes(ctx, nlanes));
     const int cores = std::max(1, omp_get_num_procs());
     const int per_lane = std::max(1, cores / (int)nlanes);
     const size_t pt_bytes = 16 * (size_t)p->d.num_vars, fb = 8 * (size_t)p->d.field_limbs;

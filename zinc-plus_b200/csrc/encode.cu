@@ -27,6 +27,17 @@ __device__ __forceinline__ uint32_t octet_reverse(uint32_t x, uint32_t digits) {
 }
 
 // ---------------------------------------------------------------------------
+// Leaf-major position of (codeword position p, global row grow).  The rows of a
+// launch form segments of 2^seg_log rows, one polynomial each, and every
+// segment is its own C x 2^seg_log block (its polynomial's codeword); seg_log
+// >= 32 means a single segment of nrows rows.
+__device__ __forceinline__ size_t lm_pos(size_t p, uint32_t grow, uint32_t nrows, uint32_t C,
+                                         uint32_t seg_log) {
+    if (seg_log >= 32) return p * nrows + grow;
+    const size_t seg = grow >> seg_log;
+    return ((seg * C + p) << seg_log) + (grow & ((1u << seg_log) - 1u));
+}
+
 // Base layer, binary evaluations (base_multiply_into_output, radix8.rs:117-161):
 //   out[ch*bd + rb][lane] = sum_c bit_lane(in[octrev(ch) + c*8^depth]) * bm[rb][c]
 // Block: 32 base rows x ceil(D/8) lane groups; the chunk's inputs are staged
@@ -37,7 +48,8 @@ __global__ void __launch_bounds__(256) k_base_bin(const uint64_t *__restrict__ e
                                                   const int32_t *__restrict__ bmT, void *out,
                                                   uint32_t row_len, uint32_t bd, uint32_t bl,
                                                   uint32_t depth, uint32_t C, uint32_t D,
-                                                  uint64_t dmask, uint32_t nrows) {
+                                                  uint64_t dmask, uint32_t nrows,
+                                                  uint32_t seg_log) {
     extern __shared__ uint64_t sx[];
     const uint32_t grow = blockIdx.z, ch = blockIdx.y;
     const uint32_t oct = octet_reverse(ch, depth);
@@ -66,7 +78,7 @@ __global__ void __launch_bounds__(256) k_base_bin(const uint64_t *__restrict__ e
         if (lane >= D) break;
         if (FINAL) {
             int64_t *o = static_cast<int64_t *>(out);
-            size_t idx = LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane;
+            size_t idx = LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) * D + lane : ((size_t)grow * C + p) * D + lane;
             o[idx] = acc[j];
         } else {
             static_cast<int32_t *>(out)[((size_t)grow * C + p) * D + lane] = acc[j];
@@ -88,7 +100,8 @@ __global__ void __launch_bounds__(128) k_base_bin2(const uint64_t *__restrict__ 
                                                    const int32_t *__restrict__ bmP, void *out,
                                                    uint32_t row_len, uint32_t bd, uint32_t bdp,
                                                    uint32_t bl, uint32_t depth, uint32_t C,
-                                                   uint32_t D, uint64_t dmask, uint32_t nrows) {
+                                                   uint32_t D, uint64_t dmask, uint32_t nrows,
+                                                   uint32_t seg_log) {
     extern __shared__ __align__(16) uint8_t smem2[];
     uint4 *lut = reinterpret_cast<uint4 *>(smem2);  // 256 x 4 packed multipliers
     uint8_t *sxb = smem2 + 256 * sizeof(uint4);     // [group][c] lane bits
@@ -147,7 +160,7 @@ __global__ void __launch_bounds__(128) k_base_bin2(const uint64_t *__restrict__ 
                 if (lane >= D) continue;
                 if (FINAL) {
                     int64_t *o = static_cast<int64_t *>(out);
-                    o[LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane] = v2[h];
+                    o[LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) * D + lane : ((size_t)grow * C + p) * D + lane] = v2[h];
                 } else {
                     static_cast<int32_t *>(out)[((size_t)grow * C + p) * D + lane] = (int32_t)v2[h];
                 }
@@ -169,7 +182,8 @@ __global__ void __launch_bounds__(512) k_base_bin3(const uint64_t *__restrict__ 
                                                    uint32_t row_len, uint32_t bd, uint32_t bdp,
                                                    uint32_t bl, uint32_t depth, uint32_t nch,
                                                    uint32_t C, uint32_t D, uint32_t ngroups,
-                                                   uint64_t dmask, uint32_t nrows) {
+                                                   uint64_t dmask, uint32_t nrows,
+                                                   uint32_t seg_log) {
     extern __shared__ __align__(16) uint8_t smem3[];
     constexpr uint32_t RO = TR / 8;
     int4 *bmS = reinterpret_cast<int4 *>(smem3);                  // [bl][TR/4]
@@ -237,7 +251,7 @@ __global__ void __launch_bounds__(512) k_base_bin3(const uint64_t *__restrict__ 
                 if (lane >= D) continue;
                 if (FINAL) {
                     int64_t *o = static_cast<int64_t *>(out);
-                    o[LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane] = v2[h];
+                    o[LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) * D + lane : ((size_t)grow * C + p) * D + lane] = v2[h];
                 } else {
                     static_cast<int32_t *>(out)[((size_t)grow * C + p) * D + lane] = (int32_t)v2[h];
                 }
@@ -398,7 +412,8 @@ __global__ void __launch_bounds__(512) k_stages2_bin(const int32_t *__restrict__
                                                      int64_t *__restrict__ out,
                                                      const int32_t *__restrict__ tw0,
                                                      const int32_t *__restrict__ tw1, uint32_t C,
-                                                     uint32_t bd, uint32_t D, uint32_t nrows) {
+                                                     uint32_t bd, uint32_t D, uint32_t nrows,
+                                                     uint32_t seg_log) {
     extern __shared__ int64_t ys[];  // [r0][c1][lane], then the twiddles
     int32_t *tws = reinterpret_cast<int32_t *>(ys + (size_t)64 * D);  // [9][56]
     const uint32_t lane = threadIdx.x, q = threadIdx.y;
@@ -432,7 +447,7 @@ __global__ void __launch_bounds__(512) k_stages2_bin(const int32_t *__restrict__
 #pragma unroll
         for (int j = 1; j < 8; j++) z += x[j] * (uint64_t)(int64_t)t1[(j - 1) * 8 + ((r1 * j) & 7)];
         const size_t p = (size_t)(8 * r1 + q) * bd + rb;
-        out[LEAF_MAJOR ? (p * nrows + grow) * D + lane : ((size_t)grow * C + p) * D + lane] = (int64_t)z;
+        out[LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) * D + lane : ((size_t)grow * C + p) * D + lane] = (int64_t)z;
     }
 }
 
@@ -445,7 +460,8 @@ template <typename Tin, bool FINAL, bool LEAF_MAJOR>
 __global__ void __launch_bounds__(256) k_stage_bin(const Tin *__restrict__ in,
                                                    int64_t *__restrict__ out,
                                                    const int32_t *__restrict__ tw, uint32_t C,
-                                                   uint32_t sub, uint32_t D, uint32_t nrows) {
+                                                   uint32_t sub, uint32_t D, uint32_t nrows,
+                                                   uint32_t seg_log) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t C8 = C / 8;
     const size_t total = (size_t)nrows * C8 * D;
@@ -465,7 +481,7 @@ __global__ void __launch_bounds__(256) k_stage_bin(const Tin *__restrict__ in,
         for (int j = 1; j < 8; j++)
             y += x[j] * (uint64_t)(int64_t)__ldg(tw + (size_t)((j - 1) * 8 + ((r * j) & 7)) * sub + i);
         const size_t p = (size_t)blk * 8 * sub + (size_t)r * sub + i;
-        const size_t idx = (FINAL && LEAF_MAJOR) ? (p * nrows + grow) * D + lane
+        const size_t idx = (FINAL && LEAF_MAJOR) ? lm_pos(p, grow, nrows, C, seg_log) * D + lane
                                                  : ((size_t)grow * C + p) * D + lane;
         out[idx] = (int64_t)y;
     }
@@ -478,7 +494,8 @@ template <bool FINAL, bool LEAF_MAJOR>
 __global__ void __launch_bounds__(256) k_base_i32(const int32_t *__restrict__ evals,
                                                   const int32_t *__restrict__ bmT, void *out,
                                                   uint32_t row_len, uint32_t bd, uint32_t bl,
-                                                  uint32_t depth, uint32_t C, uint32_t nrows) {
+                                                  uint32_t depth, uint32_t C, uint32_t nrows,
+                                                  uint32_t seg_log) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (size_t)nrows * C) return;
     const uint32_t p = (uint32_t)(t % C), grow = (uint32_t)(t / C);
@@ -490,7 +507,7 @@ __global__ void __launch_bounds__(256) k_base_i32(const int32_t *__restrict__ ev
         acc += (int64_t)__ldg(row + oct + ((size_t)c << shift)) * (int64_t)__ldg(bmT + (size_t)c * bd + rb);
     if (FINAL) {
         i128 *o = static_cast<i128 *>(out);
-        o[LEAF_MAJOR ? (size_t)p * nrows + grow : (size_t)grow * C + p] = (i128)acc;
+        o[LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) : (size_t)grow * C + p] = (i128)acc;
     } else {
         static_cast<int64_t *>(out)[(size_t)grow * C + p] = acc;
     }
@@ -501,7 +518,8 @@ template <typename Tin, bool FINAL, bool LEAF_MAJOR>
 __global__ void __launch_bounds__(256) k_stage_i128(const Tin *__restrict__ in,
                                                     i128 *__restrict__ out,
                                                     const int32_t *__restrict__ tw, uint32_t C,
-                                                    uint32_t sub, uint32_t nrows) {
+                                                    uint32_t sub, uint32_t nrows,
+                                                    uint32_t seg_log) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t C8 = C / 8;
     if (t >= (size_t)nrows * C8) return;
@@ -518,7 +536,7 @@ __global__ void __launch_bounds__(256) k_stage_i128(const Tin *__restrict__ in,
         for (int j = 1; j < 8; j++)
             y += x[j] * (u128)(i128)__ldg(tw + (size_t)((j - 1) * 8 + ((r * j) & 7)) * sub + i);
         const size_t p = (size_t)blk * 8 * sub + (size_t)r * sub + i;
-        out[(FINAL && LEAF_MAJOR) ? p * nrows + grow : (size_t)grow * C + p] = (i128)y;
+        out[(FINAL && LEAF_MAJOR) ? lm_pos(p, grow, nrows, C, seg_log) : (size_t)grow * C + p] = (i128)y;
     }
 }
 
@@ -568,7 +586,7 @@ template <int LG>
 __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__restrict__ perm1,
                           const uint32_t *__restrict__ perm2, int32_t *__restrict__ out,
                           uint32_t row_len, uint32_t n, uint32_t D, uint64_t dmask,
-                          uint32_t nrows, bool leaf_major) {
+                          uint32_t nrows, bool leaf_major, uint32_t seg_log) {
     extern __shared__ uint32_t sm[];
     uint32_t *pre = sm;                 // n x LG
     uint32_t *wt = sm + (size_t)n * LG; // 32 x LG
@@ -621,7 +639,7 @@ __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__
             tot[l] += pre[(size_t)src * LG + l];
             const uint32_t lane = lane0 + l;
             if (lane < D) {
-                size_t idx = leaf_major ? ((size_t)i * nrows + grow) * D + lane
+                size_t idx = leaf_major ? lm_pos(i, grow, nrows, n, seg_log) * D + lane
                                         : ((size_t)grow * n + i) * D + lane;
                 out[idx] = (int32_t)tot[l];
             }
@@ -633,8 +651,18 @@ __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__
 static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_t nrows,
-                        uint8_t *out_d, bool leaf_major, cudaStream_t s) {
+                        uint8_t *out_d, bool leaf_major, cudaStream_t s, uint32_t seg_rows,
+                        int base_variant) {
     zg_ctx *ctx = lane;
+    uint32_t seg_log = 32;
+    if (seg_rows != 0 && seg_rows != nrows) {
+        if ((seg_rows & (seg_rows - 1)) != 0 || nrows % seg_rows != 0 || !leaf_major) {
+            set_error("segmented encode needs power-of-two segments that divide %u rows", nrows);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        seg_log = 0;
+        while ((1u << seg_log) < seg_rows) seg_log++;
+    }
     if (nrows > 65535) {
         set_error("too many codeword rows (%u) for one launch", nrows);
         return ZG_ERR_INVALID_PARAM;
@@ -665,7 +693,7 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         ZG_CUDA(cudaFuncSetAttribute(k_raa_bin<LGV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                      (int)smem));                                                 \
         k_raa_bin<LGV><<<grid, threads, smem, s>>>(ev, p1, p2, o, L, C, D, dmask, nrows,          \
-                                                   leaf_major);                                   \
+                                                   leaf_major, seg_log);                                   \
     } while (0)
         ZG_KBEGIN(ctx, s, "k_raa_bin");
         switch (LG) {
@@ -696,7 +724,9 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         constexpr uint32_t TR3 = 64;
         const size_t smem3 = (size_t)bl * TR3 * 4 + 256 * sizeof(uint4) + (size_t)kBase3Chunks * ngroups * bl;
         const uint32_t threads3 = (TR3 / 8) * ngroups * kBase3Chunks;
-        const bool staged = packed && smem3 <= 200 * 1024 && threads3 <= 512;
+        bool staged = packed && smem3 <= 200 * 1024 && threads3 <= 512;
+        if (base_variant == 2 || base_variant == 3) staged = false;
+        const bool use_packed = packed && base_variant != 3;
         auto base_launch = [&](void *dst, bool final_out, bool lm) -> zg_status {
             ZG_KBEGIN(ctx, s, "k_base_bin");
             if (staged) {
@@ -705,23 +735,23 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
                 ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
                 ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
                 if (final_out && lm)
-                    k_base_bin3<TR3, true, true><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows);
+                    k_base_bin3<TR3, true, true><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows, seg_log);
                 else if (final_out)
-                    k_base_bin3<TR3, true, false><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows);
+                    k_base_bin3<TR3, true, false><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows, seg_log);
                 else
-                    k_base_bin3<TR3, false, false><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows);
-            } else if (packed) {
+                    k_base_bin3<TR3, false, false><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows, seg_log);
+            } else if (use_packed) {
                 if (smem2 > 48 * 1024) {
                     ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
                     ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
                     ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
                 }
                 if (final_out && lm)
-                    k_base_bin2<true, true><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows);
+                    k_base_bin2<true, true><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows, seg_log);
                 else if (final_out)
-                    k_base_bin2<true, false><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows);
+                    k_base_bin2<true, false><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows, seg_log);
                 else
-                    k_base_bin2<false, false><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows);
+                    k_base_bin2<false, false><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows, seg_log);
             } else {
                 if (smem > 48 * 1024) {
                     ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -729,11 +759,11 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
                     ZG_CUDA(cudaFuncSetAttribute(k_base_bin<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 }
                 if (final_out && lm)
-                    k_base_bin<true, true><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows);
+                    k_base_bin<true, true><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows, seg_log);
                 else if (final_out)
-                    k_base_bin<true, false><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows);
+                    k_base_bin<true, false><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows, seg_log);
                 else
-                    k_base_bin<false, false><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows);
+                    k_base_bin<false, false><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows, seg_log);
             }
             ZG_KEND(ctx, s);
             return ZG_OK;
@@ -743,8 +773,10 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         int32_t *base = ctx->stage_a.as<int32_t>();
         const uint32_t blp = (bl + 31) / 32 * 32;
         const size_t smem_m = (size_t)3 * kMmaRows * (blp + 16) + (size_t)kMmaPairs * blp * 8;
-        if (p->d_bmL && smem_m <= 200 * 1024) {
-            dim3 gm((bd + kMmaRows - 1) / kMmaRows, (nrows * nch + kMmaPairs - 1) / kMmaPairs);
+        const uint64_t mma_gy = ((uint64_t)nrows * nch + kMmaPairs - 1) / kMmaPairs;
+        if (p->d_bmL && smem_m <= 200 * 1024 && mma_gy <= 65535 &&
+            (base_variant == -1 || base_variant == 0)) {
+            dim3 gm((bd + kMmaRows - 1) / kMmaRows, (unsigned)mma_gy);
             ZG_CUDA(cudaFuncSetAttribute(k_base_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m));
             ZG_KBEGIN(ctx, s, "k_base_bin");
             k_base_mma<<<gm, 128, smem_m, s>>>(ev, p->d_bmL, base, L, bd, bl, blp, depth, nch, C, D, dmask, nrows);
@@ -759,8 +791,8 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
             const int32_t *tw0 = p->d_tw + p->tw_dev_off[0], *tw1 = p->d_tw + p->tw_dev_off[1];
             int64_t *o = reinterpret_cast<int64_t *>(out_d);
             ZG_KBEGIN(ctx, s, "k_stages2_bin");
-            if (leaf_major) k_stages2_bin<true><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows);
-            else k_stages2_bin<false><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows);
+            if (leaf_major) k_stages2_bin<true><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows, seg_log);
+            else k_stages2_bin<false><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows, seg_log);
             ZG_KEND(ctx, s);
             return ZG_OK;
         }
@@ -782,18 +814,18 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
             ZG_KBEGIN(ctx, s, k == 0 ? "k_stage_bin[0]" : "k_stage_bin[1+]");
             if (k == 0) {
                 if (last && leaf_major)
-                    k_stage_bin<int32_t, true, true><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows);
+                    k_stage_bin<int32_t, true, true><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows, seg_log);
                 else if (last)
-                    k_stage_bin<int32_t, true, false><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows);
+                    k_stage_bin<int32_t, true, false><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows, seg_log);
                 else
-                    k_stage_bin<int32_t, false, false><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows);
+                    k_stage_bin<int32_t, false, false><<<nb, tb, 0, s>>>(base, dst, tw, C, sub, D, nrows, seg_log);
             } else {
                 if (last && leaf_major)
-                    k_stage_bin<int64_t, true, true><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows);
+                    k_stage_bin<int64_t, true, true><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows, seg_log);
                 else if (last)
-                    k_stage_bin<int64_t, true, false><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows);
+                    k_stage_bin<int64_t, true, false><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows, seg_log);
                 else
-                    k_stage_bin<int64_t, false, false><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows);
+                    k_stage_bin<int64_t, false, false><<<nb, tb, 0, s>>>(prev, dst, tw, C, sub, D, nrows, seg_log);
             }
             ZG_KEND(ctx, s);
             prev = dst;
@@ -807,9 +839,9 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
     if (depth == 0) {
         ZG_KBEGIN(ctx, s, "k_base_i32");
         if (leaf_major)
-            k_base_i32<true, true><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows);
+            k_base_i32<true, true><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows, seg_log);
         else
-            k_base_i32<true, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows);
+            k_base_i32<true, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows, seg_log);
         ZG_KEND(ctx, s);
         return ZG_OK;
     }
@@ -818,7 +850,7 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
     ZG_TRY(ctx->stage_c.ensure(depth > 2 ? nbase * 16 : 16));
     int64_t *base = ctx->stage_a.as<int64_t>();
     ZG_KBEGIN(ctx, s, "k_base_i32");
-    k_base_i32<false, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, base, L, bd, bl, depth, C, nrows);
+    k_base_i32<false, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, base, L, bd, bl, depth, C, nrows, seg_log);
     ZG_KEND(ctx, s);
     const size_t nthr = (size_t)nrows * (C / 8);
     const unsigned nb = blocks_for(nthr, 256);
@@ -832,18 +864,18 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         ZG_KBEGIN(ctx, s, k == 0 ? "k_stage_i128[0]" : "k_stage_i128[1+]");
         if (k == 0) {
             if (last && leaf_major)
-                k_stage_i128<int64_t, true, true><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows);
+                k_stage_i128<int64_t, true, true><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
             else if (last)
-                k_stage_i128<int64_t, true, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows);
+                k_stage_i128<int64_t, true, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
             else
-                k_stage_i128<int64_t, false, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows);
+                k_stage_i128<int64_t, false, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
         } else {
             if (last && leaf_major)
-                k_stage_i128<i128, true, true><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows);
+                k_stage_i128<i128, true, true><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
             else if (last)
-                k_stage_i128<i128, true, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows);
+                k_stage_i128<i128, true, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
             else
-                k_stage_i128<i128, false, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows);
+                k_stage_i128<i128, false, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
         }
         ZG_KEND(ctx, s);
         prev = dst;

@@ -164,6 +164,10 @@ void ctx_release(zg_ctx *ctx, void *p, size_t bytes) {
     ctx->cache.insert({bytes, p});
 }
 
+SharedBlock::~SharedBlock() {
+    if (ptr) ctx_release(lane, ptr, bytes);
+}
+
 void ctx_cache_clear(zg_ctx *ctx) {
     std::lock_guard<std::mutex> lk(ctx->cache_mu);
     for (auto &kv : ctx->cache) cudaFree(kv.second);

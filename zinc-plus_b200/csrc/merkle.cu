@@ -20,18 +20,29 @@ struct GlobalWords {
     }
 };
 
+// Node index of leaf g when the leaves of 2^tree_log-leaf trees are hashed in
+// one launch: tree t = g >> tree_log keeps its layers in its own block of
+// 2W - 1 nodes (W = 2^tree_log).  tree_log >= 32: one tree, node g.
+__device__ __forceinline__ size_t leaf_node(uint32_t g, uint32_t tree_log) {
+    if (tree_log >= 32) return g;
+    const size_t t = g >> tree_log;
+    return t * ((2ull << tree_log) - 1) + (g & ((1u << tree_log) - 1u));
+}
+
 }  // namespace
 
 // Leaves of at most one chunk (1024 bytes): one thread per leaf, root output.
 __global__ void __launch_bounds__(128) k_leaf_small(const uint8_t *__restrict__ cw, uint32_t width,
-                                                    uint32_t leaf_bytes, uint32_t *__restrict__ leaves) {
+                                                    uint32_t leaf_bytes, uint32_t *__restrict__ leaves,
+                                                    uint32_t tree_log) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= width) return;
     GlobalWords ld{reinterpret_cast<const uint32_t *>(cw + (size_t)j * leaf_bytes), leaf_bytes};
     uint32_t h[8];
     b3::chunk_hash(ld, leaf_bytes, 0, true, h);
+    const size_t node = leaf_node(j, tree_log);
 #pragma unroll
-    for (int i = 0; i < 8; i++) leaves[(size_t)j * 8 + i] = h[i];
+    for (int i = 0; i < 8; i++) leaves[node * 8 + i] = h[i];
 }
 
 // Leaves of at most one chunk whose size is a multiple of 16 bytes: each warp
@@ -41,7 +52,8 @@ __global__ void __launch_bounds__(128) k_leaf_small(const uint8_t *__restrict__ 
 // compresses its own leaf's block from there.
 __global__ void __launch_bounds__(128) k_leaf_small_coalesced(const uint8_t *__restrict__ cw,
                                                               uint32_t width, uint32_t leaf_bytes,
-                                                              uint32_t *__restrict__ leaves) {
+                                                              uint32_t *__restrict__ leaves,
+                                                              uint32_t tree_log) {
     __shared__ uint32_t tile[4][32 * 17];  // per warp: 32 leaves x 16 words (+1 pad)
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t first = (blockIdx.x * 4 + warp) * 32;
@@ -75,8 +87,9 @@ __global__ void __launch_bounds__(128) k_leaf_small_coalesced(const uint8_t *__r
         b3::compress_cv(cv, m, 0, blen, flags);
     }
     if (first + lane < width) {
+        const size_t node = leaf_node(first + lane, tree_log);
 #pragma unroll
-        for (int i = 0; i < 8; i++) leaves[(size_t)(first + lane) * 8 + i] = cv[i];
+        for (int i = 0; i < 8; i++) leaves[node * 8 + i] = cv[i];
     }
 }
 
@@ -99,7 +112,8 @@ __global__ void __launch_bounds__(128) k_leaf_chunks(const uint8_t *__restrict__
 // Merge the chunk chaining values of each leaf in BLAKE3 tree order (the
 // incremental hasher's stack discipline), root flag on the final parent.
 __global__ void __launch_bounds__(128) k_leaf_merge(const uint32_t *__restrict__ cvs, uint32_t width,
-                                                    uint32_t nchunks, uint32_t *__restrict__ leaves) {
+                                                    uint32_t nchunks, uint32_t *__restrict__ leaves,
+                                                    uint32_t tree_log) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= width) return;
     const uint32_t *cv = cvs + (size_t)j * nchunks * 8;
@@ -118,7 +132,8 @@ __global__ void __launch_bounds__(128) k_leaf_merge(const uint32_t *__restrict__
     }
     for (int i = 0; i < 8; i++) cur[i] = cv[(size_t)(nchunks - 1) * 8 + i];
     for (int s = len - 1; s >= 0; s--) b3::parent_cv(stack[s], cur, s == 0, cur);
-    for (int i = 0; i < 8; i++) leaves[(size_t)j * 8 + i] = cur[i];
+    const size_t node = leaf_node(j, tree_log);
+    for (int i = 0; i < 8; i++) leaves[node * 8 + i] = cur[i];
 }
 
 // One tree level: node i of the next layer from nodes 2i, 2i+1.
@@ -138,19 +153,23 @@ __global__ void __launch_bounds__(256) k_merkle_level(const uint32_t *__restrict
     for (int k = 0; k < 8; k++) next[(size_t)i * 8 + k] = o[k];
 }
 
-// Tree levels k0+1 .. k0+nlev of a Merkle tree stored layer after layer
-// (layer k at node 2W - 2(W >> k)).  Block b reduces the 2^nlev nodes
+// Tree levels k0+1 .. k0+nlev of Merkle trees of `width` leaves, each stored
+// layer after layer (layer k at node 2W - 2(W >> k)) in consecutive blocks of
+// 2W - 1 nodes.  Block b of a tree reduces the 2^nlev nodes
 // [b * 2^nlev, (b+1) * 2^nlev) of layer k0 to one node, writing every
-// intermediate node; the tree's top node gets the ROOT flag.
-__global__ void __launch_bounds__(256) k_tree_levels(uint32_t *__restrict__ tree, uint32_t width,
+// intermediate node; each tree's top node gets the ROOT flag.
+__global__ void __launch_bounds__(256) k_tree_levels(uint32_t *__restrict__ forest, uint32_t width,
                                                      uint32_t k0, uint32_t nlev, uint32_t depth) {
     __shared__ uint32_t cvs[256][8];
     const uint32_t t = threadIdx.x;
     const uint32_t half = 1u << (nlev - 1);
+    const uint32_t per_tree = width >> (k0 + nlev);
+    uint32_t *tree = forest + (size_t)(blockIdx.x / per_tree) * (2ull * width - 1) * 8;
+    const uint32_t bx = blockIdx.x % per_tree;
     const size_t in_off = 2ull * width - 2ull * (width >> k0);
     uint32_t cur[8];
     if (t < half) {
-        const size_t node = in_off + ((size_t)blockIdx.x << nlev) + 2 * t;
+        const size_t node = in_off + ((size_t)bx << nlev) + 2 * t;
         uint32_t l[8], r[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) {
@@ -158,7 +177,7 @@ __global__ void __launch_bounds__(256) k_tree_levels(uint32_t *__restrict__ tree
             r[i] = tree[(node + 1) * 8 + i];
         }
         b3::parent_cv(l, r, k0 + 1 == depth, cur);
-        const size_t out = 2ull * width - 2ull * (width >> (k0 + 1)) + ((size_t)blockIdx.x << (nlev - 1)) + t;
+        const size_t out = 2ull * width - 2ull * (width >> (k0 + 1)) + ((size_t)bx << (nlev - 1)) + t;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             tree[out * 8 + i] = cur[i];
@@ -180,7 +199,7 @@ __global__ void __launch_bounds__(256) k_tree_levels(uint32_t *__restrict__ tree
         if (t < n) {
             const uint32_t k = k0 + lev;
             b3::parent_cv(l, r, k == depth, cur);
-            const size_t out = 2ull * width - 2ull * (width >> k) + ((size_t)blockIdx.x << (nlev - lev)) + t;
+            const size_t out = 2ull * width - 2ull * (width >> k) + ((size_t)bx << (nlev - lev)) + t;
 #pragma unroll
             for (int i = 0; i < 8; i++) {
                 tree[out * 8 + i] = cur[i];
@@ -192,18 +211,28 @@ __global__ void __launch_bounds__(256) k_tree_levels(uint32_t *__restrict__ tree
 }
 
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
-                           uint8_t *leaves_d, cudaStream_t s) {
+                           uint8_t *leaves_d, cudaStream_t s, uint32_t tree_width,
+                           int leaf_variant) {
     if (leaf_bytes % 4 != 0) {
         set_error("leaf size %u is not a multiple of 4 bytes", leaf_bytes);
         return ZG_ERR_INVALID_PARAM;
     }
+    uint32_t tree_log = 32;
+    if (tree_width != 0 && tree_width != width) {
+        if ((tree_width & (tree_width - 1)) != 0 || width % tree_width != 0) {
+            set_error("leaf hashing of several trees needs a power-of-two tree width dividing %u", width);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        tree_log = 31 - __builtin_clz(tree_width);
+    }
     uint32_t *leaves = reinterpret_cast<uint32_t *>(leaves_d);
     if (leaf_bytes <= b3::CHUNK_LEN) {
         ZG_KBEGIN(ctx, s, "k_leaf_small");
-        if (leaf_bytes % 16 == 0 && leaf_bytes > 0)
-            k_leaf_small_coalesced<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves);
+        if (leaf_bytes % 16 == 0 && leaf_bytes > 0 && leaf_variant != 1)
+            k_leaf_small_coalesced<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves,
+                                                                      tree_log);
         else
-            k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves);
+            k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves, tree_log);
         ZG_KEND(ctx, s);
         return ZG_OK;
     }
@@ -215,17 +244,18 @@ zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uin
     k_leaf_chunks<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw_d, width, leaf_bytes, nchunks, cvs);
     ZG_KEND(ctx, s);
     ZG_KBEGIN(ctx, s, "k_leaf_merge");
-    k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, nchunks, leaves);
+    k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, nchunks, leaves, tree_log);
     ZG_KEND(ctx, s);
     return ZG_OK;
 }
 
-zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s) {
+zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s,
+                               uint32_t ntrees) {
     uint32_t *tree = reinterpret_cast<uint32_t *>(tree_d);
     const uint32_t depth = 31 - __builtin_clz(width);
     for (uint32_t k0 = 0; k0 < depth;) {
         const uint32_t nlev = depth - k0 < 9 ? depth - k0 : 9;
-        const uint32_t blocks = width >> (k0 + nlev);
+        const uint32_t blocks = (width >> (k0 + nlev)) * ntrees;
         ZG_KBEGIN(ctx, s, "k_tree_levels");
         k_tree_levels<<<blocks, 1u << (nlev - 1), 0, s>>>(tree, width, k0, nlev, depth);
         ZG_KEND(ctx, s);
@@ -314,13 +344,13 @@ extern "C" zg_status zg_merkle_root_noalloc_d(const void *leaves_d, uint32_t wid
     const uint8_t *cw = static_cast<const uint8_t *>(leaves_d);
     // Every node is written before it is read, so nothing needs clearing.
     if (nchunks == 0) {
-        k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw, width, leaf_bytes, tree);
+        k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw, width, leaf_bytes, tree, 32u);
     } else {
         uint32_t *cvs = tree + nodes * 8;
         const uint64_t n = (uint64_t)width * nchunks;
         k_leaf_chunks<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw, width, leaf_bytes,
                                                                    (uint32_t)nchunks, cvs);
-        k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, (uint32_t)nchunks, tree);
+        k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, (uint32_t)nchunks, tree, 32u);
     }
     ZG_CUDA(cudaGetLastError());
     uint64_t off = 0;

@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cstdarg>
 #include <map>
+#include <memory>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -89,6 +90,12 @@ void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got);
 void ctx_release(zg_ctx *ctx, void *p, size_t bytes);
 void ctx_cache_clear(zg_ctx *ctx);
 
+struct BatchPlan;
+// Creates child contexts of ctx until it has n lanes.
+zg_status ensure_lanes(zg_ctx *ctx, uint32_t n);
+// validate_input's bit budget for linear combinations (pcs/utils.rs:24-54).
+zg_status validate_budget(const zg_params *p, uint32_t batch);
+
 // One pending timed launch.
 struct KernelEvent {
     const char *name;
@@ -125,6 +132,12 @@ struct zg_ctx {
     std::multimap<size_t, void *> cache;
     // child contexts (same device) used as concurrent lanes by batched calls
     std::vector<zg_ctx *> lanes;
+    // batched commit: captured plans by batch shape, autotuned kernel choices
+    // by group shape ((base, leaf) variant), launch count correction for
+    // graph capture and replay
+    std::vector<std::pair<std::string, std::shared_ptr<zg::BatchPlan>>> plans;
+    std::map<std::string, std::pair<int, int>> tune_cache;
+    int64_t launch_adjust = 0;
 };
 
 struct zg_params {
@@ -146,7 +159,19 @@ struct zg_params {
     uint32_t *d_perm = nullptr;  // perm1 then perm2
 };
 
+namespace zg {
+// A device block shared by the hints of polynomials committed in one launch
+// chain; it returns to the owning context's cache with the last hint.
+struct SharedBlock {
+    zg_ctx *lane = nullptr;
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    ~SharedBlock();
+};
+}  // namespace zg
+
 struct zg_hint {
+    std::shared_ptr<zg::SharedBlock> shared;  // set instead of `block` for group commits
     zg_params *params = nullptr;
     zg_ctx *lane = nullptr;    // context whose block cache owns `block`
     uint32_t batch = 0;
@@ -193,6 +218,27 @@ zg_status commit_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_
                         zg_hint **out);
 // tail_out: when not NULL, the proof after the b rows (combined row and column
 // openings) is written there instead of being appended to t->stream.
+// Kernel choices of a commit launch chain (-1: the built-in heuristic).
+struct CommitTuning {
+    int base_variant = -1;  // binary IPRS base layer: 0 tensor-core, 1 smem-staged, 2 packed, 3 plain
+    int leaf_variant = -1;  // one-chunk leaves: 0 warp-coalesced, 1 one thread per leaf
+};
+// Bytes of one polynomial's codeword (leaf-major) and Merkle tree in a group.
+size_t group_cw_stride(const zg_params *p);
+size_t group_tree_stride(const zg_params *p);
+// True when m polynomials of p can share one launch chain.
+bool group_fits(const zg_params *p, uint32_t m);
+// Launches only: the segmented encode of m polynomials (consecutive in
+// polys_d), the leaves of their m trees and all tree levels.  Polynomial k's
+// codeword is at cw_d + k * group_cw_stride(p), its tree at
+// tree_d + k * group_tree_stride(p) (root at node 2C - 2).
+zg_status launch_commit_group(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t m,
+                              uint8_t *cw_d, uint8_t *tree_d, cudaStream_t s,
+                              const CommitTuning &tune);
+// commit_single of m polynomials in one launch chain: hints[k] (may be NULL to
+// drop the hints) and roots (m x 32, host).
+zg_status commit_group_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t m,
+                              zg_hint **hints, uint8_t *roots, const CommitTuning &tune);
 zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void *polys_d,
                        uint32_t batch, const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
                        uint8_t *tail_out);
@@ -201,11 +247,19 @@ zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, cons
 
 // ------------------------------------------------------------- kernels
 // (defined in the .cu files; all launched on the given stream)
+// seg_rows (leaf-major only): the rows are consecutive polynomials of seg_rows
+// rows each, and each gets its own C x seg_rows codeword block; 0 = one block.
 zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_t nrows,
-                        uint8_t *out_d, bool leaf_major, cudaStream_t s);
+                        uint8_t *out_d, bool leaf_major, cudaStream_t s, uint32_t seg_rows = 0,
+                        int base_variant = -1);
+// tree_width: the `width` leaves belong to width / tree_width trees, stored in
+// consecutive blocks of 2 tree_width - 1 nodes; 0 = one tree.
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
-                           uint8_t *leaves_d, cudaStream_t s);
-zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s);
+                           uint8_t *leaves_d, cudaStream_t s, uint32_t tree_width = 0,
+                           int leaf_variant = -1);
+// All levels of ntrees trees of `width` leaves each (blocks of 2 width - 1 nodes).
+zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s,
+                               uint32_t ntrees = 1);
 
 // Node offset of Merkle layer k for `width` leaves (layers stored leaves first).
 inline size_t merkle_layer_off(size_t width, uint32_t k) { return 2 * width - 2 * (width >> k); }

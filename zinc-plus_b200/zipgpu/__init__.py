@@ -46,7 +46,7 @@ EXPORTS = (
     "zg_transcript_absorb", "zg_transcript_absorb_slice", "zg_transcript_challenge",
     "zg_transcript_sample_field", "zg_transcript_proof", "zg_prove", "zg_prove_d",
     "zg_commit_prove", "zg_commit_prove_d", "zg_commit_prove_many", "zg_proof_size", "zg_verify",
-    "zg_sumcheck_prove", "zg_mle_evaluate",
+    "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch",
 )
 
 
@@ -68,6 +68,17 @@ class ParamsInfo(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in (
         "num_rows", "row_len", "codeword_len", "depth", "base_len", "base_dim",
         "eval_bytes", "cw_bytes", "comb_bytes", "field_bytes")]
+
+
+class BatchOpts(C.Structure):
+    """Mirror of ``zg_batch_opts``."""
+
+    _fields_ = [("lanes", C.c_uint32), ("use_graph", C.c_int), ("autotune", C.c_int),
+                ("base_variant", C.c_int), ("leaf_variant", C.c_int)]
+
+    @staticmethod
+    def make(lanes=4, use_graph=True, autotune=True, base_variant=-1, leaf_variant=-1):
+        return BatchOpts(lanes, int(use_graph), int(autotune), base_variant, leaf_variant)
 
 
 class SumcheckGroupDesc(C.Structure):
@@ -123,6 +134,7 @@ def lib() -> C.CDLL:
         "zg_sumcheck_prove": ([vp, vp, vp, u32, u32, C.c_int, C.POINTER(SumcheckGroupDesc), u32,
                                C.c_int, vp, C.POINTER(sz), vp, vp], st),
         "zg_mle_evaluate": ([vp, vp, u32, vp, u32, vp, vp], st),
+        "zg_commit_batch": ([vp, u32, vp, vp, C.c_int, C.POINTER(BatchOpts), vp, vp], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -442,6 +454,33 @@ class ZipPlus:
     @staticmethod
     def commit_single(pp: ZipPlusParams, poly) -> tuple[ZipPlusHint, ZipPlusCommitment]:
         return ZipPlus.commit(pp, [poly])
+
+    @staticmethod
+    def commit_batch(pps: Sequence[ZipPlusParams], polys, ctx: Context | None = None,
+                     opts: BatchOpts | None = None, hints: bool = False, on_device: bool = False):
+        """commit_single of every polys[i] under pps[i] in one batched call
+        (zg_commit_batch).  Returns the commitments, plus the hints when asked.
+        With on_device, polys are device addresses (ints)."""
+        n = len(polys)
+        if n == 0 or len(pps) != n:
+            raise ValueError("need one parameter set per polynomial")
+        ctx = ctx or pps[0].ctx or default_context()
+        if on_device:
+            keep, ptrs = None, (C.c_void_p * n)(*[int(a) for a in polys])
+        else:
+            keep = []
+            for pp, poly in zip(pps, polys):
+                keep += _poly_ptrs(pp, [poly])[0]
+            ptrs = (C.c_void_p * n)(*[a.ctypes.data for a in keep])
+        hs = (C.c_void_p * n)() if hints else None
+        roots = C.create_string_buffer(32 * n)
+        prm = (C.c_void_p * n)(*[pp.handle.value for pp in pps])
+        check(lib().zg_commit_batch(ctx.handle, n, prm, ptrs, int(on_device),
+                                    C.byref(opts) if opts is not None else None, roots, hs))
+        comms = [ZipPlusCommitment(roots.raw[32 * i:32 * i + 32], 1) for i in range(n)]
+        if hints:
+            return comms, [ZipPlusHint(C.c_void_p(hs[i]), pps[i]) for i in range(n)]
+        return comms
 
     @staticmethod
     def prove(transcript: PcsProverTranscript, pp: ZipPlusParams, polys, point: Sequence[int],
