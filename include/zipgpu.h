@@ -98,6 +98,7 @@ typedef struct zg_ctx zg_ctx;
 typedef struct zg_params zg_params;
 typedef struct zg_hint zg_hint;
 typedef struct zg_transcript zg_transcript;
+typedef struct zg_server zg_server;
 
 /* ---- library / context --------------------------------------------------- */
 const char *zg_last_error(void);
@@ -248,6 +249,57 @@ typedef struct {
 zg_status zg_commit_batch(zg_ctx *ctx, uint32_t n, zg_params *const *params,
                           const void *const *polys, int polys_on_device, const zg_batch_opts *opts,
                           uint8_t *roots, zg_hint **hints);
+
+/* ---- Request server: continuous batching of commit+prove jobs --------------
+ * Each request is zg_commit_prove of one polynomial (commit_single,
+ * new_from_commitment, get_random_field_cfg, prove; byte-identical outputs).
+ * `workers` threads, each with its own stream and scratch, take requests as
+ * soon as they are free: the oldest request whose device footprint (input,
+ * codeword, Merkle layers, kernel scratch) fits the HBM budget is admitted
+ * together with queued requests of the same params handle (committed in one
+ * launch chain); codewords and Merkle layers stay on the device until the
+ * request's proof is done.  A request that does not fit may be passed by later
+ * ones for at most max_skip_ms, after which it blocks admission until memory
+ * frees up.  Requests arriving while others run join at the next free worker,
+ * so their kernels overlap with the running ones.  Between groups an idle
+ * worker keeps at most a quarter of the budget (of free memory when the budget
+ * is 0), split over the workers, as scratch and cached blocks. */
+typedef struct {
+    uint32_t workers;      /* concurrent lanes, 0 = 4 (max 32) */
+    uint64_t hbm_budget;   /* device bytes in flight, 0 = 60% of free memory at creation */
+    uint32_t max_group;    /* most requests per launch chain, 0 = 16 */
+    uint32_t max_skip_ms;  /* how long the oldest request may be passed by smaller ones */
+    uint64_t group_max_bytes; /* only requests whose footprint is at most this share a
+                                 launch chain, 0 = 1 GiB */
+} zg_server_opts;
+typedef struct {
+    zg_status status;
+    size_t proof_len;
+    double latency_ms;  /* submit -> proof written */
+    double queue_ms;    /* submit -> admitted */
+    uint32_t group_size;
+} zg_server_result;
+typedef struct {
+    uint64_t completed, queued, in_flight, groups, grouped_requests;
+    uint64_t budget, reserved, peak_reserved;
+    /* wall time summed over workers: input copies, group commits, prime
+     * sampling (get_random_field_cfg), proves */
+    double ms_input, ms_commit, ms_prime, ms_prove;
+} zg_server_stats;
+zg_status zg_server_create(zg_ctx *ctx, const zg_server_opts *opts, zg_server **out);
+/* poly (2^num_vars evaluations, host memory), root (32 B), eval (8 * field_limbs B)
+ * and proof (proof_cap >= zg_proof_size(p, 1)) must stay valid until the request
+ * is waited for; point: num_vars i128 (copied).  ZG_ERR_OOM if the request can
+ * never fit the budget. */
+zg_status zg_server_submit(zg_server *s, zg_params *p, const void *poly, const uint8_t *point,
+                           uint8_t *root, uint8_t *eval, uint8_t *proof, size_t proof_cap,
+                           uint64_t *id);
+/* Waits for request `id` (timeout_ms < 0: no limit; ZG_ERR_TIMEOUT if still
+ * running) and releases it; returns the request's own status. */
+zg_status zg_server_wait(zg_server *s, uint64_t id, int timeout_ms, zg_server_result *res);
+zg_status zg_server_get_stats(zg_server *s, zg_server_stats *out);
+/* Finishes every submitted request, then stops the workers. */
+zg_status zg_server_destroy(zg_server *s);
 
 /* Exact proof length for a batch (phase_commit.rs:739-805 formula). */
 size_t zg_proof_size(const zg_params *p, uint32_t batch);

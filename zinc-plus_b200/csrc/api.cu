@@ -674,6 +674,7 @@ zg_status zg_ctx_destroy(zg_ctx *ctx) {
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
                       &ctx->wprime, &ctx->prove_in, &ctx->prove_out})
         b->release();
+    cudaStreamSynchronize(ctx->stream);  // stream-ordered frees of pooled buffers
     ctx->pin_in.release();
     ctx->pin_out.release();
     ktimer_collect(ctx);

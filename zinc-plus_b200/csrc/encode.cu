@@ -690,8 +690,7 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         const uint64_t *ev = static_cast<const uint64_t *>(evals_d);
 #define ZG_RAA(LGV)                                                                               \
     do {                                                                                          \
-        ZG_CUDA(cudaFuncSetAttribute(k_raa_bin<LGV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)smem));                                                 \
+        ZG_CUDA(allow_max_smem(k_raa_bin<LGV>));                                                 \
         k_raa_bin<LGV><<<grid, threads, smem, s>>>(ev, p1, p2, o, L, C, D, dmask, nrows,          \
                                                    leaf_major, seg_log);                                   \
     } while (0)
@@ -731,9 +730,9 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
             ZG_KBEGIN(ctx, s, "k_base_bin");
             if (staged) {
                 dim3 g3((bd + TR3 - 1) / TR3, (nch + kBase3Chunks - 1) / kBase3Chunks, nrows);
-                ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
-                ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
-                ZG_CUDA(cudaFuncSetAttribute(k_base_bin3<TR3, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
+                ZG_CUDA(allow_max_smem(k_base_bin3<TR3, true, true>));
+                ZG_CUDA(allow_max_smem(k_base_bin3<TR3, true, false>));
+                ZG_CUDA(allow_max_smem(k_base_bin3<TR3, false, false>));
                 if (final_out && lm)
                     k_base_bin3<TR3, true, true><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows, seg_log);
                 else if (final_out)
@@ -742,9 +741,9 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
                     k_base_bin3<TR3, false, false><<<g3, threads3, smem3, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, nch, C, D, ngroups, dmask, nrows, seg_log);
             } else if (use_packed) {
                 if (smem2 > 48 * 1024) {
-                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin2<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+                    ZG_CUDA(allow_max_smem(k_base_bin2<true, true>));
+                    ZG_CUDA(allow_max_smem(k_base_bin2<true, false>));
+                    ZG_CUDA(allow_max_smem(k_base_bin2<false, false>));
                 }
                 if (final_out && lm)
                     k_base_bin2<true, true><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows, seg_log);
@@ -754,9 +753,9 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
                     k_base_bin2<false, false><<<grid2, block2, smem2, s>>>(ev, p->d_bmP, dst, L, bd, bdp, bl, depth, C, D, dmask, nrows, seg_log);
             } else {
                 if (smem > 48 * 1024) {
-                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                    ZG_CUDA(cudaFuncSetAttribute(k_base_bin<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    ZG_CUDA(allow_max_smem(k_base_bin<true, true>));
+                    ZG_CUDA(allow_max_smem(k_base_bin<true, false>));
+                    ZG_CUDA(allow_max_smem(k_base_bin<false, false>));
                 }
                 if (final_out && lm)
                     k_base_bin<true, true><<<grid, block, smem, s>>>(ev, p->d_bmT, dst, L, bd, bl, depth, C, D, dmask, nrows, seg_log);
@@ -777,7 +776,7 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         if (p->d_bmL && smem_m <= 200 * 1024 && mma_gy <= 65535 &&
             (base_variant == -1 || base_variant == 0)) {
             dim3 gm((bd + kMmaRows - 1) / kMmaRows, (unsigned)mma_gy);
-            ZG_CUDA(cudaFuncSetAttribute(k_base_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m));
+            ZG_CUDA(allow_max_smem(k_base_mma));
             ZG_KBEGIN(ctx, s, "k_base_bin");
             k_base_mma<<<gm, 128, smem_m, s>>>(ev, p->d_bmL, base, L, bd, bl, blp, depth, nch, C, D, dmask, nrows);
             ZG_KEND(ctx, s);

@@ -29,7 +29,7 @@ zg_status DevBuf::ensure(size_t bytes) {
     if (bytes <= cap) return ZG_OK;
     release();
     size_t want = std::max(bytes, (size_t)256);
-    cudaError_t e = cudaMalloc(&ptr, want);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(&ptr, want, pool, pool_stream) : cudaMalloc(&ptr, want);
     if (e != cudaSuccess) {
         ptr = nullptr;
         cap = 0;
@@ -40,7 +40,10 @@ zg_status DevBuf::ensure(size_t bytes) {
     return ZG_OK;
 }
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        if (pool) cudaFreeAsync(ptr, pool_stream);
+        else cudaFree(ptr);
+    }
     ptr = nullptr;
     cap = 0;
 }
@@ -126,6 +129,21 @@ void hphase(zg_ctx *ctx, const char *name) {
     ctx->hmark = now;
 }
 
+int max_smem_optin() {
+    static std::atomic<int> cached{0};
+    int v = cached.load();
+    if (v == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+            cudaGetLastError();
+            v = 48 * 1024;
+        }
+        cached.store(v);
+    }
+    return v;
+}
+
 // ------------------------------------------------------------ block cache
 static size_t cache_round(size_t bytes) {
     const size_t g = bytes >= (2u << 20) ? (2u << 20) : 4096;
@@ -133,6 +151,16 @@ static size_t cache_round(size_t bytes) {
 }
 
 void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got) {
+    if (ctx->pool) {
+        void *p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("pool allocation of %zu bytes failed", bytes);
+            return nullptr;
+        }
+        *got = bytes;
+        return p;
+    }
     const size_t want = cache_round(bytes);
     {
         std::lock_guard<std::mutex> lk(ctx->cache_mu);
@@ -160,12 +188,52 @@ void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got) {
 
 void ctx_release(zg_ctx *ctx, void *p, size_t bytes) {
     if (!p) return;
+    if (ctx->pool) {
+        cudaFreeAsync(p, ctx->stream);
+        return;
+    }
     std::lock_guard<std::mutex> lk(ctx->cache_mu);
     ctx->cache.insert({bytes, p});
 }
 
 SharedBlock::~SharedBlock() {
     if (ptr) ctx_release(lane, ptr, bytes);
+}
+
+void ctx_cache_trim(zg_ctx *ctx, size_t max_bytes) {
+    std::lock_guard<std::mutex> lk(ctx->cache_mu);
+    size_t total = 0;
+    for (auto &kv : ctx->cache) total += kv.first;
+    // drop the largest blocks first
+    while (total > max_bytes && !ctx->cache.empty()) {
+        auto it = std::prev(ctx->cache.end());
+        total -= it->first;
+        cudaFree(it->second);
+        ctx->cache.erase(it);
+    }
+}
+
+void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool) {
+    ctx->pool = pool;
+    for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out}) {
+        b->pool = pool;
+        b->pool_stream = ctx->stream;
+    }
+}
+
+size_t ctx_scratch_bytes(const zg_ctx *ctx) {
+    size_t n = 0;
+    for (const DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
+                            &ctx->wprime, &ctx->prove_in, &ctx->prove_out})
+        n += b->cap;
+    return n;
+}
+
+void ctx_scratch_release(zg_ctx *ctx) {
+    for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out})
+        b->release();
 }
 
 void ctx_cache_clear(zg_ctx *ctx) {

@@ -171,7 +171,7 @@ static zg_status eq_table_t(zg_ctx *ctx, const uint64_t *r_d, const uint64_t *om
     if (n >= 2 && n <= 20) {
         const size_t sm = ((size_t)(1u << (n / 2)) + (1u << (n - n / 2))) * L * 8;
         if (sm > 48 * 1024)
-            ZG_CUDA(cudaFuncSetAttribute(k_eq_table_split<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            ZG_CUDA(allow_max_smem(k_eq_table_split<L>));
         k_eq_table_split<L><<<(m + 255) / 256, 256, sm, s>>>(r_d, omr_d, n, f, out_d);
     } else {
         k_eq_table<L><<<(m + 255) / 256, 256, 0, s>>>(r_d, omr_d, n, f, out_d);

@@ -53,11 +53,25 @@ void set_error(const char *fmt, ...);
         ZG_CHECK_LAUNCH(ctx);                                                                     \
     } while (0)
 
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in maximum.
+// Each launch passes its own size; setting the limit to that size per launch
+// would race between threads launching the same kernel with different sizes.
+int max_smem_optin();
+template <class F>
+inline cudaError_t allow_max_smem(F *func) {
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_optin());
+}
+
 // ------------------------------------------------------- device buffers
 // A growable device allocation owned by a context and reused across calls.
+// With a memory pool set, allocation and release are stream-ordered on
+// pool_stream (cudaMallocFromPoolAsync / cudaFreeAsync) and never synchronize
+// the device.
 struct DevBuf {
     void *ptr = nullptr;
     size_t cap = 0;
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t pool_stream = nullptr;
     zg_status ensure(size_t bytes);
     void release();
     template <class T>
@@ -89,6 +103,13 @@ void hphase(zg_ctx *ctx, const char *name);
 void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got);
 void ctx_release(zg_ctx *ctx, void *p, size_t bytes);
 void ctx_cache_clear(zg_ctx *ctx);
+// Frees cached blocks, largest first, until at most max_bytes stay cached.
+void ctx_cache_trim(zg_ctx *ctx, size_t max_bytes);
+// Routes a fresh context's hint blocks and scratch through a memory pool.
+void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool);
+// Device bytes held by a context's scratch arenas, and their release.
+size_t ctx_scratch_bytes(const zg_ctx *ctx);
+void ctx_scratch_release(zg_ctx *ctx);
 
 struct BatchPlan;
 // Creates child contexts of ctx until it has n lanes.
@@ -138,6 +159,9 @@ struct zg_ctx {
     std::vector<std::pair<std::string, std::shared_ptr<zg::BatchPlan>>> plans;
     std::map<std::string, std::pair<int, int>> tune_cache;
     int64_t launch_adjust = 0;
+    // stream-ordered pool for hint blocks and scratch (request-server lanes);
+    // NULL: blocks come from the context's cache, scratch from cudaMalloc
+    cudaMemPool_t pool = nullptr;
 };
 
 struct zg_params {

@@ -46,7 +46,8 @@ EXPORTS = (
     "zg_transcript_absorb", "zg_transcript_absorb_slice", "zg_transcript_challenge",
     "zg_transcript_sample_field", "zg_transcript_proof", "zg_prove", "zg_prove_d",
     "zg_commit_prove", "zg_commit_prove_d", "zg_commit_prove_many", "zg_proof_size", "zg_verify",
-    "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch",
+    "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch", "zg_server_create",
+    "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
 )
 
 
@@ -79,6 +80,25 @@ class BatchOpts(C.Structure):
     @staticmethod
     def make(lanes=4, use_graph=True, autotune=True, base_variant=-1, leaf_variant=-1):
         return BatchOpts(lanes, int(use_graph), int(autotune), base_variant, leaf_variant)
+
+
+class ServerOpts(C.Structure):
+    """Mirror of ``zg_server_opts``."""
+
+    _fields_ = [("workers", C.c_uint32), ("hbm_budget", C.c_uint64), ("max_group", C.c_uint32),
+                ("max_skip_ms", C.c_uint32), ("group_max_bytes", C.c_uint64)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("proof_len", C.c_size_t), ("latency_ms", C.c_double),
+                ("queue_ms", C.c_double), ("group_size", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("completed", "queued", "in_flight", "groups",
+                                          "grouped_requests", "budget", "reserved",
+                                          "peak_reserved")] + \
+               [(n, C.c_double) for n in ("ms_input", "ms_commit", "ms_prime", "ms_prove")]
 
 
 class SumcheckGroupDesc(C.Structure):
@@ -135,6 +155,11 @@ def lib() -> C.CDLL:
                                C.c_int, vp, C.POINTER(sz), vp, vp], st),
         "zg_mle_evaluate": ([vp, vp, u32, vp, u32, vp, vp], st),
         "zg_commit_batch": ([vp, u32, vp, vp, C.c_int, C.POINTER(BatchOpts), vp, vp], st),
+        "zg_server_create": ([vp, C.POINTER(ServerOpts), C.POINTER(vp)], st),
+        "zg_server_submit": ([vp, vp, vp, vp, vp, vp, vp, sz, C.POINTER(C.c_uint64)], st),
+        "zg_server_wait": ([vp, C.c_uint64, C.c_int, C.POINTER(ServerResult)], st),
+        "zg_server_get_stats": ([vp, C.POINTER(ServerStats)], st),
+        "zg_server_destroy": ([vp], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -657,3 +682,56 @@ def mle_evaluate(modulus: int, limbs: int, mle: np.ndarray, point: np.ndarray,
     check(lib().zg_mle_evaluate((ctx or default_context()).handle, C.c_char_p(mod), limbs,
                                 _ptr(mle), point.shape[0], _ptr(point), _ptr(out)))
     return out
+
+
+# -------------------------------------------------------------------- serving
+class ZipServer:
+    """Continuous-batching request server for commit+prove jobs (zg_server_*)."""
+
+    def __init__(self, ctx: Context | None = None, workers: int = 4, hbm_budget: int = 0,
+                 max_group: int = 16, max_skip_ms: int = 50, group_max_bytes: int = 0):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        opts = ServerOpts(workers, hbm_budget, max_group, max_skip_ms, group_max_bytes)
+        check(lib().zg_server_create(self.ctx.handle, C.byref(opts), C.byref(h)))
+        self.handle = h
+        self._pending = {}
+
+    def submit(self, pp: ZipPlusParams, poly, point: Sequence[int]) -> int:
+        arr = _poly_ptrs(pp, [poly])[0][0]
+        pt = C.create_string_buffer(i128_bytes(point), 16 * pp.num_vars)
+        cap = pp.proof_size(1)
+        root, ev = C.create_string_buffer(32), C.create_string_buffer(8 * pp.zt.field_limbs)
+        proof = C.create_string_buffer(cap)
+        rid = C.c_uint64()
+        check(lib().zg_server_submit(self.handle, pp.handle, C.c_void_p(arr.ctypes.data), pt, root, ev,
+                                     proof, cap, C.byref(rid)))
+        self._pending[rid.value] = (arr, pt, root, ev, proof)
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1):
+        """Returns (root, eval, proof, ServerResult) of request rid."""
+        res = ServerResult()
+        st = lib().zg_server_wait(self.handle, rid, timeout_ms, C.byref(res))
+        if st == 7:  # still running: keep its buffers
+            check(st)
+        _arr, _pt, root, ev, proof = self._pending.pop(rid)
+        check(st)
+        return root.raw, ev.raw, proof.raw[: res.proof_len], res
+
+    def stats(self) -> ServerStats:
+        out = ServerStats()
+        check(lib().zg_server_get_stats(self.handle, C.byref(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            check(lib().zg_server_destroy(self.handle))
+            self.handle = None
+            self._pending.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
