@@ -811,6 +811,24 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
             ZG_CUDA(cudaMalloc(&p->d_tw, std::max<size_t>(tw32.size(), 1) * 4));
             if (!tw32.empty())
                 ZG_CUDA(cudaMemcpy(p->d_tw, tw32.data(), tw32.size() * 4, cudaMemcpyHostToDevice));
+            if (depth == 2) {
+                // twiddles of both stages per base position, in the order the
+                // fused stage kernel uses them (tw[e] with e = (j-1)*8 + ((r*j) & 7))
+                std::vector<int32_t> t2((size_t)bd * 576, 0);
+                for (uint32_t rb = 0; rb < bd; rb++) {
+                    int32_t *dst = t2.data() + (size_t)rb * 576;
+                    for (uint32_t r0 = 0; r0 < 8; r0++)
+                        for (uint32_t j = 1; j < 8; j++)
+                            dst[r0 * 8 + j] = (int32_t)p->tw[p->tw_off[0] + (size_t)rb * 56 + (j - 1) * 8 + ((r0 * j) & 7)];
+                    for (uint32_t r0 = 0; r0 < 8; r0++)
+                        for (uint32_t r1 = 0; r1 < 8; r1++)
+                            for (uint32_t j = 1; j < 8; j++)
+                                dst[64 + (r0 * 8 + r1) * 8 + j] =
+                                    (int32_t)p->tw[p->tw_off[1] + ((size_t)r0 * bd + rb) * 56 + (j - 1) * 8 + ((r1 * j) & 7)];
+                }
+                ZG_CUDA(cudaMalloc(&p->d_tw2r, t2.size() * 4));
+                ZG_CUDA(cudaMemcpy(p->d_tw2r, t2.data(), t2.size() * 4, cudaMemcpyHostToDevice));
+            }
         }
     } else {
         const uint64_t n = (uint64_t)d.row_len * d.rep;
@@ -853,6 +871,7 @@ zg_status zg_params_destroy(zg_params *p) {
         cudaFree(p->d_bmP);
         cudaFree(p->d_bmL);
         cudaFree(p->d_tw);
+        cudaFree(p->d_tw2r);
         cudaFree(p->d_perm);
     }
     delete p;

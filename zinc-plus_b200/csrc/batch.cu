@@ -53,7 +53,7 @@ std::vector<CommitTuning> candidates(const zg_params *p) {
         bases = {0, 1, 2};
     std::vector<int> leaves = {-1};
     const size_t lb = (size_t)p->info.num_rows * p->info.cw_bytes;
-    if (lb <= 1024 && lb % 16 == 0) leaves = {0, 1};
+    if (lb % 16 == 0) leaves = {0, 1};
     for (int b : bases)
         for (int l : leaves) {
             CommitTuning t;

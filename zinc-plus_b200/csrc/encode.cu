@@ -12,6 +12,8 @@
 // ring homomorphism, so the order of additions does not change any output,
 // and when the reference's checked arithmetic does not overflow the values are
 // identical.
+#include <algorithm>
+
 #include "zg_internal.h"
 
 namespace zg {
@@ -403,51 +405,72 @@ __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ e
 }
 
 // Both radix-8 stages of a depth-2 code (combine_stages, radix8.rs:58-113) for
-// one base row rb of one codeword row, with the stage-0 outputs exchanged in
-// shared memory.  Thread (lane, q): stage 0 combines the chunks 8q..8q+7,
-// stage 1 combines, for r0 = q, the eight stage-0 outputs of each chunk group.
-// Output position (8 r1 + r0) * bd + rb.
-template <bool LEAF_MAJOR>
-__global__ void __launch_bounds__(512) k_stages2_bin(const int32_t *__restrict__ base,
+// one base position rb of one codeword row and one coefficient lane, entirely
+// in registers: the thread holds the 64 base outputs x[8 q + c0] (chunk 8q+c0,
+// position rb), and for each r0 computes the stage-0 outputs y[q] of the eight
+// chunk groups, then the stage-1 outputs, written at positions
+// (8 r1 + r0) * bd + rb.  Block: D lanes x RB positions; the positions'
+// twiddles (576 each, in use order) are staged in shared memory.
+constexpr uint32_t kStageRB = 8;
+
+__global__ void __launch_bounds__(256) k_stages2_reg(const int32_t *__restrict__ base,
                                                      int64_t *__restrict__ out,
-                                                     const int32_t *__restrict__ tw0,
-                                                     const int32_t *__restrict__ tw1, uint32_t C,
+                                                     const int32_t *__restrict__ tw2r, uint32_t C,
                                                      uint32_t bd, uint32_t D, uint32_t nrows,
-                                                     uint32_t seg_log) {
-    extern __shared__ int64_t ys[];  // [r0][c1][lane], then the twiddles
-    int32_t *tws = reinterpret_cast<int32_t *>(ys + (size_t)64 * D);  // [9][56]
-    const uint32_t lane = threadIdx.x, q = threadIdx.y;
-    const uint32_t rb = blockIdx.x, grow = blockIdx.y;
-    const uint32_t tid = q * blockDim.x + lane, nthr = blockDim.x * blockDim.y;
-    // stage-0 twiddles of position rb, stage-1 twiddles of positions q*bd + rb
-    for (uint32_t e = tid; e < 9 * 56; e += nthr) {
-        const uint32_t which = e / 56, k = e % 56;
-        tws[e] = which == 0 ? tw0[(size_t)k * bd + rb]
-                            : tw1[(size_t)k * 8 * bd + (size_t)(which - 1) * bd + rb];
-    }
-    uint64_t x[8];
-#pragma unroll
-    for (int c0 = 0; c0 < 8; c0++)
-        x[c0] = (uint64_t)(int64_t)base[((size_t)grow * C + (size_t)(8 * q + c0) * bd + rb) * D + lane];
+                                                     uint32_t seg_log, bool leaf_major) {
+    __shared__ __align__(16) int32_t ts[kStageRB * 576];
+    const uint32_t lane = threadIdx.x, yi = threadIdx.y, RB = blockDim.y;
+    const uint32_t rb0 = blockIdx.x * RB, grow = blockIdx.y;
+    const uint32_t npos = min(RB, bd - rb0);
+    const uint32_t tid = yi * blockDim.x + lane, nthr = blockDim.x * RB;
+    for (uint32_t e = tid; e < npos * 576; e += nthr) ts[e] = __ldg(tw2r + (size_t)rb0 * 576 + e);
     __syncthreads();
+    const uint32_t rb = rb0 + yi;
+    if (yi >= npos) return;
+    const int32_t *src = base + ((size_t)grow * C + rb) * D + lane;
+    const size_t pstride = (size_t)bd * D;  // next chunk, same position
+    int32_t x[64];
+#pragma unroll
+    for (int c = 0; c < 64; c++) x[c] = __ldg(src + (size_t)c * pstride);
+    const int32_t *T = ts + yi * 576;
 #pragma unroll
     for (int r0 = 0; r0 < 8; r0++) {
-        uint64_t y = x[0];
+        const int4 ta = *reinterpret_cast<const int4 *>(T + r0 * 8);
+        const int4 tb = *reinterpret_cast<const int4 *>(T + r0 * 8 + 4);
+        const int32_t t0[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+        // stage 0: int32 inputs, twiddles below 2^17: exact 32x32->64 products
+        int64_t y[8];
 #pragma unroll
-        for (int j = 1; j < 8; j++) y += x[j] * (uint64_t)(int64_t)tws[(j - 1) * 8 + ((r0 * j) & 7)];
-        ys[((size_t)r0 * 8 + q) * D + lane] = (int64_t)y;
-    }
-    __syncthreads();
+        for (int q = 0; q < 8; q++) {
+            int64_t acc = x[8 * q];
 #pragma unroll
-    for (int c1 = 0; c1 < 8; c1++) x[c1] = (uint64_t)ys[((size_t)q * 8 + c1) * D + lane];
-    const int32_t *t1 = tws + 56 * (1 + q);
+            for (int j = 1; j < 8; j++) acc += (int64_t)x[8 * q + j] * (int64_t)t0[j];
+            y[q] = acc;
+        }
+        // stage 1 modulo 2^64: y = hi * 2^32 + lo, lo the signed low word
+        int32_t lo[8];
+        uint32_t hi[8];
 #pragma unroll
-    for (int r1 = 0; r1 < 8; r1++) {
-        uint64_t z = x[0];
+        for (int q = 0; q < 8; q++) {
+            lo[q] = (int32_t)(uint32_t)(uint64_t)y[q];
+            hi[q] = (uint32_t)((uint64_t)(y[q] - (int64_t)lo[q]) >> 32);
+        }
 #pragma unroll
-        for (int j = 1; j < 8; j++) z += x[j] * (uint64_t)(int64_t)t1[(j - 1) * 8 + ((r1 * j) & 7)];
-        const size_t p = (size_t)(8 * r1 + q) * bd + rb;
-        out[LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) * D + lane : ((size_t)grow * C + p) * D + lane] = (int64_t)z;
+        for (int r1 = 0; r1 < 8; r1++) {
+            const int4 ua = *reinterpret_cast<const int4 *>(T + 64 + (r0 * 8 + r1) * 8);
+            const int4 ub = *reinterpret_cast<const int4 *>(T + 64 + (r0 * 8 + r1) * 8 + 4);
+            const int32_t t1[8] = {ua.x, ua.y, ua.z, ua.w, ub.x, ub.y, ub.z, ub.w};
+            int64_t acc = y[0];
+            uint32_t hacc = 0;
+#pragma unroll
+            for (int j = 1; j < 8; j++) {
+                acc += (int64_t)lo[j] * (int64_t)t1[j];
+                hacc += hi[j] * (uint32_t)t1[j];
+            }
+            const uint64_t z = (uint64_t)acc + ((uint64_t)hacc << 32);
+            const size_t p = (size_t)(8 * r1 + r0) * bd + rb;
+            out[(leaf_major ? lm_pos(p, grow, nrows, C, seg_log) : (size_t)grow * C + p) * D + lane] = (int64_t)z;
+        }
     }
 }
 
@@ -471,15 +494,28 @@ __global__ void __launch_bounds__(256) k_stage_bin(const Tin *__restrict__ in,
     const uint32_t q = (uint32_t)(rq % C8), grow = (uint32_t)(rq / C8);
     const uint32_t blk = q / sub, i = q % sub;
     const size_t base = (size_t)grow * C + (size_t)blk * 8 * sub + i;
-    uint64_t x[8];
+    // Inputs as a signed low word and a high word: x * tw mod 2^64 =
+    // lo * tw + ((hi * tw) mod 2^32) * 2^32 (hi = 0 for int32 inputs).
+    int64_t xf[8];
+    int32_t lo[8];
+    uint32_t hi[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) x[j] = (uint64_t)(int64_t)in[(base + (size_t)j * sub) * D + lane];
+    for (int j = 0; j < 8; j++) {
+        xf[j] = (int64_t)in[(base + (size_t)j * sub) * D + lane];
+        lo[j] = (int32_t)(uint32_t)(uint64_t)xf[j];
+        hi[j] = sizeof(Tin) == 4 ? 0u : (uint32_t)((uint64_t)(xf[j] - (int64_t)lo[j]) >> 32);
+    }
 #pragma unroll
     for (int r = 0; r < 8; r++) {
-        uint64_t y = x[0];
+        int64_t acc = xf[0];
+        uint32_t hacc = 0;
 #pragma unroll
-        for (int j = 1; j < 8; j++)
-            y += x[j] * (uint64_t)(int64_t)__ldg(tw + (size_t)((j - 1) * 8 + ((r * j) & 7)) * sub + i);
+        for (int j = 1; j < 8; j++) {
+            const int32_t t = __ldg(tw + (size_t)((j - 1) * 8 + ((r * j) & 7)) * sub + i);
+            acc += (int64_t)lo[j] * (int64_t)t;
+            if (sizeof(Tin) != 4) hacc += hi[j] * (uint32_t)t;
+        }
+        const uint64_t y = (uint64_t)acc + ((uint64_t)hacc << 32);
         const size_t p = (size_t)blk * 8 * sub + (size_t)r * sub + i;
         const size_t idx = (FINAL && LEAF_MAJOR) ? lm_pos(p, grow, nrows, C, seg_log) * D + lane
                                                  : ((size_t)grow * C + p) * D + lane;
@@ -783,15 +819,13 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         } else {
             ZG_TRY(base_launch(base, false, false));
         }
-        if (depth == 2 && D * 8 <= 512) {
-            // both stages in one kernel
-            dim3 b2(D, 8), g2(bd, nrows);
-            const size_t sm = (size_t)64 * D * 8 + 9 * 56 * 4;
-            const int32_t *tw0 = p->d_tw + p->tw_dev_off[0], *tw1 = p->d_tw + p->tw_dev_off[1];
+        if (depth == 2 && p->d_tw2r && D <= 64) {
+            // both stages in one kernel, register resident
+            const uint32_t RB = std::max<uint32_t>(1, std::min<uint32_t>(kStageRB, 256 / D));
+            dim3 b2(D, RB), g2((bd + RB - 1) / RB, nrows);
             int64_t *o = reinterpret_cast<int64_t *>(out_d);
             ZG_KBEGIN(ctx, s, "k_stages2_bin");
-            if (leaf_major) k_stages2_bin<true><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows, seg_log);
-            else k_stages2_bin<false><<<g2, b2, sm, s>>>(base, o, tw0, tw1, C, bd, D, nrows, seg_log);
+            k_stages2_reg<<<g2, b2, 0, s>>>(base, o, p->d_tw2r, C, bd, D, nrows, seg_log, leaf_major);
             ZG_KEND(ctx, s);
             return ZG_OK;
         }

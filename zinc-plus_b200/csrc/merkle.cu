@@ -109,6 +109,65 @@ __global__ void __launch_bounds__(128) k_leaf_chunks(const uint8_t *__restrict__
     for (int i = 0; i < 8; i++) cvs[t * 8 + i] = h[i];
 }
 
+// Chunk chaining values of long leaves whose size is a multiple of 16 bytes:
+// each warp hashes 32 consecutive (leaf, chunk) items, one per lane.  For every
+// 64-byte block the warp loads the 32 items' blocks with 16-byte loads (four
+// lanes per block, eight 64-byte runs per instruction) into shared memory, then
+// each lane compresses its own block from there.
+__global__ void __launch_bounds__(128) k_leaf_chunks_coalesced(const uint8_t *__restrict__ cw,
+                                                               uint32_t width, uint32_t leaf_bytes,
+                                                               uint32_t nchunks,
+                                                               uint32_t *__restrict__ cvs) {
+    __shared__ uint32_t tile[4][32 * 17];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const size_t total = (size_t)width * nchunks;
+    const size_t first = ((size_t)blockIdx.x * 4 + warp) * 32;
+    uint32_t *t = tile[warp];
+    // this lane's item
+    const size_t item = first + lane;
+    const uint32_t my_c = (uint32_t)(item % nchunks);
+    const uint32_t my_len = item < total ? min(b3::CHUNK_LEN, leaf_bytes - my_c * b3::CHUNK_LEN) : 0u;
+    const uint32_t my_blocks = (my_len + 63) / 64;
+    uint32_t cv[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) cv[i] = b3::iv(i);
+    for (uint32_t blk = 0; blk < b3::CHUNK_LEN / 64; blk++) {
+#pragma unroll
+        for (int it = 0; it < 4; it++) {
+            const uint32_t l = it * 8 + lane / 4, piece = lane & 3;
+            const size_t li = first + l;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (li < total) {
+                const size_t j = li / nchunks;
+                const uint32_t c = (uint32_t)(li % nchunks);
+                const uint32_t start = c * b3::CHUNK_LEN, off = 64 * blk + 16 * piece;
+                if (start + off < leaf_bytes && off < b3::CHUNK_LEN)
+                    v = __ldg(reinterpret_cast<const uint4 *>(cw + j * leaf_bytes + start + off));
+            }
+            uint32_t *d = t + l * 17 + 4 * piece;
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            d[3] = v.w;
+        }
+        __syncwarp();
+        uint32_t m[16];
+#pragma unroll
+        for (int w = 0; w < 16; w++) m[w] = t[lane * 17 + w];
+        __syncwarp();
+        if (blk < my_blocks) {
+            const uint32_t blen = (blk + 1 < my_blocks) ? 64u : my_len - 64u * blk;
+            const uint32_t flags = (blk == 0 ? b3::CHUNK_START : 0u) |
+                                   (blk + 1 == my_blocks ? b3::CHUNK_END : 0u);
+            b3::compress_cv(cv, m, my_c, blen, flags);
+        }
+    }
+    if (item < total) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) cvs[item * 8 + i] = cv[i];
+    }
+}
+
 // Merge the chunk chaining values of each leaf in BLAKE3 tree order (the
 // incremental hasher's stack discipline), root flag on the final parent.
 __global__ void __launch_bounds__(128) k_leaf_merge(const uint32_t *__restrict__ cvs, uint32_t width,
@@ -241,7 +300,11 @@ zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uin
     ZG_TRY(ctx->chunk_cv.ensure(n * 32));
     uint32_t *cvs = ctx->chunk_cv.as<uint32_t>();
     ZG_KBEGIN(ctx, s, "k_leaf_chunks");
-    k_leaf_chunks<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw_d, width, leaf_bytes, nchunks, cvs);
+    if (leaf_bytes % 16 == 0 && leaf_variant != 1)
+        k_leaf_chunks_coalesced<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw_d, width, leaf_bytes,
+                                                                             nchunks, cvs);
+    else
+        k_leaf_chunks<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw_d, width, leaf_bytes, nchunks, cvs);
     ZG_KEND(ctx, s);
     ZG_KBEGIN(ctx, s, "k_leaf_merge");
     k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, nchunks, leaves, tree_log);

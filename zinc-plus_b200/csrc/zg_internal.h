@@ -176,6 +176,9 @@ struct zg_params {
     int32_t *d_bmP = nullptr; // base_len x round_up(base_dim, 8) (transposed, zero padded)
     uint8_t *d_bmL = nullptr; // [3][base_dim][round_up(base_len, 32)] u8 limbs of the base matrix
     int32_t *d_tw = nullptr;  // stage k: [56][sub_k], stages back to back
+    // depth 2 only: per base position rb, 576 int32 twiddles in use order:
+    // [r0][j] for stage 0 (64), then [r0][r1][j] for stage 1 (512); j = 0 unused
+    int32_t *d_tw2r = nullptr;
     std::vector<size_t> tw_off;      // offset of each stage in tw (host, [i][j-1][t])
     std::vector<size_t> tw_dev_off;  // offset of each stage in d_tw (device, [56][sub])
     // RAA permutations
