@@ -413,7 +413,23 @@ __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ e
 // twiddles (576 each, in use order) are staged in shared memory.
 constexpr uint32_t kStageRB = 8;
 
-__global__ void __launch_bounds__(256) k_stages2_reg(const int32_t *__restrict__ base,
+// d = a * b + c with a 64-bit accumulator (one wide multiply-add).
+__device__ __forceinline__ int64_t mad_wide_s32(int32_t a, int32_t b, int64_t c) {
+    int64_t d;
+    asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint32_t mad_lo_u32(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+// Output element of position p = k * bd + rb (k = 8 r1 + r0) is out[A + k * S]:
+// leaf-major single block: A = (rb * nrows + grow) * D + lane, S = bd * nrows * D;
+// leaf-major segments of 2^seg_log rows: A = (((seg * C + rb) << seg_log) + r) * D + lane,
+// S = (bd << seg_log) * D; row-major: A = (grow * C + rb) * D + lane, S = bd * D.
+__global__ void __launch_bounds__(256, 2) k_stages2_reg(const int32_t *__restrict__ base,
                                                      int64_t *__restrict__ out,
                                                      const int32_t *__restrict__ tw2r, uint32_t C,
                                                      uint32_t bd, uint32_t D, uint32_t nrows,
@@ -427,6 +443,19 @@ __global__ void __launch_bounds__(256) k_stages2_reg(const int32_t *__restrict__
     __syncthreads();
     const uint32_t rb = rb0 + yi;
     if (yi >= npos) return;
+    size_t A, S;
+    if (!leaf_major) {
+        A = ((size_t)grow * C + rb) * D + lane;
+        S = (size_t)bd * D;
+    } else if (seg_log >= 32) {
+        A = ((size_t)rb * nrows + grow) * D + lane;
+        S = (size_t)bd * nrows * D;
+    } else {
+        const size_t seg = grow >> seg_log;
+        A = ((((seg * C + rb) << seg_log) + (grow & ((1u << seg_log) - 1u))) * D) + lane;
+        S = ((size_t)bd << seg_log) * D;
+    }
+    int64_t *o = out + A;
     const int32_t *src = base + ((size_t)grow * C + rb) * D + lane;
     const size_t pstride = (size_t)bd * D;  // next chunk, same position
     int32_t x[64];
@@ -444,7 +473,7 @@ __global__ void __launch_bounds__(256) k_stages2_reg(const int32_t *__restrict__
         for (int q = 0; q < 8; q++) {
             int64_t acc = x[8 * q];
 #pragma unroll
-            for (int j = 1; j < 8; j++) acc += (int64_t)x[8 * q + j] * (int64_t)t0[j];
+            for (int j = 1; j < 8; j++) acc = mad_wide_s32(x[8 * q + j], t0[j], acc);
             y[q] = acc;
         }
         // stage 1 modulo 2^64: y = hi * 2^32 + lo, lo the signed low word
@@ -453,7 +482,7 @@ __global__ void __launch_bounds__(256) k_stages2_reg(const int32_t *__restrict__
 #pragma unroll
         for (int q = 0; q < 8; q++) {
             lo[q] = (int32_t)(uint32_t)(uint64_t)y[q];
-            hi[q] = (uint32_t)((uint64_t)(y[q] - (int64_t)lo[q]) >> 32);
+            hi[q] = (uint32_t)((uint64_t)y[q] >> 32) + (uint32_t)(lo[q] < 0);
         }
 #pragma unroll
         for (int r1 = 0; r1 < 8; r1++) {
@@ -464,12 +493,11 @@ __global__ void __launch_bounds__(256) k_stages2_reg(const int32_t *__restrict__
             uint32_t hacc = 0;
 #pragma unroll
             for (int j = 1; j < 8; j++) {
-                acc += (int64_t)lo[j] * (int64_t)t1[j];
-                hacc += hi[j] * (uint32_t)t1[j];
+                acc = mad_wide_s32(lo[j], t1[j], acc);
+                hacc = mad_lo_u32(hi[j], (uint32_t)t1[j], hacc);
             }
             const uint64_t z = (uint64_t)acc + ((uint64_t)hacc << 32);
-            const size_t p = (size_t)(8 * r1 + r0) * bd + rb;
-            out[(leaf_major ? lm_pos(p, grow, nrows, C, seg_log) : (size_t)grow * C + p) * D + lane] = (int64_t)z;
+            o[(size_t)(8 * r1 + r0) * S] = (int64_t)z;
         }
     }
 }
