@@ -232,8 +232,10 @@ zg_status zg_commit_prove_many(zg_params *p, uint32_t n, const void *const *poly
  * the first call times the kernel variants of each group shape (autotune),
  * then captures every launch of the batch as one CUDA graph, which later calls
  * replay.  Results are identical to n sequential zg_commit calls.
- * polys[i]: host memory, or device memory when polys_on_device != 0 (a
- * captured graph is rebuilt when device pointers change).  roots: n x 32 (may
+ * polys[i]: host memory, or device memory when polys_on_device != 0.  Device
+ * inputs, and host inputs that are all page-locked, are copied by DMA from the
+ * caller's buffers, whose addresses the captured graph holds (it is captured
+ * again when they change); other host inputs go through a pinned staging copy.  roots: n x 32 (may
  * be NULL when hints are requested); hints (may be NULL): n handles, each freed
  * with zg_hint_free; their device memory is shared per group and released with
  * the group's last hint.  The library keeps at most 8 plans per context, each

@@ -118,6 +118,24 @@ def test_batch_commit_device_inputs(zipgpu, ctx, rng):
     assert [c.root for c in got] == want
 
 
+def test_batch_commit_pinned_inputs(zipgpu, ctx, rng):
+    """Page-locked host inputs are read by DMA in place; new buffers recapture."""
+    import torch
+
+    sh = Shapes(zipgpu, ctx)
+    pps = [sh.get(1, 64, 0, 12)] * 2 + [sh.get(1, 32, 0, 15), sh.get(0, 1, 0, 10, 64)]
+    polys = [_evals(rng, pp.zt.eval_kind, pp.zt.degree_plus_one, 1 << pp.num_vars) for pp in pps]
+    want = [zipgpu.ZipPlus.commit(pp, [p])[1].root for pp, p in zip(pps, polys)]
+    for _ in range(2):
+        pinned = [torch.from_numpy(p.copy()).pin_memory().numpy() for p in polys]
+        for _ in range(2):
+            got = zipgpu.ZipPlus.commit_batch(pps, pinned, ctx)
+            assert [c.root for c in got] == want
+        pinned[0][:] = polys[1]  # same buffers, new contents: the replay reads them
+        got = zipgpu.ZipPlus.commit_batch(pps, pinned, ctx)
+        assert got[0].root == want[1]
+
+
 def test_batch_commit_64_polys_nv10_20_deg64(zipgpu, oracle, ctx):
     """64 polynomials, num_vars uniform in 10..20, BinaryPoly<64> Bernoulli(0.5),
     IPRS: equal to 64 sequential commits; the smallest ones also to the oracle."""

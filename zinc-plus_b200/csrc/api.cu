@@ -250,7 +250,7 @@ zg_status commit_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_
     uint8_t *hroot = ctx->pin_out.as<uint8_t>();
     if (cudaMemcpyAsync(hroot, h->d_tree + merkle_layer_off(C, h->depth) * 32, 32,
                         cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
+        ctx_sync(ctx) != cudaSuccess) {
         set_error("commit failed: %s", cudaGetErrorString(cudaGetLastError()));
         return fail(ZG_ERR_CUDA);
     }
@@ -305,7 +305,7 @@ zg_status commit_group_device(zg_params *p, zg_ctx *lane, const void *polys_d, u
     // roots: node 2C - 2 of every tree, one strided copy
     if (cudaMemcpy2DAsync(hr, 32, tree + (2 * (size_t)C - 2) * 32, trs, 32, m,
                           cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
+        ctx_sync(lane) != cudaSuccess) {
         set_error("group commit failed: %s", cudaGetErrorString(cudaGetLastError()));
         return ZG_ERR_CUDA;
     }
@@ -415,7 +415,7 @@ zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void 
     uint64_t *hb = ctx->pin_out.as<uint64_t>();
     ZG_CUDA(cudaMemcpyAsync(hb, part_d, part_bytes, cudaMemcpyDeviceToHost, s));
     hphase(ctx, "prove_setup");
-    ZG_CUDA(cudaStreamSynchronize(s));
+    ZG_CUDA(ctx_sync(ctx));
     hphase(ctx, "prove_rows_gpu");
     // b[j] = sum over polys and blocks of the partials (field addition)
     std::vector<uint64_t> bv((size_t)R * L, 0);
@@ -471,7 +471,7 @@ zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void 
     }
     uint8_t *htail = direct ? tail_out : ctx->pin_out.as<uint8_t>();
     ZG_CUDA(cudaMemcpyAsync(htail, tail_d, tail_bytes, cudaMemcpyDeviceToHost, s));
-    ZG_CUDA(cudaStreamSynchronize(s));
+    ZG_CUDA(ctx_sync(ctx));
     hphase(ctx, "prove_tail_gpu");
     if (tail_out) {
         if (!direct) std::memcpy(tail_out, htail, tail_bytes);
@@ -675,6 +675,7 @@ zg_status zg_ctx_destroy(zg_ctx *ctx) {
                       &ctx->wprime, &ctx->prove_in, &ctx->prove_out})
         b->release();
     cudaStreamSynchronize(ctx->stream);  // stream-ordered frees of pooled buffers
+    if (ctx->sync_event) cudaEventDestroy(ctx->sync_event);
     ctx->pin_in.release();
     ctx->pin_out.release();
     ktimer_collect(ctx);
@@ -994,7 +995,7 @@ static zg_status merkle_root_impl(zg_ctx *ctx, const void *rows, uint32_t n_rows
     if (st == ZG_OK) st = launch_merkle_levels(ctx, tree.as<uint8_t>(), width, s);
     if (st == ZG_OK) {
         if (cudaMemcpyAsync(root, tree.as<uint8_t>() + (o - 1) * 32, 32, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess) {
+            ctx_sync(ctx) != cudaSuccess) {
             set_error("merkle root failed");
             st = ZG_ERR_CUDA;
         }

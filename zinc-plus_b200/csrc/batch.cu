@@ -77,6 +77,7 @@ std::string tune_key(const zg_params *p, uint32_t m) {
 struct BatchPlan {
     std::string key;
     bool on_device = false;
+    bool pinned = false;  // host inputs in page-locked memory: copied by DMA, no staging
     uint32_t n = 0, nlanes = 0;
     std::vector<Group> groups;
     std::vector<const void *> dev_inputs;  // for device inputs: the pointers baked into the graph
@@ -121,7 +122,12 @@ zg_status issue_plan(zg_ctx *ctx, BatchPlan &pl, const void *const *dev_polys) {
         const size_t pb = poly_bytes(g.p);
         const uint32_t m = (uint32_t)g.members.size();
         const void *in = nullptr;
-        if (!pl.on_device) {
+        if (pl.pinned) {
+            for (uint32_t k = 0; k < m; k++)
+                ZG_CUDA(cudaMemcpyAsync(arena + g.in_off + pb * k, dev_polys[g.members[k]], pb,
+                                        cudaMemcpyHostToDevice, s));
+            in = arena + g.in_off;
+        } else if (!pl.on_device) {
             ZG_CUDA(cudaMemcpyAsync(arena + g.in_off, pl.pin_in.as<uint8_t>() + g.in_off, pb * m,
                                     cudaMemcpyHostToDevice, s));
             in = arena + g.in_off;
@@ -185,9 +191,10 @@ zg_status autotune_group(zg_ctx *ctx, BatchPlan &pl, Group &g, const void *in) {
 }
 
 zg_status build_plan(zg_ctx *ctx, uint32_t n, zg_params *const *params, int on_device,
-                     uint32_t nlanes, BatchPlan &pl) {
+                     bool pinned, uint32_t nlanes, BatchPlan &pl) {
     pl.n = n;
     pl.on_device = on_device != 0;
+    pl.pinned = pinned;
     // groups: equal parameter handles, split where one launch chain cannot hold them
     std::vector<uint32_t> order(n);
     std::iota(order.begin(), order.end(), 0u);
@@ -247,15 +254,17 @@ zg_status build_plan(zg_ctx *ctx, uint32_t n, zg_params *const *params, int on_d
         off += 32 * g.members.size();
     }
     ZG_TRY(pl.arena.ensure(round256(off)));
-    if (!pl.on_device) ZG_TRY(pl.pin_in.ensure(std::max<size_t>(pl.in_bytes, 256)));
+    if (!pl.on_device && !pl.pinned) ZG_TRY(pl.pin_in.ensure(std::max<size_t>(pl.in_bytes, 256)));
     ZG_TRY(pl.pin_roots.ensure((size_t)n * 32));
     pl.events.resize(1 + std::max<uint32_t>(pl.nlanes, 1));
     for (cudaEvent_t &e : pl.events) ZG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDefault));
     return ZG_OK;
 }
 
-std::string plan_key(uint32_t n, zg_params *const *params, int on_device, uint32_t nlanes) {
-    std::string k = std::to_string(n) + ":" + std::to_string(on_device) + ":" + std::to_string(nlanes);
+std::string plan_key(uint32_t n, zg_params *const *params, int on_device, bool pinned,
+                     uint32_t nlanes) {
+    std::string k = std::to_string(n) + ":" + std::to_string(on_device) + ":" +
+                    std::to_string((int)pinned) + ":" + std::to_string(nlanes);
     for (uint32_t i = 0; i < n; i++) {
         char b[24];
         snprintf(b, sizeof b, ":%p", (const void *)params[i]);
@@ -433,7 +442,19 @@ zg_status commit_batch_impl(zg_ctx *ctx, uint32_t n, zg_params *const *params,
                                   roots, hints);
     }
     // roots only: a cached plan, replayed as one graph
-    const std::string key = plan_key(n, params, on_device, nlanes) +
+    // host inputs that are all page-locked are copied by DMA straight from the
+    // caller's buffers (their addresses are baked into the graph, like device inputs)
+    bool pinned = false;
+    if (!on_device) {
+        pinned = true;
+        for (uint32_t i = 0; i < n && pinned; i++) {
+            cudaPointerAttributes at{};
+            if (cudaPointerGetAttributes(&at, polys[i]) != cudaSuccess || at.type != cudaMemoryTypeHost)
+                pinned = false;
+            cudaGetLastError();
+        }
+    }
+    const std::string key = plan_key(n, params, on_device, pinned, nlanes) +
                             (forced ? ":f" + std::to_string(o.base_variant) + "," + std::to_string(o.leaf_variant) : "");
     std::shared_ptr<BatchPlan> pl;
     for (auto &kv : ctx->plans)
@@ -443,13 +464,13 @@ zg_status commit_batch_impl(zg_ctx *ctx, uint32_t n, zg_params *const *params,
         if (ctx->plans.size() >= 8) ctx->plans.erase(ctx->plans.begin());
         pl = std::make_shared<BatchPlan>();
         pl->key = key;
-        ZG_TRY(build_plan(ctx, n, params, on_device, nlanes, *pl));
+        ZG_TRY(build_plan(ctx, n, params, on_device, pinned, nlanes, *pl));
         ctx->plans.push_back({key, pl});
         fresh = true;
     }
-    if (!on_device) stage_host_inputs(*pl, polys);
+    if (!on_device && !pinned) stage_host_inputs(*pl, polys);
     std::vector<const void *> dev(polys, polys + n);
-    if (on_device && pl->dev_inputs != dev) {  // baked pointers changed: capture again
+    if ((on_device || pinned) && pl->dev_inputs != dev) {  // baked pointers changed: capture again
         if (pl->exec) cudaGraphExecDestroy(pl->exec);
         if (pl->graph) cudaGraphDestroy(pl->graph);
         pl->exec = nullptr;
@@ -469,7 +490,12 @@ zg_status commit_batch_impl(zg_ctx *ctx, uint32_t n, zg_params *const *params,
             const size_t pb = poly_bytes(g.p);
             uint8_t *arena = pl->arena.as<uint8_t>();
             const void *in = nullptr;
-            if (!on_device) {
+            if (pinned) {
+                for (uint32_t k = 0; k < m; k++)
+                    ZG_CUDA(cudaMemcpyAsync(arena + g.in_off + pb * k, polys[g.members[k]], pb,
+                                            cudaMemcpyHostToDevice, lane->stream));
+                in = arena + g.in_off;
+            } else if (!on_device) {
                 ZG_CUDA(cudaMemcpyAsync(arena + g.in_off, pl->pin_in.as<uint8_t>() + g.in_off, pb * m,
                                         cudaMemcpyHostToDevice, lane->stream));
                 in = arena + g.in_off;

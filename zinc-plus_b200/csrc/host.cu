@@ -213,6 +213,12 @@ void ctx_cache_trim(zg_ctx *ctx, size_t max_bytes) {
     }
 }
 
+cudaError_t ctx_sync(zg_ctx *ctx) {
+    if (!ctx->sync_event) return cudaStreamSynchronize(ctx->stream);
+    cudaError_t e = cudaEventRecord(ctx->sync_event, ctx->stream);
+    return e == cudaSuccess ? cudaEventSynchronize(ctx->sync_event) : e;
+}
+
 void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool) {
     ctx->pool = pool;
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,

@@ -171,7 +171,7 @@ void run_group(zg_server *s, zg_ctx *lane, std::vector<Request *> &g, std::vecto
             set_error("input copy failed: %s", cudaGetErrorString(cudaGetLastError()));
             st = ZG_ERR_CUDA;
         }
-    if (st == ZG_OK && cudaStreamSynchronize(lane->stream) != cudaSuccess) st = ZG_ERR_CUDA;
+    if (st == ZG_OK && ctx_sync(lane) != cudaSuccess) st = ZG_ERR_CUDA;
     t_in = ms_since(tick);
     tick = Clock::now();
     std::vector<zg_hint *> hints(m, nullptr);
@@ -312,13 +312,29 @@ zg_status zg_server_create(zg_ctx *ctx, const zg_server_opts *opts, zg_server **
         // completed, never by making that lane wait on the other's stream
         int no = 0;
         ZG_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+        // Reserve the budget in the pool once: growing the pool while several
+        // lanes allocate serialized them (measured: 4 workers slower than 1).
+        {
+            void *r = nullptr;
+            if (cudaMallocFromPoolAsync(&r, s->budget, s->pool, ctx->stream) == cudaSuccess) {
+                cudaFreeAsync(r, ctx->stream);
+                cudaStreamSynchronize(ctx->stream);
+            }
+            cudaGetLastError();
+        }
         for (uint32_t i = 0; i < o.workers; i++) {
             zg_ctx *l = nullptr;
             ZG_TRY(zg_ctx_create(ctx->device, &l));
             ctx_use_pool(l, s->pool);
+            // several workers wait at once: sleep on events instead of spinning
+            ZG_CUDA(cudaEventCreateWithFlags(&l->sync_event,
+                                             cudaEventBlockingSync | cudaEventDisableTiming));
             s->lanes.push_back(l);
         }
-        s->prime_threads = std::max(1, omp_get_num_procs() / (int)o.workers);
+        // Each worker samples its primes on its own thread: OpenMP teams per
+        // worker spin-wait between regions and starve the other workers'
+        // launches on a shared host.
+        s->prime_threads = 1;
         zg_server *raw = s.get();
         for (uint32_t i = 0; i < o.workers; i++) raw->workers.emplace_back(worker_main, raw, i);
         *out = s.release();

@@ -105,6 +105,9 @@ void ctx_release(zg_ctx *ctx, void *p, size_t bytes);
 void ctx_cache_clear(zg_ctx *ctx);
 // Frees cached blocks, largest first, until at most max_bytes stay cached.
 void ctx_cache_trim(zg_ctx *ctx, size_t max_bytes);
+// Waits until all work queued on ctx's stream is done (spinning, or sleeping
+// when the context has a blocking-sync event).
+cudaError_t ctx_sync(zg_ctx *ctx);
 // Routes a fresh context's hint blocks and scratch through a memory pool.
 void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool);
 // Device bytes held by a context's scratch arenas, and their release.
@@ -162,6 +165,9 @@ struct zg_ctx {
     // stream-ordered pool for hint blocks and scratch (request-server lanes);
     // NULL: blocks come from the context's cache, scratch from cudaMalloc
     cudaMemPool_t pool = nullptr;
+    // Waits for the stream by sleeping on a blocking-sync event instead of
+    // spinning (lanes on which several host threads wait at once).
+    cudaEvent_t sync_event = nullptr;
 };
 
 struct zg_params {
