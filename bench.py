@@ -605,6 +605,22 @@ def run_ours(args):
     return 0
 
 
+def run_commit_case(nv, D):
+    """Two commits of one seeded BinaryPoly<D> polynomial with 2^nv evaluations
+    (IPRS, row_len 2^min(nv, 14)): a small, fixed launch sequence for ncu captures."""
+    import zipgpu as Z
+
+    ctx = Z.Context(env_int("LOCAL_RANK", 0))
+    zt = Z.ZipTypes(1, D, 5, 4, 147)
+    pp = Z.ZipPlus.setup(1 << nv, Z.IprsCode(layout_row_len(nv)), zt, ctx=ctx)
+    poly = random_binary(np.random.default_rng(1), nv, D)
+    for _ in range(2):
+        hint, comm = Z.ZipPlus.commit(pp, [poly])
+        hint.close()
+    print(json.dumps({"commit_case": {"num_vars": nv, "D": D, "root": comm.root.hex()}}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -621,9 +637,13 @@ def main():
     ap.add_argument("--serve-workers", type=int, default=4)
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched-commit and serving measurements")
+    ap.add_argument("--commit-case", type=int, nargs=2, metavar=("NV", "D"),
+                    help="only commit one seeded polynomial twice (small case for ncu captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.commit_case:
+        return run_commit_case(*args.commit_case)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
