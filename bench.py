@@ -358,6 +358,79 @@ def run_serving(Z, ctx, torch, n_req, workers, seed=0x5A1F):
     }
 
 
+def cpr_group_arrays(rng, nv, p, L, n_mles=35):
+    """MLE inners and the comb of a BigLinear CPR sumcheck group (selector,
+    eq_r, 17 up and 16 down columns; degree 3) in the reference's shape: the
+    folded linear constraints, times eq_r and (1 - selector).  Random field
+    elements stand in for the trace, which does not change the work."""
+    top = p >> (64 * (L - 1))
+    mles = rng.integers(0, 2**63, size=(n_mles, 1 << nv, L), dtype=np.uint64)
+    mles[..., L - 1] %= np.uint64(top)
+    prods = [(int.from_bytes(rng.bytes(8 * L), "little") % p, [j]) for j in range(2, n_mles)]
+    one = (1 << (64 * L)) % p
+    factors = [(0, one, 1), (one, p - one, 0)]
+    return mles, prods, factors
+
+
+def run_sumcheck(Z, ctx, torch, stream, nv, cpu_nv, with_cpu):
+    """Config 4's CPR sumcheck group (2^nv points, 35 MLEs, degree 3, a 192-bit
+    MontyField<3> prime from the transcript): MultiDegreeSumcheck on the GPU with
+    device-resident MLEs, against the oracle on the host cores at 2^cpu_nv points."""
+    from oracle import oracle as O
+
+    O.build()
+    t = O.Transcript()
+    t.absorb_slice(b"bench-sumcheck")
+    L = 3
+    p = t.get_prime(L)
+    rng = np.random.default_rng(0x5A1F)
+    mles, prods, factors = cpr_group_arrays(rng, nv, p, L)
+    dev = torch.from_numpy(mles.view(np.uint8).reshape(-1)).cuda()
+    torch.cuda.synchronize()
+    grp = Z.SumcheckGroup(3, dev.data_ptr(), prods, n_mles=mles.shape[0], factors=factors)
+
+    def run():
+        tr = Z.PcsProverTranscript()
+        out = Z.MultiDegreeSumcheck.prove_as_subprotocol(tr, p, L, nv, [grp], ctx)
+        tr.close()
+        return out
+
+    for _ in range(2):
+        run()
+    times = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        proof = run()[0]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    gpu_ms = statistics.median(times)
+    res = {"workload": f"BigLinear CPR group: 2^{nv} points, 35 MLEs, degree 3 (33 folded linear "
+                       "terms times eq_r and (1 - selector)), MontyField<3> with a transcript-sampled "
+                       "192-bit prime; MLEs device-resident; MultiDegreeSumcheck",
+           "value": (1 << nv) / (gpu_ms / 1e3), "unit": "hypercube points/s", "ms": gpu_ms,
+           "proof_bytes": len(proof)}
+    if with_cpu:
+        small, sprods, sfac = cpr_group_arrays(np.random.default_rng(7), cpu_nv, p, L)
+        O.set_threads(os.cpu_count() or 1)
+        a = time.perf_counter()
+        want = O.sumcheck_prove(O.Transcript(), p, L, cpu_nv, [(3, small, sprods, sfac)], True)
+        cpu_s = time.perf_counter() - a
+        dsmall = torch.from_numpy(small.view(np.uint8).reshape(-1)).cuda()
+        torch.cuda.synchronize()
+        tr = Z.PcsProverTranscript()
+        got = Z.MultiDegreeSumcheck.prove_as_subprotocol(
+            tr, p, L, cpu_nv, [Z.SumcheckGroup(3, dsmall.data_ptr(), sprods, n_mles=35,
+                                               factors=sfac)], ctx)
+        tr.close()
+        res["cpu_baseline"] = {"value": (1 << cpu_nv) / cpu_s, "unit": "hypercube points/s",
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"oracle MultiDegreeSumcheck at 2^{cpu_nv} points, {cpu_s:.2f} s"}
+        res["proof_equal_oracle_at_cpu_size"] = got[0] == want[0]
+    return res
+
+
 # ------------------------------------------------------------------- ours
 def algorithmic_bytes(kernel, info, nv, D):
     """Algorithmic HBM bytes of one launch of `kernel` for one polynomial."""
@@ -556,8 +629,9 @@ def run_ours(args):
                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                     "kernel_share": {k: round(v[1] / sum(x[1] for x in ktimes.values()), 4)
                                      for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][1])}}
-    batch_commit = serving = None
+    batch_commit = serving = sumcheck = None
     if not args.no_extra:
+        sumcheck = run_sumcheck(Z, ctx, torch, stream, 18, 14, rank == 0 and not args.no_cpu_baseline)
         batch_commit = run_batched_commit(Z, ctx, torch, stream, flush, reps=5, warm=2)
         serving = run_serving(Z, ctx, torch, args.serve_requests, args.serve_workers,
                               seed=0x5A1F + rank)
@@ -596,6 +670,7 @@ def run_ours(args):
             "clocks": clock_info,
             "batched_commit": batch_commit,
             "serving": serving,
+            "sumcheck": sumcheck,
             "impl": "ours",
         }
         print(json.dumps(line), flush=True)

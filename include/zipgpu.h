@@ -315,21 +315,30 @@ zg_status zg_verify(zg_params *p, const uint8_t root[32], uint32_t batch, const 
 
 /* ---- PIOP sumcheck prover ----------------------------------------------------
  * One group of MLEs with the combination function
- *   comb(v) = sum_k coeffs[k] * prod_{q in [offsets[k], offsets[k+1])} v[indices[q]],
+ *   comb(v) = (sum_k coeffs[k] * prod_{q in [offsets[k], offsets[k+1])} v[indices[q]])
+ *             * prod_f (factor_a[f] + factor_b[f] * v[factor_mles[f]]),
  * i.e. the `comb_fn: Fn(&[F]) -> F` of MLSumcheck::prove_as_subprotocol
  * (piop/src/sumcheck.rs:163-215) and of MultiDegreeSumcheckGroup
- * (piop/src/sumcheck/multi_degree.rs:44-67) written as a sum of products.
+ * (piop/src/sumcheck/multi_degree.rs:44-67) written as a sum of products
+ * times affine factors (n_factors = 0: no factor).  The combined-polynomial
+ * resolver's comb_fn of a linear UAIR is folded(v) * (1 - sel) * eq_r
+ * (combined_poly_resolver.rs:158-172): a sum of one-MLE products and two factors.
  * mles: n_mles x 2^nvars field elements, Montgomery inner values of `limbs`
  * u64 each (DenseMultilinearExtension<F::Inner>), MLE-major; coeffs:
- * n_products Montgomery inners; offsets: n_products + 1 entries. */
+ * n_products Montgomery inners; offsets: n_products + 1 entries; factor_a,
+ * factor_b: n_factors Montgomery inners each. */
 typedef struct {
-    uint32_t degree;     /* the group's degree (max product length), <= 8 */
+    uint32_t degree;     /* the group's degree (longest product + n_factors), <= 8 */
     uint32_t n_mles;
     uint32_t n_products;
     const void *mles;    /* host, or device memory when mles_on_device != 0 */
     const uint64_t *coeffs;
     const uint32_t *offsets;
     const uint32_t *indices;
+    uint32_t n_factors;
+    const uint32_t *factor_mles;
+    const uint64_t *factor_a;
+    const uint64_t *factor_b;
 } zg_sumcheck_group;
 
 /* multi == 0: MLSumcheck::prove_as_subprotocol with one group; the proof is the

@@ -41,7 +41,8 @@ class ScGroup(C.Structure):
 
     _fields_ = [("degree", C.c_uint32), ("n_mles", C.c_uint32), ("n_products", C.c_uint32),
                 ("mles", C.c_void_p), ("coeffs", C.c_void_p), ("offsets", C.c_void_p),
-                ("indices", C.c_void_p)]
+                ("indices", C.c_void_p), ("n_factors", C.c_uint32), ("factor_mles", C.c_void_p),
+                ("factor_a", C.c_void_p), ("factor_b", C.c_void_p)]
 
 
 def build() -> str:
@@ -320,9 +321,18 @@ def _limbs(x: int, L: int) -> np.ndarray:
 
 
 def _sc_groups(groups, L):
-    """groups: list of (degree, mles (K, 2^n, L) uint64, [(coeff_inner, [idx...]), ...])."""
+    """groups: list of (degree, mles (K, 2^n, L) uint64, [(coeff_inner, [idx...]), ...]
+    [, [(a_inner, b_inner, mle index), ...] affine factors])."""
     keep, arr = [], (ScGroup * len(groups))()
-    for g, (deg, mles, prods) in zip(arr, groups):
+    for g, grp in zip(arr, groups):
+        deg, mles, prods = grp[:3]
+        factors = grp[3] if len(grp) > 3 else []
+        fm = np.array([int(x[2]) for x in factors] or [0], np.uint32)
+        fa = np.array([_limbs(int(x[0]), L) for x in factors] or [[0] * L], np.uint64)
+        fb = np.array([_limbs(int(x[1]), L) for x in factors] or [[0] * L], np.uint64)
+        keep += [fm, fa, fb]
+        g.n_factors = len(factors)
+        g.factor_mles, g.factor_a, g.factor_b = fm.ctypes.data, fa.ctypes.data, fb.ctypes.data
         mles = np.ascontiguousarray(mles, dtype=np.uint64)
         coeffs = np.zeros((max(len(prods), 1), L), np.uint64)
         offsets = np.zeros(len(prods) + 1, np.uint32)

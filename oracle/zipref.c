@@ -1683,7 +1683,7 @@ static void f_from_u64(const fcfg *f, uint64_t v, uint64_t *out) {
     f_from_int(f, x, 2, out);
 }
 
-/* comb(vals) for one group */
+/* comb(vals) for one group: the sum of products, times every affine factor */
 static void sc_comb(const fcfg *f, const zr_sc_group *g, const uint64_t *vals, uint64_t *out) {
     uint32_t L = f->L;
     uint64_t acc[4] = {0};
@@ -1696,6 +1696,13 @@ static void sc_comb(const fcfg *f, const zr_sc_group *g, const uint64_t *vals, u
             memcpy(t, u, 8 * L);
         }
         fadd(f, acc, t);
+    }
+    for (uint32_t q = 0; q < g->n_factors; q++) {
+        uint64_t fv[4], u[4];
+        fmul(f, g->factor_b + (size_t)q * L, vals + (size_t)g->factor_mles[q] * L, fv);
+        fadd(f, fv, g->factor_a + (size_t)q * L);
+        fmul(f, acc, fv, u);
+        memcpy(acc, u, 8 * L);
     }
     memcpy(out, acc, 8 * L);
 }

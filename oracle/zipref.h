@@ -89,8 +89,10 @@ void zr_tr_challenge(zr_transcript *t, uint8_t *out, size_t n);
 void zr_tr_get_prime(zr_transcript *t, uint32_t limbs, uint64_t *prime_out);
 int zr_is_probable_prime_base2(const uint64_t *n, uint32_t limbs);
 
-/* Sumcheck with a sum-of-products combination function:
- * comb(v) = sum_k coeffs[k] * prod_{q in [offsets[k], offsets[k+1])} v[indices[q]].
+/* Sumcheck with a combination function made of a sum of products times
+ * affine factors:
+ * comb(v) = (sum_k coeffs[k] * prod_{q in [offsets[k], offsets[k+1])} v[indices[q]])
+ *           * prod_f (factor_a[f] + factor_b[f] * v[factor_mles[f]]).
  * mles: n_mles x 2^nvars field elements (Montgomery inner, L limbs). */
 typedef struct {
     uint32_t degree, n_mles, n_products;
@@ -98,6 +100,9 @@ typedef struct {
     const uint64_t *coeffs;
     const uint32_t *offsets;
     const uint32_t *indices;
+    uint32_t n_factors;
+    const uint32_t *factor_mles;
+    const uint64_t *factor_a, *factor_b;
 } zr_sc_group;
 int zr_sumcheck_prove(zr_transcript *t, const uint64_t *modulus, uint32_t L, uint32_t nvars,
                       int multi, const zr_sc_group *groups, uint32_t ngroups, uint8_t *proof,

@@ -331,6 +331,47 @@ def test_gpu_multi_degree_matches_oracle(oracle, zipgpu, ctx, L):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("L", [1, 2, 3, 4])
+def test_gpu_factored_groups_match_oracle(oracle, zipgpu, ctx, L):
+    """Sums of products times 1..3 random affine factors, single and multi-degree,
+    with the MLEs on the host and on the device."""
+    import torch
+
+    p, nv = MODULI[L], 9
+    rng = np.random.default_rng(300 + L)
+    groups = []
+    for nf in (1, 2, 3):
+        deg, vals, prods = rand_poly(rng, nv, p, L, (1, 3), 4)
+        g = group_arrays(deg, vals, prods, p, L)
+        factors = [(to_mont(int.from_bytes(rng.bytes(8 * L), "little"), p, L),
+                    to_mont(int.from_bytes(rng.bytes(8 * L), "little"), p, L),
+                    int(rng.integers(0, g[1].shape[0]))) for _ in range(nf)]
+        groups.append((deg + nf, g[1], g[2], factors))
+    for multi, gs in ((False, groups[:1]), (True, groups)):
+        want = oracle.sumcheck_prove(oracle.Transcript(), p, L, nv, gs, multi)
+        for on_device in (False, True):
+            keep = []
+            zgroups = []
+            for deg, mles, prods, factors in gs:
+                if on_device:
+                    d = torch.from_numpy(mles.reshape(-1).view(np.uint8).copy()).cuda()
+                    keep.append(d)
+                    zgroups.append(zipgpu.SumcheckGroup(deg, d.data_ptr(), prods,
+                                                        n_mles=mles.shape[0], factors=factors))
+                else:
+                    zgroups.append(zipgpu.SumcheckGroup(deg, mles, prods, factors=factors))
+            torch.cuda.synchronize()
+            t = zipgpu.PcsProverTranscript()
+            if multi:
+                got = zipgpu.MultiDegreeSumcheck.prove_as_subprotocol(t, p, L, nv, zgroups, ctx)
+            else:
+                got = zipgpu.MLSumcheck.prove_as_subprotocol(t, p, L, nv, zgroups[0], ctx)
+            t.close()
+            assert got[0] == want[0]
+            assert (got[1] == want[1]).all() and (got[2] == want[2]).all()
+
+
+@pytest.mark.gpu
 def test_gpu_sumcheck_edge_cases(oracle, zipgpu, ctx):
     """Zero polynomial, a constant polynomial, degree 8, and inners at p - 1."""
     L, nv = 4, 5
@@ -388,3 +429,8 @@ def test_gpu_sumcheck_rejects_bad_input(zipgpu, ctx):
         _gpu_prove(zipgpu, ctx, p, L, 3, [(2, mles, [(one, [0, 2])])], False)
     with pytest.raises(zipgpu.ZipError):  # degree above the kernel's limit
         _gpu_prove(zipgpu, ctx, p, L, 3, [(9, mles, [(one, [0, 1])])], False)
+    t = zipgpu.PcsProverTranscript()
+    with pytest.raises(zipgpu.ZipError):  # factor index out of range
+        zipgpu.MLSumcheck.prove_as_subprotocol(
+            t, p, L, 3, zipgpu.SumcheckGroup(3, mles, [(one, [0, 1])], factors=[(one, one, 2)]), ctx)
+    t.close()

@@ -7,8 +7,11 @@ folded = sum_k alpha^k g_k, the g_k linear in the columns.  Field arithmetic is
 exact, so expanding it gives the same field value at every point:
     comb = sum_j A_j * eq * v_j - sum_j A_j * sel * eq * v_j,
     A_j = sum_k alpha^k c_kj.
-The tests check the expansion against the reference formula with Python
-integers, then run the sumcheck on it with the oracle and on the GPU.
+zg_sumcheck_prove also takes the reference's own shape, a sum of one-MLE
+products times the affine factors eq_r and (1 - sel) (about a fifth of the
+field multiplies).  The tests check both forms against the reference formula
+with Python integers, check that they give the same proof, and run the sumcheck
+on them with the oracle and on the GPU.
 """
 import numpy as np
 import pytest
@@ -51,6 +54,20 @@ def expanded_products(alpha, p):
         prods.append((A[j], [EQ, j]))
         prods.append(((-A[j]) % p, [SEL, EQ, j]))
     return prods
+
+
+def factored_group(alpha, p, L, mles):
+    """The same comb in the reference's own shape: folded(v) as one-MLE products,
+    times the factors eq_r (0 + 1 * eq) and (1 - sel) (1 + (p - 1) * sel)."""
+    A = {}
+    power = 1
+    for c in constraints():
+        for j, k in c.items():
+            A[j] = (A.get(j, 0) + power * k) % p
+        power = power * alpha % p
+    prods = [(to_mont(A[j], p, L), [j]) for j in sorted(A)]
+    factors = [(0, to_mont(1, p, L), EQ), (to_mont(1, p, L), to_mont(p - 1, p, L), SEL)]
+    return (3, mles, prods, factors)
 
 
 def to_mont(v, p, L):
@@ -118,6 +135,42 @@ def test_cpr_sumcheck_oracle_subclaim(oracle):
     claimed = int.from_bytes(proof[-8 * L:], "little") * pow(1 << (64 * L), -1, p) % p
     want = sum(reference_comb([col[x] for col in vals], alpha, p) for x in range(1 << nv)) % p
     assert claimed == want
+
+
+def test_cpr_factored_form_equals_expanded(oracle):
+    """The factored comb has the same value everywhere, so the proofs are equal."""
+    L, nv = 3, 5
+    p = field_prime(oracle, L)
+    rng = np.random.default_rng(24)
+    alpha = int.from_bytes(rng.bytes(24), "little") % p
+    vals, group = cpr_group(rng, nv, p, L, alpha)
+    fgroup = factored_group(alpha, p, L, group[1])
+    for _ in range(10):
+        v = [int.from_bytes(rng.bytes(24), "little") % p for _ in range(35)]
+        got = oracle.sumcheck_comb(p, L, fgroup,
+                                   np.array([limbs(to_mont(x, p, L), L) for x in v], np.uint64))
+        got_v = sum(int(w) << (64 * i) for i, w in enumerate(got)) * pow(1 << (64 * L), -1, p) % p
+        assert got_v == reference_comb(v, alpha, p)
+    want = oracle.sumcheck_prove(oracle.Transcript(), p, L, nv, [group], True)
+    got = oracle.sumcheck_prove(oracle.Transcript(), p, L, nv, [fgroup], True)
+    assert got[0] == want[0] and (got[2] == want[2]).all()
+
+
+@pytest.mark.gpu
+def test_cpr_factored_gpu_matches_oracle(oracle, zipgpu, ctx):
+    L, nv = 3, 11
+    p = field_prime(oracle, L)
+    rng = np.random.default_rng(25)
+    alpha = int.from_bytes(rng.bytes(24), "little") % p
+    _vals, group = cpr_group(rng, nv, p, L, alpha)
+    fgroup = factored_group(alpha, p, L, group[1])
+    want = oracle.sumcheck_prove(oracle.Transcript(), p, L, nv, [fgroup], True)
+    t = zipgpu.PcsProverTranscript()
+    got = zipgpu.MultiDegreeSumcheck.prove_as_subprotocol(
+        t, p, L, nv, [zipgpu.SumcheckGroup(3, fgroup[1], fgroup[2], factors=fgroup[3])], ctx)
+    t.close()
+    assert got[0] == want[0]
+    assert (got[1] == want[1]).all() and (got[2] == want[2]).all()
 
 
 @pytest.mark.gpu

@@ -222,7 +222,7 @@ cudaError_t ctx_sync(zg_ctx *ctx) {
 void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool) {
     ctx->pool = pool;
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
-                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out}) {
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena}) {
         b->pool = pool;
         b->pool_stream = ctx->stream;
     }
@@ -231,14 +231,14 @@ void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool) {
 size_t ctx_scratch_bytes(const zg_ctx *ctx) {
     size_t n = 0;
     for (const DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
-                            &ctx->wprime, &ctx->prove_in, &ctx->prove_out})
+                            &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena})
         n += b->cap;
     return n;
 }
 
 void ctx_scratch_release(zg_ctx *ctx) {
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
-                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out})
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena})
         b->release();
 }
 

@@ -1,16 +1,19 @@
 // PIOP sumcheck prover on the GPU (piop/src/sumcheck.rs:163-215,
 // sumcheck/prover.rs:95-247, sumcheck/multi_degree.rs:259-355) for
 // combination functions of the form
-//   comb(v) = sum_k coeff_k * prod_{i in S_k} v_i,
-// the form of the reference's test comb functions (sumcheck/tests/utils.rs:60-80);
-// the BigLinear combined-polynomial comb_fn and the multipoint-evaluation
-// product expand into it.  MLE values are field elements in Montgomery form
-// (the reference's DenseMultilinearExtension<F::Inner>), layout [mle][x][limb].
+//   comb(v) = (sum_k coeff_k * prod_{i in S_k} v_i) * prod_f (a_f + b_f * v_{m_f}),
+// a sum of products (the reference's test comb functions, sumcheck/tests/
+// utils.rs:60-80) times affine factors (the combined-polynomial resolver's
+// (1 - selector) * eq_r, combined_poly_resolver.rs:158-172).  MLE values are
+// field elements in Montgomery form (DenseMultilinearExtension<F::Inner>),
+// layout [mle][x][limb].
 //
 // Round i evaluates P_i(t) = sum_b comb(v_b + t (w_b - v_b)) at t = 0..deg
-// over the pairs (v_b, w_b) = (m[2b], m[2b+1]), then every MLE is folded at
-// the challenge: m'[b] = m[2b] + r (m[2b+1] - m[2b]).  Field addition is exact,
-// so the order of the sums is free.
+// over the pairs (v_b, w_b) = (m[2b], m[2b+1]) of the MLEs folded at the
+// previous challenge, m'[b] = m[2b] + r (m[2b+1] - m[2b]).  One kernel per
+// round does both: each thread folds its four entries of the previous round
+// into its pair, writes the pair, and evaluates the comb on it.  Field
+// addition is exact, so the order of the sums is free.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -20,7 +23,9 @@
 namespace zg {
 namespace {
 
-constexpr int kScThreads = 128;
+constexpr int kScThreads = 256;
+constexpr int kScSubMax = 4;           // threads per pair when pairs are few
+constexpr size_t kScSplitBelow = 1u << 19;  // pairs below which a pair is split
 constexpr int kScMaxDeg = 8;
 
 // fix_variables_with_config (poly/src/mle/dense.rs:243-279), one variable.
@@ -44,65 +49,187 @@ __global__ void k_sc_fold(const uint64_t *__restrict__ in, uint64_t *__restrict_
     for (int w = 0; w < L; w++) d[w] = o[w];
 }
 
-// One round polynomial: block-level partial sums of P(t), t = 0..D.
-// Products: coeffs [n_products][L], offsets [n_products+1], indices.
-template <int L, int D>
-__global__ void __launch_bounds__(kScThreads) k_sc_eval(const uint64_t *__restrict__ m, size_t n,
-                                                        const uint64_t *__restrict__ coeffs,
-                                                        const uint32_t *__restrict__ offsets,
-                                                        const uint32_t *__restrict__ indices,
-                                                        uint32_t n_products, FieldCfg f,
-                                                        uint64_t *__restrict__ partials) {
-    __shared__ uint64_t red[kScThreads][(D + 1) * L];
-    const size_t half = n / 2;
-    const size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+// The combination function of one group, in device memory.
+struct ScComb {
+    const uint64_t *coeffs;   // [n_products][L]
+    const uint32_t *offsets;  // [n_products + 1]
+    const uint32_t *indices;
+    const uint32_t *fmles;    // [n_factors]
+    const uint64_t *fa, *fb;  // [n_factors][L]
+    uint32_t n_products, n_factors;
+};
+
+template <int L>
+__device__ __forceinline__ void load_el(const uint64_t *p, uint64_t (&v)[L]) {
+#pragma unroll
+    for (int w = 0; w < L; w++) v[w] = p[w];
+}
+
+// One round for one group: (fold) and the block's partial sums of P(t),
+// t = 0..D.  src: K MLEs of src_len entries; with fold, the round's MLEs (half
+// as long) are written to dst first.  kScSub consecutive threads share a pair:
+// each folds every kScSub-th MLE and evaluates every kScSub-th product, their
+// sums of products are combined by shuffles, and the first applies the factors.
+template <int L, int D, int kScSub>
+__global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restrict__ src,
+                                                         size_t src_len, uint64_t *__restrict__ dst,
+                                                         int fold, const uint64_t *__restrict__ r,
+                                                         uint32_t K, ScComb c, FieldCfg f,
+                                                         uint64_t *__restrict__ partials) {
+    __shared__ uint64_t red[kScThreads / 32][(D + 1) * L];
+    const size_t len = fold ? src_len / 2 : src_len, half = len / 2;
+    const uint32_t sub = threadIdx.x % kScSub;
+    const size_t b = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / kScSub;
+    const bool active = b < half;
     uint64_t ev[D + 1][L];
+#pragma unroll
     for (int t = 0; t <= D; t++)
+#pragma unroll
         for (int w = 0; w < L; w++) ev[t][w] = 0;
-    if (b < half) {
-        for (uint32_t k = 0; k < n_products; k++) {
+    if (active && fold) {
+        uint64_t rr[L];
+        load_el<L>(r, rr);
+        for (uint32_t j = sub; j < K; j += kScSub) {
+                const uint64_t *q = src + ((size_t)j * src_len + 4 * b) * L;
+                uint64_t *o = dst + ((size_t)j * len + 2 * b) * L;
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    uint64_t a0[L], a1[L], pr[L];
+                    load_el<L>(q + 2 * e * L, a0);
+                    load_el<L>(q + (2 * e + 1) * L, a1);
+                    fsub<L>(a1, a0, f.p);
+                    fmul<L>(rr, a1, f.p, f.n0, pr);
+                    fadd<L>(a0, pr, f.p);
+#pragma unroll
+                for (int w = 0; w < L; w++) o[e * L + w] = a0[w];
+            }
+        }
+    }
+    __syncwarp();  // the pair's folded MLEs, written by its kScSub threads, are visible
+    const uint64_t *m = fold ? dst : src;
+    if (active) {
+        // this thread's share of the sum of products at t = 0..D
+        for (uint32_t k = sub; k < c.n_products; k += kScSub) {
             uint64_t pr[D + 1][L];
+            uint64_t cf[L];
+            load_el<L>(c.coeffs + (size_t)k * L, cf);
+#pragma unroll
             for (int t = 0; t <= D; t++)
-                for (int w = 0; w < L; w++) pr[t][w] = coeffs[(size_t)k * L + w];
-            for (uint32_t q = offsets[k]; q < offsets[k + 1]; q++) {
-                const uint64_t *v0 = m + ((size_t)indices[q] * n + 2 * b) * L, *v1 = v0 + L;
+#pragma unroll
+                for (int w = 0; w < L; w++) pr[t][w] = cf[w];
+            for (uint32_t q = c.offsets[k]; q < c.offsets[k + 1]; q++) {
                 uint64_t cur[L], st[L];
-                for (int w = 0; w < L; w++) {
-                    cur[w] = v0[w];
-                    st[w] = v1[w];
-                }
-                fsub<L>(st, v0, f.p);
+                const uint64_t *v = m + ((size_t)c.indices[q] * len + 2 * b) * L;
+                load_el<L>(v, cur);
+                load_el<L>(v + L, st);
+                fsub<L>(st, cur, f.p);
+#pragma unroll
                 for (int t = 0; t <= D; t++) {
                     uint64_t o[L];
                     fmul<L>(pr[t], cur, f.p, f.n0, o);
+#pragma unroll
                     for (int w = 0; w < L; w++) pr[t][w] = o[w];
-                    fadd<L>(cur, st, f.p);
+                    if (t < D) fadd<L>(cur, st, f.p);
                 }
             }
+#pragma unroll
             for (int t = 0; t <= D; t++) fadd<L>(ev[t], pr[t], f.p);
         }
     }
-    for (int t = 0; t <= D; t++)
-        for (int w = 0; w < L; w++) red[threadIdx.x][t * L + w] = ev[t][w];
-    __syncthreads();
-    for (int h = kScThreads / 2; h > 0; h >>= 1) {
-        if ((int)threadIdx.x < h)
-            for (int t = 0; t <= D; t++) fadd<L>(&red[threadIdx.x][t * L], &red[threadIdx.x + h][t * L], f.p);
-        __syncthreads();
+    // the pair's full sum of products, in all its threads
+#pragma unroll
+    for (int off = 1; off < kScSub; off <<= 1) {
+#pragma unroll
+        for (int t = 0; t <= D; t++) {
+            uint64_t o[L];
+#pragma unroll
+            for (int w = 0; w < L; w++) o[w] = __shfl_xor_sync(0xffffffffu, ev[t][w], off);
+            fadd<L>(ev[t], o, f.p);
+        }
     }
-    if (threadIdx.x == 0)
-        for (int e = 0; e < (D + 1) * L; e++) partials[(size_t)blockIdx.x * (D + 1) * L + e] = red[0][e];
+    if (sub != 0) {
+#pragma unroll
+        for (int t = 0; t <= D; t++)
+#pragma unroll
+            for (int w = 0; w < L; w++) ev[t][w] = 0;
+    } else if (active) {
+        // affine factors a + b * v
+        for (uint32_t q = 0; q < c.n_factors; q++) {
+            uint64_t cur[L], st[L], fa[L], fbv[L];
+            const uint64_t *v = m + ((size_t)c.fmles[q] * len + 2 * b) * L;
+            load_el<L>(v, cur);
+            load_el<L>(v + L, st);
+            fsub<L>(st, cur, f.p);
+            load_el<L>(c.fa + (size_t)q * L, fa);
+            load_el<L>(c.fb + (size_t)q * L, fbv);
+#pragma unroll
+            for (int t = 0; t <= D; t++) {
+                uint64_t fv[L], o[L];
+                fmul<L>(fbv, cur, f.p, f.n0, fv);
+                fadd<L>(fv, fa, f.p);
+                fmul<L>(ev[t], fv, f.p, f.n0, o);
+#pragma unroll
+                for (int w = 0; w < L; w++) ev[t][w] = o[w];
+                if (t < D) fadd<L>(cur, st, f.p);
+            }
+        }
+    }
+    // warp tree reduction, then across the block's warps
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int t = 0; t <= D; t++) {
+            uint64_t o[L];
+#pragma unroll
+            for (int w = 0; w < L; w++) o[w] = __shfl_down_sync(0xffffffffu, ev[t][w], off);
+            fadd<L>(ev[t], o, f.p);
+        }
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t <= D; t++)
+#pragma unroll
+            for (int w = 0; w < L; w++) red[warp][t * L + w] = ev[t][w];
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t nw = blockDim.x / 32;
+#pragma unroll
+        for (int t = 0; t <= D; t++)
+#pragma unroll
+            for (int w = 0; w < L; w++) ev[t][w] = lane < nw ? red[lane][t * L + w] : 0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+            for (int t = 0; t <= D; t++) {
+                uint64_t o[L];
+#pragma unroll
+                for (int w = 0; w < L; w++) o[w] = __shfl_down_sync(0xffffffffu, ev[t][w], off);
+                fadd<L>(ev[t], o, f.p);
+            }
+        }
+        if (lane == 0)
+#pragma unroll
+            for (int t = 0; t <= D; t++)
+#pragma unroll
+                for (int w = 0; w < L; w++) partials[((size_t)blockIdx.x * (D + 1) + t) * L + w] = ev[t][w];
+    }
 }
 
 template <int L>
-zg_status launch_eval_d(zg_ctx *ctx, int D, const uint64_t *m, size_t n, const uint64_t *coeffs,
-                        const uint32_t *offsets, const uint32_t *indices, uint32_t np,
-                        const FieldCfg &f, uint64_t *partials, unsigned blocks, cudaStream_t s) {
-    ZG_KBEGIN(ctx, s, "k_sc_eval");
+zg_status launch_round(zg_ctx *ctx, int D, int sub, const uint64_t *src, size_t src_len,
+                       uint64_t *dst, bool fold, const uint64_t *r, uint32_t K, const ScComb &c,
+                       const FieldCfg &f, uint64_t *partials, unsigned blocks, cudaStream_t s) {
+    ZG_KBEGIN(ctx, s, "k_sc_round");
 #define ZG_SC_CASE(DV)                                                                            \
     case DV:                                                                                      \
-        k_sc_eval<L, DV><<<blocks, kScThreads, 0, s>>>(m, n, coeffs, offsets, indices, np, f,     \
-                                                       partials);                                 \
+        if (sub == 1)                                                                             \
+            k_sc_round<L, DV, 1><<<blocks, kScThreads, 0, s>>>(src, src_len, dst, fold ? 1 : 0, r, \
+                                                               K, c, f, partials);                \
+        else                                                                                      \
+            k_sc_round<L, DV, kScSubMax><<<blocks, kScThreads, 0, s>>>(src, src_len, dst,         \
+                                                                       fold ? 1 : 0, r, K, c, f,  \
+                                                                       partials);                 \
         break;
     switch (D) {
         ZG_SC_CASE(0)
@@ -133,27 +260,14 @@ zg_status launch_fold(zg_ctx *ctx, const uint64_t *in, uint64_t *out, uint32_t K
     return ZG_OK;
 }
 
-// Device allocations of one proof, released together.
-struct DevAllocs {
-    std::vector<void *> v;
-    void *get(size_t bytes) {
-        void *p = nullptr;
-        if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
-        v.push_back(p);
-        return p;
-    }
-    ~DevAllocs() {
-        for (void *p : v) cudaFree(p);
-    }
-};
-
+// Per-group device state, carved out of the context's sumcheck arena.
 struct GroupDev {
-    uint32_t degree = 0, K = 0, np = 0;
-    uint64_t *buf[2] = {nullptr, nullptr};  // ping-pong MLE arrays
-    uint64_t *coeffs = nullptr;
-    uint32_t *offsets = nullptr, *indices = nullptr;
+    uint32_t degree = 0, K = 0;
+    const uint64_t *in = nullptr;  // round-0 MLEs (the caller's device memory, or a staged copy)
+    uint64_t *buf[2] = {nullptr, nullptr};  // folded MLEs, alternating by round parity
+    uint64_t *partials = nullptr;
+    ScComb comb{};
 };
-
 
 // get_field_challenge (transcript/src/traits.rs:337-341): XOF of the inner's
 // byte length read as an integer and converted to Montgomery form.
@@ -173,6 +287,8 @@ void f_from_u64_host(const FieldCfg &f, uint64_t v, uint64_t *out) {
     from_signed<L>(x, 2, f, out);
 }
 
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
 template <int L>
 zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int multi,
                            const zg_sumcheck_group *groups, uint32_t ng, int on_device,
@@ -184,67 +300,104 @@ zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int mu
     const size_t fb = 8 * L;
     // proof size and validation
     size_t need = fb + (multi ? 8 + 4 * (size_t)ng : 4) + fb * ng;
+    uint32_t maxd = 0;
     for (uint32_t g = 0; g < ng; g++) {
-        if (groups[g].degree > kScMaxDeg || groups[g].n_mles == 0) {
-            set_error("sumcheck group %u: degree %u (max %d) or no MLEs", g, groups[g].degree, kScMaxDeg);
+        const zg_sumcheck_group &G = groups[g];
+        if (G.degree > kScMaxDeg || G.n_mles == 0 || (G.n_products && (!G.coeffs || !G.offsets ||
+                                                                     !G.indices)) ||
+            (G.n_factors && (!G.factor_mles || !G.factor_a || !G.factor_b)) || !G.mles) {
+            set_error("sumcheck group %u: degree %u (max %d), no MLEs or missing arrays", g, G.degree,
+                      kScMaxDeg);
             return ZG_ERR_INVALID_PARAM;
         }
-        for (uint32_t k = 0; k < groups[g].n_products; k++)
-            for (uint32_t q = groups[g].offsets[k]; q < groups[g].offsets[k + 1]; q++)
-                if (groups[g].indices[q] >= groups[g].n_mles) {
-                    set_error("sumcheck group %u: product %u uses MLE %u of %u", g, k,
-                              groups[g].indices[q], groups[g].n_mles);
+        for (uint32_t k = 0; k < G.n_products; k++)
+            for (uint32_t q = G.offsets[k]; q < G.offsets[k + 1]; q++)
+                if (G.indices[q] >= G.n_mles) {
+                    set_error("sumcheck group %u: product %u uses MLE %u of %u", g, k, G.indices[q],
+                              G.n_mles);
                     return ZG_ERR_INVALID_PARAM;
                 }
-        need += (size_t)nvars * (fb * groups[g].degree + (multi ? 0 : 4));
+        for (uint32_t q = 0; q < G.n_factors; q++)
+            if (G.factor_mles[q] >= G.n_mles) {
+                set_error("sumcheck group %u: factor %u uses MLE %u of %u", g, q, G.factor_mles[q],
+                          G.n_mles);
+                return ZG_ERR_INVALID_PARAM;
+            }
+        need += (size_t)nvars * (fb * G.degree + (multi ? 0 : 4));
+        maxd = std::max(maxd, G.degree);
     }
     if (*proof_len < need) {
         *proof_len = need;
         set_error("sumcheck proof buffer too small (%zu bytes needed)", need);
         return ZG_ERR_BUFFER_TOO_SMALL;
     }
-    // device state
+    // arena: per group [staged input][fold buffers][comb][partials], then r
+    // threads per pair in a round with `pairs` pairs, and that round's blocks
+    auto sub_of = [](size_t pairs) { return pairs < kScSplitBelow ? kScSubMax : 1; };
+    auto blocks_of = [&](size_t pairs) {
+        return (unsigned)std::max<size_t>(1, (pairs * sub_of(pairs) + kScThreads - 1) / kScThreads);
+    };
+    unsigned max_blocks = 1;
+    for (size_t pairs = n / 2; pairs >= 1; pairs /= 2) max_blocks = std::max(max_blocks, blocks_of(pairs));
+    std::vector<size_t> off_in(ng), off_b0(ng), off_b1(ng), off_meta(ng), off_part(ng);
+    size_t total = 0;
+    for (uint32_t g = 0; g < ng; g++) {
+        const zg_sumcheck_group &G = groups[g];
+        const size_t nidx = G.n_products ? G.offsets[G.n_products] : 0;
+        off_in[g] = total;
+        if (!on_device) total = align256(total + (size_t)G.n_mles * n * fb);
+        off_b1[g] = total;  // rounds 1, 3, ...: K x n/2
+        total = align256(total + (size_t)G.n_mles * std::max<size_t>(n / 2, 1) * fb);
+        off_b0[g] = total;  // rounds 2, 4, ... and the final fold: K x max(n/4, 1)
+        total = align256(total + (size_t)G.n_mles * std::max<size_t>(n / 4, 1) * fb);
+        off_meta[g] = total;
+        total = align256(total + (size_t)G.n_products * fb + 4 * ((size_t)G.n_products + 1) +
+                         4 * nidx + 4 * (size_t)G.n_factors + 2 * fb * G.n_factors + 64);
+        off_part[g] = total;
+        total = align256(total + (size_t)max_blocks * (G.degree + 1) * fb);
+    }
+    const size_t off_r = total;
+    total += 256;
+    ZG_TRY(ctx->sc_arena.ensure(total));
+    ZG_TRY(ctx->pin_in.ensure(256));
+    ZG_TRY(ctx->pin_out.ensure((size_t)ng * max_blocks * (maxd + 1) * fb));
+    uint8_t *arena = ctx->sc_arena.as<uint8_t>();
+    uint64_t *r_d = reinterpret_cast<uint64_t *>(arena + off_r);
     std::vector<GroupDev> gd(ng);
-    DevAllocs allocs;
-    auto dalloc = [&](size_t bytes) { return allocs.get(bytes); };
-    uint32_t maxd = 0;
     for (uint32_t g = 0; g < ng; g++) {
         const zg_sumcheck_group &G = groups[g];
         GroupDev &D = gd[g];
         D.degree = G.degree;
         D.K = G.n_mles;
-        D.np = G.n_products;
-        maxd = std::max(maxd, G.degree);
-        const size_t mbytes = (size_t)G.n_mles * n * fb;
-        D.buf[0] = static_cast<uint64_t *>(dalloc(mbytes));
-        D.buf[1] = static_cast<uint64_t *>(dalloc(mbytes / 2 + fb * G.n_mles));
-        D.coeffs = static_cast<uint64_t *>(dalloc((size_t)G.n_products * fb));
-        D.offsets = static_cast<uint32_t *>(dalloc(4 * ((size_t)G.n_products + 1)));
+        if (on_device) {
+            D.in = static_cast<const uint64_t *>(G.mles);
+        } else {
+            uint64_t *in = reinterpret_cast<uint64_t *>(arena + off_in[g]);
+            ZG_CUDA(cudaMemcpyAsync(in, G.mles, (size_t)G.n_mles * n * fb, cudaMemcpyHostToDevice, s));
+            D.in = in;
+        }
+        D.buf[1] = reinterpret_cast<uint64_t *>(arena + off_b1[g]);
+        D.buf[0] = reinterpret_cast<uint64_t *>(arena + off_b0[g]);
+        D.partials = reinterpret_cast<uint64_t *>(arena + off_part[g]);
+        // comb metadata: coeffs | fa | fb | offsets | indices | fmles
+        uint8_t *m = arena + off_meta[g];
         const size_t nidx = G.n_products ? G.offsets[G.n_products] : 0;
-        D.indices = static_cast<uint32_t *>(dalloc(4 * std::max<size_t>(nidx, 1)));
-        if (!D.buf[0] || !D.buf[1] || !D.coeffs || !D.offsets || !D.indices) {
-            set_error("sumcheck: device allocation failed");
-            return ZG_ERR_OOM;
-        }
-        cudaMemcpyAsync(D.buf[0], G.mles, mbytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+        uint64_t *cf = reinterpret_cast<uint64_t *>(m);
+        uint64_t *fa = cf + (size_t)G.n_products * L, *fbv = fa + (size_t)G.n_factors * L;
+        uint32_t *offs = reinterpret_cast<uint32_t *>(fbv + (size_t)G.n_factors * L);
+        uint32_t *idx = offs + G.n_products + 1, *fm = idx + nidx;
         if (G.n_products) {
-            cudaMemcpyAsync(D.coeffs, G.coeffs, (size_t)G.n_products * fb, cudaMemcpyHostToDevice, s);
-            cudaMemcpyAsync(D.offsets, G.offsets, 4 * ((size_t)G.n_products + 1), cudaMemcpyHostToDevice, s);
-            cudaMemcpyAsync(D.indices, G.indices, 4 * nidx, cudaMemcpyHostToDevice, s);
+            ZG_CUDA(cudaMemcpyAsync(cf, G.coeffs, (size_t)G.n_products * fb, cudaMemcpyHostToDevice, s));
+            ZG_CUDA(cudaMemcpyAsync(offs, G.offsets, 4 * ((size_t)G.n_products + 1), cudaMemcpyHostToDevice, s));
+            ZG_CUDA(cudaMemcpyAsync(idx, G.indices, 4 * nidx, cudaMemcpyHostToDevice, s));
         }
+        if (G.n_factors) {
+            ZG_CUDA(cudaMemcpyAsync(fa, G.factor_a, (size_t)G.n_factors * fb, cudaMemcpyHostToDevice, s));
+            ZG_CUDA(cudaMemcpyAsync(fbv, G.factor_b, (size_t)G.n_factors * fb, cudaMemcpyHostToDevice, s));
+            ZG_CUDA(cudaMemcpyAsync(fm, G.factor_mles, 4 * (size_t)G.n_factors, cudaMemcpyHostToDevice, s));
+        }
+        D.comb = ScComb{cf, offs, idx, fm, fa, fbv, G.n_products, G.n_factors};
     }
-    const unsigned max_blocks = (unsigned)std::max<size_t>(1, (n / 2 + kScThreads - 1) / kScThreads);
-    uint64_t *partials = static_cast<uint64_t *>(dalloc((size_t)ng * max_blocks * (maxd + 1) * fb));
-    uint64_t *r_d = static_cast<uint64_t *>(dalloc(fb));
-    if (!partials || !r_d) {
-        set_error("sumcheck: device allocation failed");
-        return ZG_ERR_OOM;
-    }
-    if (cudaGetLastError() != cudaSuccess) {
-        set_error("sumcheck: upload failed");
-        return ZG_ERR_CUDA;
-    }
-    std::vector<uint64_t> hpart((size_t)ng * max_blocks * (maxd + 1) * L);
     // transcript header
     uint64_t fe[4];
     f_from_u64_host<L>(f, nvars, fe);
@@ -258,36 +411,33 @@ zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int mu
         }
     std::vector<uint64_t> msgs((size_t)ng * nvars * (maxd + 1) * L, 0), claimed((size_t)ng * L, 0);
     uint64_t r[4] = {0, 0, 0, 0};
-    size_t len = n;
-    int cur = 0;
+    uint64_t *hr = ctx->pin_in.as<uint64_t>();
+    uint64_t *hpart = ctx->pin_out.as<uint64_t>();
+    std::vector<const uint64_t *> cur(ng);
+    for (uint32_t g = 0; g < ng; g++) cur[g] = gd[g].in;
+    size_t src_len = n;
     for (uint32_t rd = 0; rd < nvars; rd++) {
-        if (rd > 0) {
-            for (uint32_t g = 0; g < ng; g++) {
-                zg_status st = launch_fold<L>(ctx, gd[g].buf[cur], gd[g].buf[cur ^ 1], gd[g].K, len / 2, r_d, f, s);
-                if (st != ZG_OK) return st;
-            }
-            cur ^= 1;
-            len /= 2;
-        }
-        const unsigned blocks = (unsigned)std::max<size_t>(1, (len / 2 + kScThreads - 1) / kScThreads);
+        const bool fold = rd > 0;
+        const size_t len = fold ? src_len / 2 : src_len;
+        const unsigned blocks = blocks_of(len / 2);
         for (uint32_t g = 0; g < ng; g++) {
-            zg_status st = launch_eval_d<L>(ctx, (int)gd[g].degree, gd[g].buf[cur], len, gd[g].coeffs,
-                                            gd[g].offsets, gd[g].indices, gd[g].np, f,
-                                            partials + (size_t)g * max_blocks * (maxd + 1) * L, blocks, s);
-            if (st != ZG_OK) return st;
+            uint64_t *dst = gd[g].buf[rd & 1];
+            ZG_TRY(launch_round<L>(ctx, (int)gd[g].degree, sub_of(len / 2), cur[g], src_len, dst, fold,
+                                   r_d, gd[g].K, gd[g].comb, f, gd[g].partials, blocks, s));
+            if (fold) cur[g] = dst;
         }
         for (uint32_t g = 0; g < ng; g++)
-            cudaMemcpyAsync(hpart.data() + (size_t)g * max_blocks * (maxd + 1) * L,
-                            partials + (size_t)g * max_blocks * (maxd + 1) * L,
-                            (size_t)blocks * (gd[g].degree + 1) * fb, cudaMemcpyDeviceToHost, s);
-        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            ZG_CUDA(cudaMemcpyAsync(hpart + (size_t)g * max_blocks * (maxd + 1) * L, gd[g].partials,
+                                    (size_t)blocks * (gd[g].degree + 1) * fb, cudaMemcpyDeviceToHost, s));
+        if (ctx_sync(ctx) != cudaSuccess) {
             set_error("sumcheck round %u failed: %s", rd, cudaGetErrorString(cudaGetLastError()));
             return ZG_ERR_CUDA;
         }
+        src_len = len;
         for (uint32_t g = 0; g < ng; g++) {
             const uint32_t Dg = gd[g].degree;
             std::vector<uint64_t> ev((size_t)(Dg + 1) * L, 0);
-            const uint64_t *hp = hpart.data() + (size_t)g * max_blocks * (maxd + 1) * L;
+            const uint64_t *hp = hpart + (size_t)g * max_blocks * (maxd + 1) * L;
             for (unsigned bk = 0; bk < blocks; bk++)
                 for (uint32_t tt = 0; tt <= Dg; tt++)
                     fadd<L>(&ev[(size_t)tt * L], hp + ((size_t)bk * (Dg + 1) + tt) * L, f.p);
@@ -306,20 +456,21 @@ zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int mu
         field_challenge<L>(t, r);
         tr_absorb_field(t, r);
         if (point_out) std::memcpy(point_out + (size_t)rd * L, r, fb);
-        cudaMemcpyAsync(r_d, r, fb, cudaMemcpyHostToDevice, s);
+        std::memcpy(hr, r, fb);  // the stream is idle here: safe to overwrite
+        ZG_CUDA(cudaMemcpyAsync(r_d, hr, fb, cudaMemcpyHostToDevice, s));
     }
     // final evaluations of every MLE at the point (the last fold)
     if (finals_out) {
         size_t fo = 0;
         for (uint32_t g = 0; g < ng; g++) {
-            zg_status st = launch_fold<L>(ctx, gd[g].buf[cur], gd[g].buf[cur ^ 1], gd[g].K, 1, r_d, f, s);
-            if (st != ZG_OK) return st;
-            cudaMemcpyAsync(finals_out + fo * L, gd[g].buf[cur ^ 1], (size_t)gd[g].K * fb,
-                            cudaMemcpyDeviceToHost, s);
+            uint64_t *out = gd[g].buf[nvars & 1];
+            ZG_TRY(launch_fold<L>(ctx, cur[g], out, gd[g].K, 1, r_d, f, s));
+            ZG_CUDA(cudaMemcpyAsync(finals_out + fo * L, out, (size_t)gd[g].K * fb,
+                                    cudaMemcpyDeviceToHost, s));
             fo += gd[g].K;
         }
     }
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
+    if (ctx_sync(ctx) != cudaSuccess) {
         set_error("sumcheck final fold failed");
         return ZG_ERR_CUDA;
     }

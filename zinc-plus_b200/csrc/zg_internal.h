@@ -143,6 +143,7 @@ struct zg_ctx {
     zg::DevBuf wprime;    // alpha-projected rows (CombR)
     zg::DevBuf prove_in;  // small per-prove inputs (alphas, points, coeffs, indices)
     zg::DevBuf prove_out; // b partials, combined row + openings
+    zg::DevBuf sc_arena;  // sumcheck: staged MLEs, fold buffers, comb tables, partials
     zg::HostBuf pin_in, pin_out;
     // kernel timing
     bool timing = false;

@@ -106,7 +106,8 @@ class SumcheckGroupDesc(C.Structure):
 
     _fields_ = [("degree", C.c_uint32), ("n_mles", C.c_uint32), ("n_products", C.c_uint32),
                 ("mles", C.c_void_p), ("coeffs", C.c_void_p), ("offsets", C.c_void_p),
-                ("indices", C.c_void_p)]
+                ("indices", C.c_void_p), ("n_factors", C.c_uint32), ("factor_mles", C.c_void_p),
+                ("factor_a", C.c_void_p), ("factor_b", C.c_void_p)]
 
 
 _lib = None
@@ -606,16 +607,25 @@ class SumcheckGroup:
     sum_k coeff_k * prod_{i in products[k]} mle_i (MultiDegreeSumcheckGroup,
     piop/src/sumcheck/multi_degree.rs:44-67).
 
-    mles: (n_mles, 2^nvars, limbs) uint64 Montgomery inners; products: a list of
-    (coeff_inner, [mle indices]); degree: the longest product.
+    mles: (n_mles, 2^nvars, limbs) uint64 Montgomery inners, or the device address
+    of that array (an int) with n_mles given; products: a list of
+    (coeff_inner, [mle indices]); factors: affine factors (a_inner, b_inner,
+    mle index) that multiply the sum of products; degree: the longest product
+    plus the number of factors.
     """
 
     degree: int
-    mles: np.ndarray
+    mles: object
     products: list
+    n_mles: int = 0
+    factors: list = None
+
+    @property
+    def on_device(self) -> bool:
+        return isinstance(self.mles, int)
 
     def _arrays(self, limbs: int):
-        mles = np.ascontiguousarray(self.mles, dtype=np.uint64)
+        mles = self.mles if self.on_device else np.ascontiguousarray(self.mles, dtype=np.uint64)
         coeffs = np.zeros((max(len(self.products), 1), limbs), np.uint64)
         offsets = np.zeros(len(self.products) + 1, np.uint32)
         idx = []
@@ -626,18 +636,34 @@ class SumcheckGroup:
         indices = np.array(idx or [0], np.uint32)
         return mles, coeffs, offsets, indices
 
+    def _factor_arrays(self, limbs: int):
+        fs = self.factors or []
+        fm = np.array([int(x[2]) for x in fs] or [0], np.uint32)
+        fa = np.array([int_to_limbs(int(x[0]), limbs) for x in fs] or [[0] * limbs], np.uint64)
+        fb = np.array([int_to_limbs(int(x[1]), limbs) for x in fs] or [[0] * limbs], np.uint64)
+        return len(fs), fm, fa, fb
+
 
 def _sumcheck_prove(transcript: PcsProverTranscript, modulus: int, limbs: int, nvars: int,
                     groups: Sequence[SumcheckGroup], multi: bool, ctx: Context | None):
     keep, descs = [], (SumcheckGroupDesc * len(groups))()
     n_mles = 0
+    on_device = all(grp.on_device for grp in groups)
+    if not on_device and any(grp.on_device for grp in groups):
+        raise ValueError("MLEs of all groups must be on the device, or all on the host")
     for g, grp in zip(descs, groups):
         mles, coeffs, offsets, indices = grp._arrays(limbs)
         keep += [mles, coeffs, offsets, indices]
-        g.degree, g.n_mles, g.n_products = grp.degree, mles.shape[0], len(grp.products)
-        g.mles, g.coeffs = mles.ctypes.data, coeffs.ctypes.data
+        k = grp.n_mles if on_device else mles.shape[0]
+        g.degree, g.n_mles, g.n_products = grp.degree, k, len(grp.products)
+        g.mles = mles if on_device else mles.ctypes.data
+        g.coeffs = coeffs.ctypes.data
         g.offsets, g.indices = offsets.ctypes.data, indices.ctypes.data
-        n_mles += mles.shape[0]
+        nf, fm, fa, fb_ = grp._factor_arrays(limbs)
+        keep += [fm, fa, fb_]
+        g.n_factors, g.factor_mles = nf, fm.ctypes.data
+        g.factor_a, g.factor_b = fa.ctypes.data, fb_.ctypes.data
+        n_mles += k
     fb = 8 * limbs
     cap = fb + 8 + 4 * len(groups) + fb * len(groups) + sum(
         nvars * (fb * g.degree + 4) for g in groups)
@@ -647,7 +673,8 @@ def _sumcheck_prove(transcript: PcsProverTranscript, modulus: int, limbs: int, n
     finals = np.zeros((max(n_mles, 1), limbs), np.uint64)
     mod = int_to_limbs(modulus, limbs).tobytes()
     check(lib().zg_sumcheck_prove((ctx or default_context()).handle, transcript.handle,
-                                  C.c_char_p(mod), limbs, nvars, int(multi), descs, len(groups), 0,
+                                  C.c_char_p(mod), limbs, nvars, int(multi), descs, len(groups),
+                                  int(on_device),
                                   proof, C.byref(plen), _ptr(point), _ptr(finals)))
     return proof.raw[: plen.value], point, finals[:n_mles]
 
