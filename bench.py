@@ -696,6 +696,19 @@ def run_commit_case(nv, D):
     return 0
 
 
+def run_sumcheck_case(nv):
+    """One CPR sumcheck proof (2^nv points, device-resident MLEs), twice: a small,
+    fixed launch sequence for ncu captures."""
+    import torch
+    import zipgpu as Z
+
+    ctx = Z.Context(env_int("LOCAL_RANK", 0))
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = run_sumcheck(Z, ctx, torch, stream, nv, 10, False)
+    print(json.dumps({"sumcheck_case": {"num_vars": nv, "ms": out["ms"]}}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -712,6 +725,8 @@ def main():
     ap.add_argument("--serve-workers", type=int, default=4)
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched-commit and serving measurements")
+    ap.add_argument("--sumcheck-case", type=int, metavar="NV",
+                    help="only run the CPR sumcheck at 2^NV points (small case for ncu captures)")
     ap.add_argument("--commit-case", type=int, nargs=2, metavar=("NV", "D"),
                     help="only commit one seeded polynomial twice (small case for ncu captures)")
     args = ap.parse_args()
@@ -719,6 +734,8 @@ def main():
         args.warmup = 3
     if args.commit_case:
         return run_commit_case(*args.commit_case)
+    if args.sumcheck_case:
+        return run_sumcheck_case(args.sumcheck_case)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -24,8 +24,10 @@ namespace zg {
 namespace {
 
 constexpr int kScThreads = 256;
-constexpr int kScSubMax = 4;           // threads per pair when pairs are few
-constexpr size_t kScSplitBelow = 1u << 19;  // pairs below which a pair is split
+// threads per pair: 1 when pairs fill the GPU, more when they do not (each
+// thread's share of a pair is a long chain of dependent field products)
+constexpr int kScSubMid = 4, kScSubMax = 16;
+constexpr size_t kScSplitBelow = 1u << 19, kScSplitMore = 1u << 15;
 constexpr int kScMaxDeg = 8;
 
 // fix_variables_with_config (poly/src/mle/dense.rs:243-279), one variable.
@@ -59,6 +61,43 @@ struct ScComb {
     uint32_t n_products, n_factors;
 };
 
+// A field element passed by value (in registers across calls).
+template <int L>
+struct Fe {
+    uint64_t w[L];
+};
+
+// Out-of-line Montgomery product: one copy of its code for all the call sites
+// of the round kernel.  Inlined at every site, the round kernel is thousands of
+// straight-line instructions that a small round runs once per warp, so its time
+// was instruction-cache misses, not arithmetic.
+template <int L>
+__device__ __noinline__ Fe<L> fmul_nl(Fe<L> a, Fe<L> b, Fe<L> p, uint64_t n0) {
+    Fe<L> o;
+    fmul<L>(a.w, b.w, p.w, n0, o.w);
+    return o;
+}
+
+// OUTLINE: the out-of-line product (small rounds, bound by instruction fetch),
+// else inlined (large rounds, where independent products must overlap).
+template <int L, bool OUTLINE>
+__device__ __forceinline__ void fmul_c(const uint64_t *a, const uint64_t *b, const Fe<L> &p,
+                                       uint64_t n0, uint64_t *out) {
+    if (!OUTLINE) {
+        fmul<L>(a, b, p.w, n0, out);
+        return;
+    }
+    Fe<L> x, y;
+#pragma unroll
+    for (int w = 0; w < L; w++) {
+        x.w[w] = a[w];
+        y.w[w] = b[w];
+    }
+    const Fe<L> o = fmul_nl<L>(x, y, p, n0);
+#pragma unroll
+    for (int w = 0; w < L; w++) out[w] = o.w[w];
+}
+
 template <int L>
 __device__ __forceinline__ void load_el(const uint64_t *p, uint64_t (&v)[L]) {
 #pragma unroll
@@ -77,6 +116,9 @@ __global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restr
                                                          uint32_t K, ScComb c, FieldCfg f,
                                                          uint64_t *__restrict__ partials) {
     __shared__ uint64_t red[kScThreads / 32][(D + 1) * L];
+    Fe<L> pf;
+#pragma unroll
+    for (int w = 0; w < L; w++) pf.w[w] = f.p[w];
     const size_t len = fold ? src_len / 2 : src_len, half = len / 2;
     const uint32_t sub = threadIdx.x % kScSub;
     const size_t b = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / kScSub;
@@ -98,7 +140,7 @@ __global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restr
                     load_el<L>(q + 2 * e * L, a0);
                     load_el<L>(q + (2 * e + 1) * L, a1);
                     fsub<L>(a1, a0, f.p);
-                    fmul<L>(rr, a1, f.p, f.n0, pr);
+                    fmul_c<L, (kScSub == kScSubMax)>(rr, a1, pf, f.n0, pr);
                     fadd<L>(a0, pr, f.p);
 #pragma unroll
                 for (int w = 0; w < L; w++) o[e * L + w] = a0[w];
@@ -126,7 +168,7 @@ __global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restr
 #pragma unroll
                 for (int t = 0; t <= D; t++) {
                     uint64_t o[L];
-                    fmul<L>(pr[t], cur, f.p, f.n0, o);
+                    fmul_c<L, (kScSub == kScSubMax)>(pr[t], cur, pf, f.n0, o);
 #pragma unroll
                     for (int w = 0; w < L; w++) pr[t][w] = o[w];
                     if (t < D) fadd<L>(cur, st, f.p);
@@ -165,9 +207,9 @@ __global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restr
 #pragma unroll
             for (int t = 0; t <= D; t++) {
                 uint64_t fv[L], o[L];
-                fmul<L>(fbv, cur, f.p, f.n0, fv);
+                fmul_c<L, (kScSub == kScSubMax)>(fbv, cur, pf, f.n0, fv);
                 fadd<L>(fv, fa, f.p);
-                fmul<L>(ev[t], fv, f.p, f.n0, o);
+                fmul_c<L, (kScSub == kScSubMax)>(ev[t], fv, pf, f.n0, o);
 #pragma unroll
                 for (int w = 0; w < L; w++) ev[t][w] = o[w];
                 if (t < D) fadd<L>(cur, st, f.p);
@@ -226,6 +268,10 @@ zg_status launch_round(zg_ctx *ctx, int D, int sub, const uint64_t *src, size_t 
         if (sub == 1)                                                                             \
             k_sc_round<L, DV, 1><<<blocks, kScThreads, 0, s>>>(src, src_len, dst, fold ? 1 : 0, r, \
                                                                K, c, f, partials);                \
+        else if (sub == kScSubMid)                                                                \
+            k_sc_round<L, DV, kScSubMid><<<blocks, kScThreads, 0, s>>>(src, src_len, dst,         \
+                                                                       fold ? 1 : 0, r, K, c, f,  \
+                                                                       partials);                 \
         else                                                                                      \
             k_sc_round<L, DV, kScSubMax><<<blocks, kScThreads, 0, s>>>(src, src_len, dst,         \
                                                                        fold ? 1 : 0, r, K, c, f,  \
@@ -333,7 +379,9 @@ zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int mu
     }
     // arena: per group [staged input][fold buffers][comb][partials], then r
     // threads per pair in a round with `pairs` pairs, and that round's blocks
-    auto sub_of = [](size_t pairs) { return pairs < kScSplitBelow ? kScSubMax : 1; };
+    auto sub_of = [](size_t pairs) {
+        return pairs >= kScSplitBelow ? 1 : pairs >= kScSplitMore ? kScSubMid : kScSubMax;
+    };
     auto blocks_of = [&](size_t pairs) {
         return (unsigned)std::max<size_t>(1, (pairs * sub_of(pairs) + kScThreads - 1) / kScThreads);
     };

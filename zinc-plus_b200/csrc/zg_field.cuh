@@ -117,10 +117,123 @@ ZG_HD void fneg(uint64_t *a, const uint64_t *p) {
     for (int i = 0; i < L; i++) a[i] = t[i];
 }
 
-// Montgomery product a*b*R^-1 mod p for a < R, b < p (CIOS).
+#ifdef __CUDA_ARCH__
+// One word step of the CIOS loop (accumulate a*b_i, reduce by m*p), each in
+// one asm block so that its carry chains stay together while independent
+// products interleave.  Generated for N = 2, 4, 6, 8 words.
+template <int N>
+__device__ __forceinline__ void mont_step(uint32_t (&t)[N + 2], const uint32_t (&a)[N],
+                                          const uint32_t (&p)[N], uint32_t bi, uint32_t n0);
+template <int N>
+__device__ __forceinline__ void mont_sub(const uint32_t (&t)[N + 2], const uint32_t (&p)[N],
+                                         uint32_t (&d)[N], uint32_t &top);
+template <>
+__device__ __forceinline__ void mont_step<2>(uint32_t (&t)[4], const uint32_t (&a)[2],
+                                             const uint32_t (&p)[2], uint32_t bi, uint32_t n0) {
+    asm("{\n\t.reg .u32 m;\n\tmad.lo.cc.u32 %0, %4, %8, %0;\n\tmadc.lo.cc.u32 %1, %5, %8, %1;\n\taddc.cc.u32 %2, %2, 0;\n\taddc.u32 %3, %3, 0;\n\tmad.hi.cc.u32 %1, %4, %8, %1;\n\tmadc.hi.cc.u32 %2, %5, %8, %2;\n\taddc.u32 %3, %3, 0;\n\tmul.lo.u32 m, %0, %9;\n\tmad.lo.cc.u32 %0, m, %6, %0;\n\tmadc.lo.cc.u32 %1, m, %7, %1;\n\taddc.cc.u32 %2, %2, 0;\n\taddc.u32 %3, %3, 0;\n\tmad.hi.cc.u32 %1, m, %6, %1;\n\tmadc.hi.cc.u32 %2, m, %7, %2;\n\taddc.u32 %3, %3, 0;\n\t}"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3])
+        : "r"(a[0]), "r"(a[1]), "r"(p[0]), "r"(p[1]), "r"(bi), "r"(n0));
+}
+template <>
+__device__ __forceinline__ void mont_sub<2>(const uint32_t (&t)[4], const uint32_t (&p)[2],
+                                            uint32_t (&d)[2], uint32_t &top) {
+    asm("sub.cc.u32 %0, %3, %6;\n\tsubc.cc.u32 %1, %4, %7;\n\tsubc.u32 %2, %5, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(top)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(p[0]), "r"(p[1]));
+}
+template <>
+__device__ __forceinline__ void mont_step<4>(uint32_t (&t)[6], const uint32_t (&a)[4],
+                                             const uint32_t (&p)[4], uint32_t bi, uint32_t n0) {
+    asm("{\n\t.reg .u32 m;\n\tmad.lo.cc.u32 %0, %6, %14, %0;\n\tmadc.lo.cc.u32 %1, %7, %14, %1;\n\tmadc.lo.cc.u32 %2, %8, %14, %2;\n\tmadc.lo.cc.u32 %3, %9, %14, %3;\n\taddc.cc.u32 %4, %4, 0;\n\taddc.u32 %5, %5, 0;\n\tmad.hi.cc.u32 %1, %6, %14, %1;\n\tmadc.hi.cc.u32 %2, %7, %14, %2;\n\tmadc.hi.cc.u32 %3, %8, %14, %3;\n\tmadc.hi.cc.u32 %4, %9, %14, %4;\n\taddc.u32 %5, %5, 0;\n\tmul.lo.u32 m, %0, %15;\n\tmad.lo.cc.u32 %0, m, %10, %0;\n\tmadc.lo.cc.u32 %1, m, %11, %1;\n\tmadc.lo.cc.u32 %2, m, %12, %2;\n\tmadc.lo.cc.u32 %3, m, %13, %3;\n\taddc.cc.u32 %4, %4, 0;\n\taddc.u32 %5, %5, 0;\n\tmad.hi.cc.u32 %1, m, %10, %1;\n\tmadc.hi.cc.u32 %2, m, %11, %2;\n\tmadc.hi.cc.u32 %3, m, %12, %3;\n\tmadc.hi.cc.u32 %4, m, %13, %4;\n\taddc.u32 %5, %5, 0;\n\t}"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(bi), "r"(n0));
+}
+template <>
+__device__ __forceinline__ void mont_sub<4>(const uint32_t (&t)[6], const uint32_t (&p)[4],
+                                            uint32_t (&d)[4], uint32_t &top) {
+    asm("sub.cc.u32 %0, %5, %10;\n\tsubc.cc.u32 %1, %6, %11;\n\tsubc.cc.u32 %2, %7, %12;\n\tsubc.cc.u32 %3, %8, %13;\n\tsubc.u32 %4, %9, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(top)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]));
+}
+template <>
+__device__ __forceinline__ void mont_step<6>(uint32_t (&t)[8], const uint32_t (&a)[6],
+                                             const uint32_t (&p)[6], uint32_t bi, uint32_t n0) {
+    asm("{\n\t.reg .u32 m;\n\tmad.lo.cc.u32 %0, %8, %20, %0;\n\tmadc.lo.cc.u32 %1, %9, %20, %1;\n\tmadc.lo.cc.u32 %2, %10, %20, %2;\n\tmadc.lo.cc.u32 %3, %11, %20, %3;\n\tmadc.lo.cc.u32 %4, %12, %20, %4;\n\tmadc.lo.cc.u32 %5, %13, %20, %5;\n\taddc.cc.u32 %6, %6, 0;\n\taddc.u32 %7, %7, 0;\n\tmad.hi.cc.u32 %1, %8, %20, %1;\n\tmadc.hi.cc.u32 %2, %9, %20, %2;\n\tmadc.hi.cc.u32 %3, %10, %20, %3;\n\tmadc.hi.cc.u32 %4, %11, %20, %4;\n\tmadc.hi.cc.u32 %5, %12, %20, %5;\n\tmadc.hi.cc.u32 %6, %13, %20, %6;\n\taddc.u32 %7, %7, 0;\n\tmul.lo.u32 m, %0, %21;\n\tmad.lo.cc.u32 %0, m, %14, %0;\n\tmadc.lo.cc.u32 %1, m, %15, %1;\n\tmadc.lo.cc.u32 %2, m, %16, %2;\n\tmadc.lo.cc.u32 %3, m, %17, %3;\n\tmadc.lo.cc.u32 %4, m, %18, %4;\n\tmadc.lo.cc.u32 %5, m, %19, %5;\n\taddc.cc.u32 %6, %6, 0;\n\taddc.u32 %7, %7, 0;\n\tmad.hi.cc.u32 %1, m, %14, %1;\n\tmadc.hi.cc.u32 %2, m, %15, %2;\n\tmadc.hi.cc.u32 %3, m, %16, %3;\n\tmadc.hi.cc.u32 %4, m, %17, %4;\n\tmadc.hi.cc.u32 %5, m, %18, %5;\n\tmadc.hi.cc.u32 %6, m, %19, %6;\n\taddc.u32 %7, %7, 0;\n\t}"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(bi), "r"(n0));
+}
+template <>
+__device__ __forceinline__ void mont_sub<6>(const uint32_t (&t)[8], const uint32_t (&p)[6],
+                                            uint32_t (&d)[6], uint32_t &top) {
+    asm("sub.cc.u32 %0, %7, %14;\n\tsubc.cc.u32 %1, %8, %15;\n\tsubc.cc.u32 %2, %9, %16;\n\tsubc.cc.u32 %3, %10, %17;\n\tsubc.cc.u32 %4, %11, %18;\n\tsubc.cc.u32 %5, %12, %19;\n\tsubc.u32 %6, %13, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(top)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]));
+}
+template <>
+__device__ __forceinline__ void mont_step<8>(uint32_t (&t)[10], const uint32_t (&a)[8],
+                                             const uint32_t (&p)[8], uint32_t bi, uint32_t n0) {
+    asm("{\n\t.reg .u32 m;\n\tmad.lo.cc.u32 %0, %10, %26, %0;\n\tmadc.lo.cc.u32 %1, %11, %26, %1;\n\tmadc.lo.cc.u32 %2, %12, %26, %2;\n\tmadc.lo.cc.u32 %3, %13, %26, %3;\n\tmadc.lo.cc.u32 %4, %14, %26, %4;\n\tmadc.lo.cc.u32 %5, %15, %26, %5;\n\tmadc.lo.cc.u32 %6, %16, %26, %6;\n\tmadc.lo.cc.u32 %7, %17, %26, %7;\n\taddc.cc.u32 %8, %8, 0;\n\taddc.u32 %9, %9, 0;\n\tmad.hi.cc.u32 %1, %10, %26, %1;\n\tmadc.hi.cc.u32 %2, %11, %26, %2;\n\tmadc.hi.cc.u32 %3, %12, %26, %3;\n\tmadc.hi.cc.u32 %4, %13, %26, %4;\n\tmadc.hi.cc.u32 %5, %14, %26, %5;\n\tmadc.hi.cc.u32 %6, %15, %26, %6;\n\tmadc.hi.cc.u32 %7, %16, %26, %7;\n\tmadc.hi.cc.u32 %8, %17, %26, %8;\n\taddc.u32 %9, %9, 0;\n\tmul.lo.u32 m, %0, %27;\n\tmad.lo.cc.u32 %0, m, %18, %0;\n\tmadc.lo.cc.u32 %1, m, %19, %1;\n\tmadc.lo.cc.u32 %2, m, %20, %2;\n\tmadc.lo.cc.u32 %3, m, %21, %3;\n\tmadc.lo.cc.u32 %4, m, %22, %4;\n\tmadc.lo.cc.u32 %5, m, %23, %5;\n\tmadc.lo.cc.u32 %6, m, %24, %6;\n\tmadc.lo.cc.u32 %7, m, %25, %7;\n\taddc.cc.u32 %8, %8, 0;\n\taddc.u32 %9, %9, 0;\n\tmad.hi.cc.u32 %1, m, %18, %1;\n\tmadc.hi.cc.u32 %2, m, %19, %2;\n\tmadc.hi.cc.u32 %3, m, %20, %3;\n\tmadc.hi.cc.u32 %4, m, %21, %4;\n\tmadc.hi.cc.u32 %5, m, %22, %5;\n\tmadc.hi.cc.u32 %6, m, %23, %6;\n\tmadc.hi.cc.u32 %7, m, %24, %7;\n\tmadc.hi.cc.u32 %8, m, %25, %8;\n\taddc.u32 %9, %9, 0;\n\t}"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]), "+r"(t[8]), "+r"(t[9])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]), "r"(bi), "r"(n0));
+}
+template <>
+__device__ __forceinline__ void mont_sub<8>(const uint32_t (&t)[10], const uint32_t (&p)[8],
+                                            uint32_t (&d)[8], uint32_t &top) {
+    asm("sub.cc.u32 %0, %9, %18;\n\tsubc.cc.u32 %1, %10, %19;\n\tsubc.cc.u32 %2, %11, %20;\n\tsubc.cc.u32 %3, %12, %21;\n\tsubc.cc.u32 %4, %13, %22;\n\tsubc.cc.u32 %5, %14, %23;\n\tsubc.cc.u32 %6, %15, %24;\n\tsubc.cc.u32 %7, %16, %25;\n\tsubc.u32 %8, %17, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(top)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]), "r"(t[8]), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]));
+}
+
+// Montgomery product over N 32-bit words, R = 2^(32 N) (CIOS, Koc, Acar and
+// Kaliski 1996), with PTX carry chains: per word b_i, the low halves of a*b_i
+// are added with one carry chain and the high halves, one word up, with a
+// second; the reduction by m*p (m = t_0 * n0 mod 2^32) likewise, then the
+// accumulator shifts down one word.  t < 2p throughout for a < R, b < p, so
+// one conditional subtraction ends it.
+template <int N>
+__device__ __forceinline__ void mont_mul32(const uint32_t (&a)[N], const uint32_t (&b)[N],
+                                           const uint32_t (&p)[N], uint32_t n0, uint32_t (&out)[N]) {
+    uint32_t t[N + 2];
+#pragma unroll
+    for (int i = 0; i < N + 2; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        mont_step<N>(t, a, p, b[i], n0);
+        // t_0 is now zero: shift down one word
+#pragma unroll
+        for (int j = 0; j <= N; j++) t[j] = t[j + 1];
+        t[N + 1] = 0;
+    }
+    // d = t - p over N + 1 words; keep t if that borrows
+    uint32_t d[N], top;
+    mont_sub<N>(t, p, d, top);
+    const bool keep = (top >> 31) != 0;
+#pragma unroll
+    for (int j = 0; j < N; j++) out[j] = keep ? t[j] : d[j];
+}
+#endif
+
+// Montgomery product a*b*R^-1 mod p for a < R, b < p (CIOS).  On the device
+// the 32-bit carry-chain form above; on the host 64-bit limbs.
 template <int L>
 ZG_HD void fmul(const uint64_t *a, const uint64_t *b, const uint64_t *p, uint64_t n0,
                 uint64_t *out) {
+#ifdef __CUDA_ARCH__
+    uint32_t aw[2 * L], bw[2 * L], pw[2 * L], ow[2 * L];
+#pragma unroll
+    for (int i = 0; i < L; i++) {
+        aw[2 * i] = (uint32_t)a[i];
+        aw[2 * i + 1] = (uint32_t)(a[i] >> 32);
+        bw[2 * i] = (uint32_t)b[i];
+        bw[2 * i + 1] = (uint32_t)(b[i] >> 32);
+        pw[2 * i] = (uint32_t)p[i];
+        pw[2 * i + 1] = (uint32_t)(p[i] >> 32);
+    }
+    mont_mul32<2 * L>(aw, bw, pw, (uint32_t)n0, ow);
+#pragma unroll
+    for (int i = 0; i < L; i++) out[i] = (uint64_t)ow[2 * i] | ((uint64_t)ow[2 * i + 1] << 32);
+    return;
+#else
     uint64_t t[L + 2];
     for (int i = 0; i < L + 2; i++) t[i] = 0;
     for (int i = 0; i < L; i++) {
@@ -147,6 +260,7 @@ ZG_HD void fmul(const uint64_t *a, const uint64_t *b, const uint64_t *p, uint64_
     }
     if (t[L] || ucmp<L>(t, p) >= 0) usub<L>(t, p);
     for (int i = 0; i < L; i++) out[i] = t[i];
+#endif
 }
 
 // F::from_with_cfg(&Int<limbs>) in Montgomery form: sign and magnitude, the
