@@ -178,3 +178,15 @@ def test_commit_prove_many_equals_sequential(zipgpu, oracle, ctx, rng, lanes):
         assert (root, ev, proof) == zipgpu.ZipPlus.commit_prove(pp, [polys[i]], points[i])
         ro, po, eo, _ = oracle.commit_prove(desc, polys[i], 1, points[i])
         assert (root, ev, proof) == (ro, eo, po)
+
+
+@pytest.mark.parametrize("case", [(0, 1, 0, 12, 4096), (1, 32, 0, 14, 1 << 14),
+                                  (1, 32, 1, 12, 64), (1, 64, 0, 16, 1 << 14)])
+def test_device_verifier_verdicts_match_oracle(zipgpu, oracle, ctx, rng, case):
+    """With device parameters the verifier encodes the opened positions on the
+    GPU; its verdicts equal the oracle's and the host-only verifier's."""
+    from test_host_abi import verdicts_match_oracle
+
+    ek, D, ck, nv, L = case
+    pp = params_for(zipgpu, ek, D, ck, nv, L, ctx=ctx)
+    verdicts_match_oracle(zipgpu, oracle, pp, desc_for(ek, D, ck, nv, L), ek, D, nv, rng, cases=24)

@@ -102,6 +102,51 @@ def test_host_verifier_accepts_oracle_proofs(zipgpu, oracle, rng, case):
     assert e.value.status == 3
 
 
+def _verdict(zipgpu, pp, comm, point, inner, proof):
+    try:
+        zipgpu.ZipPlus.verify(pp, comm, point, inner, proof)
+        return 0
+    except zipgpu.ZipError as e:
+        return e.status
+
+
+def verdicts_match_oracle(zipgpu, oracle, pp, desc, ek, D, nv, rng, cases=40):
+    """Tampered and truncated proofs get the oracle's verdict (0 accept, 2 rejected
+    opening, 3 malformed), including the first failure winning over a later one."""
+    poly = binary_evals(rng, 1 << nv, D) if ek else i32_evals(rng, 1 << nv)
+    point = [(-1) ** i * (5 * i + 2) for i in range(nv)]
+    root, proof, inner, _ = oracle.commit_prove(desc, poly, 1, point)
+    comm = zipgpu.ZipPlusCommitment(root, 1)
+    variants = [proof, proof[:-1], proof[: len(proof) // 2]]
+    for pos in rng.integers(0, len(proof), size=cases):
+        bad = bytearray(proof)
+        bad[int(pos)] ^= 1 << int(rng.integers(0, 8))
+        variants.append(bytes(bad))
+    # a bad early opening together with a truncated tail: the opening wins
+    head = len(proof) - zipgpu_openings_bytes(pp)
+    bad = bytearray(proof[: len(proof) - 7])
+    bad[head + 3] ^= 1
+    variants.append(bytes(bad))
+    for v in variants:
+        want = oracle.verify(desc, root, 1, point, inner, v)
+        assert _verdict(zipgpu, pp, comm, point, inner, v) == want
+
+
+def zipgpu_openings_bytes(pp):
+    """Bytes of the column openings at the end of a batch-1 proof."""
+    i = pp.info
+    depth = i.codeword_len.bit_length() - 1
+    return pp.zt.num_openings * (i.num_rows * i.cw_bytes + 24 + 32 * depth)
+
+
+@pytest.mark.parametrize("case", [(0, 1, 0, 12, 4096), (1, 32, 0, 13, 1 << 13),
+                                  (1, 32, 1, 12, 64), (1, 64, 0, 11, 512)])
+def test_host_verifier_verdicts_match_oracle(zipgpu, oracle, rng, case):
+    ek, D, ck, nv, L = case
+    pp = params_for(zipgpu, ek, D, ck, nv, L, device=False)
+    verdicts_match_oracle(zipgpu, oracle, pp, desc_for(ek, D, ck, nv, L), ek, D, nv, rng)
+
+
 def test_device_entry_points_need_a_context(zipgpu):
     pp = params_for(zipgpu, 1, 32, 0, 10, 1024, device=False)
     with pytest.raises(zipgpu.ZipError) as e:

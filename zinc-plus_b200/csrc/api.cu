@@ -168,6 +168,52 @@ void host_encode_wide(const zg_params *p, const uint64_t *row, uint32_t limbs, u
 }
 
 // get_path_directions + MerkleProof::verify (merkle.rs:282-410).
+// encode_wide at selected codeword positions (the verifier checks only the
+// opened columns).  IPRS: position P = ch * bd + rb depends on the 8^depth base
+// outputs at base position rb and on the radix-8 stages over the chunk index;
+// RAA: the whole (cheap) codeword.  out: n x limbs.
+void host_encode_wide_at(const zg_params *p, const uint64_t *row, uint32_t limbs,
+                         const uint32_t *pos, uint32_t n, uint64_t *out) {
+    const zg_params_info &I = p->info;
+    if (p->d.code_kind == ZG_CODE_RAA) {
+        std::vector<uint64_t> all((size_t)I.codeword_len * limbs);
+        host_encode_wide(p, row, limbs, all.data());
+        for (uint32_t o = 0; o < n; o++) std::memcpy(out + (size_t)o * limbs, &all[(size_t)pos[o] * limbs], 8 * limbs);
+        return;
+    }
+    const uint32_t bd = I.base_dim, bl = I.base_len, depth = I.depth, nch = 1u << (3 * depth);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long o = 0; o < (long)n; o++) {
+        const uint32_t P = pos[o], rb = P % bd;
+        std::vector<uint64_t> cur((size_t)nch * limbs, 0), nxt((size_t)nch * limbs);
+        for (uint32_t ch = 0; ch < nch; ch++) {
+            uint32_t oct = 0, x = ch;
+            for (uint32_t k = 0; k < depth; k++) {
+                oct = (oct << 3) | (x & 7);
+                x >>= 3;
+            }
+            for (uint32_t c = 0; c < bl; c++)
+                wide_mul_s64_add(&cur[(size_t)ch * limbs], row + ((size_t)oct + ((size_t)c << (3 * depth))) * limbs,
+                                 p->bm[(size_t)rb * bl + c], (int)limbs);
+        }
+        for (uint32_t k = 0; k < depth; k++) {
+            const uint32_t stride = 1u << (3 * k);
+            const int64_t *tw = p->tw.data() + p->tw_off[k];
+            for (uint32_t ch = 0; ch < nch; ch++) {
+                const uint32_t r = (ch / stride) % 8, g0 = ch - r * stride;
+                const size_t i = (size_t)(ch % stride) * bd + rb;
+                uint64_t *y = &nxt[(size_t)ch * limbs];
+                std::memcpy(y, &cur[(size_t)g0 * limbs], 8 * limbs);
+                for (uint32_t j = 1; j < 8; j++)
+                    wide_mul_s64_add(y, &cur[(size_t)(g0 + j * stride) * limbs],
+                                     tw[(i * 7 + (j - 1)) * 8 + ((r * j) & 7)], (int)limbs);
+            }
+            cur.swap(nxt);
+        }
+        std::memcpy(out + (size_t)o * limbs, &cur[(size_t)(P / bd) * limbs], 8 * limbs);
+    }
+}
+
 bool merkle_verify(const uint8_t root[32], const uint8_t *col, size_t col_len, uint64_t li,
                    uint64_t lc, const uint8_t *sib, uint64_t ns, uint64_t expected) {
     if (li != expected) return false;
@@ -484,6 +530,33 @@ zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void 
 }
 
 // ------------------------------------------------------------------- verify
+// encode_wide at the opened positions: on the parameters' device when they
+// have one (one block per position), else on the host.
+static zg_status encode_wide_at(zg_params *p, const uint64_t *row, uint32_t CL, const uint32_t *pos,
+                                uint32_t n, uint64_t *out) {
+    if (!p->ctx || p->d.code_kind != ZG_CODE_IPRS || p->info.depth > 3) {
+        host_encode_wide_at(p, row, CL, pos, n, out);
+        return ZG_OK;
+    }
+    zg_ctx *ctx = p->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    const size_t row_b = (size_t)p->info.row_len * CL * 8, pos_b = ((size_t)n * 4 + 255) & ~(size_t)255;
+    const size_t out_b = (size_t)n * CL * 8;
+    const size_t row_off = 0, pos_off = (row_b + 255) & ~(size_t)255, out_off = pos_off + pos_b;
+    ZG_TRY(ctx->prove_in.ensure(out_off + out_b));
+    uint8_t *base = ctx->prove_in.as<uint8_t>();
+    cudaStream_t s = ctx->stream;
+    ZG_CUDA(cudaMemcpyAsync(base + row_off, row, row_b, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(base + pos_off, pos, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    ZG_TRY(launch_encode_wide_at(p, ctx, reinterpret_cast<const uint64_t *>(base + row_off), CL,
+                                 reinterpret_cast<const uint32_t *>(base + pos_off), n,
+                                 reinterpret_cast<uint64_t *>(base + out_off), s));
+    ZG_CUDA(cudaMemcpyAsync(out, base + out_off, out_b, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(ctx_sync(ctx));
+    return ZG_OK;
+}
+
 zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
                       const uint8_t *eval, const uint8_t *proof, size_t proof_len) {
     ZG_TRY(validate_budget(p, batch));
@@ -552,9 +625,15 @@ zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, cons
         set_error("proof truncated while reading the combined row");
         return ZG_ERR_SERIALIZATION;
     }
-    std::vector<uint64_t> comb((size_t)RL * CL), enc((size_t)C * CL);
+    std::vector<uint64_t> comb((size_t)RL * CL);
     std::memcpy(comb.data(), cr, comb.size() * 8);
-    host_encode_wide(p, comb.data(), CL, enc.data());
+    // The opened columns are the next num_openings challenges (nothing is
+    // absorbed in between), so draw them first and encode only those positions.
+    const uint32_t nop = p->d.num_openings;
+    std::vector<uint32_t> opened(nop);
+    for (uint32_t o = 0; o < nop; o++) opened[o] = tr_challenge_u32(&tr) % C;
+    std::vector<uint64_t> enc((size_t)nop * CL);
+    ZG_TRY(encode_wide_at(p, comb.data(), CL, opened.data(), nop, enc.data()));
     // check 2: <F(comb), q1> == <F(coeffs), b>
     uint64_t lhs[MAX_FIELD_LIMBS] = {0, 0, 0, 0}, rhs[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
     for (uint32_t c = 0; c < RL; c++) {
@@ -574,31 +653,53 @@ zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, cons
         return ZG_ERR_INVALID_OPEN;
     }
     const size_t cwb = p->info.cw_bytes, colbytes = (size_t)batch * R * cwb;
-    for (uint32_t o = 0; o < p->d.num_openings; o++) {
-        const uint32_t idx = tr_challenge_u32(&tr) % C;
+    // Parse the openings in order up to the first framing error, check the
+    // parsed ones in parallel, and report whichever failure comes first in
+    // opening order (what the sequential verifier reports).
+    struct Opening {
+        const uint8_t *col, *sib;
+        uint64_t li, lc, np;
+    };
+    std::vector<Opening> ops;
+    ops.reserve(nop);
+    zg_status parse_st = ZG_OK;
+    std::string parse_msg;
+    for (uint32_t o = 0; o < nop && parse_st == ZG_OK; o++) {
         const uint8_t *col = take(colbytes), *hdr = take(24);
         if (!col || !hdr) {
-            set_error("proof truncated in column opening %u", o);
-            return ZG_ERR_SERIALIZATION;
+            parse_st = ZG_ERR_SERIALIZATION;
+            parse_msg = "proof truncated in column opening " + std::to_string(o);
+            break;
         }
         uint64_t li, lc, np;
         std::memcpy(&li, hdr, 8);
         std::memcpy(&lc, hdr + 8, 8);
         std::memcpy(&np, hdr + 16, 8);
         if (np == 0 || li >= lc || np > 64) {
-            set_error("malformed Merkle proof in opening %u", o);
-            return ZG_ERR_SERIALIZATION;
+            parse_st = ZG_ERR_SERIALIZATION;
+            parse_msg = "malformed Merkle proof in opening " + std::to_string(o);
+            break;
         }
         const uint8_t *sib = take(32 * np);
         if (!sib) {
-            set_error("proof truncated in Merkle path %u", o);
-            return ZG_ERR_SERIALIZATION;
+            parse_st = ZG_ERR_SERIALIZATION;
+            parse_msg = "proof truncated in Merkle path " + std::to_string(o);
+            break;
         }
+        ops.push_back(Opening{col, sib, li, lc, np});
+    }
+    const uint32_t nparsed = (uint32_t)ops.size();
+    // 0 = passes, 1 = proximity failure, 2 = Merkle failure
+    std::vector<int> bad(nparsed, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long oo = 0; oo < (long)nparsed; oo++) {
+        const uint32_t o = (uint32_t)oo;
+        const Opening &op = ops[o];
         // check 3 (verify_column_testing_batched, phase_verify.rs:267-304)
         uint64_t sum[MAX_COMB_LIMBS] = {0};
         for (uint32_t b = 0; b < batch; b++)
             for (uint32_t j = 0; j < R; j++) {
-                const uint8_t *e = col + ((size_t)b * R + j) * cwb;
+                const uint8_t *e = op.col + ((size_t)b * R + j) * cwb;
                 uint64_t v[MAX_COMB_LIMBS] = {0};
                 if (!binary) {
                     uint64_t x[2];
@@ -621,14 +722,22 @@ zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, cons
                 }
                 wide_mul_i128_add(sum, v, coeffs[j], (int)CL);
             }
-        if (std::memcmp(sum, &enc[(size_t)idx * CL], 8 * CL) != 0) {
+        if (std::memcmp(sum, &enc[(size_t)o * CL], 8 * CL) != 0) bad[o] = 1;
+        else if (!merkle_verify(root, op.col, colbytes, op.li, op.lc, op.sib, op.np, opened[o])) bad[o] = 2;
+    }
+    for (uint32_t o = 0; o < nparsed; o++) {
+        if (bad[o] == 1) {
             set_error("Proximity failure");
             return ZG_ERR_INVALID_OPEN;
         }
-        if (!merkle_verify(root, col, colbytes, li, lc, sib, np, idx)) {
+        if (bad[o] == 2) {
             set_error("Column opening verification failed");
             return ZG_ERR_INVALID_OPEN;
         }
+    }
+    if (parse_st != ZG_OK) {
+        set_error("%s", parse_msg.c_str());
+        return parse_st;
     }
     return ZG_OK;
 }

@@ -712,7 +712,78 @@ __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__
 }
 
 // ---------------------------------------------------------------------------
+// Selected positions of LinearCode::encode_wide (iprs.rs:148-150) on a row of
+// CL-limb integers (wrapping).  Position P = ch * bd + rb of the codeword only
+// depends on the 8^depth base outputs at base position rb (one per chunk), and
+// stage k combines the chunks that differ in base-8 digit k of the chunk index
+// (twiddle position (ch mod 8^k) * bd + rb).  One block per position: its
+// threads compute the chunks' base outputs, then the stages run in shared memory.
+struct TwOffsets {
+    uint32_t off[4];
+};
+
+__global__ void __launch_bounds__(256) k_encode_wide_at(const uint64_t *__restrict__ row,
+                                                        const int32_t *__restrict__ bmT,
+                                                        const int32_t *__restrict__ tw, TwOffsets to,
+                                                        uint32_t bd, uint32_t bl, uint32_t depth,
+                                                        uint32_t CL, const uint32_t *__restrict__ pos,
+                                                        uint64_t *__restrict__ out) {
+    extern __shared__ uint64_t sv[];  // two buffers of nch x CL limbs
+    const uint32_t P = pos[blockIdx.x], rb = P % bd, nch = 1u << (3 * depth);
+    uint64_t *cur = sv, *nxt = sv + (size_t)nch * CL;
+    for (uint32_t ch = threadIdx.x; ch < nch; ch += blockDim.x) {
+        uint64_t acc[MAX_COMB_LIMBS];
+        for (uint32_t w = 0; w < CL; w++) acc[w] = 0;
+        const uint32_t oct = octet_reverse(ch, depth);
+        for (uint32_t c = 0; c < bl; c++)
+            wide_mul_s64_add(acc, row + ((size_t)oct + ((size_t)c << (3 * depth))) * CL,
+                             (int64_t)__ldg(bmT + (size_t)c * bd + rb), (int)CL);
+        for (uint32_t w = 0; w < CL; w++) cur[(size_t)ch * CL + w] = acc[w];
+    }
+    __syncthreads();
+    for (uint32_t k = 0; k < depth; k++) {
+        const uint32_t stride = 1u << (3 * k);
+        const size_t sub = (size_t)bd << (3 * k);
+        for (uint32_t ch = threadIdx.x; ch < nch; ch += blockDim.x) {
+            const uint32_t r = (ch / stride) % 8, g0 = ch - r * stride;
+            const size_t i = (size_t)(ch % stride) * bd + rb;
+            uint64_t acc[MAX_COMB_LIMBS];
+            for (uint32_t w = 0; w < CL; w++) acc[w] = cur[(size_t)g0 * CL + w];
+            for (uint32_t j = 1; j < 8; j++) {
+                const int32_t t = __ldg(tw + to.off[k] + (size_t)((j - 1) * 8 + ((r * j) & 7)) * sub + i);
+                wide_mul_s64_add(acc, cur + (size_t)(g0 + j * stride) * CL, (int64_t)t, (int)CL);
+            }
+            for (uint32_t w = 0; w < CL; w++) nxt[(size_t)ch * CL + w] = acc[w];
+        }
+        __syncthreads();
+        uint64_t *tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+    const uint32_t chp = P / bd;
+    for (uint32_t w = threadIdx.x; w < CL; w += blockDim.x) out[(size_t)blockIdx.x * CL + w] = cur[(size_t)chp * CL + w];
+}
+
 static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+zg_status launch_encode_wide_at(zg_params *p, zg_ctx *ctx, const uint64_t *row_d, uint32_t CL,
+                                const uint32_t *pos_d, uint32_t n, uint64_t *out_d, cudaStream_t s) {
+    const zg_params_info &I = p->info;
+    if (p->d.code_kind != ZG_CODE_IPRS || I.depth > 3 || CL > (uint32_t)MAX_COMB_LIMBS || n == 0) {
+        set_error("selected-position encode_wide needs an IPRS code of depth <= 3");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    TwOffsets to{};
+    for (uint32_t k = 0; k < I.depth; k++) to.off[k] = (uint32_t)p->tw_dev_off[k];
+    const uint32_t nch = 1u << (3 * I.depth);
+    const size_t smem = (size_t)2 * nch * CL * 8;
+    ZG_CUDA(allow_max_smem(k_encode_wide_at));
+    ZG_KBEGIN(ctx, s, "k_encode_wide_at");
+    k_encode_wide_at<<<n, std::min<uint32_t>(256, std::max<uint32_t>(32, nch)), smem, s>>>(
+        row_d, p->d_bmT, p->d_tw, to, I.base_dim, I.base_len, I.depth, CL, pos_d, out_d);
+    ZG_KEND(ctx, s);
+    return ZG_OK;
+}
 
 zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_t nrows,
                         uint8_t *out_d, bool leaf_major, cudaStream_t s, uint32_t seg_rows,

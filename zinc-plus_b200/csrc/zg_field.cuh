@@ -50,6 +50,24 @@ ZG_HD void wide_mul_i128_add(uint64_t *acc, const uint64_t *x, i128 s, int n) {
     wide_add(acc, prod, n);
 }
 
+// acc += x * s (mod 2^(64n)) for a signed 64-bit scalar: x * (s mod 2^64),
+// minus x * 2^64 when s < 0.
+ZG_HD void wide_mul_s64_add(uint64_t *acc, const uint64_t *x, int64_t s, int n) {
+    const uint64_t s0 = (uint64_t)s;
+    uint64_t c = 0, borrow = 0;
+    for (int i = 0; i < n; i++) {
+        u128 t = (u128)x[i] * s0 + acc[i] + c;
+        uint64_t v = (uint64_t)t;
+        c = (uint64_t)(t >> 64);
+        if (s < 0 && i > 0) {  // subtract x[i-1] at limb i
+            const uint64_t sub = x[i - 1], before = v;
+            v = before - sub - borrow;
+            borrow = (before < sub || (before == sub && borrow)) ? 1u : 0u;
+        }
+        acc[i] = v;
+    }
+}
+
 // Sign-extend a signed value of `from` limbs to `to` limbs.
 ZG_HD void wide_sext(const uint64_t *x, int from, uint64_t *out, int to) {
     uint64_t sg = (x[from - 1] >> 63) ? ~0ull : 0ull;

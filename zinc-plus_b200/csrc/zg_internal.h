@@ -286,6 +286,10 @@ zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, cons
 zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_t nrows,
                         uint8_t *out_d, bool leaf_major, cudaStream_t s, uint32_t seg_rows = 0,
                         int base_variant = -1);
+// encode_wide (CL-limb wrapping integers) at n selected codeword positions
+// (IPRS, depth <= 3): out is n x CL limbs.
+zg_status launch_encode_wide_at(zg_params *p, zg_ctx *ctx, const uint64_t *row_d, uint32_t CL,
+                                const uint32_t *pos_d, uint32_t n, uint64_t *out_d, cudaStream_t s);
 // tree_width: the `width` leaves belong to width / tree_width trees, stored in
 // consecutive blocks of 2 tree_width - 1 nodes; 0 = one tree.
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
