@@ -225,8 +225,8 @@ zg_status zg_commit_prove_many(zg_params *p, uint32_t n, const void *const *poly
                                uint32_t lanes, double *latency_ms);
 /* ---- Batched commit of independent polynomials of mixed shapes ---------------
  * n calls of ZipPlus::commit_single (phase_commit.rs:61-101, batch of one, one
- * Merkle tree each), polynomial i under params[i] (all created on ctx's
- * device).  Polynomials sharing a params handle are encoded and hashed in one
+ * Merkle tree each), polynomial i under params[i] (all created on ctx;
+ * destroying a parameter set drops the plans that use it).  Polynomials sharing a params handle are encoded and hashed in one
  * launch chain; the chains run on `lanes` concurrent streams.  Roots-only calls
  * (hints == NULL) keep a plan per batch shape (the sequence of params handles):
  * the first call times the kernel variants of each group shape (autotune),
@@ -244,7 +244,8 @@ typedef struct {
     uint32_t lanes;    /* concurrent streams, 0 = 4 (max 16) */
     int use_graph;     /* roots-only calls: capture and replay a CUDA graph */
     int autotune;      /* time the kernel variants of each group shape once */
-    int base_variant;  /* -1 = tuned/heuristic; binary IPRS base layer: 0 tensor-core,
+    int base_variant;  /* -1 = tuned/heuristic; binary IPRS base layer: 0 tensor-core
+                          (8 chunk rows per block), 4 / 5 tensor-core with 4 / 16,
                           1 shared-memory staged, 2 packed-lane, 3 plain */
     int leaf_variant;  /* -1 = tuned/heuristic; one-chunk leaves: 0 warp-coalesced, 1 per-thread */
 } zg_batch_opts;

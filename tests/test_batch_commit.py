@@ -61,7 +61,7 @@ def test_batch_commit_matches_oracle(zipgpu, oracle, ctx, rng):
         assert c.root == oracle.commit(d, p, 1)
 
 
-@pytest.mark.parametrize("base,leaf", [(0, 0), (1, 1), (2, 0), (3, 1), (-1, -1)])
+@pytest.mark.parametrize("base,leaf", [(0, 0), (1, 1), (2, 0), (3, 1), (4, 0), (5, 1), (-1, -1)])
 def test_batch_commit_variants_agree(zipgpu, ctx, rng, base, leaf):
     pps, polys, _ = _mixed(zipgpu, ctx, rng)
     want = [zipgpu.ZipPlus.commit(pp, [p])[1].root for pp, p in zip(pps, polys)]
@@ -150,6 +150,22 @@ def test_batch_commit_64_polys_nv10_20_deg64(zipgpu, oracle, ctx):
     for nv, p, c in zip(nvs, polys, got):
         if nv <= 11:
             assert c.root == oracle.commit(desc_for(1, 64, 0, int(nv), layout(int(nv))), p, 1)
+
+
+def test_batch_commit_after_parameters_are_freed(zipgpu, ctx, rng):
+    """Plans are keyed per parameter set, not per address: freeing a set and
+    creating sets of other shapes (which can reuse its address) commits right."""
+    import gc
+
+    for nv in (11, 13, 12, 14, 11, 15):
+        pp = params_for(zipgpu, 1, 32, 0, nv, 1 << min(nv, 14), ctx=ctx)
+        poly = binary_evals(rng, 1 << nv, 32)
+        want = zipgpu.ZipPlus.commit(pp, [poly])[1].root
+        for _ in range(2):
+            assert zipgpu.ZipPlus.commit_batch([pp], [poly], ctx)[0].root == want
+        pp.close()
+        del pp
+        gc.collect()
 
 
 def test_batch_commit_rejects_bad_input(zipgpu, ctx, rng):

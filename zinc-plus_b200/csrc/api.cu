@@ -863,6 +863,8 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
     }
     if (d.num_openings == 0) d.num_openings = 147;
     std::unique_ptr<zg_params> p(new zg_params());
+    static std::atomic<uint64_t> next_uid{1};
+    p->uid = next_uid.fetch_add(1);
     p->ctx = ctx;
     p->d = d;
     p->D = d.eval_kind == ZG_EVAL_BINPOLY ? d.degree_plus_one : 1;
@@ -977,6 +979,7 @@ zg_status zg_params_destroy(zg_params *p) {
     if (!p) return ZG_OK;
     if (p->ctx) {
         cudaSetDevice(p->ctx->device);
+        drop_plans_of(p->ctx, p);  // their graphs point at this set's device tables
         cudaFree(p->d_bmT);
         cudaFree(p->d_bmP);
         cudaFree(p->d_bmL);

@@ -50,7 +50,7 @@ std::vector<CommitTuning> candidates(const zg_params *p) {
     std::vector<CommitTuning> out;
     std::vector<int> bases = {-1};
     if (p->d.code_kind == ZG_CODE_IPRS && p->d.eval_kind == ZG_EVAL_BINPOLY && p->info.depth >= 1)
-        bases = {0, 1, 2};
+        bases = {0, 4, 5, 1, 2};
     std::vector<int> leaves = {-1};
     const size_t lb = (size_t)p->info.num_rows * p->info.cw_bytes;
     if (lb % 16 == 0) leaves = {0, 1};
@@ -106,6 +106,18 @@ struct BatchPlan {
         return n;
     }
 };
+
+void drop_plans_of(zg_ctx *ctx, const zg_params *p) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto &plans = ctx->plans;
+    plans.erase(std::remove_if(plans.begin(), plans.end(),
+                               [&](const std::pair<std::string, std::shared_ptr<BatchPlan>> &kv) {
+                                   for (const Group &g : kv.second->groups)
+                                       if (g.p == p) return true;
+                                   return false;
+                               }),
+                plans.end());
+}
 
 namespace {
 
@@ -261,15 +273,13 @@ zg_status build_plan(zg_ctx *ctx, uint32_t n, zg_params *const *params, int on_d
     return ZG_OK;
 }
 
+// Keyed by the parameter sets' unique ids: their addresses can be reused by a
+// later set of another shape once freed.
 std::string plan_key(uint32_t n, zg_params *const *params, int on_device, bool pinned,
                      uint32_t nlanes) {
     std::string k = std::to_string(n) + ":" + std::to_string(on_device) + ":" +
                     std::to_string((int)pinned) + ":" + std::to_string(nlanes);
-    for (uint32_t i = 0; i < n; i++) {
-        char b[24];
-        snprintf(b, sizeof b, ":%p", (const void *)params[i]);
-        k += b;
-    }
+    for (uint32_t i = 0; i < n; i++) k += ":" + std::to_string(params[i]->uid);
     return k;
 }
 
@@ -421,8 +431,8 @@ zg_status commit_batch_impl(zg_ctx *ctx, uint32_t n, zg_params *const *params,
             set_error("batched commit: polynomial %u has no parameters or data", i);
             return ZG_ERR_INVALID_PARAM;
         }
-        if (params[i]->ctx == nullptr || params[i]->ctx->device != ctx->device) {
-            set_error("batched commit: parameters %u belong to another device", i);
+        if (params[i]->ctx != ctx) {
+            set_error("batched commit: parameters %u were created on another context", i);
             return ZG_ERR_INVALID_PARAM;
         }
         ZG_TRY(validate_budget(params[i], 1));

@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(512) k_base_bin3(const uint64_t *__restrict__ 
 // rows 32 mw .. 32 mw + 31 (two m16 tiles) and every other (row, chunk) pair of
 // the block's kMmaPairs pairs.  Lanes are processed 32 at a time (four n8 tiles).
 constexpr uint32_t kMmaRows = 64;
-constexpr uint32_t kMmaPairs = 8;
+constexpr uint32_t kMmaPairs = 8;  // default pairs per block (variants: 4, 8, 16)
 
 __device__ __forceinline__ void mma_u8_16x8x32(int (&d)[4], const uint32_t (&a)[4], uint32_t b0,
                                                uint32_t b1) {
@@ -309,6 +309,7 @@ __device__ __forceinline__ void bits_to_bfrag(uint32_t x0, uint32_t x1, uint32_t
     b[3] = __byte_perm(hi01, hi23, 0x7632);
 }
 
+template <uint32_t PAIRS>
 __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ evals,
                                                   const uint8_t *__restrict__ bmL,
                                                   int32_t *__restrict__ out, uint32_t row_len,
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ e
     uint64_t *Xs = reinterpret_cast<uint64_t *>(smem_m + 3 * kMmaRows * astride);  // [pairs][blp]
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const uint32_t rb0 = blockIdx.x * kMmaRows;
-    const uint32_t pair0 = blockIdx.y * kMmaPairs, npairs = nrows * nch;
+    const uint32_t pair0 = blockIdx.y * PAIRS, npairs = nrows * nch;
     // A slice: 16-byte pieces (limb, row, k); rows past bd and k past bl are zero
     const uint32_t pieces_per_row = blp / 16;
     for (uint32_t e = tid; e < 3 * kMmaRows * pieces_per_row; e += nthr) {
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ e
         *reinterpret_cast<uint4 *>(As + ((size_t)limb * kMmaRows + row) * astride + k) = v;
     }
     const uint32_t shift = 3 * depth;
-    for (uint32_t e = tid; e < kMmaPairs * blp; e += nthr) {
+    for (uint32_t e = tid; e < PAIRS * blp; e += nthr) {
         const uint32_t pi = e / blp, c = e % blp, pair = pair0 + pi;
         uint64_t x = 0;
         if (pair < npairs && c < bl) {
@@ -348,7 +349,7 @@ __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ e
     const uint32_t mw = warp & 1, cw = warp >> 1;
     const uint32_t g = lane >> 2, t = lane & 3;
     const uint32_t lrow = lane & 15, lk = (lane >> 4) * 16;
-    for (uint32_t pi = cw; pi < kMmaPairs; pi += 2) {
+    for (uint32_t pi = cw; pi < PAIRS; pi += 2) {
         const uint32_t pair = pair0 + pi;
         if (pair >= npairs) break;
         const uint32_t grow = pair / nch, ch = pair % nch;
@@ -906,14 +907,24 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         ZG_TRY(ctx->stage_a.ensure((size_t)nrows * C * D * 4));
         int32_t *base = ctx->stage_a.as<int32_t>();
         const uint32_t blp = (bl + 31) / 32 * 32;
-        const size_t smem_m = (size_t)3 * kMmaRows * (blp + 16) + (size_t)kMmaPairs * blp * 8;
-        const uint64_t mma_gy = ((uint64_t)nrows * nch + kMmaPairs - 1) / kMmaPairs;
+        // tensor-core variants by pairs per block: 0 = 8 (default), 4 = 4, 5 = 16
+        const uint32_t pairs = base_variant == 4 ? 4 : base_variant == 5 ? 16 : kMmaPairs;
+        const size_t smem_m = (size_t)3 * kMmaRows * (blp + 16) + (size_t)pairs * blp * 8;
+        const uint64_t mma_gy = ((uint64_t)nrows * nch + pairs - 1) / pairs;
         if (p->d_bmL && smem_m <= 200 * 1024 && mma_gy <= 65535 &&
-            (base_variant == -1 || base_variant == 0)) {
+            (base_variant == -1 || base_variant == 0 || base_variant == 4 || base_variant == 5)) {
             dim3 gm((bd + kMmaRows - 1) / kMmaRows, (unsigned)mma_gy);
-            ZG_CUDA(allow_max_smem(k_base_mma));
             ZG_KBEGIN(ctx, s, "k_base_bin");
-            k_base_mma<<<gm, 128, smem_m, s>>>(ev, p->d_bmL, base, L, bd, bl, blp, depth, nch, C, D, dmask, nrows);
+            if (pairs == 4) {
+                ZG_CUDA(allow_max_smem(k_base_mma<4>));
+                k_base_mma<4><<<gm, 128, smem_m, s>>>(ev, p->d_bmL, base, L, bd, bl, blp, depth, nch, C, D, dmask, nrows);
+            } else if (pairs == 16) {
+                ZG_CUDA(allow_max_smem(k_base_mma<16>));
+                k_base_mma<16><<<gm, 128, smem_m, s>>>(ev, p->d_bmL, base, L, bd, bl, blp, depth, nch, C, D, dmask, nrows);
+            } else {
+                ZG_CUDA(allow_max_smem(k_base_mma<kMmaPairs>));
+                k_base_mma<kMmaPairs><<<gm, 128, smem_m, s>>>(ev, p->d_bmL, base, L, bd, bl, blp, depth, nch, C, D, dmask, nrows);
+            }
             ZG_KEND(ctx, s);
         } else {
             ZG_TRY(base_launch(base, false, false));

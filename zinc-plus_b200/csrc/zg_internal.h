@@ -115,6 +115,8 @@ size_t ctx_scratch_bytes(const zg_ctx *ctx);
 void ctx_scratch_release(zg_ctx *ctx);
 
 struct BatchPlan;
+// Drops the cached batch plans that use parameter set p (before p is freed).
+void drop_plans_of(zg_ctx *ctx, const zg_params *p);
 // Creates child contexts of ctx until it has n lanes.
 zg_status ensure_lanes(zg_ctx *ctx, uint32_t n);
 // validate_input's bit budget for linear combinations (pcs/utils.rs:24-54).
@@ -173,6 +175,7 @@ struct zg_ctx {
 
 struct zg_params {
     zg_ctx *ctx = nullptr;
+    uint64_t uid = 0;  // unique per parameter set in the process (addresses get reused)
     zg_params_desc d{};
     zg_params_info info{};
     uint32_t D = 1;  // lanes per evaluation (coefficients of BinaryPoly)
@@ -254,7 +257,8 @@ zg_status commit_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_
 // openings) is written there instead of being appended to t->stream.
 // Kernel choices of a commit launch chain (-1: the built-in heuristic).
 struct CommitTuning {
-    int base_variant = -1;  // binary IPRS base layer: 0 tensor-core, 1 smem-staged, 2 packed, 3 plain
+    int base_variant = -1;  // binary IPRS base layer: 0 tensor-core (4 / 5: 4 / 16 pairs per
+                            // block), 1 smem-staged, 2 packed, 3 plain
     int leaf_variant = -1;  // one-chunk leaves: 0 warp-coalesced, 1 one thread per leaf
 };
 // Bytes of one polynomial's codeword (leaf-major) and Merkle tree in a group.
