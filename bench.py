@@ -483,6 +483,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     import zipgpu as Z
+    from zipgpu import replicas
 
     workload = args.workload
     ek, D, ck, nv, L = WORKLOADS[workload]
@@ -563,11 +564,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, "cuda")
 
     # warm-up: device path and host path
     for i in range(W):
@@ -613,10 +610,12 @@ def run_ours(args):
     ktimes = {k: v for k, v in alltimes.items() if not k.startswith("host:")}
     host_phases = {k[5:]: round(v[1] / K, 4) for k, v in alltimes.items() if k.startswith("host:")}
 
-    plain_value = world * K * n / (total_dev / 1e3)
-    plain_e2e = world * K * n / (total_host / 1e3)
-    value = world * K * B * n / (total_bdev / 1e3)
-    e2e = world * K * B * n / (total_bhost / 1e3)
+    # every rank committed its own K (x B) polynomials: whole-job units over the
+    # slowest rank's time (the totals above are already maxima over ranks)
+    plain_value = replicas.sum_over_ranks(K * n, dist, "cuda") / (total_dev / 1e3)
+    plain_e2e = replicas.sum_over_ranks(K * n, dist, "cuda") / (total_host / 1e3)
+    value = replicas.sum_over_ranks(K * B * n, dist, "cuda") / (total_bdev / 1e3)
+    e2e = replicas.sum_over_ranks(K * B * n, dist, "cuda") / (total_bhost / 1e3)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
