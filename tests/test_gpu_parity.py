@@ -22,6 +22,8 @@ ENCODE_CASES = [
     (1, 32, 0, 10, 1024, 1),
     (1, 32, 0, 10, 32, 0),
     (1, 17, 0, 9, 512, 0),
+    (1, 40, 0, 12, 4096, 3),  # 33..64 lanes, depth 3 (base 32 x 8)
+    (1, 64, 0, 14, 1 << 14, 0),  # base 1024 x 256, two 32-lane halves
     (1, 32, 1, 12, 64, 0),    # RAA
     (1, 64, 1, 12, 64, 0),
     (1, 3, 1, 8, 16, 0),

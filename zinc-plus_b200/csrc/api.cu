@@ -9,6 +9,7 @@
 
 #include "zg_internal.h"
 #include "zg_prove.h"
+#include "zg_umma.cuh"
 
 namespace zg {
 const char *last_error();
@@ -59,6 +60,26 @@ zg_status zg::validate_budget(const zg_params *p, uint32_t batch) {
 namespace {
 
 uint64_t dmask_of(uint32_t D) { return D >= 64 ? ~0ull : ((1ull << D) - 1); }
+
+// Per-row offsets of the tcgen05 base layer: off[r] moves row r of the base
+// matrix into [-2^15, 2^15), where a u8 low byte and an s8 high byte hold it
+// exactly; the kernel subtracts off[r] x (number of set input bits).  False
+// when some row spans more than 2^16 values.
+bool build_umma_offsets(const std::vector<int64_t> &bm, uint32_t bd, uint32_t bl, std::vector<int32_t> &off) {
+    off.assign(bd, 0);
+    for (uint32_t r = 0; r < bd; r++) {
+        int64_t lo = INT64_MAX, hi = INT64_MIN;
+        for (uint32_t c = 0; c < bl; c++) {
+            lo = std::min(lo, bm[(size_t)r * bl + c]);
+            hi = std::max(hi, bm[(size_t)r * bl + c]);
+        }
+        if (bl == 0) continue;
+        if (hi - lo > 65535) return false;
+        const int64_t o = lo < -32768 ? -32768 - lo : hi > 32767 ? 32767 - hi : 0;
+        off[r] = (int32_t)o;
+    }
+    return true;
+}
 
 i128 load_i128(const uint8_t *b) {
     u128 v = 0;
@@ -768,6 +789,11 @@ zg_status zg_ctx_create(int device, zg_ctx **out) {
     c->device = device;
     ZG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     ZG_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    c->status = device_status_word(device);
+    if (!c->status) {
+        set_error("could not map the device status word");
+        return ZG_ERR_CUDA;
+    }
     *out = c.release();
     return ZG_OK;
 }
@@ -920,6 +946,30 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
                 }
             ZG_CUDA(cudaMalloc(&p->d_bmL, bmL.size()));
             ZG_CUDA(cudaMemcpy(p->d_bmL, bmL.data(), bmL.size(), cudaMemcpyHostToDevice));
+            // tcgen05 operand image: row offsets that bring every row into
+            // [-2^15, 2^15), then two byte limbs in the swizzled tile layout
+            std::vector<int32_t> off;
+            if (build_umma_offsets(p->bm, bd, bl, off)) {
+                const uint32_t kp = (bl + 127) / 128 * 128, atoms = kp / 128;
+                const uint32_t tiles = (bd + kUmmaImgRows - 1) / kUmmaImgRows;
+                std::vector<uint8_t> img((size_t)tiles * 2 * kp * kUmmaImgRows, 0);
+                off.resize((size_t)tiles * kUmmaImgRows, 0);
+                for (uint32_t r = 0; r < bd; r++) {
+                    const uint32_t t = r / kUmmaImgRows, rr = r % kUmmaImgRows;
+                    for (uint32_t c = 0; c < bl; c++) {
+                        const int32_t v = (int32_t)p->bm[(size_t)r * bl + c] + off[r];
+                        const uint8_t limb[2] = {(uint8_t)(v & 0xFF), (uint8_t)((v >> 8) & 0xFF)};
+                        for (uint32_t l = 0; l < 2; l++)
+                            img[((size_t)t * 2 + l) * atoms * kUmmaImgRows * 128 +
+                                umma::sw128_offset(rr, c, kUmmaImgRows)] = limb[l];
+                    }
+                }
+                ZG_CUDA(cudaMalloc(&p->d_bmU, img.size()));
+                ZG_CUDA(cudaMemcpy(p->d_bmU, img.data(), img.size(), cudaMemcpyHostToDevice));
+                ZG_CUDA(cudaMalloc(&p->d_bmOff, off.size() * 4));
+                ZG_CUDA(cudaMemcpy(p->d_bmOff, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+                p->umma_kp = kp;
+            }
             ZG_CUDA(cudaMalloc(&p->d_tw, std::max<size_t>(tw32.size(), 1) * 4));
             if (!tw32.empty())
                 ZG_CUDA(cudaMemcpy(p->d_tw, tw32.data(), tw32.size() * 4, cudaMemcpyHostToDevice));
@@ -983,6 +1033,8 @@ zg_status zg_params_destroy(zg_params *p) {
         cudaFree(p->d_bmT);
         cudaFree(p->d_bmP);
         cudaFree(p->d_bmL);
+        cudaFree(p->d_bmU);
+        cudaFree(p->d_bmOff);
         cudaFree(p->d_tw);
         cudaFree(p->d_tw2r);
         cudaFree(p->d_perm);

@@ -15,6 +15,7 @@
 #include <algorithm>
 
 #include "zg_internal.h"
+#include "zg_umma.cuh"
 
 namespace zg {
 
@@ -402,6 +403,178 @@ __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ e
                         }
                     }
         }
+    }
+}
+
+// Base layer on the 5th-generation tensor cores (tcgen05, accumulators in
+// tensor memory).  The same sums as k_base_mma, as one GEMM per tile:
+//   D[m][n] = sum_k bits[m][k] * (bm[n][k] + off[n]),
+//   out = D[m][n] - off[n] * popcount(bits[m][.]),
+// m = (pair, lane) of 128 input rows, n = NT base rows, k < round_up(bl, 128).
+// The offset brings every base row into [-2^15, 2^15), so two 8-bit MMAs
+// give it exactly: the u8 low byte and the s8 high byte (x 256).
+//
+// Tile pairs are taken in octet-reversed chunk order: slot q of a codeword row
+// is chunk octet_reverse(q), whose inputs are evals[q + k 8^depth], so the
+// tile's pairs read adjacent evaluations.  The CTA's threads expand the input
+// bits into the A tile (K-major, 128-byte swizzle) while one bulk copy per
+// (limb, 128-column atom) brings the pre-swizzled base-matrix tile; one thread
+// issues the MMAs and commits them to an mbarrier; each warp then reads its 32
+// TMEM lanes (one pair's lanes for D <= 32) and writes every base row's 32
+// lanes as one 128-byte line.  Waits are bounded (umma::mbar_wait): on a
+// timeout the CTA sets the device status word, stores nothing, frees its
+// tensor memory and returns.
+template <uint32_t NT>
+__global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ evals,
+                                                   const uint8_t *__restrict__ bm_img,
+                                                   const int32_t *__restrict__ bm_off,
+                                                   int32_t *__restrict__ out, uint32_t row_len,
+                                                   uint32_t bd, uint32_t bl, uint32_t kp,
+                                                   uint32_t depth, uint32_t nch, uint32_t C,
+                                                   uint32_t D, uint64_t dmask, uint32_t npairs,
+                                                   uint32_t lp, uint32_t *status) {
+    using namespace umma;
+    constexpr uint32_t kCols = 2 * NT;  // two limb accumulators of NT columns
+    extern __shared__ __align__(16) uint8_t smem_u[];
+    uint8_t *As = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_u) + 1023) & ~uintptr_t(1023));
+    uint8_t *Bs = As + 128 * kp;  // [limb][kp / 128][NT][128]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + 2 * NT * kp);  // loaded, MMA done
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t ppt = 128 / lp, halves = lp / 32, atoms = kp / 128;
+    const uint32_t mt = blockIdx.x, nt = blockIdx.y;
+
+    if (warp == 0) {
+        tmem_alloc(tslot, kCols);
+        tmem_relinquish();
+    }
+    if (tid == 32) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (tid == 32) {
+        // base-matrix limbs of rows nt*NT .. +NT: NT x 128 bytes per (limb, atom)
+        mbar_arrive_expect_tx(&bars[0], 2 * NT * kp);
+        const uint32_t t_img = (nt * NT) / kUmmaImgRows, row0 = (nt * NT) % kUmmaImgRows;
+        for (uint32_t l = 0; l < 2; l++)
+            for (uint32_t a = 0; a < atoms; a++)
+                bulk_g2s(Bs + (size_t)(l * atoms + a) * NT * 128,
+                         bm_img + ((((size_t)t_img * 2 + l) * atoms + a) * kUmmaImgRows + row0) * 128,
+                         NT * 128, &bars[0]);
+    }
+
+    // A tile: row m = pi * lp + 32 * hw + lane bit, byte k = bit of evaluation k
+    const uint32_t shift = 3 * depth;
+    const uint32_t ntask = ppt * halves * (kp / 8);
+    for (uint32_t task = tid; task < ntask; task += 128) {
+        const uint32_t pi = task % ppt, rest = task / ppt;
+        const uint32_t hw = rest % halves, g8 = rest / halves;
+        const uint32_t gp = mt * ppt + pi;
+        uint32_t x[8];
+        if (gp < npairs) {
+            const uint64_t *src = evals + (size_t)(gp / nch) * row_len + (gp % nch);
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const uint32_t k = 8 * g8 + i;
+                x[i] = k < bl ? (uint32_t)((__ldg(src + ((size_t)k << shift)) & dmask) >> (32 * hw)) : 0u;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++) x[i] = 0;
+        }
+#pragma unroll
+        for (uint32_t g = 0; g < 8; g++) {
+            uint32_t b0[4], b1[4];
+            bits_to_bfrag(x[0], x[1], x[2], x[3], g, b0);
+            bits_to_bfrag(x[4], x[5], x[6], x[7], g, b1);
+#pragma unroll
+            for (uint32_t bb = 0; bb < 4; bb++) {
+                const uint32_t m = pi * lp + 32 * hw + g + 8 * bb;
+                *reinterpret_cast<uint2 *>(As + sw128_offset(m, 8 * g8, 128)) = make_uint2(b0[bb], b1[bb]);
+            }
+        }
+    }
+    fence_async_smem();
+    __syncthreads();
+
+    // every thread observes the copy's completion itself
+    const bool loaded = mbar_wait(&bars[0], 0);
+    if (tid == 0) {
+        if (!loaded) {
+            atomicOr(status, kStatusLoadTimeout);
+            mbar_arrive(&bars[1]);
+        } else {
+            tc_fence_after();
+            const uint32_t id_lo = idesc_i8(128, NT, false, false);
+            const uint32_t id_hi = idesc_i8(128, NT, true, true);
+            const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs), b1 = b0 + atoms * NT * 128;
+            for (uint32_t ks = 0; ks < kp / 32; ks++) {
+                const uint32_t a = ks >> 2, o = (ks & 3) * 32;
+                const uint64_t ad = sdesc_k_sw128(a0 + a * 128 * 128 + o);
+                mma_i8(tmem, ad, sdesc_k_sw128(b0 + a * NT * 128 + o), id_lo, ks > 0);
+                mma_i8(tmem + NT, ad, sdesc_k_sw128(b1 + a * NT * 128 + o), id_hi, ks > 0);
+            }
+            mma_commit(&bars[1]);
+        }
+    }
+
+    // popcount of this thread's A row (row m = tid), while the MMAs run
+    uint32_t cnt = 0;
+    for (uint32_t a = 0; a < atoms; a++)
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(As + a * 128 * 128 + tid * 128 + j * 16);
+            cnt = __dp4a(v.x, 0x01010101u, cnt);
+            cnt = __dp4a(v.y, 0x01010101u, cnt);
+            cnt = __dp4a(v.z, 0x01010101u, cnt);
+            cnt = __dp4a(v.w, 0x01010101u, cnt);
+        }
+
+    const bool done = mbar_wait(&bars[1], 0);
+    tc_fence_after();
+    const bool ok = done && loaded;
+    if (!done && lane == 0) atomicOr(status, kStatusMmaTimeout);
+    if (ok) {
+        const uint32_t gp = mt * ppt + tid / lp, ln = tid % lp;
+        const bool live = gp < npairs && ln < D;
+        size_t ob = 0;
+        if (live) {
+            const uint32_t ch = octet_reverse(gp % nch, depth);
+            ob = ((size_t)(gp / nch) * C + (size_t)ch * bd) * D + ln;
+        }
+        const uint32_t lane_base = tmem + ((32 * warp) << 16);
+#pragma unroll 1
+        for (uint32_t c = 0; c < NT / 32; c++) {
+            uint32_t lo[32], hi[32];
+            tmem_ld32(lane_base + 32 * c, lo);
+            tmem_ld32(lane_base + NT + 32 * c, hi);
+            tmem_wait_ld();
+            const uint32_t r0 = nt * NT + 32 * c;
+            if (live) {
+#pragma unroll
+                for (uint32_t j = 0; j < 32; j++) {
+                    const uint32_t r = r0 + j;
+                    if (r < bd)
+                        out[ob + (size_t)r * D] =
+                            (int32_t)(lo[j] + (hi[j] << 8) - (uint32_t)__ldg(bm_off + r) * cnt);
+                }
+            }
+        }
+    }
+    // on a timeout, give copies and MMAs still in flight a second bounded wait
+    if (tid == 32 && !loaded) mbar_wait(&bars[0], 0);
+    if (tid == 0 && !done) mbar_wait(&bars[1], 0);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kCols);
     }
 }
 
@@ -906,6 +1079,35 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         if (depth == 0) return base_launch(out_d, true, leaf_major);
         ZG_TRY(ctx->stage_a.ensure((size_t)nrows * C * D * 4));
         int32_t *base = ctx->stage_a.as<int32_t>();
+        // tcgen05 base layer (default; variants 6 = 128 and 7 = 64 base rows per tile)
+        if (p->d_bmU && D <= 64 && (base_variant == -1 || base_variant == 6 || base_variant == 7)) {
+            const uint32_t NT = base_variant == 7 ? 64 : 128;
+            const uint32_t lp = D <= 32 ? 32 : 64, kp = p->umma_kp;
+            const uint64_t npairs = (uint64_t)nrows * nch;
+            // operand tiles, barriers and TMEM slot, 1024-byte alignment slack; at
+            // least a 1/(512/(2 NT) + 1) share of the SM's 228 KiB so that the CTAs
+            // resident on one SM never ask for more than its 512 TMEM columns
+            size_t smem_u = 1024 + (size_t)128 * kp + (size_t)2 * NT * kp + 32;
+            smem_u = std::max<size_t>(smem_u, 233472 / (512 / (2 * NT) + 1));
+            const uint64_t gx = (npairs + 128 / lp - 1) / (128 / lp);
+            if (smem_u <= (size_t)max_smem_optin() && gx < (1ull << 31)) {
+                dim3 gu((unsigned)gx, (bd + NT - 1) / NT);
+                ZG_KBEGIN(ctx, s, "k_base_bin");
+                if (NT == 64) {
+                    ZG_CUDA(allow_max_smem(k_base_umma<64>));
+                    k_base_umma<64><<<gu, 128, smem_u, s>>>(ev, p->d_bmU, p->d_bmOff, base, L, bd, bl, kp, depth, nch, C,
+                                                            D, dmask, (uint32_t)npairs, lp, ctx->status);
+                } else {
+                    ZG_CUDA(allow_max_smem(k_base_umma<128>));
+                    k_base_umma<128><<<gu, 128, smem_u, s>>>(ev, p->d_bmU, p->d_bmOff, base, L, bd, bl, kp, depth, nch,
+                                                             C, D, dmask, (uint32_t)npairs, lp, ctx->status);
+                }
+                ZG_KEND(ctx, s);
+                base_variant = 0;  // done: skip the other base kernels below
+                goto stages;
+            }
+        }
+        {
         const uint32_t blp = (bl + 31) / 32 * 32;
         // tensor-core variants by pairs per block: 0 = 8 (default), 4 = 4, 5 = 16
         const uint32_t pairs = base_variant == 4 ? 4 : base_variant == 5 ? 16 : kMmaPairs;
@@ -929,6 +1131,8 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         } else {
             ZG_TRY(base_launch(base, false, false));
         }
+        }
+    stages:
         if (depth == 2 && p->d_tw2r && D <= 64) {
             // both stages in one kernel, register resident
             const uint32_t RB = std::max<uint32_t>(1, std::min<uint32_t>(kStageRB, 256 / D));

@@ -214,9 +214,48 @@ void ctx_cache_trim(zg_ctx *ctx, size_t max_bytes) {
 }
 
 cudaError_t ctx_sync(zg_ctx *ctx) {
-    if (!ctx->sync_event) return cudaStreamSynchronize(ctx->stream);
-    cudaError_t e = cudaEventRecord(ctx->sync_event, ctx->stream);
-    return e == cudaSuccess ? cudaEventSynchronize(ctx->sync_event) : e;
+    cudaError_t e;
+    if (!ctx->sync_event) {
+        e = cudaStreamSynchronize(ctx->stream);
+    } else {
+        e = cudaEventRecord(ctx->sync_event, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ctx->sync_event);
+    }
+    return e == cudaSuccess ? device_status(ctx->device) : e;
+}
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::once_flag status_once;
+uint32_t *status_host = nullptr;  // kMaxDevices words, mapped and portable
+}  // namespace
+
+uint32_t *device_status_word(int device) {
+    std::call_once(status_once, [] {
+        void *h = nullptr;
+        if (cudaHostAlloc(&h, kMaxDevices * sizeof(uint32_t), cudaHostAllocMapped | cudaHostAllocPortable) ==
+            cudaSuccess) {
+            std::memset(h, 0, kMaxDevices * sizeof(uint32_t));
+            status_host = static_cast<uint32_t *>(h);
+        } else {
+            cudaGetLastError();
+        }
+    });
+    if (!status_host || device < 0 || device >= kMaxDevices) return nullptr;
+    void *d = nullptr;
+    if (cudaHostGetDevicePointer(&d, status_host + device, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return static_cast<uint32_t *>(d);
+}
+
+cudaError_t device_status(int device) {
+    if (!status_host || device < 0 || device >= kMaxDevices) return cudaSuccess;
+    const uint32_t v = reinterpret_cast<volatile uint32_t *>(status_host)[device];
+    if (v == 0) return cudaSuccess;
+    set_error("a kernel's bounded wait ran out on device %d (status %u)", device, v);
+    return cudaErrorLaunchTimeout;
 }
 
 void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool) {

@@ -108,6 +108,11 @@ void ctx_cache_trim(zg_ctx *ctx, size_t max_bytes);
 // Waits until all work queued on ctx's stream is done (spinning, or sleeping
 // when the context has a blocking-sync event).
 cudaError_t ctx_sync(zg_ctx *ctx);
+// Status word of a device, in mapped pinned host memory: a kernel whose
+// bounded wait ran out ORs a code into it (umma::kStatus*), skips its work and
+// returns.  device_status reports a set word as cudaErrorLaunchTimeout.
+uint32_t *device_status_word(int device);
+cudaError_t device_status(int device);
 // Routes a fresh context's hint blocks and scratch through a memory pool.
 void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool);
 // Device bytes held by a context's scratch arenas, and their release.
@@ -171,7 +176,14 @@ struct zg_ctx {
     // Waits for the stream by sleeping on a blocking-sync event instead of
     // spinning (lanes on which several host threads wait at once).
     cudaEvent_t sync_event = nullptr;
+    // device pointer of this device's status word (device_status_word)
+    uint32_t *status = nullptr;
 };
+
+namespace zg {
+// Base rows per tile of the tcgen05 base-layer operand image.
+constexpr uint32_t kUmmaImgRows = 128;
+}  // namespace zg
 
 struct zg_params {
     zg_ctx *ctx = nullptr;
@@ -185,6 +197,14 @@ struct zg_params {
     int32_t *d_bmT = nullptr; // base_len x base_dim (transposed)
     int32_t *d_bmP = nullptr; // base_len x round_up(base_dim, 8) (transposed, zero padded)
     uint8_t *d_bmL = nullptr; // [3][base_dim][round_up(base_len, 32)] u8 limbs of the base matrix
+    // Operand image of the tcgen05 base layer: per tile of kUmmaImgRows base
+    // rows, two limbs (u8 low byte, s8 high byte) of bm[r][c] + bm_off[r], each
+    // [round_up(base_len, 128) / 128][kUmmaImgRows][128] in the 128-byte
+    // swizzle; bm_off[r] puts row r in [-2^15, 2^15).  NULL when a row spans
+    // more than 2^16 values.
+    uint8_t *d_bmU = nullptr;
+    int32_t *d_bmOff = nullptr;
+    uint32_t umma_kp = 0;  // round_up(base_len, 128)
     int32_t *d_tw = nullptr;  // stage k: [56][sub_k], stages back to back
     // depth 2 only: per base position rb, 576 int32 twiddles in use order:
     // [r0][j] for stage 0 (64), then [r0][r1][j] for stage 1 (512); j = 0 unused
