@@ -245,10 +245,11 @@ typedef struct {
     int use_graph;     /* roots-only calls: capture and replay a CUDA graph */
     int autotune;      /* time the kernel variants of each group shape once */
     int base_variant;  /* -1 = tuned/heuristic; binary IPRS base layer: 6 / 7 tcgen05
-                          (128 / 64 base rows per tile, accumulators in tensor
-                          memory), 0 mma.sync (8 chunk rows per block), 4 / 5
-                          mma.sync with 4 / 16, 1 shared-memory staged, 2
-                          packed-lane, 3 plain */
+                          persistent (128 / 64 base rows per tile, accumulators
+                          in tensor memory), 8 / 9 tcgen05 one tile per block,
+                          0 mma.sync (8 chunk rows per block), 4 / 5 mma.sync
+                          with 4 / 16, 1 shared-memory staged, 2 packed-lane,
+                          3 plain */
     int leaf_variant;  /* -1 = tuned/heuristic; one-chunk leaves: 0 warp-coalesced, 1 per-thread */
 } zg_batch_opts;
 zg_status zg_commit_batch(zg_ctx *ctx, uint32_t n, zg_params *const *params,

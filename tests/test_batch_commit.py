@@ -62,7 +62,7 @@ def test_batch_commit_matches_oracle(zipgpu, oracle, ctx, rng):
 
 
 @pytest.mark.parametrize("base,leaf", [(0, 0), (1, 1), (2, 0), (3, 1), (4, 0), (5, 1), (6, 0), (7, 1),
-                                       (-1, -1)])
+                                       (8, 0), (9, 1), (-1, -1)])
 def test_batch_commit_variants_agree(zipgpu, ctx, rng, base, leaf):
     pps, polys, _ = _mixed(zipgpu, ctx, rng)
     want = [zipgpu.ZipPlus.commit(pp, [p])[1].root for pp, p in zip(pps, polys)]

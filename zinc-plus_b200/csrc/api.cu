@@ -966,8 +966,10 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
                 }
                 ZG_CUDA(cudaMalloc(&p->d_bmU, img.size()));
                 ZG_CUDA(cudaMemcpy(p->d_bmU, img.data(), img.size(), cudaMemcpyHostToDevice));
-                ZG_CUDA(cudaMalloc(&p->d_bmOff, off.size() * 4));
-                ZG_CUDA(cudaMemcpy(p->d_bmOff, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+                std::vector<int32_t> noff(off.size());  // the kernels add -off[r] x popcount
+                for (size_t i = 0; i < off.size(); i++) noff[i] = -off[i];
+                ZG_CUDA(cudaMalloc(&p->d_bmOff, noff.size() * 4));
+                ZG_CUDA(cudaMemcpy(p->d_bmOff, noff.data(), noff.size() * 4, cudaMemcpyHostToDevice));
                 p->umma_kp = kp;
             }
             ZG_CUDA(cudaMalloc(&p->d_tw, std::max<size_t>(tw32.size(), 1) * 4));

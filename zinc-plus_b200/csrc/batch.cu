@@ -50,7 +50,7 @@ std::vector<CommitTuning> candidates(const zg_params *p) {
     std::vector<CommitTuning> out;
     std::vector<int> bases = {-1};
     if (p->d.code_kind == ZG_CODE_IPRS && p->d.eval_kind == ZG_EVAL_BINPOLY && p->info.depth >= 1)
-        bases = {6, 7, 0, 4, 5, 1, 2};
+        bases = {6, 7, 8, 0, 4, 5, 1, 2};
     std::vector<int> leaves = {-1};
     const size_t lb = (size_t)p->info.num_rows * p->info.cw_bytes;
     if (lb % 16 == 0) leaves = {0, 1};

@@ -412,22 +412,109 @@ __global__ void __launch_bounds__(128) k_base_mma(const uint64_t *__restrict__ e
 //   out = D[m][n] - off[n] * popcount(bits[m][.]),
 // m = (pair, lane) of 128 input rows, n = NT base rows, k < round_up(bl, 128).
 // The offset brings every base row into [-2^15, 2^15), so two 8-bit MMAs
-// give it exactly: the u8 low byte and the s8 high byte (x 256).
+// give it exactly: the u8 low byte and the s8 high byte (x 256).  The table
+// holds -off[n].
 //
 // Tile pairs are taken in octet-reversed chunk order: slot q of a codeword row
 // is chunk octet_reverse(q), whose inputs are evals[q + k 8^depth], so the
-// tile's pairs read adjacent evaluations.  The CTA's threads expand the input
-// bits into the A tile (K-major, 128-byte swizzle) while one bulk copy per
-// (limb, 128-column atom) brings the pre-swizzled base-matrix tile; one thread
-// issues the MMAs and commits them to an mbarrier; each warp then reads its 32
-// TMEM lanes (one pair's lanes for D <= 32) and writes every base row's 32
-// lanes as one 128-byte line.  Waits are bounded (umma::mbar_wait): on a
+// tile's pairs read adjacent evaluations.  Input bits are expanded into the A
+// tile (K-major, 128-byte swizzle) by the CTA's threads; the pre-swizzled
+// base-matrix tile arrives by one bulk copy per (limb, 128-column atom); one
+// thread issues the MMAs and commits them to an mbarrier; TMEM lane m is A row
+// m, so a warp holds one pair's 32 lanes (D <= 32) and writes each base row's
+// lanes as one 128-byte line.  Waits are bounded (umma::mbar_wait*): on a
 // timeout the CTA sets the device status word, stores nothing, frees its
 // tensor memory and returns.
-template <uint32_t NT>
+
+// Expands the input bits of m-tile `mt` into the A tile: tasks (pair, 32-lane
+// half, 8 inputs) strided over `nthr` threads starting at `t0`.
+__device__ __forceinline__ void umma_fill_a(uint8_t *A, const uint64_t *__restrict__ evals, uint32_t mt,
+                                            uint32_t t0, uint32_t nthr, uint32_t lp, uint32_t kp,
+                                            uint32_t bl, uint32_t shift, uint32_t nch, uint32_t row_len,
+                                            uint64_t dmask, uint32_t npairs) {
+    const uint32_t ppt = 128 / lp, halves = lp / 32, ntask = ppt * halves * (kp / 8);
+    for (uint32_t task = t0; task < ntask; task += nthr) {
+        const uint32_t pi = task % ppt, rest = task / ppt;
+        const uint32_t hw = rest % halves, g8 = rest / halves;
+        const uint32_t gp = mt * ppt + pi;
+        uint32_t x[8];
+        if (gp < npairs) {
+            const uint64_t *src = evals + (size_t)(gp / nch) * row_len + (gp % nch);
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const uint32_t k = 8 * g8 + i;
+                x[i] = k < bl ? (uint32_t)((__ldg(src + ((size_t)k << shift)) & dmask) >> (32 * hw)) : 0u;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++) x[i] = 0;
+        }
+#pragma unroll
+        for (uint32_t g = 0; g < 8; g++) {
+            uint32_t b0[4], b1[4];
+            bits_to_bfrag(x[0], x[1], x[2], x[3], g, b0);
+            bits_to_bfrag(x[4], x[5], x[6], x[7], g, b1);
+#pragma unroll
+            for (uint32_t bb = 0; bb < 4; bb++) {
+                const uint32_t row = pi * lp + 32 * hw + g + 8 * bb;
+                *reinterpret_cast<uint2 *>(A + umma::sw128_offset(row, 8 * g8, 128)) = make_uint2(b0[bb], b1[bb]);
+            }
+        }
+    }
+}
+
+// Set bits of A row `row`.  Chunks are read in the order j ^ (row % 8), so
+// eight consecutive rows touch all 32 banks (conflict-free).
+__device__ __forceinline__ uint32_t umma_row_popcount(const uint8_t *A, uint32_t row, uint32_t atoms) {
+    uint32_t c = 0;
+    for (uint32_t a = 0; a < atoms; a++)
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(A + a * 128 * 128 + row * 128 + ((j ^ (row & 7u)) << 4));
+            c = __dp4a(v.x, 0x01010101u, c);
+            c = __dp4a(v.y, 0x01010101u, c);
+            c = __dp4a(v.z, 0x01010101u, c);
+            c = __dp4a(v.w, 0x01010101u, c);
+        }
+    return c;
+}
+
+// Epilogue of one 32-column chunk: TMEM columns col (low limb) and col + NT
+// (high limb) of this warp's lanes, base rows r0 .. r0 + 31 (nvalid of them
+// below bd) written at o[q * D].  DS = D when it is 32 or 64 (immediate store
+// offsets), 0 for any other D.
+template <uint32_t DS, uint32_t NT>
+__device__ __forceinline__ void umma_store_chunk(uint32_t taddr, const int32_t *__restrict__ noff, uint32_t r0,
+                                                 bool live, int32_t *o, uint32_t cnt, uint32_t D,
+                                                 uint32_t nvalid) {
+    uint32_t lo[32], hi[32];
+    umma::tmem_ld32(taddr, lo);
+    umma::tmem_ld32(taddr + NT, hi);
+    int4 o4[8];  // -off of the chunk's rows (table padded to whole 128-row tiles)
+#pragma unroll
+    for (int v = 0; v < 8; v++) o4[v] = __ldg(reinterpret_cast<const int4 *>(noff + r0) + v);
+    umma::tmem_wait_ld();
+    if (!live) return;
+    const uint32_t Dv = DS ? DS : D;
+#define ZG_UMMA_VAL(q)                                                                             \
+    (int32_t)(lo[q] + (hi[q] << 8) +                                                               \
+              (uint32_t)((q & 3) == 0 ? o4[q >> 2].x : (q & 3) == 1 ? o4[q >> 2].y : (q & 3) == 2 ? o4[q >> 2].z : o4[q >> 2].w) * cnt)
+    if (nvalid >= 32) {
+#pragma unroll
+        for (uint32_t q = 0; q < 32; q++) o[q * Dv] = ZG_UMMA_VAL(q);
+    } else {
+#pragma unroll
+        for (uint32_t q = 0; q < 32; q++)
+            if (q < nvalid) o[q * Dv] = ZG_UMMA_VAL(q);
+    }
+#undef ZG_UMMA_VAL
+}
+
+// One tile per CTA (4 warps).
+template <uint32_t NT, uint32_t DS>
 __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ evals,
                                                    const uint8_t *__restrict__ bm_img,
-                                                   const int32_t *__restrict__ bm_off,
+                                                   const int32_t *__restrict__ bm_noff,
                                                    int32_t *__restrict__ out, uint32_t row_len,
                                                    uint32_t bd, uint32_t bl, uint32_t kp,
                                                    uint32_t depth, uint32_t nch, uint32_t C,
@@ -441,8 +528,7 @@ __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ 
     uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + 2 * NT * kp);  // loaded, MMA done
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t ppt = 128 / lp, halves = lp / 32, atoms = kp / 128;
-    const uint32_t mt = blockIdx.x, nt = blockIdx.y;
+    const uint32_t atoms = kp / 128, mt = blockIdx.x, nt = blockIdx.y;
 
     if (warp == 0) {
         tmem_alloc(tslot, kCols);
@@ -468,38 +554,7 @@ __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ 
                          bm_img + ((((size_t)t_img * 2 + l) * atoms + a) * kUmmaImgRows + row0) * 128,
                          NT * 128, &bars[0]);
     }
-
-    // A tile: row m = pi * lp + 32 * hw + lane bit, byte k = bit of evaluation k
-    const uint32_t shift = 3 * depth;
-    const uint32_t ntask = ppt * halves * (kp / 8);
-    for (uint32_t task = tid; task < ntask; task += 128) {
-        const uint32_t pi = task % ppt, rest = task / ppt;
-        const uint32_t hw = rest % halves, g8 = rest / halves;
-        const uint32_t gp = mt * ppt + pi;
-        uint32_t x[8];
-        if (gp < npairs) {
-            const uint64_t *src = evals + (size_t)(gp / nch) * row_len + (gp % nch);
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const uint32_t k = 8 * g8 + i;
-                x[i] = k < bl ? (uint32_t)((__ldg(src + ((size_t)k << shift)) & dmask) >> (32 * hw)) : 0u;
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 8; i++) x[i] = 0;
-        }
-#pragma unroll
-        for (uint32_t g = 0; g < 8; g++) {
-            uint32_t b0[4], b1[4];
-            bits_to_bfrag(x[0], x[1], x[2], x[3], g, b0);
-            bits_to_bfrag(x[4], x[5], x[6], x[7], g, b1);
-#pragma unroll
-            for (uint32_t bb = 0; bb < 4; bb++) {
-                const uint32_t m = pi * lp + 32 * hw + g + 8 * bb;
-                *reinterpret_cast<uint2 *>(As + sw128_offset(m, 8 * g8, 128)) = make_uint2(b0[bb], b1[bb]);
-            }
-        }
-    }
+    umma_fill_a(As, evals, mt, tid, 128, lp, kp, bl, 3 * depth, nch, row_len, dmask, npairs);
     fence_async_smem();
     __syncthreads();
 
@@ -523,25 +578,15 @@ __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ 
             mma_commit(&bars[1]);
         }
     }
+    __syncwarp();
 
-    // popcount of this thread's A row (row m = tid), while the MMAs run
-    uint32_t cnt = 0;
-    for (uint32_t a = 0; a < atoms; a++)
-#pragma unroll
-        for (uint32_t j = 0; j < 8; j++) {
-            const uint4 v = *reinterpret_cast<const uint4 *>(As + a * 128 * 128 + tid * 128 + j * 16);
-            cnt = __dp4a(v.x, 0x01010101u, cnt);
-            cnt = __dp4a(v.y, 0x01010101u, cnt);
-            cnt = __dp4a(v.z, 0x01010101u, cnt);
-            cnt = __dp4a(v.w, 0x01010101u, cnt);
-        }
-
+    const uint32_t cnt = umma_row_popcount(As, tid, atoms);  // while the MMAs run
     const bool done = mbar_wait(&bars[1], 0);
     tc_fence_after();
     const bool ok = done && loaded;
     if (!done && lane == 0) atomicOr(status, kStatusMmaTimeout);
     if (ok) {
-        const uint32_t gp = mt * ppt + tid / lp, ln = tid % lp;
+        const uint32_t ppt = 128 / lp, gp = mt * ppt + tid / lp, ln = tid % lp;
         const bool live = gp < npairs && ln < D;
         size_t ob = 0;
         if (live) {
@@ -551,20 +596,9 @@ __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ 
         const uint32_t lane_base = tmem + ((32 * warp) << 16);
 #pragma unroll 1
         for (uint32_t c = 0; c < NT / 32; c++) {
-            uint32_t lo[32], hi[32];
-            tmem_ld32(lane_base + 32 * c, lo);
-            tmem_ld32(lane_base + NT + 32 * c, hi);
-            tmem_wait_ld();
             const uint32_t r0 = nt * NT + 32 * c;
-            if (live) {
-#pragma unroll
-                for (uint32_t j = 0; j < 32; j++) {
-                    const uint32_t r = r0 + j;
-                    if (r < bd)
-                        out[ob + (size_t)r * D] =
-                            (int32_t)(lo[j] + (hi[j] << 8) - (uint32_t)__ldg(bm_off + r) * cnt);
-                }
-            }
+            umma_store_chunk<DS, NT>(lane_base + 32 * c, bm_noff, r0, live, out + ob + (size_t)r0 * D, cnt, D,
+                                     r0 < bd ? bd - r0 : 0);
         }
     }
     // on a timeout, give copies and MMAs still in flight a second bounded wait
@@ -572,6 +606,191 @@ __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ 
     if (tid == 0 && !done) mbar_wait(&bars[1], 0);
     tc_fence_before();
     __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kCols);
+    }
+}
+
+// Persistent, warp-specialised form of k_base_umma.  One CTA per SM walks a
+// contiguous range of tiles in (m-tile, n-tile) order, so most consecutive
+// tiles share their input rows, which are expanded once per m-tile.  Roles:
+//   warps 0-7   epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (one A row
+//               per thread) and columns of half w / 4 of the tile;
+//   warp 8      producer: one bulk copy per (limb, atom) of the next base tile;
+//   warp 9      MMA issuer: 2 x kp/32 MMAs per tile into one of two
+//               accumulator sets, committed to the operand and TMEM barriers;
+//   warps 10-11 A expansion: input bits of the next m-tile and their per-row
+//               popcounts.
+// A and B tiles are double-buffered in shared memory and the accumulators in
+// TMEM (4 NT columns), so the MMAs of tile j+1 overlap the epilogue of tile j.
+// Every wait is bounded; a timeout sets the shared abort word, every role
+// leaves its loop, in-flight copies and MMAs get one more bounded wait, and
+// the CTA frees its tensor memory and returns.
+constexpr uint32_t kUmmaEpiWarps = 8;
+constexpr uint32_t kUmmaPThreads = 32 * (kUmmaEpiWarps + 4);
+
+template <uint32_t NT, uint32_t DS>
+__global__ void __launch_bounds__(kUmmaPThreads, 1) k_base_umma_p(const uint64_t *__restrict__ evals,
+                                                                 const uint8_t *__restrict__ bm_img,
+                                                                 const int32_t *__restrict__ bm_noff,
+                                                                 int32_t *__restrict__ out, uint32_t row_len,
+                                                                 uint32_t bd, uint32_t bl, uint32_t kp,
+                                                                 uint32_t depth, uint32_t nch, uint32_t C,
+                                                                 uint32_t D, uint64_t dmask, uint32_t npairs,
+                                                                 uint32_t lp, uint32_t ntn, uint32_t ntiles,
+                                                                 uint32_t *status) {
+    using namespace umma;
+    constexpr uint32_t kAcc = 2 * NT;    // one accumulator set: two limbs of NT columns
+    constexpr uint32_t kCols = 2 * kAcc; // two sets
+    constexpr uint32_t kEpiThreads = 32 * kUmmaEpiWarps;
+    constexpr uint32_t kProducer = kUmmaEpiWarps, kIssuer = kUmmaEpiWarps + 1, kExpand = kUmmaEpiWarps + 2;
+    extern __shared__ __align__(16) uint8_t smem_u[];
+    uint8_t *As = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_u) + 1023) & ~uintptr_t(1023));
+    const uint32_t a_bytes = 128 * kp, b_bytes = 2 * NT * kp;
+    uint8_t *Bs = As + 2 * a_bytes;
+    uint32_t *cnt_s = reinterpret_cast<uint32_t *>(Bs + 2 * b_bytes);  // [2][128]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(cnt_s + 256);
+    uint64_t *a_full = bars, *a_empty = bars + 2, *b_full = bars + 4, *b_empty = bars + 6;
+    uint64_t *t_full = bars + 8, *t_empty = bars + 10, *fin = bars + 12;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 13);
+    volatile uint32_t *abort = tslot + 1;
+    uint32_t *go = tslot + 2;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t ppt = 128 / lp, atoms = kp / 128;
+    const uint32_t t0 = (uint32_t)((uint64_t)blockIdx.x * ntiles / gridDim.x);
+    const uint32_t t1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * ntiles / gridDim.x);
+
+    if (warp == 0) {
+        tmem_alloc(tslot, kCols);
+        tmem_relinquish();
+    }
+    if (tid == 32) {
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&a_full[i], 64);               // the expansion threads
+            mbar_init(&a_empty[i], 1 + kEpiThreads); // MMA commit + the epilogue's popcount reads
+            mbar_init(&b_full[i], 1);
+            mbar_init(&b_empty[i], 1);
+            mbar_init(&t_full[i], 1);
+            mbar_init(&t_empty[i], kEpiThreads);
+        }
+        mbar_init(fin, 1);
+        *abort = 0;
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == kProducer) {
+        if (lane == 0) {
+            int last_par[2] = {-1, -1};
+            for (uint32_t t = t0, j = 0; t < t1; t++, j++) {
+                const uint32_t s = j & 1;
+                if (!mbar_wait_or_abort(&b_empty[s], ((j >> 1) & 1) ^ 1, abort)) break;
+                const uint32_t n = t % ntn;
+                const uint32_t t_img = (n * NT) / kUmmaImgRows, row0 = (n * NT) % kUmmaImgRows;
+                mbar_arrive_expect_tx(&b_full[s], b_bytes);
+                for (uint32_t l = 0; l < 2; l++)
+                    for (uint32_t a = 0; a < atoms; a++)
+                        bulk_g2s(Bs + s * b_bytes + (l * atoms + a) * NT * 128,
+                                 bm_img + ((((size_t)t_img * 2 + l) * atoms + a) * kUmmaImgRows + row0) * 128,
+                                 NT * 128, &b_full[s]);
+                last_par[s] = (int)((j >> 1) & 1);
+            }
+            // copies still in flight (none on the normal path)
+            for (int s = 0; s < 2; s++)
+                if (last_par[s] >= 0) mbar_wait(&b_full[s], (uint32_t)last_par[s]);
+        }
+        __syncwarp();
+    } else if (warp == kIssuer) {
+        if (lane == 0) {
+            const uint32_t id_lo = idesc_i8(128, NT, false, false), id_hi = idesc_i8(128, NT, true, true);
+            uint32_t u = 0;
+            for (uint32_t t = t0, j = 0; t < t1; t++, j++) {
+                const uint32_t m = t / ntn;
+                const bool new_m = t == t0 || m != (t - 1) / ntn;
+                if (new_m && t != t0) u++;
+                const uint32_t sa = u & 1, s = j & 1, acc = j & 1;
+                if (new_m && !mbar_wait_or_abort(&a_full[sa], (u >> 1) & 1, abort)) break;
+                if (!mbar_wait_or_abort(&b_full[s], (j >> 1) & 1, abort)) break;
+                if (!mbar_wait_or_abort(&t_empty[acc], ((j >> 1) & 1) ^ 1, abort)) break;
+                tc_fence_after();
+                const uint32_t a0 = smem_u32(As + sa * a_bytes), b0 = smem_u32(Bs + s * b_bytes);
+                const uint32_t b1 = b0 + atoms * NT * 128, d = tmem + acc * kAcc;
+                for (uint32_t ks = 0; ks < kp / 32; ks++) {
+                    const uint32_t a = ks >> 2, o = (ks & 3) * 32;
+                    const uint64_t ad = sdesc_k_sw128(a0 + a * 128 * 128 + o);
+                    mma_i8(d, ad, sdesc_k_sw128(b0 + a * NT * 128 + o), id_lo, ks > 0);
+                    mma_i8(d + NT, ad, sdesc_k_sw128(b1 + a * NT * 128 + o), id_hi, ks > 0);
+                }
+                mma_commit(&b_empty[s]);
+                mma_commit(&t_full[acc]);
+                if (t + 1 == t1 || (t + 1) / ntn != m) mma_commit(&a_empty[sa]);
+            }
+            mma_commit(fin);
+            mbar_wait(fin, 0);  // every MMA retired
+        }
+        __syncwarp();
+    } else if (warp >= kExpand) {
+        // A expansion: 64 threads; one of them waits, all follow its verdict
+        const uint32_t et = tid - 32 * kExpand;
+        uint32_t u = 0;
+        for (uint32_t t = t0; t < t1; t++) {
+            const uint32_t m = t / ntn;
+            if (t != t0 && m == (t - 1) / ntn) continue;
+            const uint32_t sa = u & 1;
+            if (et == 0) *go = mbar_wait_or_abort(&a_empty[sa], ((u >> 1) & 1) ^ 1, abort) ? 1u : 0u;
+            named_bar_sync(1, 64);
+            if (!*go) break;
+            uint8_t *A = As + sa * a_bytes;
+            umma_fill_a(A, evals, m, et, 64, lp, kp, bl, 3 * depth, nch, row_len, dmask, npairs);
+            named_bar_sync(1, 64);
+            for (uint32_t row = et; row < 128; row += 64) cnt_s[sa * 128 + row] = umma_row_popcount(A, row, atoms);
+            fence_async_smem();
+            mbar_arrive(&a_full[sa]);
+            u++;
+        }
+    } else {
+        // epilogue: TMEM lane / A row `row`, columns of half `h` of the tile
+        const uint32_t qd = warp & 3, h = warp >> 2, row = 32 * qd + lane, ln = row % lp;
+        constexpr uint32_t kChunks = NT / 32 / (kUmmaEpiWarps / 4);
+        uint32_t u = 0, cnt = 0;
+        for (uint32_t t = t0, j = 0; t < t1; t++, j++) {
+            const uint32_t m = t / ntn, n = t % ntn;
+            const bool new_m = t == t0 || m != (t - 1) / ntn;
+            if (new_m && t != t0) u++;
+            const uint32_t acc = j & 1;
+            bool ok = mbar_wait_or_abort(&t_full[acc], (j >> 1) & 1, abort);
+            if (ok && new_m) ok = mbar_wait_or_abort(&a_full[u & 1], (u >> 1) & 1, abort);
+            if (!__all_sync(0xFFFFFFFFu, ok)) break;
+            tc_fence_after();
+            if (new_m) {
+                cnt = cnt_s[(u & 1) * 128 + row];
+                mbar_arrive(&a_empty[u & 1]);
+            }
+            const uint32_t gp = m * ppt + row / lp;
+            const bool live = gp < npairs && ln < D;
+            size_t ob = 0;
+            if (live) {
+                const uint32_t ch = octet_reverse(gp % nch, depth);
+                ob = ((size_t)(gp / nch) * C + (size_t)ch * bd) * D + ln;
+            }
+            const uint32_t lane_base = tmem + ((32 * qd) << 16) + acc * kAcc;
+#pragma unroll 1
+            for (uint32_t c = h * kChunks; c < (h + 1) * kChunks; c++) {
+                const uint32_t r0 = n * NT + 32 * c;
+                umma_store_chunk<DS, NT>(lane_base + 32 * c, bm_noff, r0, live, out + ob + (size_t)r0 * D, cnt, D,
+                                         r0 < bd ? bd - r0 : 0);
+            }
+            tc_fence_before();
+            mbar_arrive(&t_empty[acc]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0 && *abort) atomicOr(status, kStatusMmaTimeout);
     if (warp == 0) {
         tc_fence_after();
         tmem_dealloc(tmem, kCols);
@@ -1079,9 +1298,40 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         if (depth == 0) return base_launch(out_d, true, leaf_major);
         ZG_TRY(ctx->stage_a.ensure((size_t)nrows * C * D * 4));
         int32_t *base = ctx->stage_a.as<int32_t>();
-        // tcgen05 base layer (default; variants 6 = 128 and 7 = 64 base rows per tile)
+        // tcgen05 base layer, persistent and warp-specialised (default; variants
+        // 6 = 128 and 7 = 64 base rows per tile), one CTA per SM
         if (p->d_bmU && D <= 64 && (base_variant == -1 || base_variant == 6 || base_variant == 7)) {
             const uint32_t NT = base_variant == 7 ? 64 : 128;
+            const uint32_t lp = D <= 32 ? 32 : 64, kp = p->umma_kp;
+            const uint64_t npairs = (uint64_t)nrows * nch;
+            const uint64_t ntm = (npairs + 128 / lp - 1) / (128 / lp), ntn = (bd + NT - 1) / NT;
+            const uint64_t ntiles = ntm * ntn;
+            const size_t smem_p = 1024 + (size_t)2 * 128 * kp + (size_t)2 * 2 * NT * kp + 1024 + 128;
+            if (smem_p <= (size_t)max_smem_optin() && ntiles < (1ull << 31) && npairs < (1ull << 32)) {
+                const unsigned g = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)std::max(ctx->num_sms, 1));
+                ZG_KBEGIN(ctx, s, "k_base_bin");
+#define ZG_UMMA_P(NTV, DSV)                                                                              \
+    do {                                                                                                 \
+        ZG_CUDA(allow_max_smem(k_base_umma_p<NTV, DSV>));                                                \
+        k_base_umma_p<NTV, DSV><<<g, kUmmaPThreads, smem_p, s>>>(ev, p->d_bmU, p->d_bmOff, base, L, bd, bl, kp, \
+                                                                 depth, nch, C, D, dmask, (uint32_t)npairs, lp, \
+                                                                 (uint32_t)ntn, (uint32_t)ntiles, ctx->status); \
+    } while (0)
+                if (NT == 64) {
+                    if (D == 32) ZG_UMMA_P(64, 32); else if (D == 64) ZG_UMMA_P(64, 64); else ZG_UMMA_P(64, 0);
+                } else {
+                    if (D == 32) ZG_UMMA_P(128, 32); else if (D == 64) ZG_UMMA_P(128, 64); else ZG_UMMA_P(128, 0);
+                }
+#undef ZG_UMMA_P
+                ZG_KEND(ctx, s);
+                goto stages;
+            }
+        }
+        // tcgen05 base layer, one tile per CTA (variant 8 = 128 base rows per
+        // tile, 9 = 64; also when the persistent kernel's buffers do not fit)
+        if (p->d_bmU && D <= 64 && (base_variant == -1 || base_variant == 6 || base_variant == 7 ||
+                                    base_variant == 8 || base_variant == 9)) {
+            const uint32_t NT = (base_variant == 7 || base_variant == 9) ? 64 : 128;
             const uint32_t lp = D <= 32 ? 32 : 64, kp = p->umma_kp;
             const uint64_t npairs = (uint64_t)nrows * nch;
             // operand tiles, barriers and TMEM slot, 1024-byte alignment slack; at
@@ -1093,17 +1343,19 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
             if (smem_u <= (size_t)max_smem_optin() && gx < (1ull << 31)) {
                 dim3 gu((unsigned)gx, (bd + NT - 1) / NT);
                 ZG_KBEGIN(ctx, s, "k_base_bin");
+#define ZG_UMMA_S(NTV, DSV)                                                                              \
+    do {                                                                                                 \
+        ZG_CUDA(allow_max_smem(k_base_umma<NTV, DSV>));                                                  \
+        k_base_umma<NTV, DSV><<<gu, 128, smem_u, s>>>(ev, p->d_bmU, p->d_bmOff, base, L, bd, bl, kp, depth, nch, C, \
+                                                      D, dmask, (uint32_t)npairs, lp, ctx->status);      \
+    } while (0)
                 if (NT == 64) {
-                    ZG_CUDA(allow_max_smem(k_base_umma<64>));
-                    k_base_umma<64><<<gu, 128, smem_u, s>>>(ev, p->d_bmU, p->d_bmOff, base, L, bd, bl, kp, depth, nch, C,
-                                                            D, dmask, (uint32_t)npairs, lp, ctx->status);
+                    if (D == 32) ZG_UMMA_S(64, 32); else if (D == 64) ZG_UMMA_S(64, 64); else ZG_UMMA_S(64, 0);
                 } else {
-                    ZG_CUDA(allow_max_smem(k_base_umma<128>));
-                    k_base_umma<128><<<gu, 128, smem_u, s>>>(ev, p->d_bmU, p->d_bmOff, base, L, bd, bl, kp, depth, nch,
-                                                             C, D, dmask, (uint32_t)npairs, lp, ctx->status);
+                    if (D == 32) ZG_UMMA_S(128, 32); else if (D == 64) ZG_UMMA_S(128, 64); else ZG_UMMA_S(128, 0);
                 }
+#undef ZG_UMMA_S
                 ZG_KEND(ctx, s);
-                base_variant = 0;  // done: skip the other base kernels below
                 goto stages;
             }
         }

@@ -201,7 +201,7 @@ struct zg_params {
     // rows, two limbs (u8 low byte, s8 high byte) of bm[r][c] + bm_off[r], each
     // [round_up(base_len, 128) / 128][kUmmaImgRows][128] in the 128-byte
     // swizzle; bm_off[r] puts row r in [-2^15, 2^15).  NULL when a row spans
-    // more than 2^16 values.
+    // more than 2^16 values.  d_bmOff holds -bm_off, padded to whole tiles.
     uint8_t *d_bmU = nullptr;
     int32_t *d_bmOff = nullptr;
     uint32_t umma_kp = 0;  // round_up(base_len, 128)

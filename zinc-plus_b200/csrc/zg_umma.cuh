@@ -3,7 +3,7 @@
 // issue and commit, TMEM loads, and the shared-memory and instruction
 // descriptors they take.  Inline PTX, one instruction per wrapper.
 //
-// Every wait is bounded: mbar_wait gives up after a wall-clock limit and
+// Every wait is bounded: mbar_wait gives up after a cycle limit and
 // returns false, so that a kernel can record the failure, release its tensor
 // memory and return instead of spinning.
 #pragma once
@@ -12,8 +12,9 @@
 namespace zg {
 namespace umma {
 
-// Upper bound of one mbarrier wait, in nanoseconds of %globaltimer.
-constexpr uint64_t kWaitLimitNs = 1000000000ull;
+// Upper bound of one mbarrier wait, in SM clock cycles (clock64: a cheap
+// per-SM counter; 2^31 cycles is about a second at the B200's clocks).
+constexpr long long kWaitLimitCycles = 1ll << 31;
 
 // Codes written to the device status word (device_status_word) by a kernel
 // whose wait ran out.
@@ -21,12 +22,6 @@ enum : uint32_t { kStatusLoadTimeout = 1, kStatusMmaTimeout = 2 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
@@ -57,7 +52,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // time limit passed first.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     const uint32_t a = smem_u32(bar);
-    const uint64_t t0 = global_ns();
+    const long long t0 = clock64();
     for (;;) {
         uint32_t done;
         asm volatile(
@@ -68,8 +63,37 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
-        if (global_ns() - t0 > kWaitLimitNs) return false;
+        if (clock64() - t0 > kWaitLimitCycles) return false;
     }
+}
+
+// mbar_wait that also gives up once *abort (shared memory) is set, and sets it
+// on its own timeout: the roles of a warp-specialised kernel then leave their
+// loops together instead of each waiting out its own limit.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t parity, volatile uint32_t *abort) {
+    const uint32_t a = smem_u32(bar);
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (*abort) return false;
+        if (clock64() - t0 > kWaitLimitCycles) {
+            *abort = 1;
+            return false;
+        }
+    }
+}
+
+// Named barrier over `nthreads` threads (a multiple of 32) of the CTA.
+__device__ __forceinline__ void named_bar_sync(uint32_t id, uint32_t nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 // Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
