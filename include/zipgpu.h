@@ -116,6 +116,17 @@ void *zg_ctx_stream(zg_ctx *ctx);
  * the totals; *len receives the length needed. */
 zg_status zg_ctx_set_kernel_timing(zg_ctx *ctx, int enable);
 zg_status zg_ctx_kernel_timing_report(zg_ctx *ctx, char *buf, size_t cap, size_t *len);
+/* Failure detection self-test (no counterpart in the reference).  The
+ * tensor-core kernels bound every wait on an mbarrier (about a second); a wait
+ * that runs out makes the kernel skip its work, free its tensor memory, return,
+ * and write a code into the device's status word, which every later
+ * synchronisation reports as ZG_ERR_CUDA.  This call runs a one-block probe
+ * whose wait can never complete (nothing arrives on its barrier), waits for
+ * it, writes the status word it left (4 = the probe's timeout code) to
+ * *status_seen, and clears the word.  It takes about a second; the context
+ * stays usable.  Run it while no other work is in flight on the device: it
+ * clears the device's word. */
+zg_status zg_selftest_bounded_wait(zg_ctx *ctx, uint32_t *status_seen);
 
 /* ---- setup: ZipPlus::setup + IprsCode::new / RaaCode::new -----------------
  * ctx may be NULL for host-only parameters (tables, encode_wide, verify);

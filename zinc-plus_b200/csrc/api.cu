@@ -828,6 +828,24 @@ uint64_t zg_ctx_kernel_launches(const zg_ctx *ctx) {
     return n;
 }
 
+zg_status zg_selftest_bounded_wait(zg_ctx *ctx, uint32_t *status_seen) {
+    if (!ctx || !status_seen) return ZG_ERR_INVALID_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    ZG_CUDA(cudaDeviceSynchronize());
+    *status_seen = 0;
+    if (device_status_value(ctx->device) != 0) {
+        set_error("device %d already reported a timed-out wait (status %u)", ctx->device,
+                  device_status_value(ctx->device));
+        return ZG_ERR_CUDA;
+    }
+    ZG_TRY(launch_wait_probe(ctx, ctx->stream));
+    ZG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *status_seen = device_status_value(ctx->device);
+    device_status_clear(ctx->device);
+    return ZG_OK;
+}
+
 zg_status zg_ctx_set_kernel_timing(zg_ctx *ctx, int enable) {
     if (!ctx) return ZG_ERR_INVALID_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);

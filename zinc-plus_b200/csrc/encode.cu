@@ -562,7 +562,7 @@ __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ 
     const bool loaded = mbar_wait(&bars[0], 0);
     if (tid == 0) {
         if (!loaded) {
-            atomicOr(status, kStatusLoadTimeout);
+            report_status(status, kStatusLoadTimeout);
             mbar_arrive(&bars[1]);
         } else {
             tc_fence_after();
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(128) k_base_umma(const uint64_t *__restrict__ 
     const bool done = mbar_wait(&bars[1], 0);
     tc_fence_after();
     const bool ok = done && loaded;
-    if (!done && lane == 0) atomicOr(status, kStatusMmaTimeout);
+    if (!done && lane == 0) report_status(status, kStatusMmaTimeout);
     if (ok) {
         const uint32_t ppt = 128 / lp, gp = mt * ppt + tid / lp, ln = tid % lp;
         const bool live = gp < npairs && ln < D;
@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(kUmmaPThreads, 1) k_base_umma_p(const uint64_t
     }
     tc_fence_before();
     __syncthreads();
-    if (tid == 0 && *abort) atomicOr(status, kStatusMmaTimeout);
+    if (tid == 0 && *abort) report_status(status, kStatusMmaTimeout);
     if (warp == 0) {
         tc_fence_after();
         tmem_dealloc(tmem, kCols);

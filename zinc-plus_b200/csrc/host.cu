@@ -250,6 +250,16 @@ uint32_t *device_status_word(int device) {
     return static_cast<uint32_t *>(d);
 }
 
+uint32_t device_status_value(int device) {
+    if (!status_host || device < 0 || device >= kMaxDevices) return 0;
+    return reinterpret_cast<volatile uint32_t *>(status_host)[device];
+}
+
+void device_status_clear(int device) {
+    if (!status_host || device < 0 || device >= kMaxDevices) return;
+    reinterpret_cast<volatile uint32_t *>(status_host)[device] = 0;
+}
+
 cudaError_t device_status(int device) {
     if (!status_host || device < 0 || device >= kMaxDevices) return cudaSuccess;
     const uint32_t v = reinterpret_cast<volatile uint32_t *>(status_host)[device];

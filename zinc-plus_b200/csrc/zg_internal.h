@@ -109,10 +109,16 @@ void ctx_cache_trim(zg_ctx *ctx, size_t max_bytes);
 // when the context has a blocking-sync event).
 cudaError_t ctx_sync(zg_ctx *ctx);
 // Status word of a device, in mapped pinned host memory: a kernel whose
-// bounded wait ran out ORs a code into it (umma::kStatus*), skips its work and
+// bounded wait ran out writes a code into it (umma::kStatus*), skips its work and
 // returns.  device_status reports a set word as cudaErrorLaunchTimeout.
 uint32_t *device_status_word(int device);
 cudaError_t device_status(int device);
+// Current value of a device's status word, and its reset to 0 (both with the
+// device's work drained).
+uint32_t device_status_value(int device);
+void device_status_clear(int device);
+// One-block kernel whose mbarrier wait runs out and sets kStatusProbeTimeout.
+zg_status launch_wait_probe(zg_ctx *ctx, cudaStream_t s);
 // Routes a fresh context's hint blocks and scratch through a memory pool.
 void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool);
 // Device bytes held by a context's scratch arenas, and their release.

@@ -18,7 +18,16 @@ constexpr long long kWaitLimitCycles = 1ll << 31;
 
 // Codes written to the device status word (device_status_word) by a kernel
 // whose wait ran out.
-enum : uint32_t { kStatusLoadTimeout = 1, kStatusMmaTimeout = 2 };
+enum : uint32_t { kStatusLoadTimeout = 1, kStatusMmaTimeout = 2, kStatusProbeTimeout = 4 };
+
+// Records a timed-out wait in the device status word (mapped pinned host
+// memory): a plain system-scope store, which every host link supports (device
+// atomics on host memory need native host atomics).  Concurrent reporters may
+// overwrite each other's code; the word is nonzero either way.
+__device__ __forceinline__ void report_status(uint32_t *status, uint32_t code) {
+    *reinterpret_cast<volatile uint32_t *>(status) = code;
+    __threadfence_system();
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);

@@ -48,6 +48,7 @@ EXPORTS = (
     "zg_commit_prove", "zg_commit_prove_d", "zg_commit_prove_many", "zg_proof_size", "zg_verify",
     "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch", "zg_server_create",
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
+    "zg_selftest_bounded_wait",
 )
 
 
@@ -128,6 +129,7 @@ def lib() -> C.CDLL:
         "zg_ctx_kernel_launches": ([vp], C.c_uint64), "zg_ctx_stream": ([vp], vp),
         "zg_ctx_set_kernel_timing": ([vp, C.c_int], st),
         "zg_ctx_kernel_timing_report": ([vp, C.c_char_p, sz, C.POINTER(sz)], st),
+        "zg_selftest_bounded_wait": ([vp, C.POINTER(C.c_uint32)], st),
         "zg_params_create": ([vp, C.POINTER(ParamsDesc), C.POINTER(vp)], st),
         "zg_params_destroy": ([vp], st),
         "zg_params_get_info": ([vp, C.POINTER(ParamsInfo)], st),
@@ -213,6 +215,13 @@ class Context:
             name, cnt, ms = line.rsplit(",", 2)
             out[name] = (int(cnt), float(ms))
         return out
+
+    def selftest_bounded_wait(self) -> int:
+        """Runs a probe kernel whose bounded wait must run out (about a second)
+        and returns the device status code it reported (4), clearing it."""
+        v = C.c_uint32()
+        check(lib().zg_selftest_bounded_wait(self.handle, C.byref(v)))
+        return v.value
 
     def close(self):
         if getattr(self, "handle", None):
