@@ -175,3 +175,23 @@ def test_batch_commit_rejects_bad_input(zipgpu, ctx, rng):
         zipgpu.ZipPlus.commit_batch([pp], [], ctx)
     with pytest.raises(ValueError):  # wrong size
         zipgpu.ZipPlus.commit_batch([pp], [binary_evals(rng, 512, 32)], ctx)
+
+
+# (D, num_vars, row_len, depth): odd lane counts (one 32-lane half padded, or two
+# halves), K padded to 128 (base_len 2..128), base dimensions below and above the
+# 64 / 128-row tiles, several codeword rows
+UMMA_SHAPES = [(3, 10, 256, 0), (17, 12, 1024, 0), (40, 12, 4096, 3), (64, 14, 4096, 0),
+               (32, 14, 1 << 14, 0), (8, 12, 1024, 1), (32, 16, 1 << 12, 0)]
+
+
+@pytest.mark.parametrize("variant", [6, 7, 8, 9])
+def test_tcgen05_base_variants_match_oracle(zipgpu, oracle, ctx, rng, variant):
+    """Each tcgen05 base-layer kernel (persistent / one tile per block, 128 or 64
+    base rows per tile) gives the oracle's roots on every shape."""
+    opts = zipgpu.BatchOpts.make(lanes=1, use_graph=False, autotune=False, base_variant=variant,
+                                 leaf_variant=-1)
+    for D, nv, L, depth in UMMA_SHAPES:
+        pp = params_for(zipgpu, 1, D, 0, nv, L, depth, ctx=ctx)
+        ev = binary_evals(rng, 1 << nv, D)
+        got = zipgpu.ZipPlus.commit_batch([pp], [ev], ctx, opts)
+        assert got[0].root == oracle.commit(desc_for(1, D, 0, nv, L, depth), ev, 1), (D, nv, L, depth)
