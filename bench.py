@@ -86,30 +86,79 @@ def config_of(workload, num_rows, depth):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi sampling during the timed region."""
+    """SM clocks and clock-event reasons during the timed region: NVML read from
+    a thread every 10 ms (reads only), with nvidia-smi as the fallback."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self, nv):
+        try:  # the CUDA device's PCI address (CUDA and NVML may number devices differently)
+            import torch
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
+        try:
+            import threading
+
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            self.stop_flag = threading.Event()
+
+            def run():
+                while not self.stop_flag.is_set():
+                    try:
+                        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.rows.append((sm, mx, [n for n, b in zip(self.NAMES, bits) if r & b]))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.01)
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.out = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
     def stop(self):
+        if self.thread:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            rows = list(self.rows)
+            if not rows:
+                return None
+            sm = [r[0] for r in rows]
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(r[1] for r in rows),
+                    "reasons": sorted({n for r in rows for n in r[2]}), "samples": len(rows),
+                    "source": "NVML, every 10 ms over the timed region"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -128,11 +177,10 @@ class ClockSampler:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi -lms 20"}
 
 
 # ------------------------------------------------------------ CPU baseline
