@@ -66,7 +66,10 @@ typedef enum {
 } zg_status;
 
 typedef enum { ZG_EVAL_I32 = 0, ZG_EVAL_BINPOLY = 1 } zg_eval_kind;
-typedef enum { ZG_CODE_IPRS = 0, ZG_CODE_RAA = 1 } zg_code_kind;
+/* ZG_CODE_RAA_SIGN_FLIP: RaaSignFlippingCode (zip-plus/src/code/raa_sign_flip.rs:
+ * 14-69), the RAA code with entries 1, 3, 5, ... negated after the repetition
+ * and after the first accumulation; same permutations and width check. */
+typedef enum { ZG_CODE_IPRS = 0, ZG_CODE_RAA = 1, ZG_CODE_RAA_SIGN_FLIP = 2 } zg_code_kind;
 
 /* One ZipTypes instantiation plus its linear code and matrix shape.
  * The reference fixes these through type parameters (pcs/structs.rs:15-60):

@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libzipref.so")
 
 EVAL_I32, EVAL_BINPOLY = 0, 1
-CODE_IPRS, CODE_RAA = 0, 1
+CODE_IPRS, CODE_RAA, CODE_RAA_SIGN_FLIP = 0, 1, 2
 
 
 class Desc(C.Structure):

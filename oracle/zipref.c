@@ -686,10 +686,12 @@ static void pntt_binary(const iprs_params *p, const uint64_t *in, uint32_t D, in
 typedef struct {
     uint32_t row_len, codeword_len;
     uint32_t *perm1, *perm2;
+    int flip; /* RaaSignFlippingCode (zip-plus/src/code/raa_sign_flip.rs:31-69) */
 } raa_params;
 
-static int raa_build(uint32_t row_len, uint32_t rep, raa_params *r) {
+static int raa_build(uint32_t row_len, uint32_t rep, int flip, raa_params *r) {
     if (row_len == 0 || (row_len & (row_len - 1)) || rep == 0 || (rep & (rep - 1))) return -1;
+    r->flip = flip;
     r->row_len = row_len;
     r->codeword_len = row_len * rep;
     r->perm1 = (uint32_t *)malloc(sizeof(uint32_t) * r->codeword_len);
@@ -703,12 +705,29 @@ static void raa_free(raa_params *r) {
     free(r->perm2);
 }
 
-/* encode_inner (raa.rs:93-127) on lanes of wrapping multi-limb values. */
+/* flip_even_signs (raa_sign_flip.rs:135-165): negate entries 1, 3, 5, ... of
+ * n elements of esz wrapping limbs (each entry is lanes x limbs). */
+static void flip_odd_entries(uint64_t *v, size_t n, uint32_t lanes, uint32_t limbs) {
+    for (size_t i = 1; i < n; i += 2)
+        for (uint32_t l = 0; l < lanes; l++) {
+            uint64_t *x = v + (i * lanes + l) * limbs;
+            u128 c = 1;
+            for (uint32_t w = 0; w < limbs; w++) {
+                u128 s = (u128)(~x[w]) + c;
+                x[w] = (uint64_t)s;
+                c = s >> 64;
+            }
+        }
+}
+
+/* encode_inner (raa.rs:93-127; with sign flips raa_sign_flip.rs:31-69) on
+ * lanes of wrapping multi-limb values. */
 static void raa_encode_wide(const raa_params *r, const uint64_t *in, uint64_t *out, uint32_t lanes,
                             uint32_t limbs) {
     size_t esz = (size_t)lanes * limbs, n = r->codeword_len;
     uint64_t *a = (uint64_t *)malloc(sizeof(uint64_t) * n * esz);
     for (size_t i = 0; i < n; i++) memcpy(a + i * esz, in + (i % r->row_len) * esz, 8 * esz);
+    if (r->flip) flip_odd_entries(a, n, lanes, limbs);
     for (int pass = 0; pass < 2; pass++) {
         const uint32_t *perm = pass == 0 ? r->perm1 : r->perm2;
         for (size_t i = 0; i < n; i++) memcpy(out + i * esz, a + (size_t)perm[i] * esz, 8 * esz);
@@ -723,7 +742,10 @@ static void raa_encode_wide(const raa_params *r, const uint64_t *in, uint64_t *o
                 }
             }
         }
-        if (pass == 0) memcpy(a, out, 8 * n * esz);
+        if (pass == 0) {
+            memcpy(a, out, 8 * n * esz);
+            if (r->flip) flip_odd_entries(a, n, lanes, limbs);
+        }
     }
     free(a);
 }
@@ -735,13 +757,19 @@ static void raa_binary(const raa_params *r, const uint64_t *in, uint32_t D, int3
     uint32_t *b = (uint32_t *)malloc(sizeof(uint32_t) * n * D);
     for (size_t i = 0; i < n; i++) {
         uint64_t x = in[i % r->row_len];
-        for (uint32_t l = 0; l < D; l++) a[i * D + l] = (uint32_t)((x >> l) & 1);
+        for (uint32_t l = 0; l < D; l++) {
+            const uint32_t v = (uint32_t)((x >> l) & 1);
+            a[i * D + l] = (r->flip && (i & 1)) ? 0u - v : v;
+        }
     }
     for (int pass = 0; pass < 2; pass++) {
         const uint32_t *perm = pass == 0 ? r->perm1 : r->perm2;
         for (size_t i = 0; i < n; i++) memcpy(b + i * D, a + (size_t)perm[i] * D, 4 * D);
         for (size_t i = 1; i < n; i++)
             for (uint32_t l = 0; l < D; l++) b[i * D + l] += b[(i - 1) * D + l];
+        if (pass == 0 && r->flip)
+            for (size_t i = 1; i < n; i += 2)
+                for (uint32_t l = 0; l < D; l++) b[i * D + l] = 0u - b[i * D + l];
         uint32_t *t = a;
         a = b;
         b = t;
@@ -780,7 +808,8 @@ static int zparams_build(const zr_desc *d, zparams *z) {
         z->codeword_len = z->iprs.codeword_len;
         z->cw_bytes = d->eval_kind == ZR_EVAL_BINPOLY ? 8 * z->D : 16;
     } else {
-        if (raa_build(d->row_len, d->rep, &z->raa)) return -1;
+        if (d->code_kind > ZR_CODE_RAA_SIGN_FLIP) return -1;
+        if (raa_build(d->row_len, d->rep, d->code_kind == ZR_CODE_RAA_SIGN_FLIP, &z->raa)) return -1;
         z->codeword_len = z->raa.codeword_len;
         z->cw_bytes = 4 * z->D;
     }
@@ -838,7 +867,7 @@ static void encode_poly(const zparams *z, const uint8_t *evals, uint8_t *cw) {
 int zr_encode_rows(const zr_desc *d, const void *evals, void *cw_out) {
     zparams z;
     if (zparams_build(d, &z)) return -1;
-    if (d->code_kind == ZR_CODE_RAA && d->eval_kind != ZR_EVAL_BINPOLY) {
+    if (d->code_kind != ZR_CODE_IPRS && d->eval_kind != ZR_EVAL_BINPOLY) {
         zparams_free(&z);
         return -1;
     }
@@ -1260,7 +1289,7 @@ static int validate_bits(const zparams *z, uint32_t batch) {
 }
 
 static int do_commit(const zparams *z, const uint8_t *polys, uint32_t batch, zhint *h) {
-    if (z->d.code_kind == ZR_CODE_RAA && z->d.eval_kind != ZR_EVAL_BINPOLY) return -1;
+    if (z->d.code_kind != ZR_CODE_IPRS && z->d.eval_kind != ZR_EVAL_BINPOLY) return -1;
     size_t rowbytes = (size_t)z->codeword_len * z->cw_bytes;
     size_t polycw = rowbytes * z->num_rows;
     size_t polyev = (size_t)z->num_rows * z->row_len * z->eval_bytes;

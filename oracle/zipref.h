@@ -20,7 +20,7 @@ extern "C" {
 #endif
 
 enum { ZR_EVAL_I32 = 0, ZR_EVAL_BINPOLY = 1 };
-enum { ZR_CODE_IPRS = 0, ZR_CODE_RAA = 1 };
+enum { ZR_CODE_IPRS = 0, ZR_CODE_RAA = 1, ZR_CODE_RAA_SIGN_FLIP = 2 };
 
 /* Same meaning as the product's zg_params_desc. */
 typedef struct {

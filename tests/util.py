@@ -25,5 +25,6 @@ def params_for(Z, eval_kind, D, code_kind, num_vars, row_len, depth=0, rep=4, de
                ctx=None, comb=None, field=4, openings=147):
     zt = Z.ZipTypes(eval_kind, D if eval_kind == Z.EVAL_BINPOLY else 1,
                     comb if comb else (3 if eval_kind == Z.EVAL_I32 else 5), field, openings)
-    code = Z.IprsCode(row_len, depth, rep) if code_kind == Z.CODE_IPRS else Z.RaaCode(row_len, rep)
+    code = (Z.IprsCode(row_len, depth, rep) if code_kind == Z.CODE_IPRS else
+            Z.RaaCode(row_len, rep) if code_kind == Z.CODE_RAA else Z.RaaSignFlippingCode(row_len, rep))
     return Z.ZipPlus.setup(1 << num_vars, code, zt, ctx=ctx, device=device)

@@ -141,14 +141,30 @@ size_t leaf_bytes_of(const zg_params *p, uint32_t batch) {
 void host_encode_wide(const zg_params *p, const uint64_t *row, uint32_t limbs, uint64_t *out) {
     const zg_params_info &I = p->info;
     const uint32_t C = I.codeword_len;
-    if (p->d.code_kind == ZG_CODE_RAA) {
+    if (p->d.code_kind != ZG_CODE_IPRS) {
+        // RAA (raa.rs:93-127); with sign flips (raa_sign_flip.rs:31-69) the
+        // repeated row's and the first accumulation's odd entries are negated,
+        // i.e. a gathered entry is negated when its source index is odd
+        const bool flip = p->d.code_kind == ZG_CODE_RAA_SIGN_FLIP;
+        auto negate = [limbs](uint64_t *x) {
+            unsigned __int128 c = 1;
+            for (uint32_t w = 0; w < limbs; w++) {
+                const unsigned __int128 t = (unsigned __int128)(~x[w]) + c;
+                x[w] = (uint64_t)t;
+                c = t >> 64;
+            }
+        };
         const uint32_t Lr = I.row_len;
         std::vector<uint64_t> a((size_t)C * limbs), b((size_t)C * limbs);
-        for (uint32_t i = 0; i < C; i++)
+        for (uint32_t i = 0; i < C; i++) {
             std::memcpy(&a[(size_t)i * limbs], row + (size_t)(p->perm1[i] % Lr) * limbs, 8 * limbs);
+            if (flip && (p->perm1[i] & 1u)) negate(&a[(size_t)i * limbs]);
+        }
         for (uint32_t i = 1; i < C; i++) wide_add(&a[(size_t)i * limbs], &a[(size_t)(i - 1) * limbs], limbs);
-        for (uint32_t i = 0; i < C; i++)
+        for (uint32_t i = 0; i < C; i++) {
             std::memcpy(&b[(size_t)i * limbs], &a[(size_t)p->perm2[i] * limbs], 8 * limbs);
+            if (flip && (p->perm2[i] & 1u)) negate(&b[(size_t)i * limbs]);
+        }
         for (uint32_t i = 1; i < C; i++) wide_add(&b[(size_t)i * limbs], &b[(size_t)(i - 1) * limbs], limbs);
         std::memcpy(out, b.data(), 8 * (size_t)C * limbs);
         return;
@@ -196,7 +212,7 @@ void host_encode_wide(const zg_params *p, const uint64_t *row, uint32_t limbs, u
 void host_encode_wide_at(const zg_params *p, const uint64_t *row, uint32_t limbs,
                          const uint32_t *pos, uint32_t n, uint64_t *out) {
     const zg_params_info &I = p->info;
-    if (p->d.code_kind == ZG_CODE_RAA) {
+    if (p->d.code_kind != ZG_CODE_IPRS) {
         std::vector<uint64_t> all((size_t)I.codeword_len * limbs);
         host_encode_wide(p, row, limbs, all.data());
         for (uint32_t o = 0; o < n; o++) std::memcpy(out + (size_t)o * limbs, &all[(size_t)pos[o] * limbs], 8 * limbs);
@@ -884,7 +900,7 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
     if (!desc || !out) return ZG_ERR_INVALID_PARAM;
     *out = nullptr;
     zg_params_desc d = *desc;
-    if (d.eval_kind > ZG_EVAL_BINPOLY || d.code_kind > ZG_CODE_RAA) {
+    if (d.eval_kind > ZG_EVAL_BINPOLY || d.code_kind > ZG_CODE_RAA_SIGN_FLIP) {
         set_error("unknown evaluation or code kind");
         return ZG_ERR_INVALID_PARAM;
     }
@@ -1077,7 +1093,7 @@ zg_status zg_params_iprs_tables(const zg_params *p, int64_t *base_matrix, int64_
 }
 
 zg_status zg_params_raa_perms(const zg_params *p, uint32_t *perm1, uint32_t *perm2) {
-    if (!p || p->d.code_kind != ZG_CODE_RAA) return ZG_ERR_INVALID_PARAM;
+    if (!p || p->d.code_kind == ZG_CODE_IPRS) return ZG_ERR_INVALID_PARAM;
     if (perm1) std::memcpy(perm1, p->perm1.data(), p->perm1.size() * 4);
     if (perm2) std::memcpy(perm2, p->perm2.data(), p->perm2.size() * 4);
     return ZG_OK;

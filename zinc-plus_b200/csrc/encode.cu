@@ -1001,7 +1001,10 @@ __global__ void __launch_bounds__(256) k_stage_i128(const Tin *__restrict__ in,
 // RAA (raa.rs:93-127) for binary evaluations: repeat x rep, permute by perm1,
 // prefix-sum, permute by perm2, prefix-sum, on i32 lanes (wrapping).  One
 // block per (row, group of LG lanes); the first prefix sum stays in shared
-// memory.  perm[i] is the source position of output i (clone_shuffled).
+// memory.  perm[i] is the source position of output i (clone_shuffled).  The
+// sign-flipping variant (raa_sign_flip.rs:31-69) negates the odd entries of
+// the repeated row and of the first prefix sum: a gathered entry is negated
+// when its source position is odd.
 template <int LG>
 __device__ void block_exclusive_scan(uint32_t (&v)[LG], uint32_t *warp_tot) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
@@ -1043,7 +1046,7 @@ template <int LG>
 __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__restrict__ perm1,
                           const uint32_t *__restrict__ perm2, int32_t *__restrict__ out,
                           uint32_t row_len, uint32_t n, uint32_t D, uint64_t dmask,
-                          uint32_t nrows, bool leaf_major, uint32_t seg_log) {
+                          uint32_t nrows, bool leaf_major, uint32_t seg_log, bool flip) {
     extern __shared__ uint32_t sm[];
     uint32_t *pre = sm;                 // n x LG
     uint32_t *wt = sm + (size_t)n * LG; // 32 x LG
@@ -1060,10 +1063,13 @@ __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__
     for (int l = 0; l < LG; l++) tot[l] = 0;
     for (uint32_t k = 0; k < cnt; k++) {
         const uint32_t i = i0 + k;
-        const uint64_t x = (row[perm1[i] % row_len] & dmask) >> lane0;
+        const uint32_t s1 = perm1[i];
+        const uint64_t x = (row[s1 % row_len] & dmask) >> lane0;
+        // sign-flip code: the repeated row's odd entries are negated (mod 2^32)
+        const uint32_t neg = (flip && (s1 & 1u)) ? ~0u : 0u;
 #pragma unroll
         for (int l = 0; l < LG; l++) {
-            tot[l] += (uint32_t)((x >> l) & 1u);
+            tot[l] += ((uint32_t)((x >> l) & 1u) ^ neg) - neg;
             pre[(size_t)i * LG + l] = tot[l];
         }
     }
@@ -1080,8 +1086,9 @@ __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__
     for (int l = 0; l < LG; l++) tot[l] = 0;
     for (uint32_t k = 0; k < cnt; k++) {
         const uint32_t src = perm2[i0 + k];
+        const uint32_t neg = (flip && (src & 1u)) ? ~0u : 0u;  // first accumulation's odd entries
 #pragma unroll
-        for (int l = 0; l < LG; l++) tot[l] += pre[(size_t)src * LG + l];
+        for (int l = 0; l < LG; l++) tot[l] += (pre[(size_t)src * LG + l] ^ neg) - neg;
     }
 #pragma unroll
     for (int l = 0; l < LG; l++) off[l] = tot[l];
@@ -1091,9 +1098,10 @@ __global__ void k_raa_bin(const uint64_t *__restrict__ evals, const uint32_t *__
     for (uint32_t k = 0; k < cnt; k++) {
         const uint32_t i = i0 + k;
         const uint32_t src = perm2[i];
+        const uint32_t neg = (flip && (src & 1u)) ? ~0u : 0u;
 #pragma unroll
         for (int l = 0; l < LG; l++) {
-            tot[l] += pre[(size_t)src * LG + l];
+            tot[l] += (pre[(size_t)src * LG + l] ^ neg) - neg;
             const uint32_t lane = lane0 + l;
             if (lane < D) {
                 size_t idx = leaf_major ? lm_pos(i, grow, nrows, n, seg_log) * D + lane
@@ -1198,7 +1206,8 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
     const zg_params_info &I = p->info;
     const uint32_t C = I.codeword_len, L = I.row_len, D = p->D;
     const uint64_t dmask = D >= 64 ? ~0ull : ((1ull << D) - 1);
-    if (p->d.code_kind == ZG_CODE_RAA) {
+    if (p->d.code_kind != ZG_CODE_IPRS) {
+        const bool flip = p->d.code_kind == ZG_CODE_RAA_SIGN_FLIP;
         if (p->d.eval_kind != ZG_EVAL_BINPOLY) {
             set_error("RAA encoding is defined for binary polynomial evaluations");
             return ZG_ERR_INVALID_PARAM;
@@ -1220,7 +1229,7 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
     do {                                                                                          \
         ZG_CUDA(allow_max_smem(k_raa_bin<LGV>));                                                 \
         k_raa_bin<LGV><<<grid, threads, smem, s>>>(ev, p1, p2, o, L, C, D, dmask, nrows,          \
-                                                   leaf_major, seg_log);                                   \
+                                                   leaf_major, seg_log, flip);                             \
     } while (0)
         ZG_KBEGIN(ctx, s, "k_raa_bin");
         switch (LG) {

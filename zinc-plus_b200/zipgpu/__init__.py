@@ -34,7 +34,7 @@ STATUS = {
     8: "ZG_ERR_NO_DEVICE", 9: "ZG_ERR_BUFFER_TOO_SMALL",
 }
 EVAL_I32, EVAL_BINPOLY = 0, 1
-CODE_IPRS, CODE_RAA = 0, 1
+CODE_IPRS, CODE_RAA, CODE_RAA_SIGN_FLIP = 0, 1, 2
 
 # Every symbol include/zipgpu.h declares.
 EXPORTS = (
@@ -276,6 +276,21 @@ class RaaCode:
     @staticmethod
     def new(row_len: int, rep: int = 4) -> "RaaCode":
         return RaaCode(row_len, rep)
+
+
+@dataclass(frozen=True)
+class RaaSignFlippingCode:
+    """RAA with sign flips (RaaSignFlippingCode<Zt, Config, REP>,
+    raa_sign_flip.rs:14-69)."""
+
+    row_len: int
+    rep: int = 4
+    depth: int = 0
+    kind: int = CODE_RAA_SIGN_FLIP
+
+    @staticmethod
+    def new(row_len: int, rep: int = 4) -> "RaaSignFlippingCode":
+        return RaaSignFlippingCode(row_len, rep)
 
 
 @dataclass(frozen=True)
