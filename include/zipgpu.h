@@ -381,6 +381,37 @@ zg_status zg_sumcheck_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulu
 zg_status zg_mle_evaluate(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs, const uint64_t *mle,
                           uint32_t nvars, const uint64_t *point, uint64_t *out);
 
+/* ---- Zinc+ prover steps 3 and 6 on the trace columns -------------------------
+ * (protocol/src/prover.rs:385-415 step3_eval_projection and 497-532
+ * step6_lift_and_project.)  Columns: n_bin binary-polynomial columns of
+ * 2^nvars BinaryPoly<degree_plus_one> u64 words (bit l = coefficient l), column
+ * after column, then n_int integer columns of 2^nvars i64.  Field: `limbs` u64
+ * LE modulus, 3 or 4 limbs, odd; every field element is a Montgomery inner
+ * (F::Inner of MontyField).
+ *
+ * zg_piop_eval_projection: project_trace_coeffs (piop/src/projections.rs:140-220:
+ * binary coefficients become one or zero, integers F::from_with_cfg) followed by
+ * evaluate_trace_to_column_mles at the projecting element a (projections.rs:
+ * 227-301).  mles_out: (n_bin + n_int) MLEs of 2^nvars elements, MLE-major, the
+ * layout zg_sumcheck_prove takes.  on_device != 0: the columns and mles_out are
+ * device pointers (the MLEs can go straight into zg_sumcheck_prove with
+ * mles_on_device); else host memory. */
+zg_status zg_piop_eval_projection(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs,
+                                  const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
+                                  const int64_t *int_cols, uint32_t n_int, uint32_t nvars,
+                                  const uint64_t *a, int on_device, uint64_t *mles_out);
+/* zg_piop_lifted_evals: compute_lifted_evals (protocol/src/lib.rs:327-395) at
+ * `point` (nvars elements, bit k of b pairs with point[k]): for binary column c,
+ * coefficient l = sum_b eq(b, point) [bit l of c[b]]; for an integer column the
+ * single coefficient sum_b eq(b, point) F(c[b]).  coeffs_out (host): n_bin x
+ * degree_plus_one then n_int elements, untrimmed (DynamicPolynomialF::
+ * new_trimmed drops trailing zero coefficients).  cols_on_device: the columns
+ * are device pointers. */
+zg_status zg_piop_lifted_evals(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs,
+                               const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
+                               const int64_t *int_cols, uint32_t n_int, uint32_t nvars,
+                               const uint64_t *point, int cols_on_device, uint64_t *coeffs_out);
+
 #ifdef __cplusplus
 }
 #endif

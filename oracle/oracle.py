@@ -104,6 +104,9 @@ def lib():
                                          vp, sz, vp, vp]
         L.zr_sumcheck_comb.argtypes = [vp, C.c_uint32, gp, vp, vp]
         L.zr_mle_evaluate.argtypes = [vp, C.c_uint32, vp, C.c_uint32, vp, vp]
+        u32 = C.c_uint32
+        L.zr_piop_eval_projection.argtypes = [vp, u32, vp, u32, u32, vp, u32, u32, vp, vp]
+        L.zr_piop_lifted_evals.argtypes = [vp, u32, vp, u32, u32, vp, u32, u32, vp, vp]
         _lib = L
     return _lib
 
@@ -395,4 +398,34 @@ def mle_evaluate(modulus: int, L: int, mle: np.ndarray, point: np.ndarray) -> np
     out = np.zeros(L, np.uint64)
     mod = _limbs(modulus, L)
     lib().zr_mle_evaluate(_ptr(mod), L, _ptr(mle), point.shape[0], _ptr(point), _ptr(out))
+    return out
+
+
+def _piop_cols(bin_cols, int_cols, nvars):
+    n = 1 << nvars
+    b = np.ascontiguousarray(bin_cols if bin_cols is not None else np.zeros((0, n)), dtype=np.uint64)
+    i = np.ascontiguousarray(int_cols if int_cols is not None else np.zeros((0, n)), dtype=np.int64)
+    assert b.ndim == 2 and i.ndim == 2 and (b.shape[0] == 0 or b.shape[1] == n) and (i.shape[0] == 0 or i.shape[1] == n)
+    return b, i
+
+
+def piop_eval_projection(modulus: int, L: int, bin_cols, D: int, int_cols, nvars: int, a) -> np.ndarray:
+    """Zinc+ prover step 3 (evaluation projection): (n_bin + n_int, 2^nvars, L)
+    Montgomery inners; a is the projecting element's Montgomery inner."""
+    b, i = _piop_cols(bin_cols, int_cols, nvars)
+    out = np.zeros((b.shape[0] + i.shape[0], 1 << nvars, L), np.uint64)
+    av = np.ascontiguousarray(a, dtype=np.uint64)
+    lib().zr_piop_eval_projection(_ptr(_limbs(modulus, L)), L, _ptr(b), b.shape[0], D, _ptr(i),
+                                  i.shape[0], nvars, _ptr(av), _ptr(out))
+    return out
+
+
+def piop_lifted_evals(modulus: int, L: int, bin_cols, D: int, int_cols, nvars: int, point) -> np.ndarray:
+    """Zinc+ prover step 6 (lifted evaluations): n_bin x D then n_int x 1
+    Montgomery inners, shape (n_bin * D + n_int, L)."""
+    b, i = _piop_cols(bin_cols, int_cols, nvars)
+    out = np.zeros((b.shape[0] * D + i.shape[0], L), np.uint64)
+    pt = np.ascontiguousarray(point, dtype=np.uint64)
+    lib().zr_piop_lifted_evals(_ptr(_limbs(modulus, L)), L, _ptr(b), b.shape[0], D, _ptr(i),
+                               i.shape[0], nvars, _ptr(pt), _ptr(out))
     return out

@@ -2061,3 +2061,74 @@ void zr_mle_evaluate(const uint64_t *modulus, uint32_t L, const uint64_t *mle, u
     memcpy(out, acc, 8 * L);
     free(eq);
 }
+
+/* ========================================================================
+ * Zinc+ prover steps 3 and 6 on the trace columns
+ * (protocol/src/prover.rs:385-415 and 497-532).
+ * ====================================================================== */
+
+/* F::from_with_cfg of a signed 64-bit trace integer (Montgomery inner). */
+static void f_from_i64(const fcfg *f, int64_t v, uint64_t *out) {
+    uint64_t x[2] = {(uint64_t)v, v < 0 ? ~0ull : 0ull};
+    f_from_int(f, x, 2, out);
+}
+
+/* Step 3, evaluation projection: project_trace_coeffs (piop/src/projections.rs:
+ * 140-220: a binary coefficient becomes one or zero, an integer F::from_with_cfg)
+ * followed by evaluate_trace_to_column_mles (projections.rs:227-301: each
+ * polynomial's inner product with the powers of a).  bin: n_bin columns of 2^nvars
+ * BinaryPoly<D> (bit l = coefficient l); ints: n_int columns of 2^nvars i64.
+ * out: (n_bin + n_int) MLEs of 2^nvars Montgomery inners, column after column. */
+void zr_piop_eval_projection(const uint64_t *modulus, uint32_t L, const uint64_t *bin, uint32_t n_bin,
+                             uint32_t D, const int64_t *ints, uint32_t n_int, uint32_t nvars,
+                             const uint64_t *a, uint64_t *out) {
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    const size_t n = (size_t)1 << nvars;
+    uint64_t pw[64][4];
+    memcpy(pw[0], f.one, 8 * L);
+    for (uint32_t l = 1; l < D; l++) fmul(&f, pw[l - 1], a, pw[l]);
+    for (uint32_t c = 0; c < n_bin; c++)
+        for (size_t b = 0; b < n; b++) {
+            const uint64_t x = bin[c * n + b];
+            uint64_t acc[4] = {0};
+            for (uint32_t l = 0; l < D; l++)
+                if ((x >> l) & 1) fadd(&f, acc, pw[l]);
+            memcpy(out + (c * n + b) * L, acc, 8 * L);
+        }
+    for (uint32_t c = 0; c < n_int; c++)
+        for (size_t b = 0; b < n; b++) f_from_i64(&f, ints[c * n + b], out + ((n_bin + c) * n + b) * L);
+}
+
+/* Step 6, lifted evaluations: compute_lifted_evals (protocol/src/lib.rs:327-395).
+ * For a binary column, coefficient l is sum_b eq(b, point) [bit l of col[b]];
+ * for an integer column the single coefficient is sum_b eq(b, point) F(col[b]).
+ * out: n_bin x D then n_int x 1 Montgomery inners (untrimmed: the reference's
+ * DynamicPolynomialF::new_trimmed drops trailing zero coefficients). */
+void zr_piop_lifted_evals(const uint64_t *modulus, uint32_t L, const uint64_t *bin, uint32_t n_bin,
+                          uint32_t D, const int64_t *ints, uint32_t n_int, uint32_t nvars,
+                          const uint64_t *point, uint64_t *out) {
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    const size_t n = (size_t)1 << nvars;
+    uint64_t *eq = (uint64_t *)malloc(8 * L * n);
+    build_eq(&f, point, nvars, eq);
+    for (uint32_t c = 0; c < n_bin; c++)
+        for (uint32_t l = 0; l < D; l++) {
+            uint64_t acc[4] = {0};
+            for (size_t b = 0; b < n; b++)
+                if ((bin[c * n + b] >> l) & 1) fadd(&f, acc, eq + b * L);
+            memcpy(out + ((size_t)c * D + l) * L, acc, 8 * L);
+        }
+    for (uint32_t c = 0; c < n_int; c++) {
+        uint64_t acc[4] = {0};
+        for (size_t b = 0; b < n; b++) {
+            uint64_t v[4], t[4];
+            f_from_i64(&f, ints[c * n + b], v);
+            fmul(&f, v, eq + b * L, t);
+            fadd(&f, acc, t);
+        }
+        memcpy(out + ((size_t)n_bin * D + c) * L, acc, 8 * L);
+    }
+    free(eq);
+}

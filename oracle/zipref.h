@@ -114,6 +114,14 @@ void zr_sumcheck_comb(const uint64_t *modulus, uint32_t L, const zr_sc_group *g,
                       const uint64_t *vals, uint64_t *out);
 void zr_mle_evaluate(const uint64_t *modulus, uint32_t L, const uint64_t *mle, uint32_t nvars,
                      const uint64_t *point, uint64_t *out);
+/* Zinc+ prover step 3 (evaluation projection) and step 6 (lifted evaluations)
+ * on binary-polynomial and i64 trace columns; see zipref.c. */
+void zr_piop_eval_projection(const uint64_t *modulus, uint32_t L, const uint64_t *bin, uint32_t n_bin,
+                             uint32_t D, const int64_t *ints, uint32_t n_int, uint32_t nvars,
+                             const uint64_t *a, uint64_t *out);
+void zr_piop_lifted_evals(const uint64_t *modulus, uint32_t L, const uint64_t *bin, uint32_t n_bin,
+                          uint32_t D, const int64_t *ints, uint32_t n_int, uint32_t nvars,
+                          const uint64_t *point, uint64_t *out);
 
 /* threads used by the parallel regions */
 void zr_set_threads(int n);

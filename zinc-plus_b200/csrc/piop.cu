@@ -1,0 +1,330 @@
+// Zinc+ prover steps 3 and 6 on the trace columns (protocol/src/prover.rs:
+// 385-415 and 497-532), the data-parallel parts around the PCS and sumcheck.
+//
+//  k_eval_proj     step 3, evaluation projection: project_trace_coeffs (a binary
+//                  coefficient becomes one or zero, an integer F::from_with_cfg;
+//                  piop/src/projections.rs:140-220) then
+//                  evaluate_trace_to_column_mles (each polynomial's inner product
+//                  with the powers of the projecting element a, :227-301).  A
+//                  binary cell is the sum of a^l over its set bits.
+//  k_lifted_bin    step 6, lifted evaluations (compute_lifted_evals,
+//  k_lifted_int    protocol/src/lib.rs:327-395): coefficient l of binary column c
+//                  is sum_b eq(b, r0) [bit l of c[b]]; an integer column's single
+//                  coefficient is sum_b eq(b, r0) F(c[b]).  Per-block partial sums,
+//                  then k_lifted_reduce.
+// Field elements are Montgomery inners (F::Inner of MontyField) of 3 or 4 limbs.
+#include <cstring>
+#include <vector>
+
+#include "zg_internal.h"
+#include "zg_prove.h"
+
+namespace zg {
+namespace {
+
+constexpr uint32_t kLiftChunkLog = 12;  // inputs b per block of the lifted sums
+
+template <int L>
+__global__ void __launch_bounds__(256) k_eval_proj(const uint64_t *__restrict__ bin, uint32_t n_bin,
+                                                   uint64_t dmask, const int64_t *__restrict__ ints,
+                                                   uint32_t n_int, uint32_t nv,
+                                                   const uint64_t *__restrict__ pw, uint32_t D, FieldCfg f,
+                                                   uint64_t *__restrict__ out) {
+    __shared__ uint64_t spw[64 * L];
+    for (uint32_t i = threadIdx.x; i < D * L; i += blockDim.x) spw[i] = pw[i];
+    __syncthreads();
+    const size_t total = (size_t)(n_bin + n_int) << nv, nbin_cells = (size_t)n_bin << nv;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        uint64_t acc[L];
+#pragma unroll
+        for (int w = 0; w < L; w++) acc[w] = 0;
+        if (e < nbin_cells) {
+            uint64_t x = bin[e] & dmask;
+            while (x) {
+                const int l = __ffsll((long long)x) - 1;
+                fadd<L>(acc, spw + l * L, f.p);
+                x &= x - 1;
+            }
+        } else {
+            const int64_t v = ints[e - nbin_cells];
+            const uint64_t w2[2] = {(uint64_t)v, v < 0 ? ~0ull : 0ull};
+            from_signed<L>(w2, 2, f, acc);
+        }
+#pragma unroll
+        for (int w = 0; w < L; w++) out[e * L + w] = acc[w];
+    }
+}
+
+// Block (LB lanes, 256 / LB rows): column blockIdx.y, inputs b of chunk
+// blockIdx.x; thread (l, w) adds eq[b] for b = chunk start + w, + rows, ...
+// when bit l of the cell is set.  partials: [column][chunk][LB][L].
+template <int L, int LB>
+__global__ void __launch_bounds__(256) k_lifted_bin(const uint64_t *__restrict__ bin, uint32_t nv,
+                                                    uint64_t dmask, const uint64_t *__restrict__ eq, FieldCfg f,
+                                                    uint64_t *__restrict__ partials) {
+    __shared__ uint64_t red[256 * L];
+    const uint32_t l = threadIdx.x, w = threadIdx.y, rows = blockDim.y;
+    const size_t n = (size_t)1 << nv, b0 = (size_t)blockIdx.x << kLiftChunkLog;
+    const size_t b1 = b0 + ((size_t)1 << kLiftChunkLog) < n ? b0 + ((size_t)1 << kLiftChunkLog) : n;
+    const uint64_t *col = bin + ((size_t)blockIdx.y << nv);
+    uint64_t acc[L];
+#pragma unroll
+    for (int k = 0; k < L; k++) acc[k] = 0;
+    for (size_t b = b0 + w; b < b1; b += rows) {
+        const uint64_t x = col[b] & dmask;
+        if ((x >> l) & 1u) fadd<L>(acc, eq + b * L, f.p);
+    }
+    const uint32_t t = w * LB + l;
+#pragma unroll
+    for (int k = 0; k < L; k++) red[t * L + k] = acc[k];
+    __syncthreads();
+    for (uint32_t h = rows / 2; h > 0; h >>= 1) {
+        if (w < h) fadd<L>(red + t * L, red + (t + h * LB) * L, f.p);
+        __syncthreads();
+    }
+    if (w == 0) {
+        uint64_t *po = partials + (((size_t)blockIdx.y * gridDim.x + blockIdx.x) * LB + l) * L;
+#pragma unroll
+        for (int k = 0; k < L; k++) po[k] = red[l * L + k];
+    }
+}
+
+// Integer columns: 256 threads per chunk, partials [column][chunk][L].
+template <int L>
+__global__ void __launch_bounds__(256) k_lifted_int(const int64_t *__restrict__ ints, uint32_t nv,
+                                                    const uint64_t *__restrict__ eq, FieldCfg f,
+                                                    uint64_t *__restrict__ partials) {
+    __shared__ uint64_t red[256 * L];
+    const size_t n = (size_t)1 << nv, b0 = (size_t)blockIdx.x << kLiftChunkLog;
+    const size_t b1 = b0 + ((size_t)1 << kLiftChunkLog) < n ? b0 + ((size_t)1 << kLiftChunkLog) : n;
+    const int64_t *col = ints + ((size_t)blockIdx.y << nv);
+    uint64_t acc[L];
+#pragma unroll
+    for (int k = 0; k < L; k++) acc[k] = 0;
+    for (size_t b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
+        const int64_t v = col[b];
+        const uint64_t w2[2] = {(uint64_t)v, v < 0 ? ~0ull : 0ull};
+        uint64_t fv[L], t[L];
+        from_signed<L>(w2, 2, f, fv);
+        fmul<L>(fv, eq + b * L, f.p, f.n0, t);
+        fadd<L>(acc, t, f.p);
+    }
+#pragma unroll
+    for (int k = 0; k < L; k++) red[threadIdx.x * L + k] = acc[k];
+    __syncthreads();
+    for (uint32_t h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) fadd<L>(red + threadIdx.x * L, red + (threadIdx.x + h) * L, f.p);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        uint64_t *po = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * L;
+#pragma unroll
+        for (int k = 0; k < L; k++) po[k] = red[k];
+    }
+}
+
+// out[o] = sum over `chunks` partials of slot o (slots: stride `width`).
+template <int L>
+__global__ void k_lifted_reduce(const uint64_t *__restrict__ partials, uint32_t nslots, uint32_t chunks,
+                                uint32_t width, FieldCfg f, uint64_t *__restrict__ out) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nslots) return;
+    const uint32_t col = o / width, lane = o % width;
+    uint64_t acc[L];
+#pragma unroll
+    for (int k = 0; k < L; k++) acc[k] = 0;
+    for (uint32_t c = 0; c < chunks; c++)
+        fadd<L>(acc, partials + (((size_t)col * chunks + c) * width + lane) * L, f.p);
+#pragma unroll
+    for (int k = 0; k < L; k++) out[(size_t)o * L + k] = acc[k];
+}
+
+struct PiopCols {
+    const uint64_t *bin;
+    uint32_t n_bin, D;
+    const int64_t *ints;
+    uint32_t n_int, nv;
+};
+
+// Device views of the columns: the caller's device pointers, or copies at
+// the start of `arena` (host columns).  Returns the bytes used.
+size_t stage_cols(const PiopCols &c, int on_device, cudaStream_t s, uint8_t *arena, const uint64_t *&bin,
+                  const int64_t *&ints, zg_status &st) {
+    st = ZG_OK;
+    if (on_device) {
+        bin = c.bin;
+        ints = c.ints;
+        return 0;
+    }
+    const size_t n = (size_t)1 << c.nv, bb = (size_t)c.n_bin * n * 8, ib = (size_t)c.n_int * n * 8;
+    if ((bb && cudaMemcpyAsync(arena, c.bin, bb, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (ib && cudaMemcpyAsync(arena + bb, c.ints, ib, cudaMemcpyHostToDevice, s) != cudaSuccess)) {
+        set_error("piop: copying the columns to the device failed");
+        st = ZG_ERR_CUDA;
+    }
+    bin = reinterpret_cast<const uint64_t *>(arena);
+    ints = reinterpret_cast<const int64_t *>(arena + bb);
+    return bb + ib;
+}
+
+size_t staged_bytes(const PiopCols &c, int on_device) {
+    return on_device ? 0 : ((size_t)c.n_bin + c.n_int) * ((size_t)8 << c.nv);
+}
+
+template <int L>
+zg_status eval_projection_t(zg_ctx *ctx, const FieldCfg &f, const PiopCols &c, const uint64_t *a, int on_device,
+                            uint64_t *out) {
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)1 << c.nv, fb = 8 * L, cells = (size_t)(c.n_bin + c.n_int) * n;
+    std::vector<uint64_t> pw((size_t)64 * L, 0);
+    std::memcpy(pw.data(), f.one, fb);
+    for (uint32_t l = 1; l < c.D; l++) fmul<L>(&pw[(size_t)(l - 1) * L], a, f.p, f.n0, &pw[(size_t)l * L]);
+    const size_t sb = (staged_bytes(c, on_device) + 255) / 256 * 256;
+    ZG_TRY(ctx->sc_arena.ensure(sb + 64 * fb + (on_device ? 0 : cells * fb)));
+    uint8_t *arena = ctx->sc_arena.as<uint8_t>();
+    const uint64_t *bin_d;
+    const int64_t *ints_d;
+    zg_status sst;
+    stage_cols(c, on_device, s, arena, bin_d, ints_d, sst);
+    ZG_TRY(sst);
+    uint64_t *pw_d = reinterpret_cast<uint64_t *>(arena + sb);
+    uint64_t *out_d = on_device ? out : pw_d + 64 * L;
+    ZG_CUDA(cudaMemcpyAsync(pw_d, pw.data(), 64 * fb, cudaMemcpyHostToDevice, s));
+    const uint64_t dmask = c.D >= 64 ? ~0ull : ((1ull << c.D) - 1);
+    const unsigned blocks = (unsigned)std::min<size_t>((cells + 255) / 256, (size_t)ctx->num_sms * 16);
+    if (cells) {
+        ZG_KBEGIN(ctx, s, "k_eval_proj");
+        k_eval_proj<L><<<blocks, 256, 0, s>>>(bin_d, c.n_bin, dmask, ints_d, c.n_int, c.nv, pw_d, c.D, f, out_d);
+        ZG_KEND(ctx, s);
+    }
+    if (!on_device) ZG_CUDA(cudaMemcpyAsync(out, out_d, cells * fb, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(ctx_sync(ctx));
+    return ZG_OK;
+}
+
+template <int L>
+zg_status lifted_evals_t(zg_ctx *ctx, const FieldCfg &f, const PiopCols &c, const uint64_t *point,
+                         int on_device, uint64_t *out) {
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)1 << c.nv, fb = 8 * L;
+    const uint32_t LB = c.D > 32 ? 64 : 32;
+    const uint32_t chunks = (uint32_t)((n + (1u << kLiftChunkLog) - 1) >> kLiftChunkLog);
+    std::vector<uint64_t> omr((size_t)std::max<uint32_t>(c.nv, 1) * L, 0);
+    for (uint32_t k = 0; k < c.nv; k++) {
+        std::memcpy(&omr[(size_t)k * L], f.one, fb);
+        fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
+    }
+    const size_t nv1 = std::max<uint32_t>(c.nv, 1);
+    const size_t pb = ((size_t)c.n_bin * chunks * LB + (size_t)c.n_int * chunks) * fb;
+    const size_t ob = ((size_t)c.n_bin * LB + c.n_int) * fb;
+    const size_t sb = (staged_bytes(c, on_device) + 255) / 256 * 256;
+    ZG_TRY(ctx->sc_arena.ensure(sb + 2 * nv1 * fb + n * fb + pb + ob + 64));
+    uint8_t *arena = ctx->sc_arena.as<uint8_t>();
+    const uint64_t *bin_d;
+    const int64_t *ints_d;
+    zg_status sst;
+    stage_cols(c, on_device, s, arena, bin_d, ints_d, sst);
+    ZG_TRY(sst);
+    uint64_t *r_d = reinterpret_cast<uint64_t *>(arena + sb), *omr_d = r_d + nv1 * L, *eq_d = omr_d + nv1 * L;
+    uint64_t *part_d = eq_d + n * L, *res_d = part_d + pb / 8;
+    ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)c.nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)c.nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_TRY(launch_eq_table(ctx, r_d, omr_d, c.nv, f, eq_d, s));
+    const uint64_t dmask = c.D >= 64 ? ~0ull : ((1ull << c.D) - 1);
+    uint64_t *part_int = part_d + (size_t)c.n_bin * chunks * LB * L;
+    uint64_t *res_int = res_d + (size_t)c.n_bin * LB * L;
+    if (c.n_bin) {
+        ZG_KBEGIN(ctx, s, "k_lifted_bin");
+        dim3 g(chunks, c.n_bin);
+        if (LB == 64)
+            k_lifted_bin<L, 64><<<g, dim3(64, 4), 0, s>>>(bin_d, c.nv, dmask, eq_d, f, part_d);
+        else
+            k_lifted_bin<L, 32><<<g, dim3(32, 8), 0, s>>>(bin_d, c.nv, dmask, eq_d, f, part_d);
+        ZG_KEND(ctx, s);
+        ZG_KBEGIN(ctx, s, "k_lifted_reduce");
+        const uint32_t slots = c.n_bin * LB;
+        k_lifted_reduce<L><<<(slots + 127) / 128, 128, 0, s>>>(part_d, slots, chunks, LB, f, res_d);
+        ZG_KEND(ctx, s);
+    }
+    if (c.n_int) {
+        ZG_KBEGIN(ctx, s, "k_lifted_int");
+        k_lifted_int<L><<<dim3(chunks, c.n_int), 256, 0, s>>>(ints_d, c.nv, eq_d, f, part_int);
+        ZG_KEND(ctx, s);
+        ZG_KBEGIN(ctx, s, "k_lifted_reduce");
+        k_lifted_reduce<L><<<(c.n_int + 127) / 128, 128, 0, s>>>(part_int, c.n_int, chunks, 1, f, res_int);
+        ZG_KEND(ctx, s);
+    }
+    std::vector<uint64_t> res(((size_t)c.n_bin * LB + c.n_int) * L);
+    if (!res.empty()) ZG_CUDA(cudaMemcpyAsync(res.data(), res_d, res.size() * 8, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(ctx_sync(ctx));
+    for (uint32_t col = 0; col < c.n_bin; col++)
+        std::memcpy(out + (size_t)col * c.D * L, &res[(size_t)col * LB * L], (size_t)c.D * fb);
+    if (c.n_int)
+        std::memcpy(out + (size_t)c.n_bin * c.D * L, &res[(size_t)c.n_bin * LB * L], (size_t)c.n_int * fb);
+    return ZG_OK;
+}
+
+zg_status piop_args(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs, const PiopCols &c,
+                    const uint64_t *elems, const void *out, FieldCfg &f) {
+    if (!ctx || !modulus || !elems || !out || (c.n_bin && !c.bin) || (c.n_int && !c.ints)) {
+        set_error("piop: null argument");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (limbs != 3 && limbs != 4) {
+        set_error("piop: field limbs must be 3 or 4 (got %u)", limbs);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (c.nv > 28 || (c.n_bin && (c.D < 1 || c.D > 64)) || (size_t)c.n_bin + c.n_int > 4096) {
+        set_error("piop: num_vars above 28, BinaryPoly width outside 1..64 or more than 4096 columns");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    uint64_t p[4] = {0, 0, 0, 0};
+    std::memcpy(p, modulus, 8 * limbs);
+    if (!(p[0] & 1)) {
+        set_error("piop: the modulus must be odd");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    field_cfg_init(f, p, (int)limbs);
+    return ZG_OK;
+}
+
+}  // namespace
+}  // namespace zg
+
+using namespace zg;
+
+extern "C" zg_status zg_piop_eval_projection(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs,
+                                             const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
+                                             const int64_t *int_cols, uint32_t n_int, uint32_t nvars,
+                                             const uint64_t *a, int on_device, uint64_t *mles_out) {
+    try {
+        const PiopCols c{bin_cols, n_bin, degree_plus_one, int_cols, n_int, nvars};
+        FieldCfg f;
+        ZG_TRY(piop_args(ctx, modulus, limbs, c, a, mles_out, f));
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ZG_CUDA(cudaSetDevice(ctx->device));
+        return limbs == 3 ? eval_projection_t<3>(ctx, f, c, a, on_device, mles_out)
+                          : eval_projection_t<4>(ctx, f, c, a, on_device, mles_out);
+    } catch (const std::exception &e) {
+        set_error("piop: %s", e.what());
+        return ZG_ERR_OOM;
+    }
+}
+
+extern "C" zg_status zg_piop_lifted_evals(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs,
+                                          const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
+                                          const int64_t *int_cols, uint32_t n_int, uint32_t nvars,
+                                          const uint64_t *point, int cols_on_device, uint64_t *coeffs_out) {
+    try {
+        const PiopCols c{bin_cols, n_bin, degree_plus_one, int_cols, n_int, nvars};
+        FieldCfg f;
+        ZG_TRY(piop_args(ctx, modulus, limbs, c, point, coeffs_out, f));
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ZG_CUDA(cudaSetDevice(ctx->device));
+        return limbs == 3 ? lifted_evals_t<3>(ctx, f, c, point, cols_on_device, coeffs_out)
+                          : lifted_evals_t<4>(ctx, f, c, point, cols_on_device, coeffs_out);
+    } catch (const std::exception &e) {
+        set_error("piop: %s", e.what());
+        return ZG_ERR_OOM;
+    }
+}

@@ -48,7 +48,7 @@ EXPORTS = (
     "zg_commit_prove", "zg_commit_prove_d", "zg_commit_prove_many", "zg_proof_size", "zg_verify",
     "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch", "zg_server_create",
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
-    "zg_selftest_bounded_wait",
+    "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals",
 )
 
 
@@ -130,6 +130,10 @@ def lib() -> C.CDLL:
         "zg_ctx_set_kernel_timing": ([vp, C.c_int], st),
         "zg_ctx_kernel_timing_report": ([vp, C.c_char_p, sz, C.POINTER(sz)], st),
         "zg_selftest_bounded_wait": ([vp, C.POINTER(C.c_uint32)], st),
+        "zg_piop_eval_projection": ([vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
+                                     C.c_uint32, C.c_uint32, vp, C.c_int, vp], st),
+        "zg_piop_lifted_evals": ([vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
+                                  C.c_uint32, C.c_uint32, vp, C.c_int, vp], st),
         "zg_params_create": ([vp, C.POINTER(ParamsDesc), C.POINTER(vp)], st),
         "zg_params_destroy": ([vp], st),
         "zg_params_get_info": ([vp, C.POINTER(ParamsInfo)], st),
@@ -786,3 +790,43 @@ class ZipServer:
             self.close()
         except Exception:
             pass
+
+
+class ZincPiop:
+    """Zinc+ prover steps 3 and 6 on the trace columns (protocol/src/prover.rs:
+    385-415 and 497-532) on the GPU.  Field elements are Montgomery inners
+    (uint64 arrays of `limbs` words); the modulus is a Python int."""
+
+    @staticmethod
+    def _cols(bin_cols, int_cols, nvars):
+        n = 1 << nvars
+        b = np.ascontiguousarray(bin_cols if bin_cols is not None else np.zeros((0, n)), dtype=np.uint64)
+        i = np.ascontiguousarray(int_cols if int_cols is not None else np.zeros((0, n)), dtype=np.int64)
+        for x in (b, i):
+            if x.ndim != 2 or (x.shape[0] and x.shape[1] != n):
+                raise ValueError("columns must be (count, 2^nvars) arrays")
+        return b, i
+
+    @staticmethod
+    def eval_projection(ctx: Context, modulus: int, limbs: int, bin_cols, degree_plus_one: int, int_cols,
+                        nvars: int, a) -> np.ndarray:
+        """step3: (n_bin + n_int, 2^nvars, limbs) MLEs of the projected trace at a."""
+        b, i = ZincPiop._cols(bin_cols, int_cols, nvars)
+        out = np.zeros((b.shape[0] + i.shape[0], 1 << nvars, limbs), np.uint64)
+        av = np.ascontiguousarray(a, dtype=np.uint64)
+        mod = modulus.to_bytes(8 * limbs, "little")
+        check(lib().zg_piop_eval_projection(ctx.handle, mod, limbs, _ptr(b), b.shape[0], degree_plus_one,
+                                            _ptr(i), i.shape[0], nvars, _ptr(av), 0, _ptr(out)))
+        return out
+
+    @staticmethod
+    def lifted_evals(ctx: Context, modulus: int, limbs: int, bin_cols, degree_plus_one: int, int_cols,
+                     nvars: int, point) -> np.ndarray:
+        """step6: (n_bin * degree_plus_one + n_int, limbs) coefficients."""
+        b, i = ZincPiop._cols(bin_cols, int_cols, nvars)
+        out = np.zeros((b.shape[0] * degree_plus_one + i.shape[0], limbs), np.uint64)
+        pt = np.ascontiguousarray(point, dtype=np.uint64)
+        mod = modulus.to_bytes(8 * limbs, "little")
+        check(lib().zg_piop_lifted_evals(ctx.handle, mod, limbs, _ptr(b), b.shape[0], degree_plus_one,
+                                         _ptr(i), i.shape[0], nvars, _ptr(pt), 0, _ptr(out)))
+        return out
