@@ -718,9 +718,10 @@ def run_ours(args):
             verify["cpu_baseline_ms"] = (time.perf_counter() - a) * 1e3
             verify["cpu_baseline_kind"] = "port (oracle, OpenMP, full encode_wide as the reference)"
             verify["oracle_accepts"] = rc == 0
-    batch_commit = serving = sumcheck = None
+    batch_commit = serving = sumcheck = piop_steps = None
     if not args.no_extra:
         sumcheck = run_sumcheck(Z, ctx, torch, stream, 18, 14, rank == 0 and not args.no_cpu_baseline)
+        piop_steps = run_piop_steps(Z, ctx, torch, stream, 18, 14, rank == 0 and not args.no_cpu_baseline)
         batch_commit = run_batched_commit(Z, ctx, torch, stream, flush, reps=5, warm=2)
         serving = run_serving(Z, ctx, torch, args.serve_requests, args.serve_workers,
                               seed=0x5A1F + rank)
@@ -760,6 +761,7 @@ def run_ours(args):
             "batched_commit": batch_commit,
             "serving": serving,
             "sumcheck": sumcheck,
+            "piop_steps": piop_steps,
             "verify": verify,
             "impl": "ours",
         }
@@ -784,6 +786,89 @@ def run_commit_case(nv, D):
         hint.close()
     print(json.dumps({"commit_case": {"num_vars": nv, "D": D, "root": comm.root.hex()}}))
     return 0
+
+
+def run_piop_steps(Z, ctx, torch, stream, nv, cpu_nv, with_cpu):
+    """Zinc+ prover steps 3 and 6 on a BigLinear-shaped trace (16 BinaryPoly<32>
+    columns and 1 integer column, 2^nv rows, a 192-bit MontyField<3> prime):
+    device-resident columns through the C ABI, CUDA events on the library's
+    stream; the oracle at 2^cpu_nv rows on one host core as the CPU baseline."""
+    from oracle import oracle as O
+
+    O.build()
+    t = O.Transcript()
+    t.absorb_slice(b"bench-piop")
+    L, D, n_bin, n_int = 3, 32, 16, 1
+    p = t.get_prime(L)
+    rng = np.random.default_rng(0x9109)
+    R = 1 << (64 * L)
+
+    def inner(v):
+        x = (v % p) * R % p
+        return [(x >> (64 * i)) & ((1 << 64) - 1) for i in range(L)]
+
+    def cols(n):
+        b = rng.integers(0, 1 << 32, size=(n_bin, 1 << n), dtype=np.uint64)
+        i = rng.integers(-2**40, 2**40, size=(n_int, 1 << n), dtype=np.int64)
+        return b, i
+
+    b, i = cols(nv)
+    a = np.array(inner(int.from_bytes(rng.bytes(24), "little")), np.uint64)
+    r = np.array([inner(int.from_bytes(rng.bytes(24), "little")) for _ in range(nv)], np.uint64)
+    bd, id_ = torch.from_numpy(b.view(np.int64)).cuda(), torch.from_numpy(i).cuda()
+    mles = torch.empty((n_bin + n_int) * (1 << nv) * L, dtype=torch.int64, device="cuda")
+    coeffs = np.zeros((n_bin * D + n_int, L), np.uint64)
+    torch.cuda.synchronize()
+    mod = p.to_bytes(8 * L, "little")
+    lib = Z.lib()
+
+    def step3():
+        Z.check(lib.zg_piop_eval_projection(ctx.handle, mod, L, bd.data_ptr(), n_bin, D, id_.data_ptr(), n_int,
+                                            nv, a.ctypes.data, 1, mles.data_ptr()))
+
+    def step6():
+        Z.check(lib.zg_piop_lifted_evals(ctx.handle, mod, L, bd.data_ptr(), n_bin, D, id_.data_ptr(), n_int, nv,
+                                         r.ctypes.data, 1, coeffs.ctypes.data))
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        ts = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    ms3, ms6 = timed(step3), timed(step6)
+    cells = (n_bin + n_int) << nv
+    res = {"workload": f"BigLinear-shaped trace: {n_bin} BinaryPoly<{D}> + {n_int} integer columns, 2^{nv} rows, "
+                       "MontyField<3> (192-bit prime from the transcript); columns resident on the device",
+           "eval_projection": {"ms": ms3, "cells_per_s": cells / (ms3 / 1e3),
+                               "output_bytes": cells * 8 * L},
+           "lifted_evals": {"ms": ms6, "cells_per_s": cells / (ms6 / 1e3)}}
+    # parity at this size against the oracle on a sample of columns is in the tests;
+    # here: the first MLE entries and the coefficients of the first column
+    if with_cpu:
+        bs, is_ = cols(cpu_nv)
+        rs = r[:cpu_nv]
+        a0 = time.perf_counter()
+        want3 = O.piop_eval_projection(p, L, bs, D, is_, cpu_nv, a)
+        c3 = time.perf_counter() - a0
+        a0 = time.perf_counter()
+        want6 = O.piop_lifted_evals(p, L, bs, D, is_, cpu_nv, rs)
+        c6 = time.perf_counter() - a0
+        got3 = Z.ZincPiop.eval_projection(ctx, p, L, bs, D, is_, cpu_nv, a)
+        got6 = Z.ZincPiop.lifted_evals(ctx, p, L, bs, D, is_, cpu_nv, rs)
+        cc = (n_bin + n_int) << cpu_nv
+        res["cpu_baseline"] = {"eval_projection_cells_per_s": cc / c3, "lifted_evals_cells_per_s": cc / c6,
+                               "cores": 1, "kind": "port",
+                               "sample": f"oracle at 2^{cpu_nv} rows ({c3:.2f} s + {c6:.2f} s)"}
+        res["equal_oracle_at_cpu_size"] = bool(np.array_equal(got3, want3) and np.array_equal(got6, want6))
+    return res
 
 
 def run_sumcheck_case(nv):

@@ -17,34 +17,153 @@
 #include <vector>
 
 #include "zg_internal.h"
-#include "zg_prove.h"
 
 namespace zg {
 namespace {
 
 constexpr uint32_t kLiftChunkLog = 12;  // inputs b per block of the lifted sums
 
+// Lazy sums of field elements (each < p < 2^(64L)): 2L 32-bit words plus a
+// 32-bit top word, added with one PTX carry chain and no reduction; up to 2^32
+// addends cannot overflow.  lazy_reduce brings V = lo + top 2^(64L) to the
+// canonical residue with two Montgomery products: lo * (R mod p) R^-1 = lo mod p
+// and top * (R^2 mod p) R^-1 = top R mod p (R = 2^(64L); both factors < R).
+template <int L>
+struct Lazy {
+    uint32_t w[2 * L + 1];
+};
+
+template <int L>
+__device__ __forceinline__ void lazy_zero(Lazy<L> &a) {
+#pragma unroll
+    for (int i = 0; i < 2 * L + 1; i++) a.w[i] = 0;
+}
+
+template <int L>
+__device__ __forceinline__ void lazy_add(Lazy<L> &a, const uint64_t *b) {
+    uint32_t v[2 * L];
+#pragma unroll
+    for (int i = 0; i < L; i++) {
+        v[2 * i] = (uint32_t)b[i];
+        v[2 * i + 1] = (uint32_t)(b[i] >> 32);
+    }
+    if constexpr (L == 3) {
+        asm("add.cc.u32 %0, %0, %7;\n\taddc.cc.u32 %1, %1, %8;\n\taddc.cc.u32 %2, %2, %9;\n\t"
+            "addc.cc.u32 %3, %3, %10;\n\taddc.cc.u32 %4, %4, %11;\n\taddc.cc.u32 %5, %5, %12;\n\t"
+            "addc.u32 %6, %6, 0;"
+            : "+r"(a.w[0]), "+r"(a.w[1]), "+r"(a.w[2]), "+r"(a.w[3]), "+r"(a.w[4]), "+r"(a.w[5]), "+r"(a.w[6])
+            : "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]));
+    } else {
+        static_assert(L == 4, "lazy sums are for 3- or 4-limb fields");
+        asm("add.cc.u32 %0, %0, %9;\n\taddc.cc.u32 %1, %1, %10;\n\taddc.cc.u32 %2, %2, %11;\n\t"
+            "addc.cc.u32 %3, %3, %12;\n\taddc.cc.u32 %4, %4, %13;\n\taddc.cc.u32 %5, %5, %14;\n\t"
+            "addc.cc.u32 %6, %6, %15;\n\taddc.cc.u32 %7, %7, %16;\n\taddc.u32 %8, %8, 0;"
+            : "+r"(a.w[0]), "+r"(a.w[1]), "+r"(a.w[2]), "+r"(a.w[3]), "+r"(a.w[4]), "+r"(a.w[5]), "+r"(a.w[6]),
+              "+r"(a.w[7]), "+r"(a.w[8])
+            : "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]));
+    }
+}
+
+// a += b for two lazy sums (reductions; the top words stay far below 2^32).
+template <int L>
+__device__ __forceinline__ void lazy_merge(Lazy<L> &a, const Lazy<L> &b) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 2 * L + 1; i++) {
+        const uint64_t t = (uint64_t)a.w[i] + b.w[i] + c;
+        a.w[i] = (uint32_t)t;
+        c = t >> 32;
+    }
+}
+
+// Canonical residue of a lazy sum below 8p: subtract 4p, 2p, p where they fit
+// (pm[k] = p << k as 2L + 1 words, k = 0..2).
+template <int L>
+__device__ __forceinline__ void lazy_reduce_small(const Lazy<L> &a, const uint32_t (*pm)[2 * L + 1],
+                                                  uint64_t *out) {
+    uint32_t v[2 * L + 1];
+#pragma unroll
+    for (int i = 0; i < 2 * L + 1; i++) v[i] = a.w[i];
+#pragma unroll
+    for (int k = 2; k >= 0; k--) {
+        uint32_t t[2 * L + 1];
+        uint64_t br = 0;
+#pragma unroll
+        for (int i = 0; i < 2 * L + 1; i++) {
+            const uint64_t d = (uint64_t)v[i] - pm[k][i] - br;
+            t[i] = (uint32_t)d;
+            br = (d >> 32) & 1u;
+        }
+#pragma unroll
+        for (int i = 0; i < 2 * L + 1; i++) v[i] = br ? v[i] : t[i];
+    }
+#pragma unroll
+    for (int i = 0; i < L; i++) out[i] = (uint64_t)v[2 * i] | ((uint64_t)v[2 * i + 1] << 32);
+}
+
+template <int L>
+__device__ __forceinline__ void lazy_reduce(const Lazy<L> &a, const FieldCfg &f, uint64_t *out) {
+    uint64_t lo[L], hi[L], t[L];
+#pragma unroll
+    for (int i = 0; i < L; i++) {
+        lo[i] = (uint64_t)a.w[2 * i] | ((uint64_t)a.w[2 * i + 1] << 32);
+        hi[i] = i == 0 ? a.w[2 * L] : 0;
+    }
+    fmul<L>(lo, f.one, f.p, f.n0, out);
+    fmul<L>(hi, f.r2, f.p, f.n0, t);
+    fadd<L>(out, t, f.p);
+}
+
+// Byte tables of the powers of a: tab[j][v] = sum of a^(8j + i) over the set
+// bits i of v (8j + i < D), canonical.  One thread per (j, v).
+template <int L>
+__global__ void k_pow_tables(const uint64_t *__restrict__ pw, uint32_t D, FieldCfg f, uint64_t *__restrict__ tab) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x, nbytes = (D + 7) / 8;
+    if (e >= nbytes * 256) return;
+    const uint32_t j = e >> 8, v = e & 255u;
+    uint64_t acc[L];
+#pragma unroll
+    for (int k = 0; k < L; k++) acc[k] = 0;
+    for (uint32_t i = 0; i < 8; i++)
+        if (((v >> i) & 1u) && 8 * j + i < D) fadd<L>(acc, pw + (size_t)(8 * j + i) * L, f.p);
+#pragma unroll
+    for (int k = 0; k < L; k++) tab[(size_t)e * L + k] = acc[k];
+}
+
+// One cell per thread (grid-stride): a binary cell is the sum of ceil(D/8)
+// table entries (a lazy sum below 8p, then three conditional subtractions); an
+// integer cell is F::from_with_cfg of the value.
 template <int L>
 __global__ void __launch_bounds__(256) k_eval_proj(const uint64_t *__restrict__ bin, uint32_t n_bin,
                                                    uint64_t dmask, const int64_t *__restrict__ ints,
                                                    uint32_t n_int, uint32_t nv,
-                                                   const uint64_t *__restrict__ pw, uint32_t D, FieldCfg f,
+                                                   const uint64_t *__restrict__ tab, uint32_t D, FieldCfg f,
                                                    uint64_t *__restrict__ out) {
-    __shared__ uint64_t spw[64 * L];
-    for (uint32_t i = threadIdx.x; i < D * L; i += blockDim.x) spw[i] = pw[i];
+    // dynamic shared memory only (the kernel may take the device's whole
+    // opt-in limit): [ceil(D/8)][256][L] table words, then p, 2p, 4p
+    extern __shared__ uint64_t stab[];
+    const uint32_t nbytes = (D + 7) / 8;
+    uint32_t(*pm)[2 * L + 1] = reinterpret_cast<uint32_t(*)[2 * L + 1]>(stab + (size_t)nbytes * 256 * L);
+    for (uint32_t i = threadIdx.x; i < nbytes * 256 * L; i += blockDim.x) stab[i] = tab[i];
+    if (threadIdx.x < 3) {
+        uint32_t c = 0;
+        for (int i = 0; i < 2 * L; i++) {
+            const uint32_t w = (uint32_t)(f.p[i / 2] >> (32 * (i & 1)));
+            pm[threadIdx.x][i] = (w << threadIdx.x) | c;
+            c = threadIdx.x ? w >> (32 - threadIdx.x) : 0u;
+        }
+        pm[threadIdx.x][2 * L] = c;
+    }
     __syncthreads();
     const size_t total = (size_t)(n_bin + n_int) << nv, nbin_cells = (size_t)n_bin << nv;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
         uint64_t acc[L];
-#pragma unroll
-        for (int w = 0; w < L; w++) acc[w] = 0;
         if (e < nbin_cells) {
-            uint64_t x = bin[e] & dmask;
-            while (x) {
-                const int l = __ffsll((long long)x) - 1;
-                fadd<L>(acc, spw + l * L, f.p);
-                x &= x - 1;
-            }
+            const uint64_t x = bin[e] & dmask;
+            Lazy<L> z;
+            lazy_zero(z);
+            for (uint32_t j = 0; j < nbytes; j++) lazy_add<L>(z, stab + ((size_t)j * 256 + ((x >> (8 * j)) & 255u)) * L);
+            lazy_reduce_small<L>(z, pm, acc);
         } else {
             const int64_t v = ints[e - nbin_cells];
             const uint64_t w2[2] = {(uint64_t)v, v < 0 ? ~0ull : 0ull};
@@ -62,30 +181,43 @@ template <int L, int LB>
 __global__ void __launch_bounds__(256) k_lifted_bin(const uint64_t *__restrict__ bin, uint32_t nv,
                                                     uint64_t dmask, const uint64_t *__restrict__ eq, FieldCfg f,
                                                     uint64_t *__restrict__ partials) {
-    __shared__ uint64_t red[256 * L];
+    __shared__ Lazy<L> red[256];
     const uint32_t l = threadIdx.x, w = threadIdx.y, rows = blockDim.y;
     const size_t n = (size_t)1 << nv, b0 = (size_t)blockIdx.x << kLiftChunkLog;
     const size_t b1 = b0 + ((size_t)1 << kLiftChunkLog) < n ? b0 + ((size_t)1 << kLiftChunkLog) : n;
     const uint64_t *col = bin + ((size_t)blockIdx.y << nv);
-    uint64_t acc[L];
+    Lazy<L> acc;
+    lazy_zero(acc);
+    size_t b = b0 + w;
+    for (; b + 7 * rows < b1; b += 8 * rows) {  // eight inputs in flight
+        uint64_t x[8], e[8][L];
 #pragma unroll
-    for (int k = 0; k < L; k++) acc[k] = 0;
-    for (size_t b = b0 + w; b < b1; b += rows) {
+        for (int u = 0; u < 8; u++) {
+            x[u] = col[b + u * rows];
+#pragma unroll
+            for (int k = 0; k < L; k++) e[u][k] = eq[(b + u * rows) * L + k];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (((x[u] & dmask) >> l) & 1u) lazy_add<L>(acc, e[u]);
+    }
+    for (; b < b1; b += rows) {
         const uint64_t x = col[b] & dmask;
-        if ((x >> l) & 1u) fadd<L>(acc, eq + b * L, f.p);
+        if ((x >> l) & 1u) lazy_add<L>(acc, eq + b * L);
     }
     const uint32_t t = w * LB + l;
-#pragma unroll
-    for (int k = 0; k < L; k++) red[t * L + k] = acc[k];
+    red[t] = acc;
     __syncthreads();
     for (uint32_t h = rows / 2; h > 0; h >>= 1) {
-        if (w < h) fadd<L>(red + t * L, red + (t + h * LB) * L, f.p);
+        if (w < h) lazy_merge<L>(red[t], red[t + h * LB]);
         __syncthreads();
     }
     if (w == 0) {
-        uint64_t *po = partials + (((size_t)blockIdx.y * gridDim.x + blockIdx.x) * LB + l) * L;
+        uint32_t *po = reinterpret_cast<uint32_t *>(partials) +
+                       (((size_t)blockIdx.y * gridDim.x + blockIdx.x) * LB + l) * (2 * L + 2);
 #pragma unroll
-        for (int k = 0; k < L; k++) po[k] = red[l * L + k];
+        for (int k = 0; k < 2 * L + 1; k++) po[k] = red[l].w[k];
+        po[2 * L + 1] = 0;
     }
 }
 
@@ -123,18 +255,72 @@ __global__ void __launch_bounds__(256) k_lifted_int(const int64_t *__restrict__ 
     }
 }
 
+// eq(b, r) over nv variables as lo[b mod 2^a] * hi[b >> a] (a = nv / 2): the
+// half tables over the first a and the last nv - a variables first (one thread
+// per entry, a chain of at most 14 products), then one product per entry.
+// Field products are exact, so the grouping does not change any value.
+template <int L>
+__global__ void k_eq_halves(const uint64_t *__restrict__ r, const uint64_t *__restrict__ omr, uint32_t nv,
+                            FieldCfg f, uint64_t *__restrict__ halves) {
+    const uint32_t a = nv / 2, na = 1u << a, nb = 1u << (nv - a);
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= na + nb) return;
+    const bool hi = e >= na;
+    const uint32_t idx = hi ? e - na : e, k0 = hi ? a : 0, kn = hi ? nv - a : a;
+    uint64_t acc[L];
+#pragma unroll
+    for (int w = 0; w < L; w++) acc[w] = f.one[w];
+    for (uint32_t k = 0; k < kn; k++) {
+        const uint64_t *sel = ((idx >> k) & 1u) ? r + (size_t)(k0 + k) * L : omr + (size_t)(k0 + k) * L;
+        uint64_t t[L];
+        fmul<L>(acc, sel, f.p, f.n0, t);
+#pragma unroll
+        for (int w = 0; w < L; w++) acc[w] = t[w];
+    }
+#pragma unroll
+    for (int w = 0; w < L; w++) halves[(size_t)e * L + w] = acc[w];
+}
+
+template <int L>
+__global__ void __launch_bounds__(256) k_eq_outer(const uint64_t *__restrict__ halves, uint32_t nv, FieldCfg f,
+                                                  uint64_t *__restrict__ eq) {
+    const uint32_t a = nv / 2, na = 1u << a;
+    const size_t n = (size_t)1 << nv;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t t[L];
+        fmul<L>(halves + (i & (na - 1)) * L, halves + (na + (i >> a)) * L, f.p, f.n0, t);
+#pragma unroll
+        for (int w = 0; w < L; w++) eq[i * L + w] = t[w];
+    }
+}
+
 // out[o] = sum over `chunks` partials of slot o (slots: stride `width`).
+// lazy: the partials are lazy sums (2L + 2 words each, the last zero), else
+// canonical field elements (L words).
 template <int L>
 __global__ void k_lifted_reduce(const uint64_t *__restrict__ partials, uint32_t nslots, uint32_t chunks,
-                                uint32_t width, FieldCfg f, uint64_t *__restrict__ out) {
+                                uint32_t width, bool lazy, FieldCfg f, uint64_t *__restrict__ out) {
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= nslots) return;
     const uint32_t col = o / width, lane = o % width;
     uint64_t acc[L];
+    if (lazy) {
+        Lazy<L> z, q;
+        lazy_zero(z);
+        for (uint32_t c = 0; c < chunks; c++) {
+            const uint32_t *pq = reinterpret_cast<const uint32_t *>(partials) +
+                                 (((size_t)col * chunks + c) * width + lane) * (2 * L + 2);
 #pragma unroll
-    for (int k = 0; k < L; k++) acc[k] = 0;
-    for (uint32_t c = 0; c < chunks; c++)
-        fadd<L>(acc, partials + (((size_t)col * chunks + c) * width + lane) * L, f.p);
+            for (int k = 0; k < 2 * L + 1; k++) q.w[k] = pq[k];
+            lazy_merge<L>(z, q);
+        }
+        lazy_reduce<L>(z, f, acc);
+    } else {
+#pragma unroll
+        for (int k = 0; k < L; k++) acc[k] = 0;
+        for (uint32_t c = 0; c < chunks; c++)
+            fadd<L>(acc, partials + (((size_t)col * chunks + c) * width + lane) * L, f.p);
+    }
 #pragma unroll
     for (int k = 0; k < L; k++) out[(size_t)o * L + k] = acc[k];
 }
@@ -179,22 +365,29 @@ zg_status eval_projection_t(zg_ctx *ctx, const FieldCfg &f, const PiopCols &c, c
     std::vector<uint64_t> pw((size_t)64 * L, 0);
     std::memcpy(pw.data(), f.one, fb);
     for (uint32_t l = 1; l < c.D; l++) fmul<L>(&pw[(size_t)(l - 1) * L], a, f.p, f.n0, &pw[(size_t)l * L]);
+    const uint32_t nbytes = (c.D + 7) / 8;
+    const size_t tab_bytes = (size_t)nbytes * 256 * fb;
     const size_t sb = (staged_bytes(c, on_device) + 255) / 256 * 256;
-    ZG_TRY(ctx->sc_arena.ensure(sb + 64 * fb + (on_device ? 0 : cells * fb)));
+    ZG_TRY(ctx->sc_arena.ensure(sb + 64 * fb + tab_bytes + (on_device ? 0 : cells * fb)));
     uint8_t *arena = ctx->sc_arena.as<uint8_t>();
     const uint64_t *bin_d;
     const int64_t *ints_d;
     zg_status sst;
     stage_cols(c, on_device, s, arena, bin_d, ints_d, sst);
     ZG_TRY(sst);
-    uint64_t *pw_d = reinterpret_cast<uint64_t *>(arena + sb);
-    uint64_t *out_d = on_device ? out : pw_d + 64 * L;
+    uint64_t *pw_d = reinterpret_cast<uint64_t *>(arena + sb), *tab_d = pw_d + 64 * L;
+    uint64_t *out_d = on_device ? out : tab_d + (size_t)nbytes * 256 * L;
     ZG_CUDA(cudaMemcpyAsync(pw_d, pw.data(), 64 * fb, cudaMemcpyHostToDevice, s));
     const uint64_t dmask = c.D >= 64 ? ~0ull : ((1ull << c.D) - 1);
-    const unsigned blocks = (unsigned)std::min<size_t>((cells + 255) / 256, (size_t)ctx->num_sms * 16);
+    const unsigned blocks = (unsigned)std::min<size_t>((cells + 255) / 256, (size_t)ctx->num_sms * 8);
     if (cells) {
+        ZG_KBEGIN(ctx, s, "k_pow_tables");
+        k_pow_tables<L><<<(nbytes * 256 + 255) / 256, 256, 0, s>>>(pw_d, c.D, f, tab_d);
+        ZG_KEND(ctx, s);
+        if (tab_bytes + 3 * (2 * L + 1) * 4 > 48 * 1024) ZG_CUDA(allow_max_smem(k_eval_proj<L>));
         ZG_KBEGIN(ctx, s, "k_eval_proj");
-        k_eval_proj<L><<<blocks, 256, 0, s>>>(bin_d, c.n_bin, dmask, ints_d, c.n_int, c.nv, pw_d, c.D, f, out_d);
+        k_eval_proj<L><<<blocks, 256, tab_bytes + 3 * (2 * L + 1) * 4, s>>>(bin_d, c.n_bin, dmask, ints_d, c.n_int,
+                                                                            c.nv, tab_d, c.D, f, out_d);
         ZG_KEND(ctx, s);
     }
     if (!on_device) ZG_CUDA(cudaMemcpyAsync(out, out_d, cells * fb, cudaMemcpyDeviceToHost, s));
@@ -215,10 +408,11 @@ zg_status lifted_evals_t(zg_ctx *ctx, const FieldCfg &f, const PiopCols &c, cons
         fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
     }
     const size_t nv1 = std::max<uint32_t>(c.nv, 1);
-    const size_t pb = ((size_t)c.n_bin * chunks * LB + (size_t)c.n_int * chunks) * fb;
+    const size_t pb = (size_t)c.n_bin * chunks * LB * (fb + 8) + (size_t)c.n_int * chunks * fb;
     const size_t ob = ((size_t)c.n_bin * LB + c.n_int) * fb;
     const size_t sb = (staged_bytes(c, on_device) + 255) / 256 * 256;
-    ZG_TRY(ctx->sc_arena.ensure(sb + 2 * nv1 * fb + n * fb + pb + ob + 64));
+    const size_t halves = ((size_t)1 << (c.nv / 2)) + ((size_t)1 << (c.nv - c.nv / 2));
+    ZG_TRY(ctx->sc_arena.ensure(sb + 2 * nv1 * fb + n * fb + pb + ob + halves * fb + 64));
     uint8_t *arena = ctx->sc_arena.as<uint8_t>();
     const uint64_t *bin_d;
     const int64_t *ints_d;
@@ -229,9 +423,16 @@ zg_status lifted_evals_t(zg_ctx *ctx, const FieldCfg &f, const PiopCols &c, cons
     uint64_t *part_d = eq_d + n * L, *res_d = part_d + pb / 8;
     ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)c.nv * fb, cudaMemcpyHostToDevice, s));
     ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)c.nv * fb, cudaMemcpyHostToDevice, s));
-    ZG_TRY(launch_eq_table(ctx, r_d, omr_d, c.nv, f, eq_d, s));
+    uint64_t *half_d = res_d + ob / 8;
+    ZG_KBEGIN(ctx, s, "k_eq_halves");
+    k_eq_halves<L><<<(unsigned)((halves + 127) / 128), 128, 0, s>>>(r_d, omr_d, c.nv, f, half_d);
+    ZG_KEND(ctx, s);
+    ZG_KBEGIN(ctx, s, "k_eq_outer");
+    k_eq_outer<L><<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8), 256, 0, s>>>(
+        half_d, c.nv, f, eq_d);
+    ZG_KEND(ctx, s);
     const uint64_t dmask = c.D >= 64 ? ~0ull : ((1ull << c.D) - 1);
-    uint64_t *part_int = part_d + (size_t)c.n_bin * chunks * LB * L;
+    uint64_t *part_int = part_d + (size_t)c.n_bin * chunks * LB * (L + 1);
     uint64_t *res_int = res_d + (size_t)c.n_bin * LB * L;
     if (c.n_bin) {
         ZG_KBEGIN(ctx, s, "k_lifted_bin");
@@ -243,7 +444,7 @@ zg_status lifted_evals_t(zg_ctx *ctx, const FieldCfg &f, const PiopCols &c, cons
         ZG_KEND(ctx, s);
         ZG_KBEGIN(ctx, s, "k_lifted_reduce");
         const uint32_t slots = c.n_bin * LB;
-        k_lifted_reduce<L><<<(slots + 127) / 128, 128, 0, s>>>(part_d, slots, chunks, LB, f, res_d);
+        k_lifted_reduce<L><<<(slots + 127) / 128, 128, 0, s>>>(part_d, slots, chunks, LB, true, f, res_d);
         ZG_KEND(ctx, s);
     }
     if (c.n_int) {
@@ -251,7 +452,7 @@ zg_status lifted_evals_t(zg_ctx *ctx, const FieldCfg &f, const PiopCols &c, cons
         k_lifted_int<L><<<dim3(chunks, c.n_int), 256, 0, s>>>(ints_d, c.nv, eq_d, f, part_int);
         ZG_KEND(ctx, s);
         ZG_KBEGIN(ctx, s, "k_lifted_reduce");
-        k_lifted_reduce<L><<<(c.n_int + 127) / 128, 128, 0, s>>>(part_int, c.n_int, chunks, 1, f, res_int);
+        k_lifted_reduce<L><<<(c.n_int + 127) / 128, 128, 0, s>>>(part_int, c.n_int, chunks, 1, false, f, res_int);
         ZG_KEND(ctx, s);
     }
     std::vector<uint64_t> res(((size_t)c.n_bin * LB + c.n_int) * L);
