@@ -411,6 +411,22 @@ zg_status zg_piop_lifted_evals(zg_ctx *ctx, const uint8_t *modulus, uint32_t lim
                                const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
                                const int64_t *int_cols, uint32_t n_int, uint32_t nvars,
                                const uint64_t *point, int cols_on_device, uint64_t *coeffs_out);
+/* zg_piop_multipoint_eval: step 5, MultipointEval::prove_as_subprotocol
+ * (piop/src/multipoint_eval.rs:119-231).  Samples n_shifts alphas then num_cols
+ * gammas from `t` (get_field_challenges), builds eq(., r') and the shift selectors
+ * next_c(r', .) (build_next_c_r_mle, poly/src/utils.rs:207-236), precombines the
+ * columns as sum_j gamma_j v_j, and runs MLSumcheck of degree 2 over
+ * eq * precombined + sum_k alpha_k next_k * v_{src_k}.  trace_mles: num_cols MLEs of
+ * 2^nvars Montgomery inners (device memory when mles_on_device != 0, e.g. from
+ * zg_piop_eval_projection); eval_point: r' (nvars inners); shift k: source column
+ * shift_src[k] and shift shift_amount[k] < 2^nvars (ShiftSpec).  proof: the
+ * SumcheckProof transcription (proof_len as for zg_sumcheck_prove); r0_out
+ * (may be NULL): the sumcheck point r_0 (nvars inners). */
+zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                                  const uint64_t *trace_mles, uint32_t num_cols, uint32_t nvars,
+                                  const uint64_t *eval_point, const uint32_t *shift_src,
+                                  const uint32_t *shift_amount, uint32_t n_shifts, int mles_on_device,
+                                  uint8_t *proof, size_t *proof_len, uint64_t *r0_out);
 
 #ifdef __cplusplus
 }

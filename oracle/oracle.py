@@ -107,6 +107,7 @@ def lib():
         u32 = C.c_uint32
         L.zr_piop_eval_projection.argtypes = [vp, u32, vp, u32, u32, vp, u32, u32, vp, vp]
         L.zr_piop_lifted_evals.argtypes = [vp, u32, vp, u32, u32, vp, u32, u32, vp, vp]
+        L.zr_tr_field_challenge.argtypes = [vp, vp, u32, vp]
         _lib = L
     return _lib
 
@@ -302,6 +303,12 @@ class Transcript:
     def absorb_slice(self, b: bytes):
         lib().zr_tr_absorb_slice(self._t, _buf(b), len(b))
 
+    def field_challenge(self, modulus: int, L: int) -> np.ndarray:
+        """get_field_challenge: a Montgomery inner (L u64)."""
+        out = np.zeros(L, np.uint64)
+        lib().zr_tr_field_challenge(self._t, _ptr(_limbs(modulus, L)), L, _ptr(out))
+        return out
+
     def challenge(self, n: int) -> bytes:
         out = C.create_string_buffer(n)
         lib().zr_tr_challenge(self._t, out, n)
@@ -429,3 +436,44 @@ def piop_lifted_evals(modulus: int, L: int, bin_cols, D: int, int_cols, nvars: i
     lib().zr_piop_lifted_evals(_ptr(_limbs(modulus, L)), L, _ptr(b), b.shape[0], D, _ptr(i),
                                i.shape[0], nvars, _ptr(pt), _ptr(out))
     return out
+
+
+def piop_multipoint_eval(t: "Transcript", modulus: int, L: int, trace_mles: np.ndarray, point: np.ndarray,
+                         shifts):
+    """MultipointEval::prove_as_subprotocol (piop/src/multipoint_eval.rs:119-231)
+    restated with Python integers around the oracle's MLSumcheck: n_shifts alphas
+    then num_cols gammas from t, eq(., r'), next_c(r', .) = eq shifted up by c with
+    zeros below (build_next_c_r_mle, poly/src/utils.rs:207-236), precombined =
+    sum_j gamma_j v_j, and the degree-2 comb eq * precombined + sum_k alpha_k
+    next_k * v_src_k.  Returns (proof bytes, r_0 (nvars, L) inners)."""
+    p, R = modulus, 1 << (64 * L)
+    Rinv = pow(R, -1, p)
+    ncols, n, _ = trace_mles.shape
+    nv = point.shape[0]
+
+    def std(v):
+        return sum(int(w) << (64 * i) for i, w in enumerate(v)) * Rinv % p
+
+    def inner(x):
+        y = x % p * R % p
+        return [(y >> (64 * i)) & ((1 << 64) - 1) for i in range(L)]
+
+    alphas = [t.field_challenge(p, L) for _ in shifts]
+    gammas = [std(t.field_challenge(p, L)) for _ in range(ncols)]
+    r = [std(v) for v in point]
+    eq = []
+    for b in range(n):
+        e = 1
+        for k in range(nv):
+            e = e * (r[k] if (b >> k) & 1 else 1 - r[k]) % p
+        eq.append(e)
+    cols = [[std(trace_mles[j, b]) for b in range(n)] for j in range(ncols)]
+    pre = [sum(g * cols[j][b] for j, g in enumerate(gammas)) % p for b in range(n)]
+    S = len(shifts)
+    mles = [eq] + [[0] * c + eq[: n - c] for _, c in shifts] + [pre] + [cols[sc] for sc, _ in shifts]
+    arr = np.array([[inner(v) for v in m] for m in mles], np.uint64)
+    prods = [(int(sum(int(w) << (64 * i) for i, w in enumerate(inner(1)))), [0, 1 + S])]
+    for k in range(S):
+        prods.append((int(sum(int(w) << (64 * i) for i, w in enumerate(alphas[k]))), [1 + k, 2 + S + k]))
+    proof, pt, _fin = sumcheck_prove(t, p, L, nv, [(2, arr, prods)], False)
+    return proof, pt

@@ -2132,3 +2132,10 @@ void zr_piop_lifted_evals(const uint64_t *modulus, uint32_t L, const uint64_t *b
     }
     free(eq);
 }
+
+/* get_field_challenge (transcript/src/traits.rs:333-340) for modulus `modulus`. */
+void zr_tr_field_challenge(zr_transcript *t, const uint64_t *modulus, uint32_t L, uint64_t *out) {
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    tr_field_challenge(t, &f, out);
+}

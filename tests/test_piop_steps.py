@@ -112,3 +112,84 @@ def test_gpu_piop_argument_errors(zipgpu, oracle, ctx):
         zipgpu.ZincPiop.eval_projection(ctx, p - 1, 3, b, 32, None, 4, np.zeros(3, np.uint64))
     with pytest.raises(zipgpu.ZipError):  # BinaryPoly width above 64
         zipgpu.ZincPiop.eval_projection(ctx, p, 3, b, 65, None, 4, np.zeros(3, np.uint64))
+
+
+# ------------------------------------------------------------------ step 5
+def mp_case(oracle, L, nv, ncols, seed):
+    p = field(oracle, L)
+    rng = np.random.default_rng(seed)
+    mles = np.array([[inner(int.from_bytes(rng.bytes(8 * L), "little"), p, L) for _ in range(1 << nv)]
+                     for _ in range(ncols)], np.uint64)
+    r = np.array([inner(int.from_bytes(rng.bytes(8 * L), "little"), p, L) for _ in range(nv)], np.uint64)
+    return p, mles, r
+
+
+@pytest.mark.parametrize("L,nv,ncols,shifts", [(3, 4, 3, [(0, 1), (2, 3)]), (4, 3, 2, [(1, 1)]),
+                                               (3, 5, 4, [])])
+def test_oracle_multipoint_claim_is_the_batched_evaluations(oracle, L, nv, ncols, shifts):
+    """The proof's claimed sum is compute_expected_sum (multipoint_eval.rs:216-219):
+    sum_j gamma_j v_j(r') + sum_k alpha_k down_k, down_k = sum_b next_c(r', b) v_src(b),
+    and the oracle's sumcheck verifier accepts the proof at the returned point."""
+    p, mles, r = mp_case(oracle, L, nv, ncols, 40 + nv)
+    proof, r0 = oracle.piop_multipoint_eval(oracle.Transcript(), p, L, mles, r, shifts)
+    twin = oracle.Transcript()
+    alphas = [std(twin.field_challenge(p, L), p, L) for _ in shifts]
+    gammas = [std(twin.field_challenge(p, L), p, L) for _ in range(ncols)]
+    rs = [std(v, p, L) for v in r]
+    n = 1 << nv
+
+    def eq(b):
+        e = 1
+        for k in range(nv):
+            e = e * (rs[k] if (b >> k) & 1 else 1 - rs[k]) % p
+        return e
+
+    col = [[std(mles[j, b], p, L) for b in range(n)] for j in range(ncols)]
+    up = [sum(eq(b) * col[j][b] for b in range(n)) % p for j in range(ncols)]
+    down = [sum(eq(b - c) * col[sc][b] for b in range(c, n)) % p for sc, c in shifts]
+    want = (sum(g * u for g, u in zip(gammas, up)) + sum(a * d for a, d in zip(alphas, down))) % p
+    claimed = int.from_bytes(proof[-8 * L:], "little") * pow(1 << (64 * L), -1, p) % p
+    assert claimed == want
+    t2 = oracle.Transcript()  # the verifier draws the same alphas and gammas first
+    for _ in range(len(shifts) + ncols):
+        t2.field_challenge(p, L)
+    rc, vpt, _exp = oracle.sumcheck_verify(t2, p, L, nv, [2], proof, False)
+    assert rc == 0 and (vpt == r0).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,nv,ncols,shifts", [(3, 6, 3, [(0, 1), (2, 3)]), (4, 8, 5, [(4, 7), (0, 1), (1, 2)]),
+                                               (3, 10, 17, [(k + 1, 1) for k in range(16)]), (3, 5, 2, [])])
+def test_gpu_multipoint_eval_matches_oracle(zipgpu, oracle, ctx, L, nv, ncols, shifts):
+    p, mles, r = mp_case(oracle, L, nv, ncols, 60 + nv)
+    want_proof, want_r0 = oracle.piop_multipoint_eval(oracle.Transcript(), p, L, mles, r, shifts)
+    t = zipgpu.PcsProverTranscript()
+    proof, r0 = zipgpu.ZincPiop.multipoint_eval(ctx, t, p, L, mles, nv, r, shifts)
+    t.close()
+    assert proof == want_proof and np.array_equal(r0, want_r0)
+
+
+@pytest.mark.gpu
+def test_gpu_steps_3_and_5_chain_on_device(zipgpu, oracle, ctx):
+    """Step 3's device-resident MLEs feed step 5 directly (no host copy)."""
+    import torch
+
+    L, nv, D = 3, 9, 32
+    p = field(oracle, L)
+    rng = np.random.default_rng(77)
+    b, i = columns(rng, 4, 1, nv, D)
+    a = np.array(inner(int.from_bytes(rng.bytes(8 * L), "little"), p, L), np.uint64)
+    r = np.array([inner(int.from_bytes(rng.bytes(8 * L), "little"), p, L) for _ in range(nv)], np.uint64)
+    shifts = [(0, 1), (3, 2)]
+    mles = oracle.piop_eval_projection(p, L, b, D, i, nv, a)
+    want_proof, want_r0 = oracle.piop_multipoint_eval(oracle.Transcript(), p, L, mles, r, shifts)
+    bd = torch.from_numpy(b.view(np.int64)).cuda()
+    idv = torch.from_numpy(i).cuda()
+    out = torch.empty(mles.size, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    zipgpu.check(zipgpu.lib().zg_piop_eval_projection(ctx.handle, p.to_bytes(8 * L, "little"), L, bd.data_ptr(), 4,
+                                                      D, idv.data_ptr(), 1, nv, a.ctypes.data, 1, out.data_ptr()))
+    t = zipgpu.PcsProverTranscript()
+    proof, r0 = zipgpu.ZincPiop.multipoint_eval(ctx, t, p, L, (out.data_ptr(), 5), nv, r, shifts)
+    t.close()
+    assert proof == want_proof and np.array_equal(r0, want_r0)

@@ -325,6 +325,28 @@ __global__ void k_lifted_reduce(const uint64_t *__restrict__ partials, uint32_t 
     for (int k = 0; k < L; k++) out[(size_t)o * L + k] = acc[k];
 }
 
+// precombined[b] = sum_j gamma_j v_j[b] (multipoint_eval.rs:160-182): one
+// product per column, summed lazily, one reduction per entry.
+template <int L>
+__global__ void __launch_bounds__(256) k_precombine(const uint64_t *__restrict__ mles, uint32_t ncols, uint32_t nv,
+                                                    const uint64_t *__restrict__ gammas, FieldCfg f,
+                                                    uint64_t *__restrict__ out) {
+    const size_t n = (size_t)1 << nv;
+    for (size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x; b < n; b += (size_t)gridDim.x * blockDim.x) {
+        Lazy<L> z;
+        lazy_zero(z);
+        for (uint32_t j = 0; j < ncols; j++) {
+            uint64_t t[L];
+            fmul<L>(gammas + (size_t)j * L, mles + (((size_t)j << nv) + b) * L, f.p, f.n0, t);
+            lazy_add<L>(z, t);
+        }
+        uint64_t r[L];
+        lazy_reduce<L>(z, f, r);
+#pragma unroll
+        for (int w = 0; w < L; w++) out[b * L + w] = r[w];
+    }
+}
+
 struct PiopCols {
     const uint64_t *bin;
     uint32_t n_bin, D;
@@ -489,6 +511,75 @@ zg_status piop_args(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs, const P
     return ZG_OK;
 }
 
+// get_field_challenge (transcript/src/traits.rs:333-340): the inner's bytes
+// from the XOF, F::new_with_cfg (to Montgomery form).
+template <int L>
+void field_challenge_h(zg_transcript *t, const FieldCfg &f, uint64_t *out) {
+    uint8_t b[8 * L];
+    tr_challenge(t, b, sizeof b);
+    uint64_t x[L];
+    std::memcpy(x, b, sizeof b);
+    fmul<L>(x, f.r2, f.p, f.n0, out);
+}
+
+// Step 5 up to the sumcheck: challenges, then the packed MLEs
+// [eq_r, next_1 .. next_S, precombined, down_1 .. down_S] in ctx->piop_arena.
+template <int L>
+zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, const uint64_t *trace,
+                             uint32_t ncols, uint32_t nv, const uint64_t *point, const uint32_t *src,
+                             const uint32_t *shift, uint32_t S, int on_device, std::vector<uint64_t> &alphas,
+                             uint64_t **packed) {
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)1 << nv, fb = 8 * L, mle = n * fb;
+    alphas.assign((size_t)S * L, 0);
+    std::vector<uint64_t> gammas((size_t)ncols * L);
+    for (uint32_t k = 0; k < S; k++) field_challenge_h<L>(t, f, &alphas[(size_t)k * L]);
+    for (uint32_t j = 0; j < ncols; j++) field_challenge_h<L>(t, f, &gammas[(size_t)j * L]);
+    std::vector<uint64_t> omr((size_t)nv * L);
+    for (uint32_t k = 0; k < nv; k++) {
+        std::memcpy(&omr[(size_t)k * L], f.one, fb);
+        fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
+    }
+    const size_t halves = ((size_t)1 << (nv / 2)) + ((size_t)1 << (nv - nv / 2));
+    const size_t npk = 2 + 2 * (size_t)S;
+    const size_t staged = on_device ? 0 : (size_t)ncols * mle;
+    const size_t small = (2 * (size_t)nv + halves + ncols) * fb;
+    ZG_TRY(ctx->piop_arena.ensure(npk * mle + staged + small + 256));
+    uint8_t *ar = ctx->piop_arena.as<uint8_t>();
+    uint64_t *pk = reinterpret_cast<uint64_t *>(ar);
+    const uint64_t *tr = on_device ? trace : reinterpret_cast<const uint64_t *>(ar + npk * mle);
+    uint64_t *r_d = reinterpret_cast<uint64_t *>(ar + npk * mle + staged), *omr_d = r_d + (size_t)nv * L;
+    uint64_t *half_d = omr_d + (size_t)nv * L, *gam_d = half_d + halves * L;
+    if (!on_device) ZG_CUDA(cudaMemcpyAsync(const_cast<uint64_t *>(tr), trace, staged, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(gam_d, gammas.data(), (size_t)ncols * fb, cudaMemcpyHostToDevice, s));
+    uint64_t *eq = pk;  // MLE 0
+    ZG_KBEGIN(ctx, s, "k_eq_halves");
+    k_eq_halves<L><<<(unsigned)((halves + 127) / 128), 128, 0, s>>>(r_d, omr_d, nv, f, half_d);
+    ZG_KEND(ctx, s);
+    const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8);
+    ZG_KBEGIN(ctx, s, "k_eq_outer");
+    k_eq_outer<L><<<grid, 256, 0, s>>>(half_d, nv, f, eq);
+    ZG_KEND(ctx, s);
+    // next_c(r', b) = 0 for b < c, eq(r', b - c) for b >= c (build_next_c_r_mle,
+    // poly/src/utils.rs:207-236); the down columns are the shifts' source columns
+    for (uint32_t k = 0; k < S; k++) {
+        uint64_t *nx = pk + (size_t)(1 + k) * n * L;
+        const size_t c = shift[k];
+        if (c) ZG_CUDA(cudaMemsetAsync(nx, 0, c * fb, s));
+        ZG_CUDA(cudaMemcpyAsync(nx + c * L, eq, (n - c) * fb, cudaMemcpyDeviceToDevice, s));
+        ZG_CUDA(cudaMemcpyAsync(pk + (size_t)(2 + S + k) * n * L, tr + (size_t)src[k] * n * L, mle,
+                                cudaMemcpyDeviceToDevice, s));
+    }
+    ZG_KBEGIN(ctx, s, "k_precombine");
+    k_precombine<L><<<grid, 256, 0, s>>>(tr, ncols, nv, gam_d, f, pk + (size_t)(1 + S) * n * L);
+    ZG_KEND(ctx, s);
+    ZG_CUDA(ctx_sync(ctx));
+    *packed = pk;
+    return ZG_OK;
+}
+
 }  // namespace
 }  // namespace zg
 
@@ -526,6 +617,79 @@ extern "C" zg_status zg_piop_lifted_evals(zg_ctx *ctx, const uint8_t *modulus, u
                           : lifted_evals_t<4>(ctx, f, c, point, cols_on_device, coeffs_out);
     } catch (const std::exception &e) {
         set_error("piop: %s", e.what());
+        return ZG_ERR_OOM;
+    }
+}
+
+extern "C" zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
+                                             uint32_t limbs, const uint64_t *trace_mles, uint32_t num_cols,
+                                             uint32_t nvars, const uint64_t *eval_point,
+                                             const uint32_t *shift_src, const uint32_t *shift_amount,
+                                             uint32_t n_shifts, int mles_on_device, uint8_t *proof,
+                                             size_t *proof_len, uint64_t *r0_out) {
+    try {
+        if (!ctx || !t || !modulus || !trace_mles || !eval_point || !proof || !proof_len || num_cols == 0 ||
+            (n_shifts && (!shift_src || !shift_amount))) {
+            set_error("multipoint eval: null argument or no columns");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        if (limbs != 3 && limbs != 4) {
+            set_error("multipoint eval: field limbs must be 3 or 4 (got %u)", limbs);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        if (nvars == 0 || nvars > 28 || n_shifts > 1024 || num_cols > 4096) {
+            set_error("multipoint eval: num_vars must be 1..28, at most 1024 shifts and 4096 columns");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        for (uint32_t k = 0; k < n_shifts; k++)
+            if (shift_src[k] >= num_cols || (uint64_t)shift_amount[k] >= (1ull << nvars)) {
+                set_error("shift %u: source column %u or shift %u out of range", k, shift_src[k], shift_amount[k]);
+                return ZG_ERR_INVALID_PARAM;
+            }
+        uint64_t p[4] = {0, 0, 0, 0};
+        std::memcpy(p, modulus, 8 * limbs);
+        if (!(p[0] & 1)) {
+            set_error("multipoint eval: the modulus must be odd");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        std::vector<uint64_t> alphas;
+        uint64_t *packed = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            ZG_CUDA(cudaSetDevice(ctx->device));
+            field_cfg_init(t->f, p, (int)limbs);
+            t->has_field = true;
+            const zg_status st =
+                limbs == 3 ? multipoint_prepare<3>(ctx, t, t->f, trace_mles, num_cols, nvars, eval_point, shift_src,
+                                                   shift_amount, n_shifts, mles_on_device, alphas, &packed)
+                           : multipoint_prepare<4>(ctx, t, t->f, trace_mles, num_cols, nvars, eval_point, shift_src,
+                                                   shift_amount, n_shifts, mles_on_device, alphas, &packed);
+            if (st != ZG_OK) return st;
+        }
+        // comb = eq * precombined + sum_k alpha_k next_k down_k, degree 2 (multipoint_eval.rs:195-213)
+        const uint32_t S = n_shifts;
+        std::vector<uint64_t> coeffs((size_t)(1 + S) * limbs);
+        std::memcpy(coeffs.data(), t->f.one, 8 * limbs);
+        if (S) std::memcpy(&coeffs[limbs], alphas.data(), (size_t)S * 8 * limbs);
+        std::vector<uint32_t> offsets(2 + S), indices(2 * (1 + S));
+        for (uint32_t k = 0; k <= 1 + S; k++) offsets[k] = 2 * k;
+        indices[0] = 0;
+        indices[1] = 1 + S;
+        for (uint32_t k = 0; k < S; k++) {
+            indices[2 * (1 + k)] = 1 + k;
+            indices[2 * (1 + k) + 1] = 2 + S + k;
+        }
+        zg_sumcheck_group g{};
+        g.degree = 2;
+        g.n_mles = 2 + 2 * S;
+        g.n_products = 1 + S;
+        g.mles = packed;
+        g.coeffs = coeffs.data();
+        g.offsets = offsets.data();
+        g.indices = indices.data();
+        return zg_sumcheck_prove(ctx, t, modulus, limbs, nvars, 0, &g, 1, 1, proof, proof_len, r0_out, nullptr);
+    } catch (const std::exception &e) {
+        set_error("multipoint eval: %s", e.what());
         return ZG_ERR_OOM;
     }
 }

@@ -157,6 +157,7 @@ struct zg_ctx {
     zg::DevBuf prove_in;  // small per-prove inputs (alphas, points, coeffs, indices)
     zg::DevBuf prove_out; // b partials, combined row + openings
     zg::DevBuf sc_arena;  // sumcheck: staged MLEs, fold buffers, comb tables, partials
+    zg::DevBuf piop_arena;  // PIOP step 5: the packed MLEs handed to the sumcheck
     zg::HostBuf pin_in, pin_out;
     // kernel timing
     bool timing = false;

@@ -48,7 +48,7 @@ EXPORTS = (
     "zg_commit_prove", "zg_commit_prove_d", "zg_commit_prove_many", "zg_proof_size", "zg_verify",
     "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch", "zg_server_create",
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
-    "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals",
+    "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
 )
 
 
@@ -134,6 +134,8 @@ def lib() -> C.CDLL:
                                      C.c_uint32, C.c_uint32, vp, C.c_int, vp], st),
         "zg_piop_lifted_evals": ([vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
                                   C.c_uint32, C.c_uint32, vp, C.c_int, vp], st),
+        "zg_piop_multipoint_eval": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp, vp,
+                                     C.c_uint32, C.c_int, vp, C.POINTER(sz), vp], st),
         "zg_params_create": ([vp, C.POINTER(ParamsDesc), C.POINTER(vp)], st),
         "zg_params_destroy": ([vp], st),
         "zg_params_get_info": ([vp, C.POINTER(ParamsInfo)], st),
@@ -830,3 +832,27 @@ class ZincPiop:
         check(lib().zg_piop_lifted_evals(ctx.handle, mod, limbs, _ptr(b), b.shape[0], degree_plus_one,
                                          _ptr(i), i.shape[0], nvars, _ptr(pt), 0, _ptr(out)))
         return out
+
+    @staticmethod
+    def multipoint_eval(ctx: Context, transcript, modulus: int, limbs: int, trace_mles, nvars: int,
+                        eval_point, shifts):
+        """step5 (MultipointEval::prove_as_subprotocol): trace_mles (num_cols, 2^nvars,
+        limbs) Montgomery inners, or a device pointer int with num_cols given as
+        trace_mles=(ptr, num_cols); shifts [(source_col, shift_amount)].  Returns
+        (SumcheckProof bytes, r_0 (nvars, limbs))."""
+        if isinstance(trace_mles, tuple):
+            ptr, ncols, on_dev = trace_mles[0], trace_mles[1], 1
+        else:
+            arr = np.ascontiguousarray(trace_mles, dtype=np.uint64)
+            ptr, ncols, on_dev = arr.ctypes.data, arr.shape[0], 0
+        r = np.ascontiguousarray(eval_point, dtype=np.uint64)
+        src = np.array([sc for sc, _ in shifts] or [0], np.uint32)
+        amt = np.array([c for _, c in shifts] or [0], np.uint32)
+        cap = C.c_size_t(64 + 16 * limbs * (4 + 3 * nvars))
+        proof = C.create_string_buffer(cap.value)
+        r0 = np.zeros((nvars, limbs), np.uint64)
+        mod = modulus.to_bytes(8 * limbs, "little")
+        check(lib().zg_piop_multipoint_eval(ctx.handle, transcript.handle, mod, limbs, ptr, ncols, nvars,
+                                            _ptr(r), _ptr(src), _ptr(amt), len(shifts), on_dev, proof,
+                                            C.byref(cap), _ptr(r0)))
+        return proof.raw[: cap.value], r0
