@@ -843,13 +843,25 @@ def run_piop_steps(Z, ctx, torch, stream, nv, cpu_nv, with_cpu):
             ts.append(e0.elapsed_time(e1))
         return statistics.median(ts)
 
+    shifts = [(k, 1) for k in range(n_bin)]  # BigLinear's down columns: the binary columns shifted by one row
+    rp = np.array([inner(int.from_bytes(rng.bytes(24), "little")) for _ in range(nv)], np.uint64)
+
+    def step5():
+        tr = Z.PcsProverTranscript()
+        Z.ZincPiop.multipoint_eval(ctx, tr, p, L, (mles.data_ptr(), n_bin + n_int), nv, rp, shifts)
+        tr.close()
+
     ms3, ms6 = timed(step3), timed(step6)
+    ms5 = timed(step5)
     cells = (n_bin + n_int) << nv
     res = {"workload": f"BigLinear-shaped trace: {n_bin} BinaryPoly<{D}> + {n_int} integer columns, 2^{nv} rows, "
                        "MontyField<3> (192-bit prime from the transcript); columns resident on the device",
            "eval_projection": {"ms": ms3, "cells_per_s": cells / (ms3 / 1e3),
                                "output_bytes": cells * 8 * L},
-           "lifted_evals": {"ms": ms6, "cells_per_s": cells / (ms6 / 1e3)}}
+           "lifted_evals": {"ms": ms6, "cells_per_s": cells / (ms6 / 1e3)},
+           "multipoint_eval": {"ms": ms5, "shifts": len(shifts), "mles_in_sumcheck": 2 + 2 * len(shifts),
+                               "what": "alphas/gammas, eq and shift selectors, precombination and the degree-2 "
+                                       "MLSumcheck over step 3's device-resident MLEs"}}
     # parity at this size against the oracle on a sample of columns is in the tests;
     # here: the first MLE entries and the coefficients of the first column
     if with_cpu:
@@ -867,7 +879,18 @@ def run_piop_steps(Z, ctx, torch, stream, nv, cpu_nv, with_cpu):
         res["cpu_baseline"] = {"eval_projection_cells_per_s": cc / c3, "lifted_evals_cells_per_s": cc / c6,
                                "cores": 1, "kind": "port",
                                "sample": f"oracle at 2^{cpu_nv} rows ({c3:.2f} s + {c6:.2f} s)"}
-        res["equal_oracle_at_cpu_size"] = bool(np.array_equal(got3, want3) and np.array_equal(got6, want6))
+        # step 5 at a size the Python restatement finishes in seconds
+        nv5 = 8
+        m5 = O.piop_eval_projection(p, L, bs[:, : 1 << nv5], D, is_[:, : 1 << nv5], nv5, a)
+        a0 = time.perf_counter()
+        want5 = O.piop_multipoint_eval(O.Transcript(), p, L, m5, rp[:nv5], shifts)
+        c5 = time.perf_counter() - a0
+        tr = Z.PcsProverTranscript()
+        got5 = Z.ZincPiop.multipoint_eval(ctx, tr, p, L, m5, nv5, rp[:nv5], shifts)
+        tr.close()
+        res["cpu_baseline"]["multipoint_eval_s_at_2^8_rows"] = c5
+        res["equal_oracle_at_cpu_size"] = bool(np.array_equal(got3, want3) and np.array_equal(got6, want6)
+                                               and got5[0] == want5[0])
     return res
 
 
