@@ -422,6 +422,25 @@ zg_status zg_piop_lifted_evals(zg_ctx *ctx, const uint8_t *modulus, uint32_t lim
  * shift_src[k] and shift shift_amount[k] < 2^nvars (ShiftSpec).  proof: the
  * SumcheckProof transcription (proof_len as for zg_sumcheck_prove); r0_out
  * (may be NULL): the sumcheck point r_0 (nvars inners). */
+/* zg_piop_cpr_linear_prove: step 4 for a linear UAIR whose constraints are
+ * homogeneous linear forms over the up and down (shifted) columns:
+ * CombinedPolyResolver::prepare_sumcheck_group, MultiDegreeSumcheck with that
+ * one group, and finalize_prover (piop/src/combined_poly_resolver.rs:71-247).
+ * Draws the folding challenge alpha from `t`, builds the last-row selector,
+ * eq(., r) at eval_point (the ideal check's point) and the down columns (source
+ * column shifted up by the shift, zero padded), proves
+ * sum_b (sum_k alpha^k g_k(b)) (1 - sel(b)) eq_r(b) (degree 3), then absorbs the
+ * up and down columns' values at the sumcheck point.  coeffs: n_constraints x
+ * (num_cols + n_shifts) Montgomery inners (constraint k's coefficients over the
+ * up columns, then the down columns; projected scalars may appear here).
+ * proof: the MultiDegreeSumcheckProof transcription; point_out (may be NULL):
+ * the point r*; evals_out (may be NULL): up_evals then down_evals (CprProof). */
+zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                                   const uint64_t *trace_mles, uint32_t num_cols, uint32_t nvars,
+                                   const uint64_t *eval_point, const uint32_t *shift_src,
+                                   const uint32_t *shift_amount, uint32_t n_shifts, uint32_t n_constraints,
+                                   const uint64_t *coeffs, int mles_on_device, uint8_t *proof,
+                                   size_t *proof_len, uint64_t *point_out, uint64_t *evals_out);
 zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
                                   const uint64_t *trace_mles, uint32_t num_cols, uint32_t nvars,
                                   const uint64_t *eval_point, const uint32_t *shift_src,

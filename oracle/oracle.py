@@ -108,6 +108,7 @@ def lib():
         L.zr_piop_eval_projection.argtypes = [vp, u32, vp, u32, u32, vp, u32, u32, vp, vp]
         L.zr_piop_lifted_evals.argtypes = [vp, u32, vp, u32, u32, vp, u32, u32, vp, vp]
         L.zr_tr_field_challenge.argtypes = [vp, vp, u32, vp]
+        L.zr_tr_absorb_field.argtypes = [vp, vp, u32, vp]
         _lib = L
     return _lib
 
@@ -309,6 +310,11 @@ class Transcript:
         lib().zr_tr_field_challenge(self._t, _ptr(_limbs(modulus, L)), L, _ptr(out))
         return out
 
+    def absorb_field(self, modulus: int, L: int, inner) -> None:
+        """absorb_random_field of a Montgomery inner (L u64)."""
+        v = np.ascontiguousarray(inner, dtype=np.uint64)
+        lib().zr_tr_absorb_field(self._t, _ptr(_limbs(modulus, L)), L, _ptr(v))
+
     def challenge(self, n: int) -> bytes:
         out = C.create_string_buffer(n)
         lib().zr_tr_challenge(self._t, out, n)
@@ -477,3 +483,47 @@ def piop_multipoint_eval(t: "Transcript", modulus: int, L: int, trace_mles: np.n
         prods.append((int(sum(int(w) << (64 * i) for i, w in enumerate(alphas[k]))), [1 + k, 2 + S + k]))
     proof, pt, _fin = sumcheck_prove(t, p, L, nv, [(2, arr, prods)], False)
     return proof, pt
+
+
+def piop_cpr_linear_prove(t: "Transcript", modulus: int, L: int, trace_mles: np.ndarray, point: np.ndarray,
+                          shifts, coeffs):
+    """CombinedPolyResolver prepare_sumcheck_group + MultiDegreeSumcheck +
+    finalize_prover (piop/src/combined_poly_resolver.rs:71-247) for a linear
+    homogeneous UAIR, restated with Python integers around the oracle's
+    sumcheck.  coeffs: n_constraints x (num_cols + n_shifts) standard integers
+    (mod p).  Returns (proof, point, evals (num_cols + n_shifts, L))."""
+    p, R = modulus, 1 << (64 * L)
+    Rinv = pow(R, -1, p)
+    ncols, n, _ = trace_mles.shape
+    nv, S = point.shape[0], len(shifts)
+
+    def std(v):
+        return sum(int(w) << (64 * i) for i, w in enumerate(v)) * Rinv % p
+
+    def inner(x):
+        y = x % p * R % p
+        return [(y >> (64 * i)) & ((1 << 64) - 1) for i in range(L)]
+
+    def as_int(v):
+        return sum(int(w) << (64 * i) for i, w in enumerate(v))
+
+    alpha = std(t.field_challenge(p, L))
+    folded = [sum(pow(alpha, k, p) * int(row[j]) for k, row in enumerate(coeffs)) % p for j in range(ncols + S)]
+    r = [std(v) for v in point]
+    eq = []
+    for b in range(n):
+        e = 1
+        for k in range(nv):
+            e = e * (r[k] if (b >> k) & 1 else 1 - r[k]) % p
+        eq.append(e)
+    cols = [[std(trace_mles[j, b]) for b in range(n)] for j in range(ncols)]
+    sel = [0] * (n - 1) + [1]
+    down = [cols[sc][c:] + [0] * c for sc, c in shifts]
+    mles = np.array([[inner(v) for v in m] for m in [sel, eq] + cols + down], np.uint64)
+    prods = [(as_int(inner(folded[j])), [2 + j]) for j in range(ncols + S)]
+    factors = [(0, as_int(inner(1)), 1), (as_int(inner(1)), as_int(inner(p - 1)), 0)]
+    proof, pt, fin = sumcheck_prove(t, p, L, nv, [(3, mles, prods, factors)], True)
+    evals = np.array(fin[2:], np.uint64)
+    for e in evals:
+        t.absorb_field(p, L, e)
+    return proof, pt, evals

@@ -2139,3 +2139,10 @@ void zr_tr_field_challenge(zr_transcript *t, const uint64_t *modulus, uint32_t L
     fcfg_init(&f, modulus, L);
     tr_field_challenge(t, &f, out);
 }
+
+/* absorb_random_field (transcript/src/traits.rs:393-413) for modulus `modulus`. */
+void zr_tr_absorb_field(zr_transcript *t, const uint64_t *modulus, uint32_t L, const uint64_t *inner) {
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    tr_absorb_field(t, &f, inner);
+}

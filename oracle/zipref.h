@@ -120,6 +120,7 @@ void zr_piop_eval_projection(const uint64_t *modulus, uint32_t L, const uint64_t
                              uint32_t D, const int64_t *ints, uint32_t n_int, uint32_t nvars,
                              const uint64_t *a, uint64_t *out);
 void zr_tr_field_challenge(zr_transcript *t, const uint64_t *modulus, uint32_t L, uint64_t *out);
+void zr_tr_absorb_field(zr_transcript *t, const uint64_t *modulus, uint32_t L, const uint64_t *inner);
 void zr_piop_lifted_evals(const uint64_t *modulus, uint32_t L, const uint64_t *bin, uint32_t n_bin,
                           uint32_t D, const int64_t *ints, uint32_t n_int, uint32_t nvars,
                           const uint64_t *point, uint64_t *out);

@@ -193,3 +193,66 @@ def test_gpu_steps_3_and_5_chain_on_device(zipgpu, oracle, ctx):
     proof, r0 = zipgpu.ZincPiop.multipoint_eval(ctx, t, p, L, (out.data_ptr(), 5), nv, r, shifts)
     t.close()
     assert proof == want_proof and np.array_equal(r0, want_r0)
+
+
+# ------------------------------------------------------------------ step 4
+def biglinear_system():
+    """BigLinear's constraints as a coefficient matrix over [up (16 binary + 1
+    integer columns), down (the 16 binary columns shifted by one row)], and its
+    shifts; the same constraints as test_sumcheck_cpr.constraints()."""
+    from test_sumcheck_cpr import constraints, UP0
+    ncols, S = 17, 16
+    rows = []
+    for c in constraints():
+        row = [0] * (ncols + S)
+        for j, k in c.items():
+            row[j - UP0] = k
+        rows.append(row)
+    return ncols, [(k, 1) for k in range(S)], rows
+
+
+@pytest.mark.parametrize("L,nv", [(3, 4), (4, 3)])
+def test_oracle_cpr_claim_is_the_folded_constraints(oracle, L, nv):
+    ncols, shifts, rows = biglinear_system()
+    p, mles, r = mp_case(oracle, L, nv, ncols, 80 + nv)
+    proof, pt, evals = oracle.piop_cpr_linear_prove(oracle.Transcript(), p, L, mles, r, shifts, rows)
+    twin = oracle.Transcript()
+    alpha = std(twin.field_challenge(p, L), p, L)
+    rs, n = [std(v, p, L) for v in r], 1 << nv
+    col = [[std(mles[j, b], p, L) for b in range(n)] for j in range(ncols)]
+    up_down = col + [col[sc][c:] + [0] * c for sc, c in shifts]
+
+    def eq(b):
+        e = 1
+        for k in range(nv):
+            e = e * (rs[k] if (b >> k) & 1 else 1 - rs[k]) % p
+        return e
+
+    want = 0
+    for b in range(n - 1):  # the selector zeroes the last row
+        folded = sum(pow(alpha, k, p) * sum(cf * up_down[j][b] for j, cf in enumerate(row)) for k, row in enumerate(rows))
+        want = (want + folded * eq(b)) % p
+    # MultiDegreeSumcheckProof: the claimed sum is the group's last field element
+    claimed = int.from_bytes(proof[-8 * L:], "little") * pow(1 << (64 * L), -1, p) % p
+    assert claimed == want
+    rc, vpt, _ = oracle.sumcheck_verify(twin, p, L, nv, [3], proof, True)
+    assert rc == 0 and (vpt == pt).all()
+    # the evaluations are the up and down MLEs at the sumcheck point
+    for j in (0, ncols - 1, ncols):
+        m = np.array([inner(v, p, L) for v in up_down[j]], np.uint64)
+        assert (oracle.mle_evaluate(p, L, m, pt) == evals[j]).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,nv", [(3, 8), (4, 6), (3, 11)])
+def test_gpu_cpr_linear_prove_matches_oracle(zipgpu, oracle, ctx, L, nv):
+    ncols, shifts, rows = biglinear_system()
+    p, mles, r = mp_case(oracle, L, nv, ncols, 90 + nv)
+    ot = oracle.Transcript()
+    want = oracle.piop_cpr_linear_prove(ot, p, L, mles, r, shifts, rows)
+    t = zipgpu.PcsProverTranscript()
+    got = zipgpu.ZincPiop.cpr_linear_prove(ctx, t, p, L, mles, nv, r, shifts, rows)
+    after = t.get_challenge(32)
+    t.close()
+    assert got[0] == want[0] and np.array_equal(got[1], want[1]) and np.array_equal(got[2], want[2])
+    assert after == ot.challenge(32)  # the up/down evaluations were absorbed the same way

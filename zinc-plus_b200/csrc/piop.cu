@@ -580,6 +580,72 @@ zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, c
     return ZG_OK;
 }
 
+// Step 4 for a linear UAIR up to the sumcheck: the folding challenge and the
+// packed MLEs [last-row selector, eq_r, up_1 .. up_J, down_1 .. down_S] in
+// ctx->piop_arena (combined_poly_resolver.rs:71-178).  coeffs: n_cons x (J + S)
+// Montgomery inners (constraint k's coefficients over up then down columns);
+// folded_out: J + S inners A_j = sum_k alpha^k coeffs[k][j].
+template <int L>
+zg_status cpr_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, const uint64_t *trace, uint32_t J,
+                      uint32_t nv, const uint64_t *point, const uint32_t *src, const uint32_t *shift, uint32_t S,
+                      uint32_t n_cons, const uint64_t *coeffs, int on_device, std::vector<uint64_t> &folded,
+                      uint64_t **packed) {
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)1 << nv, fb = 8 * L, mle = n * fb;
+    uint64_t alpha[L], pw[L];
+    field_challenge_h<L>(t, f, alpha);  // the folding challenge
+    folded.assign((size_t)(J + S) * L, 0);
+    std::memcpy(pw, f.one, fb);
+    for (uint32_t k = 0; k < n_cons; k++) {
+        for (uint32_t j = 0; j < J + S; j++) {
+            uint64_t tm[L];
+            fmul<L>(pw, coeffs + ((size_t)k * (J + S) + j) * L, f.p, f.n0, tm);
+            fadd<L>(&folded[(size_t)j * L], tm, f.p);
+        }
+        uint64_t nx[L];
+        fmul<L>(pw, alpha, f.p, f.n0, nx);
+        std::memcpy(pw, nx, fb);
+    }
+    std::vector<uint64_t> omr((size_t)nv * L);
+    for (uint32_t k = 0; k < nv; k++) {
+        std::memcpy(&omr[(size_t)k * L], f.one, fb);
+        fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
+    }
+    const size_t halves = ((size_t)1 << (nv / 2)) + ((size_t)1 << (nv - nv / 2));
+    const size_t npk = 2 + (size_t)J + S;
+    const size_t small = (2 * (size_t)nv + halves) * fb;
+    ZG_TRY(ctx->piop_arena.ensure(npk * mle + small + 256));
+    uint8_t *ar = ctx->piop_arena.as<uint8_t>();
+    uint64_t *pk = reinterpret_cast<uint64_t *>(ar);
+    uint64_t *r_d = reinterpret_cast<uint64_t *>(ar + npk * mle), *omr_d = r_d + (size_t)nv * L;
+    uint64_t *half_d = omr_d + (size_t)nv * L;
+    uint64_t *up = pk + 2 * n * L, *down = up + (size_t)J * n * L;
+    ZG_CUDA(cudaMemcpyAsync(up, trace, (size_t)J * mle, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            s));
+    ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    // last-row selector: one at index 2^nv - 1
+    ZG_CUDA(cudaMemsetAsync(pk, 0, mle, s));
+    ZG_CUDA(cudaMemcpyAsync(pk + (n - 1) * L, f.one, fb, cudaMemcpyHostToDevice, s));
+    ZG_KBEGIN(ctx, s, "k_eq_halves");
+    k_eq_halves<L><<<(unsigned)((halves + 127) / 128), 128, 0, s>>>(r_d, omr_d, nv, f, half_d);
+    ZG_KEND(ctx, s);
+    ZG_KBEGIN(ctx, s, "k_eq_outer");
+    k_eq_outer<L><<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8), 256, 0, s>>>(
+        half_d, nv, f, pk + n * L);
+    ZG_KEND(ctx, s);
+    // down column k: up column src[k] from row shift[k] on, zero padded
+    for (uint32_t k = 0; k < S; k++) {
+        uint64_t *dk = down + (size_t)k * n * L;
+        const size_t c = shift[k];
+        ZG_CUDA(cudaMemcpyAsync(dk, up + ((size_t)src[k] * n + c) * L, (n - c) * fb, cudaMemcpyDeviceToDevice, s));
+        if (c) ZG_CUDA(cudaMemsetAsync(dk + (n - c) * L, 0, c * fb, s));
+    }
+    ZG_CUDA(ctx_sync(ctx));
+    *packed = pk;
+    return ZG_OK;
+}
+
 }  // namespace
 }  // namespace zg
 
@@ -690,6 +756,100 @@ extern "C" zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, cons
         return zg_sumcheck_prove(ctx, t, modulus, limbs, nvars, 0, &g, 1, 1, proof, proof_len, r0_out, nullptr);
     } catch (const std::exception &e) {
         set_error("multipoint eval: %s", e.what());
+        return ZG_ERR_OOM;
+    }
+}
+
+extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
+                                              uint32_t limbs, const uint64_t *trace_mles, uint32_t num_cols,
+                                              uint32_t nvars, const uint64_t *eval_point,
+                                              const uint32_t *shift_src, const uint32_t *shift_amount,
+                                              uint32_t n_shifts, uint32_t n_constraints, const uint64_t *coeffs,
+                                              int mles_on_device, uint8_t *proof, size_t *proof_len,
+                                              uint64_t *point_out, uint64_t *evals_out) {
+    try {
+        if (!ctx || !t || !modulus || !trace_mles || !eval_point || !proof || !proof_len || !coeffs ||
+            num_cols == 0 || n_constraints == 0 || (n_shifts && (!shift_src || !shift_amount))) {
+            set_error("CPR: null argument, no columns or no constraints");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        if (limbs != 3 && limbs != 4) {
+            set_error("CPR: field limbs must be 3 or 4 (got %u)", limbs);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        if (nvars < 2 || nvars > 28 || n_shifts > 1024 || num_cols > 4096 || n_constraints > 65536) {
+            set_error("CPR: num_vars must be 2..28 (the protocol is not needed for 1), at most 1024 shifts, "
+                      "4096 columns and 65536 constraints");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        for (uint32_t k = 0; k < n_shifts; k++)
+            if (shift_src[k] >= num_cols || (uint64_t)shift_amount[k] >= (1ull << nvars)) {
+                set_error("shift %u: source column %u or shift %u out of range", k, shift_src[k], shift_amount[k]);
+                return ZG_ERR_INVALID_PARAM;
+            }
+        uint64_t p[4] = {0, 0, 0, 0};
+        std::memcpy(p, modulus, 8 * limbs);
+        if (!(p[0] & 1)) {
+            set_error("CPR: the modulus must be odd");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        const uint32_t J = num_cols, S = n_shifts;
+        std::vector<uint64_t> folded;
+        uint64_t *packed = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            ZG_CUDA(cudaSetDevice(ctx->device));
+            field_cfg_init(t->f, p, (int)limbs);
+            t->has_field = true;
+            const zg_status st =
+                limbs == 3 ? cpr_prepare<3>(ctx, t, t->f, trace_mles, J, nvars, eval_point, shift_src, shift_amount, S,
+                                            n_constraints, coeffs, mles_on_device, folded, &packed)
+                           : cpr_prepare<4>(ctx, t, t->f, trace_mles, J, nvars, eval_point, shift_src, shift_amount, S,
+                                            n_constraints, coeffs, mles_on_device, folded, &packed);
+            if (st != ZG_OK) return st;
+        }
+        // comb = (sum_j A_j v_j) * eq_r * (1 - selector): one-MLE products times two
+        // affine factors, degree max_degree + 2 = 3 (combined_poly_resolver.rs:147-172)
+        std::vector<uint32_t> offsets(J + S + 1), indices(J + S);
+        for (uint32_t j = 0; j <= J + S; j++) offsets[j] = j;
+        for (uint32_t j = 0; j < J + S; j++) indices[j] = 2 + j;
+        const uint32_t fm[2] = {1, 0};
+        std::vector<uint64_t> fa(2 * (size_t)limbs, 0), fbv(2 * (size_t)limbs, 0);
+        std::memcpy(&fbv[0], t->f.one, 8 * limbs);      // eq_r: 0 + 1 * eq_r
+        std::memcpy(&fa[limbs], t->f.one, 8 * limbs);   // 1 - sel: one + (p - one) * sel
+        std::memcpy(&fbv[limbs], t->f.p, 8 * limbs);
+        {
+            uint64_t *b1 = &fbv[limbs];
+            unsigned __int128 br = 0;
+            for (uint32_t w = 0; w < limbs; w++) {
+                const unsigned __int128 d = (unsigned __int128)b1[w] - t->f.one[w] - (uint64_t)br;
+                b1[w] = (uint64_t)d;
+                br = (d >> 64) & 1;
+            }
+        }
+        zg_sumcheck_group g{};
+        g.degree = 3;
+        g.n_mles = 2 + J + S;
+        g.n_products = J + S;
+        g.mles = packed;
+        g.coeffs = folded.data();
+        g.offsets = offsets.data();
+        g.indices = indices.data();
+        g.n_factors = 2;
+        g.factor_mles = fm;
+        g.factor_a = fa.data();
+        g.factor_b = fbv.data();
+        std::vector<uint64_t> finals((size_t)(2 + J + S) * limbs);
+        ZG_TRY(zg_sumcheck_prove(ctx, t, modulus, limbs, nvars, 1, &g, 1, 1, proof, proof_len, point_out,
+                                 finals.data()));
+        // finalize_prover (combined_poly_resolver.rs:192-247): the up and down
+        // columns at the sumcheck point, absorbed as random-field elements
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        for (uint32_t j = 0; j < J + S; j++) tr_absorb_field(t, &finals[(size_t)(2 + j) * limbs]);
+        if (evals_out) std::memcpy(evals_out, &finals[2 * (size_t)limbs], (size_t)(J + S) * 8 * limbs);
+        return ZG_OK;
+    } catch (const std::exception &e) {
+        set_error("CPR: %s", e.what());
         return ZG_ERR_OOM;
     }
 }

@@ -49,6 +49,7 @@ EXPORTS = (
     "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch", "zg_server_create",
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
+    "zg_piop_cpr_linear_prove",
 )
 
 
@@ -136,6 +137,8 @@ def lib() -> C.CDLL:
                                   C.c_uint32, C.c_uint32, vp, C.c_int, vp], st),
         "zg_piop_multipoint_eval": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp, vp,
                                      C.c_uint32, C.c_int, vp, C.POINTER(sz), vp], st),
+        "zg_piop_cpr_linear_prove": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp, vp,
+                                      C.c_uint32, C.c_uint32, vp, C.c_int, vp, C.POINTER(sz), vp, vp], st),
         "zg_params_create": ([vp, C.POINTER(ParamsDesc), C.POINTER(vp)], st),
         "zg_params_destroy": ([vp], st),
         "zg_params_get_info": ([vp, C.POINTER(ParamsInfo)], st),
@@ -856,3 +859,31 @@ class ZincPiop:
                                             _ptr(r), _ptr(src), _ptr(amt), len(shifts), on_dev, proof,
                                             C.byref(cap), _ptr(r0)))
         return proof.raw[: cap.value], r0
+
+    @staticmethod
+    def cpr_linear_prove(ctx: Context, transcript, modulus: int, limbs: int, trace_mles, nvars: int, eval_point,
+                         shifts, coeffs):
+        """step4 for a linear UAIR: trace_mles (num_cols, 2^nvars, limbs) inners or
+        (device pointer, num_cols); coeffs (n_constraints, num_cols + len(shifts))
+        standard integers mod the modulus.  Returns (proof, point (nvars, limbs),
+        evals (num_cols + len(shifts), limbs))."""
+        if isinstance(trace_mles, tuple):
+            ptr, ncols, on_dev = trace_mles[0], trace_mles[1], 1
+        else:
+            arr = np.ascontiguousarray(trace_mles, dtype=np.uint64)
+            ptr, ncols, on_dev = arr.ctypes.data, arr.shape[0], 0
+        R = 1 << (64 * limbs)
+        cf = np.array([[[((int(c) % modulus) * R % modulus >> (64 * w)) & ((1 << 64) - 1) for w in range(limbs)]
+                        for c in row] for row in coeffs], np.uint64)
+        r = np.ascontiguousarray(eval_point, dtype=np.uint64)
+        src = np.array([sc for sc, _ in shifts] or [0], np.uint32)
+        amt = np.array([c for _, c in shifts] or [0], np.uint32)
+        cap = C.c_size_t(64 + 8 * limbs * (8 + 6 * nvars))
+        proof = C.create_string_buffer(cap.value)
+        pt = np.zeros((nvars, limbs), np.uint64)
+        ev = np.zeros((ncols + len(shifts), limbs), np.uint64)
+        mod = modulus.to_bytes(8 * limbs, "little")
+        check(lib().zg_piop_cpr_linear_prove(ctx.handle, transcript.handle, mod, limbs, ptr, ncols, nvars, _ptr(r),
+                                             _ptr(src), _ptr(amt), len(shifts), cf.shape[0], _ptr(cf), on_dev,
+                                             proof, C.byref(cap), _ptr(pt), _ptr(ev)))
+        return proof.raw[: cap.value], pt, ev
