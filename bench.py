@@ -851,14 +851,35 @@ def run_piop_steps(Z, ctx, torch, stream, nv, cpu_nv, with_cpu):
         Z.ZincPiop.multipoint_eval(ctx, tr, p, L, (mles.data_ptr(), n_bin + n_int), nv, rp, shifts)
         tr.close()
 
+    # step 4 with BigLinear's linear constraints: the binary columns sum to the
+    # integer column; down.bin[0] equals up.int; up.bin[i] equals down.bin[i]
+    cons = []
+    row = [1] * n_bin + [-1] + [0] * n_bin
+    cons.append(row)
+    row = [0] * (n_bin + 1) + [1] + [0] * (n_bin - 1)
+    row[n_bin] = -1
+    cons.append(row)
+    for k in range(1, n_bin):
+        row = [0] * (2 * n_bin + 1)
+        row[k], row[n_bin + 1 + k] = 1, -1
+        cons.append(row)
+
+    def step4():
+        tr = Z.PcsProverTranscript()
+        Z.ZincPiop.cpr_linear_prove(ctx, tr, p, L, (mles.data_ptr(), n_bin + n_int), nv, rp, shifts, cons)
+        tr.close()
+
     ms3, ms6 = timed(step3), timed(step6)
-    ms5 = timed(step5)
+    ms5, ms4 = timed(step5), timed(step4)
     cells = (n_bin + n_int) << nv
     res = {"workload": f"BigLinear-shaped trace: {n_bin} BinaryPoly<{D}> + {n_int} integer columns, 2^{nv} rows, "
                        "MontyField<3> (192-bit prime from the transcript); columns resident on the device",
            "eval_projection": {"ms": ms3, "cells_per_s": cells / (ms3 / 1e3),
                                "output_bytes": cells * 8 * L},
            "lifted_evals": {"ms": ms6, "cells_per_s": cells / (ms6 / 1e3)},
+           "cpr_linear": {"ms": ms4, "constraints": len(cons), "mles_in_sumcheck": 2 + n_bin + n_int + len(shifts),
+                          "what": "folding challenge, selector, eq and down columns, degree-3 MultiDegreeSumcheck "
+                                  "and the absorbed up/down evaluations over step 3's device-resident MLEs"},
            "multipoint_eval": {"ms": ms5, "shifts": len(shifts), "mles_in_sumcheck": 2 + 2 * len(shifts),
                                "what": "alphas/gammas, eq and shift selectors, precombination and the degree-2 "
                                        "MLSumcheck over step 3's device-resident MLEs"}}
