@@ -435,6 +435,25 @@ zg_status zg_piop_lifted_evals(zg_ctx *ctx, const uint8_t *modulus, uint32_t lim
  * up columns, then the down columns; projected scalars may appear here).
  * proof: the MultiDegreeSumcheckProof transcription; point_out (may be NULL):
  * the point r*; evals_out (may be NULL): up_evals then down_evals (CprProof). */
+/* zg_piop_ideal_check_linear: step 2 for a linear UAIR, MLE first
+ * (IdealCheckProtocol::prove_linear, piop/src/ideal_check.rs:137-176 with
+ * combined_poly_builder::evaluate_combined_polynomials).  Draws nvars field
+ * challenges from `t` as the point r (point_out), evaluates every up column (the
+ * projected trace: binary columns as 0/1-coefficient polynomials, integer columns
+ * as constants) and every shifted down column coefficient-wise at r, applies each
+ * constraint's coefficients (n_constraints x (n_bin + n_int + n_shifts) Montgomery
+ * inners over [binary up, integer up, down in shift order]) to those polynomial
+ * values, and absorbs each constraint's combined value trimmed of trailing zero
+ * coefficients (DynamicPolynomialF::new_trimmed).  combined_out: n_constraints x
+ * degree_plus_one inners (zero padded); lengths_out: the trimmed lengths.  Shift
+ * sources index the up columns (binary first).  cols_on_device: the columns are
+ * device pointers. */
+zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                                     const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
+                                     const int64_t *int_cols, uint32_t n_int, uint32_t nvars,
+                                     const uint32_t *shift_src, const uint32_t *shift_amount, uint32_t n_shifts,
+                                     uint32_t n_constraints, const uint64_t *coeffs, int cols_on_device,
+                                     uint64_t *point_out, uint64_t *combined_out, uint32_t *lengths_out);
 zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
                                    const uint64_t *trace_mles, uint32_t num_cols, uint32_t nvars,
                                    const uint64_t *eval_point, const uint32_t *shift_src,

@@ -527,3 +527,57 @@ def piop_cpr_linear_prove(t: "Transcript", modulus: int, L: int, trace_mles: np.
     for e in evals:
         t.absorb_field(p, L, e)
     return proof, pt, evals
+
+
+def piop_ideal_check_linear(t: "Transcript", modulus: int, L: int, bin_cols, D: int, int_cols, nvars: int,
+                            shifts, coeffs):
+    """IdealCheckProtocol::prove_linear (piop/src/ideal_check.rs:137-176) restated:
+    nvars field challenges as the point, the up and shifted down columns evaluated
+    coefficient-wise there (compute_lifted_evals on the columns), each constraint's
+    coefficients (standard integers) applied, trimmed, absorbed.  Returns
+    (point (nvars, L), [combined (len, L) per constraint])."""
+    p, R = modulus, 1 << (64 * L)
+    Rinv = pow(R, -1, p)
+    n = 1 << nvars
+    b, i = _piop_cols(bin_cols, int_cols, nvars)
+    nb, ni = b.shape[0], i.shape[0]
+    point = np.array([t.field_challenge(p, L) for _ in range(nvars)], np.uint64).reshape(nvars, L)
+
+    def shifted(col, c):
+        return np.concatenate([col[c:], np.zeros(c, col.dtype)])
+
+    db = [shifted(b[sc], c) for sc, c in shifts if sc < nb]
+    di = [shifted(i[sc - nb], c) for sc, c in shifts if sc >= nb]
+    eb = np.stack(list(b) + db) if nb + len(db) else None
+    ei = np.stack(list(i) + di) if ni + len(di) else None
+    vals = piop_lifted_evals(p, L, eb, D, ei, nvars, point)
+    nb2 = nb + len(db)
+
+    def std(v):
+        return sum(int(w) << (64 * k) for k, w in enumerate(v)) * Rinv % p
+
+    def value(j):  # polynomial value (D standard coefficients) of column j of [up, down]
+        if j < nb:
+            return [std(vals[j * D + l]) for l in range(D)]
+        if j < nb + ni:
+            return [std(vals[nb2 * D + j - nb])] + [0] * (D - 1)
+        k = j - nb - ni
+        sc = shifts[k][0]
+        if sc < nb:
+            q = [kk for kk in range(len(shifts)) if shifts[kk][0] < nb].index(k)
+            return [std(vals[(nb + q) * D + l]) for l in range(D)]
+        q = [kk for kk in range(len(shifts)) if shifts[kk][0] >= nb].index(k)
+        return [std(vals[nb2 * D + ni + q])] + [0] * (D - 1)
+
+    cols = [value(j) for j in range(nb + ni + len(shifts))]
+    out = []
+    for row in coeffs:
+        comb = [sum(int(cf) * cols[j][l] for j, cf in enumerate(row)) % p for l in range(D)]
+        while comb and comb[-1] == 0:
+            comb.pop()
+        arr = np.array([[((x * R % p) >> (64 * w)) & ((1 << 64) - 1) for w in range(L)] for x in comb],
+                       np.uint64).reshape(len(comb), L)
+        for e in arr:
+            t.absorb_field(p, L, e)
+        out.append(arr)
+    return point, out

@@ -256,3 +256,59 @@ def test_gpu_cpr_linear_prove_matches_oracle(zipgpu, oracle, ctx, L, nv):
     t.close()
     assert got[0] == want[0] and np.array_equal(got[1], want[1]) and np.array_equal(got[2], want[2])
     assert after == ot.challenge(32)  # the up/down evaluations were absorbed the same way
+
+
+# ------------------------------------------------------------------ step 2
+@pytest.mark.parametrize("L,nv", [(3, 4), (4, 3)])
+def test_oracle_ideal_check_linear_is_the_definition(oracle, L, nv):
+    """Combined value of constraint k = sum_j c_kj sum_b eq(b, r) col_j(b) in F[X],
+    col_j the projected column (a binary cell's 0/1 coefficients, an integer as a
+    constant; down columns shifted up by their shift), trimmed."""
+    ncols, shifts, rows = biglinear_system()
+    D, n = 32, 1 << nv
+    p = field(oracle, L)
+    rng = np.random.default_rng(120 + nv)
+    b, i = columns(rng, 16, 1, nv, D)
+    pt, combined = oracle.piop_ideal_check_linear(oracle.Transcript(), p, L, b, D, i, nv, shifts, rows)
+    twin = oracle.Transcript()
+    r = [std(twin.field_challenge(p, L), p, L) for _ in range(nv)]
+    assert [std(v, p, L) for v in pt] == r
+
+    def eq(x):
+        e = 1
+        for k in range(nv):
+            e = e * (r[k] if (x >> k) & 1 else 1 - r[k]) % p
+        return e
+
+    def poly(j, x):  # projected cell of up column j at row x
+        if j < 16:
+            return [(int(b[j, x]) >> l) & 1 for l in range(D)]
+        return [int(i[0, x]) % p] + [0] * (D - 1)
+
+    up = [[sum(eq(x) * poly(j, x)[l] for x in range(n)) % p for l in range(D)] for j in range(ncols)]
+    down = [[sum(eq(x) * poly(sc, x + c)[l] for x in range(n - c)) % p for l in range(D)] for sc, c in shifts]
+    vals = up + down
+    for k, row in enumerate(rows):
+        want = [sum(cf * vals[j][l] for j, cf in enumerate(row)) % p for l in range(D)]
+        while want and want[-1] == 0:
+            want.pop()
+        assert [std(e, p, L) for e in combined[k]] == want
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,nv", [(3, 9), (4, 7), (3, 12)])
+def test_gpu_ideal_check_linear_matches_oracle(zipgpu, oracle, ctx, L, nv):
+    ncols, shifts, rows = biglinear_system()
+    D = 32
+    p = field(oracle, L)
+    rng = np.random.default_rng(130 + nv)
+    b, i = columns(rng, 16, 1, nv, D)
+    ot = oracle.Transcript()
+    wpt, wcomb = oracle.piop_ideal_check_linear(ot, p, L, b, D, i, nv, shifts, rows)
+    t = zipgpu.PcsProverTranscript()
+    gpt, gcomb = zipgpu.ZincPiop.ideal_check_linear(ctx, t, p, L, b, D, i, nv, shifts, rows)
+    after = t.get_challenge(32)
+    t.close()
+    assert np.array_equal(gpt, wpt)
+    assert len(gcomb) == len(wcomb) and all(np.array_equal(g, w) for g, w in zip(gcomb, wcomb))
+    assert after == ot.challenge(32)

@@ -13,6 +13,7 @@
 //                  coefficient is sum_b eq(b, r0) F(c[b]).  Per-block partial sums,
 //                  then k_lifted_reduce.
 // Field elements are Montgomery inners (F::Inner of MontyField) of 3 or 4 limbs.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -850,6 +851,123 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
         return ZG_OK;
     } catch (const std::exception &e) {
         set_error("CPR: %s", e.what());
+        return ZG_ERR_OOM;
+    }
+}
+
+// Step 2 for a linear UAIR (IdealCheckProtocol::prove_linear, piop/src/ideal_check.rs:
+// 137-176, MLE first): the point r from the transcript, every up column and every
+// shifted (down) column evaluated coefficient-wise at r (the lifted-evaluation sums
+// on copies of the columns, the down ones shifted up and zero padded), each
+// constraint's coefficients applied to those polynomial values, and the trimmed
+// combined values absorbed constraint after constraint.
+extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
+                                                uint32_t limbs, const uint64_t *bin_cols, uint32_t n_bin,
+                                                uint32_t degree_plus_one, const int64_t *int_cols, uint32_t n_int,
+                                                uint32_t nvars, const uint32_t *shift_src,
+                                                const uint32_t *shift_amount, uint32_t n_shifts,
+                                                uint32_t n_constraints, const uint64_t *coeffs, int cols_on_device,
+                                                uint64_t *point_out, uint64_t *combined_out, uint32_t *lengths_out) {
+    try {
+        const uint32_t D = degree_plus_one, J = n_bin + n_int, S = n_shifts;
+        const PiopCols c0{bin_cols, n_bin, D, int_cols, n_int, nvars};
+        FieldCfg f;
+        if (!t || !point_out || !combined_out || !lengths_out || !coeffs || n_constraints == 0 || J == 0 ||
+            (S && (!shift_src || !shift_amount)) || S > 1024 || n_constraints > 65536) {
+            set_error("ideal check: null argument, no columns or constraints, or more than 1024 shifts");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        ZG_TRY(piop_args(ctx, modulus, limbs, c0, coeffs, combined_out, f));
+        if (nvars == 0) {
+            set_error("ideal check: num_vars must be at least 1");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        for (uint32_t k = 0; k < S; k++)
+            if (shift_src[k] >= J || (uint64_t)shift_amount[k] >= (1ull << nvars)) {
+                set_error("shift %u: source column %u or shift %u out of range", k, shift_src[k], shift_amount[k]);
+                return ZG_ERR_INVALID_PARAM;
+            }
+        const size_t n = (size_t)1 << nvars, L = limbs, fb = 8 * L;
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ZG_CUDA(cudaSetDevice(ctx->device));
+        field_cfg_init(t->f, f.p, (int)limbs);
+        t->has_field = true;
+        // the evaluation point: get_field_challenges(num_vars)
+        for (uint32_t k = 0; k < nvars; k++) {
+            if (L == 3) field_challenge_h<3>(t, f, point_out + k * L);
+            else field_challenge_h<4>(t, f, point_out + k * L);
+        }
+        // extended columns: binary up, binary down, then integer up, integer down
+        std::vector<uint32_t> dbin, dint;  // shift indices by source kind
+        for (uint32_t k = 0; k < S; k++) (shift_src[k] < n_bin ? dbin : dint).push_back(k);
+        const uint32_t nb2 = n_bin + (uint32_t)dbin.size(), ni2 = n_int + (uint32_t)dint.size();
+        ZG_TRY(ctx->piop_arena.ensure(((size_t)nb2 + ni2) * n * 8 + 256));
+        uint64_t *eb = ctx->piop_arena.as<uint64_t>();
+        int64_t *ei = reinterpret_cast<int64_t *>(eb + (size_t)nb2 * n);
+        cudaStream_t s = ctx->stream;
+        const cudaMemcpyKind kind = cols_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if (n_bin) ZG_CUDA(cudaMemcpyAsync(eb, bin_cols, (size_t)n_bin * n * 8, kind, s));
+        if (n_int) ZG_CUDA(cudaMemcpyAsync(ei, int_cols, (size_t)n_int * n * 8, kind, s));
+        auto shifted = [&](void *dst, const void *src_col, size_t c) -> cudaError_t {
+            cudaError_t e = cudaMemcpyAsync(dst, static_cast<const uint8_t *>(src_col) + c * 8, (n - c) * 8, kind, s);
+            if (e == cudaSuccess && c) e = cudaMemsetAsync(static_cast<uint8_t *>(dst) + (n - c) * 8, 0, c * 8, s);
+            return e;
+        };
+        for (size_t q = 0; q < dbin.size(); q++)
+            ZG_CUDA(shifted(eb + (n_bin + q) * n, bin_cols + (size_t)shift_src[dbin[q]] * n, shift_amount[dbin[q]]));
+        for (size_t q = 0; q < dint.size(); q++)
+            ZG_CUDA(shifted(ei + (n_int + q) * n, int_cols + (size_t)(shift_src[dint[q]] - n_bin) * n,
+                            shift_amount[dint[q]]));
+        const PiopCols ext{eb, nb2, D, ei, ni2, nvars};
+        std::vector<uint64_t> vals(((size_t)nb2 * D + ni2) * L);
+        ZG_TRY(L == 3 ? lifted_evals_t<3>(ctx, f, ext, point_out, 1, vals.data())
+                      : lifted_evals_t<4>(ctx, f, ext, point_out, 1, vals.data()));
+        // column value (D coefficients) of column index j in [up (bin, int), down (shift order)]
+        auto column = [&](uint32_t j, uint32_t l) -> const uint64_t * {
+            static const uint64_t zero[4] = {0, 0, 0, 0};
+            if (j < n_bin) return &vals[((size_t)j * D + l) * L];
+            if (j < J) return l == 0 ? &vals[((size_t)nb2 * D + (j - n_bin)) * L] : zero;
+            const uint32_t k = j - J;
+            if (shift_src[k] < n_bin) {
+                const size_t q = std::find(dbin.begin(), dbin.end(), k) - dbin.begin();
+                return &vals[((size_t)(n_bin + q) * D + l) * L];
+            }
+            const size_t q = std::find(dint.begin(), dint.end(), k) - dint.begin();
+            return l == 0 ? &vals[((size_t)nb2 * D + n_int + q) * L] : zero;
+        };
+        for (uint32_t k = 0; k < n_constraints; k++) {
+            uint64_t *out = combined_out + (size_t)k * D * L;
+            std::memset(out, 0, (size_t)D * fb);
+            for (uint32_t j = 0; j < J + S; j++) {
+                const uint64_t *cf = coeffs + ((size_t)k * (J + S) + j) * L;
+                bool nz = false;
+                for (size_t w = 0; w < L; w++) nz |= cf[w] != 0;
+                if (!nz) continue;
+                for (uint32_t l = 0; l < D; l++) {
+                    uint64_t tm[4];
+                    if (L == 3) {
+                        fmul<3>(cf, column(j, l), f.p, f.n0, tm);
+                        fadd<3>(out + (size_t)l * L, tm, f.p);
+                    } else {
+                        fmul<4>(cf, column(j, l), f.p, f.n0, tm);
+                        fadd<4>(out + (size_t)l * L, tm, f.p);
+                    }
+                }
+            }
+            // DynamicPolynomialF::new_trimmed, then absorb_random_field_slice
+            uint32_t len = D;
+            while (len > 0) {
+                bool nz = false;
+                for (size_t w = 0; w < L; w++) nz |= out[(size_t)(len - 1) * L + w] != 0;
+                if (nz) break;
+                len--;
+            }
+            lengths_out[k] = len;
+            for (uint32_t l = 0; l < len; l++) tr_absorb_field(t, out + (size_t)l * L);
+        }
+        return ZG_OK;
+    } catch (const std::exception &e) {
+        set_error("ideal check: %s", e.what());
         return ZG_ERR_OOM;
     }
 }

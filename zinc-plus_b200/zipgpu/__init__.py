@@ -49,7 +49,7 @@ EXPORTS = (
     "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch", "zg_server_create",
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
-    "zg_piop_cpr_linear_prove",
+    "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear",
 )
 
 
@@ -139,6 +139,9 @@ def lib() -> C.CDLL:
                                      C.c_uint32, C.c_int, vp, C.POINTER(sz), vp], st),
         "zg_piop_cpr_linear_prove": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp, vp,
                                       C.c_uint32, C.c_uint32, vp, C.c_int, vp, C.POINTER(sz), vp, vp], st),
+        "zg_piop_ideal_check_linear": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
+                                        C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, C.c_uint32, vp, C.c_int, vp,
+                                        vp, vp], st),
         "zg_params_create": ([vp, C.POINTER(ParamsDesc), C.POINTER(vp)], st),
         "zg_params_destroy": ([vp], st),
         "zg_params_get_info": ([vp, C.POINTER(ParamsInfo)], st),
@@ -887,3 +890,28 @@ class ZincPiop:
                                              _ptr(src), _ptr(amt), len(shifts), cf.shape[0], _ptr(cf), on_dev,
                                              proof, C.byref(cap), _ptr(pt), _ptr(ev)))
         return proof.raw[: cap.value], pt, ev
+
+    @staticmethod
+    def _mont_matrix(coeffs, modulus, limbs):
+        R = 1 << (64 * limbs)
+        return np.array([[[((int(c) % modulus) * R % modulus >> (64 * w)) & ((1 << 64) - 1) for w in range(limbs)]
+                          for c in row] for row in coeffs], np.uint64)
+
+    @staticmethod
+    def ideal_check_linear(ctx: Context, transcript, modulus: int, limbs: int, bin_cols, degree_plus_one: int,
+                           int_cols, nvars: int, shifts, coeffs):
+        """step2 for a linear UAIR: returns (point (nvars, limbs), [combined value
+        per constraint as a (trimmed length, limbs) array])."""
+        b, i = ZincPiop._cols(bin_cols, int_cols, nvars)
+        cf = ZincPiop._mont_matrix(coeffs, modulus, limbs)
+        src = np.array([sc for sc, _ in shifts] or [0], np.uint32)
+        amt = np.array([c for _, c in shifts] or [0], np.uint32)
+        pt = np.zeros((nvars, limbs), np.uint64)
+        comb = np.zeros((cf.shape[0], degree_plus_one, limbs), np.uint64)
+        lens = np.zeros(cf.shape[0], np.uint32)
+        mod = modulus.to_bytes(8 * limbs, "little")
+        check(lib().zg_piop_ideal_check_linear(ctx.handle, transcript.handle, mod, limbs, _ptr(b), b.shape[0],
+                                               degree_plus_one, _ptr(i), i.shape[0], nvars, _ptr(src), _ptr(amt),
+                                               len(shifts), cf.shape[0], _ptr(cf), 0, _ptr(pt), _ptr(comb),
+                                               _ptr(lens)))
+        return pt, [comb[k, : lens[k]] for k in range(cf.shape[0])]
