@@ -869,14 +869,31 @@ def run_piop_steps(Z, ctx, torch, stream, nv, cpu_nv, with_cpu):
         Z.ZincPiop.cpr_linear_prove(ctx, tr, p, L, (mles.data_ptr(), n_bin + n_int), nv, rp, shifts, cons)
         tr.close()
 
+    def step2():
+        tr = Z.PcsProverTranscript()
+        cf = Z.ZincPiop._mont_matrix(cons, p, L)
+        pt2 = np.zeros((nv, L), np.uint64)
+        comb2 = np.zeros((len(cons), D, L), np.uint64)
+        lens = np.zeros(len(cons), np.uint32)
+        src = np.array([sc for sc, _ in shifts], np.uint32)
+        amt = np.array([c for _, c in shifts], np.uint32)
+        Z.check(lib.zg_piop_ideal_check_linear(ctx.handle, tr.handle, mod, L, bd.data_ptr(), n_bin, D,
+                                               id_.data_ptr(), n_int, nv, src.ctypes.data, amt.ctypes.data,
+                                               len(shifts), len(cons), cf.ctypes.data, 1, pt2.ctypes.data,
+                                               comb2.ctypes.data, lens.ctypes.data))
+        tr.close()
+
     ms3, ms6 = timed(step3), timed(step6)
-    ms5, ms4 = timed(step5), timed(step4)
+    ms5, ms4, ms2 = timed(step5), timed(step4), timed(step2)
     cells = (n_bin + n_int) << nv
     res = {"workload": f"BigLinear-shaped trace: {n_bin} BinaryPoly<{D}> + {n_int} integer columns, 2^{nv} rows, "
                        "MontyField<3> (192-bit prime from the transcript); columns resident on the device",
            "eval_projection": {"ms": ms3, "cells_per_s": cells / (ms3 / 1e3),
                                "output_bytes": cells * 8 * L},
            "lifted_evals": {"ms": ms6, "cells_per_s": cells / (ms6 / 1e3)},
+           "ideal_check_linear": {"ms": ms2, "constraints": len(cons),
+                                  "what": "point from the transcript, 17 up and 16 shifted columns evaluated "
+                                          "coefficient-wise, constraints applied, trimmed values absorbed"},
            "cpr_linear": {"ms": ms4, "constraints": len(cons), "mles_in_sumcheck": 2 + n_bin + n_int + len(shifts),
                           "what": "folding challenge, selector, eq and down columns, degree-3 MultiDegreeSumcheck "
                                   "and the absorbed up/down evaluations over step 3's device-resident MLEs"},
