@@ -214,6 +214,14 @@ zg_status zg_prove(zg_params *p, zg_transcript *t, const void *const *polys, uin
                    const uint8_t *point, const zg_hint *hint, uint8_t *eval_out);
 zg_status zg_prove_d(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
                      const uint8_t *point, const zg_hint *hint, uint8_t *eval_out);
+/* ZipPlus::prove_f (phase_prove.rs:119-253): as zg_prove with the point already
+ * in the field (Zinc+ step 7 opens the witness columns at r_0 this way):
+ * point_f is num_vars Montgomery inners of field_limbs u64 each, reduced mod the
+ * transcript's prime.  zg_prove_f_d takes the polynomials in device memory. */
+zg_status zg_prove_f(zg_params *p, zg_transcript *t, const void *const *polys, uint32_t batch,
+                     const uint64_t *point_f, const zg_hint *hint, uint8_t *eval_out);
+zg_status zg_prove_f_d(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
+                       const uint64_t *point_f, const zg_hint *hint, uint8_t *eval_out);
 
 /* Whole-request convenience: commit, new_from_commitment, sample field, prove.
  * Writes root, eval and the proof (proof_len in/out: capacity/size). */

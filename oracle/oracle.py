@@ -109,6 +109,7 @@ def lib():
         L.zr_piop_lifted_evals.argtypes = [vp, u32, vp, u32, u32, vp, u32, u32, vp, vp]
         L.zr_tr_field_challenge.argtypes = [vp, vp, u32, vp]
         L.zr_tr_absorb_field.argtypes = [vp, vp, u32, vp]
+        L.zr_commit_prove_f.argtypes = [C.POINTER(Desc), vp, u32, vp, vp, vp, sz, C.POINTER(C.c_size_t), vp, vp]
         _lib = L
     return _lib
 
@@ -581,3 +582,22 @@ def piop_ideal_check_linear(t: "Transcript", modulus: int, L: int, bin_cols, D: 
             t.absorb_field(p, L, e)
         out.append(arr)
     return point, out
+
+
+def commit_prove_f(desc: Desc, polys: np.ndarray, batch: int, point_u256):
+    """commit + prove_f with the point given as non-negative integers (< 2^256),
+    mapped into the field once the prime is drawn.  Returns (root, proof, eval
+    inner bytes, modulus bytes)."""
+    polys = np.ascontiguousarray(polys)
+    pt = np.array([[(int(v) >> (64 * w)) & ((1 << 64) - 1) for w in range(4)] for v in point_u256], np.uint64)
+    cap = proof_size(desc, batch) + 64
+    proof = C.create_string_buffer(cap)
+    plen = C.c_size_t(0)
+    root = C.create_string_buffer(32)
+    ev = C.create_string_buffer(8 * desc.field_limbs)
+    mod = C.create_string_buffer(8 * desc.field_limbs)
+    rc = lib().zr_commit_prove_f(C.byref(desc), _ptr(polys), batch, _ptr(pt), root, proof, cap, C.byref(plen), ev,
+                                 mod)
+    if rc:
+        raise ValueError(f"commit_prove_f failed ({rc})")
+    return root.raw, proof.raw[: plen.value], ev.raw, mod.raw

@@ -1427,12 +1427,23 @@ static void wmul_i128_add(uint64_t *acc, const uint64_t *x, i128 s, uint32_t C) 
     uadd(acc, prod, C);
 }
 
+/* When set, the next commit_prove takes its point as unsigned 256-bit integers
+ * (4 u64 each) mapped into the field after the prime is drawn: prove_f's point
+ * (phase_prove.rs:119-130) in a form that does not depend on the prime. */
+static const uint64_t *g_point_u256 = NULL;
+
 static void read_prime_and_points(zr_transcript *tr, const zparams *z, const int64_t *point,
                                   fcfg *f, uint64_t *pf) {
     uint64_t prime[4];
     zr_tr_get_prime(tr, z->d.field_limbs, prime);
     fcfg_init(f, prime, z->d.field_limbs);
     for (uint32_t i = 0; i < z->d.num_vars; i++) {
+        if (g_point_u256) {
+            uint64_t x[5] = {g_point_u256[4 * i], g_point_u256[4 * i + 1], g_point_u256[4 * i + 2],
+                             g_point_u256[4 * i + 3], 0};
+            f_from_int(f, x, 5, pf + i * f->L);
+            continue;
+        }
         i128 v = (i128)(((u128)(uint64_t)point[2 * i + 1] << 64) | (uint64_t)point[2 * i]);
         f_from_i128(f, v, pf + i * f->L);
     }
@@ -2145,4 +2156,16 @@ void zr_tr_absorb_field(zr_transcript *t, const uint64_t *modulus, uint32_t L, c
     fcfg f;
     fcfg_init(&f, modulus, L);
     tr_absorb_field(t, &f, inner);
+}
+
+/* commit + prove_f: as zr_commit_prove with the point given as unsigned 256-bit
+ * integers, F::from of each once the field is drawn. */
+int zr_commit_prove_f(const zr_desc *d, const void *polys, uint32_t batch, const uint64_t *point_u256,
+                      uint8_t root[32], uint8_t *proof, size_t proof_cap, size_t *proof_len, uint8_t *eval_out,
+                      uint8_t *modulus_out) {
+    int64_t dummy[2 * 32] = {0};
+    g_point_u256 = point_u256;
+    int rc = zr_commit_prove(d, polys, batch, dummy, root, proof, proof_cap, proof_len, eval_out, modulus_out);
+    g_point_u256 = NULL;
+    return rc;
 }

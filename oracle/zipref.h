@@ -76,6 +76,10 @@ size_t zr_proof_size(const zr_desc *d, uint32_t batch);
 int zr_commit_prove(const zr_desc *d, const void *polys, uint32_t batch, const int64_t *point,
                     uint8_t root[32], uint8_t *proof, size_t proof_cap, size_t *proof_len,
                     uint8_t *eval_out, uint8_t *modulus_out);
+/* The same with prove_f's field-valued point, given as unsigned 256-bit integers. */
+int zr_commit_prove_f(const zr_desc *d, const void *polys, uint32_t batch, const uint64_t *point_u256,
+                      uint8_t root[32], uint8_t *proof, size_t proof_cap, size_t *proof_len, uint8_t *eval_out,
+                      uint8_t *modulus_out);
 int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const int64_t *point,
               const uint8_t *eval_inner, const uint8_t *proof, size_t proof_len);
 

@@ -192,3 +192,43 @@ def test_device_verifier_verdicts_match_oracle(zipgpu, oracle, ctx, rng, case):
     ek, D, ck, nv, L = case
     pp = params_for(zipgpu, ek, D, ck, nv, L, ctx=ctx)
     verdicts_match_oracle(zipgpu, oracle, pp, desc_for(ek, D, ck, nv, L), ek, D, nv, rng, cases=24)
+
+
+@pytest.mark.parametrize("case", [(1, 32, 0, 12, 1024, 1), (1, 64, 0, 10, 256, 2), (0, 1, 0, 10, 256, 1)])
+def test_prove_f_matches_oracle_and_prove(zipgpu, oracle, ctx, rng, case):
+    """ZipPlus::prove_f (phase_prove.rs:119-253) at a field point: the oracle's
+    proof and evaluation for the same field elements, and zg_prove's bytes when
+    the field point is the image of an i128 point (prove maps the point and calls
+    prove_f)."""
+    ek, D, ck, nv, L, batch = case
+    pp = params_for(zipgpu, ek, D, ck, nv, L, ctx=ctx)
+    polys = [_evals(rng, ek, D, 1 << nv) for _ in range(batch)]
+    desc = desc_for(ek, D, ck, nv, L)
+    hint, comm = zipgpu.ZipPlus.commit(pp, polys)
+    limbs = 4
+    u = [int.from_bytes(rng.bytes(32), "little") for _ in range(nv)]
+
+    def field_point(t, values):
+        prime = t.get_random_field_cfg(limbs)
+        R = 1 << (64 * limbs)
+        return np.array([[((v % prime) * R % prime >> (64 * w)) & ((1 << 64) - 1) for w in range(limbs)]
+                         for v in values], np.uint64)
+
+    t = zipgpu.PcsProverTranscript.new_from_commitment(comm)
+    ev = zipgpu.ZipPlus.prove_f(t, pp, polys, field_point(t, u), hint)
+    root_o, proof_o, ev_o, _ = oracle.commit_prove_f(desc, np.concatenate(polys), batch, u)
+    assert comm.root == root_o and ev == ev_o and t.stream == proof_o
+    # an i128 point through prove and its field image through prove_f
+    point = [(-1) ** i * (7 * i + 2) for i in range(nv)]
+    t1 = zipgpu.PcsProverTranscript.new_from_commitment(comm)
+    t1.get_random_field_cfg(limbs)
+    ev1 = zipgpu.ZipPlus.prove(t1, pp, polys, point, hint)
+    t2 = zipgpu.PcsProverTranscript.new_from_commitment(comm)
+    ev2 = zipgpu.ZipPlus.prove_f(t2, pp, polys, field_point(t2, point), hint)
+    assert ev1 == ev2 and t1.stream == t2.stream
+    # a coordinate that is not reduced mod the prime is rejected
+    t3 = zipgpu.PcsProverTranscript.new_from_commitment(comm)
+    pf = field_point(t3, u)
+    pf[0] = np.iinfo(np.uint64).max
+    with pytest.raises(zipgpu.ZipError):
+        zipgpu.ZipPlus.prove_f(t3, pp, polys, pf, hint)

@@ -414,7 +414,7 @@ zg_status commit_group_device(zg_params *p, zg_ctx *lane, const void *polys_d, u
 // -------------------------------------------------------------------- prove
 zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void *polys_d,
                        uint32_t batch, const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
-                       uint8_t *tail_out) {
+                       uint8_t *tail_out, bool point_is_field) {
     if (!t->has_field || t->f.L != (int)p->d.field_limbs) {
         set_error("transcript has no field configuration of %u limbs (sample it first)",
                   p->d.field_limbs);
@@ -438,7 +438,22 @@ zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void 
     // point -> F, q0 (host), q1 (device) (point_to_tensor, pcs/utils.rs:90-114)
     std::vector<uint64_t> pf((size_t)(nv + 1) * L), omr((size_t)(nv + 1) * L);
     for (uint32_t i = 0; i < nv; i++) {
-        f_from_i128(f, load_i128(point + 16 * i), &pf[(size_t)i * L]);
+        if (point_is_field) {
+            // prove_f (phase_prove.rs:119-130): the point is already in the field
+            std::memcpy(&pf[(size_t)i * L], point + (size_t)8 * L * i, 8 * L);
+            bool below = false;
+            for (int w = L - 1; w >= 0; w--)
+                if (pf[(size_t)i * L + w] != f.p[w]) {
+                    below = pf[(size_t)i * L + w] < f.p[w];
+                    break;
+                }
+            if (!below) {
+                set_error("point coordinate %u is not a reduced field element", i);
+                return ZG_ERR_INVALID_PARAM;
+            }
+        } else {
+            f_from_i128(f, load_i128(point + 16 * i), &pf[(size_t)i * L]);
+        }
         std::memcpy(&omr[(size_t)i * L], f.one, 8 * L);
         f_sub(f, &omr[(size_t)i * L], &pf[(size_t)i * L]);
     }
@@ -1357,6 +1372,35 @@ static zg_status prove_impl(zg_params *p, zg_transcript *t, const void *const *p
 zg_status zg_prove(zg_params *p, zg_transcript *t, const void *const *polys, uint32_t batch,
                    const uint8_t *point, const zg_hint *hint, uint8_t *eval_out) {
     ZG_GUARD(prove_impl(p, t, polys, batch, point, hint, eval_out));
+}
+
+static zg_status prove_f_impl(zg_params *p, zg_transcript *t, const void *polys, uint32_t batch,
+                              const uint64_t *point_f, const zg_hint *hint, uint8_t *eval_out, bool on_device) {
+    if (!p || !t || !point_f || !polys) return ZG_ERR_INVALID_PARAM;
+    ZG_TRY(need_device(p));
+    std::lock_guard<std::mutex> lk(p->ctx->mu);
+    ZG_CUDA(cudaSetDevice(p->ctx->device));
+    if (batch == 0) {
+        set_error("Batch must contain at least one polynomial");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    const void *d = polys;
+    if (!on_device) {
+        ZG_TRY(stage_polys(p, p->ctx, static_cast<const void *const *>(polys), batch));
+        d = p->ctx->evals.ptr;
+    }
+    return prove_device(p, p->ctx, t, d, batch, reinterpret_cast<const uint8_t *>(point_f), hint, eval_out, nullptr,
+                        true);
+}
+
+zg_status zg_prove_f(zg_params *p, zg_transcript *t, const void *const *polys, uint32_t batch,
+                     const uint64_t *point_f, const zg_hint *hint, uint8_t *eval_out) {
+    ZG_GUARD(prove_f_impl(p, t, polys, batch, point_f, hint, eval_out, false));
+}
+
+zg_status zg_prove_f_d(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,
+                       const uint64_t *point_f, const zg_hint *hint, uint8_t *eval_out) {
+    ZG_GUARD(prove_f_impl(p, t, polys_d, batch, point_f, hint, eval_out, true));
 }
 
 static zg_status prove_d_impl(zg_params *p, zg_transcript *t, const void *polys_d, uint32_t batch,

@@ -304,9 +304,11 @@ zg_status launch_commit_group(zg_params *p, zg_ctx *lane, const void *polys_d, u
 // drop the hints) and roots (m x 32, host).
 zg_status commit_group_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t m,
                               zg_hint **hints, uint8_t *roots, const CommitTuning &tune);
+// point: num_vars i128 coordinates (prove), or with point_is_field num_vars
+// Montgomery inners of field_limbs u64 each (prove_f).
 zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void *polys_d,
                        uint32_t batch, const uint8_t *point, const zg_hint *hint, uint8_t *eval_out,
-                       uint8_t *tail_out);
+                       uint8_t *tail_out, bool point_is_field = false);
 zg_status verify_host(zg_params *p, const uint8_t root[32], uint32_t batch, const uint8_t *point,
                       const uint8_t *eval, const uint8_t *proof, size_t proof_len);
 

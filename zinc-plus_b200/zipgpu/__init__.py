@@ -49,7 +49,7 @@ EXPORTS = (
     "zg_sumcheck_prove", "zg_mle_evaluate", "zg_commit_batch", "zg_server_create",
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
-    "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear",
+    "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear", "zg_prove_f", "zg_prove_f_d",
 )
 
 
@@ -131,6 +131,8 @@ def lib() -> C.CDLL:
         "zg_ctx_set_kernel_timing": ([vp, C.c_int], st),
         "zg_ctx_kernel_timing_report": ([vp, C.c_char_p, sz, C.POINTER(sz)], st),
         "zg_selftest_bounded_wait": ([vp, C.POINTER(C.c_uint32)], st),
+        "zg_prove_f": ([vp, vp, vp, C.c_uint32, vp, vp, vp], st),
+        "zg_prove_f_d": ([vp, vp, vp, C.c_uint32, vp, vp, vp], st),
         "zg_piop_eval_projection": ([vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
                                      C.c_uint32, C.c_uint32, vp, C.c_int, vp], st),
         "zg_piop_lifted_evals": ([vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
@@ -556,6 +558,16 @@ class ZipPlus:
         ev = C.create_string_buffer(8 * pp.zt.field_limbs)
         check(lib().zg_prove(pp.handle, transcript.handle, ptrs, len(polys), C.c_char_p(pt),
                              hint.handle, ev))
+        return ev.raw
+
+    @staticmethod
+    def prove_f(transcript: PcsProverTranscript, pp: ZipPlusParams, polys, point_f, hint: ZipPlusHint) -> bytes:
+        """ZipPlus::prove_f: point_f is (num_vars, field_limbs) Montgomery inners
+        under the transcript's prime.  Returns the evaluation's inner bytes."""
+        _keep, ptrs = _poly_ptrs(pp, polys)
+        pf = np.ascontiguousarray(point_f, dtype=np.uint64)
+        ev = C.create_string_buffer(8 * pp.zt.field_limbs)
+        check(lib().zg_prove_f(pp.handle, transcript.handle, ptrs, len(polys), _ptr(pf), hint.handle, ev))
         return ev.raw
 
     @staticmethod
