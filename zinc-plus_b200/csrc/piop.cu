@@ -13,7 +13,6 @@
 //                  coefficient is sum_b eq(b, r0) F(c[b]).  Per-block partial sums,
 //                  then k_lifted_reduce.
 // Field elements are Montgomery inners (F::Inner of MontyField) of 3 or 4 limbs.
-#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -922,18 +921,18 @@ extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, c
         std::vector<uint64_t> vals(((size_t)nb2 * D + ni2) * L);
         ZG_TRY(L == 3 ? lifted_evals_t<3>(ctx, f, ext, point_out, 1, vals.data())
                       : lifted_evals_t<4>(ctx, f, ext, point_out, 1, vals.data()));
+        // position of shift k among the extended binary (or integer) columns
+        std::vector<uint32_t> ext_pos(S);
+        for (size_t q = 0; q < dbin.size(); q++) ext_pos[dbin[q]] = n_bin + (uint32_t)q;
+        for (size_t q = 0; q < dint.size(); q++) ext_pos[dint[q]] = n_int + (uint32_t)q;
         // column value (D coefficients) of column index j in [up (bin, int), down (shift order)]
+        static const uint64_t zero[4] = {0, 0, 0, 0};
         auto column = [&](uint32_t j, uint32_t l) -> const uint64_t * {
-            static const uint64_t zero[4] = {0, 0, 0, 0};
             if (j < n_bin) return &vals[((size_t)j * D + l) * L];
             if (j < J) return l == 0 ? &vals[((size_t)nb2 * D + (j - n_bin)) * L] : zero;
             const uint32_t k = j - J;
-            if (shift_src[k] < n_bin) {
-                const size_t q = std::find(dbin.begin(), dbin.end(), k) - dbin.begin();
-                return &vals[((size_t)(n_bin + q) * D + l) * L];
-            }
-            const size_t q = std::find(dint.begin(), dint.end(), k) - dint.begin();
-            return l == 0 ? &vals[((size_t)nb2 * D + n_int + q) * L] : zero;
+            if (shift_src[k] < n_bin) return &vals[((size_t)ext_pos[k] * D + l) * L];
+            return l == 0 ? &vals[((size_t)nb2 * D + ext_pos[k]) * L] : zero;
         };
         for (uint32_t k = 0; k < n_constraints; k++) {
             uint64_t *out = combined_out + (size_t)k * D * L;
