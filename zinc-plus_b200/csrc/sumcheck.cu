@@ -110,7 +110,7 @@ __device__ __forceinline__ void load_el(const uint64_t *p, uint64_t (&v)[L]) {
 // each folds every kScSub-th MLE and evaluates every kScSub-th product, their
 // sums of products are combined by shuffles, and the first applies the factors.
 template <int L, int D, int kScSub>
-__global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restrict__ src,
+__global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__restrict__ src,
                                                          size_t src_len, uint64_t *__restrict__ dst,
                                                          int fold, const uint64_t *__restrict__ r,
                                                          uint32_t K, ScComb c, FieldCfg f,
@@ -150,11 +150,30 @@ __global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restr
     __syncwarp();  // the pair's folded MLEs, written by its kScSub threads, are visible
     const uint64_t *m = fold ? dst : src;
     if (active) {
-        // this thread's share of the sum of products at t = 0..D
+        // this thread's share of the sum of products at t = 0..D.  Products of
+        // one MLE are linear in t: their sum is kept at t = 0 and t = 1 only
+        // (lin0, lin1) and extended to t = 2..D at the end (exact field values).
+        uint64_t lin0[L], lin1[L];
+#pragma unroll
+        for (int w = 0; w < L; w++) lin0[w] = lin1[w] = 0;
+        bool any_lin = false;
         for (uint32_t k = sub; k < c.n_products; k += kScSub) {
             uint64_t pr[D + 1][L];
             uint64_t cf[L];
             load_el<L>(c.coeffs + (size_t)k * L, cf);
+            // (degrees 2..6: at 1 it saves nothing, above 6 its registers spill)
+            if (D >= 2 && D <= 6 && c.offsets[k + 1] - c.offsets[k] == 1) {
+                const uint64_t *v = m + ((size_t)c.indices[c.offsets[k]] * len + 2 * b) * L;
+                uint64_t v0[L], v1[L], o[L];
+                load_el<L>(v, v0);
+                load_el<L>(v + L, v1);
+                fmul_c<L, (kScSub == kScSubMax)>(cf, v0, pf, f.n0, o);
+                fadd<L>(lin0, o, f.p);
+                fmul_c<L, (kScSub == kScSubMax)>(cf, v1, pf, f.n0, o);
+                fadd<L>(lin1, o, f.p);
+                any_lin = true;
+                continue;
+            }
 #pragma unroll
             for (int t = 0; t <= D; t++)
 #pragma unroll
@@ -176,6 +195,21 @@ __global__ void __launch_bounds__(kScThreads) k_sc_round(const uint64_t *__restr
             }
 #pragma unroll
             for (int t = 0; t <= D; t++) fadd<L>(ev[t], pr[t], f.p);
+        }
+        if (D >= 2 && D <= 6 && any_lin) {
+            uint64_t d[L], cur[L];
+#pragma unroll
+            for (int w = 0; w < L; w++) {
+                d[w] = lin1[w];
+                cur[w] = lin1[w];
+            }
+            fsub<L>(d, lin0, f.p);
+            fadd<L>(ev[0], lin0, f.p);
+#pragma unroll
+            for (int t = 1; t <= D; t++) {
+                if (t > 1) fadd<L>(cur, d, f.p);
+                fadd<L>(ev[t], cur, f.p);
+            }
         }
     }
     // the pair's full sum of products, in all its threads
