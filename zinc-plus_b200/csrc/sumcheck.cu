@@ -223,7 +223,40 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
             fadd<L>(ev[t], o, f.p);
         }
     }
-    if (sub != 0) {
+    if (kScSub > D) {
+        // affine factors a + b * v, one evaluation point per thread of the pair:
+        // thread `sub` <= D multiplies the pair's sum at t = sub by the factors
+        // there and keeps only that entry (all threads hold the full sums)
+        uint64_t keep[L];
+#pragma unroll
+        for (int w = 0; w < L; w++) keep[w] = 0;
+        if (active && (int)sub <= D) {
+#pragma unroll
+            for (int t = 0; t <= D; t++)
+                if (t == (int)sub)
+#pragma unroll
+                    for (int w = 0; w < L; w++) keep[w] = ev[t][w];
+            for (uint32_t q = 0; q < c.n_factors; q++) {
+                uint64_t cur[L], st[L], fa[L], fbv[L], fv[L], o[L];
+                const uint64_t *v = m + ((size_t)c.fmles[q] * len + 2 * b) * L;
+                load_el<L>(v, cur);
+                load_el<L>(v + L, st);
+                fsub<L>(st, cur, f.p);
+                for (uint32_t i = 0; i < sub; i++) fadd<L>(cur, st, f.p);  // v(sub)
+                load_el<L>(c.fa + (size_t)q * L, fa);
+                load_el<L>(c.fb + (size_t)q * L, fbv);
+                fmul_c<L, (kScSub == kScSubMax)>(fbv, cur, pf, f.n0, fv);
+                fadd<L>(fv, fa, f.p);
+                fmul_c<L, (kScSub == kScSubMax)>(keep, fv, pf, f.n0, o);
+#pragma unroll
+                for (int w = 0; w < L; w++) keep[w] = o[w];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t <= D; t++)
+#pragma unroll
+            for (int w = 0; w < L; w++) ev[t][w] = t == (int)sub ? keep[w] : 0;
+    } else if (sub != 0) {
 #pragma unroll
         for (int t = 0; t <= D; t++)
 #pragma unroll
