@@ -389,6 +389,10 @@ zg_status zg_sumcheck_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulu
 zg_status zg_mle_evaluate(zg_ctx *ctx, const uint8_t *modulus, uint32_t limbs, const uint64_t *mle,
                           uint32_t nvars, const uint64_t *point, uint64_t *out);
 
+/* ---- Zinc+ prover steps on the trace columns ----------------------------------
+ * The step functions below keep their intermediate MLEs in the context's
+ * arenas between phases (steps 4 and 5 prepare them, then run the sumcheck):
+ * run one of them at a time per context. */
 /* ---- Zinc+ prover steps 3 and 6 on the trace columns -------------------------
  * (protocol/src/prover.rs:385-415 step3_eval_projection and 497-532
  * step6_lift_and_project.)  Columns: n_bin binary-polynomial columns of
