@@ -28,12 +28,14 @@
  *    zg_hint_free.  "_d" entry points take device pointers and a cudaStream_t
  *    passed as void*.
  *  - Evaluations: ZG_EVAL_I32 is one int32 per evaluation (Zip, Eval = i32);
+ *    ZG_EVAL_I64 is one int64 per evaluation (the integer trace columns of
+ *    Zinc+, IntZt of protocol/benches/e2e.rs:215-227: Eval = i64, Cw = i128);
  *    ZG_EVAL_BINPOLY is one uint64 per evaluation holding the {0,1}
  *    coefficients of a BinaryPoly<D> (bit i = coefficient of X^i, bits >= D
  *    must be zero), as the reference's `simd` feature stores it
  *    (poly/src/univariate/binary_u64.rs:28).
  *  - Codewords are laid out like the reference's DenseRowMatrix (row-major
- *    num_rows x codeword_len) when copied to the host; Cw is i128 (I32 evals),
+ *    num_rows x codeword_len) when copied to the host; Cw is i128 (I32, I64 evals),
  *    DensePolynomial<i64, D> (BINPOLY + IPRS) or DensePolynomial<i32, D>
  *    (BINPOLY + RAA), little-endian, coefficient 0 first.
  *  - Field elements (MontyField<field_limbs>) are exchanged as their
@@ -65,7 +67,7 @@ typedef enum {
     ZG_ERR_BUFFER_TOO_SMALL = 9 /* caller buffer shorter than required         */
 } zg_status;
 
-typedef enum { ZG_EVAL_I32 = 0, ZG_EVAL_BINPOLY = 1 } zg_eval_kind;
+typedef enum { ZG_EVAL_I32 = 0, ZG_EVAL_BINPOLY = 1, ZG_EVAL_I64 = 2 } zg_eval_kind;
 /* ZG_CODE_RAA_SIGN_FLIP: RaaSignFlippingCode (zip-plus/src/code/raa_sign_flip.rs:
  * 14-69), the RAA code with entries 1, 3, 5, ... negated after the repetition
  * and after the first accumulation; same permutations and width check. */

@@ -15,7 +15,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libzipref.so")
 
-EVAL_I32, EVAL_BINPOLY = 0, 1
+EVAL_I32, EVAL_BINPOLY, EVAL_I64 = 0, 1, 2
 CODE_IPRS, CODE_RAA, CODE_RAA_SIGN_FLIP = 0, 1, 2
 
 
@@ -125,7 +125,7 @@ def _buf(b: bytes):
 def make_desc(eval_kind, D, code_kind, num_vars, row_len, depth=0, comb_limbs=None,
               field_limbs=4, num_openings=147, rep=4) -> Desc:
     if comb_limbs is None:
-        comb_limbs = 3 if eval_kind == EVAL_I32 else 5
+        comb_limbs = {EVAL_I32: 3, EVAL_I64: 6}.get(eval_kind, 5)
     return Desc(eval_kind, D if eval_kind == EVAL_BINPOLY else 1, code_kind, rep, num_vars,
                 row_len, depth, comb_limbs, field_limbs, num_openings)
 

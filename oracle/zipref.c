@@ -607,6 +607,9 @@ static void pntt_stages_wide(const iprs_params *p, uint64_t *out, uint32_t lanes
     free(xs);
 }
 
+/* Radix-8 stages on i128 values (MulByScalar i128 x i64, mul_by_scalar.rs:97-108). */
+static void pntt_stages_i128(const iprs_params *p, i128 *out);
+
 /* Scalar Zip: Eval i32 -> Cw i128 (mul_by_scalar.rs:89-108). */
 static void pntt_i32(const iprs_params *p, const int32_t *in, i128 *out) {
     uint32_t sh = 3 * p->depth;
@@ -618,6 +621,26 @@ static void pntt_i32(const iprs_params *p, const int32_t *in, i128 *out) {
         for (size_t c = 1; c < p->base_len; c++) acc += (i128)in[oct | (c << sh)] * bm[c];
         out[i] = acc;
     }
+    pntt_stages_i128(p, out);
+}
+
+/* Int column Zip (IntZt of protocol/benches/e2e.rs:215-227): Eval i64 -> Cw
+ * i128, i64 x i64 widened to i128 (mul_by_scalar.rs:110-116), the base sum in
+ * i128 (|sum| < 2^63 * 2^16 * base_len), the stages as for i32. */
+static void pntt_i64(const iprs_params *p, const int64_t *in, i128 *out) {
+    uint32_t sh = 3 * p->depth;
+    for (size_t i = 0; i < p->codeword_len; i++) {
+        size_t chunk = i >> p->base_dim_log2, row = i & (p->base_dim - 1);
+        size_t oct = zr_octet_reversal(chunk, p->depth);
+        const int64_t *bm = p->bm + row * p->base_len;
+        i128 acc = in[oct];
+        for (size_t c = 1; c < p->base_len; c++) acc += (i128)in[oct | (c << sh)] * bm[c];
+        out[i] = acc;
+    }
+    pntt_stages_i128(p, out);
+}
+
+static void pntt_stages_i128(const iprs_params *p, i128 *out) {
     i128 xs[8];
     for (uint32_t k = 0; k < p->depth; k++) {
         size_t sub = (size_t)p->base_dim << (3 * k);
@@ -797,9 +820,10 @@ static int zparams_build(const zr_desc *d, zparams *z) {
     if (poly % d->row_len) return -1;
     z->num_rows = (uint32_t)(poly / d->row_len);
     z->row_len = d->row_len;
+    if (d->eval_kind > ZR_EVAL_I64) return -1;
     z->D = d->eval_kind == ZR_EVAL_BINPOLY ? d->degree_plus_one : 1;
     if (d->eval_kind == ZR_EVAL_BINPOLY && (z->D == 0 || z->D > 64)) return -1;
-    z->eval_bytes = d->eval_kind == ZR_EVAL_BINPOLY ? 8 : 4;
+    z->eval_bytes = d->eval_kind == ZR_EVAL_I32 ? 4 : 8;
     if (d->field_limbs < 1 || d->field_limbs > 4 || d->comb_limbs < 1 || d->comb_limbs > 8) return -1;
     if (d->code_kind == ZR_CODE_IPRS) {
         uint32_t depth = d->iprs_depth ? d->iprs_depth : iprs_optimal_depth(d->row_len);
@@ -828,7 +852,7 @@ size_t zr_cw_bytes(const zr_desc *d) {
     zparams_free(&z);
     return r;
 }
-size_t zr_eval_bytes(const zr_desc *d) { return d->eval_kind == ZR_EVAL_BINPOLY ? 8 : 4; }
+size_t zr_eval_bytes(const zr_desc *d) { return d->eval_kind == ZR_EVAL_I32 ? 4 : 8; }
 uint32_t zr_num_rows(const zr_desc *d) {
     zparams z;
     if (zparams_build(d, &z)) return 0;
@@ -848,6 +872,7 @@ uint32_t zr_codeword_len(const zr_desc *d) {
 static void encode_row(const zparams *z, const void *row, void *cw) {
     if (z->d.code_kind == ZR_CODE_IPRS) {
         if (z->d.eval_kind == ZR_EVAL_I32) pntt_i32(&z->iprs, (const int32_t *)row, (i128 *)cw);
+        else if (z->d.eval_kind == ZR_EVAL_I64) pntt_i64(&z->iprs, (const int64_t *)row, (i128 *)cw);
         else pntt_binary(&z->iprs, (const uint64_t *)row, z->D, (int64_t *)cw);
     } else {
         raa_binary(&z->raa, (const uint64_t *)row, z->D, (int32_t *)cw);
@@ -1281,7 +1306,7 @@ static int validate_bits(const zparams *z, uint32_t batch) {
     uint32_t dd = d < 1 ? 1 : d, ld = 0;
     while ((1u << ld) < dd) ld++;
     uint32_t chal = 128 * (z->D > 1 ? 2 : 1);
-    uint32_t eval_bits = z->d.eval_kind == ZR_EVAL_BINPOLY ? 1 : 32;
+    uint32_t eval_bits = z->d.eval_kind == ZR_EVAL_BINPOLY ? 1 : z->d.eval_kind == ZR_EVAL_I64 ? 64 : 32;
     uint32_t lb = 0;
     while ((1u << lb) < batch) lb++;
     uint32_t actual = 2 * cwb + ld + chal + (eval_bits - 1) + lb;
@@ -1377,13 +1402,18 @@ static void alpha_project(const zparams *z, const uint8_t *evals, size_t n, cons
 #pragma omp parallel for schedule(static) num_threads(nt)
     for (long i = 0; i < (long)n; i++) {
         uint64_t *o = out + (size_t)i * C;
-        if (z->d.eval_kind == ZR_EVAL_I32) {
-            int32_t v;
-            memcpy(&v, evals + 4 * i, 4);
+        if (z->d.eval_kind != ZR_EVAL_BINPOLY) {
+            int64_t v;
+            if (z->d.eval_kind == ZR_EVAL_I64) memcpy(&v, evals + 8 * i, 8);
+            else {
+                int32_t v32;
+                memcpy(&v32, evals + 4 * i, 4);
+                v = v32;
+            }
             /* ScalarProduct with alphas == [1] */
             uint64_t x[8];
             uint64_t sgn = v < 0 ? ~0ull : 0;
-            x[0] = (uint64_t)(int64_t)v;
+            x[0] = (uint64_t)v;
             for (uint32_t k = 1; k < C; k++) x[k] = sgn;
             memset(o, 0, 8 * C);
             wl_mul_i64_add(o, x, (int64_t)alphas[0], C);
@@ -1460,6 +1490,94 @@ static void point_tensor(const fcfg *f, const zparams *z, const uint64_t *pf, ui
     else memcpy(q1, f->one, 8 * L);
 }
 
+/* The prove phase after the point is in the field (phase_prove.rs:132-304):
+ * alphas, b, eval, coefficients, combined row and openings on `tr`, proof
+ * bytes appended to w. */
+static void prove_core(const zparams *z, const uint8_t *polys, uint32_t batch, const zhint *h, zr_transcript *tr,
+                       const fcfg *f, const uint64_t *pf, wbuf *w, uint8_t *eval_out) {
+    uint32_t L = z->d.field_limbs, C = z->d.comb_limbs, R = z->num_rows, RL = z->row_len;
+    uint64_t *q0 = (uint64_t *)malloc(8 * L * (size_t)R), *q1 = (uint64_t *)malloc(8 * L * (size_t)RL);
+    point_tensor(f, z, pf, q0, q1);
+
+    size_t N = (size_t)R * RL, polyev = N * z->eval_bytes;
+    uint64_t *wp = (uint64_t *)malloc(sizeof(uint64_t) * C * N * batch);
+    i128 alphas[64];
+    for (uint32_t b = 0; b < batch; b++) {
+        uint32_t na = z->D > 1 ? z->D : 1;
+        if (z->D > 1)
+            for (uint32_t i = 0; i < na; i++) alphas[i] = tr_i128(tr);
+        else alphas[0] = 1;
+        alpha_project(z, polys + b * polyev, N, alphas, wp + (size_t)b * N * C);
+    }
+    /* b[j] = sum_poly <F(w'_j), q1> (phase_prove.rs:179-193) */
+    uint64_t *bv = (uint64_t *)calloc((size_t)R, 8 * L);
+    int nt = zr_get_threads();
+    (void)nt;
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (long j = 0; j < (long)R; j++) {
+        uint64_t acc[4] = {0};
+        for (uint32_t b = 0; b < batch; b++) {
+            const uint64_t *row = wp + ((size_t)b * N + (size_t)j * RL) * C;
+            for (uint32_t c = 0; c < RL; c++) {
+                uint64_t fe[4], t[4];
+                f_from_int(f, row + (size_t)c * C, C, fe);
+                fmul(f, fe, q1 + (size_t)c * L, t);
+                fadd(f, acc, t);
+            }
+        }
+        memcpy(bv + j * L, acc, 8 * L);
+    }
+    /* write_field_elements (pcs_transcript.rs:99-142), LENGTH_NUM_BYTES = 0 */
+    for (uint32_t j = 0; j < R; j++) {
+        tr_absorb_field(tr, f, bv + (size_t)j * L);
+        wput(w, f->p, 8 * L);
+        wput(w, bv + (size_t)j * L, 8 * L);
+    }
+    uint64_t ev[4] = {0};
+    for (uint32_t j = 0; j < R; j++) {
+        uint64_t t[4];
+        fmul(f, q0 + (size_t)j * L, bv + (size_t)j * L, t);
+        fadd(f, ev, t);
+    }
+    i128 *coeffs = (i128 *)malloc(sizeof(i128) * R);
+    if (R == 1) coeffs[0] = 1;
+    else
+        for (uint32_t j = 0; j < R; j++) coeffs[j] = tr_i128(tr);
+    /* combined_row (phase_prove.rs:205-244) */
+    uint64_t *comb = (uint64_t *)calloc((size_t)RL, 8 * C);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (long c = 0; c < (long)RL; c++) {
+        uint64_t *acc = comb + (size_t)c * C;
+        for (uint32_t b = 0; b < batch; b++)
+            for (uint32_t j = 0; j < R; j++)
+                wmul_i128_add(acc, wp + ((size_t)b * N + (size_t)j * RL + c) * C, coeffs[j], C);
+    }
+    wput(w, comb, (size_t)RL * 8 * C);
+    /* openings (phase_prove.rs:285-304, pcs_transcript.rs:210-221) */
+    size_t rowbytes = (size_t)z->codeword_len * z->cw_bytes;
+    uint64_t depth = h->tree.n_layers - 1;
+    for (uint32_t o = 0; o < z->d.num_openings; o++) {
+        uint32_t idx = tr_u32(tr) % z->codeword_len;
+        for (uint32_t r = 0; r < R * batch; r++) wput(w, h->cw + (size_t)r * rowbytes + (size_t)idx * z->cw_bytes, z->cw_bytes);
+        uint64_t li = idx, lc = z->codeword_len;
+        wput(w, &li, 8);
+        wput(w, &lc, 8);
+        wput(w, &depth, 8);
+        uint64_t cur = idx;
+        for (uint32_t k = 0; k < depth; k++) {
+            wput(w, h->tree.layers[k] + 32 * (cur ^ 1), 32);
+            cur >>= 1;
+        }
+    }
+    if (eval_out) memcpy(eval_out, ev, 8 * L);
+    free(comb);
+    free(coeffs);
+    free(bv);
+    free(wp);
+    free(q0);
+    free(q1);
+}
+
 int zr_commit_prove(const zr_desc *d, const void *polys_v, uint32_t batch, const int64_t *point,
                     uint8_t root[32], uint8_t *proof, size_t proof_cap, size_t *proof_len,
                     uint8_t *eval_out, uint8_t *modulus_out) {
@@ -1480,94 +1598,43 @@ int zr_commit_prove(const zr_desc *d, const void *polys_v, uint32_t batch, const
     zr_transcript *tr = zr_tr_new();
     zr_tr_absorb_slice(tr, root, 32);
     fcfg f;
-    uint32_t L = d->field_limbs, C = d->comb_limbs, R = z.num_rows, RL = z.row_len;
+    uint32_t L = d->field_limbs;
     uint64_t *pf = (uint64_t *)calloc((size_t)d->num_vars + 1, 8 * L);
     read_prime_and_points(tr, &z, point, &f, pf);
-    uint64_t *q0 = (uint64_t *)malloc(8 * L * (size_t)R), *q1 = (uint64_t *)malloc(8 * L * (size_t)RL);
-    point_tensor(&f, &z, pf, q0, q1);
-
     wbuf w = {proof, 0, proof_cap, 0};
-    size_t N = (size_t)R * RL, polyev = N * z.eval_bytes;
-    uint64_t *wp = (uint64_t *)malloc(sizeof(uint64_t) * C * N * batch);
-    i128 alphas[64];
-    for (uint32_t b = 0; b < batch; b++) {
-        uint32_t na = z.D > 1 ? z.D : 1;
-        if (z.D > 1)
-            for (uint32_t i = 0; i < na; i++) alphas[i] = tr_i128(tr);
-        else alphas[0] = 1;
-        alpha_project(&z, polys + b * polyev, N, alphas, wp + (size_t)b * N * C);
-    }
-    /* b[j] = sum_poly <F(w'_j), q1> (phase_prove.rs:179-193) */
-    uint64_t *bv = (uint64_t *)calloc((size_t)R, 8 * L);
-    int nt = zr_get_threads();
-    (void)nt;
-#pragma omp parallel for schedule(static) num_threads(nt)
-    for (long j = 0; j < (long)R; j++) {
-        uint64_t acc[4] = {0};
-        for (uint32_t b = 0; b < batch; b++) {
-            const uint64_t *row = wp + ((size_t)b * N + (size_t)j * RL) * C;
-            for (uint32_t c = 0; c < RL; c++) {
-                uint64_t fe[4], t[4];
-                f_from_int(&f, row + (size_t)c * C, C, fe);
-                fmul(&f, fe, q1 + (size_t)c * L, t);
-                fadd(&f, acc, t);
-            }
-        }
-        memcpy(bv + j * L, acc, 8 * L);
-    }
-    /* write_field_elements (pcs_transcript.rs:99-142), LENGTH_NUM_BYTES = 0 */
-    for (uint32_t j = 0; j < R; j++) {
-        tr_absorb_field(tr, &f, bv + (size_t)j * L);
-        wput(&w, f.p, 8 * L);
-        wput(&w, bv + (size_t)j * L, 8 * L);
-    }
-    uint64_t ev[4] = {0};
-    for (uint32_t j = 0; j < R; j++) {
-        uint64_t t[4];
-        fmul(&f, q0 + (size_t)j * L, bv + (size_t)j * L, t);
-        fadd(&f, ev, t);
-    }
-    i128 *coeffs = (i128 *)malloc(sizeof(i128) * R);
-    if (R == 1) coeffs[0] = 1;
-    else
-        for (uint32_t j = 0; j < R; j++) coeffs[j] = tr_i128(tr);
-    /* combined_row (phase_prove.rs:205-244) */
-    uint64_t *comb = (uint64_t *)calloc((size_t)RL, 8 * C);
-#pragma omp parallel for schedule(static) num_threads(nt)
-    for (long c = 0; c < (long)RL; c++) {
-        uint64_t *acc = comb + (size_t)c * C;
-        for (uint32_t b = 0; b < batch; b++)
-            for (uint32_t j = 0; j < R; j++)
-                wmul_i128_add(acc, wp + ((size_t)b * N + (size_t)j * RL + c) * C, coeffs[j], C);
-    }
-    wput(&w, comb, (size_t)RL * 8 * C);
-    /* openings (phase_prove.rs:285-304, pcs_transcript.rs:210-221) */
-    size_t rowbytes = (size_t)z.codeword_len * z.cw_bytes;
-    uint64_t depth = h.tree.n_layers - 1;
-    for (uint32_t o = 0; o < d->num_openings; o++) {
-        uint32_t idx = tr_u32(tr) % z.codeword_len;
-        for (uint32_t r = 0; r < R * batch; r++) wput(&w, h.cw + (size_t)r * rowbytes + (size_t)idx * z.cw_bytes, z.cw_bytes);
-        uint64_t li = idx, lc = z.codeword_len;
-        wput(&w, &li, 8);
-        wput(&w, &lc, 8);
-        wput(&w, &depth, 8);
-        uint64_t cur = idx;
-        for (uint32_t k = 0; k < depth; k++) {
-            wput(&w, h.tree.layers[k] + 32 * (cur ^ 1), 32);
-            cur >>= 1;
-        }
-    }
+    prove_core(&z, polys, batch, &h, tr, &f, pf, &w, eval_out);
     *proof_len = w.len;
-    if (eval_out) memcpy(eval_out, ev, 8 * L);
     if (modulus_out) memcpy(modulus_out, f.p, 8 * L);
-    free(comb);
-    free(coeffs);
-    free(bv);
-    free(wp);
-    free(q0);
-    free(q1);
     free(pf);
     zr_tr_free(tr);
+    zhint_free(&h);
+    zparams_free(&z);
+    return w.overflow ? -3 : 0;
+}
+
+/* ZipPlus::prove_f (phase_prove.rs:119-130) on a transcript that is already in
+ * use: the point (num_vars Montgomery inners of `field_limbs` u64) is in the
+ * field of `modulus`, which nothing here draws.  The hint is rebuilt by
+ * committing again (the commitment is deterministic). */
+int zr_prove_f_on(const zr_desc *d, const void *polys_v, uint32_t batch, zr_transcript *tr,
+                  const uint64_t *modulus, const uint64_t *point_f, uint8_t *proof, size_t proof_cap,
+                  size_t *proof_len, uint8_t *eval_out) {
+    zparams z;
+    if (batch == 0 || zparams_build(d, &z)) return -1;
+    if (validate_bits(&z, batch)) {
+        zparams_free(&z);
+        return -2;
+    }
+    zhint h;
+    if (do_commit(&z, (const uint8_t *)polys_v, batch, &h)) {
+        zparams_free(&z);
+        return -1;
+    }
+    fcfg f;
+    fcfg_init(&f, modulus, d->field_limbs);
+    wbuf w = {proof, 0, proof_cap, 0};
+    prove_core(&z, (const uint8_t *)polys_v, batch, &h, tr, &f, point_f, &w, eval_out);
+    *proof_len = w.len;
     zhint_free(&h);
     zparams_free(&z);
     return w.overflow ? -3 : 0;
@@ -1668,7 +1735,7 @@ int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const in
                 for (uint32_t j = 0; j < R; j++) {
                     const uint8_t *e = col + ((size_t)b * R + j) * z.cw_bytes;
                     uint64_t v[8] = {0};
-                    if (z.d.eval_kind == ZR_EVAL_I32) {
+                    if (z.d.eval_kind != ZR_EVAL_BINPOLY) {
                         uint64_t x[8];
                         memcpy(x, e, 16);
                         uint64_t sg = (x[1] >> 63) ? ~0ull : 0;

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-enum { ZR_EVAL_I32 = 0, ZR_EVAL_BINPOLY = 1 };
+enum { ZR_EVAL_I32 = 0, ZR_EVAL_BINPOLY = 1, ZR_EVAL_I64 = 2 };
 enum { ZR_CODE_IPRS = 0, ZR_CODE_RAA = 1, ZR_CODE_RAA_SIGN_FLIP = 2 };
 
 /* Same meaning as the product's zg_params_desc. */
@@ -85,6 +85,11 @@ int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const in
 
 /* FS transcript (Blake3Transcript) for direct tests */
 typedef struct zr_transcript zr_transcript;
+/* ZipPlus::prove_f on a transcript already in use, point in the field of
+ * `modulus` (Montgomery inners); appends nothing but writes the proof bytes. */
+int zr_prove_f_on(const zr_desc *d, const void *polys, uint32_t batch, zr_transcript *tr,
+                  const uint64_t *modulus, const uint64_t *point_f, uint8_t *proof, size_t proof_cap,
+                  size_t *proof_len, uint8_t *eval_out);
 zr_transcript *zr_tr_new(void);
 void zr_tr_free(zr_transcript *t);
 void zr_tr_absorb(zr_transcript *t, const uint8_t *buf, size_t n);

@@ -5,7 +5,7 @@ checked through the same equality and through the verifier."""
 import numpy as np
 import pytest
 
-from util import binary_evals, desc_for, i32_evals, params_for
+from util import binary_evals, desc_for, i32_evals, i64_evals, params_for
 
 pytestmark = pytest.mark.gpu
 
@@ -28,10 +28,16 @@ ENCODE_CASES = [
     (1, 64, 1, 12, 64, 0),
     (1, 3, 1, 8, 16, 0),
     (1, 32, 1, 16, 256, 0),   # RAA at the Zip+ benchmark shape
+    (2, 1, 0, 12, 4096, 0),   # i64 evaluations (Zinc+ integer columns): depth 2
+    (2, 1, 0, 14, 1024, 0),   # depth 1
+    (2, 1, 0, 10, 1024, 3),   # depth 3
+    (2, 1, 0, 6, 64, 0),
 ]
 
 
 def _evals(rng, ek, D, n):
+    if ek == 2:
+        return i64_evals(rng, n)
     return binary_evals(rng, n, D) if ek else i32_evals(rng, n, -(2**31), 2**31 - 1)
 
 
@@ -59,6 +65,7 @@ COMMIT_CASES = [
     (1, 32, 0, 12, 1024, 1), (1, 32, 0, 12, 1024, 2), (1, 64, 0, 10, 1024, 1),
     (1, 3, 0, 10, 256, 3), (1, 32, 1, 12, 64, 1), (1, 64, 1, 12, 64, 2),
     (1, 32, 0, 3, 8, 1),
+    (2, 1, 0, 12, 4096, 1), (2, 1, 0, 12, 256, 3), (2, 1, 0, 14, 1024, 1),
 ]
 
 
@@ -98,6 +105,9 @@ def test_edge_value_polynomials(zipgpu, oracle, ctx):
         (1, 32, np.zeros(1 << nv, np.uint64)),
         (1, 32, np.full(1 << nv, 0xFFFFFFFF, np.uint64)),
         (1, 64, np.full(1 << nv, 0xFFFFFFFFFFFFFFFF, np.uint64)),
+        (2, 1, np.full(1 << nv, 2**63 - 1, np.int64)),
+        (2, 1, np.full(1 << nv, -(2**63), np.int64)),
+        (2, 1, np.where(np.arange(1 << nv) % 2 == 0, 2**63 - 1, -(2**63)).astype(np.int64)),
     ]:
         L = 256
         pp = params_for(zipgpu, ek, D, 0, nv, L, ctx=ctx)
@@ -183,7 +193,7 @@ def test_commit_prove_many_equals_sequential(zipgpu, oracle, ctx, rng, lanes):
 
 
 @pytest.mark.parametrize("case", [(0, 1, 0, 12, 4096), (1, 32, 0, 14, 1 << 14),
-                                  (1, 32, 1, 12, 64), (1, 64, 0, 16, 1 << 14)])
+                                  (1, 32, 1, 12, 64), (1, 64, 0, 16, 1 << 14), (2, 1, 0, 12, 1024)])
 def test_device_verifier_verdicts_match_oracle(zipgpu, oracle, ctx, rng, case):
     """With device parameters the verifier encodes the opened positions on the
     GPU; its verdicts equal the oracle's and the host-only verifier's."""
@@ -194,7 +204,8 @@ def test_device_verifier_verdicts_match_oracle(zipgpu, oracle, ctx, rng, case):
     verdicts_match_oracle(zipgpu, oracle, pp, desc_for(ek, D, ck, nv, L), ek, D, nv, rng, cases=24)
 
 
-@pytest.mark.parametrize("case", [(1, 32, 0, 12, 1024, 1), (1, 64, 0, 10, 256, 2), (0, 1, 0, 10, 256, 1)])
+@pytest.mark.parametrize("case", [(1, 32, 0, 12, 1024, 1), (1, 64, 0, 10, 256, 2), (0, 1, 0, 10, 256, 1),
+                                  (2, 1, 0, 10, 256, 2)])
 def test_prove_f_matches_oracle_and_prove(zipgpu, oracle, ctx, rng, case):
     """ZipPlus::prove_f (phase_prove.rs:119-253) at a field point: the oracle's
     proof and evaluation for the same field elements, and zg_prove's bytes when

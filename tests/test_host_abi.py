@@ -113,7 +113,10 @@ def _verdict(zipgpu, pp, comm, point, inner, proof):
 def verdicts_match_oracle(zipgpu, oracle, pp, desc, ek, D, nv, rng, cases=40):
     """Tampered and truncated proofs get the oracle's verdict (0 accept, 2 rejected
     opening, 3 malformed), including the first failure winning over a later one."""
-    poly = binary_evals(rng, 1 << nv, D) if ek else i32_evals(rng, 1 << nv)
+    if ek == 2:
+        poly = rng.integers(-(2**63), 2**63 - 1, size=1 << nv, dtype=np.int64, endpoint=True)
+    else:
+        poly = binary_evals(rng, 1 << nv, D) if ek else i32_evals(rng, 1 << nv)
     point = [(-1) ** i * (5 * i + 2) for i in range(nv)]
     root, proof, inner, _ = oracle.commit_prove(desc, poly, 1, point)
     comm = zipgpu.ZipPlusCommitment(root, 1)
@@ -140,7 +143,7 @@ def zipgpu_openings_bytes(pp):
 
 
 @pytest.mark.parametrize("case", [(0, 1, 0, 12, 4096), (1, 32, 0, 13, 1 << 13),
-                                  (1, 32, 1, 12, 64), (1, 64, 0, 11, 512)])
+                                  (1, 32, 1, 12, 64), (1, 64, 0, 11, 512), (2, 1, 0, 12, 1024)])
 def test_host_verifier_verdicts_match_oracle(zipgpu, oracle, rng, case):
     ek, D, ck, nv, L = case
     pp = params_for(zipgpu, ek, D, ck, nv, L, device=False)

@@ -15,6 +15,11 @@ def i32_evals(rng, n, lo=-(2**15), hi=2**15):
     return rng.integers(lo, hi, size=n, dtype=np.int32)
 
 
+def i64_evals(rng, n):
+    """n i64 evaluations over the whole range."""
+    return rng.integers(-(2**63), 2**63 - 1, size=n, dtype=np.int64, endpoint=True)
+
+
 def desc_for(eval_kind, D, code_kind, num_vars, row_len, depth=0, rep=4, comb=None, field=4,
              openings=147):
     return O.make_desc(eval_kind, D, code_kind, num_vars, row_len, depth=depth, rep=rep,
@@ -24,7 +29,7 @@ def desc_for(eval_kind, D, code_kind, num_vars, row_len, depth=0, rep=4, comb=No
 def params_for(Z, eval_kind, D, code_kind, num_vars, row_len, depth=0, rep=4, device=True,
                ctx=None, comb=None, field=4, openings=147):
     zt = Z.ZipTypes(eval_kind, D if eval_kind == Z.EVAL_BINPOLY else 1,
-                    comb if comb else (3 if eval_kind == Z.EVAL_I32 else 5), field, openings)
+                    comb if comb else {Z.EVAL_I32: 3, Z.EVAL_I64: 6}.get(eval_kind, 5), field, openings)
     code = (Z.IprsCode(row_len, depth, rep) if code_kind == Z.CODE_IPRS else
             Z.RaaCode(row_len, rep) if code_kind == Z.CODE_RAA else Z.RaaSignFlippingCode(row_len, rep))
     return Z.ZipPlus.setup(1 << num_vars, code, zt, ctx=ctx, device=device)

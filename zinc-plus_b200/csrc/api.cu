@@ -45,7 +45,7 @@ zg_status zg::validate_budget(const zg_params *p, uint32_t batch) {
     const uint32_t d = ilog2u(p->info.row_len);
     const uint32_t codeword_bits = ilog_round_up(std::max<uint64_t>((uint64_t)p->d.rep * d, 1));
     const uint32_t challenge_bits = p->D > 1 ? 256 : 128;  // Chal = i128; doubled with alphas
-    const uint32_t eval_bits = p->d.eval_kind == ZG_EVAL_BINPOLY ? 1 : 32;
+    const uint32_t eval_bits = p->d.eval_kind == ZG_EVAL_BINPOLY ? 1 : p->d.eval_kind == ZG_EVAL_I64 ? 64 : 32;
     const uint32_t actual = 2 * codeword_bits + ilog_round_up(std::max<uint32_t>(d, 1)) +
                             challenge_bits + (eval_bits - 1) + ilog_round_up(batch);
     if (actual > 64 * p->d.comb_limbs) {
@@ -506,7 +506,7 @@ zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void 
     } else {
         ZG_CUDA(cudaMemcpyAsync(q1_d, f.one, 8 * L, cudaMemcpyHostToDevice, s));
     }
-    ProjectArgs pa{polys_d, binary ? 1 : 0, reinterpret_cast<const i128 *>(din), Da,
+    ProjectArgs pa{polys_d, binary ? 1 : p->d.eval_kind == ZG_EVAL_I64 ? 2 : 0, reinterpret_cast<const i128 *>(din), Da,
                    dmask_of(D), q1_d, RL, R, batch, CL, &f, ctx->wprime.as<uint64_t>(), part_d};
     ZG_TRY(launch_project_rows(ctx, pa, s));
     ZG_TRY(ctx->pin_out.ensure(std::max(part_bytes, tail_bytes) + 64));
@@ -915,11 +915,11 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
     if (!desc || !out) return ZG_ERR_INVALID_PARAM;
     *out = nullptr;
     zg_params_desc d = *desc;
-    if (d.eval_kind > ZG_EVAL_BINPOLY || d.code_kind > ZG_CODE_RAA_SIGN_FLIP) {
+    if (d.eval_kind > ZG_EVAL_I64 || d.code_kind > ZG_CODE_RAA_SIGN_FLIP) {
         set_error("unknown evaluation or code kind");
         return ZG_ERR_INVALID_PARAM;
     }
-    if (d.eval_kind == ZG_EVAL_I32) d.degree_plus_one = 1;
+    if (d.eval_kind != ZG_EVAL_BINPOLY) d.degree_plus_one = 1;
     if (d.eval_kind == ZG_EVAL_BINPOLY && (d.degree_plus_one < 1 || d.degree_plus_one > 64)) {
         set_error("BinaryPoly coefficient count must be in 1..64");
         return ZG_ERR_INVALID_PARAM;
@@ -946,7 +946,7 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
     zg_params_info &I = p->info;
     I.row_len = d.row_len;
     I.num_rows = (uint32_t)((1ull << d.num_vars) / d.row_len);
-    I.eval_bytes = d.eval_kind == ZG_EVAL_BINPOLY ? 8 : 4;
+    I.eval_bytes = d.eval_kind == ZG_EVAL_I32 ? 4 : 8;
     I.comb_bytes = 8 * d.comb_limbs;
     I.field_bytes = 8 * d.field_limbs;
     if (ctx) ZG_CUDA(cudaSetDevice(ctx->device));
@@ -1050,7 +1050,7 @@ static zg_status params_create_impl(zg_ctx *ctx, const zg_params_desc *desc, zg_
             return ZG_ERR_INVALID_PARAM;
         }
         // RaaCode::new width check (raa.rs:54-74): Cw coefficients are i32.
-        const uint32_t eval_bits = d.eval_kind == ZG_EVAL_BINPOLY ? 1 : 32;
+        const uint32_t eval_bits = d.eval_kind == ZG_EVAL_BINPOLY ? 1 : d.eval_kind == ZG_EVAL_I64 ? 64 : 32;
         const uint32_t need = eval_bits + 2 * ilog2u(d.row_len) + 2 * ilog2u(d.rep);
         if (need > 32) {
             set_error("Cannot fit %u-bit wide codeword entries in 32 bits entries", need);

@@ -12,6 +12,7 @@
 // ring homomorphism, so the order of additions does not change any output,
 // and when the reference's checked arithmetic does not overflow the values are
 // identical.
+#include <type_traits>
 #include <algorithm>
 
 #include "zg_internal.h"
@@ -945,28 +946,32 @@ __global__ void __launch_bounds__(256) k_stage_bin(const Tin *__restrict__ in,
 }
 
 // ---------------------------------------------------------------------------
-// Base layer, i32 evaluations -> i128 codeword (MulByScalar i32 x i64 -> i128,
-// utils/src/mul_by_scalar.rs:89-95).  |sum| < 2^31 * 32769 * 2^14 < 2^61 fits i64.
-template <bool FINAL, bool LEAF_MAJOR>
-__global__ void __launch_bounds__(256) k_base_i32(const int32_t *__restrict__ evals,
+// Base layer, integer evaluations -> i128 codeword.  i32 evaluations
+// (MulByScalar i32 x i64 -> i128, utils/src/mul_by_scalar.rs:89-95): |sum| <
+// 2^31 * 32769 * 2^14 < 2^61 fits i64, the base values are i64.  i64
+// evaluations (MulByScalar i64 x i64 -> i128, mul_by_scalar.rs:110-116): the
+// sum needs i128 (< 2^63 * 2^16 * 2^14), the base values are i128.
+template <typename TE, bool FINAL, bool LEAF_MAJOR>
+__global__ void __launch_bounds__(256) k_base_int(const TE *__restrict__ evals,
                                                   const int32_t *__restrict__ bmT, void *out,
                                                   uint32_t row_len, uint32_t bd, uint32_t bl,
                                                   uint32_t depth, uint32_t C, uint32_t nrows,
                                                   uint32_t seg_log) {
+    using Acc = typename std::conditional<sizeof(TE) == 4, int64_t, i128>::type;
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (size_t)nrows * C) return;
     const uint32_t p = (uint32_t)(t % C), grow = (uint32_t)(t / C);
     const uint32_t ch = p / bd, rb = p % bd;
     const uint32_t oct = octet_reverse(ch, depth), shift = 3 * depth;
-    const int32_t *row = evals + (size_t)grow * row_len;
-    int64_t acc = 0;
+    const TE *row = evals + (size_t)grow * row_len;
+    Acc acc = 0;
     for (uint32_t c = 0; c < bl; c++)
-        acc += (int64_t)__ldg(row + oct + ((size_t)c << shift)) * (int64_t)__ldg(bmT + (size_t)c * bd + rb);
+        acc += (Acc)__ldg(row + oct + ((size_t)c << shift)) * (Acc)__ldg(bmT + (size_t)c * bd + rb);
     if (FINAL) {
         i128 *o = static_cast<i128 *>(out);
         o[LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) : (size_t)grow * C + p] = (i128)acc;
     } else {
-        static_cast<int64_t *>(out)[(size_t)grow * C + p] = acc;
+        static_cast<Acc *>(out)[(size_t)grow * C + p] = acc;
     }
 }
 
@@ -1183,6 +1188,65 @@ zg_status launch_encode_wide_at(zg_params *p, zg_ctx *ctx, const uint64_t *row_d
     k_encode_wide_at<<<n, std::min<uint32_t>(256, std::max<uint32_t>(32, nch)), smem, s>>>(
         row_d, p->d_bmT, p->d_tw, to, I.base_dim, I.base_len, I.depth, CL, pos_d, out_d);
     ZG_KEND(ctx, s);
+    return ZG_OK;
+}
+
+// IPRS encode of i32 or i64 evaluation rows into i128 codewords: the base
+// layer (i64 values for i32 evaluations, i128 for i64) then the radix-8
+// stages on i128.
+template <typename TE>
+static zg_status encode_int_rows(zg_params *p, zg_ctx *ctx, const TE *ev, uint8_t *out_d, uint32_t nrows,
+                                 bool leaf_major, uint32_t seg_log, cudaStream_t s) {
+    using Base = typename std::conditional<sizeof(TE) == 4, int64_t, i128>::type;
+    const zg_params_info &I = p->info;
+    const uint32_t C = I.codeword_len, L = I.row_len;
+    const uint32_t bd = I.base_dim, bl = I.base_len, depth = I.depth;
+    const char *kname = sizeof(TE) == 4 ? "k_base_i32" : "k_base_i64";
+    const size_t nbase = (size_t)nrows * C;
+    if (depth == 0) {
+        ZG_KBEGIN(ctx, s, kname);
+        if (leaf_major)
+            k_base_int<TE, true, true><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows, seg_log);
+        else
+            k_base_int<TE, true, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows, seg_log);
+        ZG_KEND(ctx, s);
+        return ZG_OK;
+    }
+    ZG_TRY(ctx->stage_a.ensure(nbase * sizeof(Base)));
+    ZG_TRY(ctx->stage_b.ensure(nbase * 16));
+    ZG_TRY(ctx->stage_c.ensure(depth > 2 ? nbase * 16 : 16));
+    Base *base = ctx->stage_a.as<Base>();
+    ZG_KBEGIN(ctx, s, kname);
+    k_base_int<TE, false, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, base, L, bd, bl, depth, C, nrows, seg_log);
+    ZG_KEND(ctx, s);
+    const size_t nthr = (size_t)nrows * (C / 8);
+    const unsigned nb = blocks_for(nthr, 256);
+    i128 *prev = nullptr;
+    for (uint32_t k = 0; k < depth; k++) {
+        const uint32_t sub = bd << (3 * k);
+        const int32_t *tw = p->d_tw + p->tw_dev_off[k];
+        const bool last = k + 1 == depth;
+        i128 *dst = last ? reinterpret_cast<i128 *>(out_d)
+                         : (k % 2 == 0 ? ctx->stage_b.as<i128>() : ctx->stage_c.as<i128>());
+        ZG_KBEGIN(ctx, s, k == 0 ? "k_stage_i128[0]" : "k_stage_i128[1+]");
+        if (k == 0) {
+            if (last && leaf_major)
+                k_stage_i128<Base, true, true><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
+            else if (last)
+                k_stage_i128<Base, true, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
+            else
+                k_stage_i128<Base, false, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
+        } else {
+            if (last && leaf_major)
+                k_stage_i128<i128, true, true><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
+            else if (last)
+                k_stage_i128<i128, true, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
+            else
+                k_stage_i128<i128, false, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
+        }
+        ZG_KEND(ctx, s);
+        prev = dst;
+    }
     return ZG_OK;
 }
 
@@ -1441,54 +1505,12 @@ zg_status launch_encode(zg_params *p, zg_ctx *lane, const void *evals_d, uint32_
         return ZG_OK;
     }
 
-    // i32 evaluations
-    const int32_t *ev = static_cast<const int32_t *>(evals_d);
-    const size_t nbase = (size_t)nrows * C;
-    if (depth == 0) {
-        ZG_KBEGIN(ctx, s, "k_base_i32");
-        if (leaf_major)
-            k_base_i32<true, true><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows, seg_log);
-        else
-            k_base_i32<true, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, out_d, L, bd, bl, depth, C, nrows, seg_log);
-        ZG_KEND(ctx, s);
-        return ZG_OK;
-    }
-    ZG_TRY(ctx->stage_a.ensure(nbase * 8));
-    ZG_TRY(ctx->stage_b.ensure(nbase * 16));
-    ZG_TRY(ctx->stage_c.ensure(depth > 2 ? nbase * 16 : 16));
-    int64_t *base = ctx->stage_a.as<int64_t>();
-    ZG_KBEGIN(ctx, s, "k_base_i32");
-    k_base_i32<false, false><<<blocks_for(nbase, 256), 256, 0, s>>>(ev, p->d_bmT, base, L, bd, bl, depth, C, nrows, seg_log);
-    ZG_KEND(ctx, s);
-    const size_t nthr = (size_t)nrows * (C / 8);
-    const unsigned nb = blocks_for(nthr, 256);
-    i128 *prev = nullptr;
-    for (uint32_t k = 0; k < depth; k++) {
-        const uint32_t sub = bd << (3 * k);
-        const int32_t *tw = p->d_tw + p->tw_dev_off[k];
-        const bool last = k + 1 == depth;
-        i128 *dst = last ? reinterpret_cast<i128 *>(out_d)
-                         : (k % 2 == 0 ? ctx->stage_b.as<i128>() : ctx->stage_c.as<i128>());
-        ZG_KBEGIN(ctx, s, k == 0 ? "k_stage_i128[0]" : "k_stage_i128[1+]");
-        if (k == 0) {
-            if (last && leaf_major)
-                k_stage_i128<int64_t, true, true><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
-            else if (last)
-                k_stage_i128<int64_t, true, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
-            else
-                k_stage_i128<int64_t, false, false><<<nb, 256, 0, s>>>(base, dst, tw, C, sub, nrows, seg_log);
-        } else {
-            if (last && leaf_major)
-                k_stage_i128<i128, true, true><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
-            else if (last)
-                k_stage_i128<i128, true, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
-            else
-                k_stage_i128<i128, false, false><<<nb, 256, 0, s>>>(prev, dst, tw, C, sub, nrows, seg_log);
-        }
-        ZG_KEND(ctx, s);
-        prev = dst;
-    }
-    return ZG_OK;
+    // i32 and i64 evaluations
+    if (p->d.eval_kind == ZG_EVAL_I64)
+        return encode_int_rows<int64_t>(p, ctx, static_cast<const int64_t *>(evals_d), out_d, nrows, leaf_major,
+                                        seg_log, s);
+    return encode_int_rows<int32_t>(p, ctx, static_cast<const int32_t *>(evals_d), out_d, nrows, leaf_major,
+                                    seg_log, s);
 }
 
 }  // namespace zg

@@ -61,8 +61,9 @@ __global__ void __launch_bounds__(256) k_eq_table_split(const uint64_t *__restri
     for (int w = 0; w < L; w++) out[(size_t)i * L + w] = t[w];
 }
 
-// One thread per (poly, row j, column c).  Binary evaluations project to
-// sum_{bit i set} alpha_i; i32 evaluations project to themselves (alphas = [1]).
+// One thread per (poly, row j, column c).  Binary evaluations (binary == 1)
+// project to sum_{bit i set} alpha_i; i32 (binary == 0) and i64 (binary == 2)
+// evaluations project to themselves (alphas = [1]).
 // The projection fits in 3 limbs (|w'| < 64 * 2^127); it is sign-extended (or
 // truncated) to comb_limbs.
 template <int L>
@@ -77,7 +78,7 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
     __shared__ uint64_t s_red[256 * L];
     const uint32_t b = blockIdx.z, j = blockIdx.y;
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (binary) {
+    if (binary == 1) {
         for (uint32_t i = threadIdx.x; i < D; i += blockDim.x) s_alpha[i] = alphas[(size_t)b * D + i];
     }
     __syncthreads();
@@ -86,7 +87,7 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
     if (c < row_len) {
         const size_t e = ((size_t)b * num_rows + j) * row_len + c;
         uint64_t w3[3] = {0, 0, 0};
-        if (binary) {
+        if (binary == 1) {
             uint64_t x = static_cast<const uint64_t *>(evals)[e] & dmask;
             while (x) {
                 const int bit = __ffsll((long long)x) - 1;
@@ -97,7 +98,8 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
                 x &= x - 1;
             }
         } else {
-            const int64_t v = static_cast<const int32_t *>(evals)[e];
+            const int64_t v = binary == 2 ? static_cast<const int64_t *>(evals)[e]
+                                          : (int64_t) static_cast<const int32_t *>(evals)[e];
             w3[0] = (uint64_t)v;
             w3[1] = w3[2] = v < 0 ? ~0ull : 0ull;
         }

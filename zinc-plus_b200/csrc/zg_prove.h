@@ -6,7 +6,7 @@ namespace zg {
 
 struct ProjectArgs {
     const void *evals;      // batch polys back to back
-    int binary;             // ZG_EVAL_BINPOLY
+    int binary;             // 1: ZG_EVAL_BINPOLY, 0: ZG_EVAL_I32, 2: ZG_EVAL_I64
     const i128 *alphas;     // batch x D
     uint32_t D;
     uint64_t dmask;

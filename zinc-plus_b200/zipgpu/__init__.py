@@ -33,7 +33,7 @@ STATUS = {
     4: "ZG_ERR_OVERFLOW", 5: "ZG_ERR_CUDA", 6: "ZG_ERR_OOM", 7: "ZG_ERR_TIMEOUT",
     8: "ZG_ERR_NO_DEVICE", 9: "ZG_ERR_BUFFER_TOO_SMALL",
 }
-EVAL_I32, EVAL_BINPOLY = 0, 1
+EVAL_I32, EVAL_BINPOLY, EVAL_I64 = 0, 1, 2
 CODE_IPRS, CODE_RAA, CODE_RAA_SIGN_FLIP = 0, 1, 2
 
 # Every symbol include/zipgpu.h declares.
@@ -346,7 +346,7 @@ class ZipPlusParams:
 
     @property
     def eval_dtype(self):
-        return np.int32 if self.zt.eval_kind == EVAL_I32 else np.uint64
+        return {EVAL_I32: np.int32, EVAL_I64: np.int64}.get(self.zt.eval_kind, np.uint64)
 
     def proof_size(self, batch: int = 1) -> int:
         return int(lib().zg_proof_size(self.handle, batch))
