@@ -718,10 +718,11 @@ def run_ours(args):
             verify["cpu_baseline_ms"] = (time.perf_counter() - a) * 1e3
             verify["cpu_baseline_kind"] = "port (oracle, OpenMP, full encode_wide as the reference)"
             verify["oracle_accepts"] = rc == 0
-    batch_commit = serving = sumcheck = piop_steps = None
+    batch_commit = serving = sumcheck = piop_steps = zinc_prove = None
     if not args.no_extra:
         sumcheck = run_sumcheck(Z, ctx, torch, stream, 18, 14, rank == 0 and not args.no_cpu_baseline)
         piop_steps = run_piop_steps(Z, ctx, torch, stream, 18, 14, rank == 0 and not args.no_cpu_baseline)
+        zinc_prove = run_zinc_prove(Z, ctx, 18, 10, rank == 0 and not args.no_cpu_baseline)
         batch_commit = run_batched_commit(Z, ctx, torch, stream, flush, reps=5, warm=2)
         serving = run_serving(Z, ctx, torch, args.serve_requests, args.serve_workers,
                               seed=0x5A1F + rank)
@@ -762,6 +763,7 @@ def run_ours(args):
             "serving": serving,
             "sumcheck": sumcheck,
             "piop_steps": piop_steps,
+            "zinc_prove_mle_first": zinc_prove,
             "verify": verify,
             "impl": "ours",
         }
@@ -929,6 +931,56 @@ def run_piop_steps(Z, ctx, torch, stream, nv, cpu_nv, with_cpu):
         res["cpu_baseline"]["multipoint_eval_s_at_2^8_rows"] = c5
         res["equal_oracle_at_cpu_size"] = bool(np.array_equal(got3, want3) and np.array_equal(got6, want6)
                                                and got5[0] == want5[0])
+    return res
+
+
+def run_zinc_prove(Z, ctx, nv, cpu_nv, with_cpu):
+    """The MLE-first Zinc+ prover end to end on BigLinearUair (16 BinaryPoly<32>
+    columns, 1 i64 column, 16 shifts, 17 constraints; 2^nv rows; MontyField<3>;
+    both tables IPRS rate 1/4 with 16 rows of 2^(nv-4), CombR Int<6>): the trace
+    from host memory through zg_zinc_prove_mle_first to the Proof bytes in host
+    memory, timed on the host clock (the call synchronises).  The oracle's chain
+    of the same steps at 2^cpu_nv rows gives the byte-equality check and a CPU
+    time (its PIOP steps are Python integer loops, so that time says nothing
+    about the reference's speed)."""
+    from oracle import oracle as O
+    from zipgpu import uair
+
+    bins, ints = uair.trace(nv, 0xB16)
+    shifts, coeffs = uair.signature()
+
+    def tables(n):
+        L = 1 << (n - 4)
+        mk = lambda ek, D: Z.ZipPlus.setup(1 << n, Z.IprsCode(L, 0, 4), Z.ZipTypes(ek, D, 6, 3, 147), ctx=ctx)
+        return mk(Z.EVAL_BINPOLY, 32), mk(Z.EVAL_I64, 1)
+
+    pb, pi = tables(nv)
+    proof = Z.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+    ts = []
+    for _ in range(3):
+        a = time.perf_counter()
+        again = Z.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+        ts.append((time.perf_counter() - a) * 1e3)
+    res = {"workload": f"BigLinearUair, 2^{nv} rows: 16 BinaryPoly<32> + 1 i64 column, 16 shifts, 17 constraints; "
+                       "MontyField<3>; IPRS rate 1/4, 16 rows per table; 147 openings",
+           "ms": statistics.median(ts), "proof_bytes": len(proof), "deterministic": again == proof,
+           "h2d_bytes": int(bins.nbytes + ints.nbytes),
+           "what": "commit both tables, prime, ideal check, evaluation projection, CPR sumcheck, multipoint "
+                   "sumcheck, lifted evaluations, prove_f of both tables, Proof transcription"}
+    if with_cpu:
+        bs, is_ = uair.trace(cpu_nv, 0xB17)
+        pbs, pis = tables(cpu_nv)
+        Ls = 1 << (cpu_nv - 4)
+        db = O.make_desc(O.EVAL_BINPOLY, 32, 0, cpu_nv, Ls, comb_limbs=6, field_limbs=3)
+        di = O.make_desc(O.EVAL_I64, 1, 0, cpu_nv, Ls, comb_limbs=6, field_limbs=3)
+        a = time.perf_counter()
+        want = O.zinc_prove_mle_first(db, di, cpu_nv, bs, 32, is_, shifts, coeffs, 3)
+        c = time.perf_counter() - a
+        got = Z.ZincPlusPiop.prove_mle_first(pbs, pis, cpu_nv, bs, 32, is_, shifts, coeffs)
+        res["cpu_baseline"] = {"ms": c * 1e3, "cores": 1, "kind": "port",
+                               "sample": f"oracle chain at 2^{cpu_nv} rows (C commit/prove_f and sumcheck, "
+                                         "Python-integer PIOP steps)"}
+        res["equal_oracle_at_cpu_size"] = got == want
     return res
 
 

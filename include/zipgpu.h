@@ -480,6 +480,40 @@ zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, const uint8_t *
                                   const uint32_t *shift_amount, uint32_t n_shifts, int mles_on_device,
                                   uint8_t *proof, size_t *proof_len, uint64_t *r0_out);
 
+/* ---- Zinc+ prover, MLE first (ZincPlusPiop::prove::<MLE_FIRST = true>,
+ * protocol/src/prover.rs:677-706) ------------------------------------------
+ * A linear UAIR over binary-polynomial and integer witness columns (no public
+ * and no arbitrary-polynomial columns; lookups are a placeholder in the
+ * reference), e.g. BigLinearUair (test-uair/src/lib.rs:325-382: 16
+ * BinaryPoly<32> columns, 1 integer column, 16 shifts by 1, 17 constraints).
+ * Constraint k is sum_j coeffs[k][j] * col_j over [binary up, integer up, down
+ * (shifted) columns in shift order]; shift sources index the up columns, binary
+ * first.  Runs step 0 (commit both tables, absorb the roots of the binary, the
+ * empty arbitrary and the integer table), step 1 (random prime of pp's
+ * field_limbs), steps 2-6 on the GPU (zg_piop_* above), step 7 (prove_f of each
+ * table at r_0) and writes the Proof transcription (protocol/src/lib.rs:87-189:
+ * three commitments, the PCS stream, ideal check, resolver, multi-degree
+ * sumcheck, multipoint evaluation, witness lifted evaluations).
+ * pp_bin: BINPOLY parameters of num_vars (NULL when n_bin == 0); pp_int:
+ * ZG_EVAL_I64 parameters of num_vars (NULL when n_int == 0), both with a device
+ * and one context.  bin_cols: n_bin columns of 2^num_vars u64, column after
+ * column; int_cols: n_int columns of 2^num_vars i64 (device pointers when
+ * cols_on_device != 0).  proof_len: in capacity, out size. */
+typedef struct {
+    uint32_t n_bin;
+    uint32_t n_int;
+    uint32_t degree_plus_one;
+    uint32_t n_shifts;
+    const uint32_t *shift_src;
+    const uint32_t *shift_amount;
+    uint32_t n_constraints;
+    const int64_t *coeffs; /* n_constraints x (n_bin + n_int + n_shifts) */
+} zg_linear_uair;
+
+zg_status zg_zinc_prove_mle_first(zg_params *pp_bin, zg_params *pp_int, const zg_linear_uair *uair,
+                                  uint32_t num_vars, const uint64_t *bin_cols, const int64_t *int_cols,
+                                  int cols_on_device, uint8_t *proof, size_t *proof_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,7 @@ def lib():
         L.zr_tr_absorb_slice.argtypes = [vp, vp, sz]
         L.zr_tr_challenge.argtypes = [vp, vp, sz]
         L.zr_tr_get_prime.argtypes = [vp, C.c_uint32, vp]
+        L.zr_prove_f_on.argtypes = [C.POINTER(Desc), vp, C.c_uint32, vp, vp, vp, vp, sz, C.POINTER(sz), vp]
         L.zr_is_probable_prime_base2.argtypes = [vp, C.c_uint32]
         L.zr_set_threads.argtypes = [C.c_int]
         gp = C.POINTER(ScGroup)
@@ -601,3 +602,95 @@ def commit_prove_f(desc: Desc, polys: np.ndarray, batch: int, point_u256):
     if rc:
         raise ValueError(f"commit_prove_f failed ({rc})")
     return root.raw, proof.raw[: plen.value], ev.raw, mod.raw
+
+
+def prove_f_on(desc: Desc, polys: np.ndarray, batch: int, t: "Transcript", modulus: int, point_f) -> tuple[bytes, bytes]:
+    """ZipPlus::prove_f on a transcript already in use, at a point of field
+    elements (Montgomery inners, (num_vars, L)) of the prime `modulus`.
+    Returns (proof bytes, eval inner bytes)."""
+    polys = np.ascontiguousarray(polys)
+    L = desc.field_limbs
+    pt = np.ascontiguousarray(point_f, dtype=np.uint64)
+    cap = proof_size(desc, batch) + 64
+    proof = C.create_string_buffer(cap)
+    plen = C.c_size_t(0)
+    ev = C.create_string_buffer(8 * L)
+    rc = lib().zr_prove_f_on(C.byref(desc), _ptr(polys), batch, t._t, _ptr(_limbs(modulus, L)), _ptr(pt), proof,
+                             cap, C.byref(plen), ev)
+    if rc:
+        raise ValueError(f"prove_f failed ({rc})")
+    return proof.raw[: plen.value], ev.raw
+
+
+def _trim(rows: np.ndarray) -> np.ndarray:
+    n = rows.shape[0]
+    while n and not rows[n - 1].any():
+        n -= 1
+    return rows[:n]
+
+
+def _poly_vec_bytes(polys, modulus: int, L: int) -> bytes:
+    """DynamicPolyVecF transcription (poly/src/univariate/dynamic/over_field.rs:
+    409-476) of trimmed (len, L) inner arrays."""
+    if not polys:
+        return b""
+    any_ = any(q.shape[0] for q in polys)
+    out = bytes([1 if any_ else 0]) + (_limbs(modulus, L).tobytes() if any_ else b"")
+    for q in polys:
+        out += int(q.shape[0]).to_bytes(4, "little") + np.ascontiguousarray(q, np.uint64).tobytes()
+    return out
+
+
+def _sub(b: bytes) -> bytes:
+    return len(b).to_bytes(4, "little") + b
+
+
+def zinc_prove_mle_first(desc_bin: Desc, desc_int: Desc, nvars: int, bin_cols, D: int, int_cols, shifts, coeffs,
+                         L: int) -> bytes:
+    """ZincPlusPiop::prove::<MLE_FIRST = true> (protocol/src/prover.rs:677-706)
+    for a linear UAIR over binary-polynomial and i64 witness columns, chaining
+    the oracle's steps on one transcript: step 0 commitments (prover.rs:218-267;
+    the empty arbitrary table has the default root), step 1 prime, step 2
+    ideal check, step 3 the Chal (i128) projecting element and evaluation
+    projection, step 4 CPR, step 5 multipoint, step 6 lifted evaluations
+    (trimmed, each coefficient absorbed), step 7 prove_f per table, and the
+    Proof transcription (protocol/src/lib.rs:129-160).  coeffs: integer
+    constraint coefficients over [binary up, integer up, down]."""
+    b, i = _piop_cols(bin_cols, int_cols, nvars)
+    nb, ni = b.shape[0], i.shape[0]
+    roots = [b"\0" * 32, b"\0" * 32, b"\0" * 32]
+    if nb:
+        roots[0] = commit(desc_bin, b, nb)
+    if ni:
+        roots[2] = commit(desc_int, i, ni)
+    t = Transcript()
+    for r in roots:
+        t.absorb_slice(r)
+    p = t.get_prime(L)
+    R = 1 << (64 * L)
+    cf = [[int(c) % p for c in row] for row in coeffs]
+    ic_point, combined = piop_ideal_check_linear(t, p, L, b if nb else None, D, i if ni else None, nvars, shifts, cf)
+    a = int.from_bytes(t.challenge(16), "little", signed=True) % p * R % p
+    mles = piop_eval_projection(p, L, b if nb else None, D, i if ni else None, nvars, _limbs(a, L))
+    md, cpr_pt, evals = piop_cpr_linear_prove(t, p, L, mles, ic_point, shifts, cf)
+    mp, r0 = piop_multipoint_eval(t, p, L, mles, cpr_pt, shifts)
+    lifted = piop_lifted_evals(p, L, b if nb else None, D, i if ni else None, nvars, r0)
+    polys = [_trim(lifted[c * D:(c + 1) * D]) for c in range(nb)] + \
+        [_trim(lifted[nb * D + c:nb * D + c + 1]) for c in range(ni)]
+    for q in polys:
+        for e in q:
+            t.absorb_field(p, L, e)
+    zip_ = b""
+    if nb:
+        zip_ += prove_f_on(desc_bin, b, nb, t, p, r0)[0]
+    if ni:
+        zip_ += prove_f_on(desc_int, i, ni, t, p, r0)[0]
+    S = len(shifts)
+    vec = lambda rows: (_limbs(p, L).tobytes() + np.ascontiguousarray(rows, np.uint64).tobytes()) if len(rows) else b""
+    out = roots[0] + int(nb).to_bytes(8, "little") + roots[1] + bytes(8) + roots[2] + int(ni).to_bytes(8, "little")
+    out += _sub(zip_)
+    out += _sub(_poly_vec_bytes(list(combined), p, L))
+    out += _sub(_sub(vec(evals[:nb + ni])) + _sub(vec(evals[nb + ni:nb + ni + S])))
+    out += _sub(md) + _sub(mp)
+    out += _sub(_poly_vec_bytes(polys, p, L))
+    return out

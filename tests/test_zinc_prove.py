@@ -1,0 +1,190 @@
+"""The MLE-first Zinc+ prover (ZincPlusPiop::prove::<MLE_FIRST = true>,
+protocol/src/prover.rs:677-706) on BigLinearUair and smaller linear UAIRs: the
+GPU driver's Proof bytes equal the oracle's chain of the same steps; on the CPU,
+the oracle's proof parses under the reference's read_transcription_bytes_exact
+layout (protocol/src/lib.rs:93-127) and the generated traces satisfy the
+constraints."""
+import numpy as np
+import pytest
+
+from util import desc_for, params_for
+
+N_OPEN = 147
+
+
+def tables(zipgpu, nv, D, ctx, device=True):
+    L = 1 << max(nv - 2, 1)
+    pb = params_for(zipgpu, 1, D, 0, nv, L, ctx=ctx, comb=6, field=3, device=device)
+    pi = params_for(zipgpu, 2, 1, 0, nv, L, ctx=ctx, comb=6, field=3, device=device)
+    return pb, pi, desc_for(1, D, 0, nv, L, comb=6, field=3), desc_for(2, 1, 0, nv, L, comb=6, field=3)
+
+
+class Reader:
+    def __init__(self, b: bytes):
+        self.b, self.pos = b, 0
+
+    def take(self, n):
+        assert self.pos + n <= len(self.b), "proof truncated"
+        out = self.b[self.pos:self.pos + n]
+        self.pos += n
+        return out
+
+    def u32(self):
+        return int.from_bytes(self.take(4), "little")
+
+    def u64(self):
+        return int.from_bytes(self.take(8), "little")
+
+    def sub(self):
+        return Reader(self.take(self.u32()))
+
+    def done(self):
+        return self.pos == len(self.b)
+
+
+def parse_poly_vec(r: Reader, fb: int, modulus: bytes):
+    if r.done():
+        return []
+    flag = r.take(1)[0]
+    assert flag in (0, 1)
+    if flag:
+        assert r.take(fb) == modulus
+    polys = []
+    while not r.done():
+        n = r.u32()
+        assert flag or n == 0
+        polys.append(r.take(n * fb))
+    return polys
+
+
+def parse_proof(proof: bytes, L: int, nv: int):
+    """The Proof layout (lib.rs:93-127) with every nested length checked."""
+    fb = 8 * L
+    r = Reader(proof)
+    comms = [(r.take(32), r.u64()) for _ in range(3)]
+    zip_ = r.take(r.u32())
+    ic = r.sub()
+    res = r.sub()
+    md = r.sub()
+    mp = r.sub()
+    lifted = r.sub()
+    assert r.done()
+    modulus = md.take(fb)
+    ic_polys = parse_poly_vec(ic, fb, modulus)
+    up, down = res.sub(), res.sub()
+    assert res.done()
+    up_n, down_n = [(len(x.b) - fb) // fb if x.b else 0 for x in (up, down)]
+    for x in (up, down):
+        assert not x.b or x.b[:fb] == modulus
+    assert md.u32() == 1 and md.u32() == nv
+    deg = md.u32()
+    md.take(deg * nv * fb + fb)
+    assert md.done()
+    assert mp.take(fb) == modulus and mp.u32() == nv
+    for _ in range(nv):
+        mp.take(mp.u32() * fb)
+    mp.take(fb)
+    assert mp.done()
+    lifted_polys = parse_poly_vec(lifted, fb, modulus)
+    return dict(comms=comms, zip=zip_, ic=ic_polys, up=up_n, down=down_n, degree=deg, lifted=lifted_polys,
+                modulus=int.from_bytes(modulus, "little"))
+
+
+def test_biglinear_trace_satisfies_constraints(zipgpu):
+    from zipgpu import uair
+
+    bins, ints = uair.trace(8, 3)
+    shifts, coeffs = uair.signature()
+    assert bins.shape == (16, 256) and ints.shape == (1, 256) and coeffs.shape == (17, 33)
+
+    def at(x, X):  # binary polynomial values at X
+        return sum(((x >> np.uint64(k)) & np.uint64(1)).astype(np.int64) * X ** k for k in range(32))
+
+    up1 = np.stack([at(b, 1) for b in bins] + [ints[0]])
+    up2 = np.stack([at(b, 2) for b in bins] + [ints[0]])
+    down = lambda v: np.stack([np.concatenate([v[s][c:], np.zeros(c, np.int64)]) for s, c in shifts])
+    v1, v2 = np.concatenate([up1, down(up1)]), np.concatenate([up2, down(up2)])
+    rows = slice(0, 255)  # the last row has no successor
+    for k, row in enumerate(coeffs):
+        X_is_two = k == 1
+        val = row @ (v2 if X_is_two else v1)
+        assert not val[rows].any(), k
+
+
+def test_oracle_proof_layout(zipgpu, oracle):
+    from zipgpu import uair
+
+    nv = 6
+    bins, ints = uair.trace(nv, 11)
+    shifts, coeffs = uair.signature()
+    _, _, db, di = tables(zipgpu, nv, 32, None, device=False)
+    proof = oracle.zinc_prove_mle_first(db, di, nv, bins, 32, ints, shifts, coeffs, 3)
+    P = parse_proof(proof, 3, nv)
+    assert P["comms"][0] == (oracle.commit(db, bins, 16), 16)
+    assert P["comms"][1] == (bytes(32), 0)
+    assert P["comms"][2] == (oracle.commit(di, ints, 1), 1)
+    assert len(P["ic"]) == 17 and all(len(p) <= 32 * 24 for p in P["ic"])
+    assert (P["up"], P["down"], P["degree"]) == (17, 16, 3)
+    assert len(P["lifted"]) == 17 and len(P["lifted"][16]) <= 24
+    assert oracle.is_probable_prime_base2(P["modulus"], 3) and P["modulus"].bit_length() <= 192
+    # the PCS stream: two prove_f transcripts (binary table, then integer table)
+    assert len(P["zip"]) == oracle.proof_size(db, 16) + oracle.proof_size(di, 1)
+
+
+def test_driver_rejects_bad_arguments(zipgpu):
+    from zipgpu import uair
+
+    nv = 6
+    pb, pi, _, _ = tables(zipgpu, nv, 32, None, device=False)
+    bins, ints = uair.trace(nv, 1)
+    shifts, coeffs = uair.signature()
+    with pytest.raises(zipgpu.ZipError):  # parameters without a device
+        zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+    with pytest.raises(ValueError):  # coefficient rows of the wrong width
+        zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs[:, :-1])
+
+
+def small_uair(rng, nb, ni, shifts, nc, D, nv):
+    n = 1 << nv
+    mask = (1 << D) - 1
+    bins = rng.integers(0, 1 << 63, size=(nb, n), dtype=np.uint64) & np.uint64(mask)
+    ints = rng.integers(-(2**40), 2**40, size=(ni, n), dtype=np.int64)
+    coeffs = rng.integers(-3, 4, size=(nc, nb + ni + len(shifts)), dtype=np.int64)
+    return bins, ints, coeffs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nv,seed", [(6, 11), (9, 5), (10, 2)])
+def test_gpu_biglinear_proof_matches_oracle(zipgpu, oracle, ctx, nv, seed):
+    from zipgpu import uair
+
+    bins, ints = uair.trace(nv, seed)
+    shifts, coeffs = uair.signature()
+    pb, pi, db, di = tables(zipgpu, nv, 32, ctx)
+    got = zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+    want = oracle.zinc_prove_mle_first(db, di, nv, bins, 32, ints, shifts, coeffs, 3)
+    assert len(got) == len(want)
+    assert got == want
+    P = parse_proof(got, 3, nv)
+    assert (P["up"], P["down"]) == (17, 16)
+    # deterministic
+    assert zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs) == got
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nb,ni,shifts,nc,D", [
+    (3, 2, [(0, 1), (3, 2), (4, 1)], 4, 8),
+    (2, 0, [(1, 3)], 2, 32),           # binary table only
+    (0, 2, [(0, 1), (1, 1)], 3, 8),    # integer table only
+    (1, 1, [], 1, 64),                 # no shifts
+])
+def test_gpu_small_uairs_match_oracle(zipgpu, oracle, ctx, nb, ni, shifts, nc, D):
+    nv = 7
+    rng = np.random.default_rng(nb * 100 + ni * 10 + nc)
+    bins, ints, coeffs = small_uair(rng, nb, ni, shifts, nc, D, nv)
+    pb, pi, db, di = tables(zipgpu, nv, D, ctx)
+    got = zipgpu.ZincPlusPiop.prove_mle_first(pb if nb else None, pi if ni else None, nv,
+                                              bins if nb else None, D, ints if ni else None, shifts, coeffs)
+    want = oracle.zinc_prove_mle_first(db, di, nv, bins if nb else None, D, ints if ni else None, shifts, coeffs, 3)
+    assert got == want
+    parse_proof(got, 3, nv)

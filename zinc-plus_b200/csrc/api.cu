@@ -838,7 +838,8 @@ zg_status zg_ctx_destroy(zg_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
-                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena})
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena,
+                      &ctx->trace_arena, &ctx->mle_arena})
         b->release();
     cudaStreamSynchronize(ctx->stream);  // stream-ordered frees of pooled buffers
     if (ctx->sync_event) cudaEventDestroy(ctx->sync_event);

@@ -271,7 +271,8 @@ cudaError_t device_status(int device) {
 void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool) {
     ctx->pool = pool;
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
-                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena}) {
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena,
+                      &ctx->trace_arena, &ctx->mle_arena}) {
         b->pool = pool;
         b->pool_stream = ctx->stream;
     }
@@ -280,14 +281,16 @@ void ctx_use_pool(zg_ctx *ctx, cudaMemPool_t pool) {
 size_t ctx_scratch_bytes(const zg_ctx *ctx) {
     size_t n = 0;
     for (const DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
-                            &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena})
+                            &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena,
+                      &ctx->trace_arena, &ctx->mle_arena})
         n += b->cap;
     return n;
 }
 
 void ctx_scratch_release(zg_ctx *ctx) {
     for (DevBuf *b : {&ctx->evals, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->chunk_cv,
-                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena})
+                      &ctx->wprime, &ctx->prove_in, &ctx->prove_out, &ctx->sc_arena, &ctx->piop_arena,
+                      &ctx->trace_arena, &ctx->mle_arena})
         b->release();
 }
 

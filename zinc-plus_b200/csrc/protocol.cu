@@ -1,0 +1,287 @@
+// Zinc+ prover, MLE-first, for linear UAIRs: steps 0-7 on one transcript and
+// the Proof wire format (protocol/src/prover.rs:218-706, protocol/src/lib.rs:
+// 62-189).  Every step runs on the GPU through the entry points of api.cu and
+// piop.cu; this file holds the sequencing, the host-side Fiat-Shamir glue
+// between the steps and the byte layout of the proof.
+#include <cstring>
+#include <vector>
+
+#include "zg_internal.h"
+
+using namespace zg;
+
+namespace {
+
+// F::from_with_cfg(i128) into a Montgomery inner
+void f_from_i128(const FieldCfg &f, i128 v, uint64_t *out) {
+    if (f.L == 3) from_i128<3>(v, f, out);
+    else from_i128<4>(v, f, out);
+}
+
+// Growable little-endian byte writer for the proof transcription.
+struct Bytes {
+    std::vector<uint8_t> b;
+    void put(const void *p, size_t n) {
+        const uint8_t *q = static_cast<const uint8_t *>(p);
+        b.insert(b.end(), q, q + n);
+    }
+    void u32(uint32_t v) { put(&v, 4); }
+    void u64(uint64_t v) { put(&v, 8); }
+    // write_transcription_bytes_subset of a Transcribable with a u32 length
+    // prefix (transcript/src/traits.rs:48-75): the byte length, then the bytes.
+    void sub(const Bytes &x) {
+        u32((uint32_t)x.b.size());
+        put(x.b.data(), x.b.size());
+    }
+};
+
+// DynamicPolyVecF (poly/src/univariate/dynamic/over_field.rs:409-476): nothing
+// for an empty vector; else a flag byte (1 when some polynomial has a
+// coefficient, followed by the modulus), then per polynomial its u32 length and
+// its coefficients' inners.  Polynomials arrive trimmed.
+Bytes poly_vec(const std::vector<std::vector<uint64_t>> &polys, const uint64_t *p, int L) {
+    Bytes o;
+    if (polys.empty()) return o;
+    bool any = false;
+    for (const auto &q : polys) any |= !q.empty();
+    o.b.push_back(any ? 1 : 0);
+    if (any) o.put(p, 8 * (size_t)L);
+    for (const auto &q : polys) {
+        o.u32((uint32_t)(q.size() / L));
+        o.put(q.data(), q.size() * 8);
+    }
+    return o;
+}
+
+// Vec<F> (transcript/src/traits.rs:566-607): nothing when empty, else the
+// modulus and the inners.
+Bytes field_vec(const uint64_t *v, size_t n, const uint64_t *p, int L) {
+    Bytes o;
+    if (n == 0) return o;
+    o.put(p, 8 * (size_t)L);
+    o.put(v, n * 8 * (size_t)L);
+    return o;
+}
+
+// new_trimmed: drop trailing zero coefficients.
+std::vector<uint64_t> trimmed(const uint64_t *c, size_t n, int L) {
+    while (n > 0) {
+        bool zero = true;
+        for (int w = 0; w < L; w++) zero &= c[(n - 1) * L + w] == 0;
+        if (!zero) break;
+        n--;
+    }
+    return std::vector<uint64_t>(c, c + n * L);
+}
+
+struct HintGuard {
+    zg_hint *h = nullptr;
+    ~HintGuard() {
+        if (h) zg_hint_free(h);
+    }
+};
+struct TranscriptGuard {
+    zg_transcript *t = nullptr;
+    ~TranscriptGuard() {
+        if (t) zg_transcript_free(t);
+    }
+};
+
+zg_status check_uair(const zg_params *pb, const zg_params *pi, const zg_linear_uair *u, uint32_t nv) {
+    if (!u || (u->n_bin == 0 && u->n_int == 0) || u->n_constraints == 0 || !u->coeffs ||
+        (u->n_shifts && (!u->shift_src || !u->shift_amount))) {
+        set_error("zinc prove: empty UAIR or null constraint/shift arrays");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if ((u->n_bin && !pb) || (u->n_int && !pi)) {
+        set_error("zinc prove: parameters missing for a non-empty column table");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    const zg_params *any = pb ? pb : pi;
+    if (pb && pi && (pb->ctx != pi->ctx || pb->d.field_limbs != pi->d.field_limbs)) {
+        set_error("zinc prove: the two tables need one context and one field size");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (!any->ctx) {
+        set_error("zinc prove: the parameters have no device");
+        return ZG_ERR_NO_DEVICE;
+    }
+    if (any->d.field_limbs != 3 && any->d.field_limbs != 4) {
+        set_error("zinc prove: field of %u limbs (3 or 4 supported)", any->d.field_limbs);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (pb && (pb->d.eval_kind != ZG_EVAL_BINPOLY || pb->d.num_vars != nv ||
+               pb->d.degree_plus_one != u->degree_plus_one)) {
+        set_error("zinc prove: binary table parameters do not match the trace");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (pi && (pi->d.eval_kind != ZG_EVAL_I64 || pi->d.num_vars != nv)) {
+        set_error("zinc prove: integer table parameters must take i64 evaluations of the trace size");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    const uint32_t ncols = u->n_bin + u->n_int;
+    for (uint32_t k = 0; k < u->n_shifts; k++)
+        if (u->shift_src[k] >= ncols || u->shift_amount[k] == 0 || u->shift_amount[k] >= (1u << nv)) {
+            set_error("zinc prove: shift %u out of range", k);
+            return ZG_ERR_INVALID_PARAM;
+        }
+    return ZG_OK;
+}
+
+zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u, uint32_t nv, const uint64_t *bin,
+                          const int64_t *ints, int on_device, uint8_t *proof, size_t *proof_len) {
+    ZG_TRY(check_uair(pb, pi, u, nv));
+    zg_params *any = pb ? pb : pi;
+    zg_ctx *ctx = any->ctx;
+    const int L = (int)any->d.field_limbs;
+    const uint32_t nb = u->n_bin, ni = u->n_int, ncols = nb + ni, S = u->n_shifts, D = u->degree_plus_one;
+    const uint32_t nc = u->n_constraints;
+    const size_t n = (size_t)1 << nv;
+
+    // the trace in device memory: binary columns, then integer columns
+    const uint64_t *bin_d = bin;
+    const int64_t *int_d = ints;
+    if (!on_device) {
+        {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            ZG_CUDA(cudaSetDevice(ctx->device));
+            ZG_TRY(ctx->trace_arena.ensure(n * 8 * ncols + 16));
+            uint64_t *dst = ctx->trace_arena.as<uint64_t>();
+            if (nb) ZG_CUDA(cudaMemcpyAsync(dst, bin, n * 8 * nb, cudaMemcpyHostToDevice, ctx->stream));
+            if (ni)
+                ZG_CUDA(cudaMemcpyAsync(dst + n * nb, ints, n * 8 * ni, cudaMemcpyHostToDevice, ctx->stream));
+            ZG_CUDA(ctx_sync(ctx));
+            bin_d = dst;
+            int_d = reinterpret_cast<const int64_t *>(dst + n * nb);
+        }
+    }
+
+    // step 0 (prover.rs:218-267): commit each non-empty table; the arbitrary
+    // polynomial table is empty (default root, batch 0); absorb the three roots
+    HintGuard hb, hi;
+    uint8_t roots[3][32];
+    std::memset(roots, 0, sizeof roots);
+    if (nb) ZG_TRY(zg_commit_d(pb, bin_d, nb, &hb.h, roots[0]));
+    if (ni) ZG_TRY(zg_commit_d(pi, int_d, ni, &hi.h, roots[2]));
+    TranscriptGuard tg;
+    ZG_TRY(zg_transcript_new(&roots[0][0], 3, &tg.t));
+    zg_transcript *t = tg.t;
+
+    // step 1 (prover.rs:285-300): the random prime; projection happens inside
+    // the steps that read the columns
+    uint8_t mod_b[32];
+    ZG_TRY(zg_transcript_sample_field(t, (uint32_t)L, mod_b));
+    const FieldCfg &f = t->f;
+    std::vector<uint64_t> coeffs((size_t)nc * (ncols + S) * L);
+    for (size_t k = 0; k < (size_t)nc * (ncols + S); k++) f_from_i128(f, (i128)u->coeffs[k], &coeffs[k * L]);
+
+    // step 2 (prover.rs:358-380): ideal check, MLE first
+    std::vector<uint64_t> ic_point((size_t)nv * L), combined((size_t)nc * D * L);
+    std::vector<uint32_t> lens(nc);
+    ZG_TRY(zg_piop_ideal_check_linear(ctx, t, mod_b, (uint32_t)L, bin_d, nb, D, int_d, ni, nv, u->shift_src,
+                                      u->shift_amount, S, nc, coeffs.data(), 1, ic_point.data(),
+                                      combined.data(), lens.data()));
+    std::vector<std::vector<uint64_t>> ic_vals(nc);
+    for (uint32_t k = 0; k < nc; k++)
+        ic_vals[k].assign(&combined[(size_t)k * D * L], &combined[(size_t)k * D * L] + (size_t)lens[k] * L);
+
+    // step 3 (prover.rs:385-415): the projecting element a = Chal (i128) in F,
+    // the columns evaluated at a, kept on the device for steps 4 and 5
+    uint64_t a[4];
+    f_from_i128(f, tr_challenge_i128(t), a);
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ZG_CUDA(cudaSetDevice(ctx->device));
+        ZG_TRY(ctx->mle_arena.ensure(n * 8 * L * ncols + 16));
+    }
+    uint64_t *mles = ctx->mle_arena.as<uint64_t>();
+    ZG_TRY(zg_piop_eval_projection(ctx, mod_b, (uint32_t)L, bin_d, nb, D, int_d, ni, nv, a, 1, mles));
+
+    // step 4 (prover.rs:420-472): CPR group + MultiDegreeSumcheck + finalize
+    // capacity: modulus, group count, rounds, one degree (3 here, at most 8),
+    // the round messages, the claimed sum
+    size_t md_len = 8 * (size_t)L + 12 + (size_t)nv * 8 * 8 * L + 8 * (size_t)L;
+    std::vector<uint8_t> md_proof(md_len);
+    std::vector<uint64_t> cpr_point((size_t)nv * L), cpr_evals((size_t)(ncols + S) * L);
+    ZG_TRY(zg_piop_cpr_linear_prove(ctx, t, mod_b, (uint32_t)L, mles, ncols, nv, ic_point.data(), u->shift_src,
+                                    u->shift_amount, S, nc, coeffs.data(), 1, md_proof.data(), &md_len,
+                                    cpr_point.data(), cpr_evals.data()));
+    md_proof.resize(md_len);
+
+    // step 5 (prover.rs:478-492): multipoint evaluation down to r_0
+    // capacity: modulus, message count, per round a length and 2 evaluations,
+    // the claimed sum
+    size_t mp_len = 8 * (size_t)L + 4 + (size_t)nv * (4 + 2 * 8 * L) + 8 * (size_t)L;
+    std::vector<uint8_t> mp_proof(mp_len);
+    std::vector<uint64_t> r0((size_t)nv * L);
+    ZG_TRY(zg_piop_multipoint_eval(ctx, t, mod_b, (uint32_t)L, mles, ncols, nv, cpr_point.data(), u->shift_src,
+                                   u->shift_amount, S, 1, mp_proof.data(), &mp_len, r0.data()));
+    mp_proof.resize(mp_len);
+
+    // step 6 (prover.rs:497-532): lifted evaluations at r_0, trimmed, every
+    // coefficient absorbed (absorb_random_field_slice)
+    std::vector<uint64_t> lifted(((size_t)nb * D + ni) * L);
+    ZG_TRY(zg_piop_lifted_evals(ctx, mod_b, (uint32_t)L, bin_d, nb, D, int_d, ni, nv, r0.data(), 1, lifted.data()));
+    std::vector<std::vector<uint64_t>> lifted_polys(ncols);
+    for (uint32_t c = 0; c < ncols; c++) {
+        const uint64_t *src = c < nb ? &lifted[(size_t)c * D * L] : &lifted[((size_t)nb * D + (c - nb)) * L];
+        lifted_polys[c] = trimmed(src, c < nb ? D : 1, L);
+        for (size_t k = 0; k < lifted_polys[c].size() / L; k++) tr_absorb_field(t, &lifted_polys[c][k * L]);
+    }
+
+    // step 7 (prover.rs:552-597): PCS openings at r_0, binary table first
+    uint8_t ev[32];
+    if (nb) ZG_TRY(zg_prove_f_d(pb, t, bin_d, nb, r0.data(), hb.h, ev));
+    if (ni) ZG_TRY(zg_prove_f_d(pi, t, int_d, ni, r0.data(), hi.h, ev));
+
+    // finish (prover.rs:603-650) and the transcription (lib.rs:129-160)
+    const uint64_t *p = f.p;
+    Bytes out;
+    out.put(roots[0], 32);
+    out.u64(nb);
+    out.put(roots[1], 32);
+    out.u64(0);
+    out.put(roots[2], 32);
+    out.u64(ni);
+    out.u32((uint32_t)t->stream.size());
+    out.put(t->stream.data(), t->stream.size());
+    out.sub(poly_vec(ic_vals, p, L));
+    Bytes cpr;
+    cpr.sub(field_vec(cpr_evals.data(), ncols, p, L));
+    cpr.sub(field_vec(cpr_evals.data() + (size_t)ncols * L, S, p, L));
+    out.sub(cpr);
+    Bytes md, mp;
+    md.put(md_proof.data(), md_proof.size());
+    mp.put(mp_proof.data(), mp_proof.size());
+    out.sub(md);
+    out.sub(mp);
+    out.sub(poly_vec(lifted_polys, p, L));
+
+    const size_t cap = *proof_len;
+    *proof_len = out.b.size();
+    if (cap < out.b.size()) {
+        set_error("zinc prove: proof needs %zu bytes, buffer holds %zu", out.b.size(), cap);
+        return ZG_ERR_BUFFER_TOO_SMALL;
+    }
+    std::memcpy(proof, out.b.data(), out.b.size());
+    return ZG_OK;
+}
+
+}  // namespace
+
+extern "C" zg_status zg_zinc_prove_mle_first(zg_params *pp_bin, zg_params *pp_int, const zg_linear_uair *uair,
+                                             uint32_t num_vars, const uint64_t *bin_cols, const int64_t *int_cols,
+                                             int cols_on_device, uint8_t *proof, size_t *proof_len) {
+    try {
+        if (!uair || !proof_len || (*proof_len && !proof) || (uair->n_bin && !bin_cols) ||
+            (uair->n_int && !int_cols) || num_vars == 0 || num_vars > 30) {
+            set_error("zinc prove: null argument or num_vars out of range");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        return prove_mle_first(pp_bin, pp_int, uair, num_vars, bin_cols, int_cols, cols_on_device, proof,
+                               proof_len);
+    } catch (const std::exception &e) {
+        set_error("zinc prove: %s", e.what());
+        return ZG_ERR_OOM;
+    }
+}

@@ -158,6 +158,8 @@ struct zg_ctx {
     zg::DevBuf prove_out; // b partials, combined row + openings
     zg::DevBuf sc_arena;  // sumcheck: staged MLEs, fold buffers, comb tables, partials
     zg::DevBuf piop_arena;  // PIOP step 5: the packed MLEs handed to the sumcheck
+    zg::DevBuf trace_arena; // Zinc+ prover: the trace columns copied from the host
+    zg::DevBuf mle_arena;   // Zinc+ prover: the projected column MLEs (steps 3-5)
     zg::HostBuf pin_in, pin_out;
     // kernel timing
     bool timing = false;

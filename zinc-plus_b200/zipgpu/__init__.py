@@ -50,6 +50,7 @@ EXPORTS = (
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
     "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear", "zg_prove_f", "zg_prove_f_d",
+    "zg_zinc_prove_mle_first",
 )
 
 
@@ -103,6 +104,14 @@ class ServerStats(C.Structure):
                [(n, C.c_double) for n in ("ms_input", "ms_commit", "ms_prime", "ms_prove")]
 
 
+class LinearUairDesc(C.Structure):
+    """Mirror of ``zg_linear_uair``."""
+
+    _fields_ = [("n_bin", C.c_uint32), ("n_int", C.c_uint32), ("degree_plus_one", C.c_uint32),
+                ("n_shifts", C.c_uint32), ("shift_src", C.c_void_p), ("shift_amount", C.c_void_p),
+                ("n_constraints", C.c_uint32), ("coeffs", C.c_void_p)]
+
+
 class SumcheckGroupDesc(C.Structure):
     """Mirror of ``zg_sumcheck_group``."""
 
@@ -141,6 +150,8 @@ def lib() -> C.CDLL:
                                      C.c_uint32, C.c_int, vp, C.POINTER(sz), vp], st),
         "zg_piop_cpr_linear_prove": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp, vp,
                                       C.c_uint32, C.c_uint32, vp, C.c_int, vp, C.POINTER(sz), vp, vp], st),
+        "zg_zinc_prove_mle_first": ([vp, vp, C.POINTER(LinearUairDesc), C.c_uint32, vp, vp, C.c_int, vp,
+                                     C.POINTER(sz)], st),
         "zg_piop_ideal_check_linear": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
                                         C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, C.c_uint32, vp, C.c_int, vp,
                                         vp, vp], st),
@@ -810,6 +821,37 @@ class ZipServer:
             self.close()
         except Exception:
             pass
+
+
+class ZincPlusPiop:
+    """ZincPlusPiop::prove::<MLE_FIRST = true> (protocol/src/prover.rs:677-706)
+    for a linear UAIR over binary-polynomial and integer (i64) witness columns,
+    every step on the GPU; returns the Proof transcription
+    (protocol/src/lib.rs:87-189)."""
+
+    @staticmethod
+    def prove_mle_first(pp_bin, pp_int, nvars: int, bin_cols, degree_plus_one: int, int_cols, shifts,
+                        coeffs) -> bytes:
+        b, i = ZincPiop._cols(bin_cols, int_cols, nvars)
+        src = np.array([s for s, _ in shifts] or [0], np.uint32)
+        amt = np.array([a for _, a in shifts] or [0], np.uint32)
+        cf = np.ascontiguousarray(coeffs, dtype=np.int64)
+        ncols = b.shape[0] + i.shape[0]
+        if cf.ndim != 2 or cf.shape[1] != ncols + len(shifts):
+            raise ValueError("coeffs must be n_constraints x (n_bin + n_int + n_shifts)")
+        u = LinearUairDesc(b.shape[0], i.shape[0], degree_plus_one, len(shifts), src.ctypes.data, amt.ctypes.data,
+                           cf.shape[0], cf.ctypes.data)
+        pbin = pp_bin.handle if pp_bin is not None else None
+        pint = pp_int.handle if pp_int is not None else None
+        cap = 64 << 10
+        for pp in (pp_bin, pp_int):
+            if pp is not None:
+                cap += pp.proof_size(max(b.shape[0], i.shape[0], 1))
+        cap += (ncols * (degree_plus_one + 2) + cf.shape[0] * degree_plus_one + 64 * nvars) * 64
+        buf = C.create_string_buffer(cap)
+        n = C.c_size_t(cap)
+        check(lib().zg_zinc_prove_mle_first(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, buf, C.byref(n)))
+        return buf.raw[: n.value]
 
 
 class ZincPiop:
