@@ -965,8 +965,21 @@ __global__ void __launch_bounds__(256) k_base_int(const TE *__restrict__ evals,
     const uint32_t oct = octet_reverse(ch, depth), shift = 3 * depth;
     const TE *row = evals + (size_t)grow * row_len;
     Acc acc = 0;
-    for (uint32_t c = 0; c < bl; c++)
-        acc += (Acc)__ldg(row + oct + ((size_t)c << shift)) * (Acc)__ldg(bmT + (size_t)c * bd + rb);
+    if (sizeof(TE) == 8 && bl <= (1u << 14)) {
+        // x = hi * 2^32 + lo: with |bm| < 2^16 and bl <= 2^14 both partial sums
+        // stay below 2^62 in magnitude, so two int64 sums are exact
+        int64_t slo = 0, shi = 0;
+        for (uint32_t c = 0; c < bl; c++) {
+            const int64_t x = (int64_t)__ldg(row + oct + ((size_t)c << shift));
+            const int64_t m = __ldg(bmT + (size_t)c * bd + rb);
+            slo += (int64_t)(uint32_t)x * m;
+            shi += (x >> 32) * m;
+        }
+        acc = (Acc)(((i128)shi << 32) + (i128)slo);
+    } else {
+        for (uint32_t c = 0; c < bl; c++)
+            acc += (Acc)__ldg(row + oct + ((size_t)c << shift)) * (Acc)__ldg(bmT + (size_t)c * bd + rb);
+    }
     if (FINAL) {
         i128 *o = static_cast<i128 *>(out);
         o[LEAF_MAJOR ? lm_pos(p, grow, nrows, C, seg_log) : (size_t)grow * C + p] = (i128)acc;

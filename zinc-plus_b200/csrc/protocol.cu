@@ -137,6 +137,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     const uint32_t nb = u->n_bin, ni = u->n_int, ncols = nb + ni, S = u->n_shifts, D = u->degree_plus_one;
     const uint32_t nc = u->n_constraints;
     const size_t n = (size_t)1 << nv;
+    hphase_start(ctx);
 
     // the trace in device memory: binary columns, then integer columns
     const uint64_t *bin_d = bin;
@@ -154,6 +155,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
             bin_d = dst;
             int_d = reinterpret_cast<const int64_t *>(dst + n * nb);
         }
+        hphase(ctx, "zinc:h2d");
     }
 
     // step 0 (prover.rs:218-267): commit each non-empty table; the arbitrary
@@ -166,6 +168,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     TranscriptGuard tg;
     ZG_TRY(zg_transcript_new(&roots[0][0], 3, &tg.t));
     zg_transcript *t = tg.t;
+    hphase(ctx, "zinc:commit");
 
     // step 1 (prover.rs:285-300): the random prime; projection happens inside
     // the steps that read the columns
@@ -174,6 +177,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     const FieldCfg &f = t->f;
     std::vector<uint64_t> coeffs((size_t)nc * (ncols + S) * L);
     for (size_t k = 0; k < (size_t)nc * (ncols + S); k++) f_from_i128(f, (i128)u->coeffs[k], &coeffs[k * L]);
+    hphase(ctx, "zinc:prime");
 
     // step 2 (prover.rs:358-380): ideal check, MLE first
     std::vector<uint64_t> ic_point((size_t)nv * L), combined((size_t)nc * D * L);
@@ -184,6 +188,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     std::vector<std::vector<uint64_t>> ic_vals(nc);
     for (uint32_t k = 0; k < nc; k++)
         ic_vals[k].assign(&combined[(size_t)k * D * L], &combined[(size_t)k * D * L] + (size_t)lens[k] * L);
+    hphase(ctx, "zinc:ideal_check");
 
     // step 3 (prover.rs:385-415): the projecting element a = Chal (i128) in F,
     // the columns evaluated at a, kept on the device for steps 4 and 5
@@ -196,6 +201,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     }
     uint64_t *mles = ctx->mle_arena.as<uint64_t>();
     ZG_TRY(zg_piop_eval_projection(ctx, mod_b, (uint32_t)L, bin_d, nb, D, int_d, ni, nv, a, 1, mles));
+    hphase(ctx, "zinc:eval_projection");
 
     // step 4 (prover.rs:420-472): CPR group + MultiDegreeSumcheck + finalize
     // capacity: modulus, group count, rounds, one degree (3 here, at most 8),
@@ -207,6 +213,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
                                     u->shift_amount, S, nc, coeffs.data(), 1, md_proof.data(), &md_len,
                                     cpr_point.data(), cpr_evals.data()));
     md_proof.resize(md_len);
+    hphase(ctx, "zinc:cpr");
 
     // step 5 (prover.rs:478-492): multipoint evaluation down to r_0
     // capacity: modulus, message count, per round a length and 2 evaluations,
@@ -217,6 +224,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     ZG_TRY(zg_piop_multipoint_eval(ctx, t, mod_b, (uint32_t)L, mles, ncols, nv, cpr_point.data(), u->shift_src,
                                    u->shift_amount, S, 1, mp_proof.data(), &mp_len, r0.data()));
     mp_proof.resize(mp_len);
+    hphase(ctx, "zinc:multipoint");
 
     // step 6 (prover.rs:497-532): lifted evaluations at r_0, trimmed, every
     // coefficient absorbed (absorb_random_field_slice)
@@ -228,15 +236,19 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
         lifted_polys[c] = trimmed(src, c < nb ? D : 1, L);
         for (size_t k = 0; k < lifted_polys[c].size() / L; k++) tr_absorb_field(t, &lifted_polys[c][k * L]);
     }
+    hphase(ctx, "zinc:lifted");
 
     // step 7 (prover.rs:552-597): PCS openings at r_0, binary table first
     uint8_t ev[32];
     if (nb) ZG_TRY(zg_prove_f_d(pb, t, bin_d, nb, r0.data(), hb.h, ev));
     if (ni) ZG_TRY(zg_prove_f_d(pi, t, int_d, ni, r0.data(), hi.h, ev));
+    hphase(ctx, "zinc:prove_f");
 
     // finish (prover.rs:603-650) and the transcription (lib.rs:129-160)
     const uint64_t *p = f.p;
     Bytes out;
+    out.b.reserve(t->stream.size() + 128 + 8 * (size_t)L * (((size_t)nb * D + ni + (size_t)nc * D) + 2 * ncols + S) +
+                  md_proof.size() + mp_proof.size());
     out.put(roots[0], 32);
     out.u64(nb);
     out.put(roots[1], 32);
@@ -264,6 +276,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
         return ZG_ERR_BUFFER_TOO_SMALL;
     }
     std::memcpy(proof, out.b.data(), out.b.size());
+    hphase(ctx, "zinc:finish");
     return ZG_OK;
 }
 

@@ -848,10 +848,11 @@ class ZincPlusPiop:
             if pp is not None:
                 cap += pp.proof_size(max(b.shape[0], i.shape[0], 1))
         cap += (ncols * (degree_plus_one + 2) + cf.shape[0] * degree_plus_one + 64 * nvars) * 64
-        buf = C.create_string_buffer(cap)
+        buf = np.empty(cap, np.uint8)
         n = C.c_size_t(cap)
-        check(lib().zg_zinc_prove_mle_first(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, buf, C.byref(n)))
-        return buf.raw[: n.value]
+        check(lib().zg_zinc_prove_mle_first(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, _ptr(buf),
+                                            C.byref(n)))
+        return buf[: n.value].tobytes()
 
 
 class ZincPiop:
