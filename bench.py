@@ -984,6 +984,17 @@ def run_zinc_prove(Z, ctx, nv, cpu_nv, with_cpu):
     return res
 
 
+def run_zinc_prove_case(nv):
+    """The MLE-first Zinc+ prover on BigLinearUair at 2^nv rows, one warm-up and
+    one timed call: a fixed launch sequence for ncu launch lists."""
+    import zipgpu as Z
+
+    ctx = Z.Context(env_int("LOCAL_RANK", 0))
+    out = run_zinc_prove(Z, ctx, nv, 10, False)
+    print(json.dumps({"zinc_prove_case": {"num_vars": nv, "ms": out["ms"], "proof_bytes": out["proof_bytes"]}}))
+    return 0
+
+
 def run_sumcheck_case(nv):
     """One CPR sumcheck proof (2^nv points, device-resident MLEs), twice: a small,
     fixed launch sequence for ncu captures."""
@@ -1015,6 +1026,8 @@ def main():
                     help="skip the batched-commit and serving measurements")
     ap.add_argument("--sumcheck-case", type=int, metavar="NV",
                     help="only run the CPR sumcheck at 2^NV points (small case for ncu captures)")
+    ap.add_argument("--zinc-prove-case", type=int, metavar="NV",
+                    help="only run the MLE-first Zinc+ prover on BigLinear at 2^NV rows (launch lists)")
     ap.add_argument("--commit-case", type=int, nargs=2, metavar=("NV", "D"),
                     help="only commit one seeded polynomial twice (small case for ncu captures)")
     args = ap.parse_args()
@@ -1024,6 +1037,8 @@ def main():
         return run_commit_case(*args.commit_case)
     if args.sumcheck_case:
         return run_sumcheck_case(args.sumcheck_case)
+    if args.zinc_prove_case:
+        return run_zinc_prove_case(args.zinc_prove_case)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -521,10 +521,14 @@ zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void 
         for (uint32_t j = 0; j < R; j++)
             for (uint32_t q = 0; q < nparts; q++)
                 f_add(f, &bv[(size_t)j * L], hb + (((size_t)b * R + j) * nparts + q) * L);
+    hphase(ctx, "prove_b_reduce");
 
     // write_field_elements(b) (pcs_transcript.rs:99-142): no length prefix for
-    // Uint<L>; modulus | inner per element, each absorbed.
+    // Uint<L>; modulus | inner per element, each absorbed.  The stream grows
+    // by this proof at most once.
     const size_t fb = 8 * (size_t)L;
+    if (t->stream.capacity() < t->stream.size() + zg_proof_size(p, batch))
+        t->stream.reserve(std::max(t->stream.size() + zg_proof_size(p, batch), 2 * t->stream.capacity()));
     for (uint32_t j = 0; j < R; j++) {
         tr_absorb_field(t, &bv[(size_t)j * L]);
         const uint8_t *mod = reinterpret_cast<const uint8_t *>(f.p);
@@ -532,6 +536,7 @@ zg_status prove_device(zg_params *p, zg_ctx *lane, zg_transcript *t, const void 
         t->stream.insert(t->stream.end(), mod, mod + fb);
         t->stream.insert(t->stream.end(), inr, inr + fb);
     }
+    hphase(ctx, "prove_b_absorb");
     uint64_t ev[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
     for (uint32_t j = 0; j < R; j++) {
         uint64_t tmp[MAX_FIELD_LIMBS];

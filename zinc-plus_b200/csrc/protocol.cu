@@ -80,10 +80,17 @@ struct HintGuard {
         if (h) zg_hint_free(h);
     }
 };
+// The PCS stream of a proof is megabytes; the transcript borrows one buffer per
+// thread across calls so that its pages stay mapped (no first-touch faults).
+thread_local std::vector<uint8_t> t_stream_store;
+
 struct TranscriptGuard {
     zg_transcript *t = nullptr;
     ~TranscriptGuard() {
-        if (t) zg_transcript_free(t);
+        if (!t) return;
+        t->stream.clear();
+        t_stream_store.swap(t->stream);
+        zg_transcript_free(t);
     }
 };
 
@@ -168,6 +175,10 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     TranscriptGuard tg;
     ZG_TRY(zg_transcript_new(&roots[0][0], 3, &tg.t));
     zg_transcript *t = tg.t;
+    t_stream_store.clear();
+    t->stream.swap(t_stream_store);
+    // both tables' PCS proofs land in t->stream: size it once
+    t->stream.reserve((nb ? zg_proof_size(pb, nb) : 0) + (ni ? zg_proof_size(pi, ni) : 0));
     hphase(ctx, "zinc:commit");
 
     // step 1 (prover.rs:285-300): the random prime; projection happens inside
@@ -244,38 +255,42 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     if (ni) ZG_TRY(zg_prove_f_d(pi, t, int_d, ni, r0.data(), hi.h, ev));
     hphase(ctx, "zinc:prove_f");
 
-    // finish (prover.rs:603-650) and the transcription (lib.rs:129-160)
+    // finish (prover.rs:603-650) and the transcription (lib.rs:129-160),
+    // written straight into the caller's buffer once its size is known
     const uint64_t *p = f.p;
-    Bytes out;
-    out.b.reserve(t->stream.size() + 128 + 8 * (size_t)L * (((size_t)nb * D + ni + (size_t)nc * D) + 2 * ncols + S) +
-                  md_proof.size() + mp_proof.size());
-    out.put(roots[0], 32);
-    out.u64(nb);
-    out.put(roots[1], 32);
-    out.u64(0);
-    out.put(roots[2], 32);
-    out.u64(ni);
-    out.u32((uint32_t)t->stream.size());
-    out.put(t->stream.data(), t->stream.size());
-    out.sub(poly_vec(ic_vals, p, L));
+    const Bytes ic_b = poly_vec(ic_vals, p, L), lifted_b = poly_vec(lifted_polys, p, L);
     Bytes cpr;
     cpr.sub(field_vec(cpr_evals.data(), ncols, p, L));
     cpr.sub(field_vec(cpr_evals.data() + (size_t)ncols * L, S, p, L));
-    out.sub(cpr);
-    Bytes md, mp;
-    md.put(md_proof.data(), md_proof.size());
-    mp.put(mp_proof.data(), mp_proof.size());
-    out.sub(md);
-    out.sub(mp);
-    out.sub(poly_vec(lifted_polys, p, L));
-
+    const size_t total = 3 * 40 + 4 + t->stream.size() + 4 + ic_b.b.size() + 4 + cpr.b.size() + 4 + md_proof.size() +
+                         4 + mp_proof.size() + 4 + lifted_b.b.size();
     const size_t cap = *proof_len;
-    *proof_len = out.b.size();
-    if (cap < out.b.size()) {
-        set_error("zinc prove: proof needs %zu bytes, buffer holds %zu", out.b.size(), cap);
+    *proof_len = total;
+    if (cap < total) {
+        set_error("zinc prove: proof needs %zu bytes, buffer holds %zu", total, cap);
         return ZG_ERR_BUFFER_TOO_SMALL;
     }
-    std::memcpy(proof, out.b.data(), out.b.size());
+    uint8_t *w = proof;
+    auto put = [&](const void *src, size_t len) {
+        if (len) std::memcpy(w, src, len);
+        w += len;
+    };
+    auto put_u32 = [&](uint32_t v) { put(&v, 4); };
+    auto put_sub = [&](const uint8_t *src, size_t len) {
+        put_u32((uint32_t)len);
+        put(src, len);
+    };
+    const uint64_t batches[3] = {nb, 0, ni};
+    for (int k = 0; k < 3; k++) {
+        put(roots[k], 32);
+        put(&batches[k], 8);
+    }
+    put_sub(t->stream.data(), t->stream.size());
+    put_sub(ic_b.b.data(), ic_b.b.size());
+    put_sub(cpr.b.data(), cpr.b.size());
+    put_sub(md_proof.data(), md_proof.size());
+    put_sub(mp_proof.data(), mp_proof.size());
+    put_sub(lifted_b.b.data(), lifted_b.b.size());
     hphase(ctx, "zinc:finish");
     return ZG_OK;
 }

@@ -829,6 +829,8 @@ class ZincPlusPiop:
     every step on the GPU; returns the Proof transcription
     (protocol/src/lib.rs:87-189)."""
 
+    _out = None  # output buffer reused across calls (one call at a time)
+
     @staticmethod
     def prove_mle_first(pp_bin, pp_int, nvars: int, bin_cols, degree_plus_one: int, int_cols, shifts,
                         coeffs) -> bytes:
@@ -848,8 +850,10 @@ class ZincPlusPiop:
             if pp is not None:
                 cap += pp.proof_size(max(b.shape[0], i.shape[0], 1))
         cap += (ncols * (degree_plus_one + 2) + cf.shape[0] * degree_plus_one + 64 * nvars) * 64
-        buf = np.empty(cap, np.uint8)
-        n = C.c_size_t(cap)
+        buf = ZincPlusPiop._out
+        if buf is None or buf.size < cap:
+            buf = ZincPlusPiop._out = np.empty(cap, np.uint8)
+        n = C.c_size_t(buf.size)
         check(lib().zg_zinc_prove_mle_first(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, _ptr(buf),
                                             C.byref(n)))
         return buf[: n.value].tobytes()
