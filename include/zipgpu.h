@@ -482,10 +482,16 @@ zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, const uint8_t *
 
 /* ---- Zinc+ prover, MLE first (ZincPlusPiop::prove::<MLE_FIRST = true>,
  * protocol/src/prover.rs:677-706) ------------------------------------------
- * A linear UAIR over binary-polynomial and integer witness columns (no public
- * and no arbitrary-polynomial columns; lookups are a placeholder in the
- * reference), e.g. BigLinearUair (test-uair/src/lib.rs:325-382: 16
- * BinaryPoly<32> columns, 1 integer column, 16 shifts by 1, 17 constraints).
+ * A linear UAIR over binary-polynomial and integer columns (no arbitrary-
+ * polynomial columns; lookups are a placeholder in the reference), e.g.
+ * BigLinearUair (test-uair/src/lib.rs:325-382: 16 BinaryPoly<32> columns, 1
+ * integer column, 16 shifts by 1, 17 constraints) or
+ * BigLinearUairWithPublicInput (:458-489, its first 4 binary columns public).
+ * The first n_pub_bin binary and the first n_pub_int integer columns are
+ * public (UairTrace::public, uair/src/lib.rs:328-346): they are not committed
+ * or opened, each of their entries is absorbed as 8 LE bytes after the roots
+ * (absorb_public_columns, protocol/src/lib.rs:305-320), and their lifted
+ * evaluations stay out of the proof.
  * Constraint k is sum_j coeffs[k][j] * col_j over [binary up, integer up, down
  * (shifted) columns in shift order]; shift sources index the up columns, binary
  * first.  Runs step 0 (commit both tables, absorb the roots of the binary, the
@@ -494,8 +500,9 @@ zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, const uint8_t *
  * table at r_0) and writes the Proof transcription (protocol/src/lib.rs:87-189:
  * three commitments, the PCS stream, ideal check, resolver, multi-degree
  * sumcheck, multipoint evaluation, witness lifted evaluations).
- * pp_bin: BINPOLY parameters of num_vars (NULL when n_bin == 0); pp_int:
- * ZG_EVAL_I64 parameters of num_vars (NULL when n_int == 0), both with a device
+ * pp_bin: BINPOLY parameters of num_vars (NULL when no binary column is a
+ * witness); pp_int: ZG_EVAL_I64 parameters of num_vars (NULL when no integer
+ * column is a witness), both with a device
  * and one context.  bin_cols: n_bin columns of 2^num_vars u64, column after
  * column; int_cols: n_int columns of 2^num_vars i64 (device pointers when
  * cols_on_device != 0).  proof_len: in capacity, out size. */
@@ -508,6 +515,8 @@ typedef struct {
     const uint32_t *shift_amount;
     uint32_t n_constraints;
     const int64_t *coeffs; /* n_constraints x (n_bin + n_int + n_shifts) */
+    uint32_t n_pub_bin;    /* public binary columns (the first ones), <= n_bin */
+    uint32_t n_pub_int;    /* public integer columns (the first ones), <= n_int */
 } zg_linear_uair;
 
 zg_status zg_zinc_prove_mle_first(zg_params *pp_bin, zg_params *pp_int, const zg_linear_uair *uair,

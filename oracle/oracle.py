@@ -646,7 +646,7 @@ def _sub(b: bytes) -> bytes:
 
 
 def zinc_prove_mle_first(desc_bin: Desc, desc_int: Desc, nvars: int, bin_cols, D: int, int_cols, shifts, coeffs,
-                         L: int) -> bytes:
+                         L: int, n_pub_bin: int = 0, n_pub_int: int = 0) -> bytes:
     """ZincPlusPiop::prove::<MLE_FIRST = true> (protocol/src/prover.rs:677-706)
     for a linear UAIR over binary-polynomial and i64 witness columns, chaining
     the oracle's steps on one transcript: step 0 commitments (prover.rs:218-267;
@@ -655,17 +655,25 @@ def zinc_prove_mle_first(desc_bin: Desc, desc_int: Desc, nvars: int, bin_cols, D
     projection, step 4 CPR, step 5 multipoint, step 6 lifted evaluations
     (trimmed, each coefficient absorbed), step 7 prove_f per table, and the
     Proof transcription (protocol/src/lib.rs:129-160).  coeffs: integer
-    constraint coefficients over [binary up, integer up, down]."""
+    constraint coefficients over [binary up, integer up, down].  The first
+    n_pub_bin / n_pub_int columns of each table are public (UairTrace::public,
+    uair/src/lib.rs:328-346): not committed or opened, their entries absorbed
+    as 8 LE bytes each after the roots (absorb_public_columns, lib.rs:305-320),
+    their lifted evaluations left out of the proof (prover.rs:614-632)."""
     b, i = _piop_cols(bin_cols, int_cols, nvars)
     nb, ni = b.shape[0], i.shape[0]
+    wb, wi = nb - n_pub_bin, ni - n_pub_int
     roots = [b"\0" * 32, b"\0" * 32, b"\0" * 32]
-    if nb:
-        roots[0] = commit(desc_bin, b, nb)
-    if ni:
-        roots[2] = commit(desc_int, i, ni)
+    if wb:
+        roots[0] = commit(desc_bin, b[n_pub_bin:], wb)
+    if wi:
+        roots[2] = commit(desc_int, i[n_pub_int:], wi)
     t = Transcript()
     for r in roots:
         t.absorb_slice(r)
+    for col in list(b[:n_pub_bin]) + list(i[:n_pub_int]):
+        for e in np.ascontiguousarray(col).view(np.uint8).reshape(-1, 8):
+            t.absorb_slice(e.tobytes())
     p = t.get_prime(L)
     R = 1 << (64 * L)
     cf = [[int(c) % p for c in row] for row in coeffs]
@@ -681,16 +689,16 @@ def zinc_prove_mle_first(desc_bin: Desc, desc_int: Desc, nvars: int, bin_cols, D
         for e in q:
             t.absorb_field(p, L, e)
     zip_ = b""
-    if nb:
-        zip_ += prove_f_on(desc_bin, b, nb, t, p, r0)[0]
-    if ni:
-        zip_ += prove_f_on(desc_int, i, ni, t, p, r0)[0]
+    if wb:
+        zip_ += prove_f_on(desc_bin, b[n_pub_bin:], wb, t, p, r0)[0]
+    if wi:
+        zip_ += prove_f_on(desc_int, i[n_pub_int:], wi, t, p, r0)[0]
     S = len(shifts)
     vec = lambda rows: (_limbs(p, L).tobytes() + np.ascontiguousarray(rows, np.uint64).tobytes()) if len(rows) else b""
-    out = roots[0] + int(nb).to_bytes(8, "little") + roots[1] + bytes(8) + roots[2] + int(ni).to_bytes(8, "little")
+    out = roots[0] + int(wb).to_bytes(8, "little") + roots[1] + bytes(8) + roots[2] + int(wi).to_bytes(8, "little")
     out += _sub(zip_)
     out += _sub(_poly_vec_bytes(list(combined), p, L))
     out += _sub(_sub(vec(evals[:nb + ni])) + _sub(vec(evals[nb + ni:nb + ni + S])))
     out += _sub(md) + _sub(mp)
-    out += _sub(_poly_vec_bytes(polys, p, L))
+    out += _sub(_poly_vec_bytes(polys[n_pub_bin:nb] + polys[nb + n_pub_int:], p, L))
     return out

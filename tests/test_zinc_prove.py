@@ -129,6 +129,11 @@ def test_oracle_proof_layout(zipgpu, oracle):
     assert oracle.is_probable_prime_base2(P["modulus"], 3) and P["modulus"].bit_length() <= 192
     # the PCS stream: two prove_f transcripts (binary table, then integer table)
     assert len(P["zip"]) == oracle.proof_size(db, 16) + oracle.proof_size(di, 1)
+    # BigLinearUairWithPublicInput: 4 public binary columns, neither committed nor in the proof
+    Q = parse_proof(oracle.zinc_prove_mle_first(db, di, nv, bins, 32, ints, shifts, coeffs, 3, n_pub_bin=4), 3, nv)
+    assert Q["comms"][0] == (oracle.commit(db, bins[4:], 12), 12) and len(Q["lifted"]) == 13
+    assert len(Q["zip"]) == oracle.proof_size(db, 12) + oracle.proof_size(di, 1)
+    assert Q["modulus"] != P["modulus"]  # the public entries are absorbed before the prime
 
 
 def test_driver_rejects_bad_arguments(zipgpu):
@@ -172,19 +177,43 @@ def test_gpu_biglinear_proof_matches_oracle(zipgpu, oracle, ctx, nv, seed):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("nv", [6, 9])
+def test_gpu_biglinear_public_input_matches_oracle(zipgpu, oracle, ctx, nv):
+    """BigLinearUairWithPublicInput (test-uair/src/lib.rs:458-489): the first
+    four binary columns are public."""
+    from zipgpu import uair
+
+    bins, ints = uair.trace(nv, 21)
+    shifts, coeffs = uair.signature()
+    pb, pi, db, di = tables(zipgpu, nv, 32, ctx)
+    got = zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs, n_pub_bin=4)
+    want = oracle.zinc_prove_mle_first(db, di, nv, bins, 32, ints, shifts, coeffs, 3, n_pub_bin=4)
+    assert got == want
+    P = parse_proof(got, 3, nv)
+    assert P["comms"][0][1] == 12 and len(P["lifted"]) == 13
+    # the public columns change the transcript: a different proof than without them
+    assert got != zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("nb,ni,shifts,nc,D", [
     (3, 2, [(0, 1), (3, 2), (4, 1)], 4, 8),
     (2, 0, [(1, 3)], 2, 32),           # binary table only
     (0, 2, [(0, 1), (1, 1)], 3, 8),    # integer table only
     (1, 1, [], 1, 64),                 # no shifts
+    (2, 3, [(0, 1), (2, 1)], 3, 16),   # public: 1 binary, 2 integer columns
+    (1, 2, [(1, 2)], 2, 8),            # every binary column public
 ])
 def test_gpu_small_uairs_match_oracle(zipgpu, oracle, ctx, nb, ni, shifts, nc, D):
     nv = 7
+    npb, npi = {(2, 3): (1, 2), (1, 2): (1, 0)}.get((nb, ni), (0, 0))
     rng = np.random.default_rng(nb * 100 + ni * 10 + nc)
     bins, ints, coeffs = small_uair(rng, nb, ni, shifts, nc, D, nv)
     pb, pi, db, di = tables(zipgpu, nv, D, ctx)
-    got = zipgpu.ZincPlusPiop.prove_mle_first(pb if nb else None, pi if ni else None, nv,
-                                              bins if nb else None, D, ints if ni else None, shifts, coeffs)
-    want = oracle.zinc_prove_mle_first(db, di, nv, bins if nb else None, D, ints if ni else None, shifts, coeffs, 3)
+    got = zipgpu.ZincPlusPiop.prove_mle_first(pb if nb > npb else None, pi if ni > npi else None, nv,
+                                              bins if nb else None, D, ints if ni else None, shifts, coeffs,
+                                              n_pub_bin=npb, n_pub_int=npi)
+    want = oracle.zinc_prove_mle_first(db, di, nv, bins if nb else None, D, ints if ni else None, shifts, coeffs, 3,
+                                       n_pub_bin=npb, n_pub_int=npi)
     assert got == want
     parse_proof(got, 3, nv)

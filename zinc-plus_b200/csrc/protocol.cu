@@ -100,8 +100,16 @@ zg_status check_uair(const zg_params *pb, const zg_params *pi, const zg_linear_u
         set_error("zinc prove: empty UAIR or null constraint/shift arrays");
         return ZG_ERR_INVALID_PARAM;
     }
-    if ((u->n_bin && !pb) || (u->n_int && !pi)) {
-        set_error("zinc prove: parameters missing for a non-empty column table");
+    if (u->n_pub_bin > u->n_bin || u->n_pub_int > u->n_int) {
+        set_error("zinc prove: more public than total columns");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if ((u->n_bin > u->n_pub_bin && !pb) || (u->n_int > u->n_pub_int && !pi)) {
+        set_error("zinc prove: parameters missing for a table with witness columns");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (!pb && !pi) {
+        set_error("zinc prove: no parameters (every column is public)");
         return ZG_ERR_INVALID_PARAM;
     }
     const zg_params *any = pb ? pb : pi;
@@ -143,6 +151,8 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     const int L = (int)any->d.field_limbs;
     const uint32_t nb = u->n_bin, ni = u->n_int, ncols = nb + ni, S = u->n_shifts, D = u->degree_plus_one;
     const uint32_t nc = u->n_constraints;
+    const uint32_t pbn = u->n_pub_bin, pin = u->n_pub_int;  // public columns
+    const uint32_t wb = nb - pbn, wi = ni - pin;             // witness columns
     const size_t n = (size_t)1 << nv;
     hphase_start(ctx);
 
@@ -165,20 +175,39 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
         hphase(ctx, "zinc:h2d");
     }
 
-    // step 0 (prover.rs:218-267): commit each non-empty table; the arbitrary
-    // polynomial table is empty (default root, batch 0); absorb the three roots
+    // step 0 (prover.rs:218-267): commit the witness columns of each table
+    // (commit_optionally: an empty table has the default root and batch 0; the
+    // arbitrary polynomial table is empty), absorb the three roots, then every
+    // entry of the public columns (absorb_public_columns, lib.rs:305-320)
+    const uint64_t *wbin_d = bin_d + n * pbn;
+    const int64_t *wint_d = int_d + n * pin;
     HintGuard hb, hi;
     uint8_t roots[3][32];
     std::memset(roots, 0, sizeof roots);
-    if (nb) ZG_TRY(zg_commit_d(pb, bin_d, nb, &hb.h, roots[0]));
-    if (ni) ZG_TRY(zg_commit_d(pi, int_d, ni, &hi.h, roots[2]));
+    if (wb) ZG_TRY(zg_commit_d(pb, wbin_d, wb, &hb.h, roots[0]));
+    if (wi) ZG_TRY(zg_commit_d(pi, wint_d, wi, &hi.h, roots[2]));
     TranscriptGuard tg;
     ZG_TRY(zg_transcript_new(&roots[0][0], 3, &tg.t));
     zg_transcript *t = tg.t;
     t_stream_store.clear();
     t->stream.swap(t_stream_store);
+    if (pbn + pin) {
+        std::vector<uint64_t> pub;
+        const uint64_t *hb_pub = bin, *hi_pub = reinterpret_cast<const uint64_t *>(ints);
+        if (on_device) {
+            pub.resize(n * (pbn + pin));
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            ZG_CUDA(cudaSetDevice(ctx->device));
+            if (pbn) ZG_CUDA(cudaMemcpy(pub.data(), bin_d, n * 8 * pbn, cudaMemcpyDeviceToHost));
+            if (pin) ZG_CUDA(cudaMemcpy(pub.data() + n * pbn, int_d, n * 8 * pin, cudaMemcpyDeviceToHost));
+            hb_pub = pub.data();
+            hi_pub = pub.data() + n * pbn;
+        }
+        for (size_t k = 0; k < n * pbn; k++) tr_absorb_slice(t, &hb_pub[k], 8);
+        for (size_t k = 0; k < n * pin; k++) tr_absorb_slice(t, &hi_pub[k], 8);
+    }
     // both tables' PCS proofs land in t->stream: size it once
-    t->stream.reserve((nb ? zg_proof_size(pb, nb) : 0) + (ni ? zg_proof_size(pi, ni) : 0));
+    t->stream.reserve((wb ? zg_proof_size(pb, wb) : 0) + (wi ? zg_proof_size(pi, wi) : 0));
     hphase(ctx, "zinc:commit");
 
     // step 1 (prover.rs:285-300): the random prime; projection happens inside
@@ -251,14 +280,17 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
 
     // step 7 (prover.rs:552-597): PCS openings at r_0, binary table first
     uint8_t ev[32];
-    if (nb) ZG_TRY(zg_prove_f_d(pb, t, bin_d, nb, r0.data(), hb.h, ev));
-    if (ni) ZG_TRY(zg_prove_f_d(pi, t, int_d, ni, r0.data(), hi.h, ev));
+    if (wb) ZG_TRY(zg_prove_f_d(pb, t, wbin_d, wb, r0.data(), hb.h, ev));
+    if (wi) ZG_TRY(zg_prove_f_d(pi, t, wint_d, wi, r0.data(), hi.h, ev));
     hphase(ctx, "zinc:prove_f");
 
     // finish (prover.rs:603-650) and the transcription (lib.rs:129-160),
     // written straight into the caller's buffer once its size is known
     const uint64_t *p = f.p;
-    const Bytes ic_b = poly_vec(ic_vals, p, L), lifted_b = poly_vec(lifted_polys, p, L);
+    // witness lifted evaluations: public columns come first in each table
+    std::vector<std::vector<uint64_t>> witness_lifted(lifted_polys.begin() + pbn, lifted_polys.begin() + nb);
+    witness_lifted.insert(witness_lifted.end(), lifted_polys.begin() + nb + pin, lifted_polys.end());
+    const Bytes ic_b = poly_vec(ic_vals, p, L), lifted_b = poly_vec(witness_lifted, p, L);
     Bytes cpr;
     cpr.sub(field_vec(cpr_evals.data(), ncols, p, L));
     cpr.sub(field_vec(cpr_evals.data() + (size_t)ncols * L, S, p, L));
@@ -280,7 +312,7 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
         put_u32((uint32_t)len);
         put(src, len);
     };
-    const uint64_t batches[3] = {nb, 0, ni};
+    const uint64_t batches[3] = {wb, 0, wi};
     for (int k = 0; k < 3; k++) {
         put(roots[k], 32);
         put(&batches[k], 8);

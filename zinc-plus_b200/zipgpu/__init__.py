@@ -109,7 +109,8 @@ class LinearUairDesc(C.Structure):
 
     _fields_ = [("n_bin", C.c_uint32), ("n_int", C.c_uint32), ("degree_plus_one", C.c_uint32),
                 ("n_shifts", C.c_uint32), ("shift_src", C.c_void_p), ("shift_amount", C.c_void_p),
-                ("n_constraints", C.c_uint32), ("coeffs", C.c_void_p)]
+                ("n_constraints", C.c_uint32), ("coeffs", C.c_void_p), ("n_pub_bin", C.c_uint32),
+                ("n_pub_int", C.c_uint32)]
 
 
 class SumcheckGroupDesc(C.Structure):
@@ -833,7 +834,8 @@ class ZincPlusPiop:
 
     @staticmethod
     def prove_mle_first(pp_bin, pp_int, nvars: int, bin_cols, degree_plus_one: int, int_cols, shifts,
-                        coeffs) -> bytes:
+                        coeffs, n_pub_bin: int = 0, n_pub_int: int = 0) -> bytes:
+        """The first n_pub_bin binary and n_pub_int integer columns are public."""
         b, i = ZincPiop._cols(bin_cols, int_cols, nvars)
         src = np.array([s for s, _ in shifts] or [0], np.uint32)
         amt = np.array([a for _, a in shifts] or [0], np.uint32)
@@ -842,7 +844,7 @@ class ZincPlusPiop:
         if cf.ndim != 2 or cf.shape[1] != ncols + len(shifts):
             raise ValueError("coeffs must be n_constraints x (n_bin + n_int + n_shifts)")
         u = LinearUairDesc(b.shape[0], i.shape[0], degree_plus_one, len(shifts), src.ctypes.data, amt.ctypes.data,
-                           cf.shape[0], cf.ctypes.data)
+                           cf.shape[0], cf.ctypes.data, n_pub_bin, n_pub_int)
         pbin = pp_bin.handle if pp_bin is not None else None
         pint = pp_int.handle if pp_int is not None else None
         cap = 64 << 10
