@@ -3,6 +3,7 @@
 // 62-189).  Every step runs on the GPU through the entry points of api.cu and
 // piop.cu; this file holds the sequencing, the host-side Fiat-Shamir glue
 // between the steps and the byte layout of the proof.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -26,7 +27,6 @@ struct Bytes {
         b.insert(b.end(), q, q + n);
     }
     void u32(uint32_t v) { put(&v, 4); }
-    void u64(uint64_t v) { put(&v, 8); }
     // write_transcription_bytes_subset of a Transcribable with a u32 length
     // prefix (transcript/src/traits.rs:48-75): the byte length, then the bytes.
     void sub(const Bytes &x) {
@@ -165,9 +165,29 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
             ZG_CUDA(cudaSetDevice(ctx->device));
             ZG_TRY(ctx->trace_arena.ensure(n * 8 * ncols + 16));
             uint64_t *dst = ctx->trace_arena.as<uint64_t>();
-            if (nb) ZG_CUDA(cudaMemcpyAsync(dst, bin, n * 8 * nb, cudaMemcpyHostToDevice, ctx->stream));
-            if (ni)
-                ZG_CUDA(cudaMemcpyAsync(dst + n * nb, ints, n * 8 * ni, cudaMemcpyHostToDevice, ctx->stream));
+            // through page-locked staging: chunk k is copied on all host threads
+            // while chunk k - 1 is in flight to the device
+            const size_t bin_bytes = n * 8 * nb, total = n * 8 * ncols, chunk = (size_t)4 << 20;
+            ZG_TRY(ctx->pin_in.ensure(total));
+            uint8_t *stage = ctx->pin_in.as<uint8_t>();
+            for (size_t off = 0; off < total; off += chunk) {
+                const size_t len = std::min(chunk, total - off);
+                const long parts = (long)((len + 65535) / 65536);
+#pragma omp parallel for schedule(static)
+                for (long q = 0; q < parts; q++) {
+                    const size_t a = off + (size_t)q * 65536, e = std::min(a + 65536, off + len);
+                    for (size_t x = a; x < e;) {  // the span may cross from the binary to the integer columns
+                        const bool in_bin = x < bin_bytes;
+                        const size_t stop = in_bin ? std::min(e, bin_bytes) : e;
+                        const uint8_t *src = in_bin ? reinterpret_cast<const uint8_t *>(bin) + x
+                                                    : reinterpret_cast<const uint8_t *>(ints) + (x - bin_bytes);
+                        std::memcpy(stage + x, src, stop - x);
+                        x = stop;
+                    }
+                }
+                ZG_CUDA(cudaMemcpyAsync(reinterpret_cast<uint8_t *>(dst) + off, stage + off, len,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+            }
             ZG_CUDA(ctx_sync(ctx));
             bin_d = dst;
             int_d = reinterpret_cast<const int64_t *>(dst + n * nb);
