@@ -347,6 +347,36 @@ __global__ void __launch_bounds__(256) k_precombine(const uint64_t *__restrict__
     }
 }
 
+// partials[k][blockIdx.x] = sum over this block's share of b of eq[b] * mles[k][b]
+// (grid: (blocks per MLE, MLEs)); lazy sums, one reduction per block.
+template <int L>
+__global__ void __launch_bounds__(256) k_mle_dots(const uint64_t *__restrict__ mles, uint32_t nv,
+                                                  const uint64_t *__restrict__ eq, FieldCfg f,
+                                                  uint64_t *__restrict__ partials) {
+    __shared__ Lazy<L> red[256];
+    const size_t n = (size_t)1 << nv;
+    const uint64_t *v = mles + ((size_t)blockIdx.y << nv) * L;
+    Lazy<L> z;
+    lazy_zero(z);
+    for (size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x; b < n; b += (size_t)gridDim.x * blockDim.x) {
+        uint64_t t[L];
+        fmul<L>(eq + b * L, v + b * L, f.p, f.n0, t);
+        lazy_add<L>(z, t);
+    }
+    red[threadIdx.x] = z;
+    __syncthreads();
+    for (unsigned h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) lazy_merge<L>(red[threadIdx.x], red[threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        uint64_t r[L];
+        lazy_reduce<L>(red[0], f, r);
+#pragma unroll
+        for (int w = 0; w < L; w++) partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * L + w] = r[w];
+    }
+}
+
 struct PiopCols {
     const uint64_t *bin;
     uint32_t n_bin, D;
@@ -527,33 +557,48 @@ void field_challenge_h(zg_transcript *t, const FieldCfg &f, uint64_t *out) {
 template <int L>
 zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, const uint64_t *trace,
                              uint32_t ncols, uint32_t nv, const uint64_t *point, const uint32_t *src,
-                             const uint32_t *shift, uint32_t S, int on_device, std::vector<uint64_t> &alphas,
+                             const uint32_t *shift, uint32_t S, int on_device, uint32_t *n_amounts,
                              uint64_t **packed) {
     cudaStream_t s = ctx->stream;
     const size_t n = (size_t)1 << nv, fb = 8 * L, mle = n * fb;
-    alphas.assign((size_t)S * L, 0);
-    std::vector<uint64_t> gammas((size_t)ncols * L);
+    std::vector<uint64_t> alphas((size_t)S * L, 0), gammas((size_t)ncols * L);
     for (uint32_t k = 0; k < S; k++) field_challenge_h<L>(t, f, &alphas[(size_t)k * L]);
     for (uint32_t j = 0; j < ncols; j++) field_challenge_h<L>(t, f, &gammas[(size_t)j * L]);
+    // sum_k alpha_k next_{c_k} v_{src_k} = sum_c next_c (sum_{k: c_k = c} alpha_k v_{src_k}):
+    // one selector and one weighted column combination per distinct shift amount
+    std::vector<uint32_t> amounts;
+    std::vector<uint64_t> weights;  // per distinct amount: ncols inners
+    for (uint32_t k = 0; k < S; k++) {
+        uint32_t m = 0;
+        while (m < amounts.size() && amounts[m] != shift[k]) m++;
+        if (m == amounts.size()) {
+            amounts.push_back(shift[k]);
+            weights.resize(weights.size() + (size_t)ncols * L, 0);
+        }
+        fadd<L>(&weights[((size_t)m * ncols + src[k]) * L], &alphas[(size_t)k * L], f.p);
+    }
+    const uint32_t M = (uint32_t)amounts.size();
+    *n_amounts = M;
     std::vector<uint64_t> omr((size_t)nv * L);
     for (uint32_t k = 0; k < nv; k++) {
         std::memcpy(&omr[(size_t)k * L], f.one, fb);
         fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
     }
     const size_t halves = ((size_t)1 << (nv / 2)) + ((size_t)1 << (nv - nv / 2));
-    const size_t npk = 2 + 2 * (size_t)S;
+    const size_t npk = 2 + 2 * (size_t)M;
     const size_t staged = on_device ? 0 : (size_t)ncols * mle;
-    const size_t small = (2 * (size_t)nv + halves + ncols) * fb;
+    const size_t small = (2 * (size_t)nv + halves + ncols * (1 + (size_t)M)) * fb;
     ZG_TRY(ctx->piop_arena.ensure(npk * mle + staged + small + 256));
     uint8_t *ar = ctx->piop_arena.as<uint8_t>();
     uint64_t *pk = reinterpret_cast<uint64_t *>(ar);
     const uint64_t *tr = on_device ? trace : reinterpret_cast<const uint64_t *>(ar + npk * mle);
     uint64_t *r_d = reinterpret_cast<uint64_t *>(ar + npk * mle + staged), *omr_d = r_d + (size_t)nv * L;
-    uint64_t *half_d = omr_d + (size_t)nv * L, *gam_d = half_d + halves * L;
+    uint64_t *half_d = omr_d + (size_t)nv * L, *gam_d = half_d + halves * L, *wgt_d = gam_d + (size_t)ncols * L;
     if (!on_device) ZG_CUDA(cudaMemcpyAsync(const_cast<uint64_t *>(tr), trace, staged, cudaMemcpyHostToDevice, s));
     ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)nv * fb, cudaMemcpyHostToDevice, s));
     ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)nv * fb, cudaMemcpyHostToDevice, s));
     ZG_CUDA(cudaMemcpyAsync(gam_d, gammas.data(), (size_t)ncols * fb, cudaMemcpyHostToDevice, s));
+    if (M) ZG_CUDA(cudaMemcpyAsync(wgt_d, weights.data(), weights.size() * 8, cudaMemcpyHostToDevice, s));
     uint64_t *eq = pk;  // MLE 0
     ZG_KBEGIN(ctx, s, "k_eq_halves");
     k_eq_halves<L><<<(unsigned)((halves + 127) / 128), 128, 0, s>>>(r_d, omr_d, nv, f, half_d);
@@ -563,25 +608,30 @@ zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, c
     k_eq_outer<L><<<grid, 256, 0, s>>>(half_d, nv, f, eq);
     ZG_KEND(ctx, s);
     // next_c(r', b) = 0 for b < c, eq(r', b - c) for b >= c (build_next_c_r_mle,
-    // poly/src/utils.rs:207-236); the down columns are the shifts' source columns
-    for (uint32_t k = 0; k < S; k++) {
-        uint64_t *nx = pk + (size_t)(1 + k) * n * L;
-        const size_t c = shift[k];
+    // poly/src/utils.rs:207-236), one per distinct shift amount, each paired with
+    // its weighted combination of the source columns
+    for (uint32_t m = 0; m < M; m++) {
+        uint64_t *nx = pk + (size_t)(1 + m) * n * L;
+        const size_t c = amounts[m];
         if (c) ZG_CUDA(cudaMemsetAsync(nx, 0, c * fb, s));
         ZG_CUDA(cudaMemcpyAsync(nx + c * L, eq, (n - c) * fb, cudaMemcpyDeviceToDevice, s));
-        ZG_CUDA(cudaMemcpyAsync(pk + (size_t)(2 + S + k) * n * L, tr + (size_t)src[k] * n * L, mle,
-                                cudaMemcpyDeviceToDevice, s));
     }
     ZG_KBEGIN(ctx, s, "k_precombine");
-    k_precombine<L><<<grid, 256, 0, s>>>(tr, ncols, nv, gam_d, f, pk + (size_t)(1 + S) * n * L);
+    k_precombine<L><<<grid, 256, 0, s>>>(tr, ncols, nv, gam_d, f, pk + (size_t)(1 + M) * n * L);
+    for (uint32_t m = 0; m < M; m++)
+        k_precombine<L><<<grid, 256, 0, s>>>(tr, ncols, nv, wgt_d + (size_t)m * ncols * L, f,
+                                             pk + (size_t)(2 + M + m) * n * L);
     ZG_KEND(ctx, s);
     ZG_CUDA(ctx_sync(ctx));
     *packed = pk;
     return ZG_OK;
 }
 
+// Blocks per column of the CPR's closing dot products (and their partials).
+constexpr size_t kCprDotBlocks = 64;
+
 // Step 4 for a linear UAIR up to the sumcheck: the folding challenge and the
-// packed MLEs [last-row selector, eq_r, up_1 .. up_J, down_1 .. down_S] in
+// packed MLEs [last-row selector, eq_r, f, up_1 .. up_J, down_1 .. down_S] in
 // ctx->piop_arena (combined_poly_resolver.rs:71-178).  coeffs: n_cons x (J + S)
 // Montgomery inners (constraint k's coefficients over up then down columns);
 // folded_out: J + S inners A_j = sum_k alpha^k coeffs[k][j].
@@ -612,14 +662,14 @@ zg_status cpr_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, const ui
         fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
     }
     const size_t halves = ((size_t)1 << (nv / 2)) + ((size_t)1 << (nv - nv / 2));
-    const size_t npk = 2 + (size_t)J + S;
-    const size_t small = (2 * (size_t)nv + halves) * fb;
+    const size_t npk = 3 + (size_t)J + S;
+    const size_t small = (2 * (size_t)nv + halves + (size_t)(J + S) * (1 + kCprDotBlocks)) * fb;
     ZG_TRY(ctx->piop_arena.ensure(npk * mle + small + 256));
     uint8_t *ar = ctx->piop_arena.as<uint8_t>();
     uint64_t *pk = reinterpret_cast<uint64_t *>(ar);
     uint64_t *r_d = reinterpret_cast<uint64_t *>(ar + npk * mle), *omr_d = r_d + (size_t)nv * L;
-    uint64_t *half_d = omr_d + (size_t)nv * L;
-    uint64_t *up = pk + 2 * n * L, *down = up + (size_t)J * n * L;
+    uint64_t *half_d = omr_d + (size_t)nv * L, *fold_d = half_d + halves * L;
+    uint64_t *up = pk + 3 * n * L, *down = up + (size_t)J * n * L;
     ZG_CUDA(cudaMemcpyAsync(up, trace, (size_t)J * mle, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                             s));
     ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)nv * fb, cudaMemcpyHostToDevice, s));
@@ -641,8 +691,57 @@ zg_status cpr_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, const ui
         ZG_CUDA(cudaMemcpyAsync(dk, up + ((size_t)src[k] * n + c) * L, (n - c) * fb, cudaMemcpyDeviceToDevice, s));
         if (c) ZG_CUDA(cudaMemsetAsync(dk + (n - c) * L, 0, c * fb, s));
     }
+    // f = sum_j A_j v_j over the up and down columns: the comb's linear part as
+    // one MLE, so the sumcheck carries [sel, eq_r, f] instead of every column
+    ZG_CUDA(cudaMemcpyAsync(fold_d, folded.data(), (size_t)(J + S) * fb, cudaMemcpyHostToDevice, s));
+    ZG_KBEGIN(ctx, s, "k_precombine");
+    k_precombine<L><<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8), 256, 0, s>>>(
+        up, J + S, nv, fold_d, f, pk + 2 * n * L);
+    ZG_KEND(ctx, s);
     ZG_CUDA(ctx_sync(ctx));
     *packed = pk;
+    return ZG_OK;
+}
+
+// After the CPR sumcheck: the J + S up and down columns (packed after [sel, eq,
+// f]) evaluated at its point r*: eq(r*, .) into the eq slot, then one dot
+// product per column.
+template <int L>
+zg_status cpr_column_evals(zg_ctx *ctx, const FieldCfg &f, uint64_t *pk, uint32_t K, uint32_t nv,
+                           const uint64_t *point, uint64_t *evals) {
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)1 << nv, fb = 8 * L, mle = n * fb;
+    const size_t halves = ((size_t)1 << (nv / 2)) + ((size_t)1 << (nv - nv / 2));
+    uint8_t *ar = reinterpret_cast<uint8_t *>(pk);
+    uint64_t *r_d = reinterpret_cast<uint64_t *>(ar + (3 + (size_t)K) * mle), *omr_d = r_d + (size_t)nv * L;
+    uint64_t *half_d = omr_d + (size_t)nv * L, *part_d = half_d + halves * L + (size_t)K * L;
+    std::vector<uint64_t> omr((size_t)nv * L);
+    for (uint32_t k = 0; k < nv; k++) {
+        std::memcpy(&omr[(size_t)k * L], f.one, fb);
+        fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
+    }
+    ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    uint64_t *eq = pk + n * L;
+    ZG_KBEGIN(ctx, s, "k_eq_halves");
+    k_eq_halves<L><<<(unsigned)((halves + 127) / 128), 128, 0, s>>>(r_d, omr_d, nv, f, half_d);
+    ZG_KEND(ctx, s);
+    ZG_KBEGIN(ctx, s, "k_eq_outer");
+    k_eq_outer<L><<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8), 256, 0, s>>>(
+        half_d, nv, f, eq);
+    ZG_KEND(ctx, s);
+    const unsigned G = (unsigned)std::max<size_t>(1, std::min<size_t>(kCprDotBlocks, n / 2048));
+    ZG_KBEGIN(ctx, s, "k_mle_dots");
+    k_mle_dots<L><<<dim3(G, K), 256, 0, s>>>(pk + 3 * n * L, nv, eq, f, part_d);
+    ZG_KEND(ctx, s);
+    std::vector<uint64_t> part((size_t)K * G * L);
+    ZG_CUDA(cudaMemcpyAsync(part.data(), part_d, part.size() * 8, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(ctx_sync(ctx));
+    for (uint32_t k = 0; k < K; k++) {
+        uint64_t acc[L] = {};
+        for (unsigned g = 0; g < G; g++) fadd<L>(acc, &part[((size_t)k * G + g) * L], f.p);
+        std::memcpy(evals + (size_t)k * L, acc, fb);
+    }
     return ZG_OK;
 }
 
@@ -718,7 +817,7 @@ extern "C" zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, cons
             set_error("multipoint eval: the modulus must be odd");
             return ZG_ERR_INVALID_PARAM;
         }
-        std::vector<uint64_t> alphas;
+        uint32_t M = 0;  // distinct shift amounts
         uint64_t *packed = nullptr;
         {
             std::lock_guard<std::mutex> lk(ctx->mu);
@@ -727,28 +826,28 @@ extern "C" zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, cons
             t->has_field = true;
             const zg_status st =
                 limbs == 3 ? multipoint_prepare<3>(ctx, t, t->f, trace_mles, num_cols, nvars, eval_point, shift_src,
-                                                   shift_amount, n_shifts, mles_on_device, alphas, &packed)
+                                                   shift_amount, n_shifts, mles_on_device, &M, &packed)
                            : multipoint_prepare<4>(ctx, t, t->f, trace_mles, num_cols, nvars, eval_point, shift_src,
-                                                   shift_amount, n_shifts, mles_on_device, alphas, &packed);
+                                                   shift_amount, n_shifts, mles_on_device, &M, &packed);
             if (st != ZG_OK) return st;
         }
-        // comb = eq * precombined + sum_k alpha_k next_k down_k, degree 2 (multipoint_eval.rs:195-213)
-        const uint32_t S = n_shifts;
-        std::vector<uint64_t> coeffs((size_t)(1 + S) * limbs);
-        std::memcpy(coeffs.data(), t->f.one, 8 * limbs);
-        if (S) std::memcpy(&coeffs[limbs], alphas.data(), (size_t)S * 8 * limbs);
-        std::vector<uint32_t> offsets(2 + S), indices(2 * (1 + S));
-        for (uint32_t k = 0; k <= 1 + S; k++) offsets[k] = 2 * k;
+        // comb = eq * precombined + sum_k alpha_k next_k v_{src_k}, degree 2
+        // (multipoint_eval.rs:195-213), with the shift terms grouped by amount:
+        // eq * precombined + sum_c next_c * w_c, every product with coefficient one
+        std::vector<uint64_t> coeffs((size_t)(1 + M) * limbs);
+        for (uint32_t k = 0; k <= M; k++) std::memcpy(&coeffs[(size_t)k * limbs], t->f.one, 8 * limbs);
+        std::vector<uint32_t> offsets(2 + M), indices(2 * (1 + M));
+        for (uint32_t k = 0; k <= 1 + M; k++) offsets[k] = 2 * k;
         indices[0] = 0;
-        indices[1] = 1 + S;
-        for (uint32_t k = 0; k < S; k++) {
-            indices[2 * (1 + k)] = 1 + k;
-            indices[2 * (1 + k) + 1] = 2 + S + k;
+        indices[1] = 1 + M;
+        for (uint32_t m = 0; m < M; m++) {
+            indices[2 * (1 + m)] = 1 + m;
+            indices[2 * (1 + m) + 1] = 2 + M + m;
         }
         zg_sumcheck_group g{};
         g.degree = 2;
-        g.n_mles = 2 + 2 * S;
-        g.n_products = 1 + S;
+        g.n_mles = 2 + 2 * M;
+        g.n_products = 1 + M;
         g.mles = packed;
         g.coeffs = coeffs.data();
         g.offsets = offsets.data();
@@ -808,11 +907,11 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
                                             n_constraints, coeffs, mles_on_device, folded, &packed);
             if (st != ZG_OK) return st;
         }
-        // comb = (sum_j A_j v_j) * eq_r * (1 - selector): one-MLE products times two
-        // affine factors, degree max_degree + 2 = 3 (combined_poly_resolver.rs:147-172)
-        std::vector<uint32_t> offsets(J + S + 1), indices(J + S);
-        for (uint32_t j = 0; j <= J + S; j++) offsets[j] = j;
-        for (uint32_t j = 0; j < J + S; j++) indices[j] = 2 + j;
+        // comb = (sum_j A_j v_j) * eq_r * (1 - selector), degree max_degree + 2 = 3
+        // (combined_poly_resolver.rs:147-172): the sum is the precombined MLE f,
+        // times two affine factors; the round polynomials are those of the
+        // reference's comb over every column
+        const uint32_t offsets[2] = {0, 1}, indices[1] = {2};
         const uint32_t fm[2] = {1, 0};
         std::vector<uint64_t> fa(2 * (size_t)limbs, 0), fbv(2 * (size_t)limbs, 0);
         std::memcpy(&fbv[0], t->f.one, 8 * limbs);      // eq_r: 0 + 1 * eq_r
@@ -829,24 +928,28 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
         }
         zg_sumcheck_group g{};
         g.degree = 3;
-        g.n_mles = 2 + J + S;
-        g.n_products = J + S;
+        g.n_mles = 3;
+        g.n_products = 1;
         g.mles = packed;
-        g.coeffs = folded.data();
-        g.offsets = offsets.data();
-        g.indices = indices.data();
+        g.coeffs = t->f.one;
+        g.offsets = offsets;
+        g.indices = indices;
         g.n_factors = 2;
         g.factor_mles = fm;
         g.factor_a = fa.data();
         g.factor_b = fbv.data();
-        std::vector<uint64_t> finals((size_t)(2 + J + S) * limbs);
-        ZG_TRY(zg_sumcheck_prove(ctx, t, modulus, limbs, nvars, 1, &g, 1, 1, proof, proof_len, point_out,
-                                 finals.data()));
+        std::vector<uint64_t> pt((size_t)nvars * limbs), evals((size_t)(J + S) * limbs);
+        ZG_TRY(zg_sumcheck_prove(ctx, t, modulus, limbs, nvars, 1, &g, 1, 1, proof, proof_len, pt.data(),
+                                 nullptr));
+        if (point_out) std::memcpy(point_out, pt.data(), pt.size() * 8);
         // finalize_prover (combined_poly_resolver.rs:192-247): the up and down
         // columns at the sumcheck point, absorbed as random-field elements
         std::lock_guard<std::mutex> lk(ctx->mu);
-        for (uint32_t j = 0; j < J + S; j++) tr_absorb_field(t, &finals[(size_t)(2 + j) * limbs]);
-        if (evals_out) std::memcpy(evals_out, &finals[2 * (size_t)limbs], (size_t)(J + S) * 8 * limbs);
+        ZG_CUDA(cudaSetDevice(ctx->device));
+        ZG_TRY(limbs == 3 ? cpr_column_evals<3>(ctx, t->f, packed, J + S, nvars, pt.data(), evals.data())
+                          : cpr_column_evals<4>(ctx, t->f, packed, J + S, nvars, pt.data(), evals.data()));
+        for (uint32_t j = 0; j < J + S; j++) tr_absorb_field(t, &evals[(size_t)j * limbs]);
+        if (evals_out) std::memcpy(evals_out, evals.data(), evals.size() * 8);
         return ZG_OK;
     } catch (const std::exception &e) {
         set_error("CPR: %s", e.what());
