@@ -4,7 +4,8 @@
  * The reference (NethermindEth/zinc-plus) is a Rust workspace with no FFI; its
  * boundary for this path is a set of Rust traits and associated functions.
  * Each entry point below names the reference item it stands in for, so a Rust
- * host can bind this header and keep its call sites:
+ * host can bind this header with `extern "C"` declarations and keep its call
+ * sites:
  *
  *   LinearCode::{row_len, codeword_len, encode, encode_wide}
  *                                   zip-plus/src/code.rs:10-72
@@ -167,7 +168,7 @@ zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_
  * pressure, and this entry point calls neither, nor any other allocating
  * routine.  It computes the same root as zg_merkle_root over `width` leaves
  * whose preimages are consecutive `leaf_bytes`-byte ranges at leaves_d (device
- * memory, leaf-major), and writes the 32-byte root to root_d (device memory),
+ * memory, leaf-major, 4-byte aligned; leaf_bytes a multiple of 4), and writes the 32-byte root to root_d (device memory),
  * asynchronously on `stream` (a cudaStream_t; NULL = legacy default stream).
  * Its scratch is a fixed 4 MiB device array inside the library, held by every
  * GPU that loads it until the process exits: (2*width - 1) * 32 bytes of nodes
@@ -175,8 +176,10 @@ zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_
  * leaves longer than 1024 bytes must fit (e.g. 65536 leaves of at most 1024
  * bytes); larger inputs return ZG_ERR_INVALID_PARAM.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress, with that
- * device current); make that first call before any stream capture.  All calls
- * on a device share the array: calls that overlap on the GPU race. */
+ * device current); make that first call before any stream capture.  That
+ * address belongs to the device's primary context: after cudaDeviceReset the
+ * entry point must not be called again in the same process.  All calls on a
+ * device share the array: calls that overlap on the GPU race. */
 zg_status zg_merkle_root_noalloc_d(const void *leaves_d, uint32_t width, uint32_t leaf_bytes,
                                    uint8_t *root_d, void *stream);
 

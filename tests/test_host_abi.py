@@ -155,3 +155,13 @@ def test_device_entry_points_need_a_context(zipgpu):
     with pytest.raises(zipgpu.ZipError) as e:
         zipgpu.ZipPlus.commit(pp, [np.zeros(1024, np.uint64)])
     assert e.value.status == 8
+
+
+def test_noalloc_root_rejects_misaligned_leaves_before_any_device_call(zipgpu):
+    # The argument checks of zg_merkle_root_noalloc_d run before it touches the
+    # device, so a misaligned leaf pointer is refused even with no GPU present.
+    # The pointers are never dereferenced.
+    fn = zipgpu.lib().zg_merkle_root_noalloc_d
+    assert fn(0x10001, 4096, 256, 0x20000, None) == 1
+    assert b"aligned" in zipgpu.lib().zg_last_error()
+    assert fn(0x10002, 16, 16, 0x20000, None) == 1

@@ -125,7 +125,7 @@ def mp_case(oracle, L, nv, ncols, seed):
 
 
 @pytest.mark.parametrize("L,nv,ncols,shifts", [(3, 4, 3, [(0, 1), (2, 3)]), (4, 3, 2, [(1, 1)]),
-                                               (3, 5, 4, [])])
+                                               (3, 5, 4, []), (3, 4, 3, [(1, 1), (1, 1), (0, 0), (2, 1)])])
 def test_oracle_multipoint_claim_is_the_batched_evaluations(oracle, L, nv, ncols, shifts):
     """The proof's claimed sum is compute_expected_sum (multipoint_eval.rs:216-219):
     sum_j gamma_j v_j(r') + sum_k alpha_k down_k, down_k = sum_b next_c(r', b) v_src(b),
@@ -159,7 +159,11 @@ def test_oracle_multipoint_claim_is_the_batched_evaluations(oracle, L, nv, ncols
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("L,nv,ncols,shifts", [(3, 6, 3, [(0, 1), (2, 3)]), (4, 8, 5, [(4, 7), (0, 1), (1, 2)]),
-                                               (3, 10, 17, [(k + 1, 1) for k in range(16)]), (3, 5, 2, [])])
+                                               (3, 10, 17, [(k + 1, 1) for k in range(16)]), (3, 5, 2, []),
+                                               # a repeated (src, amount) pair and amount 0 among others:
+                                               # the shift terms' weights are summed per amount and source
+                                               (3, 6, 3, [(1, 1), (1, 1), (0, 0), (2, 1)]),
+                                               (4, 7, 4, [(3, 0), (0, 2), (3, 0), (0, 2), (1, 2), (2, 5)])])
 def test_gpu_multipoint_eval_matches_oracle(zipgpu, oracle, ctx, L, nv, ncols, shifts):
     p, mles, r = mp_case(oracle, L, nv, ncols, 60 + nv)
     want_proof, want_r0 = oracle.piop_multipoint_eval(oracle.Transcript(), p, L, mles, r, shifts)

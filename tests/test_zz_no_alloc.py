@@ -57,3 +57,10 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(zipgpu, ctx):
     assert status == 1
     assert b"limit" in zipgpu.lib().zg_last_error()
     assert fn(small.data_ptr(), 3, 16, root.data_ptr(), None) == 1  # not a power of two
+    # A leaf pointer at an odd offset is refused before any launch: the leaf
+    # kernels read 32-bit words.
+    assert fn(small.data_ptr() + 1, 2, 16, root.data_ptr(), None) == 1
+    assert b"aligned" in zipgpu.lib().zg_last_error()
+    # The context is still usable afterwards.
+    data = np.arange(2 * 16, dtype=np.uint8).reshape(1, 32)
+    assert _noalloc_root(zipgpu, torch, data.reshape(2, 16)) == zipgpu.MerkleTree.new(data, 16, ctx).root()

@@ -369,6 +369,12 @@ extern "C" zg_status zg_merkle_root_noalloc_d(const void *leaves_d, uint32_t wid
                   leaf_bytes);
         return ZG_ERR_INVALID_PARAM;
     }
+    // The leaf kernels read the preimages as 32-bit words: a pointer at an odd
+    // offset into the caller's pool would fault on a misaligned load.
+    if (reinterpret_cast<uintptr_t>(leaves_d) % 4 != 0) {
+        set_error("zg_merkle_root_noalloc_d: leaves_d %p is not 4-byte aligned", leaves_d);
+        return ZG_ERR_INVALID_PARAM;
+    }
     const uint64_t nchunks =
         leaf_bytes <= b3::CHUNK_LEN ? 0 : (leaf_bytes + b3::CHUNK_LEN - 1) / b3::CHUNK_LEN;
     const uint64_t nodes = 2 * (uint64_t)width - 1;
@@ -389,6 +395,9 @@ extern "C" zg_status zg_merkle_root_noalloc_d(const void *leaves_d, uint32_t wid
     {
         // One-time set-up per device, with that device current: the array's
         // name is only a host-side stand-in, so its device address is looked up.
+        // The address belongs to the device's primary context (the one the CUDA
+        // runtime uses); it stays valid until the process exits or resets the
+        // device, after which this entry point must not be called again.
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
         if (!g_noalloc_addr[dev]) {
             void *addr = nullptr;

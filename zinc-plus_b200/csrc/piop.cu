@@ -347,6 +347,29 @@ __global__ void __launch_bounds__(256) k_precombine(const uint64_t *__restrict__
     }
 }
 
+// out[b] = sum_{e < count} weights[e] * mles[idx[e]][b]: a combination of a few
+// columns, without visiting the columns whose weight is zero.
+template <int L>
+__global__ void __launch_bounds__(256) k_precombine_sparse(const uint64_t *__restrict__ mles, uint32_t nv,
+                                                           const uint32_t *__restrict__ idx,
+                                                           const uint64_t *__restrict__ weights, uint32_t count,
+                                                           FieldCfg f, uint64_t *__restrict__ out) {
+    const size_t n = (size_t)1 << nv;
+    for (size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x; b < n; b += (size_t)gridDim.x * blockDim.x) {
+        Lazy<L> z;
+        lazy_zero(z);
+        for (uint32_t e = 0; e < count; e++) {
+            uint64_t t[L];
+            fmul<L>(weights + (size_t)e * L, mles + (((size_t)idx[e] << nv) + b) * L, f.p, f.n0, t);
+            lazy_add<L>(z, t);
+        }
+        uint64_t r[L];
+        lazy_reduce<L>(z, f, r);
+#pragma unroll
+        for (int w = 0; w < L; w++) out[b * L + w] = r[w];
+    }
+}
+
 // partials[k][blockIdx.x] = sum over this block's share of b of eq[b] * mles[k][b]
 // (grid: (blocks per MLE, MLEs)); lazy sums, one reduction per block.
 template <int L>
@@ -565,19 +588,37 @@ zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, c
     for (uint32_t k = 0; k < S; k++) field_challenge_h<L>(t, f, &alphas[(size_t)k * L]);
     for (uint32_t j = 0; j < ncols; j++) field_challenge_h<L>(t, f, &gammas[(size_t)j * L]);
     // sum_k alpha_k next_{c_k} v_{src_k} = sum_c next_c (sum_{k: c_k = c} alpha_k v_{src_k}):
-    // one selector and one weighted column combination per distinct shift amount
+    // one selector and one weighted column combination per distinct shift amount.
+    // Each combination is kept sparse: its distinct source columns and their
+    // summed alphas, stored amount by amount (at most S entries in all).
     std::vector<uint32_t> amounts;
-    std::vector<uint64_t> weights;  // per distinct amount: ncols inners
+    std::vector<std::vector<uint32_t>> srcs;
+    std::vector<std::vector<uint64_t>> wts;
     for (uint32_t k = 0; k < S; k++) {
         uint32_t m = 0;
         while (m < amounts.size() && amounts[m] != shift[k]) m++;
         if (m == amounts.size()) {
             amounts.push_back(shift[k]);
-            weights.resize(weights.size() + (size_t)ncols * L, 0);
+            srcs.emplace_back();
+            wts.emplace_back();
         }
-        fadd<L>(&weights[((size_t)m * ncols + src[k]) * L], &alphas[(size_t)k * L], f.p);
+        uint32_t e = 0;
+        while (e < srcs[m].size() && srcs[m][e] != src[k]) e++;
+        if (e == srcs[m].size()) {
+            srcs[m].push_back(src[k]);
+            wts[m].resize(wts[m].size() + L, 0);
+        }
+        fadd<L>(&wts[m][(size_t)e * L], &alphas[(size_t)k * L], f.p);
     }
     const uint32_t M = (uint32_t)amounts.size();
+    std::vector<uint32_t> sp_idx, sp_off(M + 1, 0);
+    std::vector<uint64_t> sp_w;
+    for (uint32_t m = 0; m < M; m++) {
+        sp_idx.insert(sp_idx.end(), srcs[m].begin(), srcs[m].end());
+        sp_w.insert(sp_w.end(), wts[m].begin(), wts[m].end());
+        sp_off[m + 1] = (uint32_t)sp_idx.size();
+    }
+    const size_t nsp = sp_idx.size();
     *n_amounts = M;
     std::vector<uint64_t> omr((size_t)nv * L);
     for (uint32_t k = 0; k < nv; k++) {
@@ -587,7 +628,7 @@ zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, c
     const size_t halves = ((size_t)1 << (nv / 2)) + ((size_t)1 << (nv - nv / 2));
     const size_t npk = 2 + 2 * (size_t)M;
     const size_t staged = on_device ? 0 : (size_t)ncols * mle;
-    const size_t small = (2 * (size_t)nv + halves + ncols * (1 + (size_t)M)) * fb;
+    const size_t small = (2 * (size_t)nv + halves + ncols + nsp) * fb + nsp * 4;
     ZG_TRY(ctx->piop_arena.ensure(npk * mle + staged + small + 256));
     uint8_t *ar = ctx->piop_arena.as<uint8_t>();
     uint64_t *pk = reinterpret_cast<uint64_t *>(ar);
@@ -598,7 +639,11 @@ zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, c
     ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)nv * fb, cudaMemcpyHostToDevice, s));
     ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)nv * fb, cudaMemcpyHostToDevice, s));
     ZG_CUDA(cudaMemcpyAsync(gam_d, gammas.data(), (size_t)ncols * fb, cudaMemcpyHostToDevice, s));
-    if (M) ZG_CUDA(cudaMemcpyAsync(wgt_d, weights.data(), weights.size() * 8, cudaMemcpyHostToDevice, s));
+    uint32_t *idx_d = reinterpret_cast<uint32_t *>(wgt_d + nsp * L);
+    if (nsp) {
+        ZG_CUDA(cudaMemcpyAsync(wgt_d, sp_w.data(), nsp * fb, cudaMemcpyHostToDevice, s));
+        ZG_CUDA(cudaMemcpyAsync(idx_d, sp_idx.data(), nsp * 4, cudaMemcpyHostToDevice, s));
+    }
     uint64_t *eq = pk;  // MLE 0
     ZG_KBEGIN(ctx, s, "k_eq_halves");
     k_eq_halves<L><<<(unsigned)((halves + 127) / 128), 128, 0, s>>>(r_d, omr_d, nv, f, half_d);
@@ -619,8 +664,8 @@ zg_status multipoint_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, c
     ZG_KBEGIN(ctx, s, "k_precombine");
     k_precombine<L><<<grid, 256, 0, s>>>(tr, ncols, nv, gam_d, f, pk + (size_t)(1 + M) * n * L);
     for (uint32_t m = 0; m < M; m++)
-        k_precombine<L><<<grid, 256, 0, s>>>(tr, ncols, nv, wgt_d + (size_t)m * ncols * L, f,
-                                             pk + (size_t)(2 + M + m) * n * L);
+        k_precombine_sparse<L><<<grid, 256, 0, s>>>(tr, nv, idx_d + sp_off[m], wgt_d + (size_t)sp_off[m] * L,
+                                                    sp_off[m + 1] - sp_off[m], f, pk + (size_t)(2 + M + m) * n * L);
     ZG_KEND(ctx, s);
     ZG_CUDA(ctx_sync(ctx));
     *packed = pk;
