@@ -19,6 +19,9 @@
 #ifdef _OPENMP
 #include <omp.h>
 #endif
+#if defined(__AVX512F__)
+#include <immintrin.h>
+#endif
 
 typedef __int128 i128;
 typedef unsigned __int128 u128;
@@ -69,6 +72,49 @@ static inline uint32_t rotr32(uint32_t x, int n) { return (x >> n) | (x << (32 -
         v[b] = rotr32(v[b] ^ v[c], 7);                                                            \
     } while (0)
 
+#if defined(__AVX512F__) && defined(__AVX512VL__)
+/* The same compression with the 4x4 state held as four 128-bit rows: the four
+ * column G functions run lane-parallel, then the rows are rotated so the
+ * diagonals line up as columns, and rotated back (the row-wise SIMD form the
+ * BLAKE3 spec describes, which the `blake3` crate uses for one block at a time;
+ * the reference hashes each Merkle leaf with one Hasher::update,
+ * merkle.rs:148-168).  32-bit rotations are single AVX-512VL instructions. */
+#define B3ROW_G(r0, r1, r2, r3, mx, my)                                                           \
+    do {                                                                                          \
+        r0 = _mm_add_epi32(_mm_add_epi32(r0, r1), mx);                                            \
+        r3 = _mm_ror_epi32(_mm_xor_si128(r3, r0), 16);                                            \
+        r2 = _mm_add_epi32(r2, r3);                                                               \
+        r1 = _mm_ror_epi32(_mm_xor_si128(r1, r2), 12);                                            \
+        r0 = _mm_add_epi32(_mm_add_epi32(r0, r1), my);                                            \
+        r3 = _mm_ror_epi32(_mm_xor_si128(r3, r0), 8);                                             \
+        r2 = _mm_add_epi32(r2, r3);                                                               \
+        r1 = _mm_ror_epi32(_mm_xor_si128(r1, r2), 7);                                             \
+    } while (0)
+
+static void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t counter,
+                        uint32_t block_len, uint32_t flags, uint32_t out[16]) {
+    const __m128i c0 = _mm_loadu_si128((const __m128i *)cv), c1 = _mm_loadu_si128((const __m128i *)(cv + 4));
+    __m128i r0 = c0, r1 = c1, r2 = _mm_loadu_si128((const __m128i *)B3_IV);
+    __m128i r3 = _mm_set_epi32((int)flags, (int)block_len, (int)(uint32_t)(counter >> 32), (int)(uint32_t)counter);
+    for (int r = 0; r < 7; r++) {
+        const uint8_t *s = B3_SCHED[r];
+        B3ROW_G(r0, r1, r2, r3, _mm_set_epi32((int)m[s[6]], (int)m[s[4]], (int)m[s[2]], (int)m[s[0]]),
+                _mm_set_epi32((int)m[s[7]], (int)m[s[5]], (int)m[s[3]], (int)m[s[1]]));
+        r1 = _mm_shuffle_epi32(r1, _MM_SHUFFLE(0, 3, 2, 1)); /* lanes v5 v6 v7 v4 */
+        r2 = _mm_shuffle_epi32(r2, _MM_SHUFFLE(1, 0, 3, 2)); /* lanes v10 v11 v8 v9 */
+        r3 = _mm_shuffle_epi32(r3, _MM_SHUFFLE(2, 1, 0, 3)); /* lanes v15 v12 v13 v14 */
+        B3ROW_G(r0, r1, r2, r3, _mm_set_epi32((int)m[s[14]], (int)m[s[12]], (int)m[s[10]], (int)m[s[8]]),
+                _mm_set_epi32((int)m[s[15]], (int)m[s[13]], (int)m[s[11]], (int)m[s[9]]));
+        r1 = _mm_shuffle_epi32(r1, _MM_SHUFFLE(2, 1, 0, 3));
+        r2 = _mm_shuffle_epi32(r2, _MM_SHUFFLE(1, 0, 3, 2));
+        r3 = _mm_shuffle_epi32(r3, _MM_SHUFFLE(0, 3, 2, 1));
+    }
+    _mm_storeu_si128((__m128i *)out, _mm_xor_si128(r0, r2));
+    _mm_storeu_si128((__m128i *)(out + 4), _mm_xor_si128(r1, r3));
+    _mm_storeu_si128((__m128i *)(out + 8), _mm_xor_si128(r2, c0));
+    _mm_storeu_si128((__m128i *)(out + 12), _mm_xor_si128(r3, c1));
+}
+#else
 static void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t counter,
                         uint32_t block_len, uint32_t flags, uint32_t out[16]) {
     uint32_t v[16] = {cv[0],    cv[1],    cv[2],    cv[3],    cv[4],
@@ -91,6 +137,7 @@ static void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t cou
         out[i + 8] = v[i + 8] ^ cv[i];
     }
 }
+#endif
 
 static void b3_words(const uint8_t *b, size_t n, uint32_t m[16]) {
     uint8_t blk[64];
@@ -610,66 +657,125 @@ static void pntt_stages_wide(const iprs_params *p, uint64_t *out, uint32_t lanes
 /* Radix-8 stages on i128 values (MulByScalar i128 x i64, mul_by_scalar.rs:97-108). */
 static void pntt_stages_i128(const iprs_params *p, i128 *out);
 
-/* Scalar Zip: Eval i32 -> Cw i128 (mul_by_scalar.rs:89-108). */
-static void pntt_i32(const iprs_params *p, const int32_t *in, i128 *out) {
-    uint32_t sh = 3 * p->depth;
-    for (size_t i = 0; i < p->codeword_len; i++) {
+/* The reference's pNTT (radix8.rs:21-161) is data parallel at two levels:
+ * base_multiply_into_output maps every codeword position independently
+ * (`cfg_into_iter!(0..codeword_len)`, radix8.rs:133) and combine_stages works
+ * chunk by chunk (`cfg_chunks_mut!`, radix8.rs:88), while encode_rows runs the
+ * rows in parallel (phase_commit.rs:166-172).  The functions below compute a
+ * range of positions (base layer) or of butterfly columns (one stage), so
+ * encode_poly can spread rows x positions over all threads the same way. */
+
+/* Base layer, integer evaluations (Zip i32 -> i128, mul_by_scalar.rs:89-95;
+ * the Zinc+ integer columns i64 -> i128, mul_by_scalar.rs:110-116; the base
+ * sum of an i64 row stays below 2^63 * 2^16 * base_len in magnitude). */
+static void int_base_range(const iprs_params *p, const void *in_v, int is_i64, i128 *out, size_t i0,
+                           size_t i1) {
+    const uint32_t sh = 3 * p->depth;
+    const int32_t *in32 = (const int32_t *)in_v;
+    const int64_t *in64 = (const int64_t *)in_v;
+    for (size_t i = i0; i < i1; i++) {
         size_t chunk = i >> p->base_dim_log2, row = i & (p->base_dim - 1);
         size_t oct = zr_octet_reversal(chunk, p->depth);
         const int64_t *bm = p->bm + row * p->base_len;
-        i128 acc = in[oct];
-        for (size_t c = 1; c < p->base_len; c++) acc += (i128)in[oct | (c << sh)] * bm[c];
+        i128 acc = is_i64 ? (i128)in64[oct] : (i128)in32[oct];
+        if (is_i64)
+            for (size_t c = 1; c < p->base_len; c++) acc += (i128)in64[oct | (c << sh)] * bm[c];
+        else
+            for (size_t c = 1; c < p->base_len; c++) acc += (i128)in32[oct | (c << sh)] * bm[c];
         out[i] = acc;
     }
-    pntt_stages_i128(p, out);
 }
 
-/* Int column Zip (IntZt of protocol/benches/e2e.rs:215-227): Eval i64 -> Cw
- * i128, i64 x i64 widened to i128 (mul_by_scalar.rs:110-116), the base sum in
- * i128 (|sum| < 2^63 * 2^16 * base_len), the stages as for i32. */
-static void pntt_i64(const iprs_params *p, const int64_t *in, i128 *out) {
-    uint32_t sh = 3 * p->depth;
-    for (size_t i = 0; i < p->codeword_len; i++) {
-        size_t chunk = i >> p->base_dim_log2, row = i & (p->base_dim - 1);
-        size_t oct = zr_octet_reversal(chunk, p->depth);
-        const int64_t *bm = p->bm + row * p->base_len;
-        i128 acc = in[oct];
-        for (size_t c = 1; c < p->base_len; c++) acc += (i128)in[oct | (c << sh)] * bm[c];
-        out[i] = acc;
-    }
-    pntt_stages_i128(p, out);
-}
-
-static void pntt_stages_i128(const iprs_params *p, i128 *out) {
+/* One radix-8 stage on i128 values (MulByScalar i128 x i64, wrapping,
+ * mul_by_scalar.rs:97-108; butterfly.rs:24-43) for butterfly columns
+ * [i0, i1) of the chunk starting at position blk. */
+static void i128_stage_range(const iprs_params *p, uint32_t k, i128 *out, size_t blk, size_t i0, size_t i1) {
+    const size_t sub = (size_t)p->base_dim << (3 * k);
+    const int64_t *tw = p->tw[k];
+    i128 *chunk = out + blk;
     i128 xs[8];
-    for (uint32_t k = 0; k < p->depth; k++) {
-        size_t sub = (size_t)p->base_dim << (3 * k);
-        const int64_t *tw = p->tw[k];
-        for (size_t blk = 0; blk < p->codeword_len; blk += 8 * sub) {
-            i128 *chunk = out + blk;
-            for (size_t i = 0; i < sub; i++) {
-                for (int j = 0; j < 8; j++) xs[j] = chunk[j * sub + i];
-                for (int r = 0; r < 8; r++) {
-                    u128 y = (u128)xs[0];
-                    for (int j = 1; j < 8; j++)
-                        y += (u128)xs[j] * (u128)(i128)tw[(i * 7 + (j - 1)) * 8 + BUTTERFLY_TABLE[r][j - 1]];
-                    chunk[r * sub + i] = (i128)y;
-                }
-            }
+    for (size_t i = i0; i < i1; i++) {
+        for (int j = 0; j < 8; j++) xs[j] = chunk[j * sub + i];
+        for (int r = 0; r < 8; r++) {
+            u128 y = (u128)xs[0];
+            for (int j = 1; j < 8; j++)
+                y += (u128)xs[j] * (u128)(i128)tw[(i * 7 + (j - 1)) * 8 + BUTTERFLY_TABLE[r][j - 1]];
+            chunk[r * sub + i] = (i128)y;
         }
     }
 }
 
-/* Zip+: Eval BinaryPoly<D> (u64 bit mask) -> Cw DensePolynomial<i64, D>
- * (binary_u64.rs:445-456 widen; dense.rs:551-574). out: C x D i64. */
-static void pntt_binary(const iprs_params *p, const uint64_t *in, uint32_t D, int64_t *out) {
-    uint32_t sh = 3 * p->depth;
-    for (size_t i = 0; i < p->codeword_len; i++) {
+static void pntt_stages_i128(const iprs_params *p, i128 *out) {
+    for (uint32_t k = 0; k < p->depth; k++) {
+        size_t sub = (size_t)p->base_dim << (3 * k);
+        for (size_t blk = 0; blk < p->codeword_len; blk += 8 * sub) i128_stage_range(p, k, out, blk, 0, sub);
+    }
+}
+
+/* Scalar Zip: Eval i32 -> Cw i128 (mul_by_scalar.rs:89-108). */
+static void pntt_i32(const iprs_params *p, const int32_t *in, i128 *out) {
+    int_base_range(p, in, 0, out, 0, p->codeword_len);
+    pntt_stages_i128(p, out);
+}
+
+/* Int column Zip (IntZt of protocol/benches/e2e.rs:215-227): Eval i64 -> Cw i128. */
+static void pntt_i64(const iprs_params *p, const int64_t *in, i128 *out) {
+    int_base_range(p, in, 1, out, 0, p->codeword_len);
+    pntt_stages_i128(p, out);
+}
+
+/* Zip+ base layer: Eval BinaryPoly<D> (u64 bit mask) -> Cw DensePolynomial<i64,
+ * D>.  Each term is the widened polynomial (coefficient l = bm[c] if bit l is
+ * set, else 0: binary_u64.rs:445-456) added coefficient-wise with wrapping i64
+ * (dense.rs:551-574).  With AVX-512 the widen is the reference's own form
+ * (binary_u64.rs:605-661: one masked broadcast per 8 coefficients), fused here
+ * with the add as one masked add per 8 coefficients. */
+#if defined(__AVX512F__)
+static inline __attribute__((always_inline)) void bin_base_avx512(const iprs_params *p, const uint64_t *in,
+                                                                  const uint32_t NV8, int64_t *out, size_t i0,
+                                                                  size_t i1) {
+    const uint32_t sh = 3 * p->depth;
+    const __m512i one = _mm512_set1_epi64(1);
+    for (size_t i = i0; i < i1; i++) {
+        size_t chunk = i >> p->base_dim_log2, row = i & (p->base_dim - 1);
+        size_t oct = zr_octet_reversal(chunk, p->depth);
+        const int64_t *bm = p->bm + row * p->base_len;
+        __m512i acc[8];
+        const uint64_t x0 = in[oct];
+        for (uint32_t v = 0; v < NV8; v++) acc[v] = _mm512_maskz_mov_epi64((__mmask8)(x0 >> (8 * v)), one);
+        for (size_t c = 1; c < p->base_len; c++) {
+            const uint64_t x = in[oct | (c << sh)];
+            const __m512i b = _mm512_set1_epi64(bm[c]);
+            for (uint32_t v = 0; v < NV8; v++)
+                acc[v] = _mm512_mask_add_epi64(acc[v], (__mmask8)(x >> (8 * v)), acc[v], b);
+        }
+        for (uint32_t v = 0; v < NV8; v++) _mm512_storeu_si512((void *)(out + i * 8 * NV8 + 8 * v), acc[v]);
+    }
+}
+#endif
+
+static void bin_base_range(const iprs_params *p, const uint64_t *in, uint32_t D, int64_t *out, size_t i0,
+                           size_t i1) {
+#if defined(__AVX512F__)
+    switch (D) {  /* D a multiple of 8: the vector form, with the lane count a constant */
+    case 8: bin_base_avx512(p, in, 1, out, i0, i1); return;
+    case 16: bin_base_avx512(p, in, 2, out, i0, i1); return;
+    case 24: bin_base_avx512(p, in, 3, out, i0, i1); return;
+    case 32: bin_base_avx512(p, in, 4, out, i0, i1); return;
+    case 40: bin_base_avx512(p, in, 5, out, i0, i1); return;
+    case 48: bin_base_avx512(p, in, 6, out, i0, i1); return;
+    case 56: bin_base_avx512(p, in, 7, out, i0, i1); return;
+    case 64: bin_base_avx512(p, in, 8, out, i0, i1); return;
+    default: break;
+    }
+#endif
+    const uint32_t sh = 3 * p->depth;
+    const uint64_t msk = dmask(D);
+    for (size_t i = i0; i < i1; i++) {
         size_t chunk = i >> p->base_dim_log2, row = i & (p->base_dim - 1);
         size_t oct = zr_octet_reversal(chunk, p->depth);
         const int64_t *bm = p->bm + row * p->base_len;
         uint64_t acc[64];
-        const uint64_t msk = dmask(D);
         uint64_t x0 = in[oct] & msk;
         for (uint32_t l = 0; l < D; l++) acc[l] = (x0 >> l) & 1;
         for (size_t c = 1; c < p->base_len; c++) {
@@ -679,26 +785,47 @@ static void pntt_binary(const iprs_params *p, const uint64_t *in, uint32_t D, in
         }
         for (uint32_t l = 0; l < D; l++) out[i * D + l] = (int64_t)acc[l];
     }
+}
+
+/* One radix-8 stage on DensePolynomial<i64, D> values (coefficient-wise
+ * wrapping i64 x twiddle, dense.rs:551-574), butterfly columns [i0, i1) of the
+ * chunk starting at position blk. */
+static void bin_stage_range(const iprs_params *p, uint32_t k, uint32_t D, int64_t *out, size_t blk, size_t i0,
+                            size_t i1) {
+    const size_t sub = (size_t)p->base_dim << (3 * k);
+    const int64_t *tw = p->tw[k];
+    int64_t *chunk = out + blk * D;
     uint64_t xs[8][64];
-    for (uint32_t k = 0; k < p->depth; k++) {
-        size_t sub = (size_t)p->base_dim << (3 * k);
-        const int64_t *tw = p->tw[k];
-        for (size_t blk = 0; blk < p->codeword_len; blk += 8 * sub) {
-            int64_t *chunk = out + blk * D;
-            for (size_t i = 0; i < sub; i++) {
-                for (int j = 0; j < 8; j++)
-                    for (uint32_t l = 0; l < D; l++) xs[j][l] = (uint64_t)chunk[(j * sub + i) * D + l];
-                for (int r = 0; r < 8; r++) {
-                    uint64_t y[64];
-                    for (uint32_t l = 0; l < D; l++) y[l] = xs[0][l];
-                    for (int j = 1; j < 8; j++) {
-                        uint64_t t = (uint64_t)tw[(i * 7 + (j - 1)) * 8 + BUTTERFLY_TABLE[r][j - 1]];
-                        for (uint32_t l = 0; l < D; l++) y[l] += xs[j][l] * t;
-                    }
-                    for (uint32_t l = 0; l < D; l++) chunk[(r * sub + i) * D + l] = (int64_t)y[l];
-                }
+    for (size_t i = i0; i < i1; i++) {
+        for (int j = 0; j < 8; j++) memcpy(xs[j], chunk + (j * sub + i) * D, 8 * D);
+        for (int r = 0; r < 8; r++) {
+            uint64_t t[8];
+            for (int j = 1; j < 8; j++) t[j] = (uint64_t)tw[(i * 7 + (j - 1)) * 8 + BUTTERFLY_TABLE[r][j - 1]];
+            int64_t *y = chunk + (r * sub + i) * D;
+            uint32_t l = 0;
+#if defined(__AVX512F__) && defined(__AVX512DQ__)
+            for (; l + 8 <= D; l += 8) {
+                __m512i acc = _mm512_loadu_si512((const void *)(xs[0] + l));
+                for (int j = 1; j < 8; j++)
+                    acc = _mm512_add_epi64(acc, _mm512_mullo_epi64(_mm512_loadu_si512((const void *)(xs[j] + l)),
+                                                                    _mm512_set1_epi64((long long)t[j])));
+                _mm512_storeu_si512((void *)(y + l), acc);
+            }
+#endif
+            for (; l < D; l++) {
+                uint64_t a = xs[0][l];
+                for (int j = 1; j < 8; j++) a += xs[j][l] * t[j];
+                y[l] = (int64_t)a;
             }
         }
+    }
+}
+
+static void pntt_binary(const iprs_params *p, const uint64_t *in, uint32_t D, int64_t *out) {
+    bin_base_range(p, in, D, out, 0, p->codeword_len);
+    for (uint32_t k = 0; k < p->depth; k++) {
+        size_t sub = (size_t)p->base_dim << (3 * k);
+        for (size_t blk = 0; blk < p->codeword_len; blk += 8 * sub) bin_stage_range(p, k, D, out, blk, 0, sub);
     }
 }
 
@@ -879,14 +1006,54 @@ static void encode_row(const zparams *z, const void *row, void *cw) {
     }
 }
 
-/* phase_commit.rs:159-176 encode_rows: row-major num_rows x codeword_len */
+/* phase_commit.rs:159-176 encode_rows: row-major num_rows x codeword_len.
+ * IPRS: rows x position tiles of the base layer, then per stage rows x
+ * (chunk, butterfly-column tile), all threads at each level (the reference's
+ * nested rayon over rows, positions and chunks).  RAA (repeat, permute, prefix
+ * sums: sequential within a row, raa.rs:93-127): rows in parallel. */
+#define ZR_TILE 256
 static void encode_poly(const zparams *z, const uint8_t *evals, uint8_t *cw) {
     int nt = zr_get_threads();
     (void)nt;
+    const long R = (long)z->num_rows;
+    if (z->d.code_kind != ZR_CODE_IPRS) {
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
-    for (long r = 0; r < (long)z->num_rows; r++)
-        encode_row(z, evals + (size_t)r * z->row_len * z->eval_bytes,
-                   cw + (size_t)r * z->codeword_len * z->cw_bytes);
+        for (long r = 0; r < R; r++)
+            encode_row(z, evals + (size_t)r * z->row_len * z->eval_bytes,
+                       cw + (size_t)r * z->codeword_len * z->cw_bytes);
+        return;
+    }
+    const iprs_params *p = &z->iprs;
+    const size_t C = p->codeword_len, ev_row = (size_t)z->row_len * z->eval_bytes,
+                 cw_row = (size_t)C * z->cw_bytes;
+    const int bin = z->d.eval_kind == ZR_EVAL_BINPOLY;
+    const long tiles = (long)((C + ZR_TILE - 1) / ZR_TILE);
+#pragma omp parallel num_threads(nt)
+    {
+#pragma omp for schedule(static) collapse(2)
+        for (long r = 0; r < R; r++)
+            for (long t = 0; t < tiles; t++) {
+                const size_t i0 = (size_t)t * ZR_TILE, i1 = i0 + ZR_TILE < C ? i0 + ZR_TILE : C;
+                const uint8_t *in = evals + (size_t)r * ev_row;
+                uint8_t *o = cw + (size_t)r * cw_row;
+                if (bin) bin_base_range(p, (const uint64_t *)in, z->D, (int64_t *)o, i0, i1);
+                else int_base_range(p, in, z->d.eval_kind == ZR_EVAL_I64, (i128 *)o, i0, i1);
+            }
+        for (uint32_t k = 0; k < p->depth; k++) {
+            const size_t sub = (size_t)p->base_dim << (3 * k);
+            const size_t per_chunk = (sub + ZR_TILE - 1) / ZR_TILE;
+            const long units = (long)((C / (8 * sub)) * per_chunk);
+#pragma omp for schedule(static) collapse(2)
+            for (long r = 0; r < R; r++)
+                for (long u = 0; u < units; u++) {
+                    const size_t blk = (size_t)(u / per_chunk) * 8 * sub, it = (size_t)(u % per_chunk);
+                    const size_t i0 = it * ZR_TILE, i1 = i0 + ZR_TILE < sub ? i0 + ZR_TILE : sub;
+                    uint8_t *o = cw + (size_t)r * cw_row;
+                    if (bin) bin_stage_range(p, k, z->D, (int64_t *)o, blk, i0, i1);
+                    else i128_stage_range(p, k, (i128 *)o, blk, i0, i1);
+                }
+        }
+    }
 }
 
 int zr_encode_rows(const zr_desc *d, const void *evals, void *cw_out) {
