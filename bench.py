@@ -516,6 +516,112 @@ def algorithmic_bytes(kernel, info, nv, D):
     return table.get(kernel)
 
 
+def plain_line(Z, ctx, torch, stream, flush, spec, K, W, with_cpu, cpu_seconds, verify=False, seed=77):
+    """One plain Zip/Zip+ workload, one request per step: zg_commit_prove from
+    device-resident inputs (`value`) and from page-locked host inputs with the
+    proof copied back (`e2e`), CUDA events on the library's stream with the L2
+    flushed between steps; optionally ZipPlus::verify of the last proof (wall
+    clock).  The oracle times the same workload on all host cores for a bounded
+    sample (the CPU baseline)."""
+    ek, D, ck, nv, L = spec
+    n = 1 << nv
+    zt = Z.ZipTypes(ek, D if ek else 1, 5 if ek else 3, 4, 147)
+    code = Z.IprsCode(L) if ck == 0 else Z.RaaCode(L)
+    pp = Z.ZipPlus.setup(n, code, zt, ctx=ctx)
+    lib = Z.lib()
+    rng = np.random.default_rng(seed)
+    cnt = min(K + W, 8)
+    if ek:
+        host = np.stack([random_binary(rng, nv, D) for _ in range(cnt)])
+        host_t = torch.from_numpy(host.view(np.int64)).pin_memory()
+    else:
+        host = rng.integers(-(2**15), 2**15, size=(cnt, n), dtype=np.int32)
+        host_t = torch.from_numpy(host).pin_memory()
+    dev_t = host_t.to("cuda")
+    point = Z.i128_bytes([1] * nv)
+    cap = pp.proof_size(1)
+    proof_t = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    proof = C.c_void_p(proof_t.data_ptr())
+    root, ev, plen = C.create_string_buffer(32), C.create_string_buffer(32), C.c_size_t(cap)
+
+    def step(i, on_dev):
+        plen.value = cap
+        if on_dev:
+            Z.check(lib.zg_commit_prove_d(pp.handle, C.c_void_p(dev_t[i % cnt].data_ptr()), 1,
+                                          C.c_char_p(point), root, ev, proof, C.byref(plen)))
+        else:
+            ptrs = (C.c_void_p * 1)(host_t[i % cnt].data_ptr())
+            Z.check(lib.zg_commit_prove(pp.handle, ptrs, 1, C.c_char_p(point), root, ev, proof,
+                                        C.byref(plen)))
+
+    def timed(on_dev):
+        out = []
+        for i in range(K):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(W + i, on_dev)
+            e1.record(stream)
+            out.append((e0, e1))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in out]
+
+    for i in range(W):
+        step(i, True)
+        step(i, False)
+    dev_ms, host_ms = timed(True), timed(False)
+    res = {"num_vars": nv, "row_len": L, "num_rows": pp.num_rows,
+           "eval": f"BinaryPoly<{D}> Bernoulli(0.5)" if ek else "i32 uniform [-2^15, 2^15)",
+           "code": ("IPRS rate 1/4" if ck == 0 else "RAA rate 1/4"),
+           "value": K * n / (sum(dev_ms) / 1e3), "unit": "evals/s", "ms": sum(dev_ms) / K,
+           "e2e": {"value": K * n / (sum(host_ms) / 1e3), "unit": "evals/s", "ms": sum(host_ms) / K,
+                   "h2d_bytes_per_step": int(host_t[0].numel() * host_t.element_size()),
+                   "d2h_bytes_per_step": int(plen.value + 64)},
+           "latency_ms": {"p50": float(np.percentile(host_ms, 50)), "p99": float(np.percentile(host_ms, 99))},
+           "proof_bytes": int(plen.value)}
+    vproof = bytes(proof_t[: plen.value].numpy())
+    comm = Z.ZipPlusCommitment(root.raw, 1)
+    if verify:
+        Z.ZipPlus.verify(pp, comm, [1] * nv, ev.raw, vproof)
+        vt = []
+        for _ in range(5):
+            a = time.perf_counter()
+            Z.ZipPlus.verify(pp, comm, [1] * nv, ev.raw, vproof)
+            vt.append((time.perf_counter() - a) * 1e3)
+        res["verify_ms"] = statistics.median(vt)
+        res["commit_prove_verify_e2e_evals_per_s"] = n / ((res["e2e"]["ms"] + res["verify_ms"]) / 1e3)
+    if with_cpu:
+        from oracle import oracle as O
+
+        O.build()
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        desc = O.make_desc(ek, D, ck, nv, L)
+        want = O.commit_prove(desc, host[(W + K - 1) % cnt], 1, [1] * nv)
+        res["equal_oracle"] = (want[0] == root.raw and want[1] == vproof and want[2] == ev.raw[:len(want[2])])
+        steps, lat, t0 = 0, [], time.perf_counter()
+        while steps < 50 and (time.perf_counter() - t0 < cpu_seconds or steps < 2):
+            a = time.perf_counter()
+            O.commit_prove(desc, host[steps % cnt], 1, [1] * nv)
+            lat.append(time.perf_counter() - a)
+            steps += 1
+        cpu = {"value": steps * n / sum(lat), "unit": "evals/s", "cores": threads, "kind": "port",
+               "sample": f"{steps} commit+prove steps of this workload, {sum(lat):.1f} s, OpenMP on {threads} "
+                         "threads: base layer over rows x positions, stages over rows x chunk columns, "
+                         "leaves over columns, tree pairs per level, prove over rows/columns"}
+        if verify:
+            a = time.perf_counter()
+            rc = O.verify(desc, root.raw, 1, [1] * nv, ev.raw, vproof)
+            cpu["verify_ms"] = (time.perf_counter() - a) * 1e3
+            cpu["oracle_accepts_gpu_proof"] = rc == 0
+        res["cpu_baseline"] = cpu
+        res["e2e_over_cpu"] = res["e2e"]["value"] / cpu["value"]
+    pp.close()
+    return res
+
+
 def run_ours(args):
     import torch
 
@@ -718,53 +824,109 @@ def run_ours(args):
             verify["cpu_baseline_ms"] = (time.perf_counter() - a) * 1e3
             verify["cpu_baseline_kind"] = "port (oracle, OpenMP, full encode_wide as the reference)"
             verify["oracle_accepts"] = rc == 0
-    batch_commit = serving = sumcheck = piop_steps = zinc_prove = None
+    sections = {}
     if not args.no_extra:
-        sumcheck = run_sumcheck(Z, ctx, torch, stream, 18, 14, rank == 0 and not args.no_cpu_baseline)
-        piop_steps = run_piop_steps(Z, ctx, torch, stream, 18, 14, rank == 0 and not args.no_cpu_baseline)
-        zinc_prove = run_zinc_prove(Z, ctx, 18, 10, rank == 0 and not args.no_cpu_baseline)
-        batch_commit = run_batched_commit(Z, ctx, torch, stream, flush, reps=5, warm=2)
-        serving = run_serving(Z, ctx, torch, args.serve_requests, args.serve_workers,
-                              seed=0x5A1F + rank)
+        with_cpu = rank == 0 and not args.no_cpu_baseline
+        cs = args.cpu_seconds_per_config
+        # the configurations besides the headline, each a plain line of its own
+        sections["config1_zip_i32_iprs_nv12_flat"] = plain_line(
+            Z, ctx, torch, stream, flush, (0, 1, 0, 12, 4096), K, W, with_cpu, cs, verify=True)
+        sections["config1_zip_i32_iprs_nv12_square"] = plain_line(
+            Z, ctx, torch, stream, flush, (0, 1, 0, 12, 64), K, W, with_cpu, cs, verify=True)
+        sections["config2_zipplus_binpoly32_raa_nv16"] = plain_line(
+            Z, ctx, torch, stream, flush, (1, 32, 1, 16, 256), K, W, with_cpu, cs, verify=True)
+        sections["config2_zipplus_binpoly32_iprs_nv16_plain"] = plain_line(
+            Z, ctx, torch, stream, flush, (1, 32, 0, 16, 1 << 14), K, W, with_cpu, cs, verify=True)
+        nv20 = plain_line(Z, ctx, torch, stream, flush, (1, 32, 0, 20, 1 << 14), min(K, 10), W, with_cpu,
+                          cs, verify=True)
+        nv20["target"] = "plain GPU commit+prove >= 20x the host-CPU path at num_vars = 20 (e2e_over_cpu)"
+        sections["north_star_binpoly32_iprs_nv20_plain"] = nv20
+        sections["sumcheck"] = run_sumcheck(Z, ctx, torch, stream, 18, 14, with_cpu)
+        sections["piop_steps"] = run_piop_steps(Z, ctx, torch, stream, 18, 14, with_cpu)
+        sections["zinc_prove_mle_first"] = run_zinc_prove(Z, ctx, 18, 18, with_cpu)
+        sections["batched_commit"] = run_batched_commit(Z, ctx, torch, stream, flush, reps=5, warm=2)
+        sections["serving"] = run_serving(Z, ctx, torch, args.serve_requests, args.serve_workers,
+                                          seed=0x5A1F + rank)
+    sections["verify"] = verify
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_commit_prove_rate(workload, args.cpu_seconds, 50, host[:4])
         cpu.pop("latency_ms", None)
+    if roofline:
+        # the whole path against HBM: evals/s x algorithmic bytes per evaluation
+        # (2 * eval bytes + 4 * codeword-entry bytes: inputs read twice, the
+        # codeword written once and read back by the leaves, prove and openings)
+        ebytes = 8 if ek else 4
+        cw_entry = (8 * D if ck == 0 else 4 * D) if ek else 16
+        bpe = 2 * ebytes + 4 * cw_entry
+        roofline["path"] = {"bytes_per_eval": bpe, "achieved_gbs": value * bpe / 1e9,
+                            "frac": value * bpe / 1e9 / hbm,
+                            "what": "batched evals/s x bytes per evaluation over the measured HBM peak"}
+        roofline["note"] = ("kernel figures are timed on the plain path (one request per step, CUDA events "
+                            "per launch); value is the batched path")
+        if roofline.get("kernel", "").startswith("k_leaf"):
+            # the leaf hashing is bound by the integer ALU pipe: BLAKE3 compressions
+            # per second against that pipe's issue rate
+            info = pp.info
+            per_leaf = max(1, (info.num_rows * (8 * D if ek else 16) + 63) // 64)
+            comp = info.codeword_len * per_leaf
+            alu_per_comp = 584  # ALU-pipe instructions per compression, ncu (profiles/)
+            sm_mhz = (clock_info or {}).get("sm_mhz") or 1965.0
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+            peak = sms * 64 * sm_mhz * 1e6 / alu_per_comp
+            achieved = comp / (roofline["avg_launch_ms"] / 1e3)
+            roofline["int_alu"] = {"bound": "alu", "unit": "BLAKE3 compressions/s", "achieved": achieved,
+                                   "peak": peak, "frac": achieved / peak, "compressions_per_launch": comp,
+                                   "peak_basis": f"{sms} SMs x 64 ALU lanes/clk x {sm_mhz:.0f} MHz / "
+                                                 f"{alu_per_comp} ALU instructions per compression (ncu)"}
     if rank == 0:
+        for name, obj in sections.items():
+            if obj is not None:
+                print(json.dumps({"section": name, **obj}), flush=True)
         all_lat = lat_dev
+        print(json.dumps({"section": "plain_headline_workload", "value": plain_value, "e2e": plain_e2e,
+                          "ms_per_step": total_dev / K, "e2e_ms_per_step": total_host / K,
+                          "latency_ms": {"p50": float(np.percentile(all_lat, 50)),
+                                         "p99": float(np.percentile(all_lat, 99))},
+                          "e2e_latency_ms": {"p50": float(np.percentile(lat_host, 50)),
+                                             "p99": float(np.percentile(lat_host, 99))},
+                          "host_phases_ms_per_step": host_phases,
+                          "kernel_ms_per_step": {k: round(v[1] / K, 4) for k, v in
+                                                 sorted(ktimes.items(), key=lambda kv: -kv[1][1])},
+                          "kernel_share": roofline.pop("kernel_share", None) if roofline else None}),
+              flush=True)
+
+        def brief(name, keys):
+            o = sections.get(name)
+            return {k: o.get(k) for k in keys} if o else None
+
+        summary = {
+            "config1_flat": brief("config1_zip_i32_iprs_nv12_flat", ["value", "verify_ms", "e2e_over_cpu"]),
+            "config1_square": brief("config1_zip_i32_iprs_nv12_square", ["value", "verify_ms", "e2e_over_cpu"]),
+            "config2_raa": brief("config2_zipplus_binpoly32_raa_nv16", ["value", "e2e_over_cpu"]),
+            "nv20_plain": brief("north_star_binpoly32_iprs_nv20_plain", ["value", "e2e_over_cpu"]),
+            "batched_commit": brief("batched_commit", ["value", "batched_over_sequential"]),
+            "serving": brief("serving", ["value", "served_over_plain", "requests"]),
+            "zinc_prove": brief("zinc_prove_mle_first", ["ms", "equal_oracle_at_full_size", "oracle_verifier_accepts",
+                                                         "speedup_over_cpu"]),
+        }
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": total_bdev / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
             "config": config_of(workload, pp.num_rows, pp.info.depth),
-            "mode": f"batched: {B} independent commit+prove requests per step over {nl} lanes "
-                    "(zg_commit_prove_many); plain: one request per step (zg_commit_prove)",
+            "mode": f"batched: {B} commit+prove requests per step over {nl} lanes (zg_commit_prove_many)",
             "latency_ms": {"p50": float(np.percentile(req_lat, 50)),
-                           "p99": float(np.percentile(req_lat, 99)),
-                           "what": "per-request service time inside the batched steps"},
+                           "p99": float(np.percentile(req_lat, 99))},
             "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": eb * B,
-                    "d2h_bytes_per_step": (proof_len + 64) * B,
-                    "ms_per_step": total_bhost / K},
-            "plain": {"value": plain_value, "e2e": plain_e2e, "ms_per_step": total_dev / K,
-                      "e2e_ms_per_step": total_host / K,
-                      "latency_ms": {"p50": float(np.percentile(all_lat, 50)),
-                                     "p99": float(np.percentile(all_lat, 99))},
-                      "e2e_latency_ms": {"p50": float(np.percentile(lat_host, 50)),
-                                         "p99": float(np.percentile(lat_host, 99))}},
+                    "d2h_bytes_per_step": (proof_len + 64) * B, "ms_per_step": total_bhost / K},
+            "plain": {"value": plain_value, "e2e": plain_e2e},
             "batched_over_plain": value / plain_value,
             "gpu_launches": int(launches),
-            "host_phases_ms_per_step": host_phases,
-            "kernel_ms_per_step": {k: round(v[1] / K, 4) for k, v in
-                                   sorted(ktimes.items(), key=lambda kv: -kv[1][1])},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clock_info,
-            "batched_commit": batch_commit,
-            "serving": serving,
-            "sumcheck": sumcheck,
-            "piop_steps": piop_steps,
-            "zinc_prove_mle_first": zinc_prove,
-            "verify": verify,
+            "summary": summary,
             "impl": "ours",
         }
         print(json.dumps(line), flush=True)
@@ -939,10 +1101,10 @@ def run_zinc_prove(Z, ctx, nv, cpu_nv, with_cpu):
     columns, 1 i64 column, 16 shifts, 17 constraints; 2^nv rows; MontyField<3>;
     both tables IPRS rate 1/4 with 16 rows of 2^(nv-4), CombR Int<6>): the trace
     from host memory through zg_zinc_prove_mle_first to the Proof bytes in host
-    memory, timed on the host clock (the call synchronises).  The oracle's chain
-    of the same steps at 2^cpu_nv rows gives the byte-equality check and a CPU
-    time (its PIOP steps are Python integer loops, so that time says nothing
-    about the reference's speed)."""
+    memory, timed on the host clock (the call synchronises).  The CPU baseline is
+    the oracle's C chain of the same steps at the same size on all host cores
+    (its bytes must equal the GPU's), and the oracle's restated Zinc+ verifier
+    must accept the GPU's proof."""
     from oracle import oracle as O
     from zipgpu import uair
 
@@ -961,26 +1123,34 @@ def run_zinc_prove(Z, ctx, nv, cpu_nv, with_cpu):
         a = time.perf_counter()
         again = Z.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
         ts.append((time.perf_counter() - a) * 1e3)
+    ms = statistics.median(ts)
     res = {"workload": f"BigLinearUair, 2^{nv} rows: 16 BinaryPoly<32> + 1 i64 column, 16 shifts, 17 constraints; "
                        "MontyField<3>; IPRS rate 1/4, 16 rows per table; 147 openings",
-           "ms": statistics.median(ts), "proof_bytes": len(proof), "deterministic": again == proof,
-           "h2d_bytes": int(bins.nbytes + ints.nbytes),
+           "ms": ms, "rows_per_s": (1 << nv) / (ms / 1e3), "proof_bytes": len(proof),
+           "deterministic": again == proof, "h2d_bytes": int(bins.nbytes + ints.nbytes),
            "what": "commit both tables, prime, ideal check, evaluation projection, CPR sumcheck, multipoint "
                    "sumcheck, lifted evaluations, prove_f of both tables, Proof transcription"}
     if with_cpu:
-        bs, is_ = uair.trace(cpu_nv, 0xB17)
-        pbs, pis = tables(cpu_nv)
-        Ls = 1 << (cpu_nv - 4)
-        db = O.make_desc(O.EVAL_BINPOLY, 32, 0, cpu_nv, Ls, comb_limbs=6, field_limbs=3)
-        di = O.make_desc(O.EVAL_I64, 1, 0, cpu_nv, Ls, comb_limbs=6, field_limbs=3)
+        O.build()
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        L = 1 << (nv - 4)
+        db = O.make_desc(O.EVAL_BINPOLY, 32, 0, nv, L, comb_limbs=6, field_limbs=3)
+        di = O.make_desc(O.EVAL_I64, 1, 0, nv, L, comb_limbs=6, field_limbs=3)
+        U = O.Uair.linear(16, 1, 32, shifts, coeffs, uair.ideal_roots())
         a = time.perf_counter()
-        want = O.zinc_prove_mle_first(db, di, cpu_nv, bs, 32, is_, shifts, coeffs, 3)
+        want = O.zinc_prove(db, di, nv, bins, ints, U, 3, mle_first=True)
         c = time.perf_counter() - a
-        got = Z.ZincPlusPiop.prove_mle_first(pbs, pis, cpu_nv, bs, 32, is_, shifts, coeffs)
-        res["cpu_baseline"] = {"ms": c * 1e3, "cores": 1, "kind": "port",
-                               "sample": f"oracle chain at 2^{cpu_nv} rows (C commit/prove_f and sumcheck, "
-                                         "Python-integer PIOP steps)"}
-        res["equal_oracle_at_cpu_size"] = got == want
+        a = time.perf_counter()
+        verdict = O.zinc_verify(db, di, nv, None, None, U, 3, proof)
+        vs = time.perf_counter() - a
+        res["cpu_baseline"] = {"ms": c * 1e3, "rows_per_s": (1 << nv) / c, "cores": threads, "kind": "port",
+                               "sample": f"one proof by the oracle's C chain of steps 0-7 at 2^{nv} rows, OpenMP "
+                                         f"on {threads} threads (commit, PIOP steps, sumchecks, prove_f)"}
+        res["equal_oracle_at_full_size"] = want == proof
+        res["oracle_verifier_accepts"] = verdict == 0
+        res["oracle_verifier_ms"] = vs * 1e3
+        res["speedup_over_cpu"] = c * 1e3 / ms
     return res
 
 
@@ -1019,11 +1189,14 @@ def main():
     ap.add_argument("--batch", type=int, default=32, help="requests per batched step")
     ap.add_argument("--lanes", type=int, default=8, help="concurrent lanes of the batched form")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--serve-requests", type=int, default=1000,
-                    help="requests of the serving stream (10000 for the full stream)")
+    ap.add_argument("--cpu-seconds-per-config", type=float, default=4.0,
+                    help="bounded CPU-baseline sample of each secondary configuration")
+    ap.add_argument("--serve-requests", type=int, default=10000,
+                    help="requests of the serving stream (the full stream is 10000)")
     ap.add_argument("--serve-workers", type=int, default=4)
     ap.add_argument("--no-extra", action="store_true",
-                    help="skip the batched-commit and serving measurements")
+                    help="skip the secondary configurations (config 1, RAA, num_vars 20, batched "
+                         "commit, serving, PIOP steps)")
     ap.add_argument("--sumcheck-case", type=int, metavar="NV",
                     help="only run the CPR sumcheck at 2^NV points (small case for ncu captures)")
     ap.add_argument("--zinc-prove-case", type=int, metavar="NV",

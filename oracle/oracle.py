@@ -45,6 +45,78 @@ class ScGroup(C.Structure):
                 ("factor_a", C.c_void_p), ("factor_b", C.c_void_p)]
 
 
+class UairDesc(C.Structure):
+    """Mirror of ``zr_uair``: a constraint system over [binary up, integer up,
+    down] columns (see zipref.h)."""
+
+    _fields_ = [("n_bin", C.c_uint32), ("n_int", C.c_uint32), ("n_pub_bin", C.c_uint32),
+                ("n_pub_int", C.c_uint32), ("D", C.c_uint32), ("n_shifts", C.c_uint32),
+                ("shift_src", C.c_void_p), ("shift_amt", C.c_void_p), ("n_cons", C.c_uint32),
+                ("term_off", C.c_void_p), ("term_coeff", C.c_void_p), ("fac_off", C.c_void_p),
+                ("fac_col", C.c_void_p), ("ideal_kind", C.c_void_p), ("ideal_root", C.c_void_p)]
+
+
+class Uair:
+    """A UAIR for the oracle's Zinc+ prover and verifier: `constraints` is a list
+    of constraints, each a list of terms (integer coefficient, [column indices
+    into up (binary, then integer) and down (shift order)]); `ideals` one root
+    c per constraint for the ideal (X - c), or None for the zero ideal."""
+
+    def __init__(self, n_bin, n_int, D, shifts, constraints, ideals, n_pub_bin=0, n_pub_int=0):
+        self.n_bin, self.n_int, self.D = n_bin, n_int, D
+        self.shifts, self.constraints, self.ideals = list(shifts), constraints, ideals
+        self.n_pub_bin, self.n_pub_int = n_pub_bin, n_pub_int
+        toff, coef, foff, fcol = [0], [], [0], []
+        for terms in constraints:
+            for c, facs in terms:
+                coef.append(int(c))
+                fcol.extend(int(x) for x in facs)
+                foff.append(len(fcol))
+            toff.append(len(coef))
+        self._a = dict(
+            src=np.array([s for s, _ in self.shifts] or [0], np.uint32),
+            amt=np.array([a for _, a in self.shifts] or [0], np.uint32),
+            toff=np.array(toff, np.uint32), coef=np.array(coef or [0], np.int64),
+            foff=np.array(foff, np.uint32), fcol=np.array(fcol or [0], np.uint32),
+            kind=np.array([0 if r is None else 1 for r in ideals] or [0], np.uint8),
+            root=np.array([0 if r is None else int(r) for r in ideals] or [0], np.int64))
+        a = self._a
+        self.desc = UairDesc(n_bin, n_int, n_pub_bin, n_pub_int, D, len(self.shifts), _ptr(a["src"]),
+                             _ptr(a["amt"]), len(constraints), _ptr(a["toff"]), _ptr(a["coef"]),
+                             _ptr(a["foff"]), _ptr(a["fcol"]), _ptr(a["kind"]), _ptr(a["root"]))
+
+    @classmethod
+    def linear(cls, n_bin, n_int, D, shifts, coeff_rows, roots, n_pub_bin=0, n_pub_int=0):
+        """From integer coefficient rows over [up, down] (one term per nonzero)."""
+        cons = [[(int(c), [j]) for j, c in enumerate(row) if int(c) != 0] for row in coeff_rows]
+        return cls(n_bin, n_int, D, shifts, cons, roots, n_pub_bin, n_pub_int)
+
+
+def zinc_prove(desc_bin: Desc, desc_int: Desc, nvars: int, bin_cols, int_cols, uair: Uair, L: int,
+               mle_first: bool = True) -> bytes:
+    """ZincPlusPiop::prove::<MLE_FIRST> (protocol/src/prover.rs:677-706) in C:
+    the whole chain, steps 0-7, and the Proof transcription."""
+    b, i = _piop_cols(bin_cols, int_cols, nvars)
+    cap = 64 << 20
+    out = C.create_string_buffer(cap)
+    n = C.c_size_t(0)
+    rc = lib().zr_zinc_prove(C.byref(desc_bin), C.byref(desc_int), nvars, _ptr(b), _ptr(i), C.byref(uair.desc), L,
+                             1 if mle_first else 0, out, cap, C.byref(n))
+    if rc:
+        raise ValueError(f"zinc prove failed ({rc})")
+    return out.raw[: n.value]
+
+
+def zinc_verify(desc_bin: Desc, desc_int: Desc, nvars: int, pub_bin, pub_int, uair: Uair, L: int,
+                proof: bytes) -> int:
+    """ZincPlusPiop::verify (protocol/src/verifier.rs:715-771) in C: 0 accepts;
+    otherwise the failing step (1 parse, 2 ideal check, 4 CPR, 5 multipoint, 6
+    lifted evaluations, 7 PCS)."""
+    b, i = _piop_cols(pub_bin, pub_int, nvars)
+    return lib().zr_zinc_verify(C.byref(desc_bin), C.byref(desc_int), nvars, _ptr(b), _ptr(i), C.byref(uair.desc),
+                                L, _buf(proof), len(proof))
+
+
 def build() -> str:
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
@@ -111,6 +183,10 @@ def lib():
         L.zr_tr_field_challenge.argtypes = [vp, vp, u32, vp]
         L.zr_tr_absorb_field.argtypes = [vp, vp, u32, vp]
         L.zr_commit_prove_f.argtypes = [C.POINTER(Desc), vp, u32, vp, vp, vp, sz, C.POINTER(C.c_size_t), vp, vp]
+        up = C.POINTER(UairDesc)
+        L.zr_zinc_prove.argtypes = [C.POINTER(Desc), C.POINTER(Desc), u32, vp, vp, up, u32, C.c_int, vp, sz,
+                                    C.POINTER(sz)]
+        L.zr_zinc_verify.argtypes = [C.POINTER(Desc), C.POINTER(Desc), u32, vp, vp, up, u32, vp, sz]
         _lib = L
     return _lib
 
@@ -535,7 +611,8 @@ def piop_ideal_check_linear(t: "Transcript", modulus: int, L: int, bin_cols, D: 
                             shifts, coeffs):
     """IdealCheckProtocol::prove_linear (piop/src/ideal_check.rs:137-176) restated:
     nvars field challenges as the point, the up and shifted down columns evaluated
-    coefficient-wise there (compute_lifted_evals on the columns), each constraint's
+    coefficient-wise there with the last row read as zero (compute_lifted_evals on
+    copies of the columns whose last entry is cleared), each constraint's
     coefficients (standard integers) applied, trimmed, absorbed.  Returns
     (point (nvars, L), [combined (len, L) per constraint])."""
     p, R = modulus, 1 << (64 * L)
@@ -552,6 +629,12 @@ def piop_ideal_check_linear(t: "Transcript", modulus: int, L: int, bin_cols, D: 
     di = [shifted(i[sc - nb], c) for sc, c in shifts if sc >= nb]
     eb = np.stack(list(b) + db) if nb + len(db) else None
     ei = np.stack(list(i) + di) if ni + len(di) else None
+    # evaluate_combined_polynomials (ideal_check/combined_poly_builder.rs:232-252)
+    # reads zero on the last row of every up and down column
+    if eb is not None:
+        eb[:, -1] = 0
+    if ei is not None:
+        ei[:, -1] = 0
     vals = piop_lifted_evals(p, L, eb, D, ei, nvars, point)
     nb2 = nb + len(db)
 

@@ -1818,38 +1818,26 @@ static int rget(rbuf *r, void *dst, size_t n) {
     return 0;
 }
 
-/* ZipPlus::verify (phase_verify.rs:100-304).  0 = accept. */
-int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const int64_t *point,
-              const uint8_t *eval_inner, const uint8_t *proof, size_t proof_len) {
-    zparams z;
-    if (batch == 0 || zparams_build(d, &z)) return -1;
-    if (validate_bits(&z, batch)) {
-        zparams_free(&z);
-        return -2;
-    }
+/* ZipPlus::verify_with_alphas (phase_verify.rs:137-304) after the point is in
+ * the field: reads b, the combined row and the openings from rd (the PCS
+ * stream) while absorbing into tr; alphas: batch x max(D, 1) per-poly
+ * challenges (sample_alphas, phase_verify.rs:247-261).  0 = accept, 2 = a
+ * check failed, 3 = malformed stream. */
+static int verify_core(const zparams *z, const uint8_t root[32], uint32_t batch, zr_transcript *tr, const fcfg *fp,
+                       const uint64_t *pf, const uint64_t *eval_f, const i128 *alphas, rbuf *rd) {
+    const fcfg f = *fp;
     int rc = 0;
-    uint32_t L = d->field_limbs, C = d->comb_limbs, R = z.num_rows, RL = z.row_len, D = z.D;
-    zr_transcript *tr = zr_tr_new();
-    zr_tr_absorb_slice(tr, root, 32);
-    fcfg f;
-    uint64_t *pf = (uint64_t *)calloc((size_t)d->num_vars + 1, 8 * L);
-    read_prime_and_points(tr, &z, point, &f, pf);
-    i128 *alphas = (i128 *)malloc(sizeof(i128) * batch * (D > 1 ? D : 1));
-    for (uint32_t b = 0; b < batch; b++) {
-        if (D > 1)
-            for (uint32_t i = 0; i < D; i++) alphas[b * D + i] = tr_i128(tr);
-        else alphas[b] = 1;
-    }
+    const zr_desc *d = &z->d;
+    uint32_t L = d->field_limbs, C = d->comb_limbs, R = z->num_rows, RL = z->row_len, D = z->D;
     uint64_t *q0 = (uint64_t *)malloc(8 * L * (size_t)R), *q1 = (uint64_t *)malloc(8 * L * (size_t)RL);
-    point_tensor(&f, &z, pf, q0, q1);
-    rbuf rd = {proof, proof_len, 0};
+    point_tensor(&f, z, pf, q0, q1);
     uint64_t *bv = (uint64_t *)calloc((size_t)R, 8 * L);
     uint64_t *comb = NULL, *enc = NULL;
     i128 *coeffs = (i128 *)malloc(sizeof(i128) * R);
     uint8_t *col = NULL, *sib = NULL;
     for (uint32_t j = 0; j < R; j++) {
         uint64_t mod[4] = {0}, inner[4] = {0};
-        if (rget(&rd, mod, 8 * L) || rget(&rd, inner, 8 * L)) { rc = 3; goto out; }
+        if (rget(rd, mod, 8 * L) || rget(rd, inner, 8 * L)) { rc = 3; goto out; }
         if (ucmp(mod, f.p, L) != 0) { rc = 2; goto out; }
         tr_absorb_field(tr, &f, inner);
         memcpy(bv + (size_t)j * L, inner, 8 * L);
@@ -1861,14 +1849,14 @@ int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const in
             fmul(&f, q0 + (size_t)j * L, bv + (size_t)j * L, t);
             fadd(&f, ev, t);
         }
-        if (memcmp(ev, eval_inner, 8 * L)) { rc = 2; goto out; }
+        if (memcmp(ev, eval_f, 8 * L)) { rc = 2; goto out; }
     }
     if (R == 1) coeffs[0] = 1;
     else
         for (uint32_t j = 0; j < R; j++) coeffs[j] = tr_i128(tr);
     comb = (uint64_t *)malloc((size_t)RL * 8 * C);
-    if (rget(&rd, comb, (size_t)RL * 8 * C)) { rc = 3; goto out; }
-    enc = (uint64_t *)malloc((size_t)z.codeword_len * 8 * C);
+    if (rget(rd, comb, (size_t)RL * 8 * C)) { rc = 3; goto out; }
+    enc = (uint64_t *)malloc((size_t)z->codeword_len * 8 * C);
     zr_encode_wide(d, comb, C, enc);
     {
         uint64_t lhs[4] = {0}, rhs[4] = {0};
@@ -1887,22 +1875,22 @@ int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const in
         if (memcmp(lhs, rhs, 8 * L)) { rc = 2; goto out; }
     }
     {
-        size_t colbytes = (size_t)batch * R * z.cw_bytes;
+        size_t colbytes = (size_t)batch * R * z->cw_bytes;
         col = (uint8_t *)malloc(colbytes);
         sib = (uint8_t *)malloc(32 * 64);
         for (uint32_t o = 0; o < d->num_openings; o++) {
-            uint32_t idx = tr_u32(tr) % z.codeword_len;
+            uint32_t idx = tr_u32(tr) % z->codeword_len;
             uint64_t li, lc, np;
-            if (rget(&rd, col, colbytes) || rget(&rd, &li, 8) || rget(&rd, &lc, 8) || rget(&rd, &np, 8)) { rc = 3; goto out; }
+            if (rget(rd, col, colbytes) || rget(rd, &li, 8) || rget(rd, &lc, 8) || rget(rd, &np, 8)) { rc = 3; goto out; }
             if (np == 0 || np > 64 || li >= lc) { rc = 3; goto out; }
-            if (rget(&rd, sib, 32 * np)) { rc = 3; goto out; }
+            if (rget(rd, sib, 32 * np)) { rc = 3; goto out; }
             /* check 3 (phase_verify.rs:267-304) */
             uint64_t acc[8] = {0};
             for (uint32_t b = 0; b < batch; b++)
                 for (uint32_t j = 0; j < R; j++) {
-                    const uint8_t *e = col + ((size_t)b * R + j) * z.cw_bytes;
+                    const uint8_t *e = col + ((size_t)b * R + j) * z->cw_bytes;
                     uint64_t v[8] = {0};
-                    if (z.d.eval_kind != ZR_EVAL_BINPOLY) {
+                    if (z->d.eval_kind != ZR_EVAL_BINPOLY) {
                         uint64_t x[8];
                         memcpy(x, e, 16);
                         uint64_t sg = (x[1] >> 63) ? ~0ull : 0;
@@ -1912,7 +1900,7 @@ int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const in
                         for (uint32_t i = 0; i < D; i++) {
                             uint64_t x[8];
                             int64_t c64;
-                            if (z.cw_bytes == 8 * D) memcpy(&c64, e + 8 * i, 8);
+                            if (z->cw_bytes == 8 * D) memcpy(&c64, e + 8 * i, 8);
                             else {
                                 int32_t c32;
                                 memcpy(&c32, e + 4 * i, 4);
@@ -1938,6 +1926,34 @@ out:
     free(bv);
     free(q0);
     free(q1);
+    return rc;
+}
+
+/* ZipPlus::verify (phase_verify.rs:100-304).  0 = accept. */
+int zr_verify(const zr_desc *d, const uint8_t root[32], uint32_t batch, const int64_t *point,
+              const uint8_t *eval_inner, const uint8_t *proof, size_t proof_len) {
+    zparams z;
+    if (batch == 0 || zparams_build(d, &z)) return -1;
+    if (validate_bits(&z, batch)) {
+        zparams_free(&z);
+        return -2;
+    }
+    uint32_t L = d->field_limbs, D = z.D;
+    zr_transcript *tr = zr_tr_new();
+    zr_tr_absorb_slice(tr, root, 32);
+    fcfg f;
+    uint64_t *pf = (uint64_t *)calloc((size_t)d->num_vars + 1, 8 * L);
+    read_prime_and_points(tr, &z, point, &f, pf);
+    i128 *alphas = (i128 *)malloc(sizeof(i128) * batch * (D > 1 ? D : 1));
+    for (uint32_t b = 0; b < batch; b++) {
+        if (D > 1)
+            for (uint32_t i = 0; i < D; i++) alphas[b * D + i] = tr_i128(tr);
+        else alphas[b] = 1;
+    }
+    uint64_t ev[4] = {0};
+    memcpy(ev, eval_inner, 8 * L);
+    rbuf rd = {proof, proof_len, 0};
+    int rc = verify_core(&z, root, batch, tr, &f, pf, ev, alphas, &rd);
     free(alphas);
     free(pf);
     zr_tr_free(tr);
@@ -2403,3 +2419,6 @@ int zr_commit_prove_f(const zr_desc *d, const void *polys, uint32_t batch, const
     g_point_u256 = NULL;
     return rc;
 }
+
+/* The Zinc+ PIOP prover chain and verifier (oracle). */
+#include "zinc_piop.c"

@@ -134,6 +134,30 @@ void zr_piop_lifted_evals(const uint64_t *modulus, uint32_t L, const uint64_t *b
                           uint32_t D, const int64_t *ints, uint32_t n_int, uint32_t nvars,
                           const uint64_t *point, uint64_t *out);
 
+/* A UAIR as a constraint system over the columns [binary up..., integer up...,
+ * down (one per shift)]: constraint k is sum over its terms t of
+ * term_coeff[t] * prod_{q in [fac_off[t], fac_off[t+1])} column fac_col[q],
+ * in the zero ideal (ideal_kind 0) or in (X - ideal_root[k]) (ideal_kind 1).
+ * The first n_pub_bin / n_pub_int columns of each kind are public. */
+typedef struct {
+    uint32_t n_bin, n_int, n_pub_bin, n_pub_int, D;
+    uint32_t n_shifts;
+    const uint32_t *shift_src, *shift_amt;
+    uint32_t n_cons;
+    const uint32_t *term_off;
+    const int64_t *term_coeff;
+    const uint32_t *fac_off;
+    const uint32_t *fac_col;
+    const uint8_t *ideal_kind;
+    const int64_t *ideal_root;
+} zr_uair;
+/* ZincPlusPiop::prove (MLE first or combined) and ZincPlusPiop::verify; see
+ * zinc_piop.c.  bin: n_bin x 2^nvars BinaryPoly<D>, ints: n_int x 2^nvars. */
+int zr_zinc_prove(const zr_desc *db, const zr_desc *di, uint32_t nvars, const uint64_t *bin, const int64_t *ints,
+                  const zr_uair *u, uint32_t L, int mle_first, uint8_t *out, size_t cap, size_t *out_len);
+int zr_zinc_verify(const zr_desc *db, const zr_desc *di, uint32_t nvars, const uint64_t *pub_bin,
+                   const int64_t *pub_int, const zr_uair *u, uint32_t L, const uint8_t *proof, size_t len);
+
 /* threads used by the parallel regions */
 void zr_set_threads(int n);
 int zr_get_threads(void);

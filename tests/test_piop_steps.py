@@ -267,7 +267,9 @@ def test_gpu_cpr_linear_prove_matches_oracle(zipgpu, oracle, ctx, L, nv):
 def test_oracle_ideal_check_linear_is_the_definition(oracle, L, nv):
     """Combined value of constraint k = sum_j c_kj sum_b eq(b, r) col_j(b) in F[X],
     col_j the projected column (a binary cell's 0/1 coefficients, an integer as a
-    constant; down columns shifted up by their shift), trimmed."""
+    constant; down columns shifted up by their shift), over the rows b < 2^nv - 1
+    only (evaluate_combined_polynomials, ideal_check/combined_poly_builder.rs:
+    232-252, reads zero on the last row of every column), trimmed."""
     ncols, shifts, rows = biglinear_system()
     D, n = 32, 1 << nv
     p = field(oracle, L)
@@ -289,8 +291,9 @@ def test_oracle_ideal_check_linear_is_the_definition(oracle, L, nv):
             return [(int(b[j, x]) >> l) & 1 for l in range(D)]
         return [int(i[0, x]) % p] + [0] * (D - 1)
 
-    up = [[sum(eq(x) * poly(j, x)[l] for x in range(n)) % p for l in range(D)] for j in range(ncols)]
-    down = [[sum(eq(x) * poly(sc, x + c)[l] for x in range(n - c)) % p for l in range(D)] for sc, c in shifts]
+    up = [[sum(eq(x) * poly(j, x)[l] for x in range(n - 1)) % p for l in range(D)] for j in range(ncols)]
+    down = [[sum(eq(x) * poly(sc, x + c)[l] for x in range(min(n - c, n - 1))) % p for l in range(D)]
+            for sc, c in shifts]
     vals = up + down
     for k, row in enumerate(rows):
         want = [sum(cf * vals[j][l] for j, cf in enumerate(row)) % p for l in range(D)]

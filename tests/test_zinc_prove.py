@@ -217,3 +217,31 @@ def test_gpu_small_uairs_match_oracle(zipgpu, oracle, ctx, nb, ni, shifts, nc, D
                                        n_pub_bin=npb, n_pub_int=npi)
     assert got == want
     parse_proof(got, 3, nv)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nv", [14, 16, 18])
+def test_gpu_biglinear_proof_matches_c_chain_at_size(zipgpu, oracle, ctx, nv):
+    """Config 4's shape (16 rows per table, 192-bit field) at 2^14, 2^16 and
+    2^18 rows: the GPU proof equals the oracle's C chain byte for byte, and the
+    oracle's restated Zinc+ verifier accepts it; a tampered copy is rejected."""
+    from zipgpu import uair
+
+    bins, ints = uair.trace(nv, 0xB16 + nv)
+    shifts, coeffs = uair.signature()
+    L = 1 << (nv - 4)
+    pb = params_for(zipgpu, 1, 32, 0, nv, L, ctx=ctx, comb=6, field=3)
+    pi = params_for(zipgpu, 2, 1, 0, nv, L, ctx=ctx, comb=6, field=3)
+    db, di = desc_for(1, 32, 0, nv, L, comb=6, field=3), desc_for(2, 1, 0, nv, L, comb=6, field=3)
+    got = zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+    U = oracle.Uair.linear(16, 1, 32, shifts, coeffs, uair.ideal_roots())
+    oracle.set_threads(0)
+    want = oracle.zinc_prove(db, di, nv, bins, ints, U, 3, mle_first=True)
+    assert len(got) == len(want)
+    assert got == want
+    assert oracle.zinc_verify(db, di, nv, None, None, U, 3, got) == 0
+    bad = bytearray(got)
+    bad[len(bad) - 100] ^= 1  # inside the witness lifted evaluations
+    assert oracle.zinc_verify(db, di, nv, None, None, U, 3, bytes(bad)) != 0
+    pb.close()
+    pi.close()

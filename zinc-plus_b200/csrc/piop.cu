@@ -1005,7 +1005,8 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
 // Step 2 for a linear UAIR (IdealCheckProtocol::prove_linear, piop/src/ideal_check.rs:
 // 137-176, MLE first): the point r from the transcript, every up column and every
 // shifted (down) column evaluated coefficient-wise at r (the lifted-evaluation sums
-// on copies of the columns, the down ones shifted up and zero padded), each
+// on copies of the columns, the down ones shifted up and zero padded, the last row
+// of every copy cleared as the reference's evaluate_combined_polynomials reads it), each
 // constraint's coefficients applied to those polynomial values, and the trimmed
 // combined values absorbed constraint after constraint.
 extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
@@ -1065,6 +1066,11 @@ extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, c
         for (size_t q = 0; q < dint.size(); q++)
             ZG_CUDA(shifted(ei + (n_int + q) * n, int_cols + (size_t)(shift_src[dint[q]] - n_bin) * n,
                             shift_amount[dint[q]]));
+        // evaluate_combined_polynomials (ideal_check/combined_poly_builder.rs:232-252)
+        // reads zero on the last row of every up and down column: clear entry
+        // 2^nvars - 1 of each extended column (one strided memset per kind)
+        if (nb2) ZG_CUDA(cudaMemset2DAsync(eb + (n - 1), n * 8, 0, 8, nb2, s));
+        if (ni2) ZG_CUDA(cudaMemset2DAsync(ei + (n - 1), n * 8, 0, 8, ni2, s));
         const PiopCols ext{eb, nb2, D, ei, ni2, nvars};
         std::vector<uint64_t> vals(((size_t)nb2 * D + ni2) * L);
         ZG_TRY(L == 3 ? lifted_evals_t<3>(ctx, f, ext, point_out, 1, vals.data())

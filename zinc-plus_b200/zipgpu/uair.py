@@ -36,6 +36,11 @@ def signature():
     return shifts, np.stack(rows)
 
 
+def ideal_roots():
+    """The root c of each constraint's ideal (X - c), in constraint order."""
+    return [1, 2] + [1] * (N_BIN - 1)
+
+
 def _popcount32(x: np.ndarray) -> np.ndarray:
     x = x.astype(np.uint64)
     c = np.zeros(x.shape, np.int64)
