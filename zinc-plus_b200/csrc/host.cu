@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cstring>
 
+#include <functional>
+
 #include "zg_internal.h"
 
 namespace zg {
@@ -394,17 +396,31 @@ bool is_probable_prime_base2(const uint64_t *n, int L) {
 
 // get_prime: candidates are drawn one after another from the transcript
 // (each absorbed raw); the first that passes Miller-Rabin is kept.  Candidates
-// are generated ahead in groups and tested in parallel; the transcript is
-// then rewound to the state right after the accepted candidate, so the result
-// and the transcript state equal the sequential loop's.
-void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads) {
+// are generated ahead in groups and tested in parallel (run_all(n, test) runs
+// test(0..n-1), possibly on several threads); the transcript is then rewound to
+// the state right after the accepted candidate, so the result and the
+// transcript state equal the sequential loop's.
+void tr_get_prime_batched(zg_transcript *t, int L, uint64_t *prime_out, int group,
+                          const std::function<void(int, const std::function<void(int)> &)> &run_all) {
     const int nb = 8 * L;
-    const int team = threads > 0 ? threads : omp_get_max_threads();
-    // candidates generated ahead per round (speculative; a single thread tests one at a time)
-    const int group = team == 1 ? 1 : std::max(8, 2 * team);
+    group = std::max(1, group);
     std::vector<b3::Hasher> states(group);
     std::vector<uint64_t> cand((size_t)group * 4);
     std::vector<char> ok(group);
+    const std::function<void(int)> test = [&](int g) {
+        uint64_t *c = &cand[(size_t)g * 4];
+        bool zero = true;
+        for (int i = 0; i < L; i++) zero = zero && c[i] == 0;
+        if (zero) {
+            ok[g] = 0;
+            return;
+        }
+        if (!(c[0] & 1)) {  // even: subtract one (full-width borrow)
+            for (int i = 0; i < L; i++)
+                if (c[i]-- != 0) break;
+        }
+        ok[g] = is_probable_prime_base2(c, L) ? 1 : 0;
+    };
     for (;;) {
         b3::Hasher h = t->h;
         for (int g = 0; g < group; g++) {
@@ -416,21 +432,7 @@ void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads) {
             std::memset(c, 0, 32);
             std::memcpy(c, buf, nb);
         }
-#pragma omp parallel for schedule(dynamic, 1) num_threads(team)
-        for (int g = 0; g < group; g++) {
-            uint64_t *c = &cand[(size_t)g * 4];
-            bool zero = true;
-            for (int i = 0; i < L; i++) zero = zero && c[i] == 0;
-            if (zero) {
-                ok[g] = 0;
-                continue;
-            }
-            if (!(c[0] & 1)) {  // even: subtract one (full-width borrow)
-                for (int i = 0; i < L; i++)
-                    if (c[i]-- != 0) break;
-            }
-            ok[g] = is_probable_prime_base2(c, L) ? 1 : 0;
-        }
+        run_all(group, test);
         for (int g = 0; g < group; g++) {
             if (ok[g]) {
                 t->h = states[g];
@@ -440,6 +442,20 @@ void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads) {
         }
         t->h = states[group - 1];
     }
+}
+
+void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads) {
+    const int team = threads > 0 ? threads : omp_get_max_threads();
+    // candidates generated ahead per round (speculative; a single thread tests one at a time)
+    const int group = team == 1 ? 1 : std::max(8, 2 * team);
+    tr_get_prime_batched(t, L, prime_out, group, [team](int n, const std::function<void(int)> &fn) {
+        if (team == 1) {
+            for (int g = 0; g < n; g++) fn(g);
+            return;
+        }
+#pragma omp parallel for schedule(dynamic, 1) num_threads(team)
+        for (int g = 0; g < n; g++) fn(g);
+    });
 }
 
 // ------------------------------------------------------------ IPRS tables

@@ -19,6 +19,8 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <functional>
+#include <memory>
 #include <thread>
 #include <unordered_map>
 
@@ -63,6 +65,81 @@ size_t request_footprint(const zg_params *p) {
     return input + cw + tree + stage + chunks + wprime + (1u << 20);
 }
 
+// Host threads that test prime candidates for every worker.  Between rounds
+// they sleep on a condition variable (threads spinning between parallel
+// regions starved the workers' kernel launches), and the worker that posts a
+// round tests candidates too, so a round ends as soon as its tests do.
+class TestPool {
+  public:
+    explicit TestPool(int threads) {
+        for (int i = 0; i < threads; i++) th_.emplace_back([this] { loop(); });
+    }
+    ~TestPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    int threads() const { return (int)th_.size(); }
+    // Runs fn(0..n-1) on the pool and the calling thread; returns when all ran.
+    void run_all(int n, const std::function<void(int)> &fn) {
+        auto job = std::make_shared<Job>();
+        job->n = n;
+        job->fn = &fn;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back(job);
+        }
+        cv_.notify_all();
+        for (int i; (i = job->next.fetch_add(1)) < n;) {
+            fn(i);
+            finish(*job);
+        }
+        std::unique_lock<std::mutex> lk(job->m);
+        job->cv.wait(lk, [&] { return job->done == job->n; });
+    }
+
+  private:
+    struct Job {
+        int n = 0;
+        const std::function<void(int)> *fn = nullptr;
+        std::atomic<int> next{0};
+        int done = 0;
+        std::mutex m;
+        std::condition_variable cv;
+    };
+    static void finish(Job &j) {
+        std::lock_guard<std::mutex> lk(j.m);
+        if (++j.done == j.n) j.cv.notify_all();
+    }
+    void loop() {
+        for (;;) {
+            std::shared_ptr<Job> job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;  // stopping
+                job = q_.front();
+                if (job->next.load() >= job->n) {  // every test claimed
+                    q_.pop_front();
+                    continue;
+                }
+            }
+            const int i = job->next.fetch_add(1);
+            if (i >= job->n) continue;
+            (*job->fn)(i);
+            finish(*job);
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::shared_ptr<Job>> q_;
+    bool stop_ = false;
+};
+
 }  // namespace
 
 struct zg_server {
@@ -80,7 +157,8 @@ struct zg_server {
     uint64_t completed = 0, groups = 0, grouped_requests = 0, in_flight = 0;
     double ms_input = 0, ms_commit = 0, ms_prime = 0, ms_prove = 0;  // summed over workers
     bool stop = false;
-    int prime_threads = 1;
+    std::unique_ptr<TestPool> tests;  // prime candidate tests, shared by the workers
+    int prime_group = 1;              // candidates drawn ahead per round
     ~zg_server() {
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -89,6 +167,7 @@ struct zg_server {
         cv_work.notify_all();
         for (auto &t : workers)
             if (t.joinable()) t.join();
+        tests.reset();
         for (auto &kv : reqs) delete kv.second;
         for (zg_ctx *l : lanes) zg_ctx_destroy(l);
         if (pool) cudaMemPoolDestroy(pool);
@@ -171,7 +250,7 @@ void run_group(zg_server *s, zg_ctx *lane, std::vector<Request *> &g, std::vecto
             set_error("input copy failed: %s", cudaGetErrorString(cudaGetLastError()));
             st = ZG_ERR_CUDA;
         }
-    if (st == ZG_OK && ctx_sync(lane) != cudaSuccess) st = ZG_ERR_CUDA;
+    // no wait here: the commit kernels follow the copies on the lane's stream
     t_in = ms_since(tick);
     tick = Clock::now();
     std::vector<zg_hint *> hints(m, nullptr);
@@ -194,7 +273,8 @@ void run_group(zg_server *s, zg_ctx *lane, std::vector<Request *> &g, std::vecto
         tr_absorb_slice(&t, r->root, 32);
         uint64_t prime[MAX_FIELD_LIMBS] = {0, 0, 0, 0};
         tick = Clock::now();
-        tr_get_prime(&t, (int)p->d.field_limbs, prime, s->prime_threads);
+        tr_get_prime_batched(&t, (int)p->d.field_limbs, prime, s->prime_group,
+                             [s](int n, const std::function<void(int)> &fn) { s->tests->run_all(n, fn); });
         field_cfg_init(t.f, prime, (int)p->d.field_limbs);
         t.has_field = true;
         t_prime += ms_since(tick);
@@ -331,10 +411,15 @@ zg_status zg_server_create(zg_ctx *ctx, const zg_server_opts *opts, zg_server **
                                              cudaEventBlockingSync | cudaEventDisableTiming));
             s->lanes.push_back(l);
         }
-        // Each worker samples its primes on its own thread: OpenMP teams per
-        // worker spin-wait between regions and starve the other workers'
-        // launches on a shared host.
-        s->prime_threads = 1;
+        // Prime candidates are tested by one pool of sleeping threads shared by
+        // the workers (OpenMP teams per worker spin-waited between regions and
+        // starved the other workers' launches on a shared host).
+        {
+            const int hw = (int)std::max(2u, std::thread::hardware_concurrency());
+            const int nt = std::max(1, std::min(16, hw / 2));
+            s->tests.reset(new TestPool(nt));
+            s->prime_group = std::max(8, 2 * (nt + 1));
+        }
         zg_server *raw = s.get();
         for (uint32_t i = 0; i < o.workers; i++) raw->workers.emplace_back(worker_main, raw, i);
         *out = s.release();

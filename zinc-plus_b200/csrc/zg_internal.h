@@ -9,6 +9,7 @@
 #include <memory>
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -270,6 +271,9 @@ void tr_absorb_field(zg_transcript *t, const uint64_t *inner);
 // get_prime::<Uint<L>, MillerRabin> (transcript/src/lib.rs:58-72).
 // threads: 0 = the OpenMP default team.
 void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads);
+// The same search with the candidate tests of each round run by run_all(n, test).
+void tr_get_prime_batched(zg_transcript *t, int L, uint64_t *prime_out, int group,
+                          const std::function<void(int, const std::function<void(int)> &)> &run_all);
 bool is_probable_prime_base2(const uint64_t *n, int L);
 
 // IPRS parameters (params.rs:59-196); returns false if the reference rejects.
