@@ -526,6 +526,41 @@ zg_status zg_zinc_prove_mle_first(zg_params *pp_bin, zg_params *pp_int, const zg
                                   uint32_t num_vars, const uint64_t *bin_cols, const int64_t *int_cols,
                                   int cols_on_device, uint8_t *proof, size_t *proof_len);
 
+/* ---- ZincPlusPiop::prove, both paths (protocol/src/prover.rs:677-706) --------
+ * mle_first != 0: step1_mle_first + prove_linear, as zg_zinc_prove_mle_first
+ * (linear constraints only); mle_first == 0: step1_combined + prove_combined
+ * (the path the reference's Verify bench proves with, protocol/benches/
+ * e2e.rs:346-354), which takes constraints of degree two and sends an empty
+ * ideal-check value for each constraint in the zero ideal (ideal_check.rs:
+ * 178-240).  The UAIR is a list of terms: constraint k is the sum over its
+ * terms t in [term_offsets[k], term_offsets[k+1]) of term_coeffs[t] times the
+ * product of the columns factor_cols[factor_offsets[t] .. factor_offsets[t+1])
+ * (indices into [binary up, integer up, down in shift order]); a term has one
+ * or two columns (constant terms are not taken).  zero_ideal[k] != 0 when
+ * constraint k lies in the zero ideal (IdealOrZero::Zero).  Everything else
+ * (tables, columns, public columns, proof buffer) is as for
+ * zg_zinc_prove_mle_first. */
+typedef struct {
+    uint32_t n_bin;
+    uint32_t n_int;
+    uint32_t degree_plus_one;
+    uint32_t n_shifts;
+    const uint32_t *shift_src;
+    const uint32_t *shift_amount;
+    uint32_t n_constraints;
+    const uint32_t *term_offsets;   /* n_constraints + 1, starting at 0 */
+    const int64_t *term_coeffs;     /* one per term */
+    const uint32_t *factor_offsets; /* n_terms + 1 */
+    const uint32_t *factor_cols;
+    const uint8_t *zero_ideal;      /* one per constraint */
+    uint32_t n_pub_bin;
+    uint32_t n_pub_int;
+} zg_uair;
+
+zg_status zg_zinc_prove(zg_params *pp_bin, zg_params *pp_int, const zg_uair *uair, uint32_t num_vars,
+                        const uint64_t *bin_cols, const int64_t *int_cols, int cols_on_device, int mle_first,
+                        uint8_t *proof, size_t *proof_len);
+
 #ifdef __cplusplus
 }
 #endif

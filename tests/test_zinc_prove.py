@@ -245,3 +245,99 @@ def test_gpu_biglinear_proof_matches_c_chain_at_size(zipgpu, oracle, ctx, nv):
     assert oracle.zinc_verify(db, di, nv, None, None, U, 3, bytes(bad)) != 0
     pb.close()
     pi.close()
+
+
+def _terms_of_rows(coeffs):
+    """Constraint rows over [up, down] as terms (one column each)."""
+    return [[(int(c), [j]) for j, c in enumerate(row) if int(c) != 0] for row in coeffs]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nv", [10, 14])
+def test_gpu_combined_path_biglinear_matches_oracle(zipgpu, oracle, ctx, nv):
+    """The reference's default path (MLE_FIRST = false: step1_combined,
+    prove_combined) on BigLinearUair: the GPU bytes equal the oracle's combined
+    chain, and, BigLinear's ideals being non-zero, the MLE-first bytes too."""
+    from zipgpu import uair
+
+    bins, ints = uair.trace(nv, 40 + nv)
+    shifts, coeffs = uair.signature()
+    pb, pi, db, di = tables(zipgpu, nv, 32, ctx)
+    cons = _terms_of_rows(coeffs)
+    got = zipgpu.ZincPlusPiop.prove(pb, pi, nv, bins, 32, ints, shifts, cons, [False] * len(cons), mle_first=False)
+    U = oracle.Uair.linear(16, 1, 32, shifts, coeffs, uair.ideal_roots())
+    oracle.set_threads(0)
+    want = oracle.zinc_prove(db, di, nv, bins, ints, U, 3, mle_first=False)
+    assert got == want
+    assert got == zipgpu.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+    assert oracle.zinc_verify(db, di, nv, None, None, U, 3, got) == 0
+
+
+@pytest.mark.gpu
+def test_gpu_combined_path_skips_zero_ideals(zipgpu, oracle, ctx):
+    nv, D = 8, 8
+    rng = np.random.default_rng(5)
+    shifts = [(0, 1), (2, 3)]
+    bins, ints, coeffs = small_uair(rng, 2, 2, shifts, 3, D, nv)
+    pb, pi, db, di = tables(zipgpu, nv, D, ctx)
+    zero = [True, False, True]
+    cons = _terms_of_rows(coeffs)
+    got = zipgpu.ZincPlusPiop.prove(pb, pi, nv, bins, D, ints, shifts, cons, zero, mle_first=False)
+    U = oracle.Uair.linear(2, 2, D, shifts, coeffs, [None, 1, None])
+    assert got == oracle.zinc_prove(db, di, nv, bins, ints, U, 3, mle_first=False)
+    P = parse_proof(got, 3, nv)
+    assert P["ic"][0] == b"" and P["ic"][2] == b""
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nv", [8, 12])
+def test_gpu_combined_path_products_match_oracle_and_verify(zipgpu, oracle, ctx, nv):
+    """A UAIR of degree two (integer x integer, binary x integer and binary x
+    binary products, a shifted factor): the combined path's ideal check sums the
+    product polynomials row by row and the CPR comb has degree four; the bytes
+    equal the oracle's and its restated verifier accepts them."""
+    n = 1 << nv
+    rng = np.random.default_rng(nv)
+    D = 16
+    x = rng.integers(-(2**20), 2**20, size=n, dtype=np.int64)
+    y = rng.integers(-(2**20), 2**20, size=n, dtype=np.int64)
+    w = rng.integers(0, 1 << D, size=n, dtype=np.uint64)
+    v = rng.integers(0, 1 << D, size=n, dtype=np.uint64)
+    bins, ints = np.stack([w, v]), np.stack([x, y, x * y])
+    # columns: up [w 0, v 1, x 2, y 3, z 4], down [w shifted by 1 (5), y shifted by 2 (6)]
+    shifts = [(0, 1), (3, 2)]
+    cons = [
+        [(1, [2, 3]), (-1, [4])],                 # x * y - z = 0 (zero ideal)
+        [(2, [0, 2]), (-1, [1, 3]), (3, [6])],    # 2 w x - v y + 3 y_down   in (X - 1)
+        [(1, [0, 1]), (-1, [5, 5]), (1, [1])],    # w v - w_down^2 + v        in (X - 2)
+    ]
+    zero = [True, False, False]
+    pb, pi, db, di = tables(zipgpu, nv, D, ctx)
+    got = zipgpu.ZincPlusPiop.prove(pb, pi, nv, bins, D, ints, shifts, cons, zero, mle_first=False)
+    U = oracle.Uair(2, 3, D, shifts, cons, [None, 1, 2])
+    want = oracle.zinc_prove(db, di, nv, bins, ints, U, 3, mle_first=False)
+    assert got == want
+    P = parse_proof(got, 3, nv)
+    assert P["degree"] == 4 and P["ic"][0] == b""
+    # the honest x * y = z constraint passes; the other two are not in their ideals
+    # for random columns, which the verifier's ideal check rejects (step 2)
+    assert oracle.zinc_verify(db, di, nv, None, None, U, 3, got) == 2
+    U2 = oracle.Uair(2, 3, D, shifts, cons, [None, None, None])
+    got2 = zipgpu.ZincPlusPiop.prove(pb, pi, nv, bins, D, ints, shifts, cons, [True] * 3, mle_first=False)
+    assert got2 == oracle.zinc_prove(db, di, nv, bins, ints, U2, 3, mle_first=False)
+    assert oracle.zinc_verify(db, di, nv, None, None, U2, 3, got2) == 4  # the CPR sum is not zero
+    with pytest.raises(zipgpu.ZipError):  # MLE first takes linear constraints only
+        zipgpu.ZincPlusPiop.prove(pb, pi, nv, bins, D, ints, shifts, cons, zero, mle_first=True)
+
+
+@pytest.mark.gpu
+def test_gpu_combined_path_honest_product_uair_verifies(zipgpu, oracle, ctx):
+    from test_zinc_oracle_chain import product_uair
+
+    nv, D = 9, 16
+    bins, ints, U = product_uair(oracle, nv, 3)
+    pb, pi, db, di = tables(zipgpu, nv, D, ctx)
+    got = zipgpu.ZincPlusPiop.prove(pb, pi, nv, bins, D, ints, U.shifts, U.constraints,
+                                    [r is None for r in U.ideals], mle_first=False)
+    assert got == oracle.zinc_prove(db, di, nv, bins, ints, U, 3, mle_first=False)
+    assert oracle.zinc_verify(db, di, nv, None, None, U, 3, got) == 0

@@ -400,6 +400,69 @@ __global__ void __launch_bounds__(256) k_mle_dots(const uint64_t *__restrict__ m
     }
 }
 
+// Step 2 on the combined path for a term that multiplies two columns
+// (compute_combined_polynomials, ideal_check/combined_poly_builder.rs:30-95):
+// coefficient m (blockIdx.y) of the product polynomial at row b, times eq[b],
+// summed over the rows b < 2^nv - 1 (the last row is zero).  Binary x binary:
+// the coefficient is the count of bit pairs i + j = m, one popcount of u and
+// the bit-reversed w shifted into place, times the table small[count] = F(count);
+// binary x integer: F(y) where bit m is set; integer x integer: F(x) F(y) at m = 0.
+// partials[m][block]: lazy sums reduced once per block.
+template <int L>
+__global__ void __launch_bounds__(256) k_ic_product(IcFactor fa, IcFactor fb, uint64_t dmask, uint32_t nv,
+                                                    const uint64_t *__restrict__ eq,
+                                                    const uint64_t *__restrict__ small, FieldCfg f,
+                                                    uint64_t *__restrict__ partials) {
+    __shared__ Lazy<L> red[256];
+    const size_t n = (size_t)1 << nv;
+    const uint32_t m = blockIdx.y;
+    Lazy<L> z;
+    lazy_zero(z);
+    for (size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x; b + 1 < n; b += (size_t)gridDim.x * blockDim.x) {
+        const size_t ra = b + fa.shift, rb = b + fb.shift;
+        uint64_t t[L];
+        if (fa.bin && fb.bin) {
+            const uint64_t u = ra < n ? fa.bin[ra] & dmask : 0, w = rb < n ? fb.bin[rb] & dmask : 0;
+            const uint64_t rw = __brevll(w);
+            const uint64_t sh = m <= 63 ? (rw >> (63 - m)) : (rw << (m - 63));
+            const int cnt = __popcll(u & sh);
+            if (!cnt) continue;
+            fmul<L>(small + (size_t)cnt * L, eq + b * L, f.p, f.n0, t);
+        } else if (fa.bin || fb.bin) {
+            const IcFactor &fbin = fa.bin ? fa : fb, &fint = fa.bin ? fb : fa;
+            const size_t rbin = fa.bin ? ra : rb, rint = fa.bin ? rb : ra;
+            const uint64_t u = rbin < n ? fbin.bin[rbin] & dmask : 0;
+            if (!((u >> m) & 1)) continue;
+            const int64_t y = rint < n ? fint.ints[rint] : 0;
+            if (!y) continue;
+            uint64_t fy[L];
+            from_i128<L>((i128)y, f, fy);
+            fmul<L>(fy, eq + b * L, f.p, f.n0, t);
+        } else {
+            const int64_t x = ra < n ? fa.ints[ra] : 0, y = rb < n ? fb.ints[rb] : 0;
+            if (!x || !y) continue;
+            uint64_t fx[L], fy[L], xy[L];
+            from_i128<L>((i128)x, f, fx);
+            from_i128<L>((i128)y, f, fy);
+            fmul<L>(fx, fy, f.p, f.n0, xy);
+            fmul<L>(xy, eq + b * L, f.p, f.n0, t);
+        }
+        lazy_add<L>(z, t);
+    }
+    red[threadIdx.x] = z;
+    __syncthreads();
+    for (unsigned h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) lazy_merge<L>(red[threadIdx.x], red[threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        uint64_t r[L];
+        lazy_reduce<L>(red[0], f, r);
+#pragma unroll
+        for (int w = 0; w < L; w++) partials[((size_t)m * gridDim.x + blockIdx.x) * L + w] = r[w];
+    }
+}
+
 struct PiopCols {
     const uint64_t *bin;
     uint32_t n_bin, D;
@@ -684,14 +747,16 @@ template <int L>
 zg_status cpr_prepare(zg_ctx *ctx, zg_transcript *t, const FieldCfg &f, const uint64_t *trace, uint32_t J,
                       uint32_t nv, const uint64_t *point, const uint32_t *src, const uint32_t *shift, uint32_t S,
                       uint32_t n_cons, const uint64_t *coeffs, int on_device, std::vector<uint64_t> &folded,
-                      uint64_t **packed) {
+                      std::vector<uint64_t> &alpha_pows, uint64_t **packed) {
     cudaStream_t s = ctx->stream;
     const size_t n = (size_t)1 << nv, fb = 8 * L, mle = n * fb;
     uint64_t alpha[L], pw[L];
     field_challenge_h<L>(t, f, alpha);  // the folding challenge
     folded.assign((size_t)(J + S) * L, 0);
+    alpha_pows.assign((size_t)n_cons * L, 0);
     std::memcpy(pw, f.one, fb);
     for (uint32_t k = 0; k < n_cons; k++) {
+        std::memcpy(&alpha_pows[(size_t)k * L], pw, fb);
         for (uint32_t j = 0; j < J + S; j++) {
             uint64_t tm[L];
             fmul<L>(pw, coeffs + ((size_t)k * (J + S) + j) * L, f.p, f.n0, tm);
@@ -790,7 +855,66 @@ zg_status cpr_column_evals(zg_ctx *ctx, const FieldCfg &f, uint64_t *pk, uint32_
     return ZG_OK;
 }
 
+template <int L>
+zg_status ic_product_sums_t(zg_ctx *ctx, const FieldCfg &f, const uint64_t *point, uint32_t nv, const IcFactor &a,
+                            const IcFactor &b, uint32_t D, std::vector<uint64_t> &out, uint32_t &len) {
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)1 << nv, fb = 8 * L;
+    const uint32_t la = a.bin ? D : 1, lb = b.bin ? D : 1;
+    len = la + lb - 1;
+    const size_t halves = ((size_t)1 << (nv / 2)) + ((size_t)1 << (nv - nv / 2));
+    const unsigned G = (unsigned)std::max<size_t>(1, std::min<size_t>(128, n / 4096));
+    // [eq: n][r: nv][1 - r: nv][halves][small: 65][partials: len x G]
+    const size_t need = (n + 2 * (size_t)nv + halves + 65 + (size_t)len * G) * fb + 256;
+    ZG_TRY(ctx->piop_arena.ensure(need));
+    uint64_t *eq = ctx->piop_arena.as<uint64_t>(), *r_d = eq + n * L, *omr_d = r_d + (size_t)nv * L;
+    uint64_t *half_d = omr_d + (size_t)nv * L, *small_d = half_d + halves * L, *part_d = small_d + 65 * L;
+    std::vector<uint64_t> omr((size_t)nv * L), small(65 * (size_t)L, 0);
+    for (uint32_t k = 0; k < nv; k++) {
+        std::memcpy(&omr[(size_t)k * L], f.one, fb);
+        fsub<L>(&omr[(size_t)k * L], point + (size_t)k * L, f.p);
+    }
+    for (int c = 1; c <= 64; c++) {  // small[c] = F(c) = (c - 1) * one + one
+        std::memcpy(&small[(size_t)c * L], &small[(size_t)(c - 1) * L], fb);
+        fadd<L>(&small[(size_t)c * L], f.one, f.p);
+    }
+    ZG_CUDA(cudaMemcpyAsync(r_d, point, (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(omr_d, omr.data(), (size_t)nv * fb, cudaMemcpyHostToDevice, s));
+    ZG_CUDA(cudaMemcpyAsync(small_d, small.data(), small.size() * 8, cudaMemcpyHostToDevice, s));
+    ZG_KBEGIN(ctx, s, "k_eq_halves");
+    k_eq_halves<L><<<(unsigned)((halves + 127) / 128), 128, 0, s>>>(r_d, omr_d, nv, f, half_d);
+    ZG_KEND(ctx, s);
+    ZG_KBEGIN(ctx, s, "k_eq_outer");
+    k_eq_outer<L><<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8), 256, 0, s>>>(
+        half_d, nv, f, eq);
+    ZG_KEND(ctx, s);
+    const uint64_t dmask = D >= 64 ? ~0ull : ((1ull << D) - 1);
+    ZG_KBEGIN(ctx, s, "k_ic_product");
+    k_ic_product<L><<<dim3(G, len), 256, 0, s>>>(a, b, dmask, nv, eq, small_d, f, part_d);
+    ZG_KEND(ctx, s);
+    std::vector<uint64_t> part((size_t)len * G * L);
+    ZG_CUDA(cudaMemcpyAsync(part.data(), part_d, part.size() * 8, cudaMemcpyDeviceToHost, s));
+    ZG_CUDA(ctx_sync(ctx));
+    out.assign((size_t)len * L, 0);
+    for (uint32_t m = 0; m < len; m++)
+        for (unsigned g = 0; g < G; g++) fadd<L>(&out[(size_t)m * L], &part[((size_t)m * G + g) * L], f.p);
+    return ZG_OK;
+}
+
 }  // namespace
+
+zg_status ic_product_sums(zg_ctx *ctx, const FieldCfg &f, const uint64_t *point, uint32_t nv, const IcFactor &a,
+                          const IcFactor &b, uint32_t D, std::vector<uint64_t> &out, uint32_t &len) {
+    if (D == 0 || D > 64 || nv == 0 || nv > 28 || (!a.bin && !a.ints) || (!b.bin && !b.ints)) {
+        set_error("ideal check: product term with an empty factor or out-of-range sizes");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ZG_CUDA(cudaSetDevice(ctx->device));
+    return f.L == 3 ? ic_product_sums_t<3>(ctx, f, point, nv, a, b, D, out, len)
+                    : ic_product_sums_t<4>(ctx, f, point, nv, a, b, D, out, len);
+}
+
 }  // namespace zg
 
 using namespace zg;
@@ -904,13 +1028,12 @@ extern "C" zg_status zg_piop_multipoint_eval(zg_ctx *ctx, zg_transcript *t, cons
     }
 }
 
-extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
-                                              uint32_t limbs, const uint64_t *trace_mles, uint32_t num_cols,
-                                              uint32_t nvars, const uint64_t *eval_point,
-                                              const uint32_t *shift_src, const uint32_t *shift_amount,
-                                              uint32_t n_shifts, uint32_t n_constraints, const uint64_t *coeffs,
-                                              int mles_on_device, uint8_t *proof, size_t *proof_len,
-                                              uint64_t *point_out, uint64_t *evals_out) {
+zg_status zg::cpr_prove_impl(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                             const uint64_t *trace_mles, uint32_t num_cols, uint32_t nvars,
+                             const uint64_t *eval_point, const uint32_t *shift_src, const uint32_t *shift_amount,
+                             uint32_t n_shifts, uint32_t n_constraints, const uint64_t *coeffs,
+                             const std::vector<CprProduct> &products, int mles_on_device, uint8_t *proof,
+                             size_t *proof_len, uint64_t *point_out, uint64_t *evals_out) {
     try {
         if (!ctx || !t || !modulus || !trace_mles || !eval_point || !proof || !proof_len || !coeffs ||
             num_cols == 0 || n_constraints == 0 || (n_shifts && (!shift_src || !shift_amount))) {
@@ -938,7 +1061,24 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
             return ZG_ERR_INVALID_PARAM;
         }
         const uint32_t J = num_cols, S = n_shifts;
-        std::vector<uint64_t> folded;
+        uint32_t max_factors = 1;
+        for (const CprProduct &q : products) {
+            if (q.constraint >= n_constraints || q.cols.empty()) {
+                set_error("CPR: product term of constraint %u out of range or without columns", q.constraint);
+                return ZG_ERR_INVALID_PARAM;
+            }
+            for (uint32_t c : q.cols)
+                if (c >= J + S) {
+                    set_error("CPR: product column %u out of range", c);
+                    return ZG_ERR_INVALID_PARAM;
+                }
+            max_factors = std::max<uint32_t>(max_factors, (uint32_t)q.cols.size());
+        }
+        if (max_factors + 2 > 8) {
+            set_error("CPR: products of %u columns make the sumcheck degree exceed 8", max_factors);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        std::vector<uint64_t> folded, alpha_pows;
         uint64_t *packed = nullptr;
         {
             std::lock_guard<std::mutex> lk(ctx->mu);
@@ -947,16 +1087,15 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
             t->has_field = true;
             const zg_status st =
                 limbs == 3 ? cpr_prepare<3>(ctx, t, t->f, trace_mles, J, nvars, eval_point, shift_src, shift_amount, S,
-                                            n_constraints, coeffs, mles_on_device, folded, &packed)
+                                            n_constraints, coeffs, mles_on_device, folded, alpha_pows, &packed)
                            : cpr_prepare<4>(ctx, t, t->f, trace_mles, J, nvars, eval_point, shift_src, shift_amount, S,
-                                            n_constraints, coeffs, mles_on_device, folded, &packed);
+                                            n_constraints, coeffs, mles_on_device, folded, alpha_pows, &packed);
             if (st != ZG_OK) return st;
         }
         // comb = (sum_j A_j v_j) * eq_r * (1 - selector), degree max_degree + 2 = 3
         // (combined_poly_resolver.rs:147-172): the sum is the precombined MLE f,
         // times two affine factors; the round polynomials are those of the
         // reference's comb over every column
-        const uint32_t offsets[2] = {0, 1}, indices[1] = {2};
         const uint32_t fm[2] = {1, 0};
         std::vector<uint64_t> fa(2 * (size_t)limbs, 0), fbv(2 * (size_t)limbs, 0);
         std::memcpy(&fbv[0], t->f.one, 8 * limbs);      // eq_r: 0 + 1 * eq_r
@@ -971,14 +1110,33 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
                 br = (d >> 64) & 1;
             }
         }
+        // product terms (constraints of degree above one): alpha^k c_t times the
+        // product of their columns, which the sumcheck then carries as MLEs too
+        // (packed after [sel, eq, f]); the comb's degree is the longest product + 2
+        std::vector<uint64_t> pcoeffs((size_t)limbs, 0);
+        std::memcpy(pcoeffs.data(), t->f.one, 8 * limbs);
+        std::vector<uint32_t> poff{0, 1}, pidx{2};
+        for (const CprProduct &q : products) {
+            uint64_t c[4], cm[4];
+            if (limbs == 3) {
+                from_i128<3>((i128)q.coeff, t->f, c);
+                fmul<3>(c, &alpha_pows[(size_t)q.constraint * 3], t->f.p, t->f.n0, cm);
+            } else {
+                from_i128<4>((i128)q.coeff, t->f, c);
+                fmul<4>(c, &alpha_pows[(size_t)q.constraint * 4], t->f.p, t->f.n0, cm);
+            }
+            pcoeffs.insert(pcoeffs.end(), cm, cm + limbs);
+            for (uint32_t col : q.cols) pidx.push_back(3 + col);
+            poff.push_back((uint32_t)pidx.size());
+        }
         zg_sumcheck_group g{};
-        g.degree = 3;
-        g.n_mles = 3;
-        g.n_products = 1;
+        g.degree = max_factors + 2;
+        g.n_mles = products.empty() ? 3 : 3 + J + S;
+        g.n_products = (uint32_t)poff.size() - 1;
         g.mles = packed;
-        g.coeffs = t->f.one;
-        g.offsets = offsets;
-        g.indices = indices;
+        g.coeffs = pcoeffs.data();
+        g.offsets = poff.data();
+        g.indices = pidx.data();
         g.n_factors = 2;
         g.factor_mles = fm;
         g.factor_a = fa.data();
@@ -1002,6 +1160,18 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
     }
 }
 
+extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
+                                              uint32_t limbs, const uint64_t *trace_mles, uint32_t num_cols,
+                                              uint32_t nvars, const uint64_t *eval_point,
+                                              const uint32_t *shift_src, const uint32_t *shift_amount,
+                                              uint32_t n_shifts, uint32_t n_constraints, const uint64_t *coeffs,
+                                              int mles_on_device, uint8_t *proof, size_t *proof_len,
+                                              uint64_t *point_out, uint64_t *evals_out) {
+    return cpr_prove_impl(ctx, t, modulus, limbs, trace_mles, num_cols, nvars, eval_point, shift_src, shift_amount,
+                          n_shifts, n_constraints, coeffs, {}, mles_on_device, proof, proof_len, point_out,
+                          evals_out);
+}
+
 // Step 2 for a linear UAIR (IdealCheckProtocol::prove_linear, piop/src/ideal_check.rs:
 // 137-176, MLE first): the point r from the transcript, every up column and every
 // shifted (down) column evaluated coefficient-wise at r (the lifted-evaluation sums
@@ -1009,13 +1179,16 @@ extern "C" zg_status zg_piop_cpr_linear_prove(zg_ctx *ctx, zg_transcript *t, con
 // of every copy cleared as the reference's evaluate_combined_polynomials reads it), each
 // constraint's coefficients applied to those polynomial values, and the trimmed
 // combined values absorbed constraint after constraint.
-extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
-                                                uint32_t limbs, const uint64_t *bin_cols, uint32_t n_bin,
-                                                uint32_t degree_plus_one, const int64_t *int_cols, uint32_t n_int,
-                                                uint32_t nvars, const uint32_t *shift_src,
-                                                const uint32_t *shift_amount, uint32_t n_shifts,
-                                                uint32_t n_constraints, const uint64_t *coeffs, int cols_on_device,
-                                                uint64_t *point_out, uint64_t *combined_out, uint32_t *lengths_out) {
+namespace zg {
+// absorb == false: the point is drawn and the combined values are computed
+// (untrimmed, lengths_out left alone) but nothing is absorbed, for callers that
+// add more terms before the values go into the transcript.
+zg_status ideal_check_linear_impl(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                                  const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
+                                  const int64_t *int_cols, uint32_t n_int, uint32_t nvars, const uint32_t *shift_src,
+                                  const uint32_t *shift_amount, uint32_t n_shifts, uint32_t n_constraints,
+                                  const uint64_t *coeffs, int cols_on_device, uint64_t *point_out,
+                                  uint64_t *combined_out, uint32_t *lengths_out, bool absorb) {
     try {
         const uint32_t D = degree_plus_one, J = n_bin + n_int, S = n_shifts;
         const PiopCols c0{bin_cols, n_bin, D, int_cols, n_int, nvars};
@@ -1107,6 +1280,7 @@ extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, c
                     }
                 }
             }
+            if (!absorb) continue;
             // DynamicPolynomialF::new_trimmed, then absorb_random_field_slice
             uint32_t len = D;
             while (len > 0) {
@@ -1123,4 +1297,17 @@ extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, c
         set_error("ideal check: %s", e.what());
         return ZG_ERR_OOM;
     }
+}
+}  // namespace zg
+
+extern "C" zg_status zg_piop_ideal_check_linear(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus,
+                                                uint32_t limbs, const uint64_t *bin_cols, uint32_t n_bin,
+                                                uint32_t degree_plus_one, const int64_t *int_cols, uint32_t n_int,
+                                                uint32_t nvars, const uint32_t *shift_src,
+                                                const uint32_t *shift_amount, uint32_t n_shifts,
+                                                uint32_t n_constraints, const uint64_t *coeffs, int cols_on_device,
+                                                uint64_t *point_out, uint64_t *combined_out, uint32_t *lengths_out) {
+    return ideal_check_linear_impl(ctx, t, modulus, limbs, bin_cols, n_bin, degree_plus_one, int_cols, n_int, nvars,
+                                   shift_src, shift_amount, n_shifts, n_constraints, coeffs, cols_on_device,
+                                   point_out, combined_out, lengths_out, true);
 }

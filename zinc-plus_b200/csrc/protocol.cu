@@ -94,7 +94,94 @@ struct TranscriptGuard {
     }
 };
 
-zg_status check_uair(const zg_params *pb, const zg_params *pi, const zg_linear_uair *u, uint32_t nv) {
+// A UAIR as the driver takes it: the linear part of every constraint as a
+// coefficient matrix over [binary up, integer up, down] (single-column terms),
+// the terms that multiply two columns, and which constraints lie in the zero
+// ideal (the combined path skips those in the ideal check).
+struct UairRep {
+    uint32_t n_bin = 0, n_int = 0, degree_plus_one = 0, n_shifts = 0;
+    const uint32_t *shift_src = nullptr, *shift_amount = nullptr;
+    uint32_t n_constraints = 0;
+    const int64_t *coeffs = nullptr;  // n_constraints x (n_bin + n_int + n_shifts)
+    uint32_t n_pub_bin = 0, n_pub_int = 0;
+    std::vector<int64_t> coeff_store;
+    std::vector<CprProduct> products;
+    std::vector<uint8_t> zero_ideal;
+};
+
+UairRep rep_of(const zg_linear_uair *u) {
+    UairRep r;
+    r.n_bin = u->n_bin;
+    r.n_int = u->n_int;
+    r.degree_plus_one = u->degree_plus_one;
+    r.n_shifts = u->n_shifts;
+    r.shift_src = u->shift_src;
+    r.shift_amount = u->shift_amount;
+    r.n_constraints = u->n_constraints;
+    r.coeffs = u->coeffs;
+    r.n_pub_bin = u->n_pub_bin;
+    r.n_pub_int = u->n_pub_int;
+    r.zero_ideal.assign(u->n_constraints, 0);
+    return r;
+}
+
+// The term form (zg_uair) split into the linear matrix and the products.
+zg_status rep_of(const zg_uair *u, UairRep &r) {
+    if (!u->term_offsets || !u->term_coeffs || !u->factor_offsets || (u->n_constraints && !u->zero_ideal)) {
+        set_error("zinc prove: null term arrays");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    r.n_bin = u->n_bin;
+    r.n_int = u->n_int;
+    r.degree_plus_one = u->degree_plus_one;
+    r.n_shifts = u->n_shifts;
+    r.shift_src = u->shift_src;
+    r.shift_amount = u->shift_amount;
+    r.n_constraints = u->n_constraints;
+    r.n_pub_bin = u->n_pub_bin;
+    r.n_pub_int = u->n_pub_int;
+    const uint32_t W = u->n_bin + u->n_int + u->n_shifts;
+    r.coeff_store.assign((size_t)u->n_constraints * W, 0);
+    r.zero_ideal.assign(u->zero_ideal, u->zero_ideal + u->n_constraints);
+    if (u->term_offsets[0] != 0) {
+        set_error("zinc prove: term offsets must start at 0");
+        return ZG_ERR_INVALID_PARAM;
+    }
+    for (uint32_t k = 0; k < u->n_constraints; k++) {
+        if (u->term_offsets[k + 1] < u->term_offsets[k]) {
+            set_error("zinc prove: term offsets of constraint %u decrease", k);
+            return ZG_ERR_INVALID_PARAM;
+        }
+        for (uint32_t t = u->term_offsets[k]; t < u->term_offsets[k + 1]; t++) {
+            const uint32_t f0 = u->factor_offsets[t], f1 = u->factor_offsets[t + 1];
+            if (f1 < f0 || (f1 > f0 && !u->factor_cols)) {
+                set_error("zinc prove: factor offsets of term %u", t);
+                return ZG_ERR_INVALID_PARAM;
+            }
+            for (uint32_t q = f0; q < f1; q++)
+                if (u->factor_cols[q] >= W) {
+                    set_error("zinc prove: term %u names column %u of %u", t, u->factor_cols[q], W);
+                    return ZG_ERR_INVALID_PARAM;
+                }
+            if (f1 == f0) {
+                set_error("zinc prove: constant terms (constraint %u) are not supported", k);
+                return ZG_ERR_INVALID_PARAM;
+            }
+            if (f1 - f0 == 1) {
+                r.coeff_store[(size_t)k * W + u->factor_cols[f0]] += u->term_coeffs[t];
+            } else if (f1 - f0 == 2) {
+                r.products.push_back({k, u->term_coeffs[t], {u->factor_cols[f0], u->factor_cols[f0 + 1]}});
+            } else {
+                set_error("zinc prove: term %u multiplies %u columns (at most 2 supported)", t, f1 - f0);
+                return ZG_ERR_INVALID_PARAM;
+            }
+        }
+    }
+    r.coeffs = r.coeff_store.data();
+    return ZG_OK;
+}
+
+zg_status check_uair(const zg_params *pb, const zg_params *pi, const UairRep *u, uint32_t nv) {
     if (!u || (u->n_bin == 0 && u->n_int == 0) || u->n_constraints == 0 || !u->coeffs ||
         (u->n_shifts && (!u->shift_src || !u->shift_amount))) {
         set_error("zinc prove: empty UAIR or null constraint/shift arrays");
@@ -143,9 +230,15 @@ zg_status check_uair(const zg_params *pb, const zg_params *pi, const zg_linear_u
     return ZG_OK;
 }
 
-zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u, uint32_t nv, const uint64_t *bin,
-                          const int64_t *ints, int on_device, uint8_t *proof, size_t *proof_len) {
+zg_status prove_impl(zg_params *pb, zg_params *pi, const UairRep *u, uint32_t nv, const uint64_t *bin,
+                     const int64_t *ints, int on_device, bool mle_first, uint8_t *proof, size_t *proof_len) {
     ZG_TRY(check_uair(pb, pi, u, nv));
+    if (mle_first && !u->products.empty()) {
+        // prove_linear evaluates the columns first: constraints of degree above
+        // one are not supported there (combined_poly_builder.rs:201-206)
+        set_error("zinc prove: the MLE-first path takes linear constraints only");
+        return ZG_ERR_INVALID_PARAM;
+    }
     zg_params *any = pb ? pb : pi;
     zg_ctx *ctx = any->ctx;
     const int L = (int)any->d.field_limbs;
@@ -239,15 +332,58 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     for (size_t k = 0; k < (size_t)nc * (ncols + S); k++) f_from_i128(f, (i128)u->coeffs[k], &coeffs[k * L]);
     hphase(ctx, "zinc:prime");
 
-    // step 2 (prover.rs:358-380): ideal check, MLE first
+    // step 2 (prover.rs:330-380): ideal check.  The linear part of every
+    // constraint is the columns evaluated at the point first, each column's
+    // last row read as zero (prove_linear, ideal_check.rs:137-176).  On the
+    // combined path (prove_combined, ideal_check.rs:178-240) the row-by-row
+    // constraint polynomials give the same linear part (the MLE evaluation is
+    // linear); their product terms are summed row by row on the GPU, and the
+    // constraints in the zero ideal are sent empty.
     std::vector<uint64_t> ic_point((size_t)nv * L), combined((size_t)nc * D * L);
     std::vector<uint32_t> lens(nc);
-    ZG_TRY(zg_piop_ideal_check_linear(ctx, t, mod_b, (uint32_t)L, bin_d, nb, D, int_d, ni, nv, u->shift_src,
-                                      u->shift_amount, S, nc, coeffs.data(), 1, ic_point.data(),
-                                      combined.data(), lens.data()));
-    std::vector<std::vector<uint64_t>> ic_vals(nc);
+    ZG_TRY(ideal_check_linear_impl(ctx, t, mod_b, (uint32_t)L, bin_d, nb, D, int_d, ni, nv, u->shift_src,
+                                   u->shift_amount, S, nc, coeffs.data(), 1, ic_point.data(), combined.data(),
+                                   lens.data(), false));
+    uint32_t maxlen = D;
+    for (const CprProduct &q : u->products) {
+        const bool b0 = (q.cols[0] < ncols ? q.cols[0] : u->shift_src[q.cols[0] - ncols]) < nb;
+        const bool b1 = (q.cols[1] < ncols ? q.cols[1] : u->shift_src[q.cols[1] - ncols]) < nb;
+        maxlen = std::max(maxlen, (b0 ? D : 1) + (b1 ? D : 1) - 1);
+    }
+    std::vector<uint64_t> full((size_t)nc * maxlen * L, 0);
     for (uint32_t k = 0; k < nc; k++)
-        ic_vals[k].assign(&combined[(size_t)k * D * L], &combined[(size_t)k * D * L] + (size_t)lens[k] * L);
+        std::memcpy(&full[(size_t)k * maxlen * L], &combined[(size_t)k * D * L], (size_t)D * L * 8);
+    for (const CprProduct &q : u->products) {
+        IcFactor fac[2];
+        for (int e = 0; e < 2; e++) {
+            const uint32_t j = q.cols[e];
+            const uint32_t src = j < ncols ? j : u->shift_src[j - ncols];
+            fac[e].shift = j < ncols ? 0 : u->shift_amount[j - ncols];
+            fac[e].bin = src < nb ? bin_d + (size_t)src * n : nullptr;
+            fac[e].ints = src < nb ? nullptr : int_d + (size_t)(src - nb) * n;
+        }
+        std::vector<uint64_t> sums;
+        uint32_t plen = 0;
+        ZG_TRY(ic_product_sums(ctx, f, ic_point.data(), nv, fac[0], fac[1], D, sums, plen));
+        uint64_t c[4];
+        f_from_i128(f, (i128)q.coeff, c);
+        for (uint32_t m = 0; m < plen; m++) {
+            uint64_t tm[4];
+            if (L == 3) {
+                fmul<3>(c, &sums[(size_t)m * L], f.p, f.n0, tm);
+                fadd<3>(&full[((size_t)q.constraint * maxlen + m) * L], tm, f.p);
+            } else {
+                fmul<4>(c, &sums[(size_t)m * L], f.p, f.n0, tm);
+                fadd<4>(&full[((size_t)q.constraint * maxlen + m) * L], tm, f.p);
+            }
+        }
+    }
+    std::vector<std::vector<uint64_t>> ic_vals(nc);
+    for (uint32_t k = 0; k < nc; k++) {
+        if (!mle_first && u->zero_ideal[k]) continue;  // is_zero_ideal: DynamicPolynomialF::ZERO
+        ic_vals[k] = trimmed(&full[(size_t)k * maxlen * L], maxlen, L);
+        for (size_t e = 0; e < ic_vals[k].size() / L; e++) tr_absorb_field(t, &ic_vals[k][e * L]);
+    }
     hphase(ctx, "zinc:ideal_check");
 
     // step 3 (prover.rs:385-415): the projecting element a = Chal (i128) in F,
@@ -269,9 +405,9 @@ zg_status prove_mle_first(zg_params *pb, zg_params *pi, const zg_linear_uair *u,
     size_t md_len = 8 * (size_t)L + 12 + (size_t)nv * 8 * 8 * L + 8 * (size_t)L;
     std::vector<uint8_t> md_proof(md_len);
     std::vector<uint64_t> cpr_point((size_t)nv * L), cpr_evals((size_t)(ncols + S) * L);
-    ZG_TRY(zg_piop_cpr_linear_prove(ctx, t, mod_b, (uint32_t)L, mles, ncols, nv, ic_point.data(), u->shift_src,
-                                    u->shift_amount, S, nc, coeffs.data(), 1, md_proof.data(), &md_len,
-                                    cpr_point.data(), cpr_evals.data()));
+    ZG_TRY(cpr_prove_impl(ctx, t, mod_b, (uint32_t)L, mles, ncols, nv, ic_point.data(), u->shift_src,
+                          u->shift_amount, S, nc, coeffs.data(), u->products, 1, md_proof.data(), &md_len,
+                          cpr_point.data(), cpr_evals.data()));
     md_proof.resize(md_len);
     hphase(ctx, "zinc:cpr");
 
@@ -358,8 +494,28 @@ extern "C" zg_status zg_zinc_prove_mle_first(zg_params *pp_bin, zg_params *pp_in
             set_error("zinc prove: null argument or num_vars out of range");
             return ZG_ERR_INVALID_PARAM;
         }
-        return prove_mle_first(pp_bin, pp_int, uair, num_vars, bin_cols, int_cols, cols_on_device, proof,
-                               proof_len);
+        const UairRep rep = rep_of(uair);
+        return prove_impl(pp_bin, pp_int, &rep, num_vars, bin_cols, int_cols, cols_on_device, true, proof,
+                          proof_len);
+    } catch (const std::exception &e) {
+        set_error("zinc prove: %s", e.what());
+        return ZG_ERR_OOM;
+    }
+}
+
+extern "C" zg_status zg_zinc_prove(zg_params *pp_bin, zg_params *pp_int, const zg_uair *uair, uint32_t num_vars,
+                                   const uint64_t *bin_cols, const int64_t *int_cols, int cols_on_device,
+                                   int mle_first, uint8_t *proof, size_t *proof_len) {
+    try {
+        if (!uair || !proof_len || (*proof_len && !proof) || (uair->n_bin && !bin_cols) ||
+            (uair->n_int && !int_cols) || num_vars == 0 || num_vars > 30) {
+            set_error("zinc prove: null argument or num_vars out of range");
+            return ZG_ERR_INVALID_PARAM;
+        }
+        UairRep rep;
+        ZG_TRY(rep_of(uair, rep));
+        return prove_impl(pp_bin, pp_int, &rep, num_vars, bin_cols, int_cols, cols_on_device, mle_first != 0, proof,
+                          proof_len);
     } catch (const std::exception &e) {
         set_error("zinc prove: %s", e.what());
         return ZG_ERR_OOM;

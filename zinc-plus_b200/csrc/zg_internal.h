@@ -270,6 +270,44 @@ uint32_t tr_challenge_u32(zg_transcript *t);
 void tr_absorb_field(zg_transcript *t, const uint64_t *inner);
 // get_prime::<Uint<L>, MillerRabin> (transcript/src/lib.rs:58-72).
 // threads: 0 = the OpenMP default team.
+// One factor of a product of two trace columns (device memory): a binary
+// column (2^nv BinaryPoly words) or an integer column (2^nv i64), read at row
+// b + shift (zero past the last row: the zero padding of shifted columns).
+struct IcFactor {
+    const uint64_t *bin;
+    const int64_t *ints;
+    uint32_t shift;
+};
+// Combined-path ideal check of one product term: sum over the rows b < 2^nv - 1
+// of eq(b, point) times each coefficient of a(b) * b(b); coefficients_out gets
+// len_out = (a's length) + (b's length) - 1 Montgomery inners (binary: D, integer: 1).
+zg_status ic_product_sums(zg_ctx *ctx, const FieldCfg &f, const uint64_t *point, uint32_t nv, const IcFactor &a,
+                          const IcFactor &b, uint32_t D, std::vector<uint64_t> &coefficients_out, uint32_t &len_out);
+
+// zg_piop_ideal_check_linear with absorb == false: the point is drawn and the
+// values computed (untrimmed), nothing is absorbed.
+zg_status ideal_check_linear_impl(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                                  const uint64_t *bin_cols, uint32_t n_bin, uint32_t degree_plus_one,
+                                  const int64_t *int_cols, uint32_t n_int, uint32_t nvars, const uint32_t *shift_src,
+                                  const uint32_t *shift_amount, uint32_t n_shifts, uint32_t n_constraints,
+                                  const uint64_t *coeffs, int cols_on_device, uint64_t *point_out,
+                                  uint64_t *combined_out, uint32_t *lengths_out, bool absorb);
+// A product term of the CPR comb: coefficient (an integer) times the columns
+// cols (indices into [up..., down...]) of constraint k.
+struct CprProduct {
+    uint32_t constraint;
+    int64_t coeff;
+    std::vector<uint32_t> cols;
+};
+// zg_piop_cpr_linear_prove with product terms added to the comb
+// (sum_k alpha^k (linear_k + sum_t c_t prod cols_t)) (1 - sel) eq_r.
+zg_status cpr_prove_impl(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, uint32_t limbs,
+                         const uint64_t *trace_mles, uint32_t num_cols, uint32_t nvars, const uint64_t *eval_point,
+                         const uint32_t *shift_src, const uint32_t *shift_amount, uint32_t n_shifts,
+                         uint32_t n_constraints, const uint64_t *coeffs, const std::vector<CprProduct> &products,
+                         int mles_on_device, uint8_t *proof, size_t *proof_len, uint64_t *point_out,
+                         uint64_t *evals_out);
+
 void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads);
 // The same search with the candidate tests of each round run by run_all(n, test).
 void tr_get_prime_batched(zg_transcript *t, int L, uint64_t *prime_out, int group,

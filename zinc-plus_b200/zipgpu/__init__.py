@@ -50,7 +50,7 @@ EXPORTS = (
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
     "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear", "zg_prove_f", "zg_prove_f_d",
-    "zg_zinc_prove_mle_first",
+    "zg_zinc_prove_mle_first", "zg_zinc_prove",
 )
 
 
@@ -113,6 +113,16 @@ class LinearUairDesc(C.Structure):
                 ("n_pub_int", C.c_uint32)]
 
 
+class UairDesc(C.Structure):
+    """Mirror of ``zg_uair`` (constraints as terms)."""
+
+    _fields_ = [("n_bin", C.c_uint32), ("n_int", C.c_uint32), ("degree_plus_one", C.c_uint32),
+                ("n_shifts", C.c_uint32), ("shift_src", C.c_void_p), ("shift_amount", C.c_void_p),
+                ("n_constraints", C.c_uint32), ("term_offsets", C.c_void_p), ("term_coeffs", C.c_void_p),
+                ("factor_offsets", C.c_void_p), ("factor_cols", C.c_void_p), ("zero_ideal", C.c_void_p),
+                ("n_pub_bin", C.c_uint32), ("n_pub_int", C.c_uint32)]
+
+
 class SumcheckGroupDesc(C.Structure):
     """Mirror of ``zg_sumcheck_group``."""
 
@@ -153,6 +163,8 @@ def lib() -> C.CDLL:
                                       C.c_uint32, C.c_uint32, vp, C.c_int, vp, C.POINTER(sz), vp, vp], st),
         "zg_zinc_prove_mle_first": ([vp, vp, C.POINTER(LinearUairDesc), C.c_uint32, vp, vp, C.c_int, vp,
                                      C.POINTER(sz)], st),
+        "zg_zinc_prove": ([vp, vp, C.POINTER(UairDesc), C.c_uint32, vp, vp, C.c_int, C.c_int, vp, C.POINTER(sz)],
+                          st),
         "zg_piop_ideal_check_linear": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
                                         C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, C.c_uint32, vp, C.c_int, vp,
                                         vp, vp], st),
@@ -858,6 +870,50 @@ class ZincPlusPiop:
         n = C.c_size_t(buf.size)
         check(lib().zg_zinc_prove_mle_first(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, _ptr(buf),
                                             C.byref(n)))
+        return buf[: n.value].tobytes()
+
+    @staticmethod
+    def prove(pp_bin, pp_int, nvars: int, bin_cols, degree_plus_one: int, int_cols, shifts, constraints,
+              zero_ideal, mle_first: bool = False, n_pub_bin: int = 0, n_pub_int: int = 0) -> bytes:
+        """ZincPlusPiop::prove::<MLE_FIRST> with the UAIR as terms: constraints is
+        a list per constraint of (integer coefficient, [one or two column indices
+        into up (binary, then integer) and down (shift order)]); zero_ideal one
+        flag per constraint.  mle_first=False is the reference's default
+        (combined) path."""
+        b, i = ZincPiop._cols(bin_cols, int_cols, nvars)
+        src = np.array([s for s, _ in shifts] or [0], np.uint32)
+        amt = np.array([a for _, a in shifts] or [0], np.uint32)
+        toff, coef, foff, fcol = [0], [], [0], []
+        for terms in constraints:
+            for c, cols in terms:
+                coef.append(int(c))
+                fcol.extend(int(x) for x in cols)
+                foff.append(len(fcol))
+            toff.append(len(coef))
+        toff_a = np.array(toff, np.uint32)
+        coef_a = np.array(coef or [0], np.int64)
+        foff_a = np.array(foff, np.uint32)
+        fcol_a = np.array(fcol or [0], np.uint32)
+        zi = np.array([1 if z else 0 for z in zero_ideal] or [0], np.uint8)
+        if len(zero_ideal) != len(constraints):
+            raise ValueError("one zero_ideal flag per constraint")
+        u = UairDesc(b.shape[0], i.shape[0], degree_plus_one, len(shifts), src.ctypes.data, amt.ctypes.data,
+                     len(constraints), toff_a.ctypes.data, coef_a.ctypes.data, foff_a.ctypes.data,
+                     fcol_a.ctypes.data, zi.ctypes.data, n_pub_bin, n_pub_int)
+        pbin = pp_bin.handle if pp_bin is not None else None
+        pint = pp_int.handle if pp_int is not None else None
+        ncols = b.shape[0] + i.shape[0]
+        cap = 64 << 10
+        for pp in (pp_bin, pp_int):
+            if pp is not None:
+                cap += pp.proof_size(max(b.shape[0], i.shape[0], 1))
+        cap += (ncols * (degree_plus_one + 2) + len(constraints) * 2 * degree_plus_one + 64 * nvars) * 64
+        buf = ZincPlusPiop._out
+        if buf is None or buf.size < cap:
+            buf = ZincPlusPiop._out = np.empty(cap, np.uint8)
+        n = C.c_size_t(buf.size)
+        check(lib().zg_zinc_prove(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, 1 if mle_first else 0,
+                                  _ptr(buf), C.byref(n)))
         return buf[: n.value].tobytes()
 
 
