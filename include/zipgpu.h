@@ -155,6 +155,16 @@ zg_status zg_encode_rows_d(zg_params *p, const void *evals_d, void *cw_out_d, vo
  * row_len x limbs uint64, out codeword_len x limbs. */
 zg_status zg_encode_wide(zg_params *p, const uint64_t *row, uint32_t limbs, uint64_t *out);
 
+/* LinearCode::encode_f (code.rs:69-71; iprs.rs:88-106, raa.rs:155-160,
+ * raa_sign_flip.rs:101-106): row_len prime-field elements (Montgomery inners of
+ * `limbs` u64 of the odd prime `modulus`, limbs 1..4) encoded over the field
+ * into codeword_len elements, on the parameters' device.  zg_encode_f takes
+ * host buffers; zg_encode_f_d device buffers and a cudaStream_t (NULL = the
+ * context's stream, asynchronous). */
+zg_status zg_encode_f(zg_params *p, const uint8_t *modulus, uint32_t limbs, const uint64_t *row, uint64_t *out);
+zg_status zg_encode_f_d(zg_params *p, const uint8_t *modulus, uint32_t limbs, const uint64_t *row_d,
+                        uint64_t *out_d, void *stream);
+
 /* ---- MerkleTree::new(rows).root() (merkle.rs:74-103) ----------------------
  * rows: n_rows x (width*elem_bytes) bytes, row-major; width a power of two. */
 zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_t width,

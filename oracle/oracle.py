@@ -92,6 +92,16 @@ class Uair:
         return cls(n_bin, n_int, D, shifts, cons, roots, n_pub_bin, n_pub_int)
 
 
+def encode_f(desc: Desc, modulus: int, L: int, row) -> np.ndarray:
+    """LinearCode::encode_f (zip-plus/src/code.rs:69-71) of a row of Montgomery
+    inners (row_len, L) over the prime `modulus`: (codeword_len, L)."""
+    r = np.ascontiguousarray(row, dtype=np.uint64)
+    out = np.zeros((codeword_len(desc), L), np.uint64)
+    if lib().zr_encode_f(C.byref(desc), _ptr(_limbs(modulus, L)), L, _ptr(r), _ptr(out)):
+        raise ValueError("encode_f failed")
+    return out
+
+
 def zinc_prove(desc_bin: Desc, desc_int: Desc, nvars: int, bin_cols, int_cols, uair: Uair, L: int,
                mle_first: bool = True) -> bytes:
     """ZincPlusPiop::prove::<MLE_FIRST> (protocol/src/prover.rs:677-706) in C:
@@ -183,6 +193,7 @@ def lib():
         L.zr_tr_field_challenge.argtypes = [vp, vp, u32, vp]
         L.zr_tr_absorb_field.argtypes = [vp, vp, u32, vp]
         L.zr_commit_prove_f.argtypes = [C.POINTER(Desc), vp, u32, vp, vp, vp, sz, C.POINTER(C.c_size_t), vp, vp]
+        L.zr_encode_f.argtypes = [C.POINTER(Desc), vp, u32, vp, vp]
         up = C.POINTER(UairDesc)
         L.zr_zinc_prove.argtypes = [C.POINTER(Desc), C.POINTER(Desc), u32, vp, vp, up, u32, C.c_int, vp, sz,
                                     C.POINTER(sz)]

@@ -2420,5 +2420,73 @@ int zr_commit_prove_f(const zr_desc *d, const void *polys, uint32_t batch, const
     return rc;
 }
 
+/* LinearCode::encode_f (zip-plus/src/code.rs:69-71): a row of field elements
+ * (Montgomery inners of the prime `modulus`, L limbs) encoded over the field.
+ * IPRS (iprs.rs:88-106 encode_inner_f): the radix-8 pNTT with every base-matrix
+ * entry and twiddle taken as F::from_with_cfg of its i64 value.  RAA and
+ * sign-flipping RAA (raa.rs:93-127, raa_sign_flip.rs:31-69, encode_f calling
+ * encode_inner): repeat, (negate odd entries,) permute, prefix sums, (negate,)
+ * permute, prefix sums, all in the field. */
+int zr_encode_f(const zr_desc *d, const uint64_t *modulus, uint32_t L, const uint64_t *row, uint64_t *out) {
+    zparams z;
+    if (L < 1 || L > 4 || zparams_build(d, &z)) return -1;
+    fcfg f;
+    fcfg_init(&f, modulus, L);
+    if (d->code_kind == ZR_CODE_IPRS) {
+        const iprs_params *p = &z.iprs;
+        const uint32_t sh = 3 * p->depth;
+        for (size_t i = 0; i < p->codeword_len; i++) {
+            size_t chunk = i >> p->base_dim_log2, rw = i & (p->base_dim - 1);
+            size_t oct = zr_octet_reversal(chunk, p->depth);
+            const int64_t *bm = p->bm + rw * p->base_len;
+            uint64_t acc[4];
+            memcpy(acc, row + oct * L, 8 * L);
+            for (size_t c = 1; c < p->base_len; c++) {
+                uint64_t tw[4], t[4];
+                f_from_i64(&f, bm[c], tw);
+                fmul(&f, row + (oct | (c << sh)) * L, tw, t);
+                fadd(&f, acc, t);
+            }
+            memcpy(out + i * L, acc, 8 * L);
+        }
+        uint64_t xs[8][4];
+        for (uint32_t k = 0; k < p->depth; k++) {
+            size_t sub = (size_t)p->base_dim << (3 * k);
+            const int64_t *tw = p->tw[k];
+            for (size_t blk = 0; blk < p->codeword_len; blk += 8 * sub)
+                for (size_t i = 0; i < sub; i++) {
+                    for (int j = 0; j < 8; j++) memcpy(xs[j], out + (blk + j * sub + i) * L, 8 * L);
+                    for (int r = 0; r < 8; r++) {
+                        uint64_t y[4];
+                        memcpy(y, xs[0], 8 * L);
+                        for (int j = 1; j < 8; j++) {
+                            uint64_t fw[4], t[4];
+                            f_from_i64(&f, tw[(i * 7 + (j - 1)) * 8 + BUTTERFLY_TABLE[r][j - 1]], fw);
+                            fmul(&f, xs[j], fw, t);
+                            fadd(&f, y, t);
+                        }
+                        memcpy(out + (blk + r * sub + i) * L, y, 8 * L);
+                    }
+                }
+        }
+    } else {
+        const raa_params *r = &z.raa;
+        const size_t n = r->codeword_len;
+        uint64_t *a = (uint64_t *)malloc(8 * L * n);
+        for (size_t i = 0; i < n; i++) memcpy(a + i * L, row + (i % r->row_len) * L, 8 * L);
+        for (int pass = 0; pass < 2; pass++) {
+            if (r->flip)
+                for (size_t i = 1; i < n; i += 2) fneg(&f, a + i * L);
+            const uint32_t *perm = pass == 0 ? r->perm1 : r->perm2;
+            for (size_t i = 0; i < n; i++) memcpy(out + i * L, a + (size_t)perm[i] * L, 8 * L);
+            for (size_t i = 1; i < n; i++) fadd(&f, out + i * L, out + (i - 1) * L);
+            if (pass == 0) memcpy(a, out, 8 * L * n);
+        }
+        free(a);
+    }
+    zparams_free(&z);
+    return 0;
+}
+
 /* The Zinc+ PIOP prover chain and verifier (oracle). */
 #include "zinc_piop.c"

@@ -158,6 +158,10 @@ int zr_zinc_prove(const zr_desc *db, const zr_desc *di, uint32_t nvars, const ui
 int zr_zinc_verify(const zr_desc *db, const zr_desc *di, uint32_t nvars, const uint64_t *pub_bin,
                    const int64_t *pub_int, const zr_uair *u, uint32_t L, const uint8_t *proof, size_t len);
 
+/* LinearCode::encode_f: row (row_len Montgomery inners of L limbs) -> out
+ * (codeword_len inners), over the prime `modulus`; see zipref.c. */
+int zr_encode_f(const zr_desc *d, const uint64_t *modulus, uint32_t L, const uint64_t *row, uint64_t *out);
+
 /* threads used by the parallel regions */
 void zr_set_threads(int n);
 int zr_get_threads(void);

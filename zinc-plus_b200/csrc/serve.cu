@@ -82,7 +82,6 @@ class TestPool {
         cv_.notify_all();
         for (auto &t : th_) t.join();
     }
-    int threads() const { return (int)th_.size(); }
     // Runs fn(0..n-1) on the pool and the calling thread; returns when all ran.
     void run_all(int n, const std::function<void(int)> &fn) {
         auto job = std::make_shared<Job>();

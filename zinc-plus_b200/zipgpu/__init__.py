@@ -50,7 +50,7 @@ EXPORTS = (
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
     "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear", "zg_prove_f", "zg_prove_f_d",
-    "zg_zinc_prove_mle_first", "zg_zinc_prove",
+    "zg_zinc_prove_mle_first", "zg_zinc_prove", "zg_encode_f", "zg_encode_f_d",
 )
 
 
@@ -163,6 +163,8 @@ def lib() -> C.CDLL:
                                       C.c_uint32, C.c_uint32, vp, C.c_int, vp, C.POINTER(sz), vp, vp], st),
         "zg_zinc_prove_mle_first": ([vp, vp, C.POINTER(LinearUairDesc), C.c_uint32, vp, vp, C.c_int, vp,
                                      C.POINTER(sz)], st),
+        "zg_encode_f": ([vp, C.c_char_p, C.c_uint32, vp, vp], st),
+        "zg_encode_f_d": ([vp, C.c_char_p, C.c_uint32, vp, vp, vp], st),
         "zg_zinc_prove": ([vp, vp, C.POINTER(UairDesc), C.c_uint32, vp, vp, C.c_int, C.c_int, vp, C.POINTER(sz)],
                           st),
         "zg_piop_ideal_check_linear": ([vp, vp, C.c_char_p, C.c_uint32, vp, C.c_uint32, C.c_uint32, vp,
@@ -527,6 +529,17 @@ class ZipPlus:
         row = np.ascontiguousarray(row, dtype=np.uint64)
         out = np.zeros((pp.codeword_len, limbs), np.uint64)
         check(lib().zg_encode_wide(pp.handle, _ptr(row), limbs, _ptr(out)))
+        return out
+
+    @staticmethod
+    def encode_f(pp: ZipPlusParams, modulus: int, limbs: int, row: np.ndarray) -> np.ndarray:
+        """LinearCode::encode_f of (row_len, limbs) Montgomery inners over the
+        prime `modulus`: (codeword_len, limbs), on the GPU."""
+        row = np.ascontiguousarray(row, dtype=np.uint64)
+        if row.shape != (pp.info.row_len, limbs):
+            raise ValueError("row must be (row_len, limbs) Montgomery inners")
+        out = np.zeros((pp.codeword_len, limbs), np.uint64)
+        check(lib().zg_encode_f(pp.handle, modulus.to_bytes(8 * limbs, "little"), limbs, _ptr(row), _ptr(out)))
         return out
 
     @staticmethod
