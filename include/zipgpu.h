@@ -571,6 +571,33 @@ zg_status zg_zinc_prove(zg_params *pp_bin, zg_params *pp_int, const zg_uair *uai
                         const uint64_t *bin_cols, const int64_t *int_cols, int cols_on_device, int mle_first,
                         uint8_t *proof, size_t *proof_len);
 
+/* ---- Proof::read_transcription_bytes_exact (protocol/src/lib.rs:93-127) ------
+ * Parses the Proof transcription that zg_zinc_prove writes (field of `limbs`
+ * u64, num_vars rounds) into the places of its parts, checking every nested
+ * length: the three commitments, the PCS stream, the ideal check values
+ * (DynamicPolyVecF), the resolver's up and down evaluations (two Vec<F>), the
+ * MultiDegreeSumcheckProof, the multipoint SumcheckProof and the witness lifted
+ * evaluations.  Offsets are from the start of `proof`.  ZG_ERR_SERIALIZATION
+ * when the bytes are not a Proof. */
+typedef struct {
+    uint8_t roots[3][32];
+    uint64_t batch_sizes[3];
+    uint8_t modulus[32]; /* the prime, `limbs` u64 LE */
+    size_t zip_offset, zip_len;
+    size_t ideal_check_offset, ideal_check_len;
+    size_t resolver_offset, resolver_len;
+    size_t multi_degree_offset, multi_degree_len;
+    size_t multipoint_offset, multipoint_len;
+    size_t lifted_offset, lifted_len;
+    uint32_t n_ideal_values;      /* polynomials in the ideal check */
+    uint32_t n_up_evals, n_down_evals;
+    uint32_t multi_degree_groups; /* 1: the CPR group */
+    uint32_t cpr_degree;          /* the CPR group's degree (max constraint degree + 2) */
+    uint32_t n_lifted;            /* witness lifted evaluations */
+} zg_proof_layout;
+
+zg_status zg_proof_read(const uint8_t *proof, size_t len, uint32_t limbs, uint32_t num_vars, zg_proof_layout *out);
+
 #ifdef __cplusplus
 }
 #endif

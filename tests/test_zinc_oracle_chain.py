@@ -186,3 +186,35 @@ def test_combined_path_proves_products_and_the_verifier_accepts(oracle):
     bad[2, 5] += 1
     assert oracle.zinc_verify(db, di, nv, None, None, U, 3,
                               oracle.zinc_prove(db, di, nv, bins, bad, U, 3, mle_first=False)) == 4
+
+
+def test_proof_read_entry_point_parses_oracle_proofs(oracle, zipgpu):
+    """zg_proof_read (Proof::read_transcription_bytes_exact, lib.rs:93-127) on
+    proofs of both paths: the parts' places agree with the layout written, and
+    truncated or altered lengths are rejected."""
+    nv = 7
+    bins, ints, shifts, coeffs, U = biglinear(oracle, nv, 30, n_pub_bin=2)
+    db, di = descs(oracle, nv, 32)
+    proof = oracle.zinc_prove(db, di, nv, bins, ints, U, 3)
+    lay = zipgpu.read_proof(proof, 3, nv)
+    P = parse_proof(proof, 3, nv)
+    assert lay["batch_sizes"] == [14, 0, 1] and lay["roots"][1] == bytes(32)
+    assert lay["n_ideal_values"] == 17 and (lay["n_up_evals"], lay["n_down_evals"]) == (17, 16)
+    assert lay["cpr_degree"] == 3 and lay["multi_degree_groups"] == 1 and lay["n_lifted"] == 15
+    assert proof[lay["zip_offset"]:lay["zip_offset"] + lay["zip_len"]] == P["zip"]
+    assert lay["modulus"] == P["modulus"]
+    assert lay["lifted_offset"] + lay["lifted_len"] == len(proof)
+    with pytest.raises(zipgpu.ZipError) as e:
+        zipgpu.read_proof(proof[:-1], 3, nv)
+    assert e.value.status == 3
+    bad = bytearray(proof)
+    bad[lay["multi_degree_offset"] + 24] ^= 1  # the group count
+    with pytest.raises(zipgpu.ZipError):
+        zipgpu.read_proof(bytes(bad), 3, nv)
+    with pytest.raises(zipgpu.ZipError):
+        zipgpu.read_proof(proof, 3, nv + 1)  # wrong number of rounds
+    # the combined path of a degree-2 UAIR
+    bins2, ints2, U2 = product_uair(oracle, nv, 4)
+    db2, di2 = descs(oracle, nv, 16)
+    lay2 = zipgpu.read_proof(oracle.zinc_prove(db2, di2, nv, bins2, ints2, U2, 3, mle_first=False), 3, nv)
+    assert lay2["cpr_degree"] == 4 and lay2["n_ideal_values"] == 3

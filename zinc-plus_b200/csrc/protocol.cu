@@ -319,8 +319,7 @@ zg_status prove_impl(zg_params *pb, zg_params *pi, const UairRep *u, uint32_t nv
         for (size_t k = 0; k < n * pbn; k++) tr_absorb_slice(t, &hb_pub[k], 8);
         for (size_t k = 0; k < n * pin; k++) tr_absorb_slice(t, &hi_pub[k], 8);
     }
-    // both tables' PCS proofs land in t->stream: size it once
-    t->stream.reserve((wb ? zg_proof_size(pb, wb) : 0) + (wi ? zg_proof_size(pi, wi) : 0));
+    // only the PCS proofs' heads (the b rows) land in t->stream
     hphase(ctx, "zinc:commit");
 
     // step 1 (prover.rs:285-300): the random prime; projection happens inside
@@ -434,14 +433,10 @@ zg_status prove_impl(zg_params *pb, zg_params *pi, const UairRep *u, uint32_t nv
     }
     hphase(ctx, "zinc:lifted");
 
-    // step 7 (prover.rs:552-597): PCS openings at r_0, binary table first
-    uint8_t ev[32];
-    if (wb) ZG_TRY(zg_prove_f_d(pb, t, wbin_d, wb, r0.data(), hb.h, ev));
-    if (wi) ZG_TRY(zg_prove_f_d(pi, t, wint_d, wi, r0.data(), hi.h, ev));
-    hphase(ctx, "zinc:prove_f");
-
-    // finish (prover.rs:603-650) and the transcription (lib.rs:129-160),
-    // written straight into the caller's buffer once its size is known
+    // finish (prover.rs:603-650) and the transcription (lib.rs:129-160).  Every
+    // part but the PCS stream is known now, so the proof is laid out in the
+    // caller's buffer first and step 7 writes each table's openings (the bulk of
+    // the proof) straight into their place: the PCS stream is never copied
     const uint64_t *p = f.p;
     // witness lifted evaluations: public columns come first in each table
     std::vector<std::vector<uint64_t>> witness_lifted(lifted_polys.begin() + pbn, lifted_polys.begin() + nb);
@@ -450,8 +445,12 @@ zg_status prove_impl(zg_params *pb, zg_params *pi, const UairRep *u, uint32_t nv
     Bytes cpr;
     cpr.sub(field_vec(cpr_evals.data(), ncols, p, L));
     cpr.sub(field_vec(cpr_evals.data() + (size_t)ncols * L, S, p, L));
-    const size_t total = 3 * 40 + 4 + t->stream.size() + 4 + ic_b.b.size() + 4 + cpr.b.size() + 4 + md_proof.size() +
-                         4 + mp_proof.size() + 4 + lifted_b.b.size();
+    const size_t size_b = wb ? zg_proof_size(pb, wb) : 0, size_i = wi ? zg_proof_size(pi, wi) : 0;
+    const size_t head_b = wb ? (size_t)pb->info.num_rows * 2 * pb->info.field_bytes : 0;
+    const size_t head_i = wi ? (size_t)pi->info.num_rows * 2 * pi->info.field_bytes : 0;
+    const size_t zip_len = size_b + size_i;
+    const size_t total = 3 * 40 + 4 + zip_len + 4 + ic_b.b.size() + 4 + cpr.b.size() + 4 + md_proof.size() + 4 +
+                         mp_proof.size() + 4 + lifted_b.b.size();
     const size_t cap = *proof_len;
     *proof_len = total;
     if (cap < total) {
@@ -473,12 +472,35 @@ zg_status prove_impl(zg_params *pb, zg_params *pi, const UairRep *u, uint32_t nv
         put(roots[k], 32);
         put(&batches[k], 8);
     }
-    put_sub(t->stream.data(), t->stream.size());
+    put_u32((uint32_t)zip_len);
+    uint8_t *zip = w;
+    w += zip_len;
     put_sub(ic_b.b.data(), ic_b.b.size());
     put_sub(cpr.b.data(), cpr.b.size());
     put_sub(md_proof.data(), md_proof.size());
     put_sub(mp_proof.data(), mp_proof.size());
     put_sub(lifted_b.b.data(), lifted_b.b.size());
+
+    // step 7 (prover.rs:552-597): PCS openings at r_0, binary table first.  Each
+    // table's b rows (the head of its PCS proof) go to the transcript stream; the
+    // combined row and the openings (its tail) go to their place in `proof`
+    uint8_t ev[32];
+    auto prove_f_into = [&](zg_params *pp, const void *polys_d, uint32_t batch, const zg_hint *h,
+                            uint8_t *tail) -> zg_status {
+        std::lock_guard<std::mutex> lk(pp->ctx->mu);
+        ZG_CUDA(cudaSetDevice(pp->ctx->device));
+        return prove_device(pp, pp->ctx, t, polys_d, batch, reinterpret_cast<const uint8_t *>(r0.data()), h, ev,
+                            tail, true);
+    };
+    if (wb) ZG_TRY(prove_f_into(pb, wbin_d, wb, hb.h, zip + head_b));
+    if (wi) ZG_TRY(prove_f_into(pi, wint_d, wi, hi.h, zip + size_b + head_i));
+    if (t->stream.size() != head_b + head_i) {
+        set_error("internal: PCS proof heads of %zu bytes, %zu expected", t->stream.size(), head_b + head_i);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    if (head_b) std::memcpy(zip, t->stream.data(), head_b);
+    if (head_i) std::memcpy(zip + size_b, t->stream.data() + head_b, head_i);
+    hphase(ctx, "zinc:prove_f");
     hphase(ctx, "zinc:finish");
     return ZG_OK;
 }
@@ -520,4 +542,143 @@ extern "C" zg_status zg_zinc_prove(zg_params *pp_bin, zg_params *pp_int, const z
         set_error("zinc prove: %s", e.what());
         return ZG_ERR_OOM;
     }
+}
+
+namespace {
+
+// Little-endian reader over a byte range; every read is bounds checked.
+struct Reader {
+    const uint8_t *p = nullptr;
+    size_t len = 0, pos = 0;
+    bool take(size_t n, const uint8_t **out) {
+        if (n > len - pos) return false;
+        if (out) *out = p + pos;
+        pos += n;
+        return true;
+    }
+    bool u32(uint32_t *v) {
+        const uint8_t *b;
+        if (!take(4, &b)) return false;
+        std::memcpy(v, b, 4);
+        return true;
+    }
+    bool u64(uint64_t *v) {
+        const uint8_t *b;
+        if (!take(8, &b)) return false;
+        std::memcpy(v, b, 8);
+        return true;
+    }
+    // a u32 length prefix, then that many bytes as a sub-reader
+    bool sub(Reader *r, size_t *off) {
+        uint32_t n;
+        if (!u32(&n)) return false;
+        *off = pos;
+        const uint8_t *b;
+        if (!take(n, &b)) return false;
+        *r = Reader{b, n, 0};
+        return true;
+    }
+    bool done() const { return pos == len; }
+};
+
+zg_status malformed(const char *what) {
+    set_error("Proof: malformed %s", what);
+    return ZG_ERR_SERIALIZATION;
+}
+
+// DynamicPolyVecF (over_field.rs:409-476): empty, or a flag byte, the modulus
+// when the flag is set, then u32 length + inners per polynomial.
+bool read_poly_vec(Reader r, size_t fb, const uint8_t *modulus, uint32_t *count) {
+    *count = 0;
+    if (r.done()) return true;
+    const uint8_t *flag, *m;
+    if (!r.take(1, &flag) || *flag > 1) return false;
+    if (*flag && (!r.take(fb, &m) || std::memcmp(m, modulus, fb) != 0)) return false;
+    while (!r.done()) {
+        uint32_t n;
+        if (!r.u32(&n) || (!*flag && n) || !r.take((size_t)n * fb, nullptr)) return false;
+        (*count)++;
+    }
+    return true;
+}
+
+// Vec<F> (traits.rs:566-607): empty, or the modulus and whole field elements.
+bool read_field_vec(Reader r, size_t fb, const uint8_t *modulus, uint32_t *count) {
+    *count = 0;
+    if (r.done()) return true;
+    const uint8_t *m;
+    if (!r.take(fb, &m) || std::memcmp(m, modulus, fb) != 0 || (r.len - r.pos) % fb != 0) return false;
+    *count = (uint32_t)((r.len - r.pos) / fb);
+    return true;
+}
+
+}  // namespace
+
+// Proof::read_transcription_bytes_exact (protocol/src/lib.rs:93-127): the
+// parts' places in the bytes, with every nested length checked.
+extern "C" zg_status zg_proof_read(const uint8_t *proof, size_t len, uint32_t limbs, uint32_t num_vars,
+                                   zg_proof_layout *out) {
+    if (!proof || !out || limbs < 1 || limbs > MAX_FIELD_LIMBS || num_vars == 0 || num_vars > 64) {
+        set_error("Proof: null argument, field of %u limbs or num_vars %u", limbs, num_vars);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    std::memset(out, 0, sizeof *out);
+    const size_t fb = 8 * (size_t)limbs;
+    Reader r{proof, len, 0};
+    for (int k = 0; k < 3; k++) {
+        const uint8_t *root;
+        if (!r.take(32, &root) || !r.u64(&out->batch_sizes[k])) return malformed("commitments");
+        std::memcpy(out->roots[k], root, 32);
+    }
+    uint32_t zl;
+    if (!r.u32(&zl)) return malformed("PCS stream length");
+    out->zip_offset = r.pos;
+    out->zip_len = zl;
+    if (!r.take(zl, nullptr)) return malformed("PCS stream");
+    Reader ic, res, md, mp, lifted;
+    if (!r.sub(&ic, &out->ideal_check_offset) || !r.sub(&res, &out->resolver_offset) ||
+        !r.sub(&md, &out->multi_degree_offset) || !r.sub(&mp, &out->multipoint_offset) ||
+        !r.sub(&lifted, &out->lifted_offset) || !r.done())
+        return malformed("part lengths");
+    out->ideal_check_len = ic.len;
+    out->resolver_len = res.len;
+    out->multi_degree_len = md.len;
+    out->multipoint_len = mp.len;
+    out->lifted_len = lifted.len;
+    // MultiDegreeSumcheckProof (multi_degree.rs:86-190): modulus, group count,
+    // num_vars, one degree per group, the messages, one claimed sum per group
+    const uint8_t *modulus;
+    uint32_t ng, nv;
+    if (!md.take(fb, &modulus) || !md.u32(&ng) || !md.u32(&nv) || ng == 0 || ng > 64 || nv != num_vars)
+        return malformed("multi-degree sumcheck header");
+    size_t msgs = 0;
+    for (uint32_t g = 0; g < ng; g++) {
+        uint32_t d;
+        if (!md.u32(&d) || d > 64) return malformed("multi-degree sumcheck degree");
+        if (g == 0) out->cpr_degree = d;
+        msgs += (size_t)d * nv;
+    }
+    if (!md.take((msgs + ng) * fb, nullptr) || !md.done()) return malformed("multi-degree sumcheck body");
+    out->multi_degree_groups = ng;
+    std::memcpy(out->modulus, modulus, fb);
+    // SumcheckProof (sumcheck.rs:35-111): modulus, round count, per round a
+    // u32 length and that many elements, the claimed sum
+    const uint8_t *m2;
+    uint32_t rounds;
+    if (!mp.take(fb, &m2) || std::memcmp(m2, modulus, fb) != 0 || !mp.u32(&rounds) || rounds != num_vars)
+        return malformed("multipoint sumcheck header");
+    for (uint32_t k = 0; k < rounds; k++) {
+        uint32_t n;
+        if (!mp.u32(&n) || n > 64 || !mp.take((size_t)n * fb, nullptr)) return malformed("multipoint round");
+    }
+    if (!mp.take(fb, nullptr) || !mp.done()) return malformed("multipoint claimed sum");
+    // the resolver: up evaluations then down evaluations, each a sub-buffer
+    Reader up, down;
+    size_t o1, o2;
+    if (!res.sub(&up, &o1) || !res.sub(&down, &o2) || !res.done()) return malformed("resolver");
+    if (!read_field_vec(up, fb, modulus, &out->n_up_evals) || !read_field_vec(down, fb, modulus, &out->n_down_evals))
+        return malformed("resolver evaluations");
+    if (!read_poly_vec(ic, fb, modulus, &out->n_ideal_values)) return malformed("ideal check values");
+    if (!read_poly_vec(lifted, fb, modulus, &out->n_lifted)) return malformed("lifted evaluations");
+    return ZG_OK;
 }

@@ -50,7 +50,7 @@ EXPORTS = (
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
     "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear", "zg_prove_f", "zg_prove_f_d",
-    "zg_zinc_prove_mle_first", "zg_zinc_prove", "zg_encode_f", "zg_encode_f_d",
+    "zg_zinc_prove_mle_first", "zg_zinc_prove", "zg_encode_f", "zg_encode_f_d", "zg_proof_read",
 )
 
 
@@ -123,6 +123,18 @@ class UairDesc(C.Structure):
                 ("n_pub_bin", C.c_uint32), ("n_pub_int", C.c_uint32)]
 
 
+class ProofLayout(C.Structure):
+    """Mirror of ``zg_proof_layout``."""
+
+    _fields_ = [("roots", (C.c_uint8 * 32) * 3), ("batch_sizes", C.c_uint64 * 3), ("modulus", C.c_uint8 * 32)] + \
+               [(n, C.c_size_t) for n in ("zip_offset", "zip_len", "ideal_check_offset", "ideal_check_len",
+                                          "resolver_offset", "resolver_len", "multi_degree_offset",
+                                          "multi_degree_len", "multipoint_offset", "multipoint_len",
+                                          "lifted_offset", "lifted_len")] + \
+               [(n, C.c_uint32) for n in ("n_ideal_values", "n_up_evals", "n_down_evals", "multi_degree_groups",
+                                          "cpr_degree", "n_lifted")]
+
+
 class SumcheckGroupDesc(C.Structure):
     """Mirror of ``zg_sumcheck_group``."""
 
@@ -163,6 +175,7 @@ def lib() -> C.CDLL:
                                       C.c_uint32, C.c_uint32, vp, C.c_int, vp, C.POINTER(sz), vp, vp], st),
         "zg_zinc_prove_mle_first": ([vp, vp, C.POINTER(LinearUairDesc), C.c_uint32, vp, vp, C.c_int, vp,
                                      C.POINTER(sz)], st),
+        "zg_proof_read": ([C.c_char_p, sz, C.c_uint32, C.c_uint32, C.POINTER(ProofLayout)], st),
         "zg_encode_f": ([vp, C.c_char_p, C.c_uint32, vp, vp], st),
         "zg_encode_f_d": ([vp, C.c_char_p, C.c_uint32, vp, vp, vp], st),
         "zg_zinc_prove": ([vp, vp, C.POINTER(UairDesc), C.c_uint32, vp, vp, C.c_int, C.c_int, vp, C.POINTER(sz)],
@@ -928,6 +941,18 @@ class ZincPlusPiop:
         check(lib().zg_zinc_prove(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, 1 if mle_first else 0,
                                   _ptr(buf), C.byref(n)))
         return buf[: n.value].tobytes()
+
+
+def read_proof(proof: bytes, limbs: int, num_vars: int) -> dict:
+    """Proof::read_transcription_bytes_exact (protocol/src/lib.rs:93-127): the
+    places and counts of a Zinc+ proof's parts (raises ZipError if malformed)."""
+    lay = ProofLayout()
+    check(lib().zg_proof_read(proof, len(proof), limbs, num_vars, C.byref(lay)))
+    out = {f: getattr(lay, f) for f, _ in ProofLayout._fields_ if f not in ("roots", "batch_sizes", "modulus")}
+    out["roots"] = [bytes(r) for r in lay.roots]
+    out["batch_sizes"] = list(lay.batch_sizes)
+    out["modulus"] = int.from_bytes(bytes(lay.modulus)[: 8 * limbs], "little")
+    return out
 
 
 class ZincPiop:
