@@ -133,6 +133,13 @@ zg_status zg_ctx_kernel_timing_report(zg_ctx *ctx, char *buf, size_t cap, size_t
  * stays usable.  Run it while no other work is in flight on the device: it
  * clears the device's word. */
 zg_status zg_selftest_bounded_wait(zg_ctx *ctx, uint32_t *status_seen);
+/* Host-side fault injection for tests of the error paths (no counterpart in the
+ * reference): the n-th device allocation made from now on by any context of
+ * the process (n >= 1; n = 0 disarms) fails as if the device were out of
+ * memory, without calling CUDA or touching the GPU.  The call that made it
+ * returns ZG_ERR_OOM ("injected allocation failure"); a server request whose
+ * lane allocation fails completes with that status. */
+zg_status zg_debug_fail_allocation(uint32_t n);
 
 /* ---- setup: ZipPlus::setup + IprsCode::new / RaaCode::new -----------------
  * ctx may be NULL for host-only parameters (tables, encode_wide, verify);

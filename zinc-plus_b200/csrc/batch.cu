@@ -471,11 +471,9 @@ zg_status commit_batch_impl(zg_ctx *ctx, uint32_t n, zg_params *const *params,
         if (kv.first == key) pl = kv.second;
     bool fresh = false;
     if (!pl) {
-        if (ctx->plans.size() >= 8) ctx->plans.erase(ctx->plans.begin());
         pl = std::make_shared<BatchPlan>();
         pl->key = key;
         ZG_TRY(build_plan(ctx, n, params, on_device, pinned, nlanes, *pl));
-        ctx->plans.push_back({key, pl});
         fresh = true;
     }
     if (!on_device && !pinned) stage_host_inputs(*pl, polys);
@@ -487,7 +485,11 @@ zg_status commit_batch_impl(zg_ctx *ctx, uint32_t n, zg_params *const *params,
         pl->graph = nullptr;
         pl->dev_inputs = dev;
     }
-    if (fresh) {
+    // A new plan is cached only once its tuning and its sizing run succeeded:
+    // a plan cached after a failure would later be captured without the run that
+    // sizes its lanes' scratch.  On a failure the lanes' queued work is drained
+    // before the plan (its arena and lanes) is dropped.
+    auto setup = [&]() -> zg_status {
         // tuning: forced choice, or time the candidates of each group shape
         for (Group &g : pl->groups) {
             if (forced) {
@@ -523,6 +525,17 @@ zg_status commit_batch_impl(zg_ctx *ctx, uint32_t n, zg_params *const *params,
         ZG_TRY(issue_plan(ctx, *pl, polys));
         ZG_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->launch_adjust += (int64_t)pl->launches();
+        return ZG_OK;
+    };
+    if (fresh) {
+        const zg_status st = setup();
+        if (st != ZG_OK) {
+            for (zg_ctx *l : pl->lanes) cudaStreamSynchronize(l->stream);
+            cudaStreamSynchronize(ctx->stream);
+            return st;
+        }
+        if (ctx->plans.size() >= 8) ctx->plans.erase(ctx->plans.begin());
+        ctx->plans.push_back({key, pl});
     }
     if (o.use_graph && !pl->exec) {
         const uint64_t before = pl->launches();

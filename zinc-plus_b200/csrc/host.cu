@@ -27,8 +27,30 @@ void set_error(const char *fmt, ...) {
 const char *last_error() { return g_err.c_str(); }
 
 // ----------------------------------------------------------------- buffers
+// Host-side fault injection (zg_debug_fail_allocation): a countdown of device
+// allocations; the one that brings it to zero fails as out of memory before
+// any CUDA call is made.
+static std::atomic<int64_t> g_fail_countdown{0};
+
+bool injected_allocation_failure() {
+    int64_t v = g_fail_countdown.load(std::memory_order_relaxed);
+    while (v > 0) {
+        if (g_fail_countdown.compare_exchange_weak(v, v - 1)) {
+            if (v == 1) {
+                set_error("injected allocation failure (zg_debug_fail_allocation)");
+                return true;
+            }
+            return false;
+        }
+    }
+    return false;
+}
+
+void debug_fail_allocation(uint32_t n) { g_fail_countdown.store((int64_t)n); }
+
 zg_status DevBuf::ensure(size_t bytes) {
     if (bytes <= cap) return ZG_OK;
+    if (injected_allocation_failure()) return ZG_ERR_OOM;
     release();
     size_t want = std::max(bytes, (size_t)256);
     cudaError_t e = pool ? cudaMallocFromPoolAsync(&ptr, want, pool, pool_stream) : cudaMalloc(&ptr, want);
@@ -153,6 +175,7 @@ static size_t cache_round(size_t bytes) {
 }
 
 void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got) {
+    if (injected_allocation_failure()) return nullptr;
     if (ctx->pool) {
         void *p = nullptr;
         if (cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream) != cudaSuccess) {

@@ -31,3 +31,8 @@ zg_status launch_wait_probe(zg_ctx *ctx, cudaStream_t s) {
 }
 
 }  // namespace zg
+
+extern "C" zg_status zg_debug_fail_allocation(uint32_t n) {
+    zg::debug_fail_allocation(n);
+    return ZG_OK;
+}

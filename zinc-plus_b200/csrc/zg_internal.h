@@ -100,6 +100,10 @@ void ktimer_collect(zg_ctx *ctx);
 // Host phase wall time since the previous mark, reported as "host:<name>".
 void hphase_start(zg_ctx *ctx);
 void hphase(zg_ctx *ctx, const char *name);
+// Host-side fault injection: true when this device allocation is the one
+// zg_debug_fail_allocation armed (the error message is set).
+bool injected_allocation_failure();
+void debug_fail_allocation(uint32_t n);
 // Device block cache of a context.
 void *ctx_alloc(zg_ctx *ctx, size_t bytes, size_t *got);
 void ctx_release(zg_ctx *ctx, void *p, size_t bytes);
