@@ -43,15 +43,30 @@ __global__ void __launch_bounds__(256) k_eq_table_split(const uint64_t *__restri
     for (uint32_t e = threadIdx.x; e < na + nb; e += blockDim.x) {
         const bool hi = e >= na;
         const uint32_t idx = hi ? e - na : e, k0 = hi ? a : 0, kn = hi ? b : a;
-        uint64_t acc[L];
-        for (int w = 0; w < L; w++) acc[w] = f.one[w];
+        // the product of the kn factors as a balanced tree: depth ceil(log2 kn)
+        // instead of a chain of kn dependent Montgomery products
+        uint64_t v[10][L];
         for (uint32_t k = 0; k < kn; k++) {
             const uint64_t *sel = ((idx >> k) & 1u) ? r + (size_t)(k0 + k) * L : omr + (size_t)(k0 + k) * L;
-            uint64_t t[L];
-            fmul<L>(acc, sel, f.p, f.n0, t);
-            for (int w = 0; w < L; w++) acc[w] = t[w];
+            for (int w = 0; w < L; w++) v[k][w] = sel[w];
         }
-        for (int w = 0; w < L; w++) tab[(size_t)e * L + w] = acc[w];
+        uint32_t width = kn;
+        if (width == 0) {
+            for (int w = 0; w < L; w++) v[0][w] = f.one[w];
+            width = 1;
+        }
+        while (width > 1) {
+            const uint32_t half = width / 2;
+            for (uint32_t i = 0; i < half; i++) {
+                uint64_t t[L];
+                fmul<L>(v[2 * i], v[2 * i + 1], f.p, f.n0, t);
+                for (int w = 0; w < L; w++) v[i][w] = t[w];
+            }
+            if (width & 1)
+                for (int w = 0; w < L; w++) v[half][w] = v[width - 1][w];
+            width = half + (width & 1);
+        }
+        for (int w = 0; w < L; w++) tab[(size_t)e * L + w] = v[0][w];
     }
     __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

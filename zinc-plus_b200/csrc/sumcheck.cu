@@ -373,6 +373,109 @@ zg_status launch_fold(zg_ctx *ctx, const uint64_t *in, uint64_t *out, uint32_t K
     return ZG_OK;
 }
 
+// Fiat-Shamir on the device: after each round's kernels, one block sums the
+// block partials of every group into the round's evaluations and its first
+// thread runs the transcript step on a device copy of the Blake3 hasher (the
+// reference's order, piop/src/sumcheck.rs:180-199 and multi_degree.rs:300-340:
+// absorb the round messages, squeeze the challenge, absorb it).  The challenge
+// stays in device memory for the next round's fold, so the rounds run back to
+// back with no host round trip; the hasher state, messages and point come back
+// once at the end.
+constexpr uint32_t kScMaxGroups = 8;
+struct FsArgs {
+    b3::Hasher *h;
+    const uint64_t *partials[kScMaxGroups];
+    uint32_t degree[kScMaxGroups];
+    uint32_t ng, multi, blocks, rd, maxd, nvars;
+    uint64_t *msgs;     // [g][round][maxd + 1][L]: evaluations 1..deg of each round
+    uint64_t *claimed;  // [g][L]: P_0(0) + P_0(1)
+    uint64_t *r;        // this round's challenge, read by the next fold
+    uint64_t *point;    // [round][L]
+};
+
+// absorb_random_field (transcript/src/traits.rs:393-413): 0x03 | modulus | 0x05 | 0x01 | inner | 0x03
+template <int L>
+__device__ void dev_absorb_field(b3::Hasher *h, const FieldCfg &f, const uint64_t *inner) {
+    uint8_t buf[16 * L + 4];
+    int k = 0;
+    buf[k++] = 3;
+    for (int w = 0; w < L; w++)
+        for (int b = 0; b < 8; b++) buf[k++] = (uint8_t)(f.p[w] >> (8 * b));
+    buf[k++] = 5;
+    buf[k++] = 1;
+    for (int w = 0; w < L; w++)
+        for (int b = 0; b < 8; b++) buf[k++] = (uint8_t)(inner[w] >> (8 * b));
+    buf[k++] = 3;
+    h->update(buf, (size_t)k);
+}
+
+template <int L>
+__global__ void __launch_bounds__(256) k_sc_fs(FsArgs a, FieldCfg f) {
+    __shared__ uint64_t red[256][L];
+    __shared__ uint64_t ev[kScMaxGroups][kScMaxDeg + 1][L];
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t g = 0; g < a.ng; g++) {
+        const uint32_t D = a.degree[g];
+        for (uint32_t t = 0; t <= D; t++) {
+            uint64_t acc[L] = {};
+            for (uint32_t bk = tid; bk < a.blocks; bk += blockDim.x)
+                fadd<L>(acc, a.partials[g] + ((size_t)bk * (D + 1) + t) * L, f.p);
+#pragma unroll
+            for (int w = 0; w < L; w++) red[tid][w] = acc[w];
+            __syncthreads();
+            for (uint32_t h = blockDim.x / 2; h > 0; h >>= 1) {
+                if (tid < h) fadd<L>(red[tid], red[tid + h], f.p);
+                __syncthreads();
+            }
+            if (tid == 0)
+#pragma unroll
+                for (int w = 0; w < L; w++) ev[g][t][w] = red[0][w];
+            __syncthreads();
+        }
+    }
+    if (tid != 0) return;
+    for (uint32_t g = 0; g < a.ng; g++) {
+        const uint32_t D = a.degree[g];
+        if (a.rd == 0) {
+            uint64_t c[L];
+#pragma unroll
+            for (int w = 0; w < L; w++) c[w] = ev[g][0][w];
+            if (D > 0) fadd<L>(c, ev[g][1], f.p);
+#pragma unroll
+            for (int w = 0; w < L; w++) a.claimed[(size_t)g * L + w] = c[w];
+        }
+        uint64_t *m = a.msgs + (((size_t)g * a.nvars + a.rd) * (a.maxd + 1)) * L;
+        for (uint32_t e = 1; e <= D; e++)
+#pragma unroll
+            for (int w = 0; w < L; w++) m[(size_t)(e - 1) * L + w] = ev[g][e][w];
+        if (!a.multi)
+            for (uint32_t e = 1; e <= D; e++) dev_absorb_field<L>(a.h, f, ev[g][e]);
+    }
+    if (a.multi)
+        for (uint32_t g = 0; g < a.ng; g++)
+            for (uint32_t e = 1; e <= a.degree[g]; e++) dev_absorb_field<L>(a.h, f, ev[g][e]);
+    // get_field_challenge: XOF of 8L bytes, absorbed as 0x12 | bytes | 0x34, read
+    // as an integer and put into Montgomery form; then absorbed as a field element
+    uint8_t b[8 * L + 2];
+    a.h->xof(b + 1, 8 * L);
+    b[0] = 0x12;
+    b[8 * L + 1] = 0x34;
+    a.h->update(b, 8 * L + 2);
+    uint64_t x[L], r[L];
+#pragma unroll
+    for (int w = 0; w < L; w++) {
+        x[w] = 0;
+        for (int k = 0; k < 8; k++) x[w] |= (uint64_t)b[1 + 8 * w + k] << (8 * k);
+    }
+    fmul<L>(x, f.r2, f.p, f.n0, r);
+    dev_absorb_field<L>(a.h, f, r);
+#pragma unroll
+    for (int w = 0; w < L; w++) {
+        a.r[w] = r[w];
+        a.point[(size_t)a.rd * L + w] = r[w];
+    }
+}
+
 // Per-group device state, carved out of the context's sumcheck arena.
 struct GroupDev {
     uint32_t degree = 0, K = 0;
@@ -473,6 +576,19 @@ zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int mu
     }
     const size_t off_r = total;
     total += 256;
+    if (ng > kScMaxGroups) {
+        set_error("sumcheck: %u groups (at most %u)", ng, kScMaxGroups);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    // device Fiat-Shamir state: the hasher, the round messages, claimed sums, point
+    const size_t off_h = total;
+    total = align256(total + sizeof(b3::Hasher));
+    const size_t off_msgs = total;
+    total = align256(total + (size_t)ng * nvars * (maxd + 1) * fb);
+    const size_t off_claimed = total;
+    total = align256(total + (size_t)ng * fb);
+    const size_t off_point = total;
+    total = align256(total + (size_t)nvars * fb);
     ZG_TRY(ctx->sc_arena.ensure(total));
     ZG_TRY(ctx->pin_in.ensure(256));
     ZG_TRY(ctx->pin_out.ensure((size_t)ng * max_blocks * (maxd + 1) * fb));
@@ -525,12 +641,31 @@ zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int mu
             tr_absorb_field(t, fe);
         }
     std::vector<uint64_t> msgs((size_t)ng * nvars * (maxd + 1) * L, 0), claimed((size_t)ng * L, 0);
-    uint64_t r[4] = {0, 0, 0, 0};
-    uint64_t *hr = ctx->pin_in.as<uint64_t>();
-    uint64_t *hpart = ctx->pin_out.as<uint64_t>();
+    b3::Hasher *h_d = reinterpret_cast<b3::Hasher *>(arena + off_h);
+    uint64_t *msgs_d = reinterpret_cast<uint64_t *>(arena + off_msgs);
+    uint64_t *claimed_d = reinterpret_cast<uint64_t *>(arena + off_claimed);
+    uint64_t *point_d = reinterpret_cast<uint64_t *>(arena + off_point);
+    // the transcript moves to the device for the rounds (its state is a plain struct)
+    ZG_TRY(ctx->pin_in.ensure(sizeof(b3::Hasher) + 256));
+    std::memcpy(ctx->pin_in.as<uint8_t>(), &t->h, sizeof(b3::Hasher));
+    ZG_CUDA(cudaMemcpyAsync(h_d, ctx->pin_in.as<uint8_t>(), sizeof(b3::Hasher), cudaMemcpyHostToDevice, s));
     std::vector<const uint64_t *> cur(ng);
     for (uint32_t g = 0; g < ng; g++) cur[g] = gd[g].in;
     size_t src_len = n;
+    FsArgs fa{};
+    fa.h = h_d;
+    fa.ng = ng;
+    fa.multi = multi ? 1 : 0;
+    fa.maxd = maxd;
+    fa.nvars = nvars;
+    fa.msgs = msgs_d;
+    fa.claimed = claimed_d;
+    fa.r = r_d;
+    fa.point = point_d;
+    for (uint32_t g = 0; g < ng; g++) {
+        fa.partials[g] = gd[g].partials;
+        fa.degree[g] = gd[g].degree;
+    }
     for (uint32_t rd = 0; rd < nvars; rd++) {
         const bool fold = rd > 0;
         const size_t len = fold ? src_len / 2 : src_len;
@@ -541,38 +676,31 @@ zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int mu
                                    r_d, gd[g].K, gd[g].comb, f, gd[g].partials, blocks, s));
             if (fold) cur[g] = dst;
         }
-        for (uint32_t g = 0; g < ng; g++)
-            ZG_CUDA(cudaMemcpyAsync(hpart + (size_t)g * max_blocks * (maxd + 1) * L, gd[g].partials,
-                                    (size_t)blocks * (gd[g].degree + 1) * fb, cudaMemcpyDeviceToHost, s));
+        fa.blocks = blocks;
+        fa.rd = rd;
+        ZG_KBEGIN(ctx, s, "k_sc_fs");
+        k_sc_fs<L><<<1, 256, 0, s>>>(fa, f);
+        ZG_KEND(ctx, s);
+        src_len = len;
+    }
+    {
+        // the transcript state, messages, claimed sums and point back to the host
+        uint8_t *hp = ctx->pin_out.as<uint8_t>();
+        const size_t mb = msgs.size() * 8, cb = claimed.size() * 8, pb = (size_t)nvars * fb;
+        ZG_TRY(ctx->pin_out.ensure(sizeof(b3::Hasher) + mb + cb + pb + 256));
+        hp = ctx->pin_out.as<uint8_t>();
+        ZG_CUDA(cudaMemcpyAsync(hp, h_d, sizeof(b3::Hasher), cudaMemcpyDeviceToHost, s));
+        ZG_CUDA(cudaMemcpyAsync(hp + sizeof(b3::Hasher), msgs_d, mb, cudaMemcpyDeviceToHost, s));
+        ZG_CUDA(cudaMemcpyAsync(hp + sizeof(b3::Hasher) + mb, claimed_d, cb, cudaMemcpyDeviceToHost, s));
+        ZG_CUDA(cudaMemcpyAsync(hp + sizeof(b3::Hasher) + mb + cb, point_d, pb, cudaMemcpyDeviceToHost, s));
         if (ctx_sync(ctx) != cudaSuccess) {
-            set_error("sumcheck round %u failed: %s", rd, cudaGetErrorString(cudaGetLastError()));
+            set_error("sumcheck rounds failed: %s", cudaGetErrorString(cudaGetLastError()));
             return ZG_ERR_CUDA;
         }
-        src_len = len;
-        for (uint32_t g = 0; g < ng; g++) {
-            const uint32_t Dg = gd[g].degree;
-            std::vector<uint64_t> ev((size_t)(Dg + 1) * L, 0);
-            const uint64_t *hp = hpart + (size_t)g * max_blocks * (maxd + 1) * L;
-            for (unsigned bk = 0; bk < blocks; bk++)
-                for (uint32_t tt = 0; tt <= Dg; tt++)
-                    fadd<L>(&ev[(size_t)tt * L], hp + ((size_t)bk * (Dg + 1) + tt) * L, f.p);
-            if (rd == 0) {
-                std::memcpy(&claimed[(size_t)g * L], &ev[0], fb);
-                if (Dg > 0) fadd<L>(&claimed[(size_t)g * L], &ev[L], f.p);
-            }
-            std::memcpy(&msgs[((size_t)g * nvars + rd) * (maxd + 1) * L], &ev[L], fb * Dg);
-            if (!multi)
-                for (uint32_t e = 1; e <= Dg; e++) tr_absorb_field(t, &ev[(size_t)e * L]);
-        }
-        if (multi)
-            for (uint32_t g = 0; g < ng; g++)
-                for (uint32_t e = 0; e < gd[g].degree; e++)
-                    tr_absorb_field(t, &msgs[(((size_t)g * nvars + rd) * (maxd + 1) + e) * L]);
-        field_challenge<L>(t, r);
-        tr_absorb_field(t, r);
-        if (point_out) std::memcpy(point_out + (size_t)rd * L, r, fb);
-        std::memcpy(hr, r, fb);  // the stream is idle here: safe to overwrite
-        ZG_CUDA(cudaMemcpyAsync(r_d, hr, fb, cudaMemcpyHostToDevice, s));
+        std::memcpy(&t->h, hp, sizeof(b3::Hasher));
+        std::memcpy(msgs.data(), hp + sizeof(b3::Hasher), mb);
+        std::memcpy(claimed.data(), hp + sizeof(b3::Hasher) + mb, cb);
+        if (point_out) std::memcpy(point_out, hp + sizeof(b3::Hasher) + mb + cb, pb);
     }
     // final evaluations of every MLE at the point (the last fold)
     if (finals_out) {

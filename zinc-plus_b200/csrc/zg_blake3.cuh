@@ -15,6 +15,15 @@
 #endif
 #endif
 
+// Host and device, not forced inline (the incremental hasher's update and XOF).
+#ifndef ZG_HDN
+#ifdef __CUDACC__
+#define ZG_HDN __host__ __device__
+#else
+#define ZG_HDN inline
+#endif
+#endif
+
 namespace zg {
 namespace b3 {
 
@@ -157,21 +166,21 @@ struct Hasher {
     uint32_t stack[54][8];
     uint32_t stack_len = 0;
 
-    Hasher() { reset(); }
-    void reset() {
+    ZG_HDN Hasher() { reset(); }
+    ZG_HDN void reset() {
         for (int i = 0; i < 8; i++) cv[i] = iv(i);
         chunk_counter = 0;
-        std::memset(block, 0, 64);
+        for (int i = 0; i < 64; i++) block[i] = 0;
         block_len = 0;
         blocks_compressed = 0;
         stack_len = 0;
     }
-    uint32_t chunk_len() const { return 64 * blocks_compressed + block_len; }
-    uint32_t start_flag() const { return blocks_compressed == 0 ? CHUNK_START : 0; }
-    void block_words(uint32_t m[16]) const {
+    ZG_HDN uint32_t chunk_len() const { return 64 * blocks_compressed + block_len; }
+    ZG_HDN uint32_t start_flag() const { return blocks_compressed == 0 ? CHUNK_START : 0; }
+    ZG_HDN void block_words(uint32_t m[16]) const {
         for (int i = 0; i < 16; i++) m[i] = load_le32(block + 4 * i);
     }
-    void finish_chunk_and_push() {
+    ZG_HDN void finish_chunk_and_push() {
         uint32_t m[16];
         block_words(m);
         uint32_t c[8];
@@ -186,11 +195,11 @@ struct Hasher {
         stack_len++;
         chunk_counter++;
         for (int i = 0; i < 8; i++) cv[i] = iv(i);
-        std::memset(block, 0, 64);
+        for (int i = 0; i < 64; i++) block[i] = 0;
         block_len = 0;
         blocks_compressed = 0;
     }
-    void update(const uint8_t *in, size_t n) {
+    ZG_HDN void update(const uint8_t *in, size_t n) {
         while (n) {
             if (chunk_len() == CHUNK_LEN) finish_chunk_and_push();
             if (block_len == 64) {
@@ -199,20 +208,20 @@ struct Hasher {
                 compress_cv(cv, m, chunk_counter, 64, start_flag());
                 blocks_compressed++;
                 block_len = 0;
-                std::memset(block, 0, 64);
+                for (int i = 0; i < 64; i++) block[i] = 0;
             }
             size_t room = 64 - block_len;
             size_t chunk_room = CHUNK_LEN - chunk_len();
             size_t take = n < room ? n : room;
             if (take > chunk_room) take = chunk_room;
-            std::memcpy(block + block_len, in, take);
+            for (size_t i = 0; i < take; i++) block[block_len + i] = in[i];
             block_len += (uint32_t)take;
             in += take;
             n -= take;
         }
     }
     // finalize_xof().fill(out): does not change the hasher state.
-    void xof(uint8_t *out, size_t n) const {
+    ZG_HDN void xof(uint8_t *out, size_t n) const {
         uint32_t ocv[8], m[16];
         uint32_t blen = block_len, flags = start_flag() | CHUNK_END;
         uint64_t counter = chunk_counter;
@@ -238,7 +247,7 @@ struct Hasher {
             uint8_t bytes[64];
             for (int i = 0; i < 16; i++) store_le32(bytes + 4 * i, w[i]);
             size_t take = n < 64 ? n : 64;
-            std::memcpy(out, bytes, take);
+            for (size_t i = 0; i < take; i++) out[i] = bytes[i];
             out += take;
             n -= take;
         }
