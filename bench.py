@@ -312,6 +312,19 @@ def run_batched_commit(Z, ctx, torch, stream, flush, reps, warm):
         ms, seq_roots = ev_time(sequential)
         ts.append(ms)
     same = [c.root for c in comms] == seq_roots
+    # the eight largest polynomials (num_vars 19-20) alone, one after another:
+    # each fills the GPU by itself, so no batching of the 64 can beat this time
+    big = [i for i, nv in enumerate(nvs) if nv >= 19]
+
+    def sequential_big():
+        for i in big:
+            h, _c = Z.ZipPlus.commit(plist[i], [polys[i]])
+            h.close()
+
+    tl = []
+    for _ in range(reps):
+        ms, _ = ev_time(sequential_big)
+        tl.append(ms)
     b, q = statistics.median(tb), statistics.median(ts)
     return {
         "workload": "64 polynomials, num_vars uniform 10..20, BinaryPoly<64> Bernoulli(0.5), "
@@ -319,6 +332,9 @@ def run_batched_commit(Z, ctx, torch, stream, flush, reps, warm):
         "evals": total, "value": total / (b / 1e3), "unit": "evals/s", "ms": b,
         "sequential": {"value": total / (q / 1e3), "ms": q},
         "batched_over_sequential": q / b, "roots_equal_sequential": same,
+        "largest_alone": {"polys": len(big), "evals": sum(1 << nvs[i] for i in big), "ms": statistics.median(tl),
+                          "what": "only the num_vars >= 19 polynomials, committed one after another: a lower "
+                                  "bound for any schedule of the 64"},
         "gpu_launches_per_call": launches, "reps": reps,
         "mode": "zg_commit_batch: same-shape groups in one launch chain, 4 lanes, autotuned "
                 "kernel variants, one CUDA graph replay per call; inputs in page-locked host "

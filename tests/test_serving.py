@@ -91,3 +91,15 @@ def test_server_rejects_request_above_budget(zipgpu, ctx, rng):
         srv.submit(pp, poly, point)
     assert e.value.status == 6
     srv.close()
+
+
+def test_served_results_equal_the_oracle(zipgpu, oracle, ctx, rng):
+    """Served proofs checked against the oracle directly (not only through the
+    plain GPU path): a mixed stream of i32 and BinaryPoly shapes, with groups."""
+    shapes, reqs, results, stats = _stream(zipgpu, ctx, rng, 16, workers=3)
+    assert stats.completed == 16
+    for (key, poly, point), (root, ev, proof, res) in zip(reqs, results):
+        ek, D, nv = key
+        desc = oracle.make_desc(ek, D, 0, nv, 1 << min(nv, 14) if ek else 1024)
+        ro, po, eo, _ = oracle.commit_prove(desc, poly, 1, point)
+        assert root == ro and proof == po and ev[:len(eo)] == eo
