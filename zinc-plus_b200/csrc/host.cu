@@ -375,8 +375,33 @@ static bool mr_base2(const uint64_t *n) {
     bool is_one = n[0] == 1;
     for (int i = 1; i < L; i++) is_one = is_one && n[i] == 0;
     if (is_one) return false;
+    // Only n0 and R mod n are needed (field_cfg_init also builds R^2 and more by
+    // 512 modular doublings, most of a test's time).  R mod n: from 2^(b-1) < n,
+    // b = bit length of n, double 64L - b + 1 times modulo n.
     FieldCfg f;
-    field_cfg_init(f, n, L);
+    std::memset(&f, 0, sizeof f);
+    f.L = L;
+    for (int i = 0; i < L; i++) f.p[i] = n[i];
+    {
+        uint64_t inv = n[0];
+        for (int i = 0; i < 6; i++) inv *= 2 - n[0] * inv;
+        f.n0 = (uint64_t)0 - inv;
+        int b = 64 * L;
+        while (b > 0 && !((n[(b - 1) / 64] >> ((b - 1) % 64)) & 1)) b--;
+        uint64_t y[L];
+        for (int i = 0; i < L; i++) y[i] = 0;
+        y[(b - 1) / 64] = 1ull << ((b - 1) % 64);
+        for (int k = 0; k < 64 * L - b + 1; k++) {
+            uint64_t c = 0;
+            for (int i = 0; i < L; i++) {
+                const uint64_t nc = y[i] >> 63;
+                y[i] = (y[i] << 1) | c;
+                c = nc;
+            }
+            if (c || ucmp<L>(y, n) >= 0) usub<L>(y, n);
+        }
+        for (int i = 0; i < L; i++) f.one[i] = y[i];
+    }
     uint64_t nm1[L];
     for (int i = 0; i < L; i++) nm1[i] = n[i];
     nm1[0] -= 1;
