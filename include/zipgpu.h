@@ -177,6 +177,13 @@ zg_status zg_encode_f_d(zg_params *p, const uint8_t *modulus, uint32_t limbs, co
 zg_status zg_merkle_root(zg_ctx *ctx, const void *rows, uint32_t n_rows, uint32_t width,
                          uint32_t elem_bytes, uint8_t root[32]);
 
+/* MillerRabin::test to base 2 (primality/src/lib.rs:12-19, crypto-primes'
+ * strong probable-prime test; the test get_random_field_cfg applies to each
+ * transcript candidate): out[c] = 1 when candidate c (limbs u64 LE, 1..4 limbs)
+ * is a base-2 strong probable prime.  Host only (eight candidates at a time
+ * with AVX-512 IFMA when the CPU has it). */
+zg_status zg_is_probable_prime_base2(const uint64_t *n, uint32_t limbs, uint32_t count, uint8_t *out);
+
 /* ---- Allocation-free Merkle root ---------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate device
  * memory on their request path (a serving loop that reserves its device-memory

@@ -165,3 +165,34 @@ def test_noalloc_root_rejects_misaligned_leaves_before_any_device_call(zipgpu):
     assert fn(0x10001, 4096, 256, 0x20000, None) == 1
     assert b"aligned" in zipgpu.lib().zg_last_error()
     assert fn(0x10002, 16, 16, 0x20000, None) == 1
+
+
+def _mr(zipgpu, vals, L):
+    arr = np.array([[(v >> (64 * i)) & ((1 << 64) - 1) for i in range(L)] for v in vals], np.uint64)
+    out = np.zeros(len(vals), np.uint8)
+    zipgpu.check(zipgpu.lib().zg_is_probable_prime_base2(arr.ctypes.data, L, len(vals), out.ctypes.data))
+    return [bool(x) for x in out]
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 4])
+def test_miller_rabin_matches_oracle(zipgpu, oracle, L):
+    """MillerRabin::test to base 2 (primality/src/lib.rs:12-19): the library's
+    test (eight candidates per vector when the CPU has AVX-512 IFMA) agrees with
+    the oracle's scalar test on random odd candidates, primes, the base-2 strong
+    pseudoprimes of the reference's test_base_two (which pass) and small cases."""
+    rng = np.random.default_rng(100 + L)
+    top = 64 * L
+    vals = [int.from_bytes(rng.bytes(8 * L), "little") | 1 for _ in range(1500)]
+    vals += [int.from_bytes(rng.bytes(8 * L), "little") >> int(rng.integers(0, top - 3)) | 1 for _ in range(300)]
+    vals += [2047, 3277, 4033, 4681, 8321, 15841, 29341, 42799, 49141, 52633, 65281, 74665, 80581, 85489,
+             1, 2, 3, 4, 5, 9, 15, 17, 65537, (1 << 61) - 1, (1 << top) - 1]
+    if L >= 2:
+        vals += [(1 << 127) - 1, (1 << 89) - 1, 3825123056546413051]
+    if L >= 4:
+        vals += [2**255 - 19, 2**256 - 189]
+    vals = [v % (1 << top) for v in vals]
+    got = _mr(zipgpu, vals, L)
+    want = [oracle.is_probable_prime_base2(v, L) for v in vals]
+    assert got == want
+    assert all(_mr(zipgpu, [2047, 3277, 4033], L))  # strong pseudoprimes to base 2 pass
+    assert sum(got) > 0

@@ -455,19 +455,39 @@ void tr_get_prime_batched(zg_transcript *t, int L, uint64_t *prime_out, int grou
     std::vector<b3::Hasher> states(group);
     std::vector<uint64_t> cand((size_t)group * 4);
     std::vector<char> ok(group);
-    const std::function<void(int)> test = [&](int g) {
-        uint64_t *c = &cand[(size_t)g * 4];
-        bool zero = true;
-        for (int i = 0; i < L; i++) zero = zero && c[i] == 0;
-        if (zero) {
-            ok[g] = 0;
-            return;
+    // one task per eight candidates: with AVX-512 IFMA the eight odd candidates
+    // above one are tested together, one per vector lane (mr_base2_x8)
+    const bool vec = mr_ifma_available();
+    const std::function<void(int)> test = [&](int q) {
+        const int g0 = 8 * q, g1 = std::min(group, g0 + 8);
+        uint64_t packed[8 * 4];
+        int idx[8], np = 0;
+        for (int g = g0; g < g1; g++) {
+            uint64_t *c = &cand[(size_t)g * 4];
+            bool zero = true;
+            for (int i = 0; i < L; i++) zero = zero && c[i] == 0;
+            if (zero) {
+                ok[g] = 0;
+                continue;
+            }
+            if (!(c[0] & 1)) {  // even: subtract one (full-width borrow)
+                for (int i = 0; i < L; i++)
+                    if (c[i]-- != 0) break;
+            }
+            bool one = c[0] == 1;
+            for (int i = 1; i < L; i++) one = one && c[i] == 0;
+            if (!vec || one) {
+                ok[g] = is_probable_prime_base2(c, L) ? 1 : 0;
+                continue;
+            }
+            for (int i = 0; i < L; i++) packed[(size_t)np * L + i] = c[i];
+            idx[np++] = g;
         }
-        if (!(c[0] & 1)) {  // even: subtract one (full-width borrow)
-            for (int i = 0; i < L; i++)
-                if (c[i]-- != 0) break;
+        if (np) {
+            uint8_t res[8];
+            mr_base2_x8(packed, L, np, res);
+            for (int e = 0; e < np; e++) ok[idx[e]] = (char)res[e];
         }
-        ok[g] = is_probable_prime_base2(c, L) ? 1 : 0;
     };
     for (;;) {
         b3::Hasher h = t->h;
@@ -480,7 +500,7 @@ void tr_get_prime_batched(zg_transcript *t, int L, uint64_t *prime_out, int grou
             std::memset(c, 0, 32);
             std::memcpy(c, buf, nb);
         }
-        run_all(group, test);
+        run_all((group + 7) / 8, test);
         for (int g = 0; g < group; g++) {
             if (ok[g]) {
                 t->h = states[g];
@@ -494,8 +514,9 @@ void tr_get_prime_batched(zg_transcript *t, int L, uint64_t *prime_out, int grou
 
 void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads) {
     const int team = threads > 0 ? threads : omp_get_max_threads();
-    // candidates generated ahead per round (speculative; a single thread tests one at a time)
-    const int group = team == 1 ? 1 : std::max(8, 2 * team);
+    // candidates generated ahead per round (speculative): eight per thread with
+    // the vector test; without it one per thread (a single thread, one at a time)
+    const int group = mr_ifma_available() ? 8 * team : team == 1 ? 1 : std::max(8, 2 * team);
     tr_get_prime_batched(t, L, prime_out, group, [team](int n, const std::function<void(int)> &fn) {
         if (team == 1) {
             for (int g = 0; g < n; g++) fn(g);
@@ -665,3 +686,39 @@ void stdrng_shuffle_identity(uint64_t seed, uint32_t n, uint32_t *perm) {
 }
 
 }  // namespace zg
+
+// MillerRabin::test to base 2 (primality/src/lib.rs:12-19) of `count`
+// candidates of `limbs` u64 each: the vector path for odd candidates above one
+// when the CPU has it, the scalar test otherwise.
+extern "C" zg_status zg_is_probable_prime_base2(const uint64_t *n, uint32_t limbs, uint32_t count, uint8_t *out) {
+    using namespace zg;
+    if (!n || !out || limbs < 1 || limbs > MAX_FIELD_LIMBS) {
+        set_error("is_probable_prime: null argument or %u limbs (1 to %d)", limbs, MAX_FIELD_LIMBS);
+        return ZG_ERR_INVALID_PARAM;
+    }
+    const int L = (int)limbs;
+    const bool vec = mr_ifma_available();
+    uint64_t packed[8 * 4];
+    uint32_t idx[8];
+    int np = 0;
+    auto flush = [&]() {
+        uint8_t res[8];
+        mr_base2_x8(packed, L, np, res);
+        for (int e = 0; e < np; e++) out[idx[e]] = res[e];
+        np = 0;
+    };
+    for (uint32_t c = 0; c < count; c++) {
+        const uint64_t *x = n + (size_t)c * L;
+        bool one = x[0] == 1;
+        for (int i = 1; i < L; i++) one = one && x[i] == 0;
+        if (!vec || one || !(x[0] & 1)) {
+            out[c] = is_probable_prime_base2(x, L) ? 1 : 0;
+            continue;
+        }
+        for (int i = 0; i < L; i++) packed[(size_t)np * L + i] = x[i];
+        idx[np++] = c;
+        if (np == 8) flush();
+    }
+    if (np) flush();
+    return ZG_OK;
+}

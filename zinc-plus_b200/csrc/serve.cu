@@ -417,7 +417,7 @@ zg_status zg_server_create(zg_ctx *ctx, const zg_server_opts *opts, zg_server **
             const int hw = (int)std::max(2u, std::thread::hardware_concurrency());
             const int nt = std::max(1, std::min(16, hw / 2));
             s->tests.reset(new TestPool(nt));
-            s->prime_group = std::max(8, 2 * (nt + 1));
+            s->prime_group = mr_ifma_available() ? 8 * (nt + 1) : std::max(8, 2 * (nt + 1));
         }
         zg_server *raw = s.get();
         for (uint32_t i = 0; i < o.workers; i++) raw->workers.emplace_back(worker_main, raw, i);

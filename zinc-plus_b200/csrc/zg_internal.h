@@ -313,6 +313,10 @@ zg_status cpr_prove_impl(zg_ctx *ctx, zg_transcript *t, const uint8_t *modulus, 
                          uint64_t *evals_out);
 
 void tr_get_prime(zg_transcript *t, int L, uint64_t *prime_out, int threads);
+// Base-2 Miller-Rabin on up to eight odd candidates above one at once, with
+// AVX-512 IFMA (mr_ifma.cpp); only when mr_ifma_available().
+bool mr_ifma_available();
+void mr_base2_x8(const uint64_t *cand, int L, int count, uint8_t *ok);
 // The same search with the candidate tests of each round run by run_all(n, test).
 void tr_get_prime_batched(zg_transcript *t, int L, uint64_t *prime_out, int group,
                           const std::function<void(int, const std::function<void(int)> &)> &run_all);

@@ -50,7 +50,7 @@ EXPORTS = (
     "zg_server_submit", "zg_server_wait", "zg_server_get_stats", "zg_server_destroy",
     "zg_selftest_bounded_wait", "zg_piop_eval_projection", "zg_piop_lifted_evals", "zg_piop_multipoint_eval",
     "zg_piop_cpr_linear_prove", "zg_piop_ideal_check_linear", "zg_prove_f", "zg_prove_f_d",
-    "zg_zinc_prove_mle_first", "zg_zinc_prove", "zg_encode_f", "zg_encode_f_d", "zg_proof_read", "zg_debug_fail_allocation",
+    "zg_zinc_prove_mle_first", "zg_zinc_prove", "zg_encode_f", "zg_encode_f_d", "zg_proof_read", "zg_debug_fail_allocation", "zg_is_probable_prime_base2",
 )
 
 
@@ -176,6 +176,7 @@ def lib() -> C.CDLL:
         "zg_zinc_prove_mle_first": ([vp, vp, C.POINTER(LinearUairDesc), C.c_uint32, vp, vp, C.c_int, vp,
                                      C.POINTER(sz)], st),
         "zg_debug_fail_allocation": ([C.c_uint32], st),
+        "zg_is_probable_prime_base2": ([vp, C.c_uint32, C.c_uint32, vp], st),
         "zg_proof_read": ([C.c_char_p, sz, C.c_uint32, C.c_uint32, C.POINTER(ProofLayout)], st),
         "zg_encode_f": ([vp, C.c_char_p, C.c_uint32, vp, vp], st),
         "zg_encode_f_d": ([vp, C.c_char_p, C.c_uint32, vp, vp, vp], st),
