@@ -325,9 +325,10 @@ zg_status commit_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_
     };
     zg_status st = launch_encode(p, ctx, polys_d, nrows, h->d_cw, true, s);
     if (st != ZG_OK) return fail(st);
-    st = launch_leaf_hash(ctx, h->d_cw, C, (uint32_t)leaf_bytes, h->d_tree, s);
+    uint32_t done = 0;
+    st = launch_leaf_hash(ctx, h->d_cw, C, (uint32_t)leaf_bytes, h->d_tree, s, 0, -1, &done);
     if (st != ZG_OK) return fail(st);
-    st = launch_merkle_levels(ctx, h->d_tree, C, s);
+    st = launch_merkle_levels(ctx, h->d_tree, C, s, 1, done);
     if (st != ZG_OK) return fail(st);
     if ((st = ctx->pin_out.ensure(64)) != ZG_OK) return fail(st);
     uint8_t *hroot = ctx->pin_out.as<uint8_t>();
@@ -365,9 +366,10 @@ zg_status launch_commit_group(zg_params *p, zg_ctx *lane, const void *polys_d, u
     }
     const uint32_t C = p->info.codeword_len, R = p->info.num_rows;
     ZG_TRY(launch_encode(p, lane, polys_d, m * R, cw_d, true, s, m > 1 ? R : 0, tune.base_variant));
+    uint32_t done = 0;
     ZG_TRY(launch_leaf_hash(lane, cw_d, m * C, (uint32_t)leaf_bytes_of(p, 1), tree_d, s,
-                            m > 1 ? C : 0, tune.leaf_variant));
-    return launch_merkle_levels(lane, tree_d, C, s, m);
+                            m > 1 ? C : 0, tune.leaf_variant, &done));
+    return launch_merkle_levels(lane, tree_d, C, s, m, done);
 }
 
 zg_status commit_group_device(zg_params *p, zg_ctx *lane, const void *polys_d, uint32_t m,
@@ -1212,8 +1214,10 @@ static zg_status merkle_root_impl(zg_ctx *ctx, const void *rows, uint32_t n_rows
     cudaStream_t s = ctx->stream;
     st = ZG_OK;
     if (cudaMemcpyAsync(cw.ptr, lm.data(), total, cudaMemcpyHostToDevice, s) != cudaSuccess) st = ZG_ERR_CUDA;
-    if (st == ZG_OK) st = launch_leaf_hash(ctx, cw.as<uint8_t>(), width, (uint32_t)leaf, tree.as<uint8_t>(), s);
-    if (st == ZG_OK) st = launch_merkle_levels(ctx, tree.as<uint8_t>(), width, s);
+    uint32_t done = 0;
+    if (st == ZG_OK)
+        st = launch_leaf_hash(ctx, cw.as<uint8_t>(), width, (uint32_t)leaf, tree.as<uint8_t>(), s, 0, -1, &done);
+    if (st == ZG_OK) st = launch_merkle_levels(ctx, tree.as<uint8_t>(), width, s, 1, done);
     if (st == ZG_OK) {
         if (cudaMemcpyAsync(root, tree.as<uint8_t>() + (o - 1) * 32, 32, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             ctx_sync(ctx) != cudaSuccess) {

@@ -50,11 +50,15 @@ __global__ void __launch_bounds__(128) k_leaf_small(const uint8_t *__restrict__ 
 // loads the 32 leaves' blocks with 16-byte loads (four lanes per leaf, so each
 // instruction reads eight 64-byte runs) into shared memory, then every lane
 // compresses its own leaf's block from there.
+// With fuse (every block's 128 leaves in one tree of at least 128 leaves), the
+// block then reduces its leaves to their subtree's root: tree levels 1..7 from
+// shared memory, writing every node, so the level kernel starts at level 7.
 __global__ void __launch_bounds__(128) k_leaf_small_coalesced(const uint8_t *__restrict__ cw,
                                                               uint32_t width, uint32_t leaf_bytes,
                                                               uint32_t *__restrict__ leaves,
-                                                              uint32_t tree_log) {
+                                                              uint32_t tree_log, int fuse) {
     __shared__ uint32_t tile[4][32 * 17];  // per warp: 32 leaves x 16 words (+1 pad)
+    __shared__ uint32_t sub[128][9];       // the block's subtree level (+1 pad)
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t first = (blockIdx.x * 4 + warp) * 32;
     uint32_t *t = tile[warp];
@@ -90,6 +94,36 @@ __global__ void __launch_bounds__(128) k_leaf_small_coalesced(const uint8_t *__r
         const size_t node = leaf_node(first + lane, tree_log);
 #pragma unroll
         for (int i = 0; i < 8; i++) leaves[node * 8 + i] = cv[i];
+    }
+    if (!fuse) return;
+    const uint32_t tt = threadIdx.x, g0 = blockIdx.x * 128;
+    const uint32_t W = tree_log >= 32 ? width : (1u << tree_log);
+    const uint32_t depth = 31 - __clz(W);
+    const size_t tree_base = tree_log >= 32 ? 0 : (size_t)(g0 >> tree_log) * (2ull * W - 1);
+    const uint32_t local0 = g0 & (W - 1);
+#pragma unroll
+    for (int i = 0; i < 8; i++) sub[tt][i] = cv[i];
+    __syncthreads();
+    for (uint32_t k = 1; k <= 7; k++) {
+        const uint32_t n = 128u >> k;
+        uint32_t l[8], r[8], o[8];
+        if (tt < n)
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                l[i] = sub[2 * tt][i];
+                r[i] = sub[2 * tt + 1][i];
+            }
+        __syncthreads();
+        if (tt < n) {
+            b3::parent_cv(l, r, k == depth, o);
+            const size_t node = tree_base + (2ull * W - 2ull * (W >> k)) + (local0 >> k) + tt;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                leaves[node * 8 + i] = o[i];
+                sub[tt][i] = o[i];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -271,7 +305,8 @@ __global__ void __launch_bounds__(256) k_tree_levels(uint32_t *__restrict__ fore
 
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
                            uint8_t *leaves_d, cudaStream_t s, uint32_t tree_width,
-                           int leaf_variant) {
+                           int leaf_variant, uint32_t *levels_done) {
+    if (levels_done) *levels_done = 0;
     if (leaf_bytes % 4 != 0) {
         set_error("leaf size %u is not a multiple of 4 bytes", leaf_bytes);
         return ZG_ERR_INVALID_PARAM;
@@ -287,10 +322,13 @@ zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uin
     uint32_t *leaves = reinterpret_cast<uint32_t *>(leaves_d);
     if (leaf_bytes <= b3::CHUNK_LEN) {
         ZG_KBEGIN(ctx, s, "k_leaf_small");
-        if (leaf_bytes % 16 == 0 && leaf_bytes > 0 && leaf_variant != 1)
+        if (leaf_bytes % 16 == 0 && leaf_bytes > 0 && leaf_variant != 1) {
+            const uint32_t W = tree_log >= 32 ? width : (1u << tree_log);
+            const int fuse = levels_done && W >= 128 && width % 128 == 0 ? 1 : 0;
             k_leaf_small_coalesced<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves,
-                                                                      tree_log);
-        else
+                                                                      tree_log, fuse);
+            if (fuse) *levels_done = 7;
+        } else
             k_leaf_small<<<(width + 127) / 128, 128, 0, s>>>(cw_d, width, leaf_bytes, leaves, tree_log);
         ZG_KEND(ctx, s);
         return ZG_OK;
@@ -313,10 +351,10 @@ zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uin
 }
 
 zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s,
-                               uint32_t ntrees) {
+                               uint32_t ntrees, uint32_t k_start) {
     uint32_t *tree = reinterpret_cast<uint32_t *>(tree_d);
     const uint32_t depth = 31 - __builtin_clz(width);
-    for (uint32_t k0 = 0; k0 < depth;) {
+    for (uint32_t k0 = k_start; k0 < depth;) {
         const uint32_t nlev = depth - k0 < 9 ? depth - k0 : 9;
         const uint32_t blocks = (width >> (k0 + nlev)) * ntrees;
         ZG_KBEGIN(ctx, s, "k_tree_levels");

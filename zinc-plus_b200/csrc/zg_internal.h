@@ -377,12 +377,15 @@ zg_status launch_encode_wide_at(zg_params *p, zg_ctx *ctx, const uint64_t *row_d
                                 const uint32_t *pos_d, uint32_t n, uint64_t *out_d, cudaStream_t s);
 // tree_width: the `width` leaves belong to width / tree_width trees, stored in
 // consecutive blocks of 2 tree_width - 1 nodes; 0 = one tree.
+// levels_done (may be NULL: none): set to the tree levels the leaf kernel
+// already built (7 when it reduced each block's 128 leaves, else 0).
 zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uint32_t leaf_bytes,
                            uint8_t *leaves_d, cudaStream_t s, uint32_t tree_width = 0,
-                           int leaf_variant = -1);
-// All levels of ntrees trees of `width` leaves each (blocks of 2 width - 1 nodes).
+                           int leaf_variant = -1, uint32_t *levels_done = nullptr);
+// Levels k_start + 1 .. depth of ntrees trees of `width` leaves each (blocks of
+// 2 width - 1 nodes), layer k_start already built.
 zg_status launch_merkle_levels(zg_ctx *ctx, uint8_t *tree_d, uint32_t width, cudaStream_t s,
-                               uint32_t ntrees = 1);
+                               uint32_t ntrees = 1, uint32_t k_start = 0);
 
 // Node offset of Merkle layer k for `width` leaves (layers stored leaves first).
 inline size_t merkle_layer_off(size_t width, uint32_t k) { return 2 * width - 2 * (width >> k); }
