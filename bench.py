@@ -1134,10 +1134,15 @@ def run_zinc_prove(Z, ctx, nv, cpu_nv, with_cpu):
 
     pb, pi = tables(nv)
     proof = Z.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+    # a page-locked output buffer: the column openings arrive in place by DMA
+    import torch
+
+    pinned = torch.empty(len(proof) + (1 << 20), dtype=torch.uint8).pin_memory().numpy()
+    Z.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs, out_buffer=pinned)
     ts = []
     for _ in range(3):
         a = time.perf_counter()
-        again = Z.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs)
+        again = Z.ZincPlusPiop.prove_mle_first(pb, pi, nv, bins, 32, ints, shifts, coeffs, out_buffer=pinned)
         ts.append((time.perf_counter() - a) * 1e3)
     ms = statistics.median(ts)
     # the reference's default path (MLE_FIRST = false) on the same trace
@@ -1152,7 +1157,8 @@ def run_zinc_prove(Z, ctx, nv, cpu_nv, with_cpu):
     res = {"workload": f"BigLinearUair, 2^{nv} rows: 16 BinaryPoly<32> + 1 i64 column, 16 shifts, 17 constraints; "
                        "MontyField<3>; IPRS rate 1/4, 16 rows per table; 147 openings",
            "ms": ms, "rows_per_s": (1 << nv) / (ms / 1e3), "proof_bytes": len(proof),
-           "deterministic": again == proof, "h2d_bytes": int(bins.nbytes + ints.nbytes),
+           "deterministic": bytes(again) == proof, "h2d_bytes": int(bins.nbytes + ints.nbytes),
+           "output": "page-locked host buffer (the column openings land in place by DMA)",
            "what": "commit both tables, prime, ideal check, evaluation projection, CPR sumcheck, multipoint "
                    "sumcheck, lifted evaluations, prove_f of both tables, Proof transcription"}
     res.update(res0)

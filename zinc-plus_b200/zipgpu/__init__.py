@@ -874,8 +874,11 @@ class ZincPlusPiop:
 
     @staticmethod
     def prove_mle_first(pp_bin, pp_int, nvars: int, bin_cols, degree_plus_one: int, int_cols, shifts,
-                        coeffs, n_pub_bin: int = 0, n_pub_int: int = 0) -> bytes:
-        """The first n_pub_bin binary and n_pub_int integer columns are public."""
+                        coeffs, n_pub_bin: int = 0, n_pub_int: int = 0, out_buffer=None) -> bytes:
+        """The first n_pub_bin binary and n_pub_int integer columns are public.
+        out_buffer (optional): a uint8 array the proof is written into (a
+        page-locked one receives the column openings by DMA); the proof is then
+        returned as a view of it (valid until the buffer is reused), not a copy."""
         b, i = ZincPiop._cols(bin_cols, int_cols, nvars)
         src = np.array([s for s, _ in shifts] or [0], np.uint32)
         amt = np.array([a for _, a in shifts] or [0], np.uint32)
@@ -892,12 +895,16 @@ class ZincPlusPiop:
             if pp is not None:
                 cap += pp.proof_size(max(b.shape[0], i.shape[0], 1))
         cap += (ncols * (degree_plus_one + 2) + cf.shape[0] * degree_plus_one + 64 * nvars) * 64
-        buf = ZincPlusPiop._out
+        buf = out_buffer if out_buffer is not None else ZincPlusPiop._out
         if buf is None or buf.size < cap:
+            if out_buffer is not None:
+                raise ValueError(f"out_buffer holds {out_buffer.size} bytes, {cap} needed")
             buf = ZincPlusPiop._out = np.empty(cap, np.uint8)
         n = C.c_size_t(buf.size)
         check(lib().zg_zinc_prove_mle_first(pbin, pint, C.byref(u), nvars, _ptr(b), _ptr(i), 0, _ptr(buf),
                                             C.byref(n)))
+        if out_buffer is not None:
+            return memoryview(buf)[: n.value]
         return buf[: n.value].tobytes()
 
     @staticmethod
