@@ -319,6 +319,9 @@ def test_gpu_combined_path_products_match_oracle_and_verify(zipgpu, oracle, ctx,
     assert got == want
     P = parse_proof(got, 3, nv)
     assert P["degree"] == 4 and P["ic"][0] == b""
+    lay = zipgpu.read_proof(got, 3, nv)  # the library's own Proof reader agrees
+    assert lay["cpr_degree"] == 4 and lay["n_ideal_values"] == 3 and lay["n_lifted"] == 5
+    assert got[lay["zip_offset"]:lay["zip_offset"] + lay["zip_len"]] == P["zip"]
     # the honest x * y = z constraint passes; the other two are not in their ideals
     # for random columns, which the verifier's ideal check rejects (step 2)
     assert oracle.zinc_verify(db, di, nv, None, None, U, 3, got) == 2
