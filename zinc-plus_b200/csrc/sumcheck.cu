@@ -104,26 +104,20 @@ __device__ __forceinline__ void load_el(const uint64_t *p, uint64_t (&v)[L]) {
     for (int w = 0; w < L; w++) v[w] = p[w];
 }
 
-// One round for one group: (fold) and the block's partial sums of P(t),
-// t = 0..D.  src: K MLEs of src_len entries; with fold, the round's MLEs (half
-// as long) are written to dst first.  kScSub consecutive threads share a pair:
-// each folds every kScSub-th MLE and evaluates every kScSub-th product, their
-// sums of products are combined by shuffles, and the first applies the factors.
-template <int L, int D, int kScSub>
-__global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__restrict__ src,
-                                                         size_t src_len, uint64_t *__restrict__ dst,
-                                                         int fold, const uint64_t *__restrict__ r,
-                                                         uint32_t K, ScComb c, FieldCfg f,
-                                                         uint64_t *__restrict__ partials) {
-    __shared__ uint64_t red[kScThreads / 32][(D + 1) * L];
-    Fe<L> pf;
-#pragma unroll
-    for (int w = 0; w < L; w++) pf.w[w] = f.p[w];
-    const size_t len = fold ? src_len / 2 : src_len, half = len / 2;
-    const uint32_t sub = threadIdx.x % kScSub;
-    const size_t b = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / kScSub;
-    const bool active = b < half;
-    uint64_t ev[D + 1][L];
+// One thread's part of one pair in a round: with fold, the pair's MLEs are
+// folded at r and written to dst first (each of the pair's kScSub threads folds
+// every kScSub-th MLE); then the thread's share of the sum of products at
+// t = 0..D, combined over the pair's threads by shuffles, times the affine
+// factors.  Summing ev over every thread of every pair gives P(t).  All 32
+// lanes of the warp must call it together (the shuffles take the full warp).
+// OUTLINE selects the out-of-line field product.
+template <int L, int D, int kScSub, bool OUTLINE>
+__device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t src_len,
+                                        uint64_t *__restrict__ dst, int fold,
+                                        const uint64_t *__restrict__ r, uint32_t K, const ScComb &c,
+                                        const FieldCfg &f, const Fe<L> &pf, size_t b, bool active,
+                                        uint32_t sub, uint64_t (&ev)[D + 1][L]) {
+    const size_t len = fold ? src_len / 2 : src_len;
 #pragma unroll
     for (int t = 0; t <= D; t++)
 #pragma unroll
@@ -140,7 +134,7 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
                     load_el<L>(q + 2 * e * L, a0);
                     load_el<L>(q + (2 * e + 1) * L, a1);
                     fsub<L>(a1, a0, f.p);
-                    fmul_c<L, (kScSub == kScSubMax)>(rr, a1, pf, f.n0, pr);
+                    fmul_c<L, OUTLINE>(rr, a1, pf, f.n0, pr);
                     fadd<L>(a0, pr, f.p);
 #pragma unroll
                 for (int w = 0; w < L; w++) o[e * L + w] = a0[w];
@@ -167,9 +161,9 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
                 uint64_t v0[L], v1[L], o[L];
                 load_el<L>(v, v0);
                 load_el<L>(v + L, v1);
-                fmul_c<L, (kScSub == kScSubMax)>(cf, v0, pf, f.n0, o);
+                fmul_c<L, OUTLINE>(cf, v0, pf, f.n0, o);
                 fadd<L>(lin0, o, f.p);
-                fmul_c<L, (kScSub == kScSubMax)>(cf, v1, pf, f.n0, o);
+                fmul_c<L, OUTLINE>(cf, v1, pf, f.n0, o);
                 fadd<L>(lin1, o, f.p);
                 any_lin = true;
                 continue;
@@ -187,7 +181,7 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
 #pragma unroll
                 for (int t = 0; t <= D; t++) {
                     uint64_t o[L];
-                    fmul_c<L, (kScSub == kScSubMax)>(pr[t], cur, pf, f.n0, o);
+                    fmul_c<L, OUTLINE>(pr[t], cur, pf, f.n0, o);
 #pragma unroll
                     for (int w = 0; w < L; w++) pr[t][w] = o[w];
                     if (t < D) fadd<L>(cur, st, f.p);
@@ -245,9 +239,9 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
                 for (uint32_t i = 0; i < sub; i++) fadd<L>(cur, st, f.p);  // v(sub)
                 load_el<L>(c.fa + (size_t)q * L, fa);
                 load_el<L>(c.fb + (size_t)q * L, fbv);
-                fmul_c<L, (kScSub == kScSubMax)>(fbv, cur, pf, f.n0, fv);
+                fmul_c<L, OUTLINE>(fbv, cur, pf, f.n0, fv);
                 fadd<L>(fv, fa, f.p);
-                fmul_c<L, (kScSub == kScSubMax)>(keep, fv, pf, f.n0, o);
+                fmul_c<L, OUTLINE>(keep, fv, pf, f.n0, o);
 #pragma unroll
                 for (int w = 0; w < L; w++) keep[w] = o[w];
             }
@@ -274,15 +268,36 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
 #pragma unroll
             for (int t = 0; t <= D; t++) {
                 uint64_t fv[L], o[L];
-                fmul_c<L, (kScSub == kScSubMax)>(fbv, cur, pf, f.n0, fv);
+                fmul_c<L, OUTLINE>(fbv, cur, pf, f.n0, fv);
                 fadd<L>(fv, fa, f.p);
-                fmul_c<L, (kScSub == kScSubMax)>(ev[t], fv, pf, f.n0, o);
+                fmul_c<L, OUTLINE>(ev[t], fv, pf, f.n0, o);
 #pragma unroll
                 for (int w = 0; w < L; w++) ev[t][w] = o[w];
                 if (t < D) fadd<L>(cur, st, f.p);
             }
         }
     }
+}
+
+// One round for one group: (fold) and the block's partial sums of P(t),
+// t = 0..D.  src: K MLEs of src_len entries; with fold, the round's MLEs (half
+// as long) are written to dst first.  kScSub consecutive threads share a pair.
+template <int L, int D, int kScSub>
+__global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__restrict__ src,
+                                                         size_t src_len, uint64_t *__restrict__ dst,
+                                                         int fold, const uint64_t *__restrict__ r,
+                                                         uint32_t K, ScComb c, FieldCfg f,
+                                                         uint64_t *__restrict__ partials) {
+    __shared__ uint64_t red[kScThreads / 32][(D + 1) * L];
+    Fe<L> pf;
+#pragma unroll
+    for (int w = 0; w < L; w++) pf.w[w] = f.p[w];
+    const size_t len = fold ? src_len / 2 : src_len, half = len / 2;
+    const uint32_t sub = threadIdx.x % kScSub;
+    const size_t b = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / kScSub;
+    uint64_t ev[D + 1][L];
+    sc_pair<L, D, kScSub, kScSub == kScSubMax>(src, src_len, dst, fold, r, K, c, f, pf, b, b < half,
+                                                sub, ev);
     // warp tree reduction, then across the block's warps
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -393,87 +408,187 @@ struct FsArgs {
     uint64_t *point;    // [round][L]
 };
 
-// absorb_random_field (transcript/src/traits.rs:393-413): 0x03 | modulus | 0x05 | 0x01 | inner | 0x03
+// Byte j of absorb_random_field's encoding of `inner` (transcript/src/
+// traits.rs:393-413): 0x03 | modulus | 0x05 | 0x01 | inner | 0x03, 16L + 4 bytes.
 template <int L>
-__device__ void dev_absorb_field(b3::Hasher *h, const FieldCfg &f, const uint64_t *inner) {
-    uint8_t buf[16 * L + 4];
-    int k = 0;
-    buf[k++] = 3;
-    for (int w = 0; w < L; w++)
-        for (int b = 0; b < 8; b++) buf[k++] = (uint8_t)(f.p[w] >> (8 * b));
-    buf[k++] = 5;
-    buf[k++] = 1;
-    for (int w = 0; w < L; w++)
-        for (int b = 0; b < 8; b++) buf[k++] = (uint8_t)(inner[w] >> (8 * b));
-    buf[k++] = 3;
-    h->update(buf, (size_t)k);
+__device__ __forceinline__ uint8_t field_byte(const FieldCfg &f, const uint64_t *inner, uint32_t j) {
+    if (j == 0 || j == 16 * L + 3) return 3;
+    if (j <= 8 * L) {
+        const uint32_t k = j - 1;
+        return (uint8_t)(f.p[k >> 3] >> (8 * (k & 7)));
+    }
+    if (j == 8 * L + 1) return 5;
+    if (j == 8 * L + 2) return 1;
+    const uint32_t k = j - 8 * L - 3;
+    return (uint8_t)(inner[k >> 3] >> (8 * (k & 7)));
+}
+
+// Hasher::update by one warp on a hasher in shared memory: lane 0 takes the
+// block and chunk boundaries (the compressions), the lanes copy the bytes.  The
+// same state changes as the one-thread update, so the same transcript; one
+// thread copying byte by byte was most of a round's transcript time.
+__device__ void warp_update(b3::Hasher *h, const uint8_t *in, uint32_t n) {
+    const uint32_t lane = threadIdx.x & 31;
+    while (n) {
+        if (lane == 0) {
+            if (h->chunk_len() == b3::CHUNK_LEN) h->finish_chunk_and_push();
+            if (h->block_len == 64) {
+                uint32_t m[16];
+                h->block_words(m);
+                b3::compress_cv_h(h->cv, m, h->chunk_counter, 64, h->start_flag());
+                h->blocks_compressed++;
+                h->block_len = 0;
+                h->clear_block();
+            }
+        }
+        __syncwarp();
+        const uint32_t bl = h->block_len;
+        const uint32_t take = n < 64 - bl ? n : 64 - bl;
+        for (uint32_t i = lane; i < take; i += 32) h->block[bl + i] = in[i];
+        __syncwarp();
+        if (lane == 0) h->block_len = bl + take;
+        __syncwarp();
+        in += take;
+        n -= take;
+    }
+}
+
+// Hasher::xof for the first 8L output bytes, as L little-endian words.
+template <int L>
+__device__ void xof_words(const b3::Hasher *h, uint64_t *x) {
+    uint32_t ocv[8], m[16];
+    uint32_t blen = h->block_len, flags = h->start_flag() | b3::CHUNK_END;
+    uint64_t counter = h->chunk_counter;
+    for (int i = 0; i < 8; i++) ocv[i] = h->cv[i];
+    h->block_words(m);
+    for (int s = (int)h->stack_len - 1; s >= 0; s--) {
+        uint32_t c[8];
+        for (int i = 0; i < 8; i++) c[i] = ocv[i];
+        b3::compress_cv_h(c, m, counter, blen, flags);
+        for (int i = 0; i < 8; i++) {
+            m[i] = h->stack[s][i];
+            m[8 + i] = c[i];
+            ocv[i] = b3::iv(i);
+        }
+        counter = 0;
+        blen = 64;
+        flags = b3::PARENT;
+    }
+    uint32_t w[16];
+    b3::compress_h(ocv, m, 0, blen, flags | b3::ROOT, w);
+    for (int j = 0; j < L; j++) x[j] = (uint64_t)w[2 * j] | ((uint64_t)w[2 * j + 1] << 32);
+}
+
+// Bytes of the transcript step of one round: every round message, the squeeze
+// and the challenge, at most kScMaxGroups x kScMaxDeg field elements.
+constexpr uint32_t kFsBufBytes = kScMaxGroups * kScMaxDeg * (16 * 4 + 4) + 128;
+
+// Block-cooperative copy of a hasher (global <-> shared memory).  The
+// transcript step runs on a shared-memory copy.
+__device__ __forceinline__ void hasher_copy(b3::Hasher *dst, const b3::Hasher *src) {
+    static_assert(sizeof(b3::Hasher) % 8 == 0, "hasher size");
+    const uint64_t *s = reinterpret_cast<const uint64_t *>(src);
+    uint64_t *d = reinterpret_cast<uint64_t *>(dst);
+    for (uint32_t i = threadIdx.x; i < sizeof(b3::Hasher) / 8; i += blockDim.x) d[i] = s[i];
+}
+
+// One round's transcript step, by one warp (all 32 lanes call it), in the
+// reference's order (piop/src/sumcheck.rs:180-199, multi_degree.rs:300-340):
+// the round-0 claimed sums are kept, the round messages P(1..deg) stored and
+// absorbed (MLSumcheck: its one group's; MultiDegreeSumcheck: every group's in
+// group order, the same byte sequence), the challenge squeezed
+// (get_field_challenge: XOF of 8L bytes absorbed as 0x12 | bytes | 0x34, read
+// as an integer and put into Montgomery form) and absorbed.  The challenge goes
+// to r_out[0..L) and point[rd].  buf: kFsBufBytes of shared memory.
+template <int L>
+__device__ void fs_round(b3::Hasher *h, const FieldCfg &f, const uint64_t (*ev)[kScMaxDeg + 1][L],
+                         const uint32_t *degree, uint32_t ng, uint32_t multi, uint32_t rd,
+                         uint32_t maxd, uint32_t nvars, uint64_t *msgs, uint64_t *claimed,
+                         uint64_t *point, uint64_t *r_out, uint8_t *buf) {
+    const uint32_t lane = threadIdx.x & 31;
+    constexpr uint32_t FB = 16 * L + 4;
+    (void)multi;
+    if (lane == 0)
+        for (uint32_t g = 0; g < ng; g++) {
+            const uint32_t D = degree[g];
+            if (rd == 0) {
+                uint64_t c[L];
+#pragma unroll
+                for (int w = 0; w < L; w++) c[w] = ev[g][0][w];
+                if (D > 0) fadd<L>(c, ev[g][1], f.p);
+#pragma unroll
+                for (int w = 0; w < L; w++) claimed[(size_t)g * L + w] = c[w];
+            }
+            uint64_t *m = msgs + (((size_t)g * nvars + rd) * (maxd + 1)) * L;
+            for (uint32_t e = 1; e <= D; e++)
+#pragma unroll
+                for (int w = 0; w < L; w++) m[(size_t)(e - 1) * L + w] = ev[g][e][w];
+        }
+    uint32_t n = 0;
+    for (uint32_t g = 0; g < ng; g++)
+        for (uint32_t e = 1; e <= degree[g]; e++) {
+            for (uint32_t j = lane; j < FB; j += 32) buf[n + j] = field_byte<L>(f, ev[g][e], j);
+            n += FB;
+        }
+    __syncwarp();
+    warp_update(h, buf, n);
+    uint64_t *xs = reinterpret_cast<uint64_t *>(buf + kFsBufBytes - 128), *rs = xs + 4;
+    if (lane == 0) xof_words<L>(h, xs);
+    __syncwarp();
+    for (uint32_t j = lane; j < 8 * L + 2; j += 32)
+        buf[j] = j == 0 ? 0x12 : j == 8 * L + 1 ? 0x34 : (uint8_t)(xs[(j - 1) >> 3] >> (8 * ((j - 1) & 7)));
+    __syncwarp();
+    warp_update(h, buf, 8 * L + 2);
+    if (lane == 0) {
+        uint64_t x[L], r[L];
+#pragma unroll
+        for (int w = 0; w < L; w++) x[w] = xs[w];
+        fmul<L>(x, f.r2, f.p, f.n0, r);
+#pragma unroll
+        for (int w = 0; w < L; w++) {
+            rs[w] = r[w];
+            r_out[w] = r[w];
+            point[(size_t)rd * L + w] = r[w];
+        }
+    }
+    __syncwarp();
+    for (uint32_t j = lane; j < FB; j += 32) buf[j] = field_byte<L>(f, rs, j);
+    __syncwarp();
+    warp_update(h, buf, FB);
 }
 
 template <int L>
 __global__ void __launch_bounds__(256) k_sc_fs(FsArgs a, FieldCfg f) {
-    __shared__ uint64_t red[256][L];
     __shared__ uint64_t ev[kScMaxGroups][kScMaxDeg + 1][L];
-    const uint32_t tid = threadIdx.x;
+    __shared__ __align__(16) uint8_t hbuf[sizeof(b3::Hasher)];
+    __shared__ __align__(16) uint8_t fsbuf[kFsBufBytes];
+    b3::Hasher *h = reinterpret_cast<b3::Hasher *>(hbuf);
+    hasher_copy(h, a.h);
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x / 32;
+    // warp w sums the block partials of evaluations t = w, w + nwarps, ...
     for (uint32_t g = 0; g < a.ng; g++) {
         const uint32_t D = a.degree[g];
-        for (uint32_t t = 0; t <= D; t++) {
+        for (uint32_t t = warp; t <= D; t += nwarps) {
             uint64_t acc[L] = {};
-            for (uint32_t bk = tid; bk < a.blocks; bk += blockDim.x)
+            for (uint32_t bk = lane; bk < a.blocks; bk += 32)
                 fadd<L>(acc, a.partials[g] + ((size_t)bk * (D + 1) + t) * L, f.p);
+            for (int off = 16; off > 0; off >>= 1) {
+                uint64_t o[L];
 #pragma unroll
-            for (int w = 0; w < L; w++) red[tid][w] = acc[w];
-            __syncthreads();
-            for (uint32_t h = blockDim.x / 2; h > 0; h >>= 1) {
-                if (tid < h) fadd<L>(red[tid], red[tid + h], f.p);
-                __syncthreads();
+                for (int w = 0; w < L; w++) o[w] = __shfl_down_sync(0xffffffffu, acc[w], off);
+                fadd<L>(acc, o, f.p);
             }
-            if (tid == 0)
+            if (lane == 0)
 #pragma unroll
-                for (int w = 0; w < L; w++) ev[g][t][w] = red[0][w];
-            __syncthreads();
+                for (int w = 0; w < L; w++) ev[g][t][w] = acc[w];
         }
     }
-    if (tid != 0) return;
-    for (uint32_t g = 0; g < a.ng; g++) {
-        const uint32_t D = a.degree[g];
-        if (a.rd == 0) {
-            uint64_t c[L];
-#pragma unroll
-            for (int w = 0; w < L; w++) c[w] = ev[g][0][w];
-            if (D > 0) fadd<L>(c, ev[g][1], f.p);
-#pragma unroll
-            for (int w = 0; w < L; w++) a.claimed[(size_t)g * L + w] = c[w];
-        }
-        uint64_t *m = a.msgs + (((size_t)g * a.nvars + a.rd) * (a.maxd + 1)) * L;
-        for (uint32_t e = 1; e <= D; e++)
-#pragma unroll
-            for (int w = 0; w < L; w++) m[(size_t)(e - 1) * L + w] = ev[g][e][w];
-        if (!a.multi)
-            for (uint32_t e = 1; e <= D; e++) dev_absorb_field<L>(a.h, f, ev[g][e]);
-    }
-    if (a.multi)
-        for (uint32_t g = 0; g < a.ng; g++)
-            for (uint32_t e = 1; e <= a.degree[g]; e++) dev_absorb_field<L>(a.h, f, ev[g][e]);
-    // get_field_challenge: XOF of 8L bytes, absorbed as 0x12 | bytes | 0x34, read
-    // as an integer and put into Montgomery form; then absorbed as a field element
-    uint8_t b[8 * L + 2];
-    a.h->xof(b + 1, 8 * L);
-    b[0] = 0x12;
-    b[8 * L + 1] = 0x34;
-    a.h->update(b, 8 * L + 2);
-    uint64_t x[L], r[L];
-#pragma unroll
-    for (int w = 0; w < L; w++) {
-        x[w] = 0;
-        for (int k = 0; k < 8; k++) x[w] |= (uint64_t)b[1 + 8 * w + k] << (8 * k);
-    }
-    fmul<L>(x, f.r2, f.p, f.n0, r);
-    dev_absorb_field<L>(a.h, f, r);
-#pragma unroll
-    for (int w = 0; w < L; w++) {
-        a.r[w] = r[w];
-        a.point[(size_t)a.rd * L + w] = r[w];
-    }
+    __syncthreads();
+    if (warp == 0)
+        fs_round<L>(h, f, ev, a.degree, a.ng, a.multi, a.rd, a.maxd, a.nvars, a.msgs, a.claimed,
+                    a.point, a.r, fsbuf);
+    __syncthreads();
+    hasher_copy(a.h, h);
 }
 
 // Per-group device state, carved out of the context's sumcheck arena.
@@ -504,6 +619,7 @@ void f_from_u64_host(const FieldCfg &f, uint64_t v, uint64_t *out) {
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
 
 template <int L>
 zg_status sumcheck_prove_t(zg_ctx *ctx, zg_transcript *t, uint32_t nvars, int multi,

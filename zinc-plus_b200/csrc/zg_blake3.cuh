@@ -4,6 +4,7 @@
 // its Fiat-Shamir transcript is a blake3::Hasher with XOF output
 // (transcript/src/lib.rs:12-77).
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 
@@ -114,6 +115,34 @@ ZG_HD void compress_cv(uint32_t cv[8], const uint32_t m[16], uint64_t counter, u
     for (int i = 0; i < 8; i++) cv[i] = out[i];
 }
 
+#ifdef __CUDA_ARCH__
+// The compression out of line: one copy of its unrolled code for every call
+// of the incremental hasher (the transcript, one thread), instead of one per
+// call site.  The leaf and tree kernels inline it.
+static __device__ __noinline__ void compress_ool(const uint32_t cv[8], const uint32_t m[16],
+                                                 uint64_t counter, uint32_t block_len,
+                                                 uint32_t flags, uint32_t out[16]) {
+    compress(cv, m, counter, block_len, flags, out);
+}
+#endif
+
+// The compression used by the incremental hasher: out of line on the device.
+ZG_HD void compress_h(const uint32_t cv[8], const uint32_t m[16], uint64_t counter,
+                      uint32_t block_len, uint32_t flags, uint32_t out[16]) {
+#ifdef __CUDA_ARCH__
+    compress_ool(cv, m, counter, block_len, flags, out);
+#else
+    compress(cv, m, counter, block_len, flags, out);
+#endif
+}
+
+ZG_HD void compress_cv_h(uint32_t cv[8], const uint32_t m[16], uint64_t counter,
+                         uint32_t block_len, uint32_t flags) {
+    uint32_t out[16];
+    compress_h(cv, m, counter, block_len, flags, out);
+    for (int i = 0; i < 8; i++) cv[i] = out[i];
+}
+
 ZG_HD uint32_t load_le32(const uint8_t *p) {
     return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
 }
@@ -156,6 +185,18 @@ ZG_HD void chunk_hash(const Loader &load, uint32_t n, uint64_t counter, bool roo
     for (int i = 0; i < 8; i++) out[i] = cv[i];
 }
 
+// Non-root parent chaining value through the hasher's compression.
+ZG_HD void parent_h(const uint32_t l[8], const uint32_t r[8], uint32_t out[8]) {
+    uint32_t m[16], cv[8];
+    for (int i = 0; i < 8; i++) {
+        m[i] = l[i];
+        m[8 + i] = r[i];
+        cv[i] = iv(i);
+    }
+    compress_cv_h(cv, m, 0, 64, PARENT);
+    for (int i = 0; i < 8; i++) out[i] = cv[i];
+}
+
 // Incremental hasher with XOF finalisation (host; used by the transcript).
 struct Hasher {
     uint32_t cv[8];
@@ -170,32 +211,47 @@ struct Hasher {
     ZG_HDN void reset() {
         for (int i = 0; i < 8; i++) cv[i] = iv(i);
         chunk_counter = 0;
-        for (int i = 0; i < 64; i++) block[i] = 0;
+        clear_block();
         block_len = 0;
         blocks_compressed = 0;
         stack_len = 0;
     }
     ZG_HDN uint32_t chunk_len() const { return 64 * blocks_compressed + block_len; }
     ZG_HDN uint32_t start_flag() const { return blocks_compressed == 0 ? CHUNK_START : 0; }
+    // The block as words / cleared.  On the device, 32-bit accesses (the block
+    // sits at a multiple of 8 bytes in the struct); bytes on the host.
+    ZG_HDN void clear_block() {
+#ifdef __CUDA_ARCH__
+        uint32_t *w = reinterpret_cast<uint32_t *>(block);
+        for (int i = 0; i < 16; i++) w[i] = 0;
+#else
+        for (int i = 0; i < 64; i++) block[i] = 0;
+#endif
+    }
     ZG_HDN void block_words(uint32_t m[16]) const {
+#ifdef __CUDA_ARCH__
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(block);
+        for (int i = 0; i < 16; i++) m[i] = w[i];
+#else
         for (int i = 0; i < 16; i++) m[i] = load_le32(block + 4 * i);
+#endif
     }
     ZG_HDN void finish_chunk_and_push() {
         uint32_t m[16];
         block_words(m);
         uint32_t c[8];
         for (int i = 0; i < 8; i++) c[i] = cv[i];
-        compress_cv(c, m, chunk_counter, block_len, start_flag() | CHUNK_END);
+        compress_cv_h(c, m, chunk_counter, block_len, start_flag() | CHUNK_END);
         uint64_t total = chunk_counter + 1;
         while ((total & 1) == 0) {
-            parent_cv(stack[--stack_len], c, false, c);
+            parent_h(stack[--stack_len], c, c);
             total >>= 1;
         }
         for (int i = 0; i < 8; i++) stack[stack_len][i] = c[i];
         stack_len++;
         chunk_counter++;
         for (int i = 0; i < 8; i++) cv[i] = iv(i);
-        for (int i = 0; i < 64; i++) block[i] = 0;
+        clear_block();
         block_len = 0;
         blocks_compressed = 0;
     }
@@ -205,17 +261,24 @@ struct Hasher {
             if (block_len == 64) {
                 uint32_t m[16];
                 block_words(m);
-                compress_cv(cv, m, chunk_counter, 64, start_flag());
+                compress_cv_h(cv, m, chunk_counter, 64, start_flag());
                 blocks_compressed++;
                 block_len = 0;
-                for (int i = 0; i < 64; i++) block[i] = 0;
+                clear_block();
             }
-            size_t room = 64 - block_len;
-            size_t chunk_room = CHUNK_LEN - chunk_len();
-            size_t take = n < room ? n : room;
-            if (take > chunk_room) take = chunk_room;
-            for (size_t i = 0; i < take; i++) block[block_len + i] = in[i];
-            block_len += (uint32_t)take;
+            // (the chunk has room for the rest of the block: at most 15 blocks
+            // are compressed before its last one)
+            const uint32_t bl = block_len;
+            const uint32_t take = n < 64 - bl ? (uint32_t)n : 64 - bl;
+            // Local restrict pointers: through `this`, every byte store could
+            // alias block_len and force a reload per byte.
+            uint8_t *__restrict__ dst = block + bl;
+            const uint8_t *__restrict__ src = in;
+#ifdef __CUDA_ARCH__
+#pragma unroll 8
+#endif
+            for (uint32_t i = 0; i < take; i++) dst[i] = src[i];
+            block_len = bl + take;
             in += take;
             n -= take;
         }
@@ -230,7 +293,7 @@ struct Hasher {
         for (int s = (int)stack_len - 1; s >= 0; s--) {
             uint32_t c[8];
             for (int i = 0; i < 8; i++) c[i] = ocv[i];
-            compress_cv(c, m, counter, blen, flags);
+            compress_cv_h(c, m, counter, blen, flags);
             for (int i = 0; i < 8; i++) {
                 m[i] = stack[s][i];
                 m[8 + i] = c[i];
@@ -243,7 +306,7 @@ struct Hasher {
         uint64_t ob = 0;
         while (n) {
             uint32_t w[16];
-            compress(ocv, m, ob++, blen, flags | ROOT, w);
+            compress_h(ocv, m, ob++, blen, flags | ROOT, w);
             uint8_t bytes[64];
             for (int i = 0; i < 16; i++) store_le32(bytes + 4 * i, w[i]);
             size_t take = n < 64 ? n : 64;
@@ -253,6 +316,8 @@ struct Hasher {
         }
     }
 };
+
+static_assert(offsetof(Hasher, block) % 4 == 0, "the block is read and cleared as words on the device");
 
 // One-shot hash of a host buffer.
 inline void hash(const uint8_t *in, size_t n, uint8_t out[32]) {
