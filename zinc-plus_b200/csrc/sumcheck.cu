@@ -25,9 +25,12 @@ namespace {
 
 constexpr int kScThreads = 256;
 // threads per pair: 1 when pairs fill the GPU, more when they do not (each
-// thread's share of a pair is a long chain of dependent field products)
+// thread's share of a pair is a long chain of dependent field products).  The
+// thresholds are measured (CPR group at 2^18 points, 2.18 -> 1.90 ms, from
+// 2^19 / 2^15): splitting a pair costs shuffles and idle threads, worth it
+// only once a round has fewer than 2^16 pairs.
 constexpr int kScSubMid = 4, kScSubMax = 16;
-constexpr size_t kScSplitBelow = 1u << 19, kScSplitMore = 1u << 15;
+constexpr size_t kScSplitBelow = 1u << 16, kScSplitMore = 1u << 13;
 constexpr int kScMaxDeg = 8;
 
 // fix_variables_with_config (poly/src/mle/dense.rs:243-279), one variable.
