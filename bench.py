@@ -886,6 +886,10 @@ def run_ours(args):
             info = pp.info
             per_leaf = max(1, (info.num_rows * (8 * D if ek else 16) + 63) // 64)
             comp = info.codeword_len * per_leaf
+            if per_leaf <= 16 and info.codeword_len % 128 == 0:
+                # the leaf kernel also reduces each block's 128 leaves to their
+                # subtree root: 127 parent compressions per 128 leaves
+                comp += info.codeword_len // 128 * 127
             alu_per_comp = 584  # ALU-pipe instructions per compression, ncu (profiles/)
             sm_mhz = (clock_info or {}).get("sm_mhz") or 1965.0
             sms = torch.cuda.get_device_properties(local).multi_processor_count
