@@ -202,6 +202,39 @@ __global__ void __launch_bounds__(128) k_leaf_chunks_coalesced(const uint8_t *__
     }
 }
 
+// The same merge for a power-of-two chunk count n <= 32, in parallel: a leaf's
+// n chaining values sit in n consecutive lanes (32 / n leaves per warp) and are
+// reduced pairwise, log2(n) levels of parents (for such n the hasher's stack
+// discipline builds exactly this perfect tree), the last with the root flag.
+// One thread per leaf runs n - 1 dependent compressions; here the chain is
+// log2(n) deep, at the cost of n / 2 + n / 4 + ... idle lanes per level, which
+// pays only while the leaves are too few to fill the GPU.
+__global__ void __launch_bounds__(128) k_leaf_merge_pow2(const uint32_t *__restrict__ cvs,
+                                                         uint32_t width, uint32_t nchunks,
+                                                         uint32_t *__restrict__ leaves,
+                                                         uint32_t tree_log) {
+    const uint32_t lane = threadIdx.x & 31;
+    const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (leaf, chunk) item
+    const size_t total = (size_t)width * nchunks;
+    uint32_t cur[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) cur[i] = g < total ? cvs[g * 8 + i] : 0u;
+    const uint32_t c = lane & (nchunks - 1);  // chunk index within the leaf
+    const uint32_t levels = 31 - __clz(nchunks);
+    for (uint32_t lev = 1; lev <= levels; lev++) {
+        const uint32_t half = 1u << (lev - 1);
+        uint32_t r[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) r[i] = __shfl_down_sync(0xffffffffu, cur[i], half);
+        if ((c & ((half << 1) - 1)) == 0) b3::parent_cv(cur, r, lev == levels, cur);
+    }
+    if (c == 0 && g < total) {
+        const size_t node = leaf_node((uint32_t)(g / nchunks), tree_log);
+#pragma unroll
+        for (int i = 0; i < 8; i++) leaves[node * 8 + i] = cur[i];
+    }
+}
+
 // Merge the chunk chaining values of each leaf in BLAKE3 tree order (the
 // incremental hasher's stack discipline), root flag on the final parent.
 __global__ void __launch_bounds__(128) k_leaf_merge(const uint32_t *__restrict__ cvs, uint32_t width,
@@ -345,7 +378,13 @@ zg_status launch_leaf_hash(zg_ctx *ctx, const uint8_t *cw_d, uint32_t width, uin
         k_leaf_chunks<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cw_d, width, leaf_bytes, nchunks, cvs);
     ZG_KEND(ctx, s);
     ZG_KBEGIN(ctx, s, "k_leaf_merge");
-    k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, nchunks, leaves, tree_log);
+    // few leaves: one warp per leaf's chunks (the serial merge would leave most
+    // SMs idle); many leaves: one thread per leaf, 32x fewer warp instructions
+    if (nchunks <= 32 && (nchunks & (nchunks - 1)) == 0 && width < 16384)
+        k_leaf_merge_pow2<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(cvs, width, nchunks, leaves,
+                                                                      tree_log);
+    else
+        k_leaf_merge<<<(width + 127) / 128, 128, 0, s>>>(cvs, width, nchunks, leaves, tree_log);
     ZG_KEND(ctx, s);
     return ZG_OK;
 }

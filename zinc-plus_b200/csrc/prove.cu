@@ -137,19 +137,39 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
     }
 }
 
-__global__ void __launch_bounds__(256) k_combined_row(const uint64_t *__restrict__ wprime,
-                                                      const i128 *__restrict__ coeffs,
-                                                      uint32_t batch, uint32_t num_rows,
-                                                      uint32_t row_len, uint32_t comb_limbs,
-                                                      uint64_t *__restrict__ out) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= row_len) return;
+// blockDim (32, Y): 32 columns per block, the batch x num_rows products of a
+// column split over Y threads, whose partial sums (exact, wrapping at
+// 64 * comb_limbs bits, so their order is free) are added in shared memory.
+// With one thread per column, a tall matrix (RAA: 256 rows of 256) ran a
+// chain of 256 dependent multiply-adds on 256 threads.
+__global__ void __launch_bounds__(1024) k_combined_row(const uint64_t *__restrict__ wprime,
+                                                       const i128 *__restrict__ coeffs,
+                                                       uint32_t batch, uint32_t num_rows,
+                                                       uint32_t row_len, uint32_t comb_limbs,
+                                                       uint64_t *__restrict__ out) {
+    extern __shared__ uint64_t part[];  // [Y][32][comb_limbs]
+    const uint32_t tx = threadIdx.x, ty = threadIdx.y, Y = blockDim.y;
+    const uint32_t c = blockIdx.x * 32 + tx;
     uint64_t acc[MAX_COMB_LIMBS];
     for (uint32_t k = 0; k < comb_limbs; k++) acc[k] = 0;
-    for (uint32_t b = 0; b < batch; b++)
-        for (uint32_t j = 0; j < num_rows; j++)
-            wide_mul_i128_add(acc, wprime + (((size_t)b * num_rows + j) * row_len + c) * comb_limbs,
-                              coeffs[j], (int)comb_limbs);
+    const uint32_t total = batch * num_rows;
+    if (c < row_len)
+        for (uint32_t q = ty; q < total; q += Y)  // q = b * num_rows + j
+            wide_mul_i128_add(acc, wprime + ((size_t)q * row_len + c) * comb_limbs, coeffs[q % num_rows],
+                              (int)comb_limbs);
+    for (uint32_t k = 0; k < comb_limbs; k++) part[((size_t)ty * 32 + tx) * comb_limbs + k] = acc[k];
+    __syncthreads();
+    if (ty != 0 || c >= row_len) return;
+    for (uint32_t y = 1; y < Y; y++) {
+        const uint64_t *p = part + ((size_t)y * 32 + tx) * comb_limbs;
+        uint64_t carry = 0;
+        for (uint32_t k = 0; k < comb_limbs; k++) {
+            const uint64_t t = acc[k] + carry, c1 = t < carry;
+            const uint64_t u = t + p[k], c2 = u < t;
+            acc[k] = u;
+            carry = c1 | c2;
+        }
+    }
     for (uint32_t k = 0; k < comb_limbs; k++) out[(size_t)c * comb_limbs + k] = acc[k];
 }
 
@@ -220,9 +240,15 @@ zg_status launch_project_rows(zg_ctx *ctx, const ProjectArgs &a, cudaStream_t s)
 
 zg_status launch_combined_and_openings(zg_ctx *ctx, const CombineArgs &a, cudaStream_t s) {
     ZG_KBEGIN(ctx, s, "k_combined_row");
-    k_combined_row<<<(a.row_len + 255) / 256, 256, 0, s>>>(a.wprime, a.coeffs, a.batch,
-                                                           a.num_rows, a.row_len, a.comb_limbs,
-                                                           a.comb_out);
+    // Y threads per column: about 2^17 threads in all, at most the rows, at most
+    // 32, and their partials within 48 KB of shared memory
+    uint32_t Y = 1;
+    const uint32_t rows = a.batch * a.num_rows;
+    while (Y < 32 && 2 * Y <= rows && (size_t)a.row_len * Y < (1u << 17) &&
+           (size_t)2 * Y * 32 * a.comb_limbs * 8 <= 48 * 1024)
+        Y *= 2;
+    k_combined_row<<<(a.row_len + 31) / 32, dim3(32, Y), (size_t)Y * 32 * a.comb_limbs * 8, s>>>(
+        a.wprime, a.coeffs, a.batch, a.num_rows, a.row_len, a.comb_limbs, a.comb_out);
     ZG_KEND(ctx, s);
     ZG_KBEGIN(ctx, s, "k_openings");
     k_openings<<<a.n_open, 128, 0, s>>>(a.cw, a.leaf_bytes, a.tree, a.depth, a.width, a.idxs,
