@@ -121,9 +121,22 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
         uint64_t *wo = wprime + e * comb_limbs;
         const uint64_t sg = (w3[2] >> 63) ? ~0ull : 0ull;
         for (uint32_t k = 0; k < comb_limbs; k++) wo[k] = k < 3 ? w3[k] : sg;
-        uint64_t fw[L];
-        from_signed<L>(w3, 3, f, fw);
-        fmul<L>(fw, q1 + (size_t)c * L, f.p, f.n0, fe);
+        // |w3| < 2^134 < p (at most 64 alphas of 128 bits, or one 64-bit value),
+        // so its magnitude is a field element as it stands.  Times q1 (the
+        // Montgomery form Q R of the eq entry) it gives the plain residue of
+        // |w3| Q: one product where the conversion to Montgomery form took
+        // another.  The block's plain sum is put into Montgomery form once,
+        // times R^2 (the sum is linear, so the same value).
+        const bool neg = (w3[2] >> 63) != 0;
+        uint64_t mag[L];
+        uint64_t cy = neg ? 1 : 0;
+        for (int w = 0; w < L; w++) {
+            const uint64_t v = w < 3 ? (neg ? ~w3[w] : w3[w]) : 0;
+            mag[w] = v + cy;
+            cy = mag[w] < cy;
+        }
+        fmul<L>(mag, q1 + (size_t)c * L, f.p, f.n0, fe);
+        if (neg) fneg<L>(fe, f.p);
     }
     for (int w = 0; w < L; w++) s_red[threadIdx.x * L + w] = fe[w];
     __syncthreads();
@@ -133,7 +146,9 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
     }
     if (threadIdx.x == 0) {
         uint64_t *po = partial + (((size_t)b * num_rows + j) * gridDim.x + blockIdx.x) * L;
-        for (int w = 0; w < L; w++) po[w] = s_red[w];
+        uint64_t m[L];
+        fmul<L>(&s_red[0], f.r2, f.p, f.n0, m);
+        for (int w = 0; w < L; w++) po[w] = m[w];
     }
 }
 
