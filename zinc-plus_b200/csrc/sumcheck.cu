@@ -120,8 +120,11 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
                                         const uint64_t *__restrict__ r, uint32_t K, const ScComb &c,
                                         const FieldCfg &f, const Fe<L> &pf, size_t b, bool active,
                                         uint32_t sub, uint64_t (&ev)[D + 1][L]) {
+    // the out-of-line form also keeps its loops over t rolled: it serves the
+    // small rounds, whose time is the cold fetch of the kernel's code
+    constexpr int kUT = OUTLINE ? 1 : 32;
     const size_t len = fold ? src_len / 2 : src_len;
-#pragma unroll
+#pragma unroll kUT
     for (int t = 0; t <= D; t++)
 #pragma unroll
         for (int w = 0; w < L; w++) ev[t][w] = 0;
@@ -171,7 +174,7 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
                 any_lin = true;
                 continue;
             }
-#pragma unroll
+#pragma unroll kUT
             for (int t = 0; t <= D; t++)
 #pragma unroll
                 for (int w = 0; w < L; w++) pr[t][w] = cf[w];
@@ -181,7 +184,7 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
                 load_el<L>(v, cur);
                 load_el<L>(v + L, st);
                 fsub<L>(st, cur, f.p);
-#pragma unroll
+#pragma unroll kUT
                 for (int t = 0; t <= D; t++) {
                     uint64_t o[L];
                     fmul_c<L, OUTLINE>(pr[t], cur, pf, f.n0, o);
@@ -190,7 +193,7 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
                     if (t < D) fadd<L>(cur, st, f.p);
                 }
             }
-#pragma unroll
+#pragma unroll kUT
             for (int t = 0; t <= D; t++) fadd<L>(ev[t], pr[t], f.p);
         }
         if (D >= 2 && D <= 6 && any_lin) {
@@ -202,7 +205,7 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
             }
             fsub<L>(d, lin0, f.p);
             fadd<L>(ev[0], lin0, f.p);
-#pragma unroll
+#pragma unroll kUT
             for (int t = 1; t <= D; t++) {
                 if (t > 1) fadd<L>(cur, d, f.p);
                 fadd<L>(ev[t], cur, f.p);
@@ -210,9 +213,9 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
         }
     }
     // the pair's full sum of products, in all its threads
-#pragma unroll
+#pragma unroll kUT
     for (int off = 1; off < kScSub; off <<= 1) {
-#pragma unroll
+#pragma unroll kUT
         for (int t = 0; t <= D; t++) {
             uint64_t o[L];
 #pragma unroll
@@ -228,7 +231,7 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
 #pragma unroll
         for (int w = 0; w < L; w++) keep[w] = 0;
         if (active && (int)sub <= D) {
-#pragma unroll
+#pragma unroll kUT
             for (int t = 0; t <= D; t++)
                 if (t == (int)sub)
 #pragma unroll
@@ -249,12 +252,12 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
                 for (int w = 0; w < L; w++) keep[w] = o[w];
             }
         }
-#pragma unroll
+#pragma unroll kUT
         for (int t = 0; t <= D; t++)
 #pragma unroll
             for (int w = 0; w < L; w++) ev[t][w] = t == (int)sub ? keep[w] : 0;
     } else if (sub != 0) {
-#pragma unroll
+#pragma unroll kUT
         for (int t = 0; t <= D; t++)
 #pragma unroll
             for (int w = 0; w < L; w++) ev[t][w] = 0;
@@ -268,7 +271,7 @@ __device__ __forceinline__ void sc_pair(const uint64_t *__restrict__ src, size_t
             fsub<L>(st, cur, f.p);
             load_el<L>(c.fa + (size_t)q * L, fa);
             load_el<L>(c.fb + (size_t)q * L, fbv);
-#pragma unroll
+#pragma unroll kUT
             for (int t = 0; t <= D; t++) {
                 uint64_t fv[L], o[L];
                 fmul_c<L, OUTLINE>(fbv, cur, pf, f.n0, fv);
@@ -292,6 +295,7 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
                                                          uint32_t K, ScComb c, FieldCfg f,
                                                          uint64_t *__restrict__ partials) {
     __shared__ uint64_t red[kScThreads / 32][(D + 1) * L];
+    constexpr int kUT = kScSub == kScSubMax ? 1 : 32;  // rolled in the small rounds' form
     Fe<L> pf;
 #pragma unroll
     for (int w = 0; w < L; w++) pf.w[w] = f.p[w];
@@ -303,9 +307,9 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
                                                 sub, ev);
     // warp tree reduction, then across the block's warps
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
+#pragma unroll kUT
     for (int off = 16; off > 0; off >>= 1) {
-#pragma unroll
+#pragma unroll kUT
         for (int t = 0; t <= D; t++) {
             uint64_t o[L];
 #pragma unroll
@@ -314,20 +318,20 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
         }
     }
     if (lane == 0)
-#pragma unroll
+#pragma unroll kUT
         for (int t = 0; t <= D; t++)
 #pragma unroll
             for (int w = 0; w < L; w++) red[warp][t * L + w] = ev[t][w];
     __syncthreads();
     if (warp == 0) {
         const uint32_t nw = blockDim.x / 32;
-#pragma unroll
+#pragma unroll kUT
         for (int t = 0; t <= D; t++)
 #pragma unroll
             for (int w = 0; w < L; w++) ev[t][w] = lane < nw ? red[lane][t * L + w] : 0;
-#pragma unroll
+#pragma unroll kUT
         for (int off = 16; off > 0; off >>= 1) {
-#pragma unroll
+#pragma unroll kUT
             for (int t = 0; t <= D; t++) {
                 uint64_t o[L];
 #pragma unroll
@@ -336,7 +340,7 @@ __global__ void __launch_bounds__(kScThreads, 2) k_sc_round(const uint64_t *__re
             }
         }
         if (lane == 0)
-#pragma unroll
+#pragma unroll kUT
             for (int t = 0; t <= D; t++)
 #pragma unroll
                 for (int w = 0; w < L; w++) partials[((size_t)blockIdx.x * (D + 1) + t) * L + w] = ev[t][w];
