@@ -1222,7 +1222,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch", type=int, default=64, help="requests per batched step")
+    ap.add_argument("--batch", type=int, default=128, help="requests per batched step")
     ap.add_argument("--lanes", type=int, default=16, help="concurrent lanes of the batched form")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--cpu-seconds-per-config", type=float, default=4.0,
