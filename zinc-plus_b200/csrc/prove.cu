@@ -121,11 +121,11 @@ __global__ void __launch_bounds__(256) k_project_rows(const void *__restrict__ e
         uint64_t *wo = wprime + e * comb_limbs;
         const uint64_t sg = (w3[2] >> 63) ? ~0ull : 0ull;
         for (uint32_t k = 0; k < comb_limbs; k++) wo[k] = k < 3 ? w3[k] : sg;
-        // |w3| < 2^134 < p (at most 64 alphas of 128 bits, or one 64-bit value),
-        // so its magnitude is a field element as it stands.  Times q1 (the
-        // Montgomery form Q R of the eq entry) it gives the plain residue of
-        // |w3| Q: one product where the conversion to Montgomery form took
-        // another.  The block's plain sum is put into Montgomery form once,
+        // |w3| < 2^134 (at most 64 alphas of 128 bits, or one 64-bit value) is
+        // below R, which is all the Montgomery product asks of its first operand.
+        // Times q1 (the Montgomery form Q R of the eq entry) it gives the plain
+        // residue of |w3| Q: one product where the conversion to Montgomery form
+        // took another.  The block's plain sum is put into Montgomery form once,
         // times R^2 (the sum is linear, so the same value).
         const bool neg = (w3[2] >> 63) != 0;
         uint64_t mag[L];
