@@ -182,28 +182,32 @@ __global__ void __launch_bounds__(256) k_lifted_bin(const uint64_t *__restrict__
                                                     uint64_t dmask, const uint64_t *__restrict__ eq, FieldCfg f,
                                                     uint64_t *__restrict__ partials) {
     __shared__ Lazy<L> red[256];
+    // a tile of 256 inputs: their cells and eq entries, loaded coalesced, then
+    // read by every lane as shared-memory broadcasts (one load per warp and
+    // input from L2 left the kernel waiting: 15 long-scoreboard stalls per issue)
+    constexpr uint32_t kTile = 256;
+    __shared__ uint64_t sx[kTile];
+    __shared__ uint64_t se[kTile * L];
     const uint32_t l = threadIdx.x, w = threadIdx.y, rows = blockDim.y;
+    const uint32_t tid = w * LB + l, nthr = LB * rows;
     const size_t n = (size_t)1 << nv, b0 = (size_t)blockIdx.x << kLiftChunkLog;
     const size_t b1 = b0 + ((size_t)1 << kLiftChunkLog) < n ? b0 + ((size_t)1 << kLiftChunkLog) : n;
     const uint64_t *col = bin + ((size_t)blockIdx.y << nv);
     Lazy<L> acc;
     lazy_zero(acc);
-    size_t b = b0 + w;
-    for (; b + 7 * rows < b1; b += 8 * rows) {  // eight inputs in flight
-        uint64_t x[8], e[8][L];
+    for (size_t tb = b0; tb < b1; tb += kTile) {
+        const uint32_t cnt = b1 - tb < kTile ? (uint32_t)(b1 - tb) : kTile;
+        for (uint32_t i = tid; i < cnt; i += nthr) sx[i] = col[tb + i] & dmask;
+        for (uint32_t i = tid; i < cnt * L; i += nthr) se[i] = eq[tb * L + i];
+        __syncthreads();
+        uint32_t j = w;
+        for (; j + 7 * rows < cnt; j += 8 * rows)
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            x[u] = col[b + u * rows];
-#pragma unroll
-            for (int k = 0; k < L; k++) e[u][k] = eq[(b + u * rows) * L + k];
-        }
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-            if (((x[u] & dmask) >> l) & 1u) lazy_add<L>(acc, e[u]);
-    }
-    for (; b < b1; b += rows) {
-        const uint64_t x = col[b] & dmask;
-        if ((x >> l) & 1u) lazy_add<L>(acc, eq + b * L);
+            for (int u = 0; u < 8; u++)
+                if ((sx[j + u * rows] >> l) & 1u) lazy_add<L>(acc, se + (size_t)(j + u * rows) * L);
+        for (; j < cnt; j += rows)
+            if ((sx[j] >> l) & 1u) lazy_add<L>(acc, se + (size_t)j * L);
+        __syncthreads();
     }
     const uint32_t t = w * LB + l;
     red[t] = acc;
