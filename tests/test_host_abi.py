@@ -70,6 +70,26 @@ def test_transcript_and_prime_match_oracle(zipgpu, oracle):
     assert t.get_challenge(32) == o.challenge(32)
 
 
+def test_transcript_across_block_and_chunk_boundaries(zipgpu, oracle):
+    """The library's host transcript (the incremental BLAKE3 hasher shared with
+    the device's Fiat-Shamir step) against the oracle's, whose BLAKE3 is pinned
+    to the blake3 package: absorbs of random sizes cross 64-byte blocks and
+    1 KiB chunks many times (chunk completions, stack merges), with challenges
+    read between them."""
+    rng = np.random.default_rng(0xB1A)
+    t = zipgpu.PcsProverTranscript()
+    o = oracle.Transcript()
+    for _ in range(120):
+        n = int(rng.choice([0, 1, 3, 26, 52, 63, 64, 65, 127, 1023, 1024, 1025, int(rng.integers(0, 3000))]))
+        b = rng.bytes(n)
+        t.absorb(b)
+        o.absorb(b)
+        if rng.random() < 0.4:
+            k = int(rng.integers(1, 80))
+            assert t.get_challenge(k) == o.challenge(k)
+    assert t.get_challenge(32) == o.challenge(32)
+
+
 @pytest.mark.parametrize("code_kind,row_len", [(0, 1024), (0, 64), (1, 64)])
 def test_encode_wide_matches_oracle(zipgpu, oracle, code_kind, row_len):
     pp = params_for(zipgpu, 1, 32, code_kind, 12, row_len, device=False)
